@@ -1,0 +1,47 @@
+// case.cuh -- one simulation case resident on one GPU (internal).
+#pragma once
+#include <vector>
+
+#include "../../include/impact_b200.h"
+#include "common.cuh"
+#include "solver.cuh"
+
+namespace impact {
+
+// per-axis row sums used by get_dtime: sum_l |cpp(l,i)| and sum_l |cp1(l,i)|
+struct DtRows {
+  const double* spp[3];
+  const double* sp1[3];
+};
+
+struct CaseState {
+  int device = 0;
+  int precision = 0;
+  Geom g{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  // coefficient tables, FP64 and FP32 copies, in one allocation each
+  double* coef64 = nullptr;
+  float* coef32 = nullptr;
+  Coeffs<double> c64{};
+  Coeffs<float> c32{};
+  DtRows dt{};
+  // fields
+  double* f[IMPACT_B200_NFIELDS] = {};
+  double* work[3] = {};   // velocities interpolated to pressure points
+  uint8_t* label = nullptr;
+  // FP64 Krylov work (8 fields), or the mixed-precision set
+  KrylovWork<double> kw64{};
+  MixedWork mw{};
+  double* partial = nullptr;     // reduction scratch of the step kernels
+  double* dscal = nullptr;       // small device scalars (dt, mean pressure, ...)
+  double* hscal = nullptr;       // pinned host mirror
+  SolverScalars* scal_host = nullptr;
+  std::vector<void*> allocs;
+};
+
+}  // namespace impact
+
+struct impact_b200_case {
+  impact::CaseState s;
+};

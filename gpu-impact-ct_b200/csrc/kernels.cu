@@ -1,0 +1,606 @@
+// kernels.cu -- staggered-grid stencil operators, relaxation sweeps and reductions of the
+// IMPACT fractional step, hand-written for sm_100a.
+//
+// Each kernel restates one reference routine (cited at the kernel).  Stencils wrap their
+// neighbour indices periodically (see common.cuh), so the kernels need no ghost exchange.
+// Thread mapping: a 32 x 8 block covers 32 x-points by 8 y-points of one z-plane; every
+// warp reads 32 consecutive doubles of a row (256 B, sector aligned because the interior
+// starts at offset 4 of a row whose length is a multiple of 8 for cell counts divisible
+// by 8).
+#include "kernels.cuh"
+
+namespace impact {
+
+constexpr int BX = 32, BY = 8;
+
+static inline dim3 grid3(const Geom& g) {
+  return dim3((g.n1 + BX - 1) / BX, (g.n2 + BY - 1) / BY, g.n3);
+}
+
+#define POINT_PROLOGUE                              \
+  const int i = blockIdx.x * BX + threadIdx.x + 1;  \
+  const int j = blockIdx.y * BY + threadIdx.y + 1;  \
+  const int k = blockIdx.z + 1;                     \
+  if (i > g.n1 || j > g.n2) return;
+
+// coordinate / extent / stride of axis a (0,1,2)
+__device__ __forceinline__ int coord(int a, int i, int j, int k) { return a == 0 ? i : (a == 1 ? j : k); }
+__device__ __forceinline__ int extent(const Geom& g, int a) { return a == 0 ? g.n1 : (a == 1 ? g.n2 : g.n3); }
+__device__ __forceinline__ long long stride(const Geom& g, int a) {
+  return a == 0 ? 1LL : (a == 1 ? (long long)g.nx : g.nxy);
+}
+
+// s = sum_{l=LO}^{LO+CNT-1} c(l,row) f(q+l along axis a), in the reference's order.
+template <typename T, int LO, int CNT>
+__device__ __forceinline__ T stencil_axis(const T* __restrict__ c, int row, const T* __restrict__ f,
+                                          long long base, long long st, int q, int n) {
+  const T* cr = c + (long long)row * CNT;
+  T s = cr[0] * __ldg(f + base + (long long)(wrapi(q + LO, n) + 3) * st);
+#pragma unroll
+  for (int l = 1; l < CNT; ++l) s = s + cr[l] * __ldg(f + base + (long long)(wrapi(q + LO + l, n) + 3) * st);
+  return s;
+}
+// same, accumulating into s0 first (divergence for m = 2, 3)
+template <typename T, int LO, int CNT>
+__device__ __forceinline__ T stencil_axis_acc(T s, const T* __restrict__ c, int row,
+                                              const T* __restrict__ f, long long base, long long st,
+                                              int q, int n) {
+  const T* cr = c + (long long)row * CNT;
+#pragma unroll
+  for (int l = 0; l < CNT; ++l) s = s + cr[l] * __ldg(f + base + (long long)(wrapi(q + LO + l, n) + 3) * st);
+  return s;
+}
+// base offset of (i,j,k) with the coordinate along axis a removed (Fortran index -3 there)
+__device__ __forceinline__ long long base_off(const Geom& g, int a, int i, int j, int k) {
+  return off(g, a == 0 ? -3 : i, a == 1 ? -3 : j, a == 2 ? -3 : k);
+}
+
+// ------------------------------------------------------------------------------------
+// gradient (mod_diff.f90:309-414; gradient_kernel.cu): pressure -> velocity point m
+// ------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(BX* BY) k_gradient(int a, Geom g, const T* __restrict__ cG,
+                                                     const T* __restrict__ phi, T* __restrict__ grad) {
+  POINT_PROLOGUE
+  const int q = coord(a, i, j, k);
+  grad[off(g, i, j, k)] = stencil_axis<T, G_LO, NG>(cG, q, phi, base_off(g, a, i, j, k), stride(g, a), q, extent(g, a));
+}
+template <typename T>
+void launch_gradient(int m, const Geom& g, const T* cG, const T* phi, T* grad, cudaStream_t s) {
+  k_gradient<T><<<grid3(g), dim3(BX, BY), 0, s>>>(m - 1, g, cG, phi, grad);
+}
+
+// ------------------------------------------------------------------------------------
+// divergence (mod_diff.f90:52-118; divergence_kernel.cu): m = 1 overwrites, 2,3 accumulate
+// ------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(BX* BY) k_divergence(int a, Geom g, const T* __restrict__ cD,
+                                                       const T* __restrict__ phi, T* __restrict__ div) {
+  POINT_PROLOGUE
+  const int q = coord(a, i, j, k);
+  const long long p = off(g, i, j, k);
+  if (a == 0)
+    div[p] = stencil_axis<T, D_LO, ND>(cD, q, phi, base_off(g, a, i, j, k), 1, q, g.n1);
+  else
+    div[p] = stencil_axis_acc<T, D_LO, ND>(div[p], cD, q, phi, base_off(g, a, i, j, k), stride(g, a), q, extent(g, a));
+}
+template <typename T>
+void launch_divergence(int m, const Geom& g, const T* cD, const T* phi, T* div, cudaStream_t s) {
+  k_divergence<T><<<grid3(g), dim3(BX, BY), 0, s>>>(m - 1, g, cD, phi, div);
+}
+
+// ------------------------------------------------------------------------------------
+// divergence2 (mod_diff.f90:130-215; divergence2_kernel.cu): div = D1 u + D2 v + D3 w
+// ------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T div2_point(const Geom& g, const T* __restrict__ cD1, const T* __restrict__ cD2,
+                                        const T* __restrict__ cD3, const T* __restrict__ u,
+                                        const T* __restrict__ v, const T* __restrict__ w, int i, int j, int k) {
+  T s = stencil_axis<T, D_LO, ND>(cD1, i, u, off(g, -3, j, k), 1, i, g.n1);
+  s = stencil_axis_acc<T, D_LO, ND>(s, cD2, j, v, off(g, i, -3, k), g.nx, j, g.n2);
+  s = stencil_axis_acc<T, D_LO, ND>(s, cD3, k, w, off(g, i, j, -3), g.nxy, k, g.n3);
+  return s;
+}
+template <typename T>
+__global__ void __launch_bounds__(BX* BY) k_divergence2(Geom g, const T* __restrict__ cD1, const T* __restrict__ cD2,
+                                                        const T* __restrict__ cD3, const T* __restrict__ u,
+                                                        const T* __restrict__ v, const T* __restrict__ w,
+                                                        T* __restrict__ div) {
+  POINT_PROLOGUE
+  div[off(g, i, j, k)] = div2_point(g, cD1, cD2, cD3, u, v, w, i, j, k);
+}
+template <typename T>
+void launch_divergence2(const Geom& g, const T* cD1, const T* cD2, const T* cD3, const T* u, const T* v,
+                        const T* w, T* div, cudaStream_t s) {
+  k_divergence2<T><<<grid3(g), dim3(BX, BY), 0, s>>>(g, cD1, cD2, cD3, u, v, w, div);
+}
+
+// ------------------------------------------------------------------------------------
+// Helmholtz_explicit (mod_diff.f90:549-762; helmholtz_explicit_kernel.cu)
+// nl -= multL * (cx u_xx + cy u_yy + cz u_zz), 7-point second derivatives
+// ------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T lap7_point(const Geom& g, const T* __restrict__ cx, const T* __restrict__ cy,
+                                        const T* __restrict__ cz, const T* __restrict__ vel, int i, int j, int k) {
+  T dd = stencil_axis<T, B_LO, NB>(cx, i, vel, off(g, -3, j, k), 1, i, g.n1);
+  dd = stencil_axis_acc<T, B_LO, NB>(dd, cy, j, vel, off(g, i, -3, k), g.nx, j, g.n2);
+  dd = stencil_axis_acc<T, B_LO, NB>(dd, cz, k, vel, off(g, i, j, -3), g.nxy, k, g.n3);
+  return dd;
+}
+template <typename T>
+__global__ void __launch_bounds__(BX* BY) k_helmholtz(Geom g, const T* __restrict__ cx, const T* __restrict__ cy,
+                                                      const T* __restrict__ cz, T multL, const T* __restrict__ vel,
+                                                      T* __restrict__ nl) {
+  POINT_PROLOGUE
+  const long long p = off(g, i, j, k);
+  nl[p] = nl[p] - multL * lap7_point(g, cx, cy, cz, vel, i, j, k);
+}
+template <typename T>
+void launch_helmholtz(int m, const Geom& g, const T* cx, const T* cy, const T* cz, T multL, const T* vel, T* nl,
+                      cudaStream_t s) {
+  (void)m;
+  k_helmholtz<T><<<grid3(g), dim3(BX, BY), 0, s>>>(g, cx, cy, cz, multL, vel, nl);
+}
+
+// ------------------------------------------------------------------------------------
+// interpolations (mod_diff.f90:1567-1648 and :1740-1825; interpolate2_*_kernel.cu)
+// ------------------------------------------------------------------------------------
+template <typename T, int LO, int CNT>
+__global__ void __launch_bounds__(BX* BY) k_interp(int a, Geom g, const T* __restrict__ cI, const T* __restrict__ phi,
+                                                   T* __restrict__ out) {
+  POINT_PROLOGUE
+  const int q = coord(a, i, j, k);
+  out[off(g, i, j, k)] = stencil_axis<T, LO, CNT>(cI, q, phi, base_off(g, a, i, j, k), stride(g, a), q, extent(g, a));
+}
+template <typename T>
+void launch_interp_pre_vel(int m, const Geom& g, const T* cI, const T* phi, T* out, cudaStream_t s) {
+  k_interp<T, G_LO, NG><<<grid3(g), dim3(BX, BY), 0, s>>>(m - 1, g, cI, phi, out);
+}
+template <typename T>
+void launch_interp_vel_pre(int m, const Geom& g, const T* cI, const T* phi, T* out, cudaStream_t s) {
+  k_interp<T, D_LO, ND><<<grid3(g), dim3(BX, BY), 0, s>>>(m - 1, g, cI, phi, out);
+}
+
+// ------------------------------------------------------------------------------------
+// one upwind advection term (mod_diff.f90:784-1424; Nonlinear_upwind_kernel.cu)
+// component_id = 3(m-1) + a; the first axis of a component overwrites nl
+// ------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(BX* BY) k_nl_upwind(int a, int first, Geom g, const T* __restrict__ cU,
+                                                      const T* __restrict__ cDn, const T* __restrict__ pp,
+                                                      const T* __restrict__ vel, T* __restrict__ nl) {
+  POINT_PROLOGUE
+  const long long p = off(g, i, j, k);
+  const int q = coord(a, i, j, k);
+  const T ppv = pp[p];
+  const T* tab = (ppv >= T(0)) ? cU : cDn;
+  const T dd = stencil_axis<T, B_LO, NB>(tab, q, vel, base_off(g, a, i, j, k), stride(g, a), q, extent(g, a));
+  nl[p] = first ? dd * ppv : nl[p] + dd * ppv;
+}
+template <typename T>
+void launch_nonlinear_upwind(int cid, const Geom& g, const T* cU, const T* cDn, const T* pp, const T* vel, T* nl,
+                             cudaStream_t s) {
+  const int a = (cid - 1) % 3;
+  k_nl_upwind<T><<<grid3(g), dim3(BX, BY), 0, s>>>(a, a == 0, g, cU, cDn, pp, vel, nl);
+}
+
+// ------------------------------------------------------------------------------------
+// axpby (axpby_kernel.cu:6-17)
+// ------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(BX* BY) k_axpby(Geom g, T a, T b, const T* __restrict__ x, const T* __restrict__ y,
+                                                  T* __restrict__ z) {
+  POINT_PROLOGUE
+  const long long p = off(g, i, j, k);
+  z[p] = a * x[p] + b * y[p];
+}
+template <typename T>
+void launch_axpby(const Geom& g, T a, T b, const T* x, const T* y, T* z, cudaStream_t s) {
+  k_axpby<T><<<grid3(g), dim3(BX, BY), 0, s>>>(g, a, b, x, y, z);
+}
+
+// ------------------------------------------------------------------------------------
+// compact 7-point Laplacian cdg (product_div_grad_relax, mod_laplace.f90:216-327;
+// product_dg_relax_kernel.cu) and damped Jacobi / JOR (relaxation_div_grad,
+// mod_laplace.f90:339-613; jacobi_kernel.cu)
+// ------------------------------------------------------------------------------------
+template <typename T>
+struct Nb7 {
+  T c, xm, xp, ym, yp, zm, zp;
+};
+template <typename T>
+__device__ __forceinline__ Nb7<T> load_nb7(const Geom& g, const T* __restrict__ f, int i, int j, int k) {
+  Nb7<T> n;
+  const long long p = off(g, i, j, k);
+  n.c = __ldg(f + p);
+  n.xm = __ldg(f + off(g, wrapi(i - 1, g.n1), j, k));
+  n.xp = __ldg(f + off(g, wrapi(i + 1, g.n1), j, k));
+  n.ym = __ldg(f + off(g, i, wrapi(j - 1, g.n2), k));
+  n.yp = __ldg(f + off(g, i, wrapi(j + 1, g.n2), k));
+  n.zm = __ldg(f + off(g, i, j, wrapi(k - 1, g.n3)));
+  n.zp = __ldg(f + off(g, i, j, wrapi(k + 1, g.n3)));
+  return n;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BX* BY) k_dg_relax(Geom g, const T* __restrict__ c1, const T* __restrict__ c2,
+                                                     const T* __restrict__ c3, const T* __restrict__ x,
+                                                     T* __restrict__ lap) {
+  POINT_PROLOGUE
+  const Nb7<T> n = load_nb7(g, x, i, j, k);
+  const T* a = c1 + 3 * (i - 1);
+  const T* b = c2 + 3 * (j - 1);
+  const T* c = c3 + 3 * (k - 1);
+  lap[off(g, i, j, k)] = a[0] * n.xm + a[2] * n.xp + b[0] * n.ym + b[2] * n.yp + c[0] * n.zm + c[2] * n.zp +
+                         (a[1] + b[1] + c[1]) * n.c;
+}
+template <typename T>
+void launch_dg_relax(const Geom& g, const T* c1, const T* c2, const T* c3, const T* x, T* lap, cudaStream_t s) {
+  k_dg_relax<T><<<grid3(g), dim3(BX, BY), 0, s>>>(g, c1, c2, c3, x, lap);
+}
+
+template <typename T>
+__device__ __forceinline__ T jacobi_point(const Geom& g, const T* a, const T* b, const T* c, T omega, T bb,
+                                          const Nb7<T>& n) {
+  return omega * (bb - a[0] * n.xm - a[2] * n.xp - b[0] * n.ym - b[2] * n.yp - c[0] * n.zm - c[2] * n.zp) /
+             (a[1] + b[1] + c[1]) +
+         (T(1) - omega) * n.c;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BX* BY) k_jacobi(Geom g, const T* __restrict__ c1, const T* __restrict__ c2,
+                                                   const T* __restrict__ c3, T omega, const T* __restrict__ bb,
+                                                   const T* __restrict__ rel, T* __restrict__ out) {
+  POINT_PROLOGUE
+  const long long p = off(g, i, j, k);
+  const Nb7<T> n = load_nb7(g, rel, i, j, k);
+  out[p] = jacobi_point(g, c1 + 3 * (i - 1), c2 + 3 * (j - 1), c3 + 3 * (k - 1), omega, __ldg(bb + p), n);
+}
+template <typename T>
+void launch_jacobi(const Geom& g, const T* c1, const T* c2, const T* c3, T omega, const T* bb, const T* rel, T* out,
+                   cudaStream_t s) {
+  k_jacobi<T><<<grid3(g), dim3(BX, BY), 0, s>>>(g, c1, c2, c3, omega, bb, rel, out);
+}
+
+// init sweep: rel = omega*bb/diag (mod_laplace.f90:~470, r == 1 .AND. init_yes)
+template <typename T>
+__device__ __forceinline__ T init_val(const T* __restrict__ c1, const T* __restrict__ c2, const T* __restrict__ c3,
+                                      T omega, T bb, int i, int j, int k) {
+  return omega * bb / (c1[3 * (i - 1) + 1] + c2[3 * (j - 1) + 1] + c3[3 * (k - 1) + 1]);
+}
+template <typename T>
+__global__ void __launch_bounds__(BX* BY) k_jacobi_init1(Geom g, const T* __restrict__ c1, const T* __restrict__ c2,
+                                                         const T* __restrict__ c3, T omega, const T* __restrict__ bb,
+                                                         T* __restrict__ out) {
+  POINT_PROLOGUE
+  const long long p = off(g, i, j, k);
+  out[p] = init_val(c1, c2, c3, omega, __ldg(bb + p), i, j, k);
+}
+// init sweep fused with the following sweep: the start values at the 7 points are formed
+// from bb on the fly, so the pair of sweeps reads bb once and writes once.
+template <typename T>
+__global__ void __launch_bounds__(BX* BY) k_jacobi_init2(Geom g, const T* __restrict__ c1, const T* __restrict__ c2,
+                                                         const T* __restrict__ c3, T omega, const T* __restrict__ bb,
+                                                         T* __restrict__ out) {
+  POINT_PROLOGUE
+  const Nb7<T> b = load_nb7(g, bb, i, j, k);
+  const int im = wrapi(i - 1, g.n1), ip = wrapi(i + 1, g.n1);
+  const int jm = wrapi(j - 1, g.n2), jp = wrapi(j + 1, g.n2);
+  const int km = wrapi(k - 1, g.n3), kp = wrapi(k + 1, g.n3);
+  Nb7<T> n;
+  n.c = init_val(c1, c2, c3, omega, b.c, i, j, k);
+  n.xm = init_val(c1, c2, c3, omega, b.xm, im, j, k);
+  n.xp = init_val(c1, c2, c3, omega, b.xp, ip, j, k);
+  n.ym = init_val(c1, c2, c3, omega, b.ym, i, jm, k);
+  n.yp = init_val(c1, c2, c3, omega, b.yp, i, jp, k);
+  n.zm = init_val(c1, c2, c3, omega, b.zm, i, j, km);
+  n.zp = init_val(c1, c2, c3, omega, b.zp, i, j, kp);
+  out[off(g, i, j, k)] = jacobi_point(g, c1 + 3 * (i - 1), c2 + 3 * (j - 1), c3 + 3 * (k - 1), omega, b.c, n);
+}
+template <typename T>
+void launch_jacobi_init2(const Geom& g, const T* c1, const T* c2, const T* c3, T omega, const T* bb, T* out,
+                         cudaStream_t s) {
+  k_jacobi_init2<T><<<grid3(g), dim3(BX, BY), 0, s>>>(g, c1, c2, c3, omega, bb, out);
+}
+template <typename T>
+void launch_jacobi_init1(const Geom& g, const T* c1, const T* c2, const T* c3, T omega, const T* bb, T* out,
+                         cudaStream_t s) {
+  k_jacobi_init1<T><<<grid3(g), dim3(BX, BY), 0, s>>>(g, c1, c2, c3, omega, bb, out);
+}
+
+// ------------------------------------------------------------------------------------
+// JOR sweep with the reference's six ghost-face arrays (jor_kernel_v2.cu:5-645), made
+// deterministic: it writes a separate output field instead of updating rel in place.
+// Face layouts (jor_kernel_v2.cu:95-97): rear/front (i-1)+n1(j-1), west/east (j-1)+n2(k-1),
+// lower/upper (i-1)+n1(k-1).
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(BX* BY) k_jor_faces(Geom g, double omega, const double* __restrict__ c1,
+                                                      const double* __restrict__ c2, const double* __restrict__ c3,
+                                                      const double* __restrict__ rel, const double* __restrict__ bb,
+                                                      const double* __restrict__ rear, const double* __restrict__ front,
+                                                      const double* __restrict__ upper, const double* __restrict__ lower,
+                                                      const double* __restrict__ west, const double* __restrict__ east,
+                                                      double* __restrict__ out) {
+  POINT_PROLOGUE
+  const long long p = off(g, i, j, k);
+  Nb7<double> n;
+  n.c = rel[p];
+  n.xm = (i == 1) ? west[(j - 1) + (long long)g.n2 * (k - 1)] : rel[p - 1];
+  n.xp = (i == g.n1) ? east[(j - 1) + (long long)g.n2 * (k - 1)] : rel[p + 1];
+  n.ym = (j == 1) ? lower[(i - 1) + (long long)g.n1 * (k - 1)] : rel[p - g.nx];
+  n.yp = (j == g.n2) ? upper[(i - 1) + (long long)g.n1 * (k - 1)] : rel[p + g.nx];
+  n.zm = (k == 1) ? rear[(i - 1) + (long long)g.n1 * (j - 1)] : rel[p - g.nxy];
+  n.zp = (k == g.n3) ? front[(i - 1) + (long long)g.n1 * (j - 1)] : rel[p + g.nxy];
+  out[p] = jacobi_point(g, c1 + 3 * (i - 1), c2 + 3 * (j - 1), c3 + 3 * (k - 1), omega, bb[p], n);
+}
+void launch_jor_faces(const Geom& g, int ny_cdg1, int ny_cdg2, int ny_cdg3, int grid_id, double omega,
+                      const double* c1, const double* c2, const double* c3, const double* rel, const double* bb,
+                      const double* rear, const double* front, const double* upper, const double* lower,
+                      const double* west, const double* east, double* out, cudaStream_t s) {
+  // cdg(-1:1, 1:ny_cdg, 1:n_grids): level grid_id starts at (grid_id-1)*ny_cdg*3
+  const long long o1 = (long long)(grid_id - 1) * ny_cdg1 * 3, o2 = (long long)(grid_id - 1) * ny_cdg2 * 3,
+                  o3 = (long long)(grid_id - 1) * ny_cdg3 * 3;
+  k_jor_faces<<<grid3(g), dim3(BX, BY), 0, s>>>(g, omega, c1 + o1, c2 + o2, c3 + o3, rel, bb, rear, front, upper,
+                                                lower, west, east, out);
+}
+
+// get_ghost (get_ghost.cu): copy the six boundary planes of rel into the face arrays
+__global__ void __launch_bounds__(BX* BY) k_get_ghost(Geom g, const double* __restrict__ rel, double* rear,
+                                                      double* front, double* upper, double* lower, double* west,
+                                                      double* east) {
+  POINT_PROLOGUE
+  const long long p = off(g, i, j, k);
+  const double v = rel[p];
+  if (k == 1) rear[(i - 1) + (long long)g.n1 * (j - 1)] = v;
+  if (k == g.n3) front[(i - 1) + (long long)g.n1 * (j - 1)] = v;
+  if (j == 1) lower[(i - 1) + (long long)g.n1 * (k - 1)] = v;
+  if (j == g.n2) upper[(i - 1) + (long long)g.n1 * (k - 1)] = v;
+  if (i == 1) west[(j - 1) + (long long)g.n2 * (k - 1)] = v;
+  if (i == g.n1) east[(j - 1) + (long long)g.n2 * (k - 1)] = v;
+}
+void launch_get_ghost(const Geom& g, const double* rel, double* rear, double* front, double* upper, double* lower,
+                      double* west, double* east, cudaStream_t s) {
+  k_get_ghost<<<grid3(g), dim3(BX, BY), 0, s>>>(g, rel, rear, front, upper, lower, west, east);
+}
+
+__global__ void __launch_bounds__(BX* BY) k_copy_interior(Geom g, const double* __restrict__ src,
+                                                          double* __restrict__ dst) {
+  POINT_PROLOGUE
+  const long long p = off(g, i, j, k);
+  dst[p] = src[p];
+}
+void launch_copy_interior(const Geom& g, const double* src, double* dst, cudaStream_t s) {
+  k_copy_interior<<<grid3(g), dim3(BX, BY), 0, s>>>(g, src, dst);
+}
+
+// periodic ghost fill of all three directions, three planes per side (mod_exchange.f90:133-140):
+// every ghost point of a face (tangential indices 1..N) takes the value of its periodic image.
+__global__ void k_fill_ghosts(Geom g, double* __restrict__ phi) {
+  // one thread per (i,j,k) of the padded box restricted to face ghosts
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int X = g.nx, Y = g.ny;
+  const long long total = g.nfield;
+  if (t >= total) return;
+  const int ci = (int)(t % X);
+  const int cj = (int)((t / X) % Y);
+  const int ck = (int)(t / g.nxy);
+  int i = ci - 3, j = cj - 3, k = ck - 3;
+  const int N1 = g.n1 + 1, N2 = g.n2 + 1, N3 = g.n3 + 1;
+  // x-face ghosts: i in -2..0 or N1..N1+2, j in 1..N2, k in 1..N3 (and likewise y, z)
+  auto img = [](int q, int n) { return q < 1 ? q + n : (q > n ? q - n : q); };
+  const bool gx = (i >= -2 && i <= 0) || (i >= N1 && i <= N1 + 2);
+  const bool gy = (j >= -2 && j <= 0) || (j >= N2 && j <= N2 + 2);
+  const bool gz = (k >= -2 && k <= 0) || (k >= N3 && k <= N3 + 2);
+  const bool ix = i >= 1 && i <= N1, iy = j >= 1 && j <= N2, iz = k >= 1 && k <= N3;
+  int si = i, sj = j, sk = k;
+  if (gx && iy && iz) si = img(i, g.n1);
+  else if (gy && ix && iz) sj = img(j, g.n2);
+  else if (gz && ix && iy) sk = img(k, g.n3);
+  else return;
+  // N (the periodic image of 1) is itself filled from 1
+  si = (si == N1) ? 1 : si;
+  sj = (sj == N2) ? 1 : sj;
+  sk = (sk == N3) ? 1 : sk;
+  phi[t] = phi[off(g, si, sj, sk)];
+}
+void launch_fill_ghosts(const Geom& g, double* phi, cudaStream_t s) {
+  const long long n = g.nfield;
+  k_fill_ghosts<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, phi);
+}
+
+// ------------------------------------------------------------------------------------
+// high-order Laplacian A x = sum_m D_m (G_m x)  (product_div_grad, mod_laplace.f90:38-197)
+// evaluated on the fly: per axis the six gradient values at the neighbouring velocity points
+// are formed from x and combined with the divergence weights, in the reference's order
+// (gradient stored to a double, then divergence m = 1 overwrite, m = 2,3 accumulate).
+// ------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T divgrad_axis(const Geom& g, const T* __restrict__ cG, const T* __restrict__ cD,
+                                          const T* __restrict__ x, long long base, long long st, int q, int n,
+                                          T acc, bool first) {
+  T xs[11];
+#pragma unroll
+  for (int l = 0; l < 11; ++l) xs[l] = __ldg(x + base + (long long)(wrapi(q - 5 + l, n) + 3) * st);
+  const T* cd = cD + (long long)q * ND;
+  T s = acc;
+#pragma unroll
+  for (int l = 0; l < ND; ++l) {
+    const int qq = wrapi(q + D_LO + l, n);  // velocity point q-3+l
+    const T* cg = cG + (long long)qq * NG;
+    // gradient at velocity point q-3+l uses x at (q-3+l) + (-2..3) -> xs index l .. l+5
+    T gv = cg[0] * xs[l];
+#pragma unroll
+    for (int r = 1; r < NG; ++r) gv = gv + cg[r] * xs[l + r];
+    s = (first && l == 0) ? cd[0] * gv : s + cd[l] * gv;
+  }
+  return s;
+}
+template <typename T>
+__global__ void __launch_bounds__(BX* BY) k_div_grad(Geom g, Coeffs<T> c, const T* __restrict__ x, T* __restrict__ lap) {
+  POINT_PROLOGUE
+  T s = divgrad_axis(g, c.cG[0], c.cD[0], x, off(g, -3, j, k), 1, i, g.n1, T(0), true);
+  s = divgrad_axis(g, c.cG[1], c.cD[1], x, off(g, i, -3, k), g.nx, j, g.n2, s, false);
+  s = divgrad_axis(g, c.cG[2], c.cD[2], x, off(g, i, j, -3), g.nxy, k, g.n3, s, false);
+  lap[off(g, i, j, k)] = s;
+}
+template <typename T>
+void launch_div_grad(const Geom& g, const Coeffs<T>& c, const T* x, T* lap, cudaStream_t s) {
+  k_div_grad<T><<<grid3(g), dim3(BX, BY), 0, s>>>(g, c, x, lap);
+}
+
+// ------------------------------------------------------------------------------------
+// pressure Dirichlet values on labelled planes (apply_pressure_BC_CT, usr_func.f90:857-897;
+// set_pressure_BC_kernel.cu).  The plane test uses the Fortran index k == k_start_index-1
+// of the CPU routine.
+// ------------------------------------------------------------------------------------
+template <typename L>
+__global__ void __launch_bounds__(BX* BY) k_pressure_bc(Geom g, int t1, int t2, int t3, int ks, double p_in,
+                                                        double p_out, double p_out2, const L* __restrict__ label,
+                                                        double* __restrict__ rel) {
+  POINT_PROLOGUE
+  const long long p = off(g, i, j, k);
+  const double lb = (double)label[p];
+  if (t1 == 1 && lb == 5.0 && k == ks - 1) rel[p] = p_in;
+  if (t2 == 1 && lb == 9.0 && k == ks - 1) rel[p] = p_out;
+  if (t3 == 1 && lb == 11.0) rel[p] = p_out2;
+}
+void launch_pressure_bc(const Geom& g, int t1, int t2, int t3, int ks, double p_in, double p_out, double p_out2,
+                        const uint8_t* label, double* rel, cudaStream_t s) {
+  k_pressure_bc<uint8_t><<<grid3(g), dim3(BX, BY), 0, s>>>(g, t1, t2, t3, ks, p_in, p_out, p_out2, label, rel);
+}
+void launch_pressure_bc_f64label(const Geom& g, int t1, int t2, int t3, int ks, double p_in, double p_out,
+                                 double p_out2, const double* label, double* rel, cudaStream_t s) {
+  k_pressure_bc<double><<<grid3(g), dim3(BX, BY), 0, s>>>(g, t1, t2, t3, ks, p_in, p_out, p_out2, label, rel);
+}
+
+// ------------------------------------------------------------------------------------
+// deterministic FP64 reductions (product_scalar / get_norms, mod_solvers.f90:2319-2470):
+// a fixed grid of RED_BLOCKS blocks walks the interior in a fixed order, each block writes
+// one partial, and a single block sums the partials in block order.
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+template <int NQ>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NQ], const int (&kind)[NQ], double* partial) {
+  __shared__ double sh[NQ][RED_THREADS / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) v[q] = kind[q] ? warp_max(v[q]) : warp_sum(v[q]);
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) sh[q][w] = v[q];
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      double x = lane < RED_THREADS / 32 ? sh[q][lane] : (kind[q] ? 0.0 : 0.0);
+      x = kind[q] ? warp_max(x) : warp_sum(x);
+      if (lane == 0) partial[(long long)blockIdx.x * NQ + q] = x;
+    }
+  }
+}
+
+// interior points enumerated as t = i-1 + n1*((j-1) + n2*(k-1)), grid-stride with a fixed grid
+#define RED_LOOP(g)                                                                     \
+  const long long ntot = (long long)(g).n1 * (g).n2 * (g).n3;                           \
+  for (long long t = (long long)blockIdx.x * RED_THREADS + threadIdx.x; t < ntot;       \
+       t += (long long)RED_BLOCKS * RED_THREADS)
+
+__device__ __forceinline__ long long interior_off(const Geom& g, long long t) {
+  const int i = (int)(t % g.n1) + 1;
+  const long long r = t / g.n1;
+  const int j = (int)(r % g.n2) + 1;
+  const int k = (int)(r / g.n2) + 1;
+  return off(g, i, j, k);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS) k_dot_partials(Geom g, const T* __restrict__ a, const T* __restrict__ b,
+                                                              double* __restrict__ partial) {
+  double v[1] = {0.0};
+  const int kind[1] = {0};
+  RED_LOOP(g) {
+    const long long p = interior_off(g, t);
+    v[0] += (double)a[p] * (double)b[p];
+  }
+  block_reduce_store<1>(v, kind, partial);
+}
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS) k_norm_partials(Geom g, const T* __restrict__ a,
+                                                               double* __restrict__ partial) {
+  double v[2] = {0.0, 0.0};
+  const int kind[2] = {1, 0};
+  RED_LOOP(g) {
+    const double x = (double)a[interior_off(g, t)];
+    v[0] = fmax(v[0], fabs(x));
+    v[1] += x * x;
+  }
+  block_reduce_store<2>(v, kind, partial);
+}
+template <typename T>
+void launch_dot_partials(const Geom& g, const T* a, const T* b, double* partial, cudaStream_t s) {
+  k_dot_partials<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, a, b, partial);
+}
+template <typename T>
+void launch_norm_partials(const Geom& g, const T* a, double* partial, cudaStream_t s) {
+  k_norm_partials<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, a, partial);
+}
+
+__global__ void k_finalize(const double* __restrict__ partial, int nq, int kinds_mask, double* __restrict__ out) {
+  // one warp per quantity, fixed order: lane l sums blocks l, l+32, ... then a fixed tree
+  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (q >= nq) return;
+  const bool isMax = (kinds_mask >> q) & 1;
+  double v = 0.0;
+  for (int b = lane; b < RED_BLOCKS; b += 32) {
+    const double x = partial[(long long)b * nq + q];
+    v = isMax ? fmax(v, x) : v + x;
+  }
+  v = isMax ? warp_max(v) : warp_sum(v);
+  if (lane == 0) out[q] = v;
+}
+void launch_finalize(const double* partial, int nq, const int* kinds_host, double* out, cudaStream_t s) {
+  int mask = 0;
+  for (int q = 0; q < nq; ++q) mask |= (kinds_host[q] ? 1 : 0) << q;
+  k_finalize<<<1, 32 * nq, 0, s>>>(partial, nq, mask, out);
+}
+
+// ------------------------------------------------------------------------------------
+// explicit instantiations
+// ------------------------------------------------------------------------------------
+#define INST(T)                                                                                               \
+  template void launch_gradient<T>(int, const Geom&, const T*, const T*, T*, cudaStream_t);                  \
+  template void launch_divergence<T>(int, const Geom&, const T*, const T*, T*, cudaStream_t);                \
+  template void launch_divergence2<T>(const Geom&, const T*, const T*, const T*, const T*, const T*, const T*, \
+                                      T*, cudaStream_t);                                                      \
+  template void launch_helmholtz<T>(int, const Geom&, const T*, const T*, const T*, T, const T*, T*,          \
+                                    cudaStream_t);                                                            \
+  template void launch_interp_pre_vel<T>(int, const Geom&, const T*, const T*, T*, cudaStream_t);            \
+  template void launch_interp_vel_pre<T>(int, const Geom&, const T*, const T*, T*, cudaStream_t);            \
+  template void launch_nonlinear_upwind<T>(int, const Geom&, const T*, const T*, const T*, const T*, T*,      \
+                                           cudaStream_t);                                                     \
+  template void launch_axpby<T>(const Geom&, T, T, const T*, const T*, T*, cudaStream_t);                     \
+  template void launch_dg_relax<T>(const Geom&, const T*, const T*, const T*, const T*, T*, cudaStream_t);    \
+  template void launch_jacobi<T>(const Geom&, const T*, const T*, const T*, T, const T*, const T*, T*,        \
+                                 cudaStream_t);                                                               \
+  template void launch_jacobi_init2<T>(const Geom&, const T*, const T*, const T*, T, const T*, T*,            \
+                                       cudaStream_t);                                                         \
+  template void launch_jacobi_init1<T>(const Geom&, const T*, const T*, const T*, T, const T*, T*,            \
+                                       cudaStream_t);                                                         \
+  template void launch_div_grad<T>(const Geom&, const Coeffs<T>&, const T*, T*, cudaStream_t);                \
+  template void launch_dot_partials<T>(const Geom&, const T*, const T*, double*, cudaStream_t);              \
+  template void launch_norm_partials<T>(const Geom&, const T*, double*, cudaStream_t);
+INST(double)
+INST(float)
+#undef INST
+
+}  // namespace impact

@@ -1,0 +1,618 @@
+// step.cu -- one RK3 fractional time step of IMPACT on resident device fields, and the case
+// life cycle (the GPU_setup / GPU_malloc / GPU_memcopy / GPU_memfree of mod_mem_GPU.f90:18-437).
+//
+// The substep (mod_timeint.f90:275-377) is reorganised into fused passes:
+//   interpolate_vel  -> k_interp_vel3   (3 interpolations, one pass)
+//   rhs_vel          -> k_nl_rhs        (pp interpolation, 3 upwind terms, explicit Helmholtz and
+//                                        both RK updates of one component in one pass)
+//   explicit         -> divergence2 of rhs, Poisson solve, k_project (vel = rhs - G pre, 3 comps)
+// Every pass keeps the reference's order of floating-point operations per point.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "case.cuh"
+#include "kernels.cuh"
+#include "solver.cuh"
+
+namespace impact {
+
+constexpr int BX = 32, BY = 8, NT = BX * BY;
+static inline dim3 grid3(const Geom& g) { return dim3((g.n1 + BX - 1) / BX, (g.n2 + BY - 1) / BY, g.n3); }
+
+// RK3 coefficients (mod_vars.f90:774-775)
+static const double aRK[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+static const double bRK[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+
+#define PT                                                  \
+  const int i = blockIdx.x * BX + threadIdx.x + 1;          \
+  const int j = blockIdx.y * BY + threadIdx.y + 1;          \
+  const int k = blockIdx.z + 1;                             \
+  if (i > g.n1 || j > g.n2) return;                         \
+  const long long p = off(g, i, j, k);
+
+__device__ __forceinline__ int crd(int a, int i, int j, int k) { return a == 0 ? i : (a == 1 ? j : k); }
+__device__ __forceinline__ int ext(const Geom& g, int a) { return a == 0 ? g.n1 : (a == 1 ? g.n2 : g.n3); }
+__device__ __forceinline__ long long strd(const Geom& g, int a) { return a == 0 ? 1LL : (a == 1 ? (long long)g.nx : g.nxy); }
+
+template <int LO, int CNT>
+__device__ __forceinline__ double st1(const double* __restrict__ c, const double* __restrict__ f, const Geom& g, int a,
+                                      int i, int j, int k, long long p) {
+  const int q = crd(a, i, j, k), n = ext(g, a);
+  const long long s = strd(g, a);
+  const long long base = p - (long long)q * s;  // offset with the axis coordinate at 0
+  const double* cr = c + (long long)q * CNT;
+  double v = cr[0] * __ldg(f + base + (long long)wrapi(q + LO, n) * s);
+#pragma unroll
+  for (int l = 1; l < CNT; ++l) v = v + cr[l] * __ldg(f + base + (long long)wrapi(q + LO + l, n) * s);
+  return v;
+}
+template <int LO, int CNT>
+__device__ __forceinline__ double st1_acc(double v, const double* __restrict__ c, const double* __restrict__ f,
+                                          const Geom& g, int a, int i, int j, int k, long long p) {
+  const int q = crd(a, i, j, k), n = ext(g, a);
+  const long long s = strd(g, a);
+  const long long base = p - (long long)q * s;
+  const double* cr = c + (long long)q * CNT;
+#pragma unroll
+  for (int l = 0; l < CNT; ++l) v = v + cr[l] * __ldg(f + base + (long long)wrapi(q + LO + l, n) * s);
+  return v;
+}
+
+// interpolate_vel (mod_diff.f90:1436-1472): work_m = I_{u_m -> p} vel_m, three components
+__global__ void __launch_bounds__(NT) k_interp_vel3(Geom g, Coeffs<double> c, const double* __restrict__ u,
+                                                    const double* __restrict__ v, const double* __restrict__ w,
+                                                    double* __restrict__ w1, double* __restrict__ w2,
+                                                    double* __restrict__ w3) {
+  PT
+  w1[p] = st1<D_LO, ND>(c.cIup[0], u, g, 0, i, j, k, p);
+  w2[p] = st1<D_LO, ND>(c.cIup[1], v, g, 1, i, j, k, p);
+  w3[p] = st1<D_LO, ND>(c.cIup[2], w, g, 2, i, j, k, p);
+}
+
+// rhs_vel (mod_rhs.f90:35-140) for component m: nonlinear (upwind) + Helmholtz_explicit + RK update
+template <int M>
+__global__ void __launch_bounds__(NT) k_nl_rhs(Geom g, Coeffs<double> c, double multL, double mult_b, double mult_a,
+                                               int use_old, const double* __restrict__ vel,
+                                               const double* __restrict__ work1, const double* __restrict__ work2,
+                                               const double* __restrict__ work3, double* __restrict__ nl,
+                                               double* __restrict__ rhs) {
+  PT
+  const double* wk[3] = {work1, work2, work3};
+  double acc = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    // pp = interpolate2_pre_vel(M, work_a): along axis M
+    const double pp = st1<G_LO, NG>(c.cIpu[M], wk[a], g, M, i, j, k, p);
+    const double* cU = (a == M) ? c.cNuU[a] : c.cNpU[a];
+    const double* cDn = (a == M) ? c.cNuD[a] : c.cNpD[a];
+    const double dd = st1<B_LO, NB>(pp >= 0.0 ? cU : cDn, vel, g, a, i, j, k, p);
+    acc = (a == 0) ? dd * pp : acc + dd * pp;
+  }
+  // Helmholtz_explicit: x, y, z second derivatives of vel_M
+  double lap = st1<B_LO, NB>(M == 0 ? c.cuu[0] : c.cpp[0], vel, g, 0, i, j, k, p);
+  lap = st1_acc<B_LO, NB>(lap, M == 1 ? c.cuu[1] : c.cpp[1], vel, g, 1, i, j, k, p);
+  lap = st1_acc<B_LO, NB>(lap, M == 2 ? c.cuu[2] : c.cpp[2], vel, g, 2, i, j, k, p);
+  const double nln = acc - multL * lap;
+  double r = vel[p];
+  if (use_old) r = r - mult_b * nl[p];
+  r = r - mult_a * nln;
+  nl[p] = nln;
+  rhs[p] = r;
+}
+
+// pre = pre * ab * dt  (mod_timeint.f90:318)  /  pre = pre / ab / dt  (:372)
+__global__ void __launch_bounds__(NT) k_scale_pre(Geom g, double ab, double dt, int divide, double* __restrict__ pre) {
+  PT
+  pre[p] = divide ? pre[p] / ab / dt : pre[p] * ab * dt;
+}
+
+// explicit (mod_solvers.f90:180-330): vel_m = rhs_m - G_m pre for the three components
+__global__ void __launch_bounds__(NT) k_project(Geom g, Coeffs<double> c, const double* __restrict__ pre,
+                                                const double* __restrict__ r1, const double* __restrict__ r2,
+                                                const double* __restrict__ r3, double* __restrict__ u,
+                                                double* __restrict__ v, double* __restrict__ w) {
+  PT
+  u[p] = 1.0 * r1[p] + (-1.0) * st1<G_LO, NG>(c.cG[0], pre, g, 0, i, j, k, p);
+  v[p] = 1.0 * r2[p] + (-1.0) * st1<G_LO, NG>(c.cG[1], pre, g, 1, i, j, k, p);
+  w[p] = 1.0 * r3[p] + (-1.0) * st1<G_LO, NG>(c.cG[2], pre, g, 2, i, j, k, p);
+}
+
+// get_dtime (mod_lib.f90:46-250), timeint_mode 1: block max of radius / stabilitylimit(angle)
+__constant__ double c_stab[41];
+
+__device__ __forceinline__ double wmax_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double wsum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void __launch_bounds__(NT) k_dtime(Geom g, Coeffs<double> c, DtRows dr, double Re, const double* __restrict__ u,
+                                              const double* __restrict__ v, const double* __restrict__ w,
+                                              double* __restrict__ partial) {
+  const int i = blockIdx.x * BX + threadIdx.x + 1;
+  const int j = blockIdx.y * BY + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  double beta = 0.0;
+  if (i <= g.n1 && j <= g.n2) {
+    const long long p = off(g, i, j, k);
+    const double w1 = st1<D_LO, ND>(c.cIup[0], u, g, 0, i, j, k, p);
+    const double w2 = st1<D_LO, ND>(c.cIup[1], v, g, 1, i, j, k, p);
+    const double w3 = st1<D_LO, ND>(c.cIup[2], w, g, 2, i, j, k, p);
+    double are = dr.spp[0][i] + dr.spp[1][j];
+    are = are + dr.spp[2][k];
+    are = are / Re;
+    double aim = dr.sp1[0][i] * fabs(w1);
+    aim = aim + dr.sp1[1][j] * fabs(w2);
+    aim = aim + dr.sp1[2][k] * fabs(w3);
+    const double pi = 3.14159265358979323846;
+    const double angle = (fabs(aim) < 1e-16) ? pi / 2.0 : atan(are / aim);
+    const double radius = sqrt(are * are + aim * aim);
+    long long idx = llround(2.0 * 40.0 * angle / pi);
+    idx = idx < 0 ? 0 : (idx > 40 ? 40 : idx);
+    beta = radius / c_stab[idx];
+  }
+  __shared__ double sh[NT / 32];
+  const int tid = threadIdx.x + BX * threadIdx.y;
+  beta = wmax_d(beta);
+  if ((tid & 31) == 0) sh[tid >> 5] = beta;
+  __syncthreads();
+  if (tid < 32) {
+    double x = tid < NT / 32 ? sh[tid] : 0.0;
+    x = wmax_d(x);
+    if (tid == 0) partial[blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = x;
+  }
+}
+
+// fixed-order max / sum over n partials (single block)
+__global__ void __launch_bounds__(1024) k_reduce_partials(const double* __restrict__ partial, long long n, int is_max,
+                                                          double* __restrict__ out) {
+  __shared__ double sh[32];
+  double v = 0.0;
+  for (long long b = threadIdx.x; b < n; b += blockDim.x) v = is_max ? fmax(v, partial[b]) : v + partial[b];
+  v = is_max ? wmax_d(v) : wsum_d(v);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double x = sh[threadIdx.x];
+    x = is_max ? wmax_d(x) : wsum_d(x);
+    if (threadIdx.x == 0) *out = x;
+  }
+}
+
+// sum of pre over the unique points, block partials (level_pressure, mod_lib.f90:507-537)
+__global__ void __launch_bounds__(NT) k_sum(Geom g, const double* __restrict__ a, double* __restrict__ partial) {
+  const int i = blockIdx.x * BX + threadIdx.x + 1;
+  const int j = blockIdx.y * BY + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  double s = (i <= g.n1 && j <= g.n2) ? a[off(g, i, j, k)] : 0.0;
+  __shared__ double sh[NT / 32];
+  const int tid = threadIdx.x + BX * threadIdx.y;
+  s = wsum_d(s);
+  if ((tid & 31) == 0) sh[tid >> 5] = s;
+  __syncthreads();
+  if (tid < 32) {
+    double x = tid < NT / 32 ? sh[tid] : 0.0;
+    x = wsum_d(x);
+    if (tid == 0) partial[blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = x;
+  }
+}
+__global__ void __launch_bounds__(NT) k_sub_mean(Geom g, const double* __restrict__ sum, double* __restrict__ pre) {
+  PT
+  const double m = *sum / (double)g.n1 / (double)g.n2 / (double)g.n3;
+  pre[p] = pre[p] - m;
+}
+
+// apply_CT_forcing (usr_func.f90:909-1049, idealized branch): label 0/7 -> u = 0; 5 -> inflow
+__global__ void __launch_bounds__(NT) k_mask(Geom g, const uint8_t* __restrict__ label, double u_in,
+                                             double* __restrict__ u, double* __restrict__ v, double* __restrict__ w) {
+  PT
+  const uint8_t lb = label[p];
+  if (lb == 0 || lb == 7) {
+    u[p] = 0.0;
+    v[p] = 0.0;
+    w[p] = 0.0;
+  } else if (lb == 5) {
+    w[p] = u_in;
+    v[p] = 0.0;
+    u[p] = 0.0;
+  }
+}
+
+}  // namespace impact
+
+using namespace impact;
+
+// =========================================================================================
+// case life cycle
+// =========================================================================================
+static long long nblocks(const Geom& g) {
+  const dim3 d = grid3(g);
+  return (long long)d.x * d.y * d.z;
+}
+
+extern "C" long long impact_b200_case_bytes(int N1, int N2, int N3, int precision) {
+  const Geom g = make_geom(N1, N2, N3);
+  const long long f = g.nfield * 8;
+  long long b = f * (IMPACT_B200_NFIELDS + 3);            // fields + work
+  b += g.nfield;                                          // labels
+  if (precision == 0)
+    b += 8 * f;                                           // FP64 Krylov set
+  else
+    b += f + 10 * (f / 2);                                // r64 + FP32 r, e + 8 inner fields
+  b += 2 * reduce_partial_doubles(g, 4) * 8 + (1 << 20);  // reduction scratch, coefficients
+  return b;
+}
+
+static int case_alloc(CaseState& s, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) return impact_set_error(e, "cudaMalloc (case)", __FILE__, __LINE__);
+  s.allocs.push_back(*p);
+  return 0;
+}
+
+extern "C" int impact_b200_case_destroy(impact_b200_case* c) {
+  if (!c) return 0;
+  CaseState& s = c->s;
+  cudaSetDevice(s.device);
+  if (s.stream) cudaStreamSynchronize(s.stream);
+  for (void* p : s.allocs) cudaFree(p);
+  if (s.hscal) cudaFreeHost(s.hscal);
+  if (s.scal_host) cudaFreeHost(s.scal_host);
+  if (s.mw.scal64_host) cudaFreeHost(s.mw.scal64_host);
+  if (s.own_stream && s.stream) cudaStreamDestroy(s.stream);
+  delete c;
+  return 0;
+}
+
+extern "C" int impact_b200_case_create(const impact_b200_case_desc* desc, const impact_b200_coeffs* co,
+                                       impact_b200_case** out) {
+  if (!desc || !co || !out) return impact_set_error_msg(-1, "impact_b200_case_create: null argument");
+  *out = nullptr;
+  if (desc->N1 < 9 || desc->N2 < 9 || desc->N3 < 9)
+    return impact_set_error_msg(-1, "impact_b200_case_create: need at least 8 unique points per axis");
+  if (desc->precision != 0 && desc->precision != 1)
+    return impact_set_error_msg(-1, "impact_b200_case_create: precision must be 0 (FP64) or 1 (mixed)");
+  for (int a = 0; a < 3; ++a)
+    if (!co->axis[a]) return impact_set_error_msg(-1, "impact_b200_case_create: missing coefficient tables");
+  IMPACT_CUDA_CHECK(cudaSetDevice(desc->device));
+  impact_b200_case* c = new impact_b200_case();
+  CaseState& s = c->s;
+  s.device = desc->device;
+  s.precision = desc->precision;
+  s.g = make_geom(desc->N1, desc->N2, desc->N3);
+  const Geom& g = s.g;
+  int rc = 0;
+  if (desc->stream) {
+    s.stream = static_cast<cudaStream_t>(desc->stream);
+  } else {
+    cudaError_t e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete c;
+      return impact_set_error(e, "cudaStreamCreate", __FILE__, __LINE__);
+    }
+    s.own_stream = true;
+  }
+  const int Nax[3] = {desc->N1, desc->N2, desc->N3};
+  // ---- coefficients: 12 tables per axis + 2 dt row-sum tables per axis ----
+  size_t total = 0;
+  size_t sz[3][14];
+  for (int a = 0; a < 3; ++a) {
+    const size_t M = Nax[a];
+    const size_t t6 = 6 * (M + 1), t7 = 7 * (M + 1), t3 = 3 * M, tr = M + 1;
+    const size_t tmp[14] = {t6, t6, t6, t6, t7, t7, t7, t7, t7, t7, t7, t3, tr, tr};
+    for (int q = 0; q < 14; ++q) {
+      sz[a][q] = tmp[q];
+      total += tmp[q];
+    }
+  }
+  std::vector<double> h64(total);
+  std::vector<float> h32(total);
+  size_t o = 0;
+  size_t offs[3][14];
+  for (int a = 0; a < 3; ++a) {
+    const impact_b200_axis_tables* t = co->axis[a];
+    const double* src[12] = {t->cG, t->cD, t->cIpu, t->cIup, t->cNpU, t->cNpD, t->cNuU, t->cNuD, t->cp1, t->cpp, t->cuu, t->cdg};
+    for (int q = 0; q < 12; ++q) {
+      if (!src[q]) {
+        impact_b200_case_destroy(c);
+        return impact_set_error_msg(-1, "impact_b200_case_create: null coefficient table");
+      }
+      offs[a][q] = o;
+      std::memcpy(&h64[o], src[q], sz[a][q] * sizeof(double));
+      o += sz[a][q];
+    }
+    // row sums of |cpp| and |cp1| (get_dtime), in the reference's summation order
+    offs[a][12] = o;
+    offs[a][13] = o + sz[a][12];
+    const size_t M = Nax[a];
+    for (size_t r = 0; r <= M; ++r) {
+      double spp = 0.0, sp1 = 0.0;
+      for (int l = 0; l < 7; ++l) {
+        spp = spp + std::fabs(t->cpp[r * 7 + l]);
+        sp1 = sp1 + std::fabs(t->cp1[r * 7 + l]);
+      }
+      h64[o + r] = spp;
+      h64[o + sz[a][12] + r] = sp1;
+    }
+    o += sz[a][12] + sz[a][13];
+  }
+  for (size_t q = 0; q < total; ++q) h32[q] = static_cast<float>(h64[q]);
+  rc |= case_alloc(s, (void**)&s.coef64, total * sizeof(double));
+  rc |= case_alloc(s, (void**)&s.coef32, total * sizeof(float));
+  if (rc) {
+    impact_b200_case_destroy(c);
+    return -1;
+  }
+  cudaMemcpy(s.coef64, h64.data(), total * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(s.coef32, h32.data(), total * sizeof(float), cudaMemcpyHostToDevice);
+  for (int a = 0; a < 3; ++a) {
+    const double* b = s.coef64;
+    const float* f = s.coef32;
+#define SETC(fld, q)                 \
+  s.c64.fld[a] = b + offs[a][q];     \
+  s.c32.fld[a] = f + offs[a][q];
+    SETC(cG, 0) SETC(cD, 1) SETC(cIpu, 2) SETC(cIup, 3) SETC(cNpU, 4) SETC(cNpD, 5) SETC(cNuU, 6) SETC(cNuD, 7)
+    SETC(cp1, 8) SETC(cpp, 9) SETC(cuu, 10) SETC(cdg, 11)
+#undef SETC
+    s.dt.spp[a] = b + offs[a][12];
+    s.dt.sp1[a] = b + offs[a][13];
+  }
+  // ---- fields ----
+  const size_t fb = (size_t)g.nfield * sizeof(double);
+  for (int q = 0; q < IMPACT_B200_NFIELDS; ++q) rc |= case_alloc(s, (void**)&s.f[q], fb);
+  for (int q = 0; q < 3; ++q) rc |= case_alloc(s, (void**)&s.work[q], fb);
+  rc |= case_alloc(s, (void**)&s.label, (size_t)g.nfield);
+  const size_t pd = (size_t)reduce_partial_doubles(g, 4) * sizeof(double);
+  rc |= case_alloc(s, (void**)&s.partial, pd);
+  rc |= case_alloc(s, (void**)&s.dscal, 64 * sizeof(double));
+  if (s.precision == 0) {
+    KrylovWork<double>& w = s.kw64;
+    double** pf[8] = {&w.rr, &w.rh, &w.pp, &w.Ap, &w.Ar, &w.z1, &w.z2, &w.comp};
+    for (double** q : pf) rc |= case_alloc(s, (void**)q, fb);
+    w.partial = s.partial;
+    w.partial_capacity = pd / sizeof(double);
+    rc |= case_alloc(s, (void**)&w.scal, sizeof(SolverScalars));
+  } else {
+    MixedWork& w = s.mw;
+    const size_t fb32 = (size_t)g.nfield * sizeof(float);
+    rc |= case_alloc(s, (void**)&w.r64, fb);
+    rc |= case_alloc(s, (void**)&w.r32, fb32);
+    rc |= case_alloc(s, (void**)&w.e32, fb32);
+    float** pf[8] = {&w.inner.rr, &w.inner.rh, &w.inner.pp, &w.inner.Ap, &w.inner.Ar, &w.inner.z1, &w.inner.z2, &w.inner.comp};
+    for (float** q : pf) rc |= case_alloc(s, (void**)q, fb32);
+    w.inner.partial = s.partial;
+    w.inner.partial_capacity = pd / sizeof(double);
+    rc |= case_alloc(s, (void**)&w.inner.scal, sizeof(SolverScalars));
+    rc |= case_alloc(s, (void**)&w.partial64, pd);
+  }
+  if (rc) {
+    impact_b200_case_destroy(c);
+    return -1;
+  }
+  cudaError_t e = cudaMallocHost((void**)&s.hscal, 64 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&s.scal_host, sizeof(SolverScalars));
+  if (e != cudaSuccess) {
+    impact_b200_case_destroy(c);
+    return impact_set_error(e, "cudaMallocHost", __FILE__, __LINE__);
+  }
+  s.kw64.scal_host = s.scal_host;
+  s.mw.inner.scal_host = s.scal_host;
+  // zero every field so that the ghost layers hold defined values
+  for (void* p : s.allocs) (void)p;
+  for (int q = 0; q < IMPACT_B200_NFIELDS; ++q) cudaMemsetAsync(s.f[q], 0, fb, s.stream);
+  for (int q = 0; q < 3; ++q) cudaMemsetAsync(s.work[q], 0, fb, s.stream);
+  cudaMemsetAsync(s.label, 1, (size_t)g.nfield, s.stream);
+  if (s.precision == 0) {
+    KrylovWork<double>& w = s.kw64;
+    double* pf[8] = {w.rr, w.rh, w.pp, w.Ap, w.Ar, w.z1, w.z2, w.comp};
+    for (double* q : pf) cudaMemsetAsync(q, 0, fb, s.stream);
+  } else {
+    MixedWork& w = s.mw;
+    const size_t fb32 = (size_t)g.nfield * sizeof(float);
+    cudaMemsetAsync(w.r64, 0, fb, s.stream);
+    cudaMemsetAsync(w.r32, 0, fb32, s.stream);
+    cudaMemsetAsync(w.e32, 0, fb32, s.stream);
+    float* pf[8] = {w.inner.rr, w.inner.rh, w.inner.pp, w.inner.Ap, w.inner.Ar, w.inner.z1, w.inner.z2, w.inner.comp};
+    for (float* q : pf) cudaMemsetAsync(q, 0, fb32, s.stream);
+  }
+  e = cudaStreamSynchronize(s.stream);
+  if (e != cudaSuccess) {
+    impact_b200_case_destroy(c);
+    return impact_set_error(e, "case init", __FILE__, __LINE__);
+  }
+  *out = c;
+  return 0;
+}
+
+extern "C" int impact_b200_case_upload(impact_b200_case* c, int field, const double* host) {
+  if (!c || !host || field < 0 || field >= IMPACT_B200_NFIELDS)
+    return impact_set_error_msg(-1, "impact_b200_case_upload: bad arguments");
+  CaseState& s = c->s;
+  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  IMPACT_CUDA_CHECK(cudaMemcpyAsync(s.f[field], host, (size_t)s.g.nfield * sizeof(double), cudaMemcpyHostToDevice, s.stream));
+  IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
+  return 0;
+}
+extern "C" int impact_b200_case_download(impact_b200_case* c, int field, double* host) {
+  if (!c || !host || field < 0 || field >= IMPACT_B200_NFIELDS)
+    return impact_set_error_msg(-1, "impact_b200_case_download: bad arguments");
+  CaseState& s = c->s;
+  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  IMPACT_CUDA_CHECK(cudaMemcpyAsync(host, s.f[field], (size_t)s.g.nfield * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+  IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
+  return 0;
+}
+extern "C" int impact_b200_case_set_labels(impact_b200_case* c, const uint8_t* host) {
+  if (!c || !host) return impact_set_error_msg(-1, "impact_b200_case_set_labels: bad arguments");
+  CaseState& s = c->s;
+  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  IMPACT_CUDA_CHECK(cudaMemcpyAsync(s.label, host, (size_t)s.g.nfield, cudaMemcpyHostToDevice, s.stream));
+  IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
+  return 0;
+}
+extern "C" double* impact_b200_case_field_ptr(impact_b200_case* c, int field) {
+  if (!c || field < 0 || field >= IMPACT_B200_NFIELDS) return nullptr;
+  return c->s.f[field];
+}
+extern "C" void* impact_b200_case_stream(impact_b200_case* c) { return c ? (void*)c->s.stream : nullptr; }
+
+static SolverOpts to_opts(const impact_b200_solver_params* p) {
+  SolverOpts o{};
+  o.tol_rel = p->tol_rel;
+  o.tol_abs_inf = p->tol_abs_inf;
+  o.max_it = p->max_it;
+  o.n_sweeps = p->n_sweeps;
+  o.omega = p->omega;
+  o.init_yes = p->init_yes;
+  o.check_every = p->check_every > 0 ? p->check_every : 1;
+  return o;
+}
+
+static int run_poisson(CaseState& s, const double* b, double* x, const impact_b200_solver_params* p,
+                       impact_b200_solver_result* r) {
+  SolverResult res{};
+  int inner = 0;
+  int rc;
+  if (s.precision == 0) {
+    rc = bicgstab<double>(s.g, s.c64, to_opts(p), b, x, s.kw64, s.stream, &res);
+  } else {
+    SolverOpts outer = to_opts(p);
+    SolverOpts in = to_opts(p);
+    in.tol_rel = p->inner_tol_rel > 0 ? p->inner_tol_rel : 1e-4;
+    in.tol_abs_inf = 0.0;
+    in.max_it = p->inner_max_it > 0 ? p->inner_max_it : p->max_it * 4;
+    outer.max_it = p->max_it;
+    if (p->init_yes) {
+      cudaMemsetAsync(x, 0, (size_t)s.g.nfield * sizeof(double), s.stream);
+    }
+    rc = mixed_solve(s.g, s.c64, s.c32, outer, in, b, x, s.mw, s.stream, &res, &inner);
+  }
+  if (rc) return rc;
+  if (r) {
+    r->iterations = res.iterations;
+    r->inner_iterations = inner;
+    r->status = res.status;
+    r->res_inf = res.res_inf;
+    r->res_two = res.res_two;
+    r->b_two = res.b_two;
+  }
+  return 0;
+}
+
+extern "C" int impact_b200_case_poisson(impact_b200_case* c, int field_b, int field_x,
+                                        const impact_b200_solver_params* p, impact_b200_solver_result* r) {
+  if (!c || !p || field_b < 0 || field_x < 0 || field_b >= IMPACT_B200_NFIELDS || field_x >= IMPACT_B200_NFIELDS ||
+      field_b == field_x)
+    return impact_set_error_msg(-1, "impact_b200_case_poisson: bad arguments");
+  CaseState& s = c->s;
+  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  int rc = run_poisson(s, s.f[field_b], s.f[field_x], p, r);
+  if (rc) return rc;
+  IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
+  IMPACT_CUDA_CHECK(cudaGetLastError());
+  return 0;
+}
+
+static double stab_host[41];
+static bool stab_ready = false;
+
+static void stability_limits(double* lim) {
+  // first r > 0 with |1 + z + z^2/2 + z^3/6| = 1 on the ray z = r(-sin t + i cos t), t = n pi / 80
+  for (int n = 0; n <= 40; ++n) {
+    const double t = n * 3.14159265358979323846 / 80.0;
+    auto g = [t](double r) {
+      const double zr = -r * std::sin(t), zi = r * std::cos(t);
+      const double z2r = zr * zr - zi * zi, z2i = 2.0 * zr * zi;
+      const double z3r = z2r * zr - z2i * zi, z3i = z2r * zi + z2i * zr;
+      const double re = 1.0 + zr + 0.5 * z2r + z3r / 6.0, im = zi + 0.5 * z2i + z3i / 6.0;
+      return re * re + im * im - 1.0;
+    };
+    double lo = 1e-3, hi = lo;
+    while (g(hi) < 0.0 && hi < 10.0) {
+      lo = hi;
+      hi += 1e-3;
+    }
+    for (int it = 0; it < 200; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      (g(mid) < 0.0 ? lo : hi) = mid;
+    }
+    lim[n] = 0.5 * (lo + hi);
+  }
+}
+
+extern "C" int impact_b200_case_step(impact_b200_case* c, const impact_b200_step_params* p,
+                                     impact_b200_step_state* st, int nsteps) {
+  if (!c || !p || !st || nsteps < 0) return impact_set_error_msg(-1, "impact_b200_case_step: bad arguments");
+  CaseState& s = c->s;
+  const Geom& g = s.g;
+  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  if (!stab_ready) {
+    stability_limits(stab_host);
+    stab_ready = true;
+  }
+  IMPACT_CUDA_CHECK(cudaMemcpyToSymbolAsync(c_stab, stab_host, sizeof(stab_host), 0, cudaMemcpyHostToDevice, s.stream));
+  const dim3 gr = grid3(g), bl(BX, BY);
+  const long long nb = nblocks(g);
+  double* vel[3] = {s.f[IMPACT_B200_VEL1], s.f[IMPACT_B200_VEL2], s.f[IMPACT_B200_VEL3]};
+  double* nl[3] = {s.f[IMPACT_B200_NL1], s.f[IMPACT_B200_NL2], s.f[IMPACT_B200_NL3]};
+  double* rhs[3] = {s.f[IMPACT_B200_RHS1], s.f[IMPACT_B200_RHS2], s.f[IMPACT_B200_RHS3]};
+  double* pre = s.f[IMPACT_B200_PRE];
+  double* res = s.f[IMPACT_B200_RES];
+  const double multL = 1.0 / p->Re;
+  for (int step = 0; step < nsteps; ++step) {
+    // ---- get_dtime ----
+    k_dtime<<<gr, bl, 0, s.stream>>>(g, s.c64, s.dt, p->Re, vel[0], vel[1], vel[2], s.partial);
+    k_reduce_partials<<<1, 1024, 0, s.stream>>>(s.partial, nb, 1, s.dscal);
+    IMPACT_CUDA_CHECK(cudaMemcpyAsync(s.hscal, s.dscal, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
+    const double beta1 = s.hscal[0];
+    double dt;
+    const double dinv = beta1 / p->CFL;
+    if (std::fabs(dinv) < 1.0 / p->dtime_max)
+      dt = p->dtime_max;
+    else
+      dt = 1.0 / dinv;
+    if (st->timestep == 0 && dt > p->dtime0) dt = p->dtime0;
+    st->dtime = dt;
+    // ---- three RK substeps ----
+    for (int sub = 0; sub < 3; ++sub) {
+      k_interp_vel3<<<gr, bl, 0, s.stream>>>(g, s.c64, vel[0], vel[1], vel[2], s.work[0], s.work[1], s.work[2]);
+      const double mb = dt * bRK[sub], ma = dt * aRK[sub];
+      const int use_old = sub != 0;
+      k_nl_rhs<0><<<gr, bl, 0, s.stream>>>(g, s.c64, multL, mb, ma, use_old, vel[0], s.work[0], s.work[1], s.work[2], nl[0], rhs[0]);
+      k_nl_rhs<1><<<gr, bl, 0, s.stream>>>(g, s.c64, multL, mb, ma, use_old, vel[1], s.work[0], s.work[1], s.work[2], nl[1], rhs[1]);
+      k_nl_rhs<2><<<gr, bl, 0, s.stream>>>(g, s.c64, multL, mb, ma, use_old, vel[2], s.work[0], s.work[1], s.work[2], nl[2], rhs[2]);
+      const double ab = aRK[sub] + bRK[sub];
+      k_scale_pre<<<gr, bl, 0, s.stream>>>(g, ab, dt, 0, pre);
+      launch_divergence2<double>(g, s.c64.cD[0], s.c64.cD[1], s.c64.cD[2], rhs[0], rhs[1], rhs[2], res, s.stream);
+      impact_b200_solver_result r{};
+      int rc = run_poisson(s, res, pre, &p->poisson, &r);
+      if (rc) return rc;
+      st->poisson_iterations[sub] = r.iterations;
+      st->inner_iterations[sub] = r.inner_iterations;
+      st->poisson_status[sub] = r.status;
+      st->poisson_res_rel[sub] = r.b_two > 0.0 ? r.res_two / r.b_two : 0.0;
+      k_project<<<gr, bl, 0, s.stream>>>(g, s.c64, pre, rhs[0], rhs[1], rhs[2], vel[0], vel[1], vel[2]);
+      k_scale_pre<<<gr, bl, 0, s.stream>>>(g, ab, dt, 1, pre);
+    }
+    st->timestep += 1;
+    st->time += dt;
+    const double u_in = p->U0 * (1.0 + 0.5 * std::sin(2.0 * 3.14159265358979323846 * st->time / p->T_pulse));
+    k_mask<<<gr, bl, 0, s.stream>>>(g, s.label, u_in, vel[0], vel[1], vel[2]);
+    if (p->level_pressure) {
+      k_sum<<<gr, bl, 0, s.stream>>>(g, pre, s.partial);
+      k_reduce_partials<<<1, 1024, 0, s.stream>>>(s.partial, nb, 0, s.dscal + 1);
+      k_sub_mean<<<gr, bl, 0, s.stream>>>(g, s.dscal + 1, pre);
+    }
+  }
+  IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
+  IMPACT_CUDA_CHECK(cudaGetLastError());
+  return 0;
+}

@@ -1,0 +1,323 @@
+"""impact_b200 -- Python host side of the B200 implementation of IMPACT's fractional-step hot path.
+
+Everything here is a thin ctypes layer over ``libimpact_b200.so`` (the CUDA kernels and the C
+ABI declared in ``include/impact_b200.h``).  There is no CPU fallback: if the shared library is
+missing or cannot be loaded, every entry point raises.
+
+* ``Grid``       -- coordinates and FD coefficient tables of one periodic grid (FD_coeffs,
+                    mod_coeffs.f90:37-112; get_stencil, mod_coeffs.f90:1048).
+* ``Case``       -- one vessel case resident on one GPU: fields, Poisson solve, RK3 steps.
+* ``launchers``  -- the reference's launcher FFI (``gradient_launcher_`` ...) on device pointers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libimpact_b200.so")
+_lib = None
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_u8p = C.POINTER(C.c_uint8)
+_vp = C.c_void_p
+
+FIELDS = {"vel1": 0, "vel2": 1, "vel3": 2, "pre": 3, "nl1": 4, "nl2": 5, "nl3": 6, "res": 7,
+          "rhs1": 8, "rhs2": 9, "rhs3": 10}
+
+
+class ImpactError(RuntimeError):
+    pass
+
+
+class AxisTables(C.Structure):
+    _fields_ = [(n, _dp) for n in ("cG", "cD", "cIpu", "cIup", "cNpU", "cNpD", "cNuU", "cNuD",
+                                   "cp1", "cpp", "cuu", "cdg")]
+
+
+class Coeffs(C.Structure):
+    _fields_ = [("axis", C.POINTER(AxisTables) * 3)]
+
+
+class CaseDesc(C.Structure):
+    _fields_ = [("N1", C.c_int), ("N2", C.c_int), ("N3", C.c_int), ("precision", C.c_int),
+                ("device", C.c_int), ("stream", _vp)]
+
+
+class SolverParams(C.Structure):
+    _fields_ = [("tol_rel", C.c_double), ("tol_abs_inf", C.c_double), ("max_it", C.c_int),
+                ("n_sweeps", C.c_int), ("omega", C.c_double), ("init_yes", C.c_int),
+                ("check_every", C.c_int), ("inner_tol_rel", C.c_double), ("inner_max_it", C.c_int)]
+
+
+class SolverResult(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("inner_iterations", C.c_int), ("status", C.c_int),
+                ("res_inf", C.c_double), ("res_two", C.c_double), ("b_two", C.c_double)]
+
+
+class StepParams(C.Structure):
+    _fields_ = [("Re", C.c_double), ("CFL", C.c_double), ("dtime_max", C.c_double),
+                ("dtime0", C.c_double), ("U0", C.c_double), ("T_pulse", C.c_double),
+                ("level_pressure", C.c_int), ("poisson", SolverParams)]
+
+
+class StepState(C.Structure):
+    _fields_ = [("time", C.c_double), ("dtime", C.c_double), ("timestep", C.c_int),
+                ("poisson_iterations", C.c_int * 3), ("inner_iterations", C.c_int * 3),
+                ("poisson_res_rel", C.c_double * 3), ("poisson_status", C.c_int * 3)]
+
+
+_PP = C.POINTER(_dp)  # double**
+
+
+def lib():
+    """Load libimpact_b200.so (raises ImpactError when it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImpactError(f"{LIB_PATH} is missing: build it with `python -m impact_b200.build` "
+                          "(there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    i, d = C.c_int, C.c_double
+    P = C.POINTER
+    sigs = {
+        "impact_b200_last_error": (C.c_char_p, []),
+        "impact_b200_clear_error": (None, []),
+        "impact_b200_version": (i, []),
+        "impact_b200_set_stream": (None, [_vp]),
+        "impact_b200_sync": (i, []),
+        "impact_b200_axis_coords": (i, [i, d, i, _dp, _dp]),
+        "impact_b200_axis_coeffs": (i, [i, _dp, _dp, P(AxisTables)]),
+        "impact_b200_fd_exact": (i, [i, i, d, _dp]),
+        "impact_b200_case_create": (i, [P(CaseDesc), P(Coeffs), P(_vp)]),
+        "impact_b200_case_destroy": (i, [_vp]),
+        "impact_b200_case_bytes": (C.c_longlong, [i, i, i, i]),
+        "impact_b200_case_upload": (i, [_vp, i, _dp]),
+        "impact_b200_case_download": (i, [_vp, i, _dp]),
+        "impact_b200_case_set_labels": (i, [_vp, _u8p]),
+        "impact_b200_case_field_ptr": (_vp, [_vp, i]),
+        "impact_b200_case_stream": (_vp, [_vp]),
+        "impact_b200_case_poisson": (i, [_vp, i, i, P(SolverParams), P(SolverResult)]),
+        "impact_b200_case_step": (i, [_vp, P(StepParams), P(StepState), i]),
+        "impact_b200_jacobi_solve": (i, [i, i, i, i, i, i, d, _dp, _dp, _dp, _dp, _dp, i, d, i, _ip, _dp]),
+        "impact_b200_product_scalar": (i, [i, i, i, _vp, _vp, _dp]),
+        # reference launcher FFI (every argument by reference)
+        "gradient_launcher_": (None, [_ip] * 6 + [_PP] * 3),
+        "divergence_launcher_": (None, [_ip] * 6 + [_PP] * 3),
+        "divergence2_launcher_": (None, [_ip] * 6 + [_PP] * 5),
+        "helmholtz_explicit_launcher_": (None, [_ip] * 7 + [_dp] + [_PP] * 5),
+        "nonlinear_upwind_launcher_": (None, [_ip] * 6 + [_PP] * 5),
+        "interpolate2_pre_vel_launcher_": (None, [_ip] * 6 + [_PP] * 3),
+        "interpolate2_vel_pre_launcher_": (None, [_ip] * 6 + [_PP] * 3),
+        "axpby_launcher_": (None, [_ip] * 3 + [_dp] * 2 + [_PP] * 3),
+        "jor_launcher_": (None, [_ip] * 8 + [_dp] + [_PP] * 11),
+        "get_ghost_launcher_": (None, [_ip] * 3 + [_PP] * 7),
+        "pressure_bc_launcher_": (None, [_ip] * 7 + [_dp] * 3 + [_PP] * 2),
+        "jacobi_launcher_": (None, [_ip] * 8 + [_dp] + [_PP] * 6),
+        "product_dg_relax_launcher_": (None, [_ip] * 8 + [_PP] * 5),
+    }
+    for name, (res, args) in sigs.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return lib().impact_b200_last_error().decode()
+
+
+def check(rc: int, what: str = ""):
+    if rc != 0:
+        raise ImpactError(f"{what}: {last_error()} (rc={rc})")
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"], "float64 C-contiguous array expected"
+    return a.ctypes.data_as(_dp)
+
+
+# Interior table widths (mod_dims.f90 ncb*(4)): 7 central, 6 gradient / divergence.
+TABLE_WIDTH = {"cG": 6, "cD": 6, "cIpu": 6, "cIup": 6, "cNpU": 7, "cNpD": 7, "cNuU": 7, "cNuD": 7,
+               "cp1": 7, "cpp": 7, "cuu": 7}
+
+
+class Grid:
+    """Coordinates and every coefficient table of a periodic grid with N = (N1, N2, N3) points.
+
+    kinds[a] = 0 equidistant, 1 sinh-stretched.  Tables are numpy arrays in the reference layout.
+    """
+
+    def __init__(self, N, L=(1.0, 1.0, 1.0), kinds=(0, 0, 0)):
+        self.N = tuple(int(n) for n in N)
+        self.L = tuple(float(x) for x in L)
+        self.kinds = tuple(int(k) for k in kinds)
+        L_ = lib()
+        self.xp, self.xu, self.tab = [], [], {n: [None] * 3 for n in list(TABLE_WIDTH) + ["cdg"]}
+        self._axis = []
+        for a in range(3):
+            M = self.N[a]
+            xp, xu = np.zeros(M + 7), np.zeros(M + 7)
+            check(L_.impact_b200_axis_coords(M, self.L[a], self.kinds[a], _ptr(xp), _ptr(xu)), "axis_coords")
+            t = AxisTables()
+            for n, w in TABLE_WIDTH.items():
+                arr = np.zeros(w * (M + 1))
+                self.tab[n][a] = arr
+                setattr(t, n, _ptr(arr))
+            cdg = np.zeros(3 * M)
+            self.tab["cdg"][a] = cdg
+            t.cdg = _ptr(cdg)
+            check(L_.impact_b200_axis_coeffs(M, _ptr(xp), _ptr(xu), C.byref(t)), "axis_coeffs")
+            self.xp.append(xp)
+            self.xu.append(xu)
+            self._axis.append(t)
+        self.coeffs = Coeffs()
+        for a in range(3):
+            self.coeffs.axis[a] = C.pointer(self._axis[a])
+
+    @property
+    def shape(self):
+        N1, N2, N3 = self.N
+        return (N3 + 7, N2 + 7, N1 + 7)
+
+    @property
+    def cells(self):
+        return (self.N[0] - 1) * (self.N[1] - 1) * (self.N[2] - 1)
+
+    def zeros(self, n=None):
+        return np.zeros(self.shape if n is None else (n,) + self.shape)
+
+    def interior(self, a):
+        N1, N2, N3 = self.N
+        return a[..., 4:N3 + 3, 4:N2 + 3, 4:N1 + 3]
+
+
+def solver_params(tol_rel=1e-8, tol_abs_inf=0.0, max_it=2000, n_sweeps=4, omega=0.8, init_yes=0,
+                  check_every=4, inner_tol_rel=1e-4, inner_max_it=0) -> SolverParams:
+    return SolverParams(tol_rel, tol_abs_inf, max_it, n_sweeps, omega, init_yes, check_every,
+                        inner_tol_rel, inner_max_it)
+
+
+def step_params(Re=200.0, CFL=0.2, dtime_max=1e-2, dtime0=1e9, U0=1.0, T_pulse=1.0, level_pressure=1,
+                **solver) -> StepParams:
+    return StepParams(Re, CFL, dtime_max, dtime0, U0, T_pulse, level_pressure, solver_params(**solver))
+
+
+class Case:
+    """One simulation case resident on one GPU (impact_b200_case_* of include/impact_b200.h)."""
+
+    def __init__(self, grid: Grid, precision: int = 0, device: int = 0, stream=None):
+        self.grid = grid
+        self.precision = precision
+        desc = CaseDesc(grid.N[0], grid.N[1], grid.N[2], precision, device, stream)
+        h = _vp()
+        check(lib().impact_b200_case_create(C.byref(desc), C.byref(grid.coeffs), C.byref(h)), "case_create")
+        self._h = h
+        self.state = StepState()
+
+    def close(self):
+        if self._h:
+            lib().impact_b200_case_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def bytes_needed(N, precision=0) -> int:
+        return int(lib().impact_b200_case_bytes(N[0], N[1], N[2], precision))
+
+    def upload(self, field, host: np.ndarray):
+        f = FIELDS[field] if isinstance(field, str) else field
+        check(lib().impact_b200_case_upload(self._h, f, _ptr(np.ascontiguousarray(host))), "case_upload")
+
+    def download(self, field, out: np.ndarray | None = None) -> np.ndarray:
+        f = FIELDS[field] if isinstance(field, str) else field
+        out = self.grid.zeros() if out is None else out
+        check(lib().impact_b200_case_download(self._h, f, _ptr(out)), "case_download")
+        return out
+
+    def set_labels(self, labels: np.ndarray):
+        lb = np.ascontiguousarray(labels, dtype=np.uint8)
+        check(lib().impact_b200_case_set_labels(self._h, lb.ctypes.data_as(_u8p)), "case_set_labels")
+
+    def field_ptr(self, field) -> int:
+        f = FIELDS[field] if isinstance(field, str) else field
+        return lib().impact_b200_case_field_ptr(self._h, f)
+
+    @property
+    def stream(self):
+        return lib().impact_b200_case_stream(self._h)
+
+    def poisson(self, b="res", x="pre", params: SolverParams | None = None) -> SolverResult:
+        params = solver_params() if params is None else params
+        r = SolverResult()
+        bi = FIELDS[b] if isinstance(b, str) else b
+        xi = FIELDS[x] if isinstance(x, str) else x
+        check(lib().impact_b200_case_poisson(self._h, bi, xi, C.byref(params), C.byref(r)), "case_poisson")
+        return r
+
+    def step(self, params: StepParams, nsteps: int = 1) -> StepState:
+        check(lib().impact_b200_case_step(self._h, C.byref(params), C.byref(self.state), nsteps), "case_step")
+        return self.state
+
+
+def fd_exact(abl, n, deltaX0):
+    cc = np.zeros(n)
+    check(lib().impact_b200_fd_exact(abl, n, float(deltaX0), _ptr(cc)), "fd_exact")
+    return cc
+
+
+def product_scalar(N, a_dev: int, b_dev: int) -> float:
+    out = C.c_double()
+    check(lib().impact_b200_product_scalar(N[0], N[1], N[2], a_dev, b_dev, C.byref(out)), "product_scalar")
+    return out.value
+
+
+def jacobi_solve(grid: Grid, rel: np.ndarray, bb: np.ndarray, omega=0.8, mode_j=20, tol_abs_inf=0.0,
+                 max_sweeps=100000, M=None):
+    """device_jacobi_solver replacement on host arrays; returns (sweeps, res_inf)."""
+    N1, N2, N3 = grid.N
+    M1, M2, M3 = M if M is not None else grid.N
+    sw, ri = C.c_int(), C.c_double()
+    c = grid.tab["cdg"]
+    check(lib().impact_b200_jacobi_solve(N1, N2, N3, M1, M2, M3, omega, _ptr(c[0]), _ptr(c[1]), _ptr(c[2]),
+                                         _ptr(rel), _ptr(bb), mode_j, tol_abs_inf, max_sweeps, C.byref(sw),
+                                         C.byref(ri)), "jacobi_solve")
+    return sw.value, ri.value
+
+
+class launchers:
+    """The reference's launcher FFI on device pointers (ints), every argument passed by reference."""
+
+    @staticmethod
+    def call(name, *args):
+        """args: ('i', int) | ('d', float) | ('p', device pointer)"""
+        conv = []
+        keep = []
+        for kind, v in args:
+            if kind == "i":
+                o = C.c_int(int(v))
+            elif kind == "d":
+                o = C.c_double(float(v))
+            else:
+                o = C.cast(C.c_void_p(int(v)), _dp)
+            keep.append(o)
+            conv.append(C.byref(o))
+        getattr(lib(), name)(*conv)
+        err = last_error()
+        if err:
+            lib().impact_b200_clear_error()
+            raise ImpactError(f"{name}: {err}")
+
+    @staticmethod
+    def sync():
+        check(lib().impact_b200_sync(), "sync")

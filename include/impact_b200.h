@@ -1,0 +1,221 @@
+/*
+ * impact_b200.h -- C ABI of the B200 (sm_100a) implementation of IMPACT's fractional-step
+ * hot path (GPU-IMPACT-CT).  Plain pointers and sizes only; no C++ or torch types.
+ *
+ * Part 1 -- the reference's own FFI.  IMPACT's Fortran wrappers (src/*_host.f90) bind the
+ * trailing-underscore launchers of src/*_launcher.cu through gfortran's implicit interface:
+ * every argument by reference, device arrays as double** (the Fortran c_ptr variables of
+ * mod_vars_GPU.f90).  This library exports the same symbols with the same arguments, so the
+ * unchanged *_host.f90 files link against it instead of the reference's .cu objects.  Arrays
+ * use the reference layout: column-major phi(-3:N1+3,-3:N2+3,-3:N3+3), nx_dev = N1+7;
+ * coefficient tables c(lo:hi,0:N) as c[i*nx_coef + (l-lo)]; cdg(-1:1,1:N,1:n_grids).
+ * Boundaries are periodic in all directions (the only case the reference kernels cover).
+ * The launchers run asynchronously on the library's current stream (impact_b200_set_stream,
+ * default: the legacy default stream, as the reference) and report errors through
+ * impact_b200_last_error(); like the reference launchers they return nothing.
+ *
+ * Part 2 -- device-resident entry points that replace whole Fortran loops (the GPU
+ * Poisson solve of jacobi_solver_host_v4.f90, BiCGstab_orig, one RK3 time step), so that
+ * fields stay in HBM between calls instead of crossing PCIe on every operator call.
+ *
+ * All functions returning int return 0 on success and a negative code on error; the
+ * message is available from impact_b200_last_error().
+ */
+#ifndef IMPACT_B200_H
+#define IMPACT_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ========================================================================================
+ * Part 1: reference launcher ABI
+ * ====================================================================================== */
+
+/* gradient_kernel_launcher.cu:12 -- grad = G_m phi (pressure -> velocity point m) */
+void gradient_launcher_(int* dimension_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nx_grad_coef,
+                        int* ny_grad_coef, double** phi_grad_dev, double** cGp_dev, double** grad_dev);
+/* divergence_kernel_launcher.cu:12 -- div (=, m=1 / +=, m=2,3) D_m phi */
+void divergence_launcher_(int* dimension_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nx_div_coef,
+                          int* ny_div_coef, double** phi_div_dev, double** div_dev, double** cD_dev);
+/* divergence2_kernel_launcher.cu:12 -- div = D1 u + D2 v + D3 w, phi = vel(:,:,:,1:3) packed */
+void divergence2_launcher_(int* nx_dev, int* ny_dev, int* nz_dev, int* nx_div_coef1, int* nx_div_coef2,
+                           int* nx_div_coef3, double** phi_div2_dev, double** div2_dev, double** cDu1_dev,
+                           double** cDv2_dev, double** cDw3_dev);
+/* helmholtz_explicit_kernel_launcher.cu:12 -- helm -= multL (cS1 u_xx + cS2 u_yy + cS3 u_zz) */
+void helmholtz_explicit_launcher_(int* component_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nxs1, int* nxs2,
+                                  int* nxs3, double* multL, double** vel1_dev, double** helm_dev,
+                                  double** cS1_helm_dev, double** cS2_helm_dev, double** cS3_helm_dev);
+/* Nonlinear_upwind_kernel_launcher.cu:12 -- nl (=/+=) pp * D^{up|down}_a vel, component_id = 3(m-1)+a;
+ * cN1 holds the table used where pp >= 0, cN21 the one used where pp < 0 */
+void nonlinear_upwind_launcher_(int* component_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nxn1, int* nyn1,
+                                double** pp_dev, double** vel_dev, double** nl_dev, double** cN1_dev,
+                                double** cN21_dev);
+/* interpolate2_pre_vel_kernel_launcher.cu:12 -- pressure -> velocity point m */
+void interpolate2_pre_vel_launcher_(int* dimension_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nxIpu1,
+                                    int* nyIpu1, double** phi_inter_pv_dev, double** cIpu_dev,
+                                    double** inter_pv_dev);
+/* interpolate2_vel_pre_kernel_launcher.cu:12 -- velocity point m -> pressure */
+void interpolate2_vel_pre_launcher_(int* dimension_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nxIup1,
+                                    int* nyIup1, double** phi_inter_vp_dev, double** cIup_dev,
+                                    double** inter_vp_dev);
+/* axpby_kernel_launcher.cu:12 -- z = a x + b y */
+void axpby_launcher_(int* nx_dev, int* ny_dev, int* nz_dev, double* a, double* b, double** d_x, double** d_y,
+                     double** d_z);
+/* jor_kernel_launcher.cu:12 -- one JOR sweep of the compact Laplacian cdg, boundary neighbours
+ * taken from the six ghost-face arrays.  The reference updates rel in place (a data race between
+ * neighbouring threads); this implementation is deterministic: it sweeps out of place into a
+ * library-owned buffer and copies the result back into rel. */
+void jor_launcher_(int* grid_id, int* nx_dev, int* ny_dev, int* nz_dev, int* ny_cdg1, int* ny_cdg2, int* ny_cdg3,
+                   int* nx_cdg1, double* omega, double** cdg1_dev, double** cdg2_dev, double** cdg3_dev,
+                   double** rel_dev, double** bb_dev, double** rear_ghost_dev, double** front_ghost_dev,
+                   double** upper_ghost_dev, double** lower_ghost_dev, double** west_ghost_dev,
+                   double** east_ghost_dev);
+/* get_ghost_launcher.cu:12 -- copy the six boundary planes of rel into the face arrays */
+void get_ghost_launcher_(int* nx_dev, int* ny_dev, int* nz_dev, double** rel_dev, double** rear_ghost_dev,
+                         double** front_ghost_dev, double** upper_ghost_dev, double** lower_ghost_dev,
+                         double** west_ghost_dev, double** east_ghost_dev);
+/* set_pressure_BC_kernel_launcher.cu:12 -- Dirichlet pressure on labelled cells (labels as FP64,
+ * the ct_geometry array of the reference).  Planes are matched with the Fortran index test
+ * k == k_start_index-1 of apply_pressure_BC_CT (usr_func.f90:857-897). */
+void pressure_bc_launcher_(int* type_id1, int* type_id2, int* type_id3, int* k_start_index, int* nx_dev,
+                           int* ny_dev, int* nz_dev, double* pre_inlet, double* pre_outlet, double* pre_outlet_2,
+                           double** ct_geometry_dev, double** rel_dev);
+/* jacobi_kernel_launcher.cu:12 -- comp = one damped-Jacobi sweep of rel (multigrid level grid_id) */
+void jacobi_launcher_(int* grid_id, int* nx_dev_g, int* ny_dev_g, int* nz_dev_g, int* ny_cdg1_g, int* ny_cdg2_g,
+                      int* ny_cdg3_g, int* nx_cdg1_g, double* omega_g, double** cdg1_dev3, double** cdg2_dev3,
+                      double** cdg3_dev3, double** rel_dev3, double** bb_dev3, double** comp_dev3);
+/* product_dg_relax_kernel_launcher.cu:12 -- comp = cdg Laplacian of rel (level grid_id) */
+void product_dg_relax_launcher_(int* grid_id, int* nx_dev_g, int* ny_dev_g, int* nz_dev_g, int* ny_cdg1_g,
+                                int* ny_cdg2_g, int* ny_cdg3_g, int* nx_cdg1_g, double** cdg1_dev2,
+                                double** cdg2_dev2, double** cdg3_dev2, double** rel_dev2, double** comp_dev2);
+
+/* ========================================================================================
+ * Part 2: library control and device-resident entry points
+ * ====================================================================================== */
+
+/* sticky message of the last error of the calling process ("" if none) */
+const char* impact_b200_last_error(void);
+void impact_b200_clear_error(void);
+int impact_b200_version(void);
+/* stream (a cudaStream_t) used by the Part 1 launchers; NULL = legacy default stream */
+void impact_b200_set_stream(void* stream);
+/* synchronise the launcher stream; returns the first pending CUDA error, if any */
+int impact_b200_sync(void);
+
+/* ---- grid set-up (mod_geometry.f90:37 / usr_geometry.f90:93; mod_coeffs.f90:37, 1048) ----
+ * Coordinates of one periodic axis with M points: xp, xu over indices -3..M+3 (M+7 values).
+ * kind 0 equidistant, 1 x(s) = L/2 (1 + sinh(2(s/(M-1) - 1/2)) / sinh 1). */
+int impact_b200_axis_coords(int M, double L, int kind, double* xp, double* xu);
+
+/* Every coefficient table of one periodic axis, FD_coeffs with mapping_yes = T.  Each pointer
+ * is caller memory: 6*(M+1) doubles for cG, cD, cIpu, cIup; 7*(M+1) for cNpU, cNpD, cNuU,
+ * cNuD, cp1, cpp, cuu; 3*M for cdg. */
+typedef struct {
+  double *cG, *cD, *cIpu, *cIup, *cNpU, *cNpD, *cNuU, *cNuD, *cp1, *cpp, *cuu, *cdg;
+} impact_b200_axis_tables;
+int impact_b200_axis_coeffs(int M, const double* xp, const double* xu, impact_b200_axis_tables* out);
+
+/* Exact equidistant finite-difference weights (diff_coeffs_exact, mod_coeffs.f90:598-751). */
+int impact_b200_fd_exact(int abl, int n, double deltaX0, double* cc);
+
+/* ---- one simulation case resident on one GPU ----------------------------------------- */
+typedef struct impact_b200_case impact_b200_case;
+
+typedef struct {
+  int N1, N2, N3;  /* IMPACT point counts; N-1 unique periodic points per axis */
+  int precision;   /* 0: FP64 throughout (plain drop-in); 1: mixed (FP32 inner Poisson solve,
+                      FP64 outer residual, correction, inner products and RHS operators) */
+  int device;      /* CUDA device ordinal */
+  void* stream;    /* cudaStream_t to run on; NULL: the case creates its own stream */
+} impact_b200_case_desc;
+
+typedef struct {
+  const impact_b200_axis_tables* axis[3]; /* host tables of the three axes (copied to the GPU) */
+} impact_b200_coeffs;
+
+/* field ids of impact_b200_case_upload/download/field_ptr */
+enum {
+  IMPACT_B200_VEL1 = 0, IMPACT_B200_VEL2 = 1, IMPACT_B200_VEL3 = 2, IMPACT_B200_PRE = 3,
+  IMPACT_B200_NL1 = 4, IMPACT_B200_NL2 = 5, IMPACT_B200_NL3 = 6, IMPACT_B200_RES = 7,
+  IMPACT_B200_RHS1 = 8, IMPACT_B200_RHS2 = 9, IMPACT_B200_RHS3 = 10, IMPACT_B200_NFIELDS = 11
+};
+
+int impact_b200_case_create(const impact_b200_case_desc* desc, const impact_b200_coeffs* coeffs,
+                            impact_b200_case** out);
+int impact_b200_case_destroy(impact_b200_case* c);
+/* device bytes held by a case of this size and precision (admission control) */
+long long impact_b200_case_bytes(int N1, int N2, int N3, int precision);
+/* whole padded field (nx*ny*nz doubles, reference layout) host <-> device, on the case stream */
+int impact_b200_case_upload(impact_b200_case* c, int field, const double* host);
+int impact_b200_case_download(impact_b200_case* c, int field, double* host);
+/* voxel labels (padded layout, one byte per point): 0 solid, 1 fluid, 5 inflow, 7 wall, 9/11 outlets */
+int impact_b200_case_set_labels(impact_b200_case* c, const uint8_t* host_labels);
+double* impact_b200_case_field_ptr(impact_b200_case* c, int field);
+void* impact_b200_case_stream(impact_b200_case* c);
+
+typedef struct {
+  double tol_rel;      /* ||b - A x||_2 <= tol_rel ||b||_2 (0 = off) */
+  double tol_abs_inf;  /* ||b - A x||_inf < tol_abs_inf (0 = off; the reference's epsU) */
+  int max_it;          /* BiCGstab iterations (outer refinements in mixed precision) */
+  int n_sweeps;        /* damped-Jacobi sweeps per preconditioner application (0 = none) */
+  double omega;        /* their relaxation factor (0.8 for the BiCGstab preconditioner) */
+  int init_yes;        /* 1: start from x = 0 */
+  int check_every;     /* iterations between host polls of the device convergence flag */
+  double inner_tol_rel;/* mixed precision: relative tolerance of each FP32 inner solve */
+  int inner_max_it;    /* mixed precision: iteration cap of each inner solve */
+} impact_b200_solver_params;
+
+typedef struct {
+  int iterations;       /* BiCGstab iterations (mixed: outer refinements) */
+  int inner_iterations; /* mixed precision: FP32 BiCGstab iterations summed over refinements */
+  int status;           /* 0 converged, 1 iteration cap, 2 breakdown, 3 non-finite */
+  double res_inf, res_two, b_two;
+} impact_b200_solver_result;
+
+/* Pressure Poisson solve A x = b on resident fields (BiCGstab_orig, mod_solvers.f90:1509-1935;
+ * A = product_div_grad, preconditioner = Jacobi sweeps of the compact cdg Laplacian). */
+int impact_b200_case_poisson(impact_b200_case* c, int field_b, int field_x, const impact_b200_solver_params* p,
+                             impact_b200_solver_result* r);
+
+typedef struct {
+  double Re, CFL, dtime_max, dtime0; /* get_dtime (mod_lib.f90:46-250), timeint_mode 1 */
+  double U0, T_pulse;                /* inflow u_z = U0 (1 + 0.5 sin(2 pi t / T)) on label 5 */
+  int level_pressure;                /* subtract the mean pressure after each step */
+  impact_b200_solver_params poisson;
+} impact_b200_step_params;
+
+typedef struct {
+  double time, dtime;
+  int timestep;
+  int poisson_iterations[3];
+  int inner_iterations[3];
+  double poisson_res_rel[3];
+  int poisson_status[3];
+} impact_b200_step_state;
+
+/* nsteps RK3 time steps (mod_timeint.f90:242-578) on the resident fields. */
+int impact_b200_case_step(impact_b200_case* c, const impact_b200_step_params* p, impact_b200_step_state* st,
+                          int nsteps);
+
+/* ---- device_jacobi_solver (jacobi_solver_host_v4.f90:5) replacement -------------------
+ * Host arrays rel (in/out) and bb in the reference layout.  Deterministic out-of-place JOR
+ * sweeps of the compact Laplacian on the device, periodic neighbours read in place (no ghost
+ * faces cross PCIe), stopping on the reference's heuristic relative-change test evaluated every
+ * mode_j sweeps, or when ||bb - A rel||_inf < tol_abs_inf (if > 0), or after max_sweeps.
+ * cdg1..3: host tables cdg(-1:1,1:N) of level 1.  Returns the sweeps done in *sweeps. */
+int impact_b200_jacobi_solve(int N1, int N2, int N3, int M1, int M2, int M3, double omega, const double* cdg1,
+                             const double* cdg2, const double* cdg3, double* rel, const double* bb, int mode_j,
+                             double tol_abs_inf, int max_sweeps, int* sweeps, double* res_inf);
+
+/* Deterministic FP64 inner product over the unique periodic points (product_scalar,
+ * mod_solvers.f90:2319-2354) of two device fields of a grid with N1 x N2 x N3 points.
+ * Uses a per-call scratch allocation for the block partials. */
+int impact_b200_product_scalar(int N1, int N2, int N3, const double* a_dev, const double* b_dev, double* result);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,918 @@
+/*
+ * impact_oracle.c -- CPU FP64 oracle for the IMPACT fractional-step hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (see impact_oracle.h).  Each routine names the reference
+ * routine it restates.  Loop order, summation order and the stencil index ranges follow
+ * the reference so that FP64 results agree to rounding; the only structural additions
+ * are OpenMP over the slowest axis and per-plane partial sums for the reductions (a
+ * deterministic, thread-count independent order).
+ */
+#include "impact_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define PI_D 3.14159265358979323846
+
+/* RK3 coefficients (mod_vars.f90:774-775). */
+static const double aRK[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+static const double bRK[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+
+/* ------------------------------------------------------------------------------------ */
+/* layout helpers                                                                       */
+/* ------------------------------------------------------------------------------------ */
+typedef struct {
+  int N1, N2, N3;
+  size_t sx, sy; /* strides of j and k */
+} dims_t;
+
+static inline dims_t mkdims(int N1, int N2, int N3) {
+  dims_t d;
+  d.N1 = N1;
+  d.N2 = N2;
+  d.N3 = N3;
+  d.sx = (size_t)(N1 + 7);
+  d.sy = d.sx * (size_t)(N2 + 7);
+  return d;
+}
+static inline size_t IX(const dims_t* d, int i, int j, int k) {
+  return (size_t)(i + 3) + d->sx * (size_t)(j + 3) + d->sy * (size_t)(k + 3);
+}
+static inline size_t field_size(const dims_t* d) { return d->sy * (size_t)(d->N3 + 7); }
+/* coefficient c(l, i) of a table with lower bound lo and n per row */
+#define CF(tab, lo, n, l, i) ((tab)[(size_t)(i) * (n) + ((l) - (lo))])
+#define CDG(tab, l, i) ((tab)[(size_t)((i)-1) * 3 + ((l) + 1)])
+
+/* ------------------------------------------------------------------------------------ */
+/* coordinates (mod_geometry.f90:37, usr_geometry.f90:93-156)                           */
+/* ------------------------------------------------------------------------------------ */
+static double coord_fn(int kind, int M, double L, double s) {
+  /* s is the 1-based point index (half-integer for velocity points) */
+  if (kind == 0) return (s - 1.0) * L / ((double)M - 1.0); /* coord_tanh, equidistant branch */
+  double t = (s - 1.0) / ((double)M - 1.0);
+  return 0.5 * L * (1.0 + sinh(2.0 * (t - 0.5)) / sinh(1.0));
+}
+
+void orc_coords(int M, double L, int kind, double* xp, double* xu) {
+  /* arrays cover indices -3..M+3 (offset 3) */
+  for (int i = -3; i <= M + 3; i++) {
+    xp[i + 3] = 0.0;
+    xu[i + 3] = 0.0;
+  }
+  for (int i = 1; i <= M; i++) xp[i + 3] = coord_fn(kind, M, L, (double)i);
+  for (int i = 0; i <= M; i++) xu[i + 3] = coord_fn(kind, M, L, (double)i + 0.5);
+  /* periodic continuation (mod_geometry.f90:95-103): lower ghosts from M-4..M-1, upper from 1..4 */
+  for (int i = -3; i <= 0; i++) {
+    xp[i + 3] = xp[(M - 1 + i) + 3] - L;
+    xu[i + 3] = xu[(M - 1 + i) + 3] - L;
+  }
+  for (int i = M; i <= M + 3; i++) {
+    xp[i + 3] = xp[(i - M + 1) + 3] + L;
+    xu[i + 3] = xu[(i - M + 1) + 3] + L;
+  }
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* exact equidistant FD weights (diff_coeffs_exact, mod_coeffs.f90:598-751)             */
+/* ------------------------------------------------------------------------------------ */
+static int64_t gcd64(int64_t a, int64_t b) {
+  if (a < 0) a = -a;
+  if (b < 0) b = -b;
+  while (b) {
+    int64_t t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+int orc_fd_exact(int abl, int n, double deltaX0, double* cc) {
+  /* Lagrange weights of derivative order abl at 0 for points x_j = deltaX0 + j, computed in
+   * exact integer arithmetic on the doubled offsets s_j = 2 x_j, then rounded once. */
+  if (n < 1 || n > 12 || abl < 0 || abl >= n) return -1;
+  int64_t s[12];
+  for (int j = 0; j < n; j++) s[j] = (int64_t)llround(2.0 * (deltaX0 + (double)j));
+  int64_t fact = 1, pow2 = 1;
+  for (int q = 1; q <= abl; q++) {
+    fact *= q;
+    pow2 *= 2;
+  }
+  for (int j = 0; j < n; j++) {
+    /* poly(t) = prod_{m != j} (t - s_m), coefficients in increasing power */
+    int64_t poly[13] = {0};
+    poly[0] = 1;
+    int deg = 0;
+    int64_t den = 1;
+    for (int m = 0; m < n; m++) {
+      if (m == j) continue;
+      for (int q = deg + 1; q >= 1; q--) poly[q] = poly[q - 1] - s[m] * poly[q];
+      poly[0] = -s[m] * poly[0];
+      deg++;
+      den *= (s[j] - s[m]);
+    }
+    int64_t num = poly[abl] * fact * pow2;
+    int64_t g = gcd64(num, den);
+    if (g == 0) g = 1;
+    num /= g;
+    den /= g;
+    if (den < 0) {
+      den = -den;
+      num = -num;
+    }
+    cc[j] = (double)num / (double)den;
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* diff_coeffs (mod_coeffs.f90:200-597), periodic boundaries, mapping_yes = T           */
+/* ------------------------------------------------------------------------------------ */
+int orc_diff_coeffs(int abl, int upwind, int grid_type, int N, int bL, int bU, int n_coeff,
+                    const double* xC, const double* xE, double* cc) {
+  (void)xE;
+  const int nrow = bU - bL + 1;
+  const int iStart = (grid_type == 0 || grid_type == 3) ? 1 : 0;
+  memset(cc, 0, sizeof(double) * (size_t)nrow * (size_t)(N + 1));
+  for (int i = iStart; i <= N; i++) {
+    int n = n_coeff;
+    if (!(n > 0 && n > abl)) continue;
+    int right;
+    if (grid_type == 0 || grid_type == 1) {
+      if (n % 2 == 0) return -2; /* central stencils need an odd count */
+      right = (n - 1) / 2;
+    } else if (grid_type == 2) {
+      if (n % 2 != 0) return -2;
+      right = n / 2;
+    } else {
+      if (n % 2 != 0) return -2;
+      right = n / 2 - 1;
+    }
+    int left = right - n + 1;
+    if (upwind == -1) {
+      n -= 1;
+      left += 1;
+    }
+    if (upwind == 1) {
+      n -= 1;
+      right -= 1;
+    }
+    if (right > bU || left < bL) return -3;
+    double dx0;
+    if (grid_type == 2)
+      dx0 = (double)left - 0.5;
+    else if (grid_type == 3)
+      dx0 = (double)left + 0.5;
+    else
+      dx0 = (double)left;
+    double w[12];
+    if (abl == 1 || abl == 2) {
+      double cxi[2][12];
+      double dxi[2] = {0.0, 0.0};
+      for (int k = 1; k <= abl; k++) {
+        orc_fd_exact(k, n, dx0, cxi[k - 1]);
+        for (int ii = left; ii <= right; ii++) dxi[k - 1] = dxi[k - 1] + cxi[k - 1][ii - left] * xC[i + ii + 3];
+      }
+      for (int ii = left; ii <= right; ii++) {
+        if (abl == 1)
+          w[ii - left] = cxi[0][ii - left] / dxi[0];
+        else
+          w[ii - left] = cxi[1][ii - left] / (dxi[0] * dxi[0]) -
+                         cxi[0][ii - left] * dxi[1] / (dxi[0] * dxi[0] * dxi[0]);
+      }
+    } else if (abl == 0 && (grid_type == 2 || grid_type == 3)) {
+      orc_fd_exact(0, n, dx0, w);
+    } else {
+      return -4; /* filters / integrators are not on the hot path */
+    }
+    for (int ii = left; ii <= right; ii++) cc[(size_t)i * nrow + (ii - bL)] = w[ii - left];
+  }
+  return 0;
+}
+
+/* get_stencil (mod_coeffs.f90:1048-1259), level 1, periodic branch */
+void orc_get_stencil(int N, const double* xp, const double* xu, double* cdg) {
+  double* cD = (double*)calloc((size_t)2 * (N + 1), sizeof(double)); /* cDu1R(-1:0, 0:N) */
+  double* cG = (double*)calloc((size_t)2 * (N + 1), sizeof(double)); /* cGp1R(0:1, 0:N) */
+  for (int i = 1; i <= N; i++) {
+    cD[2 * i + 0] = -1.0 / (xu[i + 3] - xu[i - 1 + 3]);
+    cD[2 * i + 1] = 1.0 / (xu[i + 3] - xu[i - 1 + 3]);
+  }
+  for (int i = 1; i <= N - 1; i++) {
+    cG[2 * i + 0] = -1.0 / (xp[i + 1 + 3] - xp[i + 3]);
+    cG[2 * i + 1] = 1.0 / (xp[i + 1 + 3] - xp[i + 3]);
+  }
+  cG[0] = -1.0 / (xp[1 + 3] - xp[0 + 3]);
+  cG[1] = 1.0 / (xp[1 + 3] - xp[0 + 3]);
+  cG[2 * N + 0] = -1.0 / (xp[N + 1 + 3] - xp[N + 3]);
+  cG[2 * N + 1] = 1.0 / (xp[N + 1 + 3] - xp[N + 3]);
+  for (int i = 1; i <= N; i++) {
+    CDG(cdg, -1, i) = cD[2 * i + 0] * cG[2 * (i - 1) + 0];
+    CDG(cdg, 0, i) = cD[2 * i + 0] * cG[2 * (i - 1) + 1] + cD[2 * i + 1] * cG[2 * i + 0];
+    CDG(cdg, 1, i) = cD[2 * i + 1] * cG[2 * i + 1];
+  }
+  free(cD);
+  free(cG);
+}
+
+/* RK3 stability limits along the rays z = r (-sin t + i cos t), t = n pi/80, n = 0..40:
+ * the first r where |1 + z + z^2/2 + z^3/6| = 1 (the quantity tabulated at mod_vars.f90:785). */
+static double amp2(double r, double t) {
+  double zr = -r * sin(t), zi = r * cos(t);
+  double z2r = zr * zr - zi * zi, z2i = 2.0 * zr * zi;
+  double z3r = z2r * zr - z2i * zi, z3i = z2r * zi + z2i * zr;
+  double re = 1.0 + zr + 0.5 * z2r + z3r / 6.0;
+  double im = zi + 0.5 * z2i + z3i / 6.0;
+  return re * re + im * im - 1.0;
+}
+void orc_stability_limits(double* lim41) {
+  for (int n = 0; n <= 40; n++) {
+    double t = (double)n * PI_D / 80.0;
+    double lo = 1e-3, hi = lo;
+    while (amp2(hi, t) < 0.0 && hi < 10.0) {
+      lo = hi;
+      hi += 1e-3;
+    }
+    for (int it = 0; it < 200; it++) {
+      double mid = 0.5 * (lo + hi);
+      if (amp2(mid, t) < 0.0)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    lim41[n] = 0.5 * (lo + hi);
+  }
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* ghost fill (mod_exchange.f90:133-140), periodic branch                               */
+/* ------------------------------------------------------------------------------------ */
+void orc_exchange(int dir, int N1, int N2, int N3, double* phi) {
+  dims_t d = mkdims(N1, N2, N3);
+  if (dir == 1) {
+    for (int k = 1; k <= N3; k++)
+      for (int j = 1; j <= N2; j++) {
+        for (int i = -3; i <= -1; i++) phi[IX(&d, 1 + i, j, k)] = phi[IX(&d, N1 + i, j, k)];
+        for (int i = 1; i <= 3; i++) phi[IX(&d, N1 - 1 + i, j, k)] = phi[IX(&d, i, j, k)];
+      }
+  } else if (dir == 2) {
+    for (int k = 1; k <= N3; k++)
+      for (int i = 1; i <= N1; i++) {
+        for (int j = -3; j <= -1; j++) phi[IX(&d, i, 1 + j, k)] = phi[IX(&d, i, N2 + j, k)];
+        for (int j = 1; j <= 3; j++) phi[IX(&d, i, N2 - 1 + j, k)] = phi[IX(&d, i, j, k)];
+      }
+  } else {
+    for (int j = 1; j <= N2; j++)
+      for (int i = 1; i <= N1; i++) {
+        for (int k = -3; k <= -1; k++) phi[IX(&d, i, j, 1 + k)] = phi[IX(&d, i, j, N3 + k)];
+        for (int k = 1; k <= 3; k++) phi[IX(&d, i, j, N3 - 1 + k)] = phi[IX(&d, i, j, k)];
+      }
+  }
+}
+static void exchange_all(int N1, int N2, int N3, double* phi) {
+  orc_exchange(1, N1, N2, N3, phi);
+  orc_exchange(2, N1, N2, N3, phi);
+  orc_exchange(3, N1, N2, N3, phi);
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* 1-D stencil helper: out = sum_l c(l, row) * phi(point + l*stride)                    */
+/* ------------------------------------------------------------------------------------ */
+static inline double stencil1(const double* tab, int lo, int hi, int row, const double* phi,
+                              size_t p, ptrdiff_t stride) {
+  const int n = hi - lo + 1;
+  double s = CF(tab, lo, n, lo, row) * phi[(ptrdiff_t)p + (ptrdiff_t)lo * stride];
+  for (int l = lo + 1; l <= hi; l++) s = s + CF(tab, lo, n, l, row) * phi[(ptrdiff_t)p + (ptrdiff_t)l * stride];
+  return s;
+}
+static inline ptrdiff_t axis_stride(const dims_t* d, int a) {
+  return a == 1 ? (ptrdiff_t)1 : (a == 2 ? (ptrdiff_t)d->sx : (ptrdiff_t)d->sy);
+}
+static inline int axis_row(int a, int i, int j, int k) { return a == 1 ? i : (a == 2 ? j : k); }
+
+/* ------------------------------------------------------------------------------------ */
+/* operators (mod_diff.f90)                                                             */
+/* ------------------------------------------------------------------------------------ */
+/* gradient (mod_diff.f90:309-414) */
+void orc_gradient(int m, int N1, int N2, int N3, const orc_coeffs* c, double* phi, double* grad) {
+  dims_t d = mkdims(N1, N2, N3);
+  orc_exchange(m, N1, N2, N3, phi);
+  const double* tab = c->cG[m - 1];
+  const ptrdiff_t st = axis_stride(&d, m);
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= N3 - 1; k++)
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        size_t p = IX(&d, i, j, k);
+        grad[p] = stencil1(tab, ORC_G_LO, ORC_G_HI, axis_row(m, i, j, k), phi, p, st);
+      }
+}
+
+/* divergence (mod_diff.f90:52-118): m = 1 overwrites, m = 2, 3 accumulate */
+void orc_divergence(int m, int N1, int N2, int N3, const orc_coeffs* c, double* phi, double* div) {
+  dims_t d = mkdims(N1, N2, N3);
+  orc_exchange(m, N1, N2, N3, phi);
+  const double* tab = c->cD[m - 1];
+  const ptrdiff_t st = axis_stride(&d, m);
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= N3 - 1; k++)
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        size_t p = IX(&d, i, j, k);
+        int row = axis_row(m, i, j, k);
+        if (m == 1) {
+          div[p] = stencil1(tab, ORC_D_LO, ORC_D_HI, row, phi, p, st);
+        } else {
+          double s = div[p];
+          for (int l = ORC_D_LO; l <= ORC_D_HI; l++)
+            s = s + CF(tab, ORC_D_LO, ORC_ND, l, row) * phi[(ptrdiff_t)p + (ptrdiff_t)l * st];
+          div[p] = s;
+        }
+      }
+}
+
+/* divergence2 (mod_diff.f90:130-215) */
+void orc_divergence2(int N1, int N2, int N3, const orc_coeffs* c, double* u, double* v, double* w,
+                     double* div) {
+  dims_t d = mkdims(N1, N2, N3);
+  orc_exchange(1, N1, N2, N3, u);
+  orc_exchange(2, N1, N2, N3, v);
+  orc_exchange(3, N1, N2, N3, w);
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= N3 - 1; k++)
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        size_t p = IX(&d, i, j, k);
+        double s = stencil1(c->cD[0], ORC_D_LO, ORC_D_HI, i, u, p, 1);
+        for (int l = ORC_D_LO; l <= ORC_D_HI; l++)
+          s = s + CF(c->cD[1], ORC_D_LO, ORC_ND, l, j) * v[(ptrdiff_t)p + (ptrdiff_t)l * (ptrdiff_t)d.sx];
+        for (int l = ORC_D_LO; l <= ORC_D_HI; l++)
+          s = s + CF(c->cD[2], ORC_D_LO, ORC_ND, l, k) * w[(ptrdiff_t)p + (ptrdiff_t)l * (ptrdiff_t)d.sy];
+        div[p] = s;
+      }
+}
+
+/* Helmholtz_explicit (mod_diff.f90:549-762): nl_m -= multL * (d2/dx2 + d2/dy2 + d2/dz2) u_m */
+void orc_helmholtz(int m, int N1, int N2, int N3, const orc_coeffs* c, double multL, double* vel,
+                   double* nl) {
+  dims_t d = mkdims(N1, N2, N3);
+  exchange_all(N1, N2, N3, vel);
+  const double* cx = (m == 1) ? c->cuu[0] : c->cpp[0];
+  const double* cy = (m == 2) ? c->cuu[1] : c->cpp[1];
+  const double* cz = (m == 3) ? c->cuu[2] : c->cpp[2];
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= N3 - 1; k++)
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        size_t p = IX(&d, i, j, k);
+        double dd1 = stencil1(cx, ORC_B_LO, ORC_B_HI, i, vel, p, 1);
+        for (int l = ORC_B_LO; l <= ORC_B_HI; l++)
+          dd1 = dd1 + CF(cy, ORC_B_LO, ORC_NB, l, j) * vel[(ptrdiff_t)p + (ptrdiff_t)l * (ptrdiff_t)d.sx];
+        for (int l = ORC_B_LO; l <= ORC_B_HI; l++)
+          dd1 = dd1 + CF(cz, ORC_B_LO, ORC_NB, l, k) * vel[(ptrdiff_t)p + (ptrdiff_t)l * (ptrdiff_t)d.sy];
+        nl[p] = nl[p] - multL * dd1;
+      }
+}
+
+/* interpolate2_pre_vel (mod_diff.f90:1567-1648): pressure points -> u_m points */
+void orc_interpolate_pre_vel(int m, int N1, int N2, int N3, const orc_coeffs* c, double* phi,
+                             double* inter) {
+  dims_t d = mkdims(N1, N2, N3);
+  orc_exchange(m, N1, N2, N3, phi);
+  const ptrdiff_t st = axis_stride(&d, m);
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= N3 - 1; k++)
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        size_t p = IX(&d, i, j, k);
+        inter[p] = stencil1(c->cIpu[m - 1], ORC_G_LO, ORC_G_HI, axis_row(m, i, j, k), phi, p, st);
+      }
+}
+
+/* interpolate2_vel_pre (mod_diff.f90:1740-1825): u_m points -> pressure points */
+void orc_interpolate_vel_pre(int m, int N1, int N2, int N3, const orc_coeffs* c, double* phi,
+                             double* inter) {
+  dims_t d = mkdims(N1, N2, N3);
+  orc_exchange(m, N1, N2, N3, phi);
+  const ptrdiff_t st = axis_stride(&d, m);
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= N3 - 1; k++)
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        size_t p = IX(&d, i, j, k);
+        inter[p] = stencil1(c->cIup[m - 1], ORC_D_LO, ORC_D_HI, axis_row(m, i, j, k), phi, p, st);
+      }
+}
+
+/* one upwind term of nonlinear (mod_diff.f90:784-1424); component_id = 3*(m-1) + a */
+void orc_nonlinear_upwind(int component_id, int N1, int N2, int N3, const orc_coeffs* c,
+                          const double* pp, double* vel, double* nl) {
+  dims_t d = mkdims(N1, N2, N3);
+  const int m = (component_id - 1) / 3 + 1;
+  const int a = (component_id - 1) % 3 + 1;
+  orc_exchange(a, N1, N2, N3, vel);
+  const double* cU = (a == m) ? c->cNuU[a - 1] : c->cNpU[a - 1];
+  const double* cDn = (a == m) ? c->cNuD[a - 1] : c->cNpD[a - 1];
+  const ptrdiff_t st = axis_stride(&d, a);
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= N3 - 1; k++)
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        size_t p = IX(&d, i, j, k);
+        int row = axis_row(a, i, j, k);
+        double dd1 = (pp[p] >= 0.0) ? stencil1(cU, ORC_B_LO, ORC_B_HI, row, vel, p, st)
+                                    : stencil1(cDn, ORC_B_LO, ORC_B_HI, row, vel, p, st);
+        if (a == 1)
+          nl[p] = dd1 * pp[p];
+        else
+          nl[p] = nl[p] + dd1 * pp[p];
+      }
+}
+
+void orc_nonlinear(int m, int N1, int N2, int N3, const orc_coeffs* c, double* vel_m,
+                   double* work1, double* work2, double* work3, double* pp, double* nl_m) {
+  double* wk[3] = {work1, work2, work3};
+  for (int a = 1; a <= 3; a++) {
+    orc_interpolate_pre_vel(m, N1, N2, N3, c, wk[a - 1], pp);
+    orc_nonlinear_upwind(3 * (m - 1) + a, N1, N2, N3, c, pp, vel_m, nl_m);
+  }
+}
+
+/* axpby (axpby_kernel.cu:6-17 / mod_solvers.f90:281) */
+void orc_axpby(int N1, int N2, int N3, double a, double b, const double* x, const double* y,
+               double* z) {
+  dims_t d = mkdims(N1, N2, N3);
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= N3 - 1; k++)
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        size_t p = IX(&d, i, j, k);
+        z[p] = a * x[p] + b * y[p];
+      }
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Laplacians and relaxation (mod_laplace.f90)                                          */
+/* ------------------------------------------------------------------------------------ */
+/* product_div_grad (mod_laplace.f90:38-197) */
+void orc_product_div_grad(int N1, int N2, int N3, const orc_coeffs* c, double* phi, double* dig,
+                          double* lap) {
+  for (int m = 1; m <= 3; m++) {
+    orc_gradient(m, N1, N2, N3, c, phi, dig);
+    orc_divergence(m, N1, N2, N3, c, dig, lap);
+  }
+}
+
+/* product_div_grad_relax (mod_laplace.f90:216-327) */
+void orc_product_dg_relax(int N1, int N2, int N3, const orc_coeffs* c, double* phi, double* lap) {
+  dims_t d = mkdims(N1, N2, N3);
+  exchange_all(N1, N2, N3, phi);
+  const ptrdiff_t sx = (ptrdiff_t)d.sx, sy = (ptrdiff_t)d.sy;
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= N3 - 1; k++)
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        size_t p = IX(&d, i, j, k);
+        lap[p] = CDG(c->cdg[0], -1, i) * phi[p - 1] + CDG(c->cdg[0], 1, i) * phi[p + 1] +
+                 CDG(c->cdg[1], -1, j) * phi[p - sx] + CDG(c->cdg[1], 1, j) * phi[p + sx] +
+                 CDG(c->cdg[2], -1, k) * phi[p - sy] + CDG(c->cdg[2], 1, k) * phi[p + sy] +
+                 (CDG(c->cdg[0], 0, i) + CDG(c->cdg[1], 0, j) + CDG(c->cdg[2], 0, k)) * phi[p];
+      }
+}
+
+/* relaxation_div_grad, Jacobi branch (mod_laplace.f90:339-613) */
+void orc_jacobi(int N1, int N2, int N3, const orc_coeffs* c, int init_yes, int n_relax,
+                double omega, const double* bb, double* rel, double* comp) {
+  dims_t d = mkdims(N1, N2, N3);
+  const ptrdiff_t sx = (ptrdiff_t)d.sx, sy = (ptrdiff_t)d.sy;
+  for (int r = 1; r <= n_relax; r++) {
+    if (r == 1 && init_yes) {
+#pragma omp parallel for schedule(static)
+      for (int k = 1; k <= N3 - 1; k++)
+        for (int j = 1; j <= N2 - 1; j++)
+          for (int i = 1; i <= N1 - 1; i++) {
+            size_t p = IX(&d, i, j, k);
+            rel[p] = omega * bb[p] / (CDG(c->cdg[0], 0, i) + CDG(c->cdg[1], 0, j) + CDG(c->cdg[2], 0, k));
+          }
+    } else {
+      exchange_all(N1, N2, N3, rel);
+#pragma omp parallel for schedule(static)
+      for (int k = 1; k <= N3 - 1; k++)
+        for (int j = 1; j <= N2 - 1; j++)
+          for (int i = 1; i <= N1 - 1; i++) {
+            size_t p = IX(&d, i, j, k);
+            comp[p] = omega *
+                          (bb[p] - CDG(c->cdg[0], -1, i) * rel[p - 1] - CDG(c->cdg[0], 1, i) * rel[p + 1] -
+                           CDG(c->cdg[1], -1, j) * rel[p - sx] - CDG(c->cdg[1], 1, j) * rel[p + sx] -
+                           CDG(c->cdg[2], -1, k) * rel[p - sy] - CDG(c->cdg[2], 1, k) * rel[p + sy]) /
+                          (CDG(c->cdg[0], 0, i) + CDG(c->cdg[1], 0, j) + CDG(c->cdg[2], 0, k)) +
+                      (1.0 - omega) * rel[p];
+          }
+#pragma omp parallel for schedule(static)
+      for (int k = 1; k <= N3 - 1; k++)
+        for (int j = 1; j <= N2 - 1; j++)
+          for (int i = 1; i <= N1 - 1; i++) {
+            size_t p = IX(&d, i, j, k);
+            rel[p] = comp[p];
+          }
+    }
+  }
+}
+
+/* apply_pressure_BC_CT (usr_func.f90:857-897) with the label set of set_pressure_BC_kernel.cu */
+void orc_pressure_bc(int N1, int N2, int N3, const uint8_t* label, int k_start_index,
+                     double p_inlet, double p_outlet, double p_outlet2, double* rel) {
+  dims_t d = mkdims(N1, N2, N3);
+  for (int k = 1; k <= N3 - 1; k++)
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        size_t p = IX(&d, i, j, k);
+        if (label[p] == 5 && k == k_start_index - 1) rel[p] = p_inlet;
+        if (label[p] == 9 && k == k_start_index - 1) rel[p] = p_outlet;
+        if (label[p] == 11) rel[p] = p_outlet2;
+      }
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* reductions (mod_solvers.f90:2319-2470)                                               */
+/* ------------------------------------------------------------------------------------ */
+double orc_product_scalar(int N1, int N2, int N3, const double* a, const double* b) {
+  dims_t d = mkdims(N1, N2, N3);
+  double* part = (double*)calloc((size_t)N3, sizeof(double));
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= N3 - 1; k++) {
+    double s = 0.0;
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        size_t p = IX(&d, i, j, k);
+        s = s + a[p] * b[p];
+      }
+    part[k] = s;
+  }
+  double s = 0.0;
+  for (int k = 1; k <= N3 - 1; k++) s += part[k];
+  free(part);
+  return s;
+}
+
+void orc_norms(int N1, int N2, int N3, const double* a, double* norm_inf, double* norm_two_sq) {
+  dims_t d = mkdims(N1, N2, N3);
+  double* pi = (double*)calloc((size_t)N3, sizeof(double));
+  double* p2 = (double*)calloc((size_t)N3, sizeof(double));
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= N3 - 1; k++) {
+    double mi = 0.0, s = 0.0;
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        double v = a[IX(&d, i, j, k)];
+        mi = fmax(fabs(v), mi);
+        s = s + v * v;
+      }
+    pi[k] = mi;
+    p2[k] = s;
+  }
+  double mi = 0.0, s = 0.0;
+  for (int k = 1; k <= N3 - 1; k++) {
+    mi = fmax(pi[k], mi);
+    s += p2[k];
+  }
+  *norm_inf = mi;
+  *norm_two_sq = s;
+  free(pi);
+  free(p2);
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* BiCGstab_orig (mod_solvers.f90:1509-1935), problem_type 2                            */
+/* ------------------------------------------------------------------------------------ */
+static void copy_interior(const dims_t* d, const double* src, double* dst) {
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= d->N3 - 1; k++)
+    for (int j = 1; j <= d->N2 - 1; j++)
+      for (int i = 1; i <= d->N1 - 1; i++) dst[IX(d, i, j, k)] = src[IX(d, i, j, k)];
+}
+
+static void precond(int N1, int N2, int N3, const orc_coeffs* c, const orc_solver_opts* o, double* v,
+                    double* z, double* comp) {
+  /* single-level multigridV (mod_solvers.f90:456-585 with n_grids = 1): Jacobi sweeps from zero */
+  orc_jacobi(N1, N2, N3, c, 1, o->n_sweeps, o->omega, v, z, comp);
+}
+
+static int converged(const orc_solver_opts* o, double ninf, double n2sq, double b2) {
+  if (o->tol_abs_inf > 0.0 && ninf < o->tol_abs_inf) return 1;
+  if (o->tol_rel > 0.0 && sqrt(n2sq) <= o->tol_rel * b2) return 1;
+  return 0;
+}
+
+void orc_bicgstab(int N1, int N2, int N3, const orc_coeffs* c, const orc_solver_opts* o,
+                  double* bb, double* phi, double* work, orc_solver_result* res) {
+  dims_t d = mkdims(N1, N2, N3);
+  const size_t fs = field_size(&d);
+  double* rr = work + 0 * fs;
+  double* rh = work + 1 * fs;
+  double* pp = work + 2 * fs;
+  double* Ap = work + 3 * fs;
+  double* Ar = work + 4 * fs;
+  double* z1 = work + 5 * fs;
+  double* z2 = work + 6 * fs;
+  double* comp = work + 7 * fs;
+  double* dig = work + 8 * fs;
+  const int pre_on = o->n_sweeps > 0;
+  const int init_yes = o->init_yes;
+  double norm_inf = 0.0, norm2 = 0.0, b2sq = 0.0, dummy;
+  double rhr = 0.0, rhr_prev, alpha = 0.0, omega = 0.0, beta, rhAp, rAr, ArAr;
+
+  orc_norms(N1, N2, N3, bb, &dummy, &b2sq);
+  const double b2 = sqrt(b2sq);
+  if (!init_yes) {
+    orc_product_div_grad(N1, N2, N3, c, phi, dig, rr);
+#pragma omp parallel for schedule(static)
+    for (int k = 1; k <= N3 - 1; k++)
+      for (int j = 1; j <= N2 - 1; j++)
+        for (int i = 1; i <= N1 - 1; i++) {
+          size_t p = IX(&d, i, j, k);
+          rr[p] = bb[p] - rr[p];
+          rh[p] = rr[p];
+        }
+    orc_norms(N1, N2, N3, rr, &norm_inf, &norm2);
+  } else {
+    orc_norms(N1, N2, N3, bb, &norm_inf, &norm2);
+  }
+  res->status = 1;
+  int counter = 0;
+  for (;;) {
+    int exit_yes = converged(o, norm_inf, norm2, b2) || counter == o->max_it;
+    if (counter < 1 && norm_inf != 0.0 && counter != o->max_it) exit_yes = 0;
+    if (exit_yes) {
+      if (counter == 0 && init_yes) {
+#pragma omp parallel for schedule(static)
+        for (int k = 1; k <= N3 - 1; k++)
+          for (int j = 1; j <= N2 - 1; j++)
+            for (int i = 1; i <= N1 - 1; i++) phi[IX(&d, i, j, k)] = 0.0;
+      }
+      res->status = converged(o, norm_inf, norm2, b2) ? 0 : 1;
+      break;
+    }
+    if (!isfinite(norm_inf)) {
+      res->status = 3;
+      break;
+    }
+    counter++;
+    rhr_prev = rhr;
+    if (init_yes)
+      rhr = (counter == 1) ? norm2 : orc_product_scalar(N1, N2, N3, rr, bb);
+    else
+      rhr = orc_product_scalar(N1, N2, N3, rr, rh);
+    if (fabs(rhr) == 0.0) {
+      copy_interior(&d, rr, rh);
+      rhr = orc_product_scalar(N1, N2, N3, rr, rh);
+    }
+    if (counter >= 2) {
+      if (omega == 0.0 || rhr_prev == 0.0) {
+        res->status = 2;
+        break;
+      }
+      beta = (alpha / omega) * (rhr / rhr_prev);
+      omega = -beta * omega;
+#pragma omp parallel for schedule(static)
+      for (int k = 1; k <= N3 - 1; k++)
+        for (int j = 1; j <= N2 - 1; j++)
+          for (int i = 1; i <= N1 - 1; i++) {
+            size_t p = IX(&d, i, j, k);
+            pp[p] = rr[p] + beta * pp[p] + omega * Ap[p];
+          }
+    } else {
+      copy_interior(&d, (init_yes && counter == 1) ? bb : rr, pp);
+    }
+    if (pre_on) {
+      precond(N1, N2, N3, c, o, pp, z1, comp);
+      orc_product_div_grad(N1, N2, N3, c, z1, dig, Ap);
+    } else {
+      orc_product_div_grad(N1, N2, N3, c, pp, dig, Ap);
+    }
+    rhAp = orc_product_scalar(N1, N2, N3, Ap, init_yes ? bb : rh);
+    if (fabs(rhAp) == 0.0) {
+      res->status = 2;
+      break;
+    }
+    alpha = rhr / rhAp;
+    {
+      const double* src = (init_yes && counter == 1) ? bb : rr;
+#pragma omp parallel for schedule(static)
+      for (int k = 1; k <= N3 - 1; k++)
+        for (int j = 1; j <= N2 - 1; j++)
+          for (int i = 1; i <= N1 - 1; i++) {
+            size_t p = IX(&d, i, j, k);
+            rr[p] = src[p] - alpha * Ap[p];
+          }
+    }
+    if (pre_on) {
+      precond(N1, N2, N3, c, o, rr, z2, comp);
+      orc_product_div_grad(N1, N2, N3, c, z2, dig, Ar);
+    } else {
+      orc_product_div_grad(N1, N2, N3, c, rr, dig, Ar);
+    }
+    rAr = orc_product_scalar(N1, N2, N3, rr, Ar);
+    ArAr = orc_product_scalar(N1, N2, N3, Ar, Ar);
+    if (fabs(ArAr) == 0.0) {
+      res->status = 2;
+      break;
+    }
+    omega = rAr / ArAr;
+    const int first = (counter == 1 && init_yes);
+    const double* zA = pre_on ? z1 : pp;
+    const double* zB = pre_on ? z2 : rr;
+#pragma omp parallel for schedule(static)
+    for (int k = 1; k <= N3 - 1; k++)
+      for (int j = 1; j <= N2 - 1; j++)
+        for (int i = 1; i <= N1 - 1; i++) {
+          size_t p = IX(&d, i, j, k);
+          if (first)
+            phi[p] = alpha * zA[p] + omega * zB[p];
+          else
+            phi[p] = phi[p] + omega * zB[p] + alpha * zA[p];
+          rr[p] = rr[p] - omega * Ar[p];
+        }
+    orc_norms(N1, N2, N3, rr, &norm_inf, &norm2);
+  }
+  res->iterations = counter;
+  res->res_inf = norm_inf;
+  res->res_two = sqrt(norm2);
+  res->b_two = b2;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* time step pieces                                                                      */
+/* ------------------------------------------------------------------------------------ */
+double orc_get_dtime(int N1, int N2, int N3, const orc_coeffs* c, const double* stab41,
+                     double Re, double CFL, double dtime_max, double* vel, double* work) {
+  dims_t d = mkdims(N1, N2, N3);
+  const size_t fs = field_size(&d);
+  for (int m = 1; m <= 3; m++) orc_interpolate_vel_pre(m, N1, N2, N3, c, vel + (size_t)(m - 1) * fs, work + (size_t)(m - 1) * fs);
+  double* part = (double*)calloc((size_t)N3, sizeof(double));
+#pragma omp parallel for schedule(static)
+  for (int k = 1; k <= N3 - 1; k++) {
+    double beta1 = 0.0;
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        size_t p = IX(&d, i, j, k);
+        double are = 0.0;
+        for (int l = ORC_B_LO; l <= ORC_B_HI; l++) are = are + fabs(CF(c->cpp[0], ORC_B_LO, ORC_NB, l, i));
+        for (int l = ORC_B_LO; l <= ORC_B_HI; l++) are = are + fabs(CF(c->cpp[1], ORC_B_LO, ORC_NB, l, j));
+        for (int l = ORC_B_LO; l <= ORC_B_HI; l++) are = are + fabs(CF(c->cpp[2], ORC_B_LO, ORC_NB, l, k));
+        are = are / Re;
+        double dd1 = 0.0;
+        for (int l = ORC_B_LO; l <= ORC_B_HI; l++) dd1 = dd1 + fabs(CF(c->cp1[0], ORC_B_LO, ORC_NB, l, i));
+        double aim = dd1 * fabs(work[p]);
+        dd1 = 0.0;
+        for (int l = ORC_B_LO; l <= ORC_B_HI; l++) dd1 = dd1 + fabs(CF(c->cp1[1], ORC_B_LO, ORC_NB, l, j));
+        aim = aim + dd1 * fabs(work[fs + p]);
+        dd1 = 0.0;
+        for (int l = ORC_B_LO; l <= ORC_B_HI; l++) dd1 = dd1 + fabs(CF(c->cp1[2], ORC_B_LO, ORC_NB, l, k));
+        aim = aim + dd1 * fabs(work[2 * fs + p]);
+        double angle = (fabs(aim) < 1e-16) ? PI_D / 2.0 : atan(are / aim);
+        double radius = sqrt(are * are + aim * aim);
+        long idx = lround(2.0 * 40.0 * angle / PI_D);
+        if (idx < 0) idx = 0;
+        if (idx > 40) idx = 40;
+        beta1 = fmax(beta1, radius / stab41[idx]);
+      }
+    part[k] = beta1;
+  }
+  double beta1 = 0.0;
+  for (int k = 1; k <= N3 - 1; k++) beta1 = fmax(beta1, part[k]);
+  free(part);
+  double dinv = beta1 / CFL;
+  if (fabs(dinv) < 1.0 / dtime_max) return dtime_max;
+  return 1.0 / dinv;
+}
+
+void orc_mask_forcing(int N1, int N2, int N3, const uint8_t* label, double u_inflow, double* vel) {
+  dims_t d = mkdims(N1, N2, N3);
+  const size_t fs = field_size(&d);
+  for (int k = 1; k <= N3 - 1; k++)
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) {
+        size_t p = IX(&d, i, j, k);
+        uint8_t lb = label[p];
+        if (lb == 0 || lb == 7) {
+          vel[p] = 0.0;
+          vel[fs + p] = 0.0;
+          vel[2 * fs + p] = 0.0;
+        } else if (lb == 5) {
+          vel[2 * fs + p] = u_inflow;
+          vel[fs + p] = 0.0;
+          vel[p] = 0.0;
+        }
+      }
+}
+
+void orc_level_pressure(int N1, int N2, int N3, double* pre) {
+  dims_t d = mkdims(N1, N2, N3);
+  double pre0 = 0.0;
+  for (int k = 1; k <= N3 - 1; k++) {
+    double s = 0.0;
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) s = s + pre[IX(&d, i, j, k)];
+    pre0 += s;
+  }
+  pre0 = pre0 / (double)(N1 - 1) / (double)(N2 - 1) / (double)(N3 - 1);
+  for (int k = 1; k <= N3 - 1; k++)
+    for (int j = 1; j <= N2 - 1; j++)
+      for (int i = 1; i <= N1 - 1; i++) pre[IX(&d, i, j, k)] = pre[IX(&d, i, j, k)] - pre0;
+}
+
+/* one time step (mod_timeint.f90:242-578, substeps :275-377; rhs_vel mod_rhs.f90:35-140;
+ * explicit mod_solvers.f90:64-346) */
+void orc_time_step(int N1, int N2, int N3, const orc_coeffs* c, const orc_step_params* p,
+                   const double* stab41, const uint8_t* label, double* vel, double* nl, double* pre,
+                   double* scratch, orc_step_state* st) {
+  dims_t d = mkdims(N1, N2, N3);
+  const size_t fs = field_size(&d);
+  double* rhs = scratch + 0 * fs;  /* 3 fields */
+  double* work = scratch + 3 * fs; /* 3 fields */
+  double* res = scratch + 6 * fs;
+  double* pp = scratch + 7 * fs;
+  double* sol = scratch + 8 * fs; /* 9 fields for the solver */
+
+  double dt = orc_get_dtime(N1, N2, N3, c, stab41, p->Re, p->CFL, p->dtime_max, vel, work);
+  if (st->timestep == 0 && dt > p->dtime0) dt = p->dtime0;
+  st->dtime = dt;
+  const double multL = 1.0 / p->Re;
+
+  for (int s = 0; s < 3; s++) {
+    /* exchange_all_all + interpolate_vel */
+    for (int m = 0; m < 3; m++) exchange_all(N1, N2, N3, vel + m * fs);
+    for (int m = 1; m <= 3; m++) {
+      orc_interpolate_vel_pre(m, N1, N2, N3, c, vel + (m - 1) * fs, work + (m - 1) * fs);
+      exchange_all(N1, N2, N3, work + (m - 1) * fs);
+    }
+    /* rhs_vel */
+    for (int m = 0; m < 3; m++) copy_interior(&d, vel + m * fs, rhs + m * fs);
+    if (s != 0) {
+      const double mult = dt * bRK[s];
+      for (int m = 0; m < 3; m++) {
+        double* r = rhs + m * fs;
+        const double* q = nl + m * fs;
+#pragma omp parallel for schedule(static)
+        for (int k = 1; k <= N3 - 1; k++)
+          for (int j = 1; j <= N2 - 1; j++)
+            for (int i = 1; i <= N1 - 1; i++) {
+              size_t x = IX(&d, i, j, k);
+              r[x] = r[x] - mult * q[x];
+            }
+      }
+    }
+    for (int m = 1; m <= 3; m++)
+      orc_nonlinear(m, N1, N2, N3, c, vel + (m - 1) * fs, work, work + fs, work + 2 * fs, pp, nl + (m - 1) * fs);
+    for (int m = 1; m <= 3; m++) orc_helmholtz(m, N1, N2, N3, c, multL, vel + (m - 1) * fs, nl + (m - 1) * fs);
+    {
+      const double mult = dt * aRK[s];
+      for (int m = 0; m < 3; m++) {
+        double* r = rhs + m * fs;
+        const double* q = nl + m * fs;
+#pragma omp parallel for schedule(static)
+        for (int k = 1; k <= N3 - 1; k++)
+          for (int j = 1; j <= N2 - 1; j++)
+            for (int i = 1; i <= N1 - 1; i++) {
+              size_t x = IX(&d, i, j, k);
+              r[x] = r[x] - mult * q[x];
+            }
+      }
+    }
+    /* pressure pre-scaling (mod_timeint.f90:318) */
+    const double ab = aRK[s] + bRK[s];
+#pragma omp parallel for schedule(static)
+    for (int k = 1; k <= N3 - 1; k++)
+      for (int j = 1; j <= N2 - 1; j++)
+        for (int i = 1; i <= N1 - 1; i++) {
+          size_t x = IX(&d, i, j, k);
+          pre[x] = pre[x] * ab * dt;
+        }
+    /* explicit */
+    for (int m = 0; m < 3; m++) copy_interior(&d, rhs + m * fs, vel + m * fs);
+    orc_divergence2(N1, N2, N3, c, vel, vel + fs, vel + 2 * fs, res);
+    orc_solver_result r;
+    orc_bicgstab(N1, N2, N3, c, &p->poisson, res, pre, sol, &r);
+    st->poisson_iterations[s] = r.iterations;
+    st->poisson_status[s] = r.status;
+    st->poisson_res_rel[s] = r.b_two > 0.0 ? r.res_two / r.b_two : 0.0;
+    for (int m = 1; m <= 3; m++) {
+      double* g = pp;
+      orc_gradient(m, N1, N2, N3, c, pre, g);
+      orc_axpby(N1, N2, N3, 1.0, -1.0, vel + (m - 1) * fs, g, vel + (m - 1) * fs);
+    }
+#pragma omp parallel for schedule(static)
+    for (int k = 1; k <= N3 - 1; k++)
+      for (int j = 1; j <= N2 - 1; j++)
+        for (int i = 1; i <= N1 - 1; i++) {
+          size_t x = IX(&d, i, j, k);
+          pre[x] = pre[x] / ab / dt;
+        }
+  }
+  st->timestep += 1;
+  st->time += dt;
+  const double u_in = p->U0 * (1.0 + 0.5 * sin(2.0 * PI_D * st->time / p->T_pulse));
+  orc_mask_forcing(N1, N2, N3, label, u_in, vel);
+  if (p->level_pressure) orc_level_pressure(N1, N2, N3, pre);
+}

@@ -1,0 +1,314 @@
+"""ctypes front end of the CPU FP64 oracle (liboracle.so built from impact_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and the
+CPU-baseline / reference legs of ``bench.py``.  The CUDA product never imports it.
+
+Fields are numpy float64 arrays of shape (N3+7, N2+7, N1+7) -- C order, i.e. the same
+memory as IMPACT's column-major ``phi(-3:N1+3, -3:N2+3, -3:N3+3)`` (mod_vars.f90:476-518).
+``interior(a)`` is the view of the unique periodic points 1..N-1 per axis.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+_dp = C.POINTER(C.c_double)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class OrcCoeffs(C.Structure):
+    _fields_ = [(name, _dp * 3) for name in (
+        "cG", "cD", "cIpu", "cIup", "cNpU", "cNpD", "cNuU", "cNuD", "cp1", "cpp", "cuu", "cdg")]
+
+
+class OrcSolverOpts(C.Structure):
+    _fields_ = [("tol_rel", C.c_double), ("tol_abs_inf", C.c_double), ("max_it", C.c_int),
+                ("n_sweeps", C.c_int), ("omega", C.c_double), ("init_yes", C.c_int)]
+
+
+class OrcSolverResult(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("res_inf", C.c_double),
+                ("res_two", C.c_double), ("b_two", C.c_double)]
+
+
+class OrcStepParams(C.Structure):
+    _fields_ = [("Re", C.c_double), ("CFL", C.c_double), ("dtime_max", C.c_double),
+                ("dtime0", C.c_double), ("U0", C.c_double), ("T_pulse", C.c_double),
+                ("level_pressure", C.c_int), ("poisson", OrcSolverOpts)]
+
+
+class OrcStepState(C.Structure):
+    _fields_ = [("time", C.c_double), ("dtime", C.c_double), ("timestep", C.c_int),
+                ("poisson_iterations", C.c_int * 3), ("poisson_res_rel", C.c_double * 3),
+                ("poisson_status", C.c_int * 3)]
+
+
+def build():
+    """Compile liboracle.so with the Makefile beside this file."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        i, d = C.c_int, C.c_double
+        P = C.POINTER
+        sig = {
+            "orc_coords": (None, [i, d, i, _dp, _dp]),
+            "orc_fd_exact": (i, [i, i, d, _dp]),
+            "orc_diff_coeffs": (i, [i, i, i, i, i, i, i, _dp, _dp, _dp]),
+            "orc_get_stencil": (None, [i, _dp, _dp, _dp]),
+            "orc_stability_limits": (None, [_dp]),
+            "orc_exchange": (None, [i, i, i, i, _dp]),
+            "orc_gradient": (None, [i, i, i, i, P(OrcCoeffs), _dp, _dp]),
+            "orc_divergence": (None, [i, i, i, i, P(OrcCoeffs), _dp, _dp]),
+            "orc_divergence2": (None, [i, i, i, P(OrcCoeffs), _dp, _dp, _dp, _dp]),
+            "orc_helmholtz": (None, [i, i, i, i, P(OrcCoeffs), d, _dp, _dp]),
+            "orc_interpolate_pre_vel": (None, [i, i, i, i, P(OrcCoeffs), _dp, _dp]),
+            "orc_interpolate_vel_pre": (None, [i, i, i, i, P(OrcCoeffs), _dp, _dp]),
+            "orc_nonlinear_upwind": (None, [i, i, i, i, P(OrcCoeffs), _dp, _dp, _dp]),
+            "orc_nonlinear": (None, [i, i, i, i, P(OrcCoeffs), _dp, _dp, _dp, _dp, _dp, _dp]),
+            "orc_axpby": (None, [i, i, i, d, d, _dp, _dp, _dp]),
+            "orc_product_div_grad": (None, [i, i, i, P(OrcCoeffs), _dp, _dp, _dp]),
+            "orc_product_dg_relax": (None, [i, i, i, P(OrcCoeffs), _dp, _dp]),
+            "orc_jacobi": (None, [i, i, i, P(OrcCoeffs), i, i, d, _dp, _dp, _dp]),
+            "orc_pressure_bc": (None, [i, i, i, _u8p, i, d, d, d, _dp]),
+            "orc_product_scalar": (d, [i, i, i, _dp, _dp]),
+            "orc_norms": (None, [i, i, i, _dp, _dp, _dp]),
+            "orc_bicgstab": (None, [i, i, i, P(OrcCoeffs), P(OrcSolverOpts), _dp, _dp, _dp,
+                                    P(OrcSolverResult)]),
+            "orc_get_dtime": (d, [i, i, i, P(OrcCoeffs), _dp, d, d, d, _dp, _dp]),
+            "orc_mask_forcing": (None, [i, i, i, _u8p, d, _dp]),
+            "orc_level_pressure": (None, [i, i, i, _dp]),
+            "orc_time_step": (None, [i, i, i, P(OrcCoeffs), P(OrcStepParams), _dp, _u8p, _dp,
+                                     _dp, _dp, _dp, P(OrcStepState)]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def u8ptr(a: np.ndarray):
+    assert a.dtype == np.uint8 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_u8p)
+
+
+# Interior stencil widths of IMPACT (mod_dims.f90 ncb*c/g/d last entries; mod_vars.f90:157-214).
+N_CENTRAL, N_GRAD, N_DIV = 7, 6, 6
+B_LO, B_HI, D_LO, D_HI, G_LO, G_HI = -3, 3, -3, 2, -2, 3
+
+
+class Grid:
+    """Coordinates and every coefficient table of one periodic IMPACT grid (oracle side).
+
+    N = (N1, N2, N3) are IMPACT's point counts (cells = N - 1 per periodic axis);
+    kinds[a] = 0 equidistant, 1 sinh-stretched (x(s) = L/2 (1 + sinh(2(s/(N-1) - 1/2))/sinh 1)).
+    Follows FD_coeffs (mod_coeffs.f90:37-112) and get_stencil (mod_coeffs.f90:1048).
+    """
+
+    def __init__(self, N, L=(1.0, 1.0, 1.0), kinds=(0, 0, 0)):
+        self.N = tuple(int(n) for n in N)
+        self.L = tuple(float(x) for x in L)
+        self.kinds = tuple(int(k) for k in kinds)
+        lb = lib()
+        self.xp, self.xu, self.tab = [], [], {}
+        names = ("cG", "cD", "cIpu", "cIup", "cNpU", "cNpD", "cNuU", "cNuD", "cp1", "cpp", "cuu", "cdg")
+        for n in names:
+            self.tab[n] = [None, None, None]
+        for a in range(3):
+            M = self.N[a]
+            xp = np.zeros(M + 7)
+            xu = np.zeros(M + 7)
+            lb.orc_coords(M, self.L[a], self.kinds[a], ptr(xp), ptr(xu))
+            self.xp.append(xp)
+            self.xu.append(xu)
+
+            def dc(abl, upw, gt, lo, hi, n, xC, xE):
+                cc = np.zeros((M + 1) * (hi - lo + 1))
+                rc = lb.orc_diff_coeffs(abl, upw, gt, M, lo, hi, n, ptr(xC), ptr(xE), ptr(cc))
+                if rc != 0:
+                    raise RuntimeError(f"orc_diff_coeffs failed ({rc})")
+                return cc
+
+            self.tab["cNpD"][a] = dc(1, -1, 0, B_LO, B_HI, N_CENTRAL, xp, xp)
+            self.tab["cNpU"][a] = dc(1, 1, 0, B_LO, B_HI, N_CENTRAL, xp, xp)
+            self.tab["cNuD"][a] = dc(1, -1, 1, B_LO, B_HI, N_CENTRAL, xu, xu)
+            self.tab["cNuU"][a] = dc(1, 1, 1, B_LO, B_HI, N_CENTRAL, xu, xu)
+            self.tab["cp1"][a] = dc(1, 0, 0, B_LO, B_HI, N_CENTRAL, xp, xp)
+            self.tab["cpp"][a] = dc(2, 0, 0, B_LO, B_HI, N_CENTRAL, xp, xp)
+            self.tab["cuu"][a] = dc(2, 0, 1, B_LO, B_HI, N_CENTRAL, xu, xu)
+            self.tab["cG"][a] = dc(1, 0, 2, G_LO, G_HI, N_GRAD, xp, xu)
+            self.tab["cD"][a] = dc(1, 0, 3, D_LO, D_HI, N_DIV, xu, xp)
+            self.tab["cIpu"][a] = dc(0, 0, 2, G_LO, G_HI, N_GRAD, xp, xu)
+            self.tab["cIup"][a] = dc(0, 0, 3, D_LO, D_HI, N_DIV, xu, xp)
+            cdg = np.zeros(3 * M)
+            lb.orc_get_stencil(M, ptr(xp), ptr(xu), ptr(cdg))
+            self.tab["cdg"][a] = cdg
+        self.c = OrcCoeffs()
+        for n in names:
+            setattr(self.c, n, (_dp * 3)(*[ptr(t) for t in self.tab[n]]))
+        self.stab = np.zeros(41)
+        lb.orc_stability_limits(ptr(self.stab))
+
+    # ---- fields ----
+    @property
+    def shape(self):
+        N1, N2, N3 = self.N
+        return (N3 + 7, N2 + 7, N1 + 7)
+
+    @property
+    def cells(self):
+        return (self.N[0] - 1) * (self.N[1] - 1) * (self.N[2] - 1)
+
+    def zeros(self, n=None):
+        return np.zeros(self.shape if n is None else (n,) + self.shape)
+
+    def interior(self, a):
+        N1, N2, N3 = self.N
+        return a[..., 4:N3 + 3, 4:N2 + 3, 4:N1 + 3]
+
+    def random(self, seed, n=None, lo=-1.0, hi=1.0):
+        rng = np.random.default_rng(seed)
+        f = self.zeros(n)
+        self.interior(f)[...] = rng.uniform(lo, hi, size=self.interior(f).shape)
+        return f
+
+    def fill_ghosts(self, a):
+        """Periodic ghost fill of a field (all three directions)."""
+        lb = lib()
+        for d in (1, 2, 3):
+            lb.orc_exchange(d, *self.N, ptr(a))
+        return a
+
+    # ---- operators ----
+    def gradient(self, m, phi, out=None):
+        out = self.zeros() if out is None else out
+        lib().orc_gradient(m, *self.N, C.byref(self.c), ptr(phi), ptr(out))
+        return out
+
+    def divergence(self, m, phi, div):
+        lib().orc_divergence(m, *self.N, C.byref(self.c), ptr(phi), ptr(div))
+        return div
+
+    def divergence2(self, u, v, w, out=None):
+        out = self.zeros() if out is None else out
+        lib().orc_divergence2(*self.N, C.byref(self.c), ptr(u), ptr(v), ptr(w), ptr(out))
+        return out
+
+    def helmholtz(self, m, multL, vel, nl):
+        lib().orc_helmholtz(m, *self.N, C.byref(self.c), multL, ptr(vel), ptr(nl))
+        return nl
+
+    def interpolate_pre_vel(self, m, phi, out=None):
+        out = self.zeros() if out is None else out
+        lib().orc_interpolate_pre_vel(m, *self.N, C.byref(self.c), ptr(phi), ptr(out))
+        return out
+
+    def interpolate_vel_pre(self, m, phi, out=None):
+        out = self.zeros() if out is None else out
+        lib().orc_interpolate_vel_pre(m, *self.N, C.byref(self.c), ptr(phi), ptr(out))
+        return out
+
+    def nonlinear_upwind(self, cid, pp, vel, nl):
+        lib().orc_nonlinear_upwind(cid, *self.N, C.byref(self.c), ptr(pp), ptr(vel), ptr(nl))
+        return nl
+
+    def nonlinear(self, m, vel_m, w1, w2, w3, out=None):
+        out = self.zeros() if out is None else out
+        pp = self.zeros()
+        lib().orc_nonlinear(m, *self.N, C.byref(self.c), ptr(vel_m), ptr(w1), ptr(w2), ptr(w3),
+                            ptr(pp), ptr(out))
+        return out
+
+    def axpby(self, a, b, x, y, z):
+        lib().orc_axpby(*self.N, a, b, ptr(x), ptr(y), ptr(z))
+        return z
+
+    def product_div_grad(self, phi, out=None):
+        out = self.zeros() if out is None else out
+        dig = self.zeros()
+        lib().orc_product_div_grad(*self.N, C.byref(self.c), ptr(phi), ptr(dig), ptr(out))
+        return out
+
+    def product_dg_relax(self, phi, out=None):
+        out = self.zeros() if out is None else out
+        lib().orc_product_dg_relax(*self.N, C.byref(self.c), ptr(phi), ptr(out))
+        return out
+
+    def jacobi(self, bb, rel, n_relax, omega, init_yes=False):
+        comp = self.zeros()
+        lib().orc_jacobi(*self.N, C.byref(self.c), int(init_yes), n_relax, omega, ptr(bb), ptr(rel),
+                         ptr(comp))
+        return rel
+
+    def pressure_bc(self, label, k_start_index, p_in, p_out, p_out2, rel):
+        lib().orc_pressure_bc(*self.N, u8ptr(label), k_start_index, p_in, p_out, p_out2, ptr(rel))
+        return rel
+
+    def dot(self, a, b):
+        return lib().orc_product_scalar(*self.N, ptr(a), ptr(b))
+
+    def norms(self, a):
+        ni, n2 = C.c_double(), C.c_double()
+        lib().orc_norms(*self.N, ptr(a), C.byref(ni), C.byref(n2))
+        return ni.value, n2.value
+
+    def bicgstab(self, bb, phi, tol_rel=1e-8, tol_abs_inf=0.0, max_it=1000, n_sweeps=4, omega=0.8,
+                 init_yes=False):
+        o = OrcSolverOpts(tol_rel, tol_abs_inf, max_it, n_sweeps, omega, int(init_yes))
+        work = self.zeros(9)
+        r = OrcSolverResult()
+        lib().orc_bicgstab(*self.N, C.byref(self.c), C.byref(o), ptr(bb), ptr(phi), ptr(work),
+                           C.byref(r))
+        return r
+
+    def get_dtime(self, vel, Re, CFL, dtime_max):
+        work = self.zeros(3)
+        return lib().orc_get_dtime(*self.N, C.byref(self.c), ptr(self.stab), Re, CFL, dtime_max,
+                                   ptr(vel), ptr(work))
+
+    def mask_forcing(self, label, u_in, vel):
+        lib().orc_mask_forcing(*self.N, u8ptr(label), u_in, ptr(vel))
+        return vel
+
+    def level_pressure(self, pre):
+        lib().orc_level_pressure(*self.N, ptr(pre))
+        return pre
+
+    def time_step(self, params: OrcStepParams, label, vel, nl, pre, state: OrcStepState, scratch=None):
+        scratch = self.zeros(17) if scratch is None else scratch
+        lib().orc_time_step(*self.N, C.byref(self.c), C.byref(params), ptr(self.stab), u8ptr(label),
+                            ptr(vel), ptr(nl), ptr(pre), ptr(scratch), C.byref(state))
+        return state
+
+
+def step_params(Re=200.0, CFL=0.2, dtime_max=1e-2, dtime0=1e9, U0=1.0, T_pulse=1.0, level_pressure=1,
+                tol_rel=1e-8, max_it=2000, n_sweeps=4, omega=0.8):
+    return OrcStepParams(Re, CFL, dtime_max, dtime0, U0, T_pulse, level_pressure,
+                         OrcSolverOpts(tol_rel, 0.0, max_it, n_sweeps, omega, 0))
+
+
+def fd_exact(abl, n, deltaX0):
+    cc = np.zeros(n)
+    rc = lib().orc_fd_exact(abl, n, float(deltaX0), ptr(cc))
+    if rc != 0:
+        raise ValueError("bad stencil")
+    return cc

@@ -1,0 +1,122 @@
+"""Device Poisson solvers against the CPU FP64 oracle (mod_solvers.f90 restatement).
+
+* BiCGstab_orig with the Jacobi preconditioner: a fixed number of iterations must track the
+  oracle's iterates (the only difference is the order of the FP64 inner-product sums);
+* a converged solve reaches ||b - A x||_2 <= 1e-8 ||b||_2 measured with the oracle's operator;
+* the mixed-precision solve (FP32 inner BiCGstab, FP64 refinement) reaches the same residual;
+* the device_jacobi_solver replacement equals the same number of oracle JOR sweeps;
+* failures (non-finite input, iteration cap) come back as status codes, never as a hang.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import impact_b200 as I
+from _util import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _rhs(og, seed):
+    b = og.random(seed)
+    og.interior(b)[...] -= og.interior(b).mean()  # periodic Laplacian: consistent right-hand side
+    return b
+
+
+def _case(N, L=(1.0, 1.0, 2.0), kinds=(0, 0, 0), precision=0):
+    og, ig = O.Grid(N, L, kinds), I.Grid(N, L, kinds)
+    return og, ig, I.Case(ig, precision=precision)
+
+
+@pytest.mark.parametrize("init_yes", [1, 0])
+@pytest.mark.parametrize("n_sweeps", [0, 1, 4])
+def test_bicgstab_iterates_track_oracle(init_yes, n_sweeps):
+    og, ig, case = _case((17, 25, 33), kinds=(1, 0, 0))
+    b = _rhs(og, 1)
+    x0 = og.random(2) if not init_yes else og.zeros()
+    want = x0.copy()
+    r_o = og.bicgstab(b.copy(), want, tol_rel=0.0, max_it=8, n_sweeps=n_sweeps, omega=0.8, init_yes=bool(init_yes))
+    case.upload("res", b)
+    case.upload("pre", x0)
+    r = case.poisson("res", "pre", I.solver_params(tol_rel=0.0, max_it=8, n_sweeps=n_sweeps, omega=0.8,
+                                                   init_yes=init_yes, check_every=3))
+    got = case.download("pre")
+    assert r.iterations == r_o.iterations == 8
+    assert rel_err(og.interior(got), og.interior(want)) <= 1e-9
+
+
+@pytest.mark.parametrize("kinds", [(0, 0, 0), (1, 1, 0)])
+def test_bicgstab_converges_to_1e8(kinds):
+    og, ig, case = _case((33, 33, 65), kinds=kinds)
+    b = _rhs(og, 3)
+    case.upload("res", b)
+    case.upload("pre", og.zeros())
+    r = case.poisson("res", "pre", I.solver_params(tol_rel=1e-8, max_it=2000, n_sweeps=4, omega=0.8, init_yes=1))
+    assert r.status == 0
+    x = case.download("pre")
+    Ax = og.product_div_grad(x.copy())
+    res = og.interior(b) - og.interior(Ax)
+    assert np.sqrt((res ** 2).sum()) <= 1.5e-8 * np.sqrt((og.interior(b) ** 2).sum())
+    want = og.zeros()
+    r_o = og.bicgstab(b.copy(), want, tol_rel=1e-8, max_it=2000, n_sweeps=4, omega=0.8, init_yes=True)
+    assert abs(r.iterations - r_o.iterations) <= 3
+    d = og.interior(x) - og.interior(want)
+    d -= d.mean()  # the periodic problem fixes x up to a constant
+    assert np.abs(d).max() <= 1e-6 * np.abs(og.interior(want)).max()
+
+
+def test_mixed_precision_solve_reaches_fp64_residual():
+    og, ig, case = _case((33, 33, 65), precision=1)
+    b = _rhs(og, 4)
+    case.upload("res", b)
+    case.upload("pre", og.zeros())
+    r = case.poisson("res", "pre", I.solver_params(tol_rel=1e-8, max_it=20, n_sweeps=4, omega=0.8, init_yes=1,
+                                                   inner_tol_rel=1e-4))
+    assert r.status == 0, r.status
+    assert r.inner_iterations > 0 and r.iterations >= 2
+    x = case.download("pre")
+    Ax = og.product_div_grad(x.copy())
+    res = og.interior(b) - og.interior(Ax)
+    assert np.sqrt((res ** 2).sum()) <= 1e-8 * np.sqrt((og.interior(b) ** 2).sum())
+    want = og.zeros()
+    og.bicgstab(b.copy(), want, tol_rel=1e-10, max_it=4000, n_sweeps=4, omega=0.8, init_yes=True)
+    d = og.interior(x) - og.interior(want)
+    d -= d.mean()
+    assert np.abs(d).max() <= 1e-6 * np.abs(og.interior(want)).max()
+
+
+def test_jacobi_solve_matches_sweeps():
+    og, ig = O.Grid((17, 17, 25)), I.Grid((17, 17, 25))
+    b, rel = og.random(5), og.random(6)
+    want = og.jacobi(b.copy(), rel.copy(), 37, 0.8, init_yes=False)
+    got = rel.copy()
+    sweeps, _ = I.jacobi_solve(ig, got, b, omega=0.8, mode_j=1000, max_sweeps=37)
+    assert sweeps == 37
+    assert rel_err(og.interior(got), og.interior(want)) <= 1e-12
+
+
+def test_jacobi_solve_heuristic_stop_terminates():
+    og, ig = O.Grid((17, 17, 17)), I.Grid((17, 17, 17))
+    b = _rhs(og, 7)
+    rel = og.zeros()
+    sweeps, res = I.jacobi_solve(ig, rel, b, omega=0.8, mode_j=20, max_sweeps=20000)
+    assert 0 < sweeps < 20000 and np.isfinite(res)
+
+
+def test_nonfinite_rhs_reports_status():
+    og, ig, case = _case((17, 17, 17))
+    b = _rhs(og, 8)
+    og.interior(b)[3, 4, 5] = np.nan
+    case.upload("res", b)
+    case.upload("pre", og.zeros())
+    r = case.poisson("res", "pre", I.solver_params(tol_rel=1e-8, max_it=50, init_yes=1))
+    assert r.status == 3
+
+
+def test_iteration_cap_reports_status():
+    og, ig, case = _case((17, 17, 33))
+    b = _rhs(og, 9)
+    case.upload("res", b)
+    case.upload("pre", og.zeros())
+    r = case.poisson("res", "pre", I.solver_params(tol_rel=1e-14, max_it=3, init_yes=1))
+    assert r.status == 1 and r.iterations == 3
