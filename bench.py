@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""bench.py -- IMPACT fractional-step throughput on B200: Mcell-steps/s at a 1e-8 relative
+pressure residual, mixed precision (headline) vs plain FP64.
+
+Workload (default, the mixed-precision single case of the benchmark suite): stenosed vessel on a
+384 x 384 x 768 periodic box (L = 1 x 1 x 2, uniform spacing); cylinder of radius 0.25 L1 with a
+Gaussian constriction at mid-length (60 % area reduction, sigma = 0.5 R); pulsatile plug inflow
+u_z = U0 (1 + 0.5 sin(2 pi t / T)), U0 = 1, T = 1, on the label-5 buffer; Re = 500; dt = 0.2 x the
+RK3 stability limit (get_dtime with CFL = 0.2); every Poisson solve is BiCGstab with a 4-sweep
+JOR (omega = 0.8) preconditioner to ||b - A x||_2 <= 1e-8 ||b||_2.  Starts from rest.  One
+"step" is one RK3 time step (3 substeps, 3 Poisson solves).  Fields are ~0.95 GB each, far
+larger than L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size n]
+
+With N > 1 (launched by torchrun, one rank per GPU) every rank advances an independent replica
+of the case (the path does not shard: replicas only) and `value` is the whole-job aggregate.
+`--impl reference` times IMPACT's CPU algorithm (the FP64 oracle restatement, all host cores)
+on bounded samples of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gpu-impact-ct_b200"))
+
+METRIC = "Mcell-steps/s at 1e-8 pressure residual, mixed vs FP64; serve p50/p99 latency"
+UNIT = "Mcell-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=384, help="cells per x/y axis (z has twice as many)")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--n-sweeps", type=int, default=4)
+    ap.add_argument("--inner-tol", type=float, default=1e-4)
+    ap.add_argument("--precond", type=int, default=1, help="0: JOR sweeps, 1: multigrid V-cycle (default)")
+    ap.add_argument("--check-every", type=int, default=2)
+    return ap.parse_args()
+
+
+def workload(n):
+    return {"workload": f"stenosed-vessel-{n}x{n}x{2 * n}", "cells": n * n * 2 * n, "box": [1.0, 1.0, 2.0],
+            "radius": 0.25, "stenosis": {"z": 1.0, "area_reduction": 0.6, "sigma": 0.125}, "Re": 500.0,
+            "inflow": "U0 (1 + 0.5 sin(2 pi t / T)), U0 = 1, T = 1", "dt": "0.2 x CFL limit",
+            "poisson": "BiCGstab + multigrid V-cycle (damped-Jacobi omega=0.8, 4/4/4 sweeps) to 1e-8 relative", "start": "rest",
+            "l2_flush": "not needed: every field (0.95 GB at 384) exceeds the 126 MB L2"}
+
+
+def build_case(n, precision, device):
+    import impact_b200 as I
+    from impact_b200 import geometry as G
+    N = (n + 1, n + 1, 2 * n + 1)
+    grid = I.Grid(N, (1.0, 1.0, 2.0))
+    lab = G.straight_vessel(grid, radius_frac=0.25, stenoses=[(1.0, 0.6, 0.125)])
+    case = I.Case(grid, precision=precision, device=device)
+    case.set_labels(lab)
+    return grid, lab, case
+
+
+def step_params(args, precision):
+    import impact_b200 as I
+    return I.step_params(Re=500.0, CFL=0.2, dtime_max=1.0, dtime0=1e9, U0=1.0, T_pulse=1.0, level_pressure=1,
+                         tol_rel=1e-8, max_it=(5000 if args.precond == 0 else 200) if precision == 0 else 40,
+                         n_sweeps=args.n_sweeps, omega=0.8, init_yes=0, check_every=args.check_every,
+                         inner_tol_rel=args.inner_tol, inner_max_it=4000 if args.precond == 0 else 400,
+                         precond=args.precond, mg_down=4, mg_up=4, mg_bottom=4)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(gpu_index)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "of measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
+
+
+def traffic_per_cell():
+    """dram bytes per cell and launch of the profiled kernels, from the committed ncu summary."""
+    out = {}
+    p = os.path.join(ROOT, "profiles", "traffic_per_cell.txt")
+    if os.path.exists(p):
+        for line in open(p):
+            if line.startswith("#") or not line.strip():
+                continue
+            k, v = line.split()[:2]
+            out[k] = float(v)
+    return out
+
+
+def run_arm(args, precision, device, rank, world, dist, profile_on, e2e_on):
+    """W warm-up and K timed steps of one case; returns timings and solver statistics."""
+    import numpy as np
+    import torch
+
+    import impact_b200 as I
+
+    grid, lab, case = build_case(args.size, precision, device)
+    sp = step_params(args, precision)
+    for _ in range(args.warmup):
+        case.step(sp)
+    stream = torch.cuda.ExternalStream(case.stream, device=device)
+    # pinned host copies of the state the Fortran host owns between steps (velocity, pressure,
+    # nonlinear term): uploaded before and downloaded after every step, as a drop-in call would
+    host = {f: torch.empty(grid.shape, dtype=torch.float64, pin_memory=True).numpy()
+            for f in ("vel1", "vel2", "vel3", "pre", "nl1", "nl2", "nl3")} if e2e_on else {}
+    for f, a in host.items():
+        case.download(f, a)
+    bytes_in = bytes_out = sum(a.nbytes for a in host.values())
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    if profile_on:
+        I.profile(True)
+    launches0 = I.launch_count()
+    sampler = ClockSampler(device) if rank == 0 and profile_on else None
+    t_dev, t_e2e, its, inner, stats = 0.0, 0.0, [], [], []
+    for _ in range(args.steps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record(stream)
+        for f, a in host.items():
+            case.upload(f, a)
+        e[1].record(stream)
+        st = case.step(sp)
+        e[2].record(stream)
+        for f, a in host.items():
+            case.download(f, a)
+        e[3].record(stream)
+        e[3].synchronize()
+        t_dev += e[1].elapsed_time(e[2])
+        t_e2e += e[0].elapsed_time(e[3])
+        its.append(list(st.poisson_iterations))
+        inner.append(list(st.inner_iterations))
+        stats.append(list(st.poisson_status))
+    torch.cuda.synchronize(device)
+    launches = I.launch_count() - launches0
+    clocks = sampler.stop() if sampler else None
+    prof = I.profile_read() if profile_on else None
+    if profile_on:
+        I.profile(False)
+    if dist is not None:
+        t = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_dev, t_e2e = float(t[0]), float(t[1])
+    out = {"ms_dev": t_dev, "ms_e2e": t_e2e, "iterations": its, "inner_iterations": inner, "status": stats,
+           "launches": launches, "clocks": clocks, "prof": prof, "bytes_in": bytes_in, "bytes_out": bytes_out,
+           "dt": st.dtime, "time": st.time}
+    fields = {f: case.download(f) for f in ("vel1", "vel2", "vel3", "pre", "nl1", "nl2", "nl3")} if rank == 0 else None
+    case.close()
+    del case
+    torch.cuda.empty_cache()
+    return out, fields, grid, lab
+
+
+def cpu_baseline(args, fields, lab, fp64_iters):
+    """The FP64 CPU oracle on the host cores, on a bounded sample of the same workload: one time
+    step with every Poisson solve capped at 2 BiCGstab iterations, plus 2 extra iterations on the
+    resident Poisson problem to price one iteration; scaled to a full step with the iteration count
+    the FP64 device run needed (same algorithm, same preconditioner)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+
+    import oracle as O
+
+    n = args.size
+    N = (n + 1, n + 1, 2 * n + 1)
+    g = O.Grid(N, (1.0, 1.0, 2.0))
+    vel = np.stack([fields["vel1"], fields["vel2"], fields["vel3"]])
+    nl = np.stack([fields["nl1"], fields["nl2"], fields["nl3"]])
+    pre = fields["pre"].copy()
+    st = O.OrcStepState()
+    st.timestep = 10
+    mg = g.multigrid() if args.precond == 1 else None
+    p = O.step_params(Re=500.0, CFL=0.2, dtime_max=1.0, tol_rel=1e-8, max_it=1, n_sweeps=args.n_sweeps, omega=0.8,
+                      mg=mg)
+    t0 = time.perf_counter()
+    g.time_step(p, lab, vel, nl, pre, st)
+    t_capped = time.perf_counter() - t0
+    used = sum(st.poisson_iterations)
+    # price of two more BiCGstab iterations on the current Poisson problem
+    b = g.divergence2(vel[0].copy(), vel[1].copy(), vel[2].copy())
+    t0 = time.perf_counter()
+    if mg is not None:
+        r = mg.bicgstab(b, pre.copy(), tol_rel=0.0, max_it=2, omega=0.8, init_yes=False)
+    else:
+        r = g.bicgstab(b, pre.copy(), tol_rel=0.0, max_it=2, n_sweeps=args.n_sweeps, omega=0.8, init_yes=False)
+    t_two = time.perf_counter() - t0
+    t_it = t_two / max(1, r.iterations)
+    full = t_capped + max(0.0, sum(fp64_iters) - used) * t_it
+    cells = n * n * 2 * n
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": cells / full / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": (f"FP64 oracle, {n}x{n}x{2*n}, same preconditioner: one step with Poisson solves capped at 1 BiCGstab "
+                       f"iterations ({t_capped:.1f} s) + 2 iterations ({t_two:.1f} s); scaled to "
+                       f"{sum(fp64_iters)} iterations per step (FP64 device run)"),
+            "seconds_per_step": full}
+
+
+def reference_arm(args, rank, world):
+    """IMPACT's CPU algorithm (FP64 oracle, all host cores) on bounded samples of the workload."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+
+    import oracle as O
+    from impact_b200 import geometry as G
+
+    n = args.size
+    N = (n + 1, n + 1, 2 * n + 1)
+    g = O.Grid(N, (1.0, 1.0, 2.0))
+    lab = G.straight_vessel(g, radius_frac=0.25, stenoses=[(1.0, 0.6, 0.125)])
+    vel, nl, pre = g.zeros(3), g.zeros(3), g.zeros()
+    st = O.OrcStepState()
+    # warm-up: develop the flow with capped solves (bounded work), then time capped steps and
+    # price BiCGstab iterations; extrapolate to the iteration count a full 1e-8 solve needs
+    cap = 1
+    mg = g.multigrid() if args.precond == 1 else None
+    p = O.step_params(Re=500.0, CFL=0.2, dtime_max=1.0, tol_rel=1e-8, max_it=cap, n_sweeps=args.n_sweeps, omega=0.8,
+                      mg=mg)
+    for _ in range(min(args.warmup, 2)):
+        g.time_step(p, lab, vel, nl, pre, st)
+    ref_iters = 3 * _iters_estimate(n, args.precond)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        g.time_step(p, lab, vel, nl, pre, st)
+        t_capped = time.perf_counter() - t0
+        used = sum(st.poisson_iterations)
+        b = g.divergence2(vel[0].copy(), vel[1].copy(), vel[2].copy())
+        t0 = time.perf_counter()
+        if mg is not None:
+            r = mg.bicgstab(b, pre.copy(), tol_rel=0.0, max_it=2, omega=0.8)
+        else:
+            r = g.bicgstab(b, pre.copy(), tol_rel=0.0, max_it=2, n_sweeps=args.n_sweeps, omega=0.8)
+        t_it = (time.perf_counter() - t0) / max(1, r.iterations)
+        times.append(t_capped + max(0, ref_iters - used) * t_it)
+    cells = n * n * 2 * n
+    val = cells * len(times) / sum(times) / 1e6
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload(n),
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": (f"each step: one FP64 oracle step with Poisson solves capped at {cap} "
+                                        f"BiCGstab iterations + 2 priced iterations, extrapolated to {ref_iters} "
+                                        "iterations per step")},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _iters_estimate(n, precond=1):
+    """BiCGstab iterations per 1e-8 solve measured on the device for this workload family:
+    JOR-4 preconditioner ~1.6 n (64: 110, 128: 210, 256: 405); multigrid V-cycle ~8, independent
+    of n."""
+    return 8 if precond == 1 else int(round(1.6 * n))
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    device = local if world > 1 else 0
+    mixed, fields, grid, lab = run_arm(args, 1, device, rank, world, dist, profile_on=True, e2e_on=True)
+    fp64 = None
+    if not args.no_fp64:
+        fp64, fields64, _, _ = run_arm(args, 0, device, rank, world, dist, profile_on=False, e2e_on=False)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    cells = args.size * args.size * 2 * args.size
+    K = args.steps
+    value = world * cells * K / (mixed["ms_dev"] / 1e3) / 1e6
+    e2e = world * cells * K / (mixed["ms_e2e"] / 1e3) / 1e6
+    peaks, peak_note = measured_peaks()
+    prof = mixed["prof"] or {}
+    dom = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
+    roof = None
+    if dom and dom[1][0] > 0:
+        name, (launches, ms, byts) = dom
+        per_launch_bytes = byts / launches
+        achieved = per_launch_bytes / (ms / launches / 1e3) / 1e9
+        tpc = traffic_per_cell().get(name)
+        roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peak_note,
+                "traffic": (tpc * cells) if tpc else None, "algorithmic_bytes_per_launch": per_launch_bytes,
+                "launches": launches, "avg_launch_ms": ms / launches,
+                "share_of_step": round(ms / mixed["ms_dev"], 3),
+                "all_kernels": {k: {"launches": v[0], "ms": round(v[1], 2),
+                                    "GB/s": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] > 0 else None}
+                                for k, v in prof.items() if v[0] > 0}}
+    line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": mixed["ms_dev"] / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner solve / f64 residual+RHS", "data": "synthetic",
+            "config": dict(workload(args.size), parallelism=f"replicas x{world}" if world > 1 else "single GPU",
+                           precision="mixed"),
+            "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": mixed["bytes_in"],
+                    "d2h_bytes_per_step": mixed["bytes_out"]},
+            "gpu_launches": mixed["launches"], "clocks": mixed["clocks"], "roofline": roof,
+            "solver": {"mixed_outer_per_substep": mixed["iterations"], "mixed_inner_per_substep": mixed["inner_iterations"],
+                       "status": mixed["status"], "dt": mixed["dt"]}}
+    if fp64 is not None:
+        v64 = world * cells * K / (fp64["ms_dev"] / 1e3) / 1e6
+        line["fp64"] = {"value": round(v64, 3), "unit": UNIT, "ms_per_step": fp64["ms_dev"] / K,
+                        "iterations_per_substep": fp64["iterations"], "status": fp64["status"]}
+        line["mixed_over_fp64"] = round(value / v64, 3)
+    if world == 1 and not args.no_cpu:
+        its = fp64["iterations"][-1] if fp64 is not None else [_iters_estimate(args.size, args.precond)] * 3
+        try:
+            line["cpu_baseline"] = cpu_baseline(args, fields, lab, its)
+        except Exception as ex:  # the CPU sample must never hide the device number
+            line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

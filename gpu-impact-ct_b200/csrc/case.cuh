@@ -4,6 +4,7 @@
 
 #include "../../include/impact_b200.h"
 #include "common.cuh"
+#include "mg.cuh"
 #include "solver.cuh"
 
 namespace impact {
@@ -33,6 +34,11 @@ struct CaseState {
   // FP64 Krylov work (8 fields), or the mixed-precision set
   KrylovWork<double> kw64{};
   MixedWork mw{};
+  // multigrid hierarchy (levels >= 1 own their fields); FP64 for plain cases, FP32 for the
+  // inner solve of mixed-precision cases
+  int mg_levels = 0;
+  MGData<double> mg64{};
+  MGData<float> mg32{};
   double* partial = nullptr;     // reduction scratch of the step kernels
   double* dscal = nullptr;       // small device scalars (dt, mean pressure, ...)
   double* hscal = nullptr;       // pinned host mirror

@@ -175,3 +175,87 @@ extern "C" int impact_b200_axis_coeffs(int M, const double* xp, const double* xu
   }
   return 0;
 }
+
+// ---------------------------------------------------------------------------------------
+// multigrid hierarchy (periodic)
+// ---------------------------------------------------------------------------------------
+#include "mg_host.h"
+
+namespace impact {
+
+static void compact_laplacian(int M, const double* xp, const double* xu, double* cdg) {
+  std::vector<double> dm(M + 1), dp(M + 1), gm(M + 1), gp(M + 1);
+  for (int i = 1; i <= M; ++i) {
+    dm[i] = -1.0 / (xu[i + 3] - xu[i - 1 + 3]);
+    dp[i] = 1.0 / (xu[i + 3] - xu[i - 1 + 3]);
+  }
+  for (int i = 0; i <= M; ++i) {
+    gm[i] = -1.0 / (xp[i + 1 + 3] - xp[i + 3]);
+    gp[i] = 1.0 / (xp[i + 1 + 3] - xp[i + 3]);
+  }
+  for (int i = 1; i <= M; ++i) {
+    cdg[3 * (i - 1) + 0] = dm[i] * gm[i - 1];
+    cdg[3 * (i - 1) + 1] = dm[i] * gp[i - 1] + dp[i] * gm[i];
+    cdg[3 * (i - 1) + 2] = dp[i] * gp[i];
+  }
+}
+
+std::vector<MGHostLevel> build_mg_hierarchy(const int N[3], const double* const xp[3], const double* const xu[3],
+                                            const double L[3], int n_grids_limit) {
+  constexpr int GMAX = 15;
+  int MM[GMAX][3];
+  for (int m = 0; m < 3; ++m) MM[0][m] = N[m];
+  int ng = 1;
+  for (int g = 1; g < GMAX; ++g)
+    for (int m = 0; m < 3; ++m) {
+      if ((MM[g - 1][m] - 1) % 2 == 0 && MM[g - 1][m] >= 5) {  // 5 = 2 (Nmin - 1) + 1
+        MM[g][m] = (MM[g - 1][m] - 1) / 2 + 1;
+        ng = g + 1;
+      } else {
+        MM[g][m] = MM[g - 1][m];
+      }
+    }
+  if (n_grids_limit < 1) n_grids_limit = 1;
+  if (ng > n_grids_limit) ng = n_grids_limit;
+  std::vector<MGHostLevel> lv(ng);
+  for (int g = 0; g < ng; ++g)
+    for (int m = 0; m < 3; ++m) {
+      const int M = MM[g][m];
+      MGHostLevel& L_ = lv[g];
+      L_.M[m] = M;
+      L_.ratio[m] = (g + 1 < ng) ? (MM[g][m] - 1) / (MM[g + 1][m] - 1) : 1;
+      const double* y1p = xp[m];
+      std::vector<double> p(M + 7, 0.0), u(M + 7, 0.0);
+      const int di = (MM[0][m] - 1) / (M - 1);  // level spacing in finest-grid points
+      if (g == 0) {
+        p.assign(xp[m], xp[m] + M + 7);
+        u.assign(xu[m], xu[m] + M + 7);
+      } else {
+        for (int i = 1; i <= M; ++i) p[i + 3] = y1p[1 + di * i - di + 3];
+        for (int i = 1; i <= M - 1; ++i) u[i + 3] = y1p[1 + di * i - di / 2 + 3];
+        for (int i = -3; i <= 0; ++i) {
+          p[i + 3] = p[M - 1 + i + 3] - L[m];
+          u[i + 3] = u[M - 1 + i + 3] - L[m];
+        }
+        for (int i = M; i <= M + 3; ++i) {
+          p[i + 3] = p[i - M + 1 + 3] + L[m];
+          u[i + 3] = u[i - M + 1 + 3] + L[m];
+        }
+      }
+      L_.cdg[m].assign(3 * M, 0.0);
+      compact_laplacian(M, p.data(), u.data(), L_.cdg[m].data());
+      L_.cI[m].assign(2 * (M + 1), 0.0);
+      if (g + 1 < ng) {
+        for (int i = 2; i <= M - 1; i += 2) {
+          const int i0 = 1 + (i - 1) * di;
+          const double Dx10 = y1p[i0 + 3] - y1p[i0 - di + 3];
+          const double Dx12 = y1p[i0 + di + 3] - y1p[i0 - di + 3];
+          L_.cI[m][2 * i + 0] = 1. - Dx10 / Dx12;
+          L_.cI[m][2 * i + 1] = Dx10 / Dx12;
+        }
+      }
+    }
+  return lv;
+}
+
+}  // namespace impact

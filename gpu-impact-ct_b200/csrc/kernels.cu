@@ -8,6 +8,7 @@
 // starts at offset 4 of a row whose length is a multiple of 8 for cell counts divisible
 // by 8).
 #include "kernels.cuh"
+#include "stencil25d.cuh"
 
 namespace impact {
 
@@ -415,37 +416,8 @@ void launch_fill_ghosts(const Geom& g, double* phi, cudaStream_t s) {
 // (gradient stored to a double, then divergence m = 1 overwrite, m = 2,3 accumulate).
 // ------------------------------------------------------------------------------------
 template <typename T>
-__device__ __forceinline__ T divgrad_axis(const Geom& g, const T* __restrict__ cG, const T* __restrict__ cD,
-                                          const T* __restrict__ x, long long base, long long st, int q, int n,
-                                          T acc, bool first) {
-  T xs[11];
-#pragma unroll
-  for (int l = 0; l < 11; ++l) xs[l] = __ldg(x + base + (long long)(wrapi(q - 5 + l, n) + 3) * st);
-  const T* cd = cD + (long long)q * ND;
-  T s = acc;
-#pragma unroll
-  for (int l = 0; l < ND; ++l) {
-    const int qq = wrapi(q + D_LO + l, n);  // velocity point q-3+l
-    const T* cg = cG + (long long)qq * NG;
-    // gradient at velocity point q-3+l uses x at (q-3+l) + (-2..3) -> xs index l .. l+5
-    T gv = cg[0] * xs[l];
-#pragma unroll
-    for (int r = 1; r < NG; ++r) gv = gv + cg[r] * xs[l + r];
-    s = (first && l == 0) ? cd[0] * gv : s + cd[l] * gv;
-  }
-  return s;
-}
-template <typename T>
-__global__ void __launch_bounds__(BX* BY) k_div_grad(Geom g, Coeffs<T> c, const T* __restrict__ x, T* __restrict__ lap) {
-  POINT_PROLOGUE
-  T s = divgrad_axis(g, c.cG[0], c.cD[0], x, off(g, -3, j, k), 1, i, g.n1, T(0), true);
-  s = divgrad_axis(g, c.cG[1], c.cD[1], x, off(g, i, -3, k), g.nx, j, g.n2, s, false);
-  s = divgrad_axis(g, c.cG[2], c.cD[2], x, off(g, i, j, -3), g.nxy, k, g.n3, s, false);
-  lap[off(g, i, j, k)] = s;
-}
-template <typename T>
 void launch_div_grad(const Geom& g, const Coeffs<T>& c, const T* x, T* lap, cudaStream_t s) {
-  k_div_grad<T><<<grid3(g), dim3(BX, BY), 0, s>>>(g, c, x, lap);
+  launch_divgrad25<T, 0>(g, c, nullptr, x, lap, nullptr, nullptr, s);
 }
 
 // ------------------------------------------------------------------------------------

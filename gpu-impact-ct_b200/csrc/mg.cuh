@@ -1,0 +1,31 @@
+// mg.cuh -- geometric multigrid V-cycle on the device (internal).
+#pragma once
+#include "common.cuh"
+
+namespace impact {
+
+constexpr int MG_MAX_LEVELS = 15;
+
+template <typename T>
+struct MGLevel {
+  Geom g;
+  const T* cdg[3];  // compact Laplacian of the level
+  const T* cI[3];   // interpolation weights cI(1:2, 0:M) of the level
+  int ratio[3];     // coarsening factor to the next level
+  T *A, *B, *C;     // right-hand side, solution, work (levels >= 1)
+};
+
+template <typename T>
+struct MGData {
+  int n = 0;
+  MGLevel<T> lv[MG_MAX_LEVELS];
+  int n_down = 4, n_up = 4, n_bottom = 4;
+  double omega = 0.8;
+};
+
+// multigridV (mod_solvers.f90:456-585) with init_yes = .TRUE., gstart = 1: z = M v.
+// work0: one level-1 field; every kernel is a no-op once sc reports the solve as finished.
+template <typename T>
+void mg_vcycle(const MGData<T>& mg, const SolverScalars* sc, const T* v, T* z, T* work0, cudaStream_t s);
+
+}  // namespace impact

@@ -1,0 +1,119 @@
+// prof.cu -- event-based per-kernel timing and launch counting (see prof.cuh).
+#include <atomic>
+#include <mutex>
+#include <vector>
+
+#include "../../include/impact_b200.h"
+#include "prof.cuh"
+
+namespace impact {
+namespace prof {
+
+namespace {
+struct Pending {
+  int kid;
+  double bytes;
+  cudaEvent_t a, b;
+};
+std::mutex mu;
+bool on = false;
+std::vector<cudaEvent_t> pool;
+std::vector<Pending> pending;
+std::vector<cudaEvent_t> open_start;  // token -> start event
+long long launches[K_COUNT] = {};
+double total_ms[K_COUNT] = {};
+double total_bytes[K_COUNT] = {};
+std::atomic<long long> g_count{0};
+
+cudaEvent_t take() {
+  if (!pool.empty()) {
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+const char* kNames[K_COUNT] = {"jacobi_sweep", "jacobi_init2", "div_grad_dot", "x_update", "p_update",
+                               "r_update", "nl_rhs", "project", "divergence2"};
+}  // namespace
+
+bool enabled() { return on; }
+
+int begin(cudaStream_t s) {
+  if (!on) return -1;
+  std::lock_guard<std::mutex> lk(mu);
+  cudaEvent_t e = take();
+  cudaEventRecord(e, s);
+  open_start.push_back(e);
+  return (int)open_start.size() - 1;
+}
+
+void end(int token, int kid, double bytes, cudaStream_t s) {
+  if (token < 0) return;
+  std::lock_guard<std::mutex> lk(mu);
+  cudaEvent_t e = take();
+  cudaEventRecord(e, s);
+  pending.push_back({kid, bytes, open_start[token], e});
+  open_start[token] = nullptr;
+  // compact the token table once every open pair is closed
+  bool all_closed = true;
+  for (cudaEvent_t x : open_start)
+    if (x) {
+      all_closed = false;
+      break;
+    }
+  if (all_closed) open_start.clear();
+}
+
+void flush() {
+  if (!on) return;
+  std::lock_guard<std::mutex> lk(mu);
+  std::vector<Pending> keep;
+  for (Pending& p : pending) {
+    if (cudaEventQuery(p.b) != cudaSuccess) {
+      keep.push_back(p);
+      continue;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, p.a, p.b);
+    launches[p.kid] += 1;
+    total_ms[p.kid] += ms;
+    total_bytes[p.kid] += p.bytes;
+    pool.push_back(p.a);
+    pool.push_back(p.b);
+  }
+  pending.swap(keep);
+}
+
+void count(long long n) { g_count += n; }
+
+}  // namespace prof
+}  // namespace impact
+
+using namespace impact::prof;
+
+extern "C" void impact_b200_profile_enable(int enable) {
+  std::lock_guard<std::mutex> lk(mu);
+  on = enable != 0;
+}
+extern "C" void impact_b200_profile_reset(void) {
+  std::lock_guard<std::mutex> lk(mu);
+  for (int k = 0; k < K_COUNT; ++k) {
+    launches[k] = 0;
+    total_ms[k] = 0.0;
+    total_bytes[k] = 0.0;
+  }
+}
+extern "C" int impact_b200_profile_read(int kid, long long* n, double* ms, double* bytes, const char** name) {
+  flush();
+  if (kid < 0 || kid >= K_COUNT) return -1;
+  std::lock_guard<std::mutex> lk(mu);
+  if (n) *n = launches[kid];
+  if (ms) *ms = total_ms[kid];
+  if (bytes) *bytes = total_bytes[kid];
+  if (name) *name = kNames[kid];
+  return 0;
+}
+extern "C" long long impact_b200_launch_count(void) { return g_count.load(); }

@@ -8,7 +8,10 @@
 #include <cmath>
 #include <cstdio>
 
+#include "prof.cuh"
 #include "solver.cuh"
+#include "stencil25d.cuh"
+#include <cstdlib>
 
 namespace impact {
 
@@ -26,6 +29,8 @@ long long reduce_partial_doubles(const Geom& g, int nq) {
   (void)nq;
   return nblocks3(g) * 4 + FIN1_BLOCKS * 4 + 64;
 }
+// stage-1 sums live at partial + nb*4 with nb the block count of the producing kernel; the raw
+// results of callers sit past the largest such region
 static inline double* raw_results(double* partial, const Geom& g) { return partial + nblocks3(g) * 4 + FIN1_BLOCKS * 4; }
 template <typename T>
 long long krylov_partial_doubles(const Geom& g) {
@@ -219,6 +224,7 @@ static void finalize(const double* partial, long long nb, int nq, int maxmask, i
   double* p1 = const_cast<double*>(partial) + nb * 4;
   k_fin1<<<FIN1_BLOCKS, 256, 0, s>>>(partial, nb, nq, maxmask, p1, (mode == FIN_RAW || mode == FIN_INIT) ? nullptr : sc);
   k_fin2<<<1, 256, 0, s>>>(p1, FIN1_BLOCKS, nq, maxmask, mode, sc, raw_out);
+  prof::count(2);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -298,49 +304,6 @@ __global__ void __launch_bounds__(NT) k_init_residual(Geom g, int zero_phi, cons
   block_partials<4, 1>(v, partial);
 }
 
-// high-order Laplacian fused with dot products: out = A x; partials of out.d1 (and out.out, d2.out)
-template <typename T>
-__device__ __forceinline__ T divgrad_axis(const T* __restrict__ cG, const T* __restrict__ cD, const T* __restrict__ x,
-                                          long long base, long long st, int q, int n, T acc, bool first) {
-  T xs[11];
-#pragma unroll
-  for (int l = 0; l < 11; ++l) xs[l] = __ldg(x + base + (long long)(wrapi(q - 5 + l, n) + 3) * st);
-  const T* cd = cD + (long long)q * ND;
-  T s = acc;
-#pragma unroll
-  for (int l = 0; l < ND; ++l) {
-    const int qq = wrapi(q + D_LO + l, n);
-    const T* cg = cG + (long long)qq * NG;
-    T gv = cg[0] * xs[l];
-#pragma unroll
-    for (int r = 1; r < NG; ++r) gv = gv + cg[r] * xs[l + r];
-    s = (first && l == 0) ? cd[0] * gv : s + cd[l] * gv;
-  }
-  return s;
-}
-template <typename T, int MODE>  // MODE 1: partial out.d1 ; MODE 2: partials d1.out, out.out
-__global__ void __launch_bounds__(NT) k_divgrad_dot(Geom g, Coeffs<T> c, const SolverScalars* __restrict__ sc,
-                                                    const T* __restrict__ x, T* __restrict__ out,
-                                                    const T* __restrict__ d1, double* __restrict__ partial) {
-  if (halted(sc)) return;
-  PT_SETUP
-  double v[MODE] = {};
-  if (in) {
-    T s = divgrad_axis(c.cG[0], c.cD[0], x, off(g, -3, j, k), 1, i, g.n1, T(0), true);
-    s = divgrad_axis(c.cG[1], c.cD[1], x, off(g, i, -3, k), g.nx, j, g.n2, s, false);
-    s = divgrad_axis(c.cG[2], c.cD[2], x, off(g, i, j, -3), g.nxy, k, g.n3, s, false);
-    out[p] = s;
-    const double sd = (double)s;
-    if (MODE == 1) {
-      v[0] = sd * (double)d1[p];
-    } else {
-      v[0] = (double)d1[p] * sd;
-      v[MODE - 1] = sd * sd;
-    }
-  }
-  block_partials<MODE, 0>(v, partial);
-}
-
 // Jacobi preconditioner sweeps, halted-aware wrappers
 template <typename T>
 __device__ __forceinline__ T init_val(const T* c1, const T* c2, const T* c3, T omega, T bb, int i, int j, int k) {
@@ -361,57 +324,23 @@ __global__ void __launch_bounds__(NT) k_pc_init1(Geom g, Coeffs<T> c, T omega, c
   out[p] = init_val(c.cdg[0], c.cdg[1], c.cdg[2], omega, bb[p], i, j, k);
 }
 template <typename T>
-__global__ void __launch_bounds__(NT) k_pc_init2(Geom g, Coeffs<T> c, T omega, const SolverScalars* __restrict__ sc,
-                                                 const T* __restrict__ bb, T* __restrict__ out) {
-  if (halted(sc)) return;
-  PT_SETUP
-  if (!in) return;
-  const int im = wrapi(i - 1, g.n1), ip = wrapi(i + 1, g.n1), jm = wrapi(j - 1, g.n2), jp = wrapi(j + 1, g.n2),
-            km = wrapi(k - 1, g.n3), kp = wrapi(k + 1, g.n3);
-  const T* c1 = c.cdg[0];
-  const T* c2 = c.cdg[1];
-  const T* c3 = c.cdg[2];
-  const T bc = __ldg(bb + p);
-  const T xc = init_val(c1, c2, c3, omega, bc, i, j, k);
-  const T xm = init_val(c1, c2, c3, omega, __ldg(bb + off(g, im, j, k)), im, j, k);
-  const T xp = init_val(c1, c2, c3, omega, __ldg(bb + off(g, ip, j, k)), ip, j, k);
-  const T ym = init_val(c1, c2, c3, omega, __ldg(bb + off(g, i, jm, k)), i, jm, k);
-  const T yp = init_val(c1, c2, c3, omega, __ldg(bb + off(g, i, jp, k)), i, jp, k);
-  const T zm = init_val(c1, c2, c3, omega, __ldg(bb + off(g, i, j, km)), i, j, km);
-  const T zp = init_val(c1, c2, c3, omega, __ldg(bb + off(g, i, j, kp)), i, j, kp);
-  out[p] = jac(c1 + 3 * (i - 1), c2 + 3 * (j - 1), c3 + 3 * (k - 1), omega, bc, xc, xm, xp, ym, yp, zm, zp);
-}
-template <typename T>
-__global__ void __launch_bounds__(NT) k_pc_sweep(Geom g, Coeffs<T> c, T omega, const SolverScalars* __restrict__ sc,
-                                                 const T* __restrict__ bb, const T* __restrict__ rel,
-                                                 T* __restrict__ out) {
-  if (halted(sc)) return;
-  PT_SETUP
-  if (!in) return;
-  const T* c1 = c.cdg[0];
-  const T* c2 = c.cdg[1];
-  const T* c3 = c.cdg[2];
-  out[p] = jac(c1 + 3 * (i - 1), c2 + 3 * (j - 1), c3 + 3 * (k - 1), omega, __ldg(bb + p), __ldg(rel + p),
-               __ldg(rel + off(g, wrapi(i - 1, g.n1), j, k)), __ldg(rel + off(g, wrapi(i + 1, g.n1), j, k)),
-               __ldg(rel + off(g, i, wrapi(j - 1, g.n2), k)), __ldg(rel + off(g, i, wrapi(j + 1, g.n2), k)),
-               __ldg(rel + off(g, i, j, wrapi(k - 1, g.n3))), __ldg(rel + off(g, i, j, wrapi(k + 1, g.n3))));
-}
-
-template <typename T>
 static void precond(const Geom& g, const Coeffs<T>& c, int n, T omega, const SolverScalars* sc, const T* v, T* z,
                     T* comp, cudaStream_t s) {
   const dim3 gr = grid3(g), bl(BX, BY);
+  const double cells = (double)g.n1 * g.n2 * g.n3;
   if (n == 1) {
-    k_pc_init1<T><<<gr, bl, 0, s>>>(g, c, omega, sc, v, z);
+    IMPACT_PROF(prof::K_PC_INIT2, 2.0 * sizeof(T) * cells, s, k_pc_init1<T><<<gr, bl, 0, s>>>(g, c, omega, sc, v, z));
     return;
   }
   // writes w_1 .. w_{n-1}; the last one must land in z
   T* bufs[2] = {z, comp};
   int tgt = ((n - 1) % 2 == 1) ? 0 : 1;
-  k_pc_init2<T><<<gr, bl, 0, s>>>(g, c, omega, sc, v, bufs[tgt]);
+  IMPACT_PROF(prof::K_PC_INIT2, 2.0 * sizeof(T) * cells, s,
+              (launch_jacobi25<T, 1>(g, c, sc, omega, v, nullptr, bufs[tgt], s)));
   for (int w = 2; w <= n - 1; ++w) {
     const int nt = 1 - tgt;
-    k_pc_sweep<T><<<gr, bl, 0, s>>>(g, c, omega, sc, v, bufs[tgt], bufs[nt]);
+    IMPACT_PROF(prof::K_PC_SWEEP, 3.0 * sizeof(T) * cells, s,
+                (launch_jacobi25<T, 0>(g, c, sc, omega, v, bufs[tgt], bufs[nt], s)));
     tgt = nt;
   }
 }
@@ -437,16 +366,21 @@ int bicgstab(const Geom& g, const Coeffs<T>& c, const SolverOpts& o, const T* bb
              cudaStream_t s, SolverResult* res) {
   const dim3 gr = grid3(g), bl(BX, BY);
   const long long nb = nblocks3(g);
-  const bool pre_on = o.n_sweeps > 0;
+  const long long nb25 = s25_blocks(g);
+  const double cells = (double)g.n1 * g.n2 * g.n3;
+  const bool use_mg = o.precond == 1 && o.mg != nullptr;
+  const bool pre_on = use_mg || o.n_sweeps > 0;
   const T om = (T)o.omega;
+  const MGData<T>* mg = static_cast<const MGData<T>*>(o.mg);
   SolverScalars init{};
   init.tol_rel = o.tol_rel;
   init.tol_abs_inf = o.tol_abs_inf;
   init.max_it = o.max_it;
   cudaMemcpyAsync(w.scal, &init, sizeof(SolverScalars), cudaMemcpyHostToDevice, s);
   // initial residual
-  if (!o.init_yes) k_divgrad_dot<T, 1><<<gr, bl, 0, s>>>(g, c, w.scal, phi, w.rr, w.rr, w.partial);
+  if (!o.init_yes) launch_divgrad25<T, 0>(g, c, w.scal, phi, w.rr, nullptr, nullptr, s);
   k_init_residual<T><<<gr, bl, 0, s>>>(g, o.init_yes, bb, phi, w.rr, w.rh, w.partial);
+  prof::count(o.init_yes ? 1 : 2);
   finalize(w.partial, nb, 4, 1, FIN_INIT, w.scal, nullptr, s);
 
   const int chunk = o.check_every > 0 ? o.check_every : 1;
@@ -454,30 +388,43 @@ int bicgstab(const Geom& g, const Coeffs<T>& c, const SolverOpts& o, const T* bb
   for (;;) {
     for (int t = 0; t < chunk; ++t) {
       k_begin<<<1, 1, 0, s>>>(w.scal);
-      k_p_update<T><<<gr, bl, 0, s>>>(g, w.scal, w.rr, w.Ap, w.pp);
+      prof::count(1);
+      IMPACT_PROF(prof::K_P_UPDATE, 4.0 * sizeof(T) * cells, s,
+                  k_p_update<T><<<gr, bl, 0, s>>>(g, w.scal, w.rr, w.Ap, w.pp));
       T* z1 = w.pp;
-      if (pre_on) {
+      if (use_mg) {
+        mg_vcycle<T>(*mg, w.scal, w.pp, w.z1, w.comp, s);
+        z1 = w.z1;
+      } else if (pre_on) {
         precond<T>(g, c, o.n_sweeps, om, w.scal, w.pp, w.z1, w.comp, s);
         z1 = w.z1;
       }
-      k_divgrad_dot<T, 1><<<gr, bl, 0, s>>>(g, c, w.scal, z1, w.Ap, w.rh, w.partial);
-      finalize(w.partial, nb, 1, 0, FIN_ALPHA, w.scal, nullptr, s);
-      k_r_update<T><<<gr, bl, 0, s>>>(g, w.scal, w.Ap, w.rr);
+      IMPACT_PROF(prof::K_DIVGRAD, 3.0 * sizeof(T) * cells, s,
+                  (launch_divgrad25<T, 1>(g, c, w.scal, z1, w.Ap, w.rh, w.partial, s)));
+      finalize(w.partial, nb25, 1, 0, FIN_ALPHA, w.scal, nullptr, s);
+      IMPACT_PROF(prof::K_R_UPDATE, 3.0 * sizeof(T) * cells, s,
+                  k_r_update<T><<<gr, bl, 0, s>>>(g, w.scal, w.Ap, w.rr));
       T* z2 = w.rr;
-      if (pre_on) {
+      if (use_mg) {
+        mg_vcycle<T>(*mg, w.scal, w.rr, w.z2, w.comp, s);
+        z2 = w.z2;
+      } else if (pre_on) {
         precond<T>(g, c, o.n_sweeps, om, w.scal, w.rr, w.z2, w.comp, s);
         z2 = w.z2;
       }
-      k_divgrad_dot<T, 2><<<gr, bl, 0, s>>>(g, c, w.scal, z2, w.Ar, w.rr, w.partial);
-      finalize(w.partial, nb, 2, 0, FIN_OMEGA, w.scal, nullptr, s);
+      IMPACT_PROF(prof::K_DIVGRAD, 3.0 * sizeof(T) * cells, s,
+                  (launch_divgrad25<T, 2>(g, c, w.scal, z2, w.Ar, w.rr, w.partial, s)));
+      finalize(w.partial, nb25, 2, 0, FIN_OMEGA, w.scal, nullptr, s);
       // without a preconditioner z2 aliases rr: the x update reads rr before overwriting it
-      k_x_update<T><<<gr, bl, 0, s>>>(g, w.scal, z1, z2, w.Ar, w.rh, phi, w.rr, w.partial);
+      IMPACT_PROF(prof::K_X_UPDATE, 8.0 * sizeof(T) * cells, s,
+                  k_x_update<T><<<gr, bl, 0, s>>>(g, w.scal, z1, z2, w.Ar, w.rh, phi, w.rr, w.partial));
       finalize(w.partial, nb, 3, 1, FIN_NORMS, w.scal, nullptr, s);
       ++launched;
     }
     cudaError_t e = cudaMemcpyAsync(w.scal_host, w.scal, sizeof(SolverScalars), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return impact_set_error(e, "bicgstab poll", __FILE__, __LINE__);
+    prof::flush();
     const SolverScalars& h = *w.scal_host;
     if (h.status == 4) {
       // rhr == 0: new shadow residual rh = rr, as the reference does, then redo the iteration start
@@ -537,48 +484,66 @@ template void reduce_norms<float>(const Geom&, const float*, double*, double*, c
 // ---------------------------------------------------------------------------------------
 // mixed precision: FP64 iterative refinement around an FP32 BiCGstab
 // ---------------------------------------------------------------------------------------
-// r64 = b - A64 x ; r32 = (float) r64 ; partials [max|r|, sum r^2, sum b^2]
+// r64 = b - A64 x ; partials [max|r|, sum r^2, sum b^2]
 __global__ void __launch_bounds__(NT) k_outer_residual(Geom g, const double* __restrict__ bb,
                                                        const double* __restrict__ ax, double* __restrict__ r64,
-                                                       float* __restrict__ r32, double* __restrict__ partial) {
+                                                       double* __restrict__ partial) {
   PT_SETUP
   double v[3] = {0.0, 0.0, 0.0};
   if (in) {
     const double b = bb[p];
     const double r = b - ax[p];
     r64[p] = r;
-    r32[p] = (float)r;
     v[0] = fabs(r);
     v[1] = r * r;
     v[2] = b * b;
   }
   block_partials<3, 1>(v, partial);
 }
-__global__ void __launch_bounds__(NT) k_apply_correction(Geom g, const float* __restrict__ e, double* __restrict__ x) {
+// r32 = (float)(r64 * scale): the inner right-hand side normalised to |r|_inf = 1
+__global__ void __launch_bounds__(NT) k_to_f32(Geom g, const double* __restrict__ r64, double scale,
+                                               float* __restrict__ r32) {
   PT_SETUP
   if (!in) return;
-  x[p] = x[p] + (double)e[p];
+  r32[p] = (float)(r64[p] * scale);
+}
+// x += unscale * e
+__global__ void __launch_bounds__(NT) k_apply_correction(Geom g, const float* __restrict__ e, double unscale,
+                                                         double* __restrict__ x) {
+  PT_SETUP
+  if (!in) return;
+  x[p] = x[p] + unscale * (double)e[p];
 }
 
+// Iterative refinement (mod_solvers.f90 has no counterpart; the FP64 outer loop wraps the
+// reference's BiCGstab run in FP32): r = b - A x in FP64, e = A^-1 r approximately by an FP32
+// BiCGstab on the normalised r, x += e.  An inner solve that breaks down or turns non-finite is
+// discarded and retried once with a looser tolerance.
 int mixed_solve(const Geom& g, const Coeffs<double>& c64, const Coeffs<float>& c32, const SolverOpts& outer,
                 const SolverOpts& inner, const double* bb, double* phi, MixedWork& w, cudaStream_t s,
                 SolverResult* res, int* inner_iterations) {
   const dim3 gr = grid3(g), bl(BX, BY);
   const long long nb = nblocks3(g);
+  const bool dbg = std::getenv("IMPACT_B200_DEBUG") != nullptr;
   int total_inner = 0;
   int outer_it = 0;
+  int retries = 0;
   double q[4];
   double* qd = raw_results(w.partial64, g);
   res->status = 1;
   for (;;) {
     // r = b - A x  (FP64, the reference operator)
     launch_div_grad<double>(g, c64, phi, w.r64, s);
-    k_outer_residual<<<gr, bl, 0, s>>>(g, bb, w.r64, w.r64, w.r32, w.partial64);
+    k_outer_residual<<<gr, bl, 0, s>>>(g, bb, w.r64, w.r64, w.partial64);
+    prof::count(2);
     finalize(w.partial64, nb, 3, 1, FIN_RAW, nullptr, qd, s);
     cudaError_t e = cudaMemcpyAsync(q, qd, 3 * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return impact_set_error(e, "mixed_solve residual", __FILE__, __LINE__);
     const double rinf = q[0], r2 = sqrt(q[1]), b2 = sqrt(q[2]);
+    if (dbg)
+      std::fprintf(stderr, "[impact_b200] mixed outer %d: |r|inf %.3e |r|2 %.3e |b|2 %.3e inner so far %d\n", outer_it,
+                   rinf, r2, b2, total_inner);
     res->res_inf = rinf;
     res->res_two = r2;
     res->b_two = b2;
@@ -596,23 +561,36 @@ int mixed_solve(const Geom& g, const Coeffs<double>& c64, const Coeffs<float>& c
       res->status = 1;
       break;
     }
-    // inner FP32 solve A e = r from e = 0, to a relative tolerance of the current residual
+    // inner FP32 solve A e = r / |r|_inf from e = 0
     SolverOpts io = inner;
     io.init_yes = 1;
+    if (retries > 0) {
+      io.tol_rel = fmax(io.tol_rel, 0.1);
+      io.max_it = io.max_it < 200 ? io.max_it : 200;
+    }
     if (outer.tol_rel > 0.0 && r2 > 0.0) {
       const double need = outer.tol_rel * b2 / r2;  // reduction still required
       if (need > io.tol_rel) io.tol_rel = fmin(0.5, need * 0.5);
     }
+    k_to_f32<<<gr, bl, 0, s>>>(g, w.r64, 1.0 / rinf, w.r32);
+    prof::count(1);
     SolverResult ir{};
     int rc = bicgstab<float>(g, c32, io, w.r32, w.e32, w.inner, s, &ir);
     if (rc) return rc;
+    if (dbg)
+      std::fprintf(stderr, "[impact_b200]   inner: it %d status %d |r|2/|b|2 %.3e tol %.1e\n", ir.iterations, ir.status,
+                   ir.b_two > 0 ? ir.res_two / ir.b_two : 0.0, io.tol_rel);
     total_inner += ir.iterations;
-    k_apply_correction<<<gr, bl, 0, s>>>(g, w.e32, phi);
-    ++outer_it;
-    if (ir.status == 3) {
-      res->status = 3;
-      break;
+    if (ir.status == 2 || ir.status == 3) {
+      if (++retries > 2) {
+        res->status = ir.status;
+        break;
+      }
+      continue;  // discard this correction, retry with a looser tolerance
     }
+    k_apply_correction<<<gr, bl, 0, s>>>(g, w.e32, rinf, phi);
+    prof::count(1);
+    ++outer_it;
   }
   res->iterations = outer_it;
   if (inner_iterations) *inner_iterations = total_inner;

@@ -2,6 +2,7 @@
 #pragma once
 #include "common.cuh"
 #include "kernels.cuh"
+#include "mg.cuh"
 
 namespace impact {
 
@@ -13,6 +14,8 @@ struct SolverOpts {
   double omega;        // relaxation of the preconditioner sweeps
   int init_yes;        // start from phi = 0
   int check_every;     // read the residual norm back to the host every this many iterations
+  int precond;         // 0: n_sweeps Jacobi sweeps (none if 0); 1: multigrid V-cycle (mg)
+  const void* mg;      // MGData<T>* of the field type when precond == 1
 };
 
 struct SolverResult {

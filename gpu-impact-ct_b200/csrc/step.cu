@@ -13,7 +13,9 @@
 #include <vector>
 
 #include "case.cuh"
+#include "mg_host.h"
 #include "kernels.cuh"
+#include "prof.cuh"
 #include "solver.cuh"
 
 namespace impact {
@@ -396,6 +398,69 @@ extern "C" int impact_b200_case_create(const impact_b200_case_desc* desc, const 
     impact_b200_case_destroy(c);
     return -1;
   }
+  // ---- multigrid hierarchy ----
+  if (co->xp[0] && co->xp[1] && co->xp[2] && co->xu[0] && co->xu[1] && co->xu[2]) {
+    const int N[3] = {desc->N1, desc->N2, desc->N3};
+    std::vector<MGHostLevel> lv = build_mg_hierarchy(N, co->xp, co->xu, co->L, MG_MAX_LEVELS);
+    s.mg_levels = (int)lv.size();
+    // tables of every level in one FP64 and one FP32 allocation
+    size_t tot = 0;
+    for (auto& L : lv)
+      for (int m = 0; m < 3; ++m) tot += L.cdg[m].size() + L.cI[m].size();
+    std::vector<double> t64;
+    t64.reserve(tot);
+    std::vector<size_t> o_cdg(lv.size() * 3), o_cI(lv.size() * 3);
+    for (size_t g = 0; g < lv.size(); ++g)
+      for (int m = 0; m < 3; ++m) {
+        o_cdg[g * 3 + m] = t64.size();
+        t64.insert(t64.end(), lv[g].cdg[m].begin(), lv[g].cdg[m].end());
+        o_cI[g * 3 + m] = t64.size();
+        t64.insert(t64.end(), lv[g].cI[m].begin(), lv[g].cI[m].end());
+      }
+    std::vector<float> t32(t64.begin(), t64.end());
+    double* d64 = nullptr;
+    float* d32 = nullptr;
+    rc |= case_alloc(s, (void**)&d64, t64.size() * sizeof(double));
+    rc |= case_alloc(s, (void**)&d32, t32.size() * sizeof(float));
+    if (rc) {
+      impact_b200_case_destroy(c);
+      return -1;
+    }
+    cudaMemcpy(d64, t64.data(), t64.size() * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(d32, t32.data(), t32.size() * sizeof(float), cudaMemcpyHostToDevice);
+    s.mg64.n = s.mg32.n = s.mg_levels;
+    for (int g = 0; g < s.mg_levels; ++g) {
+      const Geom gg = make_geom(lv[g].M[0], lv[g].M[1], lv[g].M[2]);
+      MGLevel<double>& a = s.mg64.lv[g];
+      MGLevel<float>& b = s.mg32.lv[g];
+      a.g = b.g = gg;
+      for (int m = 0; m < 3; ++m) {
+        a.cdg[m] = d64 + o_cdg[g * 3 + m];
+        a.cI[m] = d64 + o_cI[g * 3 + m];
+        b.cdg[m] = d32 + o_cdg[g * 3 + m];
+        b.cI[m] = d32 + o_cI[g * 3 + m];
+        a.ratio[m] = b.ratio[m] = lv[g].ratio[m];
+      }
+      a.A = a.B = a.C = nullptr;
+      b.A = b.B = b.C = nullptr;
+      if (g == 0) continue;
+      if (s.precision == 0) {
+        for (double** q : {&a.A, &a.B, &a.C}) {
+          rc |= case_alloc(s, (void**)q, (size_t)gg.nfield * sizeof(double));
+          if (!rc) cudaMemsetAsync(*q, 0, (size_t)gg.nfield * sizeof(double), s.stream);
+        }
+      } else {
+        for (float** q : {&b.A, &b.B, &b.C}) {
+          rc |= case_alloc(s, (void**)q, (size_t)gg.nfield * sizeof(float));
+          if (!rc) cudaMemsetAsync(*q, 0, (size_t)gg.nfield * sizeof(float), s.stream);
+        }
+      }
+    }
+    if (rc) {
+      impact_b200_case_destroy(c);
+      return -1;
+    }
+  }
   cudaError_t e = cudaMallocHost((void**)&s.hscal, 64 * sizeof(double));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&s.scal_host, sizeof(SolverScalars));
   if (e != cudaSuccess) {
@@ -465,6 +530,8 @@ extern "C" void* impact_b200_case_stream(impact_b200_case* c) { return c ? (void
 
 static SolverOpts to_opts(const impact_b200_solver_params* p) {
   SolverOpts o{};
+  o.precond = p->precond;
+  o.mg = nullptr;
   o.tol_rel = p->tol_rel;
   o.tol_abs_inf = p->tol_abs_inf;
   o.max_it = p->max_it;
@@ -480,11 +547,24 @@ static int run_poisson(CaseState& s, const double* b, double* x, const impact_b2
   SolverResult res{};
   int inner = 0;
   int rc;
+  if (p->precond == 1 && s.mg_levels == 0)
+    return impact_set_error_msg(-1, "multigrid preconditioner requested but the case was created without coordinates");
+  auto set_mg = [&](auto& mgd) {
+    mgd.n_down = p->mg_down > 0 ? p->mg_down : 4;
+    mgd.n_up = p->mg_up > 0 ? p->mg_up : 4;
+    mgd.n_bottom = p->mg_bottom > 0 ? p->mg_bottom : 4;
+    mgd.omega = p->omega;
+  };
+  set_mg(s.mg64);
+  set_mg(s.mg32);
   if (s.precision == 0) {
-    rc = bicgstab<double>(s.g, s.c64, to_opts(p), b, x, s.kw64, s.stream, &res);
+    SolverOpts o = to_opts(p);
+    if (o.precond == 1) o.mg = &s.mg64;
+    rc = bicgstab<double>(s.g, s.c64, o, b, x, s.kw64, s.stream, &res);
   } else {
     SolverOpts outer = to_opts(p);
     SolverOpts in = to_opts(p);
+    if (in.precond == 1) in.mg = &s.mg32;
     in.tol_rel = p->inner_tol_rel > 0 ? p->inner_tol_rel : 1e-4;
     in.tol_abs_inf = 0.0;
     in.max_it = p->inner_max_it > 0 ? p->inner_max_it : p->max_it * 4;
@@ -515,6 +595,47 @@ extern "C" int impact_b200_case_poisson(impact_b200_case* c, int field_b, int fi
   IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
   int rc = run_poisson(s, s.f[field_b], s.f[field_x], p, r);
   if (rc) return rc;
+  IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
+  IMPACT_CUDA_CHECK(cudaGetLastError());
+  prof::flush();
+  return 0;
+}
+
+extern "C" int impact_b200_case_mg_levels(impact_b200_case* c) { return c ? c->s.mg_levels : 0; }
+
+extern "C" int impact_b200_case_precond(impact_b200_case* c, int field_in, int field_out,
+                                        const impact_b200_solver_params* p) {
+  if (!c || !p || field_in < 0 || field_out < 0 || field_in >= IMPACT_B200_NFIELDS || field_out >= IMPACT_B200_NFIELDS ||
+      field_in == field_out)
+    return impact_set_error_msg(-1, "impact_b200_case_precond: bad arguments");
+  CaseState& s = c->s;
+  if (s.precision != 0) return impact_set_error_msg(-1, "impact_b200_case_precond: FP64 cases only");
+  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  if (p->precond == 1) {
+    if (s.mg_levels == 0) return impact_set_error_msg(-1, "impact_b200_case_precond: case has no multigrid hierarchy");
+    s.mg64.n_down = p->mg_down > 0 ? p->mg_down : 4;
+    s.mg64.n_up = p->mg_up > 0 ? p->mg_up : 4;
+    s.mg64.n_bottom = p->mg_bottom > 0 ? p->mg_bottom : 4;
+    s.mg64.omega = p->omega;
+    mg_vcycle<double>(s.mg64, nullptr, s.f[field_in], s.f[field_out], s.kw64.comp, s.stream);
+  } else {
+    // n_sweeps sweeps from zero (single-level multigridV)
+    if (p->n_sweeps < 1) return impact_set_error_msg(-1, "impact_b200_case_precond: n_sweeps must be >= 1");
+    MGData<double> one{};
+    one.n = 1;
+    one.lv[0] = s.mg_levels ? s.mg64.lv[0] : MGLevel<double>{};
+    if (!s.mg_levels) {
+      one.lv[0].g = s.g;
+      for (int m = 0; m < 3; ++m) one.lv[0].cdg[m] = s.c64.cdg[m];
+    }
+    one.n_down = one.n_up = 0;
+    one.n_bottom = p->n_sweeps;  // relax_bottom runs the init sweep set and a second set
+    one.omega = p->omega;
+    // single level: relax_bottom does n_bottom sweeps from zero then n_bottom more; use half
+    if (p->n_sweeps % 2 != 0) return impact_set_error_msg(-1, "impact_b200_case_precond: use an even n_sweeps");
+    one.n_bottom = p->n_sweeps / 2;
+    mg_vcycle<double>(one, nullptr, s.f[field_in], s.f[field_out], s.kw64.comp, s.stream);
+  }
   IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
   IMPACT_CUDA_CHECK(cudaGetLastError());
   return 0;
@@ -560,6 +681,7 @@ extern "C" int impact_b200_case_step(impact_b200_case* c, const impact_b200_step
   IMPACT_CUDA_CHECK(cudaMemcpyToSymbolAsync(c_stab, stab_host, sizeof(stab_host), 0, cudaMemcpyHostToDevice, s.stream));
   const dim3 gr = grid3(g), bl(BX, BY);
   const long long nb = nblocks(g);
+  const double cells = (double)g.n1 * g.n2 * g.n3;
   double* vel[3] = {s.f[IMPACT_B200_VEL1], s.f[IMPACT_B200_VEL2], s.f[IMPACT_B200_VEL3]};
   double* nl[3] = {s.f[IMPACT_B200_NL1], s.f[IMPACT_B200_NL2], s.f[IMPACT_B200_NL3]};
   double* rhs[3] = {s.f[IMPACT_B200_RHS1], s.f[IMPACT_B200_RHS2], s.f[IMPACT_B200_RHS3]};
@@ -570,6 +692,7 @@ extern "C" int impact_b200_case_step(impact_b200_case* c, const impact_b200_step
     // ---- get_dtime ----
     k_dtime<<<gr, bl, 0, s.stream>>>(g, s.c64, s.dt, p->Re, vel[0], vel[1], vel[2], s.partial);
     k_reduce_partials<<<1, 1024, 0, s.stream>>>(s.partial, nb, 1, s.dscal);
+    prof::count(2);
     IMPACT_CUDA_CHECK(cudaMemcpyAsync(s.hscal, s.dscal, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
     const double beta1 = s.hscal[0];
@@ -584,14 +707,18 @@ extern "C" int impact_b200_case_step(impact_b200_case* c, const impact_b200_step
     // ---- three RK substeps ----
     for (int sub = 0; sub < 3; ++sub) {
       k_interp_vel3<<<gr, bl, 0, s.stream>>>(g, s.c64, vel[0], vel[1], vel[2], s.work[0], s.work[1], s.work[2]);
+      prof::count(1);
       const double mb = dt * bRK[sub], ma = dt * aRK[sub];
       const int use_old = sub != 0;
-      k_nl_rhs<0><<<gr, bl, 0, s.stream>>>(g, s.c64, multL, mb, ma, use_old, vel[0], s.work[0], s.work[1], s.work[2], nl[0], rhs[0]);
-      k_nl_rhs<1><<<gr, bl, 0, s.stream>>>(g, s.c64, multL, mb, ma, use_old, vel[1], s.work[0], s.work[1], s.work[2], nl[1], rhs[1]);
-      k_nl_rhs<2><<<gr, bl, 0, s.stream>>>(g, s.c64, multL, mb, ma, use_old, vel[2], s.work[0], s.work[1], s.work[2], nl[2], rhs[2]);
+      const double nlb = (use_old ? 7.0 : 6.0) * 8.0 * cells;
+      IMPACT_PROF(prof::K_NL_RHS, nlb, s.stream, k_nl_rhs<0><<<gr, bl, 0, s.stream>>>(g, s.c64, multL, mb, ma, use_old, vel[0], s.work[0], s.work[1], s.work[2], nl[0], rhs[0]));
+      IMPACT_PROF(prof::K_NL_RHS, nlb, s.stream, k_nl_rhs<1><<<gr, bl, 0, s.stream>>>(g, s.c64, multL, mb, ma, use_old, vel[1], s.work[0], s.work[1], s.work[2], nl[1], rhs[1]));
+      IMPACT_PROF(prof::K_NL_RHS, nlb, s.stream, k_nl_rhs<2><<<gr, bl, 0, s.stream>>>(g, s.c64, multL, mb, ma, use_old, vel[2], s.work[0], s.work[1], s.work[2], nl[2], rhs[2]));
       const double ab = aRK[sub] + bRK[sub];
       k_scale_pre<<<gr, bl, 0, s.stream>>>(g, ab, dt, 0, pre);
-      launch_divergence2<double>(g, s.c64.cD[0], s.c64.cD[1], s.c64.cD[2], rhs[0], rhs[1], rhs[2], res, s.stream);
+      prof::count(1);
+      IMPACT_PROF(prof::K_DIV2, 4.0 * 8.0 * cells, s.stream,
+                  launch_divergence2<double>(g, s.c64.cD[0], s.c64.cD[1], s.c64.cD[2], rhs[0], rhs[1], rhs[2], res, s.stream));
       impact_b200_solver_result r{};
       int rc = run_poisson(s, res, pre, &p->poisson, &r);
       if (rc) return rc;
@@ -599,20 +726,82 @@ extern "C" int impact_b200_case_step(impact_b200_case* c, const impact_b200_step
       st->inner_iterations[sub] = r.inner_iterations;
       st->poisson_status[sub] = r.status;
       st->poisson_res_rel[sub] = r.b_two > 0.0 ? r.res_two / r.b_two : 0.0;
-      k_project<<<gr, bl, 0, s.stream>>>(g, s.c64, pre, rhs[0], rhs[1], rhs[2], vel[0], vel[1], vel[2]);
+      IMPACT_PROF(prof::K_PROJECT, 7.0 * 8.0 * cells, s.stream,
+                  k_project<<<gr, bl, 0, s.stream>>>(g, s.c64, pre, rhs[0], rhs[1], rhs[2], vel[0], vel[1], vel[2]));
       k_scale_pre<<<gr, bl, 0, s.stream>>>(g, ab, dt, 1, pre);
+      prof::count(1);
     }
     st->timestep += 1;
     st->time += dt;
     const double u_in = p->U0 * (1.0 + 0.5 * std::sin(2.0 * 3.14159265358979323846 * st->time / p->T_pulse));
     k_mask<<<gr, bl, 0, s.stream>>>(g, s.label, u_in, vel[0], vel[1], vel[2]);
+    prof::count(1);
     if (p->level_pressure) {
       k_sum<<<gr, bl, 0, s.stream>>>(g, pre, s.partial);
       k_reduce_partials<<<1, 1024, 0, s.stream>>>(s.partial, nb, 0, s.dscal + 1);
       k_sub_mean<<<gr, bl, 0, s.stream>>>(g, s.dscal + 1, pre);
+      prof::count(3);
     }
   }
   IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
+  IMPACT_CUDA_CHECK(cudaGetLastError());
+  prof::flush();
+  return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// measurement entry: launch one hot kernel `iters` times on the case's resident fields
+// (kid 0 Jacobi sweep, 1 fused init+sweep, 2 A x with one inner product, 3 A x alone,
+//  4 the reference-style one-thread-per-point Jacobi sweep) in the case's precision;
+// returns the average milliseconds per launch (CUDA events on the case stream).
+// ---------------------------------------------------------------------------------------
+#include "stencil25d.cuh"
+extern "C" int impact_b200_case_kernel_bench(impact_b200_case* c, int kid, int iters, double* ms_per_launch) {
+  if (!c || iters < 1 || !ms_per_launch) return impact_set_error_msg(-1, "impact_b200_case_kernel_bench: bad arguments");
+  CaseState& s = c->s;
+  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  const Geom& g = s.g;
+  cudaEvent_t a, b;
+  IMPACT_CUDA_CHECK(cudaEventCreate(&a));
+  IMPACT_CUDA_CHECK(cudaEventCreate(&b));
+  auto launch = [&]() -> int {
+    if (s.precision == 0) {
+      double* x = s.f[IMPACT_B200_PRE];
+      double* bb = s.f[IMPACT_B200_RES];
+      double* o = s.f[IMPACT_B200_RHS1];
+      switch (kid) {
+        case 0: launch_jacobi25<double, 0>(g, s.c64, nullptr, 0.8, bb, x, o, s.stream); break;
+        case 1: launch_jacobi25<double, 1>(g, s.c64, nullptr, 0.8, bb, nullptr, o, s.stream); break;
+        case 2: launch_divgrad25<double, 1>(g, s.c64, nullptr, x, o, bb, s.partial, s.stream); break;
+        case 3: launch_divgrad25<double, 0>(g, s.c64, nullptr, x, o, nullptr, nullptr, s.stream); break;
+        case 4: launch_jacobi<double>(g, s.c64.cdg[0], s.c64.cdg[1], s.c64.cdg[2], 0.8, bb, x, o, s.stream); break;
+        default: return -1;
+      }
+    } else {
+      float* x = s.mw.inner.z1;
+      float* bb = s.mw.inner.rr;
+      float* o = s.mw.inner.z2;
+      switch (kid) {
+        case 0: launch_jacobi25<float, 0>(g, s.c32, nullptr, 0.8f, bb, x, o, s.stream); break;
+        case 1: launch_jacobi25<float, 1>(g, s.c32, nullptr, 0.8f, bb, nullptr, o, s.stream); break;
+        case 2: launch_divgrad25<float, 1>(g, s.c32, nullptr, x, o, bb, s.partial, s.stream); break;
+        case 3: launch_divgrad25<float, 0>(g, s.c32, nullptr, x, o, nullptr, nullptr, s.stream); break;
+        case 4: launch_jacobi<float>(g, s.c32.cdg[0], s.c32.cdg[1], s.c32.cdg[2], 0.8f, bb, x, o, s.stream); break;
+        default: return -1;
+      }
+    }
+    return 0;
+  };
+  if (launch()) return impact_set_error_msg(-1, "impact_b200_case_kernel_bench: unknown kernel id");
+  cudaEventRecord(a, s.stream);
+  for (int t = 0; t < iters; ++t) launch();
+  cudaEventRecord(b, s.stream);
+  IMPACT_CUDA_CHECK(cudaEventSynchronize(b));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  *ms_per_launch = ms / iters;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
   IMPACT_CUDA_CHECK(cudaGetLastError());
   return 0;
 }

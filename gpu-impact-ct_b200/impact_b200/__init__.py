@@ -39,7 +39,7 @@ class AxisTables(C.Structure):
 
 
 class Coeffs(C.Structure):
-    _fields_ = [("axis", C.POINTER(AxisTables) * 3)]
+    _fields_ = [("axis", C.POINTER(AxisTables) * 3), ("xp", _dp * 3), ("xu", _dp * 3), ("L", C.c_double * 3)]
 
 
 class CaseDesc(C.Structure):
@@ -50,7 +50,8 @@ class CaseDesc(C.Structure):
 class SolverParams(C.Structure):
     _fields_ = [("tol_rel", C.c_double), ("tol_abs_inf", C.c_double), ("max_it", C.c_int),
                 ("n_sweeps", C.c_int), ("omega", C.c_double), ("init_yes", C.c_int),
-                ("check_every", C.c_int), ("inner_tol_rel", C.c_double), ("inner_max_it", C.c_int)]
+                ("check_every", C.c_int), ("inner_tol_rel", C.c_double), ("inner_max_it", C.c_int),
+                ("precond", C.c_int), ("mg_down", C.c_int), ("mg_up", C.c_int), ("mg_bottom", C.c_int)]
 
 
 class SolverResult(C.Structure):
@@ -103,8 +104,15 @@ def lib():
         "impact_b200_case_stream": (_vp, [_vp]),
         "impact_b200_case_poisson": (i, [_vp, i, i, P(SolverParams), P(SolverResult)]),
         "impact_b200_case_step": (i, [_vp, P(StepParams), P(StepState), i]),
+        "impact_b200_case_precond": (i, [_vp, i, i, P(SolverParams)]),
+        "impact_b200_case_mg_levels": (i, [_vp]),
         "impact_b200_jacobi_solve": (i, [i, i, i, i, i, i, d, _dp, _dp, _dp, _dp, _dp, i, d, i, _ip, _dp]),
         "impact_b200_product_scalar": (i, [i, i, i, _vp, _vp, _dp]),
+        "impact_b200_profile_enable": (None, [i]),
+        "impact_b200_profile_reset": (None, []),
+        "impact_b200_profile_read": (i, [i, P(C.c_longlong), _dp, _dp, P(C.c_char_p)]),
+        "impact_b200_launch_count": (C.c_longlong, []),
+        "impact_b200_case_kernel_bench": (i, [_vp, i, i, _dp]),
         # reference launcher FFI (every argument by reference)
         "gradient_launcher_": (None, [_ip] * 6 + [_PP] * 3),
         "divergence_launcher_": (None, [_ip] * 6 + [_PP] * 3),
@@ -179,6 +187,9 @@ class Grid:
         self.coeffs = Coeffs()
         for a in range(3):
             self.coeffs.axis[a] = C.pointer(self._axis[a])
+            self.coeffs.xp[a] = _ptr(self.xp[a])
+            self.coeffs.xu[a] = _ptr(self.xu[a])
+            self.coeffs.L[a] = self.L[a]
 
     @property
     def shape(self):
@@ -198,9 +209,11 @@ class Grid:
 
 
 def solver_params(tol_rel=1e-8, tol_abs_inf=0.0, max_it=2000, n_sweeps=4, omega=0.8, init_yes=0,
-                  check_every=4, inner_tol_rel=1e-4, inner_max_it=0) -> SolverParams:
+                  check_every=4, inner_tol_rel=1e-4, inner_max_it=0, precond=0, mg_down=4, mg_up=4,
+                  mg_bottom=4) -> SolverParams:
+    """precond 0: n_sweeps damped-Jacobi sweeps; 1: multigrid V-cycle (mg_down/up/bottom sweeps)."""
     return SolverParams(tol_rel, tol_abs_inf, max_it, n_sweeps, omega, init_yes, check_every,
-                        inner_tol_rel, inner_max_it)
+                        inner_tol_rel, inner_max_it, precond, mg_down, mg_up, mg_bottom)
 
 
 def step_params(Re=200.0, CFL=0.2, dtime_max=1e-2, dtime0=1e9, U0=1.0, T_pulse=1.0, level_pressure=1,
@@ -265,9 +278,50 @@ class Case:
         check(lib().impact_b200_case_poisson(self._h, bi, xi, C.byref(params), C.byref(r)), "case_poisson")
         return r
 
+    @property
+    def mg_levels(self) -> int:
+        return lib().impact_b200_case_mg_levels(self._h)
+
+    def precond(self, field_in="res", field_out="pre", params: SolverParams | None = None):
+        """field_out = M field_in with the preconditioner of params (FP64 cases)."""
+        params = solver_params() if params is None else params
+        fi = FIELDS[field_in] if isinstance(field_in, str) else field_in
+        fo = FIELDS[field_out] if isinstance(field_out, str) else field_out
+        check(lib().impact_b200_case_precond(self._h, fi, fo, C.byref(params)), "case_precond")
+
+    def kernel_bench(self, kid: int, iters: int = 10) -> float:
+        """average ms of one hot kernel launched iters times on the resident fields"""
+        ms = C.c_double()
+        check(lib().impact_b200_case_kernel_bench(self._h, kid, iters, C.byref(ms)), "kernel_bench")
+        return ms.value
+
     def step(self, params: StepParams, nsteps: int = 1) -> StepState:
         check(lib().impact_b200_case_step(self._h, C.byref(params), C.byref(self.state), nsteps), "case_step")
         return self.state
+
+
+PROFILE_KERNELS = 9
+
+
+def profile(enable: bool = True, reset: bool = True):
+    """Turn the library's per-kernel CUDA-event timing on or off."""
+    if reset:
+        lib().impact_b200_profile_reset()
+    lib().impact_b200_profile_enable(int(enable))
+
+
+def profile_read():
+    """{kernel name: (launches, total ms, algorithmic bytes)} of the profiled kernels."""
+    out = {}
+    for k in range(PROFILE_KERNELS):
+        n, ms, by, nm = C.c_longlong(), C.c_double(), C.c_double(), C.c_char_p()
+        check(lib().impact_b200_profile_read(k, C.byref(n), C.byref(ms), C.byref(by), C.byref(nm)), "profile_read")
+        out[nm.value.decode()] = (n.value, ms.value, by.value)
+    return out
+
+
+def launch_count() -> int:
+    return int(lib().impact_b200_launch_count())
 
 
 def fd_exact(abl, n, deltaX0):

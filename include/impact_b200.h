@@ -134,6 +134,11 @@ typedef struct {
 
 typedef struct {
   const impact_b200_axis_tables* axis[3]; /* host tables of the three axes (copied to the GPU) */
+  /* optional: the grid coordinates x1p/x1u.. over -3..N+3 and the box lengths; when given, the
+   * case also builds the multigrid hierarchy of the pressure Poisson preconditioner */
+  const double* xp[3];
+  const double* xu[3];
+  double L[3];
 } impact_b200_coeffs;
 
 /* field ids of impact_b200_case_upload/download/field_ptr */
@@ -166,6 +171,9 @@ typedef struct {
   int check_every;     /* iterations between host polls of the device convergence flag */
   double inner_tol_rel;/* mixed precision: relative tolerance of each FP32 inner solve */
   int inner_max_it;    /* mixed precision: iteration cap of each inner solve */
+  int precond;         /* 0: n_sweeps damped-Jacobi sweeps; 1: multigrid V-cycle (multigridV,
+                          mod_solvers.f90:456-585; needs the coordinates at case creation) */
+  int mg_down, mg_up, mg_bottom; /* V-cycle sweeps (n_relax_down / _up / _bottom), relaxation omega */
 } impact_b200_solver_params;
 
 typedef struct {
@@ -179,6 +187,11 @@ typedef struct {
  * A = product_div_grad, preconditioner = Jacobi sweeps of the compact cdg Laplacian). */
 int impact_b200_case_poisson(impact_b200_case* c, int field_b, int field_x, const impact_b200_solver_params* p,
                              impact_b200_solver_result* r);
+
+/* Apply the preconditioner of p once: field_out = M field_in (FP64 cases). */
+int impact_b200_case_precond(impact_b200_case* c, int field_in, int field_out, const impact_b200_solver_params* p);
+/* levels of the multigrid hierarchy of the case (0 when it has none) */
+int impact_b200_case_mg_levels(impact_b200_case* c);
 
 typedef struct {
   double Re, CFL, dtime_max, dtime0; /* get_dtime (mod_lib.f90:46-250), timeint_mode 1 */
@@ -214,6 +227,21 @@ int impact_b200_jacobi_solve(int N1, int N2, int N3, int M1, int M2, int M3, dou
  * mod_solvers.f90:2319-2354) of two device fields of a grid with N1 x N2 x N3 points.
  * Uses a per-call scratch allocation for the block partials. */
 int impact_b200_product_scalar(int N1, int N2, int N3, const double* a_dev, const double* b_dev, double* result);
+
+/* ---- measurement hooks -----------------------------------------------------------------
+ * When enabled, the library records CUDA events on the launching stream around its hot kernels
+ * and accumulates, per kernel kind kid (0 jacobi_sweep, 1 jacobi_init2, 2 div_grad_dot,
+ * 3 x_update, 4 p_update, 5 r_update, 6 nl_rhs, 7 project, 8 divergence2), the launches, the
+ * elapsed milliseconds and the algorithmic bytes moved.  launch_count counts every kernel
+ * launch the library has issued since load. */
+void impact_b200_profile_enable(int enable);
+void impact_b200_profile_reset(void);
+int impact_b200_profile_read(int kid, long long* launches, double* total_ms, double* total_bytes, const char** name);
+long long impact_b200_launch_count(void);
+/* launch one hot kernel iters times on the case's resident fields (kid 0 Jacobi sweep, 1 fused
+ * init + sweep, 2 A x with a fused inner product, 3 A x, 4 one-thread-per-point Jacobi sweep), in
+ * the case's precision; *ms_per_launch = average device time (CUDA events on the case stream) */
+int impact_b200_case_kernel_bench(impact_b200_case* c, int kid, int iters, double* ms_per_launch);
 
 #ifdef __cplusplus
 }

@@ -592,10 +592,16 @@ static void copy_interior(const dims_t* d, const double* src, double* dst) {
       for (int i = 1; i <= d->N1 - 1; i++) dst[IX(d, i, j, k)] = src[IX(d, i, j, k)];
 }
 
-static void precond(int N1, int N2, int N3, const orc_coeffs* c, const orc_solver_opts* o, double* v,
-                    double* z, double* comp) {
+typedef void (*precond_fn)(const void* ctx, double* v, double* z, double* comp);
+typedef struct {
+  int N1, N2, N3;
+  const orc_coeffs* c;
+  const orc_solver_opts* o;
+} jac_ctx;
+static void precond_jacobi(const void* ctx, double* v, double* z, double* comp) {
   /* single-level multigridV (mod_solvers.f90:456-585 with n_grids = 1): Jacobi sweeps from zero */
-  orc_jacobi(N1, N2, N3, c, 1, o->n_sweeps, o->omega, v, z, comp);
+  const jac_ctx* j = (const jac_ctx*)ctx;
+  orc_jacobi(j->N1, j->N2, j->N3, j->c, 1, j->o->n_sweeps, j->o->omega, v, z, comp);
 }
 
 static int converged(const orc_solver_opts* o, double ninf, double n2sq, double b2) {
@@ -604,8 +610,9 @@ static int converged(const orc_solver_opts* o, double ninf, double n2sq, double 
   return 0;
 }
 
-void orc_bicgstab(int N1, int N2, int N3, const orc_coeffs* c, const orc_solver_opts* o,
-                  double* bb, double* phi, double* work, orc_solver_result* res) {
+static void bicgstab_impl(int N1, int N2, int N3, const orc_coeffs* c, const orc_solver_opts* o,
+                          precond_fn pfn, const void* pctx, double* bb, double* phi, double* work,
+                          orc_solver_result* res) {
   dims_t d = mkdims(N1, N2, N3);
   const size_t fs = field_size(&d);
   double* rr = work + 0 * fs;
@@ -617,7 +624,7 @@ void orc_bicgstab(int N1, int N2, int N3, const orc_coeffs* c, const orc_solver_
   double* z2 = work + 6 * fs;
   double* comp = work + 7 * fs;
   double* dig = work + 8 * fs;
-  const int pre_on = o->n_sweeps > 0;
+  const int pre_on = pfn != NULL;
   const int init_yes = o->init_yes;
   double norm_inf = 0.0, norm2 = 0.0, b2sq = 0.0, dummy;
   double rhr = 0.0, rhr_prev, alpha = 0.0, omega = 0.0, beta, rhAp, rAr, ArAr;
@@ -685,7 +692,7 @@ void orc_bicgstab(int N1, int N2, int N3, const orc_coeffs* c, const orc_solver_
       copy_interior(&d, (init_yes && counter == 1) ? bb : rr, pp);
     }
     if (pre_on) {
-      precond(N1, N2, N3, c, o, pp, z1, comp);
+      pfn(pctx, pp, z1, comp);
       orc_product_div_grad(N1, N2, N3, c, z1, dig, Ap);
     } else {
       orc_product_div_grad(N1, N2, N3, c, pp, dig, Ap);
@@ -707,7 +714,7 @@ void orc_bicgstab(int N1, int N2, int N3, const orc_coeffs* c, const orc_solver_
           }
     }
     if (pre_on) {
-      precond(N1, N2, N3, c, o, rr, z2, comp);
+      pfn(pctx, rr, z2, comp);
       orc_product_div_grad(N1, N2, N3, c, z2, dig, Ar);
     } else {
       orc_product_div_grad(N1, N2, N3, c, rr, dig, Ar);
@@ -739,6 +746,231 @@ void orc_bicgstab(int N1, int N2, int N3, const orc_coeffs* c, const orc_solver_
   res->res_inf = norm_inf;
   res->res_two = sqrt(norm2);
   res->b_two = b2;
+}
+
+static void precond_mg(const void* ctx, double* v, double* z, double* comp);
+typedef struct {
+  const orc_mg* mg;
+  int n_down, n_up, n_bottom;
+  double omega;
+} mg_ctx;
+
+void orc_bicgstab(int N1, int N2, int N3, const orc_coeffs* c, const orc_solver_opts* o,
+                  double* bb, double* phi, double* work, orc_solver_result* res) {
+  if (o->precond == 1 && o->mg != NULL) {
+    mg_ctx m = {o->mg, o->mg_down, o->mg_up, o->mg_bottom, o->omega};
+    bicgstab_impl(N1, N2, N3, c, o, precond_mg, &m, bb, phi, work, res);
+    return;
+  }
+  jac_ctx j = {N1, N2, N3, c, o};
+  bicgstab_impl(N1, N2, N3, c, o, o->n_sweeps > 0 ? precond_jacobi : NULL, &j, bb, phi, work, res);
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* geometric multigrid, periodic (mod_setup.f90:95-143 level sizes, mod_geometry.f90:66-103 */
+/* level coordinates, get_stencil per level, interp_coeffs mod_coeffs.f90:1683-1746,     */
+/* restr_coeffs :1879-2100 (constant 1/4 1/2 1/4 for periodic axes), multigridV /       */
+/* restrict / interpolate mod_solvers.f90:353-1150)                                       */
+/* ------------------------------------------------------------------------------------ */
+static void jacobi_cdg(int N1, int N2, int N3, const double* const* cdg, int init_yes, int n_relax,
+                       double omega, const double* bb, double* rel, double* comp) {
+  orc_coeffs c;
+  memset(&c, 0, sizeof(c));
+  for (int a = 0; a < 3; a++) c.cdg[a] = cdg[a];
+  orc_jacobi(N1, N2, N3, &c, init_yes, n_relax, omega, bb, rel, comp);
+}
+static void dg_relax_cdg(int N1, int N2, int N3, const double* const* cdg, double* phi, double* lap) {
+  orc_coeffs c;
+  memset(&c, 0, sizeof(c));
+  for (int a = 0; a < 3; a++) c.cdg[a] = cdg[a];
+  orc_product_dg_relax(N1, N2, N3, &c, phi, lap);
+}
+
+int orc_mg_build(int N1, int N2, int N3, const double* const* xp, const double* const* xu, const double* L,
+                 int n_grids_limit, orc_mg* mg) {
+  memset(mg, 0, sizeof(*mg));
+  int MM[ORC_MG_MAX][3];
+  MM[0][0] = N1;
+  MM[0][1] = N2;
+  MM[0][2] = N3;
+  int ng = 1;
+  for (int g = 1; g < ORC_MG_MAX; g++)
+    for (int m = 0; m < 3; m++) {
+      if ((MM[g - 1][m] - 1) % 2 == 0 && MM[g - 1][m] >= 5) {
+        MM[g][m] = (MM[g - 1][m] - 1) / 2 + 1;
+        ng = g + 1;
+      } else {
+        MM[g][m] = MM[g - 1][m];
+      }
+    }
+  if (ng > n_grids_limit) ng = n_grids_limit;
+  if (ng < 1) ng = 1;
+  mg->n_grids = ng;
+  for (int g = 0; g < ng; g++)
+    for (int m = 0; m < 3; m++) {
+      const int M = MM[g][m];
+      mg->M[g][m] = M;
+      mg->ratio[g][m] = (g + 1 < ng) ? (MM[g][m] - 1) / (MM[g + 1][m] - 1) : 1;
+      double* p = (double*)calloc((size_t)M + 7, sizeof(double));
+      double* u = (double*)calloc((size_t)M + 7, sizeof(double));
+      const double* y1p = xp[m]; /* finest, offset 3 */
+      if (g == 0) {
+        memcpy(p, xp[m], sizeof(double) * (size_t)(M + 7));
+        memcpy(u, xu[m], sizeof(double) * (size_t)(M + 7));
+      } else {
+        const int di = (MM[0][m] - 1) / (M - 1);
+        for (int i = 1; i <= M; i++) p[i + 3] = y1p[1 + di * i - di + 3];
+        for (int i = 1; i <= M - 1; i++) u[i + 3] = y1p[1 + di * i - di / 2 + 3];
+        for (int i = -3; i <= 0; i++) {
+          p[i + 3] = p[(M - 1 + i) + 3] - L[m];
+          u[i + 3] = u[(M - 1 + i) + 3] - L[m];
+        }
+        for (int i = M; i <= M + 3; i++) {
+          p[i + 3] = p[(i - M + 1) + 3] + L[m];
+          u[i + 3] = u[(i - M + 1) + 3] + L[m];
+        }
+      }
+      mg->xp[g][m] = p;
+      mg->xu[g][m] = u;
+      double* cdg = (double*)calloc((size_t)3 * M, sizeof(double));
+      orc_get_stencil(M, p, u, cdg);
+      mg->cdg[g][m] = cdg;
+      double* ci = (double*)calloc((size_t)2 * (M + 1), sizeof(double));
+      if (g + 1 < ng) {
+        const int di = (MM[0][m] - 1) / (M - 1);
+        for (int i = 2; i <= M - 1; i += 2) {
+          const int i0 = 1 + (i - 1) * di;
+          const double Dx10 = y1p[i0 + 3] - y1p[i0 - di + 3];
+          const double Dx12 = y1p[i0 + di + 3] - y1p[i0 - di + 3];
+          ci[2 * i + 0] = 1. - Dx10 / Dx12;
+          ci[2 * i + 1] = Dx10 / Dx12;
+        }
+      }
+      mg->cI[g][m] = ci;
+    }
+  for (int g = 1; g < ng; g++) {
+    const size_t fs = (size_t)(mg->M[g][0] + 7) * (size_t)(mg->M[g][1] + 7) * (size_t)(mg->M[g][2] + 7);
+    for (int q = 0; q < 3; q++) mg->f[g][q] = (double*)calloc(fs, sizeof(double));
+  }
+  return 0;
+}
+
+void orc_mg_free(orc_mg* mg) {
+  for (int g = 0; g < ORC_MG_MAX; g++)
+    for (int m = 0; m < 3; m++) {
+      free(mg->xp[g][m]);
+      free(mg->xu[g][m]);
+      free(mg->cdg[g][m]);
+      free(mg->cI[g][m]);
+      free(mg->f[g][m]);
+    }
+  memset(mg, 0, sizeof(*mg));
+}
+
+/* restrict(.TRUE., g, coarse, fine1, fine2): coarse = R (fine1 - fine2), cR = 1/4, 1/2, 1/4 */
+static void mg_restrict(const orc_mg* mg, int g, const double* fine1, const double* fine2, double* coarse) {
+  const int* Mf = mg->M[g];
+  const int* Mc = mg->M[g + 1];
+  dims_t df = mkdims(Mf[0], Mf[1], Mf[2]);
+  dims_t dc = mkdims(Mc[0], Mc[1], Mc[2]);
+  const int r1 = mg->ratio[g][0], r2 = mg->ratio[g][1], r3 = mg->ratio[g][2];
+  const int n1 = Mf[0] - 1, n2 = Mf[1] - 1, n3 = Mf[2] - 1;
+  const double cm = 1. / 4., c0 = 2. / 4., cp = 1. / 4.;
+#define WR(q, n) ((q) < 1 ? (q) + (n) : ((q) > (n) ? (q) - (n) : (q)))
+#define DF(i, j, k) (fine1[IX(&df, WR(i, n1), WR(j, n2), WR(k, n3))] - fine2[IX(&df, WR(i, n1), WR(j, n2), WR(k, n3))])
+#pragma omp parallel for schedule(static)
+  for (int kk = 1; kk <= Mc[2] - 1; kk++)
+    for (int jj = 1; jj <= Mc[1] - 1; jj++)
+      for (int ii = 1; ii <= Mc[0] - 1; ii++) {
+        const int i = r1 * (ii - 1) + 1, j = r2 * (jj - 1) + 1, k = r3 * (kk - 1) + 1;
+        coarse[IX(&dc, ii, jj, kk)] = ((c0 + c0 + c0) * DF(i, j, k) + cm * DF(i - 1, j, k) + cp * DF(i + 1, j, k) +
+                                       cm * DF(i, j - 1, k) + cp * DF(i, j + 1, k) + cm * DF(i, j, k - 1) +
+                                       cp * DF(i, j, k + 1)) /
+                                      3.;
+      }
+#undef DF
+}
+
+/* interpolate(.TRUE., g, coarse, fine, work): fine += P coarse (z, then y, then x passes) */
+static void mg_interpolate_add(const orc_mg* mg, int g, double* coarse, double* fine, double* work) {
+  const int* Mf = mg->M[g];
+  const int* Mc = mg->M[g + 1];
+  dims_t df = mkdims(Mf[0], Mf[1], Mf[2]);
+  dims_t dc = mkdims(Mc[0], Mc[1], Mc[2]);
+  const int di = mg->ratio[g][0], dj = mg->ratio[g][1], dk = mg->ratio[g][2];
+  const int imax = Mf[0], jmax = Mf[1], kmax = Mf[2];
+  exchange_all(Mc[0], Mc[1], Mc[2], coarse); /* exchange_relax: coarse(Mc) = coarse(1) */
+  for (int kk = 1; kk <= Mc[2]; kk++)
+    for (int jj = 1; jj <= Mc[1]; jj++)
+      for (int ii = 1; ii <= Mc[0]; ii++)
+        work[IX(&df, di * (ii - 1) + 1, dj * (jj - 1) + 1, dk * (kk - 1) + 1)] = coarse[IX(&dc, ii, jj, kk)];
+  const double* c1 = mg->cI[g][0];
+  const double* c2 = mg->cI[g][1];
+  const double* c3 = mg->cI[g][2];
+  if (dk != 1)
+    for (int k = 2; k <= kmax - 1; k += dk)
+      for (int j = 1; j <= jmax; j += dj)
+        for (int i = 1; i <= imax; i += di)
+          work[IX(&df, i, j, k)] = c3[2 * k] * work[IX(&df, i, j, k - 1)] + c3[2 * k + 1] * work[IX(&df, i, j, k + 1)];
+  if (dj != 1)
+    for (int k = 1; k <= kmax; k++)
+      for (int j = 2; j <= jmax - 1; j += dj)
+        for (int i = 1; i <= imax; i += di)
+          work[IX(&df, i, j, k)] = c2[2 * j] * work[IX(&df, i, j - 1, k)] + c2[2 * j + 1] * work[IX(&df, i, j + 1, k)];
+  if (di != 1)
+    for (int k = 1; k <= kmax; k++)
+      for (int j = 1; j <= jmax; j++)
+        for (int i = 2; i <= imax - 1; i += di)
+          work[IX(&df, i, j, k)] = c1[2 * i] * work[IX(&df, i - 1, j, k)] + c1[2 * i + 1] * work[IX(&df, i + 1, j, k)];
+  for (int k = 1; k <= kmax - 1; k++)
+    for (int j = 1; j <= jmax - 1; j++)
+      for (int i = 1; i <= imax - 1; i++) fine[IX(&df, i, j, k)] = fine[IX(&df, i, j, k)] + work[IX(&df, i, j, k)];
+}
+
+void orc_mg_vcycle(const orc_mg* mg, int n_down, int n_up, int n_bottom, double omega, double* bb, double* phi,
+                   double* work) {
+  const int ng = mg->n_grids;
+  double* A[ORC_MG_MAX];
+  double* B[ORC_MG_MAX];
+  double* Cw[ORC_MG_MAX];
+  A[0] = bb;
+  B[0] = phi;
+  Cw[0] = work;
+  for (int g = 1; g < ng; g++) {
+    A[g] = mg->f[g][0];
+    B[g] = mg->f[g][1];
+    Cw[g] = mg->f[g][2];
+  }
+  for (int g = 0; g < ng - 1; g++) { /* relax_restrict */
+    const int* M = mg->M[g];
+    jacobi_cdg(M[0], M[1], M[2], (const double* const*)mg->cdg[g], 1, n_down, omega, A[g], B[g], Cw[g]);
+    dg_relax_cdg(M[0], M[1], M[2], (const double* const*)mg->cdg[g], B[g], Cw[g]);
+    mg_restrict(mg, g, A[g], Cw[g], A[g + 1]);
+  }
+  { /* relax_bottom */
+    const int* M = mg->M[ng - 1];
+    jacobi_cdg(M[0], M[1], M[2], (const double* const*)mg->cdg[ng - 1], 1, n_bottom, omega, A[ng - 1], B[ng - 1],
+               Cw[ng - 1]);
+    jacobi_cdg(M[0], M[1], M[2], (const double* const*)mg->cdg[ng - 1], 0, n_bottom, omega, A[ng - 1], B[ng - 1],
+               Cw[ng - 1]);
+  }
+  for (int g = ng - 2; g >= 0; g--) { /* interpolate_relax */
+    const int* M = mg->M[g];
+    mg_interpolate_add(mg, g, B[g + 1], B[g], Cw[g]);
+    jacobi_cdg(M[0], M[1], M[2], (const double* const*)mg->cdg[g], 0, n_up, omega, A[g], B[g], Cw[g]);
+  }
+}
+
+static void precond_mg(const void* ctx, double* v, double* z, double* comp) {
+  const mg_ctx* m = (const mg_ctx*)ctx;
+  orc_mg_vcycle(m->mg, m->n_down, m->n_up, m->n_bottom, m->omega, v, z, comp);
+}
+
+void orc_bicgstab_mg(int N1, int N2, int N3, const orc_coeffs* c, const orc_mg* mg, const orc_solver_opts* o,
+                     int n_down, int n_up, int n_bottom, double* bb, double* phi, double* work,
+                     orc_solver_result* res) {
+  mg_ctx m = {mg, n_down, n_up, n_bottom, o->omega};
+  bicgstab_impl(N1, N2, N3, c, o, precond_mg, &m, bb, phi, work, res);
 }
 
 /* ------------------------------------------------------------------------------------ */

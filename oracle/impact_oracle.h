@@ -131,6 +131,9 @@ typedef struct {
   int n_sweeps;       /* Jacobi sweeps per preconditioner application (0 = none) */
   double omega;       /* Jacobi/JOR relaxation of the preconditioner */
   int init_yes;       /* 1: start from phi = 0 as BiCGstab_orig with init_yes */
+  int precond;        /* 0: n_sweeps Jacobi sweeps; 1: multigrid V-cycle (mg) */
+  const struct orc_mg_s* mg;
+  int mg_down, mg_up, mg_bottom;
 } orc_solver_opts;
 
 typedef struct {
@@ -181,6 +184,35 @@ double orc_get_dtime(int N1, int N2, int N3, const orc_coeffs* c, const double* 
 void orc_mask_forcing(int N1, int N2, int N3, const uint8_t* label, double u_inflow, double* vel);
 /* level_pressure (mod_lib.f90:507-537). */
 void orc_level_pressure(int N1, int N2, int N3, double* pre);
+
+
+/* ---------------- geometric multigrid (mod_solvers.f90:353-1150, mod_setup.f90:95-143,
+ * mod_geometry.f90:66-103, mod_coeffs.f90:1048-1259 and 1683-2100), periodic ---------------- */
+#define ORC_MG_MAX 15
+typedef struct orc_mg_s {
+  int n_grids;
+  int M[ORC_MG_MAX][3];     /* points per axis (NN) of every level */
+  int ratio[ORC_MG_MAX][3]; /* coarsening factor from level g to g+1 (2 or 1) */
+  double* xp[ORC_MG_MAX][3]; /* level coordinates over -3..M+3 */
+  double* xu[ORC_MG_MAX][3];
+  double* cdg[ORC_MG_MAX][3]; /* compact Laplacian cdg(-1:1,1:M) of the level */
+  double* cI[ORC_MG_MAX][3];  /* interpolation weights cI(1:2, 0:M) of the level (even points) */
+  double* f[ORC_MG_MAX][3];   /* level fields: bb, phi, work (padded, level 1 unused) */
+} orc_mg;
+
+/* Build the hierarchy of a periodic grid from its finest global coordinates (xp/xu over
+ * -3..N+3 per axis) and box lengths; n_grids_limit caps the number of levels. */
+int orc_mg_build(int N1, int N2, int N3, const double* const* xp, const double* const* xu, const double* L,
+                 int n_grids_limit, orc_mg* mg);
+void orc_mg_free(orc_mg* mg);
+/* multigridV(init_yes = .TRUE., gstart = 1, bb, phi) with damped-Jacobi smoothing
+ * (n_down / n_up / n_bottom sweeps, relaxation omega); work: one padded level-1 field. */
+void orc_mg_vcycle(const orc_mg* mg, int n_down, int n_up, int n_bottom, double omega, double* bb, double* phi,
+                   double* work);
+/* BiCGstab_orig with the multigrid V-cycle preconditioner (precond_Poisson = 1). */
+void orc_bicgstab_mg(int N1, int N2, int N3, const orc_coeffs* c, const orc_mg* mg, const orc_solver_opts* o,
+                     int n_down, int n_up, int n_bottom, double* bb, double* phi, double* work,
+                     orc_solver_result* res);
 
 #ifdef __cplusplus
 }

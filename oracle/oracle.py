@@ -30,12 +30,22 @@ class OrcCoeffs(C.Structure):
 
 class OrcSolverOpts(C.Structure):
     _fields_ = [("tol_rel", C.c_double), ("tol_abs_inf", C.c_double), ("max_it", C.c_int),
-                ("n_sweeps", C.c_int), ("omega", C.c_double), ("init_yes", C.c_int)]
+                ("n_sweeps", C.c_int), ("omega", C.c_double), ("init_yes", C.c_int), ("precond", C.c_int),
+                ("mg", C.c_void_p), ("mg_down", C.c_int), ("mg_up", C.c_int), ("mg_bottom", C.c_int)]
 
 
 class OrcSolverResult(C.Structure):
     _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("res_inf", C.c_double),
                 ("res_two", C.c_double), ("b_two", C.c_double)]
+
+
+MG_MAX = 15
+
+
+class OrcMG(C.Structure):
+    _fields_ = [("n_grids", C.c_int), ("M", (C.c_int * 3) * MG_MAX), ("ratio", (C.c_int * 3) * MG_MAX),
+                ("xp", (_dp * 3) * MG_MAX), ("xu", (_dp * 3) * MG_MAX), ("cdg", (_dp * 3) * MG_MAX),
+                ("cI", (_dp * 3) * MG_MAX), ("f", (_dp * 3) * MG_MAX)]
 
 
 class OrcStepParams(C.Structure):
@@ -88,6 +98,11 @@ def lib():
             "orc_bicgstab": (None, [i, i, i, P(OrcCoeffs), P(OrcSolverOpts), _dp, _dp, _dp,
                                     P(OrcSolverResult)]),
             "orc_get_dtime": (d, [i, i, i, P(OrcCoeffs), _dp, d, d, d, _dp, _dp]),
+            "orc_mg_build": (i, [i, i, i, P(_dp), P(_dp), _dp, i, P(OrcMG)]),
+            "orc_mg_free": (None, [P(OrcMG)]),
+            "orc_mg_vcycle": (None, [P(OrcMG), i, i, i, d, _dp, _dp, _dp]),
+            "orc_bicgstab_mg": (None, [i, i, i, P(OrcCoeffs), P(OrcMG), P(OrcSolverOpts), i, i, i, _dp, _dp, _dp,
+                                       P(OrcSolverResult)]),
             "orc_mask_forcing": (None, [i, i, i, _u8p, d, _dp]),
             "orc_level_pressure": (None, [i, i, i, _dp]),
             "orc_time_step": (None, [i, i, i, P(OrcCoeffs), P(OrcStepParams), _dp, _u8p, _dp,
@@ -273,12 +288,16 @@ class Grid:
 
     def bicgstab(self, bb, phi, tol_rel=1e-8, tol_abs_inf=0.0, max_it=1000, n_sweeps=4, omega=0.8,
                  init_yes=False):
-        o = OrcSolverOpts(tol_rel, tol_abs_inf, max_it, n_sweeps, omega, int(init_yes))
+        o = OrcSolverOpts(tol_rel, tol_abs_inf, max_it, n_sweeps, omega, int(init_yes), 0, None, 4, 4, 4)
         work = self.zeros(9)
         r = OrcSolverResult()
         lib().orc_bicgstab(*self.N, C.byref(self.c), C.byref(o), ptr(bb), ptr(phi), ptr(work),
                            C.byref(r))
         return r
+
+    def multigrid(self, n_grids_limit=15):
+        """Build the multigrid hierarchy of this grid (mod_setup.f90:95-143)."""
+        return MG(self, n_grids_limit)
 
     def get_dtime(self, vel, Re, CFL, dtime_max):
         work = self.zeros(3)
@@ -300,10 +319,61 @@ class Grid:
         return state
 
 
+class MG:
+    """Multigrid hierarchy of a periodic oracle grid (levels, coordinates, cdg, cI, level fields)."""
+
+    def __init__(self, grid: "Grid", n_grids_limit=15):
+        self.grid = grid
+        self.s = OrcMG()
+        xp = (_dp * 3)(*[ptr(a) for a in grid.xp])
+        xu = (_dp * 3)(*[ptr(a) for a in grid.xu])
+        L = np.array(grid.L, dtype=np.float64)
+        rc = lib().orc_mg_build(*grid.N, xp, xu, ptr(L), n_grids_limit, C.byref(self.s))
+        if rc != 0:
+            raise RuntimeError("orc_mg_build failed")
+
+    @property
+    def n_grids(self):
+        return self.s.n_grids
+
+    def level_sizes(self):
+        return [tuple(self.s.M[g][m] for m in range(3)) for g in range(self.n_grids)]
+
+    def level_table(self, name, g, m):
+        M = self.s.M[g][m]
+        n = {"xp": M + 7, "xu": M + 7, "cdg": 3 * M, "cI": 2 * (M + 1)}[name]
+        return np.ctypeslib.as_array(getattr(self.s, name)[g][m], shape=(n,)).copy()
+
+    def vcycle(self, bb, phi, n_down=4, n_up=4, n_bottom=4, omega=0.98):
+        work = self.grid.zeros()
+        lib().orc_mg_vcycle(C.byref(self.s), n_down, n_up, n_bottom, omega, ptr(bb), ptr(phi), ptr(work))
+        return phi
+
+    def bicgstab(self, bb, phi, tol_rel=1e-8, max_it=200, omega=0.98, n_down=4, n_up=4, n_bottom=4,
+                 init_yes=False):
+        g = self.grid
+        o = OrcSolverOpts(tol_rel, 0.0, max_it, 1, omega, int(init_yes), 0, None, n_down, n_up, n_bottom)
+        work = g.zeros(9)
+        r = OrcSolverResult()
+        lib().orc_bicgstab_mg(*g.N, C.byref(g.c), C.byref(self.s), C.byref(o), n_down, n_up, n_bottom, ptr(bb),
+                              ptr(phi), ptr(work), C.byref(r))
+        return r
+
+    def __del__(self):
+        try:
+            lib().orc_mg_free(C.byref(self.s))
+        except Exception:
+            pass
+
+
 def step_params(Re=200.0, CFL=0.2, dtime_max=1e-2, dtime0=1e9, U0=1.0, T_pulse=1.0, level_pressure=1,
-                tol_rel=1e-8, max_it=2000, n_sweeps=4, omega=0.8):
-    return OrcStepParams(Re, CFL, dtime_max, dtime0, U0, T_pulse, level_pressure,
-                         OrcSolverOpts(tol_rel, 0.0, max_it, n_sweeps, omega, 0))
+                tol_rel=1e-8, max_it=2000, n_sweeps=4, omega=0.8, mg=None, mg_down=4, mg_up=4, mg_bottom=4):
+    """mg: an MG hierarchy (Grid.multigrid()) selects the V-cycle preconditioner."""
+    o = OrcSolverOpts(tol_rel, 0.0, max_it, n_sweeps, omega, 0, 1 if mg is not None else 0,
+                      C.cast(C.pointer(mg.s), C.c_void_p) if mg is not None else None, mg_down, mg_up, mg_bottom)
+    p = OrcStepParams(Re, CFL, dtime_max, dtime0, U0, T_pulse, level_pressure, o)
+    p._keep = mg
+    return p
 
 
 def fd_exact(abl, n, deltaX0):

@@ -16,13 +16,14 @@ from _util import rel_err
 pytestmark = pytest.mark.gpu
 
 
-def _run(precision, nsteps=3, N=(33, 33, 65), L=(1.0, 1.0, 2.0), Re=200.0):
+def _run(precision, nsteps=3, N=(33, 33, 65), L=(1.0, 1.0, 2.0), Re=200.0, precond=0):
     og, ig = O.Grid(N, L), I.Grid(N, L)
     lab = G.straight_vessel(ig, stenoses=[(1.0, 0.6, 0.125)])
+    mg = og.multigrid() if precond == 1 else None
     # oracle
     vel, nl, pre = og.zeros(3), og.zeros(3), og.zeros()
     st = O.OrcStepState()
-    p = O.step_params(Re=Re, tol_rel=1e-8, n_sweeps=4, omega=0.8)
+    p = O.step_params(Re=Re, tol_rel=1e-8, n_sweeps=4, omega=0.8, mg=mg)
     hist = []
     for _ in range(nsteps):
         og.time_step(p, lab, vel, nl, pre, st)
@@ -30,7 +31,8 @@ def _run(precision, nsteps=3, N=(33, 33, 65), L=(1.0, 1.0, 2.0), Re=200.0):
     # device
     case = I.Case(ig, precision=precision)
     case.set_labels(lab)
-    sp = I.step_params(Re=Re, tol_rel=1e-8, n_sweeps=4, omega=0.8, max_it=2000 if precision == 0 else 30)
+    sp = I.step_params(Re=Re, tol_rel=1e-8, n_sweeps=4, omega=0.8, max_it=2000 if precision == 0 else 30,
+                       precond=precond, inner_tol_rel=1e-3)
     dh = []
     for _ in range(nsteps):
         s = case.step(sp)
@@ -39,8 +41,9 @@ def _run(precision, nsteps=3, N=(33, 33, 65), L=(1.0, 1.0, 2.0), Re=200.0):
     return og, vel, pre, hist, case, got, dh
 
 
-def test_step_fp64_matches_oracle():
-    og, vel, pre, hist, case, got, dh = _run(0)
+@pytest.mark.parametrize("precond", [0, 1], ids=["jor4", "multigrid"])
+def test_step_fp64_matches_oracle(precond):
+    og, vel, pre, hist, case, got, dh = _run(0, precond=precond)
     for (dt_o, it_o), (dt_g, it_g, stat) in zip(hist, dh):
         assert abs(dt_g - dt_o) <= 1e-12 * dt_o
         assert all(s == 0 for s in stat)
@@ -53,8 +56,9 @@ def test_step_fp64_matches_oracle():
     assert np.abs(d).max() <= 1e-6 * np.abs(og.interior(pre)).max()
 
 
-def test_step_mixed_matches_oracle():
-    og, vel, pre, hist, case, got, dh = _run(1)
+@pytest.mark.parametrize("precond", [0, 1], ids=["jor4", "multigrid"])
+def test_step_mixed_matches_oracle(precond):
+    og, vel, pre, hist, case, got, dh = _run(1, precond=precond)
     for (dt_o, _), (dt_g, _, stat) in zip(hist, dh):
         assert abs(dt_g - dt_o) <= 1e-9 * dt_o
         assert all(s == 0 for s in stat)
