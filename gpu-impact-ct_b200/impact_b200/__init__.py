@@ -108,6 +108,7 @@ def lib():
         "impact_b200_case_mg_levels": (i, [_vp]),
         "impact_b200_jacobi_solve": (i, [i, i, i, i, i, i, d, _dp, _dp, _dp, _dp, _dp, i, d, i, _ip, _dp]),
         "impact_b200_product_scalar": (i, [i, i, i, _vp, _vp, _dp]),
+        "impact_b200_product_scalar_noalloc": (i, [i, i, i, _vp, _vp, _dp]),
         "impact_b200_profile_enable": (None, [i]),
         "impact_b200_profile_reset": (None, []),
         "impact_b200_profile_read": (i, [i, P(C.c_longlong), _dp, _dp, P(C.c_char_p)]),
@@ -333,6 +334,14 @@ def fd_exact(abl, n, deltaX0):
 def product_scalar(N, a_dev: int, b_dev: int) -> float:
     out = C.c_double()
     check(lib().impact_b200_product_scalar(N[0], N[1], N[2], a_dev, b_dev, C.byref(out)), "product_scalar")
+    return out.value
+
+
+def product_scalar_noalloc(N, a_dev: int, b_dev: int) -> float:
+    """product_scalar without any device allocation (fixed library scratch; see the C header)."""
+    out = C.c_double()
+    check(lib().impact_b200_product_scalar_noalloc(N[0], N[1], N[2], a_dev, b_dev, C.byref(out)),
+          "product_scalar_noalloc")
     return out.value
 
 

@@ -228,6 +228,17 @@ int impact_b200_jacobi_solve(int N1, int N2, int N3, int M1, int M2, int M3, dou
  * Uses a per-call scratch allocation for the block partials. */
 int impact_b200_product_scalar(int N1, int N2, int N3, const double* a_dev, const double* b_dev, double* result);
 
+/* The same inner product for callers that cannot let the library allocate device memory: a
+ * host code whose GPU memory is all claimed by its own allocator, or a loop that cannot pay for
+ * cudaMalloc/cudaFree (they can synchronise the device).  No counterpart in the reference.  Its
+ * scratch is a fixed 128 KiB array in device memory, held by every GPU that loads the library
+ * until exit; grids with more than 16384 unique z-planes (N3 > 16385) are rejected.  The first
+ * call on a device resolves the array's address (make it before any stream capture there); calls
+ * whose kernels overlap on the GPU share the array and race, so serialise them.  Runs on the
+ * legacy default stream; returns once *result (host memory) is written. */
+int impact_b200_product_scalar_noalloc(int N1, int N2, int N3, const double* a_dev, const double* b_dev,
+                                       double* result);
+
 /* ---- measurement hooks -----------------------------------------------------------------
  * When enabled, the library records CUDA events on the launching stream around its hot kernels
  * and accumulates, per kernel kind kid (0 jacobi_sweep, 1 jacobi_init2, 2 div_grad_dot,
