@@ -4,6 +4,7 @@
 
 #include "../../include/impact_b200.h"
 #include "common.cuh"
+#include "engine.cuh"
 #include "mg.cuh"
 #include "solver.cuh"
 
@@ -43,6 +44,17 @@ struct CaseState {
   double* dscal = nullptr;       // small device scalars (dt, mean pressure, ...)
   double* hscal = nullptr;       // pinned host mirror
   SolverScalars* scal_host = nullptr;
+  // product_div_grad collapsed to 11-point stencils per axis, FP64 and FP32 (rows 1..n)
+  const double* W64[3] = {};
+  const float* W32[3] = {};
+  int zuni = 0;      // every z row of the collapsed weights is the same (uniform z spacing)
+  int cdg_zuni = 0;  // every z row of the fine compact Laplacian is the same
+  // Poisson engines (a batch of one), built on first use and rebuilt when the solver
+  // parameters or the right-hand side / solution fields change
+  Engine<double>* e64 = nullptr;
+  MixedEngine* emx = nullptr;
+  const double* eng_b = nullptr;
+  double* eng_x = nullptr;
   std::vector<void*> allocs;
 };
 

@@ -1,0 +1,1987 @@
+// engine.cu -- batched pressure Poisson engine: BiCGstab_orig with the multigrid V-cycle (or
+// damped-Jacobi sweeps) as preconditioner, every kernel over a job list of cases / levels.
+//
+//   BiCGstab_orig           mod_solvers.f90:1509-1935   k_kr_* and the scalar finalisation
+//   product_div_grad        mod_laplace.f90:38-197      k_kr_ax (collapsed 11-point form, z-march)
+//   multigridV              mod_solvers.f90:456-585     schedule built in Engine::build
+//   relaxation_div_grad     mod_laplace.f90:339-613     k_lv_smooth
+//   product_div_grad_relax  mod_laplace.f90:216-327     k_lv_resid (fused with the subtraction)
+//   restrict                mod_solvers.f90:588-808     k_lv_restrict
+//   interpolate             mod_solvers.f90:955-1141    k_lv_prolong
+//   product_scalar/get_norms mod_solvers.f90:2319-2470  per-tile partials + fixed-order k_efin
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+
+#include "engine.cuh"
+#include "prof.cuh"
+
+namespace impact {
+
+namespace {
+
+enum EFin { EFIN_RAW = 0, EFIN_INIT, EFIN_ALPHA, EFIN_OMEGA, EFIN_NORMS, EFIN_RESET };
+
+__device__ __forceinline__ bool e_halted(const SolverScalars* sc) { return sc->done | sc->status; }
+
+// job owning tile b: the largest q with ts[q] <= b (jobs without tiles are skipped over)
+__device__ __forceinline__ int find_job(const int* __restrict__ ts, int nj, int b) {
+  int lo = 0, hi = nj - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(ts + mid) <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// tile t of grid g: this thread's column (i, j) (the first of vw consecutive columns) and the
+// plane range k0..k1
+__device__ __forceinline__ void tile_at(const Geom& g, int kc, int t, int& i, int& j, int& k0, int& k1, int vw = 1) {
+  const int tx = (g.n1 + ETX * vw - 1) / (ETX * vw), ty = (g.n2 + ETY - 1) / ETY;
+  const int a = t % tx;
+  const int r = t / tx;
+  const int c = r / ty;
+  i = (a * ETX + threadIdx.x) * vw + 1;
+  j = (r - c * ty) * ETY + threadIdx.y + 1;
+  k0 = c * kc + 1;
+  k1 = min(g.n3, k0 + kc - 1);
+}
+
+__device__ __forceinline__ double e_wsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double e_wmax(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// elements per block of loads: 4 planes in FP32, 2 in FP64
+template <typename T>
+struct Ublk {
+  static constexpr int U = sizeof(T) == 4 ? 4 : 2;
+};
+
+// 16-byte vectors: 4 floats or 2 doubles per thread in the vectorised level kernels
+template <typename T>
+struct VecT;
+template <>
+struct VecT<float> {
+  static constexpr int W = 4;
+};
+template <>
+struct VecT<double> {
+  static constexpr int W = 2;
+};
+template <typename T>
+__device__ __forceinline__ void vload(const T* p, T (&o)[VecT<T>::W]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+    o[3] = v.w;
+  } else {
+    const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+  }
+}
+template <typename T>
+__device__ __forceinline__ void vstore(T* p, const T (&o)[VecT<T>::W]) {
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+  } else {
+    *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
+  }
+}
+
+// NQ block-wide partials of one tile into out[0..NQ-1]; bit q of MAXMASK: max instead of sum
+template <int NQ, int MAXMASK>
+__device__ __forceinline__ void tile_partials(double (&v)[NQ], double* __restrict__ out) {
+  __shared__ double sh[NQ][ENT / 32];
+  const int tid = threadIdx.x + ETX * threadIdx.y;
+  const int lane = tid & 31, w = tid >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) v[q] = ((MAXMASK >> q) & 1) ? e_wmax(v[q]) : e_wsum(v[q]);
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) sh[q][w] = v[q];
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      double x = lane < ENT / 32 ? sh[q][lane] : 0.0;
+      x = ((MAXMASK >> q) & 1) ? e_wmax(x) : e_wsum(x);
+      if (lane == 0) out[q] = x;
+    }
+  }
+  __syncthreads();
+}
+
+// ------------------------------------------------------------------------------------------
+// scalar finalisation: one block per job, the job's tile partials in tile order
+// ------------------------------------------------------------------------------------------
+__device__ void e_scalar_update(int mode, const double* q, SolverScalars* sc) {
+  switch (mode) {
+    case EFIN_INIT:  // q = [max|r|, sum r^2, r.rh, sum b^2]
+      sc->norm_inf = q[0];
+      sc->norm_two_sq = q[1];
+      sc->rhr_next = q[2];
+      sc->b_two_sq = q[3];
+      sc->rhr = 0.0;
+      sc->alpha = sc->omega = sc->beta = 0.0;
+      sc->it = 0;
+      sc->status = 0;
+      sc->done = (q[0] == 0.0) ? 1 : 0;  // the reference iterates at least once unless r == 0
+      if (sc->max_it <= 0) sc->done = 1;
+      if (!isfinite(q[0]) || !isfinite(q[1])) sc->status = 3;
+      break;
+    case EFIN_ALPHA:
+      sc->rhAp = q[0];
+      if (q[0] == 0.0)
+        sc->status = 2;
+      else
+        sc->alpha = sc->rhr / q[0];
+      break;
+    case EFIN_OMEGA:
+      sc->rAr = q[0];
+      sc->ArAr = q[1];
+      if (q[1] == 0.0)
+        sc->status = 2;
+      else
+        sc->omega = q[0] / q[1];
+      break;
+    case EFIN_NORMS: {
+      sc->norm_inf = q[0];
+      sc->norm_two_sq = q[1];
+      sc->rhr_next = q[2];
+      if (!isfinite(q[0]) || !isfinite(q[1])) {
+        sc->status = 3;
+        break;
+      }
+      const bool conv = (sc->tol_abs_inf > 0.0 && q[0] < sc->tol_abs_inf) ||
+                        (sc->tol_rel > 0.0 && sqrt(q[1]) <= sc->tol_rel * sqrt(sc->b_two_sq));
+      if (conv) {
+        sc->done = 1;
+      } else if (sc->it >= sc->max_it) {
+        sc->done = 1;
+        sc->status = 1;
+      }
+      break;
+    }
+    case EFIN_RESET:  // new shadow residual rh = rr: rhr = rr.rr, redo the iteration start
+      sc->rhr_next = q[0];
+      sc->status = 0;
+      sc->it -= 1;
+      sc->rhr = sc->rhr_prev;
+      break;
+    default:
+      break;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_efin(const int* __restrict__ ts, const double* __restrict__ partial, int nq,
+                                              int maxmask, int mode, SolverScalars* __restrict__ scal,
+                                              double* __restrict__ raw) {
+  const int q = blockIdx.x;
+  SolverScalars* sc = scal ? scal + q : nullptr;
+  if (sc) {
+    if (mode == EFIN_RESET) {
+      if (sc->status != 4) return;
+    } else if (mode == EFIN_INIT) {
+      if (sc->done) return;
+    } else if (mode != EFIN_RAW) {
+      if (e_halted(sc)) return;
+    }
+  }
+  const int t0 = ts[q], t1 = ts[q + 1];
+  __shared__ double sh[4][8];
+  __shared__ double tot[4];
+  for (int c = 0; c < nq; ++c) {
+    const bool mx = (maxmask >> c) & 1;
+    double v = 0.0;
+    for (int t = t0 + threadIdx.x; t < t1; t += 256) {
+      const double x = partial[(long long)t * 4 + c];
+      v = mx ? fmax(v, x) : v + x;
+    }
+    v = mx ? e_wmax(v) : e_wsum(v);
+    if ((threadIdx.x & 31) == 0) sh[c][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    for (int c = 0; c < nq; ++c) {
+      const bool mx = (maxmask >> c) & 1;
+      double x = threadIdx.x < 8 ? sh[c][threadIdx.x] : 0.0;
+      x = mx ? e_wmax(x) : e_wsum(x);
+      if (threadIdx.x == 0) tot[c] = x;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int c = 0; c < nq; ++c) r[c] = tot[c];
+    if (mode == EFIN_RAW) {
+      for (int c = 0; c < 4; ++c) raw[q * 4 + c] = r[c];
+    } else {
+      e_scalar_update(mode, r, sc);
+    }
+  }
+}
+
+// start of an iteration (mod_solvers.f90:~1600-1680): rhr, breakdown tests, beta, omega
+__global__ void k_ebegin(SolverScalars* __restrict__ scal, int n) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  SolverScalars* sc = scal + q;
+  if (e_halted(sc)) return;
+  sc->it += 1;
+  sc->rhr_prev = sc->rhr;
+  sc->rhr = sc->rhr_next;
+  if (sc->rhr == 0.0) {  // shadow residual orthogonal to r: the host resets rh = rr
+    sc->status = 4;
+    return;
+  }
+  if (sc->it >= 2) {
+    if (sc->omega == 0.0 || sc->rhr_prev == 0.0) {
+      sc->status = 2;
+      return;
+    }
+    sc->beta = (sc->alpha / sc->omega) * (sc->rhr / sc->rhr_prev);
+    sc->omega = -sc->beta * sc->omega;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// BiCGstab vector kernels over the Krylov job list
+// ------------------------------------------------------------------------------------------
+// initial residual: rr = bb - rr (rr = A phi), or rr = bb with phi = 0; rh = rr
+// partials [max|rr|, sum rr^2, rr.rh, sum bb^2]
+template <typename T>
+__global__ void __launch_bounds__(ENT) k_kr_init(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+                                                 int nj, int ntiles, int zero_phi, double* __restrict__ partial) {
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const KrylovJob<T>& J = jobs[q];
+    if (J.sc->done) continue;
+    const Geom g = J.g;
+    int i, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (i <= g.n1 && j <= g.n2) {
+      const T* __restrict__ bb = J.bb;
+      T* __restrict__ phi = J.phi;
+      T* __restrict__ rr = J.rr;
+      T* __restrict__ rh = J.rh;
+      long long p = off(g, i, j, k0);
+      for (int k = k0; k <= k1; ++k, p += g.nxy) {
+        const T bv = bb[p];
+        T r;
+        if (zero_phi) {
+          phi[p] = T(0);
+          r = bv;
+        } else {
+          r = bv - rr[p];
+        }
+        rr[p] = r;
+        rh[p] = r;
+        const double rd = (double)r, bd = (double)bv;
+        v[0] = fmax(v[0], fabs(rd));
+        v[1] += rd * rd;
+        v[2] += rd * rd;
+        v[3] += bd * bd;
+      }
+    }
+    tile_partials<4, 1>(v, partial + (long long)b * 4);
+  }
+}
+
+// pp = rr (first iteration) or pp = rr + beta pp + omega Ap (omega already holds -beta omega)
+template <typename T>
+__global__ void __launch_bounds__(ENT) k_kr_p(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts, int nj,
+                                              int ntiles) {
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const KrylovJob<T>& J = jobs[q];
+    const SolverScalars* sc = J.sc;
+    if (e_halted(sc)) continue;
+    const Geom g = J.g;
+    int i, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
+    if (i > g.n1 || j > g.n2) continue;
+    const T* __restrict__ rr = J.rr;
+    const T* __restrict__ Ap = J.Ap;
+    T* __restrict__ pp = J.pp;
+    constexpr int U = 2 * Ublk<T>::U;
+    const long long nxy = g.nxy;
+    long long p = off(g, i, j, k0);
+    int k = k0;
+    if (sc->it == 1) {
+      for (; k + U - 1 <= k1; k += U, p += U * nxy) {
+        T r[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) r[u] = rr[p + u * nxy];
+#pragma unroll
+        for (int u = 0; u < U; ++u) pp[p + u * nxy] = r[u];
+      }
+      for (; k <= k1; ++k, p += nxy) pp[p] = rr[p];
+    } else {
+      const T be = (T)sc->beta, om = (T)sc->omega;
+      for (; k + U - 1 <= k1; k += U, p += U * nxy) {
+        T r[U], q0[U], a[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          r[u] = rr[p + u * nxy];
+          q0[u] = pp[p + u * nxy];
+          a[u] = Ap[p + u * nxy];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) pp[p + u * nxy] = r[u] + be * q0[u] + om * a[u];
+      }
+      for (; k <= k1; ++k, p += nxy) pp[p] = rr[p] + be * pp[p] + om * Ap[p];
+    }
+  }
+}
+
+// rr = rr - alpha Ap
+template <typename T>
+__global__ void __launch_bounds__(ENT) k_kr_r(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts, int nj,
+                                              int ntiles) {
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const KrylovJob<T>& J = jobs[q];
+    const SolverScalars* sc = J.sc;
+    if (e_halted(sc)) continue;
+    const Geom g = J.g;
+    int i, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
+    if (i > g.n1 || j > g.n2) continue;
+    const T* __restrict__ Ap = J.Ap;
+    T* __restrict__ rr = J.rr;
+    const T al = (T)sc->alpha;
+    constexpr int U = 2 * Ublk<T>::U;
+    const long long nxy = g.nxy;
+    long long p = off(g, i, j, k0);
+    int k = k0;
+    for (; k + U - 1 <= k1; k += U, p += U * nxy) {
+      T r[U], a[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        r[u] = rr[p + u * nxy];
+        a[u] = Ap[p + u * nxy];
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) rr[p + u * nxy] = r[u] - al * a[u];
+    }
+    for (; k <= k1; ++k, p += nxy) rr[p] = rr[p] - al * Ap[p];
+  }
+}
+
+// phi += omega z2 + alpha z1 ; rr -= omega Ar ; partials [max|rr|, sum rr^2, rr.rh]
+template <typename T>
+__global__ void __launch_bounds__(ENT) k_kr_x(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts, int nj,
+                                              int ntiles, double* __restrict__ partial) {
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const KrylovJob<T>& J = jobs[q];
+    const SolverScalars* sc = J.sc;
+    if (e_halted(sc)) continue;
+    const Geom g = J.g;
+    int i, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
+    double v[3] = {0.0, 0.0, 0.0};
+    if (i <= g.n1 && j <= g.n2) {
+      const T* __restrict__ z1 = J.z1;
+      const T* __restrict__ z2 = J.z2;
+      const T* __restrict__ Ar = J.Ar;
+      const T* __restrict__ rh = J.rh;
+      T* __restrict__ phi = J.phi;
+      T* __restrict__ rr = J.rr;
+      const T om = (T)sc->omega, al = (T)sc->alpha;
+      constexpr int U = Ublk<T>::U;
+      const long long nxy = g.nxy;
+      long long p = off(g, i, j, k0);
+      auto point = [&](long long q, T ph, T a2, T a1, T r0, T ar, T h) {
+        // without a preconditioner z2 aliases rr: it was read before rr is overwritten
+        phi[q] = ph + om * a2 + al * a1;
+        const T r = r0 - om * ar;
+        rr[q] = r;
+        const double rd = (double)r;
+        v[0] = fmax(v[0], fabs(rd));
+        v[1] += rd * rd;
+        v[2] += rd * (double)h;
+      };
+      int k = k0;
+      for (; k + U - 1 <= k1; k += U, p += U * nxy) {
+        T ph[U], a2[U], a1[U], r0[U], ar[U], h[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const long long q = p + u * nxy;
+          ph[u] = phi[q];
+          a2[u] = z2[q];
+          a1[u] = z1[q];
+          r0[u] = rr[q];
+          ar[u] = Ar[q];
+          h[u] = rh[q];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) point(p + u * nxy, ph[u], a2[u], a1[u], r0[u], ar[u], h[u]);
+      }
+      for (; k <= k1; ++k, p += nxy) point(p, phi[p], z2[p], z1[p], rr[p], Ar[p], rh[p]);
+    }
+    tile_partials<3, 1>(v, partial + (long long)b * 4);
+  }
+}
+
+// rh = rr for the cases whose shadow residual was lost (status 4); partial sum rr.rr
+template <typename T>
+__global__ void __launch_bounds__(ENT) k_kr_reset(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+                                                  int nj, int ntiles, double* __restrict__ partial) {
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const KrylovJob<T>& J = jobs[q];
+    if (J.sc->status != 4) continue;
+    const Geom g = J.g;
+    int i, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
+    double v[1] = {0.0};
+    if (i <= g.n1 && j <= g.n2) {
+      long long p = off(g, i, j, k0);
+      for (int k = k0; k <= k1; ++k, p += g.nxy) {
+        const T r = J.rr[p];
+        J.rh[p] = r;
+        v[0] += (double)r * (double)r;
+      }
+    }
+    tile_partials<1, 0>(v, partial + (long long)b * 4);
+  }
+}
+
+// asynchronous global -> shared copy of one element (kept in L1 as well), and its group control
+template <typename T>
+__device__ __forceinline__ void cp_async1(T* smem, const T* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// A x = sum_m D_m G_m x with the two 6-point stencils of each axis collapsed into one 11-point
+// stencil W_m (weights formed once on the host in FP64).  A block owns 32 x 8 columns over kc
+// planes.  Each plane of the tile with its 5-wide x/y halo (42 x 18 elements, periodic images),
+// and the inner-product partner of the plane, are staged by cp.async into a ring of R shared-
+// memory slots R-1 planes ahead of their use, so that about R planes of DRAM traffic are in
+// flight per block.  x and y neighbours and the z values k..k+5 of the column are read from
+// the ring; the z values k-5..k-1 stay in a register window.
+//   MODE 0: rr = A phi                 (initial residual)
+//   MODE 1: Ap = A z1, partial rh.Ap   (alpha)
+//   MODE 2: Ar = A z2, partials Ar.rr, Ar.Ar (omega)
+constexpr int AX_TW = ETX + 10, AX_TH = ETY + 10, AX_TE = AX_TW * AX_TH;
+constexpr int AX_PER = (AX_TE + ENT - 1) / ENT;  // staged elements per thread and plane
+// ring depth: planes k .. k+5 are read at plane k, the rest of the ring is in flight
+template <typename T>
+struct AxRing {
+  static constexpr int R = sizeof(T) == 4 ? 12 : 10;
+};
+template <typename T>
+constexpr size_t ax_smem_bytes() {
+  constexpr int R = AxRing<T>::R;
+  return sizeof(T) * ((size_t)R * AX_TE + (size_t)R * ENT + (size_t)KC_MAX * AXW + ETY * AXW + AXW * ETX);
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+                                                  int nj, int ntiles, double* __restrict__ partial) {
+  constexpr int AX_R = AxRing<T>::R;
+  extern __shared__ __align__(16) unsigned char ax_smem[];
+  T(*ring)[AX_TH][AX_TW] = reinterpret_cast<T(*)[AX_TH][AX_TW]>(ax_smem);
+  T(*dring)[ENT] = reinterpret_cast<T(*)[ENT]>(ax_smem + sizeof(T) * AX_R * AX_TE);
+  T(*wzs)[AXW] = reinterpret_cast<T(*)[AXW]>(ax_smem + sizeof(T) * (AX_R * AX_TE + AX_R * ENT));
+  T(*wys)[AXW] = reinterpret_cast<T(*)[AXW]>(ax_smem + sizeof(T) * (AX_R * AX_TE + AX_R * ENT + KC_MAX * AXW));
+  T(*wxs)[ETX] =
+      reinterpret_cast<T(*)[ETX]>(ax_smem + sizeof(T) * (AX_R * AX_TE + AX_R * ENT + KC_MAX * AXW + ETY * AXW));
+  const int tid = threadIdx.x + ETX * threadIdx.y;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const KrylovJob<T>& J = jobs[q];
+    const SolverScalars* sc = J.sc;
+    if (MODE == 0 ? (sc->done != 0) : e_halted(sc)) continue;
+    const Geom g = J.g;
+    int i, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
+    const int i0 = i - tx, j0 = j - ty;
+    const bool in = i <= g.n1 && j <= g.n2;
+    const T* __restrict__ x = MODE == 0 ? J.phi : (MODE == 1 ? J.z1 : J.z2);
+    T* __restrict__ out = MODE == 0 ? J.rr : (MODE == 1 ? J.Ap : J.Ar);
+    const T* __restrict__ d1 = MODE == 1 ? J.rh : J.rr;
+    const long long nxy = g.nxy;
+    // weights of the tile: z rows of its planes, y rows of its 8 rows, x rows of its 32 columns
+    const int nzw = (k1 - k0 + 1) * AXW;
+    for (int t = tid; t < nzw; t += ENT) wzs[t / AXW][t % AXW] = J.W[2][(k0 - 1) * AXW + t];
+    for (int t = tid; t < ETY * AXW; t += ENT) {
+      const int jj = j0 + t / AXW;
+      wys[t / AXW][t % AXW] = jj <= g.n2 ? J.W[1][(jj - 1) * AXW + t % AXW] : T(0);
+    }
+    for (int t = tid; t < ETX * AXW; t += ENT) {
+      const int ii = i0 + t / AXW;
+      wxs[t % AXW][t / AXW] = ii <= g.n1 ? J.W[0][(ii - 1) * AXW + t % AXW] : T(0);
+    }
+    // in-plane offsets of this thread's staged elements (periodic images of the halo)
+    int eo[AX_PER];
+#pragma unroll
+    for (int e = 0; e < AX_PER; ++e) {
+      const int t = tid + e * ENT;
+      const int r = t / AX_TW, c = t % AX_TW;
+      const int gi = wrapi(i0 - 5 + c, g.n1), gj = wrapi(j0 - 5 + r, g.n2);
+      eo[e] = t < AX_TE ? (gi + 3) + g.nx * (gj + 3) : -1;
+    }
+    const int own = (in ? i + 3 : 4) + g.nx * ((in ? j : 1) + 3);  // the column's in-plane offset
+    auto zoff = [&](int k) -> long long {  // plane k (periodic) + 3 ghost planes
+      return (long long)((k < 1 ? k + g.n3 : (k > g.n3 ? k - g.n3 : k)) + 3) * nxy;
+    };
+    // plane kk (k0-5 <= kk <= k1+5) into its ring slot; the partner only for kk in k0..k1
+    auto stage = [&](int kk) {
+      if (kk <= k1 + 5) {
+        const int sl = (kk - k0 + AX_R * 8) % AX_R;
+        T* slot = &ring[sl][0][0];
+        const T* src = x + zoff(kk);
+#pragma unroll
+        for (int e = 0; e < AX_PER; ++e)
+          if (eo[e] >= 0) cp_async1(slot + tid + e * ENT, src + eo[e]);
+        if (MODE != 0 && kk >= k0 && kk <= k1 && in) cp_async1(&dring[sl][tid], d1 + zoff(kk) + own);
+      }
+      cp_commit();
+    };
+    __syncthreads();  // weights visible
+    T wx[AXW];
+#pragma unroll
+    for (int l = 0; l < AXW; ++l) wx[l] = wxs[l][tx];
+    // the past z values x(k0-5 .. k0-1) of the column, then the ring from plane k0
+    T zp[5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) zp[l] = in ? x[zoff(k0 - 5 + l) + own] : T(0);
+#pragma unroll
+    for (int l = 0; l < AX_R - 1; ++l) stage(k0 + l);
+    double v0 = 0.0, v1 = 0.0;
+    for (int k = k0; k <= k1; ++k) {
+      cp_wait<AX_R - 7>();  // this thread's copies of planes k .. k+5 have landed
+      __syncthreads();      // everybody's have; the slot of plane k-1 is free again
+      stage(k + AX_R - 1);
+      const int sl = (k - k0) % AX_R;
+      const T (*sp)[AX_TW] = ring[sl];
+      if (in) {
+        const T c = sp[ty + 5][tx + 5];
+        T ax = wx[0] * sp[ty + 5][tx];
+#pragma unroll
+        for (int l = 1; l < AXW; ++l) ax += wx[l] * (l == 5 ? c : sp[ty + 5][tx + l]);
+        T ay = wys[ty][0] * sp[ty][tx + 5];
+#pragma unroll
+        for (int l = 1; l < AXW; ++l) ay += wys[ty][l] * (l == 5 ? c : sp[ty + l][tx + 5]);
+        const T* wz = wzs[k - k0];
+        T az = wz[0] * zp[0];
+#pragma unroll
+        for (int l = 1; l < 5; ++l) az += wz[l] * zp[l];
+        az += wz[5] * c;
+#pragma unroll
+        for (int l = 6; l < AXW; ++l) az += wz[l] * ring[(sl + l - 5) % AX_R][ty + 5][tx + 5];
+        const T r = ax + ay + az;
+        out[zoff(k) + own] = r;
+        if (MODE == 1) v0 += (double)r * (double)dring[sl][tid];
+        if (MODE == 2) {
+          v0 += (double)r * (double)dring[sl][tid];
+          v1 += (double)r * (double)r;
+        }
+#pragma unroll
+        for (int l = 0; l < 4; ++l) zp[l] = zp[l + 1];
+        zp[4] = c;
+      }
+    }
+    cp_wait<0>();
+    if (MODE == 1) {
+      double v[1] = {v0};
+      tile_partials<1, 0>(v, partial + (long long)b * 4);
+    } else if (MODE == 2) {
+      double v[2] = {v0, v1};
+      tile_partials<2, 0>(v, partial + (long long)b * 4);
+    } else {
+      __syncthreads();  // the ring and the weights are rewritten by the next tile
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// multigrid kernels over level job lists
+// ------------------------------------------------------------------------------------------
+// One column (i, j), planes k0..k1, of the compact 7-point operator cdg.  The column is walked
+// in blocks of U planes: all loads of a block (the next planes' centres, the right-hand side
+// and the four lateral neighbours) are issued before its stores, so that every thread keeps
+// several DRAM requests in flight; the z-neighbours stay in registers.
+//   OP 0: damped-Jacobi sweep  out = omega (bb - offdiag x) / diag + (1 - omega) x
+//   OP 1: residual             out = bb - (offdiag x + diag x)
+template <typename T, int OP, int U, bool ZU>
+__device__ __forceinline__ void march7(const Geom& g, int i, int j, int k0, int k1, const T* __restrict__ cx,
+                                       const T* __restrict__ cy, const T* __restrict__ cz, T omega,
+                                       const T* __restrict__ bb, const T* __restrict__ x, T* __restrict__ out) {
+  const T a0 = cx[3 * (i - 1)], a1 = cx[3 * (i - 1) + 1], a2 = cx[3 * (i - 1) + 2];
+  const T b0 = cy[3 * (j - 1)], b1 = cy[3 * (j - 1) + 1], b2 = cy[3 * (j - 1) + 2];
+  // uniform z: one z row for the whole column, and omega / diag formed once (the per-point
+  // division omega r / diag becomes r (omega / diag))
+  const T zcm = ZU ? cz[0] : T(0), zcc = ZU ? cz[1] : T(0), zcp = ZU ? cz[2] : T(0);
+  const T inv = ZU ? omega / (a1 + b1 + zcc) : T(0);
+  const T dg = ZU ? a1 + b1 + zcc : T(0);
+  const long long nxy = g.nxy;
+  const int dW = (i == 1) ? g.n1 - 1 : -1;
+  const int dE = (i == g.n1) ? 1 - g.n1 : 1;
+  const int dS = (j == 1) ? (g.n2 - 1) * g.nx : -g.nx;
+  const int dN = (j == g.n2) ? -(g.n2 - 1) * g.nx : g.nx;
+  const long long wz = (long long)(g.n3 - 1) * nxy;
+  long long p = off(g, i, j, k0);
+  T xm = x[k0 == 1 ? p + wz : p - nxy];
+  T xc = x[p];
+  auto point = [&](int k, long long q, T bv, T w, T e, T s, T n, T zm, T zc, T zp) {
+    const T cm = ZU ? zcm : cz[3 * (k - 1)];
+    const T cc = ZU ? zcc : cz[3 * (k - 1) + 1];
+    const T cp = ZU ? zcp : cz[3 * (k - 1) + 2];
+    if (OP == 0) {
+      const T r = bv - a0 * w - a2 * e - b0 * s - b2 * n - cm * zm - cp * zp;
+      out[q] = (ZU ? r * inv : omega * r / (a1 + b1 + cc)) + (T(1) - omega) * zc;
+    } else {
+      const T lap = a0 * w + a2 * e + b0 * s + b2 * n + cm * zm + cp * zp + (ZU ? dg : a1 + b1 + cc) * zc;
+      out[q] = bv - lap;
+    }
+  };
+  int k = k0;
+  for (; k + U - 1 <= k1; k += U) {
+    T xn[U], bv[U], w[U], e[U], s[U], n[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const long long q = p + u * nxy;
+      xn[u] = x[(k + u == g.n3) ? q - wz : q + nxy];
+      bv[u] = bb[q];
+      w[u] = x[q + dW];
+      e[u] = x[q + dE];
+      s[u] = x[q + dS];
+      n[u] = x[q + dN];
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const T zc = u == 0 ? xc : xn[u - 1];
+      const T zm = u == 0 ? xm : (u == 1 ? xc : xn[u - 2]);
+      point(k + u, p + u * nxy, bv[u], w[u], e[u], s[u], n[u], zm, zc, xn[u]);
+    }
+    xm = U >= 2 ? xn[U - 2] : xc;
+    xc = xn[U - 1];
+    p += U * nxy;
+  }
+  for (; k <= k1; ++k, p += nxy) {
+    const T xp = x[k == g.n3 ? p - wz : p + nxy];
+    point(k, p, bb[p], x[p + dW], x[p + dE], x[p + dS], x[p + dN], xm, xc, xp);
+    xm = xc;
+    xc = xp;
+  }
+}
+
+// The same column walk for W = 16 / sizeof(T) consecutive columns i .. i+W-1 per thread, with
+// 16-byte loads and stores (requires n1 % W == 0).  The x-neighbours inside the vector are
+// registers, the ones across vectors come from the adjacent lanes by shuffles (a scalar load at
+// the warp edges and at the periodic boundary).  Every lane of the warp runs the walk (inactive
+// lanes only take part in the shuffles).
+template <typename T, int OP, int U, bool ZU>
+__device__ __forceinline__ void march7v(const Geom& g, int i, int j, int k0, int k1, bool act,
+                                        const T* __restrict__ cx, const T* __restrict__ cy,
+                                        const T* __restrict__ cz, T omega, const T* __restrict__ bb,
+                                        const T* __restrict__ x, T* __restrict__ out) {
+  constexpr int V = VecT<T>::W;
+  const int lane = threadIdx.x & 31;
+  const int ic = act ? i : 1, jc = act ? j : 1;
+  T a0[V], a1[V], a2[V], inv[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    a0[v] = cx[3 * (ic - 1 + v)];
+    a1[v] = cx[3 * (ic - 1 + v) + 1];
+    a2[v] = cx[3 * (ic - 1 + v) + 2];
+  }
+  const T b0 = cy[3 * (jc - 1)], b1 = cy[3 * (jc - 1) + 1], b2 = cy[3 * (jc - 1) + 2];
+  const T zcm = ZU ? cz[0] : T(0), zcc = ZU ? cz[1] : T(0), zcp = ZU ? cz[2] : T(0);
+#pragma unroll
+  for (int v = 0; v < V; ++v) inv[v] = ZU ? omega / (a1[v] + b1 + zcc) : T(0);
+  const long long nxy = g.nxy;
+  const int dS = (jc == 1) ? (g.n2 - 1) * g.nx : -g.nx;
+  const int dN = (jc == g.n2) ? -(g.n2 - 1) * g.nx : g.nx;
+  const int wOff = (ic == 1) ? g.n1 - 1 : -1;            // west of the first column
+  const int eOff = (ic + V - 1 == g.n1) ? 1 - ic : V;    // east of the last column
+  const bool lw = lane == 0 || ic == 1;
+  const bool le = lane == 31 || ic + V - 1 == g.n1;
+  const long long wzf = (long long)(g.n3 - 1) * nxy;
+  long long p = off(g, ic, jc, k0);
+  T xm[V], xc[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) xm[v] = xc[v] = T(0);
+  if (act) {
+    vload(x + (k0 == 1 ? p + wzf : p - nxy), xm);
+    vload(x + p, xc);
+  }
+  for (int k = k0; k <= k1; k += U) {
+    const int nk = min(U, k1 - k + 1);
+    T xn[U][V], bv[U][V], sv[U][V], nv[U][V], ws[U], es[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      ws[u] = es[u] = T(0);
+#pragma unroll
+      for (int v = 0; v < V; ++v) xn[u][v] = bv[u][v] = sv[u][v] = nv[u][v] = T(0);
+      if (act && u < nk) {
+        const long long q = p + u * nxy;
+        vload(x + ((k + u == g.n3) ? q - wzf : q + nxy), xn[u]);
+        vload(bb + q, bv[u]);
+        vload(x + q + dS, sv[u]);
+        vload(x + q + dN, nv[u]);
+        if (lw) ws[u] = x[q + wOff];
+        if (le) es[u] = x[q + eOff];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (u < nk) {
+        T zc[V], zm[V], ov[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          zc[v] = u == 0 ? xc[v] : xn[u - 1][v];
+          zm[v] = u == 0 ? xm[v] : (u == 1 ? xc[v] : xn[u - 2][v]);
+        }
+        const T wsh = __shfl_up_sync(0xffffffffu, zc[V - 1], 1);
+        const T esh = __shfl_down_sync(0xffffffffu, zc[0], 1);
+        const int kk = k + u;
+        const T cm = ZU ? zcm : cz[3 * (kk - 1)];
+        const T cc = ZU ? zcc : cz[3 * (kk - 1) + 1];
+        const T cp = ZU ? zcp : cz[3 * (kk - 1) + 2];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const T w = v == 0 ? (lw ? ws[u] : wsh) : zc[v - 1];
+          const T e = v == V - 1 ? (le ? es[u] : esh) : zc[v + 1];
+          if (OP == 0) {
+            const T r = bv[u][v] - a0[v] * w - a2[v] * e - b0 * sv[u][v] - b2 * nv[u][v] - cm * zm[v] - cp * xn[u][v];
+            ov[v] = (ZU ? r * inv[v] : omega * r / (a1[v] + b1 + cc)) + (T(1) - omega) * zc[v];
+          } else {
+            const T lap = a0[v] * w + a2[v] * e + b0 * sv[u][v] + b2 * nv[u][v] + cm * zm[v] + cp * xn[u][v] +
+                          (a1[v] + b1 + cc) * zc[v];
+            ov[v] = bv[u][v] - lap;
+          }
+        }
+        if (act) vstore(out + p + u * nxy, ov);
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      xm[v] = U >= 2 ? xn[U - 2][v] : xc[v];
+      xc[v] = xn[U - 1][v];
+    }
+    p += U * nxy;
+  }
+}
+
+// MODE 0: one damped-Jacobi sweep  dst = omega (A - offdiag src) / diag + (1 - omega) src
+// MODE 1: the init sweep           dst = omega A / diag
+// MODE 2: copy                     C = B
+// flip selects the buffers: sweep 0: B -> C, 1: C -> B; init: destination 0 = B, 1 = C
+template <typename T, int MODE>
+__global__ void __launch_bounds__(ENT) k_lv_smooth(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+                                                   int nj, int ntiles, T omega, int flip) {
+  constexpr int U = Ublk<T>::U;
+  constexpr int V = VecT<T>::W;
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const LevelJob<T>& J = jobs[q];
+    if (e_halted(J.sc)) continue;
+    const Geom g = J.g;
+    const int vw = J.vw;
+    int i, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i, j, k0, k1, vw);
+    const bool act = i <= g.n1 && j <= g.n2;
+    if (MODE == 0) {
+      const T* src = flip ? J.C : J.B;
+      T* dst = flip ? J.B : J.C;
+      if (vw > 1) {  // every lane walks (shuffles); inactive lanes load and store nothing
+        if (J.zuni)
+          march7v<T, 0, 2, true>(g, i, j, k0, k1, act, J.cdg[0], J.cdg[1], J.cdg[2], omega, J.A, src, dst);
+        else
+          march7v<T, 0, 2, false>(g, i, j, k0, k1, act, J.cdg[0], J.cdg[1], J.cdg[2], omega, J.A, src, dst);
+      } else if (act) {
+        if (J.zuni)
+          march7<T, 0, U, true>(g, i, j, k0, k1, J.cdg[0], J.cdg[1], J.cdg[2], omega, J.A, src, dst);
+        else
+          march7<T, 0, U, false>(g, i, j, k0, k1, J.cdg[0], J.cdg[1], J.cdg[2], omega, J.A, src, dst);
+      }
+      continue;
+    }
+    if (!act) continue;
+    long long p = off(g, i, j, k0);
+    const long long nxy = g.nxy;
+    if (MODE == 2) {
+      const T* __restrict__ src = J.B;
+      T* __restrict__ dst = J.C;
+      if (vw > 1) {
+        int k = k0;
+        for (; k + 3 <= k1; k += 4, p += 4 * nxy) {
+          T v[4][V];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) vload(src + p + u * nxy, v[u]);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) vstore(dst + p + u * nxy, v[u]);
+        }
+        for (; k <= k1; ++k, p += nxy) {
+          T v[V];
+          vload(src + p, v);
+          vstore(dst + p, v);
+        }
+      } else {
+        int k = k0;
+        for (; k + 2 * U - 1 <= k1; k += 2 * U, p += 2 * U * nxy) {
+          T v[2 * U];
+#pragma unroll
+          for (int u = 0; u < 2 * U; ++u) v[u] = src[p + u * nxy];
+#pragma unroll
+          for (int u = 0; u < 2 * U; ++u) dst[p + u * nxy] = v[u];
+        }
+        for (; k <= k1; ++k, p += nxy) dst[p] = src[p];
+      }
+      continue;
+    }
+    const T b1 = J.cdg[1][3 * (j - 1) + 1];
+    const T* __restrict__ c3 = J.cdg[2];
+    const T* __restrict__ bb = J.A;
+    T* __restrict__ dst = flip ? J.C : J.B;
+    const bool zu = J.zuni != 0;
+    if (vw > 1) {
+      T a1[V], inv[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        a1[v] = J.cdg[0][3 * (i - 1 + v) + 1];
+        inv[v] = omega / (a1[v] + b1 + c3[1]);  // uniform z: omega / diag of the whole column
+      }
+      int k = k0;
+      for (; k + 3 <= k1; k += 4, p += 4 * nxy) {
+        T v[4][V];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) vload(bb + p + u * nxy, v[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+#pragma unroll
+          for (int c = 0; c < V; ++c)
+            v[u][c] = zu ? v[u][c] * inv[c] : omega * v[u][c] / (a1[c] + b1 + c3[3 * (k + u - 1) + 1]);
+          vstore(dst + p + u * nxy, v[u]);
+        }
+      }
+      for (; k <= k1; ++k, p += nxy) {
+        T v[V];
+        vload(bb + p, v);
+#pragma unroll
+        for (int c = 0; c < V; ++c) v[c] = zu ? v[c] * inv[c] : omega * v[c] / (a1[c] + b1 + c3[3 * (k - 1) + 1]);
+        vstore(dst + p, v);
+      }
+      continue;
+    }
+    const T a1 = J.cdg[0][3 * (i - 1) + 1];
+    const T inv = omega / (a1 + b1 + c3[1]);
+    int k = k0;
+    for (; k + 2 * U - 1 <= k1; k += 2 * U, p += 2 * U * nxy) {
+      T v[2 * U];
+#pragma unroll
+      for (int u = 0; u < 2 * U; ++u) v[u] = bb[p + u * nxy];
+#pragma unroll
+      for (int u = 0; u < 2 * U; ++u)
+        dst[p + u * nxy] = zu ? v[u] * inv : omega * v[u] / (a1 + b1 + c3[3 * (k + u - 1) + 1]);
+    }
+    for (; k <= k1; ++k, p += nxy) dst[p] = zu ? bb[p] * inv : omega * bb[p] / (a1 + b1 + c3[3 * (k - 1) + 1]);
+  }
+}
+
+// C = A - cdg(B): the residual that restrict forms as fine1 - fine2 (fine2 = product_div_grad_relax)
+template <typename T>
+__global__ void __launch_bounds__(ENT) k_lv_resid(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+                                                  int nj, int ntiles) {
+  constexpr int U = Ublk<T>::U;
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const LevelJob<T>& J = jobs[q];
+    if (e_halted(J.sc)) continue;
+    const Geom g = J.g;
+    int i, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i, j, k0, k1, J.vw);
+    const bool act = i <= g.n1 && j <= g.n2;
+    if (J.vw > 1) {
+      if (J.zuni)
+        march7v<T, 1, 2, true>(g, i, j, k0, k1, act, J.cdg[0], J.cdg[1], J.cdg[2], T(0), J.A, J.B, J.C);
+      else
+        march7v<T, 1, 2, false>(g, i, j, k0, k1, act, J.cdg[0], J.cdg[1], J.cdg[2], T(0), J.A, J.B, J.C);
+      continue;
+    }
+    if (!act) continue;
+    if (J.zuni)
+      march7<T, 1, U, true>(g, i, j, k0, k1, J.cdg[0], J.cdg[1], J.cdg[2], T(0), J.A, J.B, J.C);
+    else
+      march7<T, 1, U, false>(g, i, j, k0, k1, J.cdg[0], J.cdg[1], J.cdg[2], T(0), J.A, J.B, J.C);
+  }
+}
+
+// this (coarse) level: A(ii,jj,kk) = (1.5 d(c) + sum over the six fine neighbours of 1/4 d) / 3
+template <typename T>
+__global__ void __launch_bounds__(ENT) k_lv_restrict(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+                                                     int nj, int ntiles) {
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const LevelJob<T>& J = jobs[q];
+    if (e_halted(J.sc)) continue;
+    const Geom g = J.g;
+    int i0, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i0, j, k0, k1, J.vw);
+    for (int i = i0; i < i0 + J.vw; ++i) {
+    if (i > g.n1 || j > g.n2) continue;
+    const Geom gf = J.gf;
+    const T* __restrict__ d = J.Cf;
+    T* __restrict__ coarse = const_cast<T*>(J.A);
+    const int fi = J.rf[0] * (i - 1) + 1, fj = J.rf[1] * (j - 1) + 1;
+    const int fim = wrapi(fi - 1, gf.n1), fip = wrapi(fi + 1, gf.n1);
+    const int fjm = wrapi(fj - 1, gf.n2), fjp = wrapi(fj + 1, gf.n2);
+    const T cm = T(1) / T(4), c0 = T(2) / T(4), cp = T(1) / T(4);
+    for (int k = k0; k <= k1; ++k) {
+      const int fk = J.rf[2] * (k - 1) + 1;
+      const T v = (c0 + c0 + c0) * d[off(gf, fi, fj, fk)] + cm * d[off(gf, fim, fj, fk)] + cp * d[off(gf, fip, fj, fk)] +
+                  cm * d[off(gf, fi, fjm, fk)] + cp * d[off(gf, fi, fjp, fk)] +
+                  cm * d[off(gf, fi, fj, wrapi(fk - 1, gf.n3))] + cp * d[off(gf, fi, fj, wrapi(fk + 1, gf.n3))];
+      coarse[off(g, i, j, k)] = v / T(3);
+    }
+    }
+  }
+}
+
+// coarse indices bracketing fine index q (lo == hi for coincident points)
+__device__ __forceinline__ void bracket(int q, int r, int nc, int& lo, int& hi, bool& mid) {
+  if (r == 1) {
+    lo = hi = q;
+    mid = false;
+  } else if (q & 1) {
+    lo = hi = (q - 1) / 2 + 1;
+    mid = false;
+  } else {
+    lo = q / 2;
+    hi = q / 2 + 1 > nc ? 1 : q / 2 + 1;
+    mid = true;
+  }
+}
+
+// V consecutive fine columns i .. i+V-1 of B += P Bc, per fine point exactly as the sequential
+// z, y, x passes would (z weights first, then y, then x).  Every column keeps the four (x, y)
+// corner values of the two most recent coarse planes in registers, so consecutive fine planes
+// reuse them; with V > 1 the fine values move as 16-byte vectors.
+template <typename T, int V>
+__device__ __forceinline__ void prolong_cols(const LevelJob<T>& J, const Geom& g, int i, int j, int k0, int k1) {
+  const Geom gc = J.gc;
+  const T* __restrict__ coarse = J.Bc;
+  const T* __restrict__ cI3 = J.cI[2];
+  T* __restrict__ fine = J.B;
+  int yl, yh;
+  bool my;
+  bracket(j, J.rc[1], gc.n2, yl, yh, my);
+  const T wy0 = J.cI[1][2 * j], wy1 = J.cI[1][2 * j + 1];
+  bool mx[V];
+  T wx0[V], wx1[V];
+  int o[V][4];  // corners (xl,yl), (xl,yh), (xh,yl), (xh,yh) of each column in coarse plane 0
+  const T* __restrict__ c0 = coarse + off(gc, 0, 0, 0);
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    int xl, xh;
+    bracket(i + v, J.rc[0], gc.n1, xl, xh, mx[v]);
+    wx0[v] = J.cI[0][2 * (i + v)];
+    wx1[v] = J.cI[0][2 * (i + v) + 1];
+    o[v][0] = xl + gc.nx * yl;
+    o[v][1] = xl + gc.nx * yh;
+    o[v][2] = xh + gc.nx * yl;
+    o[v][3] = xh + gc.nx * yh;
+  }
+  // coarse planes zl (P0) and zl + 1 (P1) of the current fine plane, kept while k advances
+  int zcur = -1;
+  bool have1 = false;
+  T P0[V][4], P1[V][4];
+  auto load = [&](int z, T (&w)[V][4]) {
+    const T* __restrict__ cz = c0 + (long long)z * gc.nxy;
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) w[v][c] = cz[o[v][c]];
+  };
+  long long p = off(g, i, j, k0);
+  for (int k = k0; k <= k1; ++k, p += g.nxy) {
+    int zl, zh;
+    bool mz;
+    bracket(k, J.rc[2], gc.n3, zl, zh, mz);
+    if (zl != zcur) {
+      const int nxt = zcur + 1 > gc.n3 ? 1 : zcur + 1;
+      if (zcur >= 0 && have1 && zl == nxt) {
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) P0[v][c] = P1[v][c];
+      } else {
+        load(zl, P0);
+      }
+      zcur = zl;
+      have1 = false;
+    }
+    if (mz && !have1) {
+      load(zh, P1);
+      have1 = true;
+    }
+    const T wz0 = cI3[2 * k], wz1 = cI3[2 * k + 1];
+    T f[V];
+    if constexpr (V > 1)
+      vload(fine + p, f);
+    else
+      f[0] = fine[p];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      T Z[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) Z[c] = mz ? wz0 * P0[v][c] + wz1 * P1[v][c] : P0[v][c];
+      const T Yl = my ? wy0 * Z[0] + wy1 * Z[1] : Z[0];  // x = xl
+      const T Yh = my ? wy0 * Z[2] + wy1 * Z[3] : Z[2];  // x = xh
+      f[v] = f[v] + (mx[v] ? wx0[v] * Yl + wx1[v] * Yh : Yl);
+    }
+    if constexpr (V > 1)
+      vstore(fine + p, f);
+    else
+      fine[p] = f[0];
+  }
+}
+
+// this (fine) level: B += P Bc (interpolate, mod_solvers.f90:955-1141)
+template <typename T>
+__global__ void __launch_bounds__(ENT) k_lv_prolong(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+                                                    int nj, int ntiles) {
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const LevelJob<T>& J = jobs[q];
+    if (e_halted(J.sc)) continue;
+    const Geom g = J.g;
+    int i, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i, j, k0, k1, J.vw);
+    if (i > g.n1 || j > g.n2) continue;
+    if (J.vw > 1)
+      prolong_cols<T, VecT<T>::W>(J, g, i, j, k0, k1);
+    else
+      prolong_cols<T, 1>(J, g, i, j, k0, k1);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// mixed precision: FP64 residual / conversion / correction over the MixJob list
+// ------------------------------------------------------------------------------------------
+// r64 = bb - r64 (r64 = A x on entry); partials [max|r|, sum r^2, sum bb^2]
+__global__ void __launch_bounds__(ENT) k_mx_res(const MixJob* __restrict__ jobs, const int* __restrict__ ts, int nj,
+                                                int ntiles, const SolverScalars* __restrict__ osc,
+                                                double* __restrict__ partial) {
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    if (osc[q].done) continue;
+    const MixJob& J = jobs[q];
+    const Geom g = J.g;
+    int i, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
+    double v[3] = {0.0, 0.0, 0.0};
+    if (i <= g.n1 && j <= g.n2) {
+      const double* __restrict__ bb = J.bb;
+      double* __restrict__ r64 = J.r64;
+      long long p = off(g, i, j, k0);
+      for (int k = k0; k <= k1; ++k, p += g.nxy) {
+        const double bv = bb[p];
+        const double r = bv - r64[p];
+        r64[p] = r;
+        v[0] = fmax(v[0], fabs(r));
+        v[1] += r * r;
+        v[2] += bv * bv;
+      }
+    }
+    tile_partials<3, 1>(v, partial + (long long)b * 4);
+  }
+}
+// r32 = (float)(r64 / |r|_inf): the inner right-hand side normalised to |r|_inf = 1
+__global__ void __launch_bounds__(ENT) k_mx_tof32(const MixJob* __restrict__ jobs, const int* __restrict__ ts, int nj,
+                                                  int ntiles, const SolverScalars* __restrict__ osc) {
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    if (osc[q].done) continue;
+    const MixJob& J = jobs[q];
+    const Geom g = J.g;
+    int i, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
+    if (i > g.n1 || j > g.n2) continue;
+    const double scale = 1.0 / J.q[0];
+    const double* __restrict__ r64 = J.r64;
+    float* __restrict__ r32 = J.r32;
+    long long p = off(g, i, j, k0);
+#pragma unroll 4
+    for (int k = k0; k <= k1; ++k, p += g.nxy) r32[p] = (float)(r64[p] * scale);
+  }
+}
+// x += |r|_inf e for the cases whose inner solve ended with status 0 or 1
+__global__ void __launch_bounds__(ENT) k_mx_apply(const MixJob* __restrict__ jobs, const int* __restrict__ ts, int nj,
+                                                  int ntiles, const SolverScalars* __restrict__ osc) {
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    if (osc[q].done) continue;
+    const MixJob& J = jobs[q];
+    const int st = J.isc->status;
+    if (st != 0 && st != 1) continue;
+    const Geom g = J.g;
+    int i, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
+    if (i > g.n1 || j > g.n2) continue;
+    const double unscale = J.q[0];
+    const float* __restrict__ e = J.e32;
+    double* __restrict__ x = J.x;
+    long long p = off(g, i, j, k0);
+#pragma unroll 4
+    for (int k = k0; k <= k1; ++k, p += g.nxy) x[p] = x[p] + unscale * (double)e[p];
+  }
+}
+
+// the operator kernels use more than 48 KB of dynamic shared memory: opt in once per process
+// and device
+void ax_attributes() {
+  static bool done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || done[dev]) return;
+  cudaFuncSetAttribute(k_kr_ax<float, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<float>());
+  cudaFuncSetAttribute(k_kr_ax<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<float>());
+  cudaFuncSetAttribute(k_kr_ax<float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<float>());
+  cudaFuncSetAttribute(k_kr_ax<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
+  cudaFuncSetAttribute(k_kr_ax<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
+  cudaFuncSetAttribute(k_kr_ax<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
+  done[dev] = true;
+}
+
+int g_sms = 0;
+inline int grid_for(int ntiles) {
+  if (g_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sms <= 0) g_sms = 148;
+  }
+  const int cap = g_sms * 8;
+  return ntiles < cap ? ntiles : cap;
+}
+const dim3 kBlock(ETX, ETY);
+
+}  // namespace
+
+// =========================================================================================
+// host side
+// =========================================================================================
+void collapse_divgrad(int M, const double* cG, const double* cD, std::vector<double>& W) {
+  const int n = M - 1;
+  W.assign((size_t)n * AXW, 0.0);
+  auto wrap = [n](int q) { return q < 1 ? q + n : (q > n ? q - n : q); };
+  for (int i = 1; i <= n; ++i)
+    for (int o = -5; o <= 5; ++o) {
+      double s = 0.0;
+      for (int a = -3; a <= 2; ++a) {
+        const int bq = o - a;
+        if (bq < -2 || bq > 3) continue;
+        s += cD[(size_t)i * 6 + (a + 3)] * cG[(size_t)wrap(i + a) * 6 + (bq + 2)];
+      }
+      W[(size_t)(i - 1) * AXW + (o + 5)] = s;
+    }
+}
+
+template <typename J>
+int ListArena::add(const std::vector<J>& jobs, const std::vector<int>& tiles) {
+  auto align = [this](size_t a) {
+    while (host.size() % a) host.push_back(0);
+  };
+  DevList L;
+  L.njobs = (int)jobs.size();
+  align(16);
+  ts_off.push_back(host.size());
+  int acc = 0;
+  std::vector<int> ts(jobs.size() + 1);
+  for (size_t q = 0; q < jobs.size(); ++q) {
+    ts[q] = acc;
+    acc += tiles[q];
+  }
+  ts[jobs.size()] = acc;
+  L.ntiles = acc;
+  const unsigned char* tb = reinterpret_cast<const unsigned char*>(ts.data());
+  host.insert(host.end(), tb, tb + ts.size() * sizeof(int));
+  align(16);
+  job_off.push_back(host.size());
+  const unsigned char* jb = reinterpret_cast<const unsigned char*>(jobs.data());
+  host.insert(host.end(), jb, jb + jobs.size() * sizeof(J));
+  lists.push_back(L);
+  return (int)lists.size() - 1;
+}
+
+int ListArena::upload(cudaStream_t s) {
+  if (dev) {
+    cudaFree(dev);
+    dev = nullptr;
+  }
+  if (host.empty()) return 0;
+  cudaError_t e = cudaMalloc((void**)&dev, host.size());
+  if (e != cudaSuccess) return impact_set_error(e, "cudaMalloc (job lists)", __FILE__, __LINE__);
+  e = cudaMemcpyAsync(dev, host.data(), host.size(), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return impact_set_error(e, "job list upload", __FILE__, __LINE__);
+  for (size_t q = 0; q < lists.size(); ++q) {
+    lists[q].ts = reinterpret_cast<const int*>(dev + ts_off[q]);
+    lists[q].jobs = dev + job_off[q];
+  }
+  return 0;
+}
+
+void ListArena::release() {
+  if (dev) cudaFree(dev);
+  dev = nullptr;
+  host.clear();
+  lists.clear();
+  ts_off.clear();
+  job_off.clear();
+}
+
+template <typename T>
+void Engine<T>::release() {
+  if (graph_) cudaGraphExecDestroy(graph_);
+  graph_ = nullptr;
+  arena_.release();
+  if (partial_) cudaFree(partial_);
+  if (scal_) cudaFree(scal_);
+  if (scal_host_) cudaFreeHost(scal_host_);
+  partial_ = nullptr;
+  scal_ = nullptr;
+  scal_host_ = nullptr;
+  vc_[0].clear();
+  vc_[1].clear();
+  cells_.clear();
+  cells_f_.clear();
+  cells_c_.clear();
+  cs_.clear();
+  built_ = false;
+}
+
+template <typename T>
+void Engine<T>::smooth(std::vector<Phase>& out, int list, int init, int sweeps) {
+  if (sweeps <= 0) return;
+  // targets alternate so that the last write lands in B; the first write may not read its target
+  int tgt = (sweeps % 2 == 1) ? 0 : 1;
+  int src = 0;
+  int w = 0;
+  if (init) {
+    out.push_back({PH_INIT, list, tgt});
+    src = tgt;
+    tgt ^= 1;
+    ++w;
+  } else if (tgt == 0) {  // odd number of plain sweeps: stage the start in C first
+    out.push_back({PH_COPY, list, 0});
+    src = 1;
+  }
+  for (; w < sweeps; ++w) {
+    out.push_back({PH_SWEEP, list, src});
+    src = tgt;
+    tgt ^= 1;
+  }
+}
+
+template <typename T>
+int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p, cudaStream_t s) {
+  release();
+  ax_attributes();
+  cs_ = cs;
+  p_ = p;
+  p_.kc = std::max(1, std::min(KC_MAX, p.kc));
+  s_ = s;
+  const int n = (int)cs.size();
+  if (n == 0) return impact_set_error_msg(-1, "engine: no cases");
+  const bool use_mg = p_.precond == 1;
+  if (use_mg)
+    for (const auto& c : cs)
+      if (!c.mg || c.mg->n < 1) return impact_set_error_msg(-1, "engine: multigrid requested for a case without hierarchy");
+  const bool pre_on = use_mg || p_.n_sweeps > 0;
+  const int kc = p_.kc;
+  cudaError_t e = cudaMalloc((void**)&scal_, n * sizeof(SolverScalars));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&scal_host_, n * sizeof(SolverScalars));
+  long long tiles_fine = 0;
+  for (const auto& c : cs) tiles_fine += tiles_of(c.g, kc);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&partial_, (size_t)(tiles_fine * 4 + 64) * sizeof(double));
+  if (e != cudaSuccess) {
+    release();
+    return impact_set_error(e, "engine allocation", __FILE__, __LINE__);
+  }
+  cudaMemsetAsync(scal_, 0, n * sizeof(SolverScalars), s);
+  // ---- Krylov list ----
+  {
+    std::vector<KrylovJob<T>> kj(n);
+    std::vector<int> kt(n);
+    for (int c = 0; c < n; ++c) {
+      KrylovJob<T>& J = kj[c];
+      const EngineCase<T>& C = cs[c];
+      J = KrylovJob<T>{};
+      J.g = C.g;
+      J.kc = kc;
+      for (int m = 0; m < 3; ++m) J.W[m] = C.W[m];
+      J.zuni = C.zuni;
+      J.bb = C.bb;
+      J.phi = C.phi;
+      J.rr = C.rr;
+      J.rh = C.rh;
+      J.pp = C.pp;
+      J.Ap = C.Ap;
+      J.Ar = C.Ar;
+      J.z1 = pre_on ? C.z1 : C.pp;
+      J.z2 = pre_on ? C.z2 : C.rr;
+      J.sc = scal_ + c;
+      kt[c] = tiles_of(C.g, kc);
+    }
+    kr_list_ = arena_.add(kj, kt);
+  }
+  // ---- preconditioner schedules ----
+  auto lvjob = [&](int c, int g, int variant) {
+    const EngineCase<T>& C = cs[c];
+    LevelJob<T> J{};
+    const MGData<T>* mg = (C.mg && C.mg->n > 0) ? C.mg : nullptr;
+    if (mg) {
+      const MGLevel<T>& L = mg->lv[g];
+      J.g = L.g;
+      J.zuni = L.zuni;
+      for (int m = 0; m < 3; ++m) J.cdg[m] = L.cdg[m];
+    } else {
+      J.g = C.g;
+      J.zuni = C.cdg_zuni;
+      for (int m = 0; m < 3; ++m) J.cdg[m] = C.cdg[m];
+    }
+    J.kc = kc;
+    J.vw = (J.g.n1 % VecT<T>::W == 0) ? VecT<T>::W : 1;
+    if (g == 0) {
+      J.A = variant ? C.rr : C.pp;
+      J.B = variant ? C.z2 : C.z1;
+      J.C = C.comp;
+    } else {
+      J.A = mg->lv[g].A;
+      J.B = mg->lv[g].B;
+      J.C = mg->lv[g].C;
+      const MGLevel<T>& F = mg->lv[g - 1];
+      J.gf = F.g;
+      for (int m = 0; m < 3; ++m) J.rf[m] = F.ratio[m];
+      J.Cf = (g - 1 == 0) ? C.comp : F.C;
+    }
+    if (mg && g + 1 < mg->n) {
+      const MGLevel<T>& L = mg->lv[g];
+      const MGLevel<T>& Cc = mg->lv[g + 1];
+      J.gc = Cc.g;
+      for (int m = 0; m < 3; ++m) {
+        J.rc[m] = L.ratio[m];
+        J.cI[m] = L.cI[m];
+      }
+      J.Bc = Cc.B;
+    }
+    J.sc = scal_ + c;
+    return J;
+  };
+  auto vol = [](const Geom& g) { return (double)g.n1 * g.n2 * g.n3; };
+  auto note = [&](int list, double c, double f, double cc) {
+    cells_.resize(list + 1, 0.0);
+    cells_f_.resize(list + 1, 0.0);
+    cells_c_.resize(list + 1, 0.0);
+    cells_[list] = c;
+    cells_f_[list] = f;
+    cells_c_[list] = cc;
+  };
+  {
+    double c = 0.0;
+    for (const auto& C : cs) c += vol(C.g);
+    note(kr_list_, c, 0.0, 0.0);
+  }
+  // vec: allow several columns per thread (lists walked by the smoothing and residual kernels);
+  // the restriction lists keep one column per thread
+  auto add_list = [&](const std::vector<std::pair<int, int>>& members, int variant, bool vec = true) {
+    std::vector<LevelJob<T>> jobs;
+    std::vector<int> tiles;
+    double c = 0.0, f = 0.0, cc = 0.0;
+    for (auto& m : members) {
+      jobs.push_back(lvjob(m.first, m.second, variant));
+      if (!vec) jobs.back().vw = 1;
+      const LevelJob<T>& J = jobs.back();
+      tiles.push_back(tiles_of(J.g, kc, J.vw));
+      c += vol(J.g);
+      if (J.Cf) f += vol(J.gf);
+      if (J.Bc) cc += vol(J.gc);
+    }
+    const int id = arena_.add(jobs, tiles);
+    note(id, c, f, cc);
+    return id;
+  };
+  std::vector<int> nlev(n, 1);
+  int gmax = 1;
+  for (int c = 0; c < n; ++c) {
+    nlev[c] = (use_mg && cs[c].mg) ? cs[c].mg->n : 1;
+    gmax = std::max(gmax, nlev[c]);
+  }
+  if (use_mg) {
+    // level >= 1 lists are shared by both schedules
+    std::vector<int> down(gmax, -1), rs(gmax, -1);
+    for (int g = 1; g + 1 < gmax; ++g) {
+      std::vector<std::pair<int, int>> m;
+      for (int c = 0; c < n; ++c)
+        if (nlev[c] >= g + 2) m.push_back({c, g});
+      down[g] = add_list(m, 0);
+    }
+    for (int g = 1; g < gmax; ++g) {
+      std::vector<std::pair<int, int>> m;
+      for (int c = 0; c < n; ++c)
+        if (nlev[c] >= g + 1) m.push_back({c, g});
+      rs[g] = add_list(m, 0, false);
+    }
+    for (int v = 0; v < 2; ++v) {
+      std::vector<std::pair<int, int>> m0, bot;
+      for (int c = 0; c < n; ++c) {
+        if (nlev[c] >= 2) m0.push_back({c, 0});
+        bot.push_back({c, nlev[c] - 1});
+      }
+      const int down0 = add_list(m0, v);
+      const int botl = add_list(bot, v);
+      if (v == 0) {
+        down0_ = down0;
+        rs1_ = gmax > 1 ? rs[1] : -1;
+      }
+      std::vector<Phase>& sch = vc_[v];
+      for (int g = 0; g + 1 < gmax; ++g) {  // relax_restrict
+        const int D = g == 0 ? down0 : down[g];
+        smooth(sch, D, 1, p_.mg_down);
+        sch.push_back({PH_RESID, D, 0});
+        sch.push_back({PH_RESTRICT, rs[g + 1], 0});
+      }
+      smooth(sch, botl, 1, p_.mg_bottom);  // relax_bottom
+      smooth(sch, botl, 0, p_.mg_bottom);
+      for (int g = gmax - 2; g >= 0; --g) {  // interpolate_relax
+        const int D = g == 0 ? down0 : down[g];
+        sch.push_back({PH_PROLONG, D, 0});
+        smooth(sch, D, 0, p_.mg_up);
+      }
+    }
+  } else if (p_.n_sweeps > 0) {
+    for (int v = 0; v < 2; ++v) {
+      std::vector<std::pair<int, int>> m0;
+      for (int c = 0; c < n; ++c) m0.push_back({c, 0});
+      const int l0 = add_list(m0, v);
+      if (v == 0) down0_ = l0;
+      smooth(vc_[v], l0, 1, p_.n_sweeps);
+    }
+  }
+  int rc = arena_.upload(s);
+  if (rc) {
+    release();
+    return rc;
+  }
+  // launches per iteration (for the launch counter under graph replay)
+  long long l = 9;
+  for (int v = 0; v < 2; ++v)
+    for (const Phase& ph : vc_[v])
+      if (arena_.lists[ph.list].ntiles > 0) ++l;
+  launches_iter_ = l;
+  built_ = true;
+  return 0;
+}
+
+template <typename T>
+void Engine<T>::enqueue_phase(const Phase& ph) {
+  const DevList& L = arena_.lists[ph.list];
+  if (L.ntiles == 0) return;
+  const LevelJob<T>* J = static_cast<const LevelJob<T>*>(L.jobs);
+  const int grid = grid_for(L.ntiles);
+  const T om = (T)p_.omega;
+  cudaStream_t s = s_;
+  const double sz = sizeof(T), c = cells_[ph.list], cf = cells_f_[ph.list], cc = cells_c_[ph.list];
+  switch (ph.kind) {
+    case PH_INIT:
+      IMPACT_PROF(prof::K_MG_INIT, 2 * sz * c, s, (k_lv_smooth<T, 1><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles, om, ph.flip)));
+      break;
+    case PH_SWEEP:
+      IMPACT_PROF(prof::K_MG_SWEEP, 3 * sz * c, s, (k_lv_smooth<T, 0><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles, om, ph.flip)));
+      break;
+    case PH_COPY:
+      IMPACT_PROF(prof::K_MG_OTHER, 2 * sz * c, s, (k_lv_smooth<T, 2><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles, om, 0)));
+      break;
+    case PH_RESID:
+      IMPACT_PROF(prof::K_MG_RESID, 3 * sz * c, s, (k_lv_resid<T><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles)));
+      break;
+    case PH_RESTRICT:
+      IMPACT_PROF(prof::K_MG_OTHER, sz * (c + cf), s, (k_lv_restrict<T><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles)));
+      break;
+    case PH_PROLONG:
+      IMPACT_PROF(prof::K_MG_OTHER, sz * (2 * c + cc), s, (k_lv_prolong<T><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles)));
+      break;
+    default:
+      break;
+  }
+}
+
+template <typename T>
+void Engine<T>::enqueue_precond(int variant) {
+  for (const Phase& ph : vc_[variant]) enqueue_phase(ph);
+}
+
+template <typename T>
+void Engine<T>::enqueue_iteration() {
+  const DevList& K = arena_.lists[kr_list_];
+  const KrylovJob<T>* J = static_cast<const KrylovJob<T>*>(K.jobs);
+  const int n = K.njobs;
+  const int grid = grid_for(K.ntiles);
+  cudaStream_t s = s_;
+  const double fb = sizeof(T) * cells_[kr_list_];
+  k_ebegin<<<(n + 31) / 32, 32, 0, s>>>(scal_, n);
+  prof::count(1);
+  IMPACT_PROF(prof::K_P_UPDATE, 4 * fb, s, (k_kr_p<T><<<grid, kBlock, 0, s>>>(J, K.ts, n, K.ntiles)));
+  enqueue_precond(0);
+  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (k_kr_ax<T, 1><<<grid, kBlock, ax_smem_bytes<T>(), s>>>(J, K.ts, n, K.ntiles, partial_)));
+  k_efin<<<n, 256, 0, s>>>(K.ts, partial_, 1, 0, EFIN_ALPHA, scal_, nullptr);
+  IMPACT_PROF(prof::K_R_UPDATE, 3 * fb, s, (k_kr_r<T><<<grid, kBlock, 0, s>>>(J, K.ts, n, K.ntiles)));
+  enqueue_precond(1);
+  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (k_kr_ax<T, 2><<<grid, kBlock, ax_smem_bytes<T>(), s>>>(J, K.ts, n, K.ntiles, partial_)));
+  k_efin<<<n, 256, 0, s>>>(K.ts, partial_, 2, 0, EFIN_OMEGA, scal_, nullptr);
+  IMPACT_PROF(prof::K_X_UPDATE, 8 * fb, s, (k_kr_x<T><<<grid, kBlock, 0, s>>>(J, K.ts, n, K.ntiles, partial_)));
+  k_efin<<<n, 256, 0, s>>>(K.ts, partial_, 3, 1, EFIN_NORMS, scal_, nullptr);
+  prof::count(3);
+}
+
+template <typename T>
+int Engine<T>::poll(bool& all_done) {
+  const int n = (int)cs_.size();
+  cudaError_t e = cudaMemcpyAsync(scal_host_, scal_, n * sizeof(SolverScalars), cudaMemcpyDeviceToHost, s_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s_);
+  if (e != cudaSuccess) return impact_set_error(e, "engine poll", __FILE__, __LINE__);
+  prof::flush();
+  all_done = true;
+  for (int c = 0; c < n; ++c) {
+    const SolverScalars& h = scal_host_[c];
+    if (!(h.done || (h.status != 0 && h.status != 4))) all_done = false;
+  }
+  return 0;
+}
+
+template <typename T>
+int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::vector<SolverResult>& res) {
+  if (!built_) return impact_set_error_msg(-1, "engine: not built");
+  const int n = (int)cs_.size();
+  if ((int)init.size() != n) return impact_set_error_msg(-1, "engine: wrong number of initial scalars");
+  int max_it = 0;
+  for (int c = 0; c < n; ++c) {
+    scal_host_[c] = init[c];
+    scal_host_[c].it = 0;
+    scal_host_[c].status = 0;
+    if (!init[c].done) max_it = std::max(max_it, init[c].max_it);
+  }
+  cudaError_t e = cudaMemcpyAsync(scal_, scal_host_, n * sizeof(SolverScalars), cudaMemcpyHostToDevice, s_);
+  if (e != cudaSuccess) return impact_set_error(e, "engine scalars", __FILE__, __LINE__);
+  const DevList& K = arena_.lists[kr_list_];
+  const KrylovJob<T>* J = static_cast<const KrylovJob<T>*>(K.jobs);
+  const int grid = grid_for(K.ntiles);
+  if (!zero_phi) {
+    k_kr_ax<T, 0><<<grid, kBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_);
+    prof::count(1);
+  }
+  k_kr_init<T><<<grid, kBlock, 0, s_>>>(J, K.ts, n, K.ntiles, zero_phi, partial_);
+  k_efin<<<n, 256, 0, s_>>>(K.ts, partial_, 4, 1, EFIN_INIT, scal_, nullptr);
+  prof::count(2);
+  const int chunk = p_.check_every > 0 ? p_.check_every : 1;
+  const bool graphs = p_.use_graph && !prof::enabled();
+  if (graphs && !graph_) {
+    cudaGraph_t gr = nullptr;
+    e = cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      for (int t = 0; t < chunk; ++t) enqueue_iteration();
+      e = cudaStreamEndCapture(s_, &gr);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&graph_, gr, 0);
+    if (gr) cudaGraphDestroy(gr);
+    if (e != cudaSuccess) {  // capture unavailable on this stream: launch directly from now on
+      cudaGetLastError();
+      graph_ = nullptr;
+      p_.use_graph = 0;
+    }
+    prof::count(-(long long)chunk * launches_iter_);  // the capture counted launches that did not run
+  }
+  int launched = 0;
+  for (;;) {
+    if (graph_ && p_.use_graph && !prof::enabled()) {
+      e = cudaGraphLaunch(graph_, s_);
+      if (e != cudaSuccess) return impact_set_error(e, "engine graph launch", __FILE__, __LINE__);
+      prof::count((long long)chunk * launches_iter_);
+    } else {
+      for (int t = 0; t < chunk; ++t) enqueue_iteration();
+    }
+    launched += chunk;
+    bool all_done = false;
+    int rc = poll(all_done);
+    if (rc) return rc;
+    bool reset = false;
+    for (int c = 0; c < n; ++c)
+      if (scal_host_[c].status == 4) reset = true;
+    if (reset) {
+      // rhr == 0: new shadow residual rh = rr, as the reference does, then redo the iteration start
+      k_kr_reset<T><<<grid, kBlock, 0, s_>>>(J, K.ts, n, K.ntiles, partial_);
+      k_efin<<<n, 256, 0, s_>>>(K.ts, partial_, 1, 0, EFIN_RESET, scal_, nullptr);
+      prof::count(2);
+      continue;
+    }
+    if (all_done) break;
+    if (launched > max_it + 8) break;  // safety net: the device flags should have stopped it
+  }
+  res.resize(n);
+  for (int c = 0; c < n; ++c) {
+    const SolverScalars& h = scal_host_[c];
+    res[c].iterations = h.it;
+    res[c].status = h.status;
+    res[c].res_inf = h.norm_inf;
+    res[c].res_two = std::sqrt(h.norm_two_sq);
+    res[c].b_two = std::sqrt(h.b_two_sq);
+  }
+  return 0;
+}
+
+template <typename T>
+int Engine<T>::apply_precond() {
+  if (!built_) return impact_set_error_msg(-1, "engine: not built");
+  const int n = (int)cs_.size();
+  for (int c = 0; c < n; ++c) scal_host_[c] = SolverScalars{};
+  cudaError_t e = cudaMemcpyAsync(scal_, scal_host_, n * sizeof(SolverScalars), cudaMemcpyHostToDevice, s_);
+  if (e != cudaSuccess) return impact_set_error(e, "engine scalars", __FILE__, __LINE__);
+  enqueue_precond(0);
+  e = cudaStreamSynchronize(s_);
+  if (e != cudaSuccess) return impact_set_error(e, "engine precond", __FILE__, __LINE__);
+  return 0;
+}
+
+template <typename T>
+int Engine<T>::apply_operator() {
+  if (!built_) return impact_set_error_msg(-1, "engine: not built");
+  const int n = (int)cs_.size();
+  for (int c = 0; c < n; ++c) scal_host_[c] = SolverScalars{};
+  cudaError_t e = cudaMemcpyAsync(scal_, scal_host_, n * sizeof(SolverScalars), cudaMemcpyHostToDevice, s_);
+  if (e != cudaSuccess) return impact_set_error(e, "engine scalars", __FILE__, __LINE__);
+  const DevList& K = arena_.lists[kr_list_];
+  const KrylovJob<T>* J = static_cast<const KrylovJob<T>*>(K.jobs);
+  k_kr_ax<T, 0><<<grid_for(K.ntiles), kBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_);
+  prof::count(1);
+  e = cudaStreamSynchronize(s_);
+  if (e != cudaSuccess) return impact_set_error(e, "engine operator", __FILE__, __LINE__);
+  return 0;
+}
+
+template <typename T>
+int Engine<T>::bench(int kind, int iters, double* ms, double* bytes) {
+  if (!built_) return impact_set_error_msg(-1, "engine: not built");
+  const int n = (int)cs_.size();
+  for (int c = 0; c < n; ++c) {
+    scal_host_[c] = SolverScalars{};
+    scal_host_[c].it = 2;
+    scal_host_[c].max_it = 1 << 30;
+  }
+  cudaError_t e = cudaMemcpyAsync(scal_, scal_host_, n * sizeof(SolverScalars), cudaMemcpyHostToDevice, s_);
+  if (e != cudaSuccess) return impact_set_error(e, "engine scalars", __FILE__, __LINE__);
+  const DevList& K = arena_.lists[kr_list_];
+  const KrylovJob<T>* J = static_cast<const KrylovJob<T>*>(K.jobs);
+  const int grid = grid_for(K.ntiles);
+  const double sz = sizeof(T), fc = cells_[kr_list_];
+  double by = 0.0;
+  std::function<void()> f;
+  auto need = [&](int l) { return l >= 0 && arena_.lists[l].ntiles > 0; };
+  switch (kind) {
+    case 0:
+    case 1:
+    case 2:
+    case 3: {
+      if (!need(down0_)) return impact_set_error_msg(-1, "engine bench: no finest-level list");
+      if (kind == 3 && rs1_ < 0) return impact_set_error_msg(-1, "engine bench: no coarse level");
+      const int kinds[4] = {PH_SWEEP, PH_INIT, PH_RESID, PH_PROLONG};
+      const Phase ph{kinds[kind], down0_, 0};
+      const double c = cells_[down0_];
+      by = kind == 0 || kind == 2 ? 3 * sz * c : (kind == 1 ? 2 * sz * c : sz * (2 * c + cells_c_[down0_]));
+      f = [this, ph]() { enqueue_phase(ph); };
+      break;
+    }
+    case 4: {
+      if (!need(rs1_)) return impact_set_error_msg(-1, "engine bench: no coarse level");
+      const Phase ph{PH_RESTRICT, rs1_, 0};
+      by = sz * (cells_[rs1_] + cells_f_[rs1_]);
+      f = [this, ph]() { enqueue_phase(ph); };
+      break;
+    }
+    case 5:
+      by = 3 * sz * fc;
+      f = [&]() { k_kr_ax<T, 1><<<grid, kBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_); };
+      break;
+    case 6:
+      by = 3 * sz * fc;
+      f = [&]() { k_kr_ax<T, 2><<<grid, kBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_); };
+      break;
+    case 7:
+      by = 8 * sz * fc;
+      f = [&]() { k_kr_x<T><<<grid, kBlock, 0, s_>>>(J, K.ts, n, K.ntiles, partial_); };
+      break;
+    case 8:
+      by = 4 * sz * fc;
+      f = [&]() { k_kr_p<T><<<grid, kBlock, 0, s_>>>(J, K.ts, n, K.ntiles); };
+      break;
+    case 9:
+      by = 3 * sz * fc;
+      f = [&]() { k_kr_r<T><<<grid, kBlock, 0, s_>>>(J, K.ts, n, K.ntiles); };
+      break;
+    case 10:
+      f = [this]() { enqueue_precond(0); };
+      break;
+    case 11:
+      f = [this]() { enqueue_iteration(); };
+      break;
+    default:
+      return impact_set_error_msg(-1, "engine bench: unknown kernel kind");
+  }
+  f();  // warm-up
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, s_);
+  for (int t = 0; t < iters; ++t) f();
+  cudaEventRecord(b, s_);
+  e = cudaEventSynchronize(b);
+  float t_ms = 0.f;
+  cudaEventElapsedTime(&t_ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return impact_set_error(e, "engine bench", __FILE__, __LINE__);
+  *ms = t_ms / iters;
+  *bytes = by;
+  return 0;
+}
+
+template class Engine<double>;
+template class Engine<float>;
+
+// =========================================================================================
+// mixed precision
+// =========================================================================================
+void MixedEngine::release() {
+  inner_.release();
+  arena_.release();
+  if (partial_) cudaFree(partial_);
+  if (q_) cudaFree(q_);
+  if (q_host_) cudaFreeHost(q_host_);
+  if (oscal_) cudaFree(oscal_);
+  partial_ = nullptr;
+  q_ = nullptr;
+  q_host_ = nullptr;
+  oscal_ = nullptr;
+  cs_.clear();
+  built_ = false;
+}
+
+int MixedEngine::build(const std::vector<Case>& cs, const EngineParams& p, cudaStream_t s) {
+  release();
+  cs_ = cs;
+  s_ = s;
+  const int n = (int)cs.size();
+  std::vector<EngineCase<float>> ic;
+  for (const Case& c : cs) ic.push_back(c.inner);
+  int rc = inner_.build(ic, p, s);
+  if (rc) return rc;
+  const int kc = inner_.params().kc;
+  long long tiles = 0;
+  for (const Case& c : cs) tiles += tiles_of(c.g, kc);
+  cudaError_t e = cudaMalloc((void**)&partial_, (size_t)(tiles * 4 + 64) * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&q_, (size_t)n * 4 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&q_host_, (size_t)n * 4 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&oscal_, (size_t)n * sizeof(SolverScalars));
+  if (e != cudaSuccess) {
+    release();
+    return impact_set_error(e, "mixed engine allocation", __FILE__, __LINE__);
+  }
+  cudaMemsetAsync(oscal_, 0, (size_t)n * sizeof(SolverScalars), s);
+  std::vector<KrylovJob<double>> aj(n);
+  std::vector<MixJob> mj(n);
+  std::vector<int> t(n);
+  for (int c = 0; c < n; ++c) {
+    const Case& C = cs[c];
+    KrylovJob<double>& A = aj[c];
+    A = KrylovJob<double>{};
+    A.g = C.g;
+    A.kc = kc;
+    for (int m = 0; m < 3; ++m) A.W[m] = C.W64[m];
+    A.zuni = C.zuni;
+    A.phi = C.x;
+    A.rr = C.r64;
+    A.sc = oscal_ + c;
+    MixJob& M = mj[c];
+    M = MixJob{};
+    M.g = C.g;
+    M.kc = kc;
+    M.bb = C.bb;
+    M.x = C.x;
+    M.r64 = C.r64;
+    M.r32 = C.r32;
+    M.e32 = C.e32;
+    M.q = q_ + 4 * c;
+    M.isc = inner_.scal_dev() + c;
+    t[c] = tiles_of(C.g, kc);
+  }
+  ax_list_ = arena_.add(aj, t);
+  mix_list_ = arena_.add(mj, t);
+  rc = arena_.upload(s);
+  if (rc) {
+    release();
+    return rc;
+  }
+  built_ = true;
+  return 0;
+}
+
+// Iterative refinement (no counterpart in mod_solvers.f90; the FP64 outer loop wraps the
+// reference's BiCGstab run in FP32): r = b - A x in FP64, e ~ A^-1 r by the FP32 engine on the
+// normalised r, x += |r|_inf e.  A case whose inner solve breaks down or turns non-finite has
+// its correction discarded and is retried with a looser tolerance (twice at most).
+int MixedEngine::solve(const std::vector<SolverScalars>& outer, double inner_tol, int inner_max_it, int zero_x,
+                       std::vector<SolverResult>& res, std::vector<int>& inner_its) {
+  if (!built_) return impact_set_error_msg(-1, "mixed engine: not built");
+  const int n = (int)cs_.size();
+  const bool dbg = std::getenv("IMPACT_B200_DEBUG") != nullptr;
+  res.assign(n, SolverResult{});
+  inner_its.assign(n, 0);
+  std::vector<int> done(n, 0), outer_it(n, 0), retries(n, 0);
+  std::vector<SolverScalars> osc(n);
+  for (int c = 0; c < n; ++c) {
+    done[c] = outer[c].done;
+    res[c].status = 1;
+    if (zero_x && !done[c]) cudaMemsetAsync(cs_[c].x, 0, (size_t)cs_[c].g.nfield * sizeof(double), s_);
+  }
+  const DevList& AL = arena_.lists[ax_list_];
+  const DevList& ML = arena_.lists[mix_list_];
+  const KrylovJob<double>* AJ = static_cast<const KrylovJob<double>*>(AL.jobs);
+  const MixJob* MJ = static_cast<const MixJob*>(ML.jobs);
+  const int grid = grid_for(ML.ntiles);
+  auto push_flags = [&]() -> int {
+    for (int c = 0; c < n; ++c) {
+      osc[c] = SolverScalars{};
+      osc[c].done = done[c];
+    }
+    cudaError_t e = cudaMemcpyAsync(oscal_, osc.data(), n * sizeof(SolverScalars), cudaMemcpyHostToDevice, s_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s_);  // osc is pageable and reused
+    if (e != cudaSuccess) return impact_set_error(e, "mixed engine flags", __FILE__, __LINE__);
+    return 0;
+  };
+  std::vector<SolverScalars> init(n);
+  std::vector<SolverResult> ir;
+  for (;;) {
+    int rc = push_flags();
+    if (rc) return rc;
+    // r = b - A x  (FP64, the reference operator)
+    k_kr_ax<double, 0><<<grid, kBlock, ax_smem_bytes<double>(), s_>>>(AJ, AL.ts, n, AL.ntiles, partial_);
+    k_mx_res<<<grid, kBlock, 0, s_>>>(MJ, ML.ts, n, ML.ntiles, oscal_, partial_);
+    k_efin<<<n, 256, 0, s_>>>(ML.ts, partial_, 3, 1, EFIN_RAW, nullptr, q_);
+    prof::count(3);
+    cudaError_t e = cudaMemcpyAsync(q_host_, q_, (size_t)n * 4 * sizeof(double), cudaMemcpyDeviceToHost, s_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s_);
+    if (e != cudaSuccess) return impact_set_error(e, "mixed engine residual", __FILE__, __LINE__);
+    bool any = false;
+    for (int c = 0; c < n; ++c) {
+      init[c] = SolverScalars{};
+      init[c].done = 1;
+      if (done[c]) continue;
+      const double rinf = q_host_[4 * c], r2 = std::sqrt(q_host_[4 * c + 1]), b2 = std::sqrt(q_host_[4 * c + 2]);
+      if (dbg)
+        std::fprintf(stderr, "[impact_b200] case %d outer %d: |r|inf %.3e |r|2 %.3e |b|2 %.3e inner so far %d\n", c,
+                     outer_it[c], rinf, r2, b2, inner_its[c]);
+      res[c].res_inf = rinf;
+      res[c].res_two = r2;
+      res[c].b_two = b2;
+      if (!std::isfinite(rinf) || !std::isfinite(r2)) {
+        res[c].status = 3;
+        done[c] = 1;
+        continue;
+      }
+      const SolverScalars& o = outer[c];
+      const bool conv = (o.tol_abs_inf > 0.0 && rinf < o.tol_abs_inf) || (o.tol_rel > 0.0 && r2 <= o.tol_rel * b2) ||
+                        rinf == 0.0;
+      if (conv) {
+        res[c].status = 0;
+        done[c] = 1;
+        continue;
+      }
+      if (outer_it[c] >= o.max_it) {
+        res[c].status = 1;
+        done[c] = 1;
+        continue;
+      }
+      // inner FP32 solve A e = r / |r|_inf from e = 0
+      double tol = inner_tol;
+      int mit = inner_max_it;
+      if (retries[c] > 0) {
+        tol = std::fmax(tol, 0.1);
+        mit = std::min(mit, 200);
+      }
+      if (o.tol_rel > 0.0 && r2 > 0.0) {
+        const double need = o.tol_rel * b2 / r2;  // reduction still required
+        if (need > tol) tol = std::fmin(0.5, need * 0.5);
+      }
+      init[c].done = 0;
+      init[c].tol_rel = tol;
+      init[c].tol_abs_inf = 0.0;
+      init[c].max_it = mit;
+      any = true;
+    }
+    if (!any) break;
+    rc = push_flags();
+    if (rc) return rc;
+    k_mx_tof32<<<grid, kBlock, 0, s_>>>(MJ, ML.ts, n, ML.ntiles, oscal_);
+    prof::count(1);
+    rc = inner_.solve(init, 1, ir);
+    if (rc) return rc;
+    for (int c = 0; c < n; ++c) {
+      if (init[c].done) continue;
+      if (dbg)
+        std::fprintf(stderr, "[impact_b200] case %d   inner: it %d status %d |r|2/|b|2 %.3e tol %.1e\n", c,
+                     ir[c].iterations, ir[c].status, ir[c].b_two > 0 ? ir[c].res_two / ir[c].b_two : 0.0,
+                     init[c].tol_rel);
+      inner_its[c] += ir[c].iterations;
+      if (ir[c].status == 2 || ir[c].status == 3) {
+        if (++retries[c] > 2) {
+          res[c].status = ir[c].status;
+          done[c] = 1;
+        }
+      } else {
+        ++outer_it[c];
+      }
+    }
+    rc = push_flags();
+    if (rc) return rc;
+    k_mx_apply<<<grid, kBlock, 0, s_>>>(MJ, ML.ts, n, ML.ntiles, oscal_);
+    prof::count(1);
+  }
+  for (int c = 0; c < n; ++c) res[c].iterations = outer_it[c];
+  return 0;
+}
+
+}  // namespace impact

@@ -10,6 +10,7 @@ template <typename T>
 struct MGLevel {
   Geom g;
   const T* cdg[3];  // compact Laplacian of the level
+  int zuni = 0;     // 1: every z row of cdg[2] is the same (uniform z spacing on this level)
   const T* cI[3];   // interpolation weights cI(1:2, 0:M) of the level
   int ratio[3];     // coarsening factor to the next level
   T *A, *B, *C;     // right-hand side, solution, work (levels >= 1)

@@ -36,7 +36,8 @@ cudaEvent_t take() {
   return e;
 }
 const char* kNames[K_COUNT] = {"jacobi_sweep", "jacobi_init2", "div_grad_dot", "x_update", "p_update",
-                               "r_update", "nl_rhs", "project", "divergence2"};
+                               "r_update", "nl_rhs", "project", "divergence2", "mg_sweep", "mg_init",
+                               "mg_residual", "mg_transfer"};
 }  // namespace
 
 bool enabled() { return on; }

@@ -16,6 +16,10 @@ enum Kid {
   K_NL_RHS,        // advection + Helmholtz + RK update of one component
   K_PROJECT,       // vel = rhs - G pre
   K_DIV2,          // divergence of rhs
+  K_MG_SWEEP,      // multigrid damped-Jacobi sweep (every level)
+  K_MG_INIT,       // multigrid init sweep
+  K_MG_RESID,      // multigrid residual
+  K_MG_OTHER,      // restriction, prolongation, copies
   K_COUNT
 };
 

@@ -9,6 +9,7 @@
 // Every pass keeps the reference's order of floating-point operations per point.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -249,6 +250,23 @@ extern "C" long long impact_b200_case_bytes(int N1, int N2, int N3, int precisio
   else
     b += f + 10 * (f / 2);                                // r64 + FP32 r, e + 8 inner fields
   b += 2 * reduce_partial_doubles(g, 4) * 8 + (1 << 20);  // reduction scratch, coefficients
+  // multigrid levels >= 1 (three fields each, at most 1/8 of the previous level, padded)
+  const long long elt = precision == 0 ? 8 : 4;
+  long long lvl = 0;
+  int m[3] = {N1 - 1, N2 - 1, N3 - 1};
+  for (int q = 1; q < MG_MAX_LEVELS; ++q) {
+    bool any = false;
+    for (int a = 0; a < 3; ++a)
+      if (m[a] % 2 == 0 && m[a] >= 4) {
+        m[a] /= 2;
+        any = true;
+      }
+    if (!any) break;
+    lvl += (long long)(m[0] + 8) * (m[1] + 8) * (m[2] + 8);
+  }
+  b += 3 * elt * lvl;
+  b += 12LL * 11 * (N1 + N2 + N3);  // collapsed operator weights
+  b += 4LL * 8 * (g.nfield / 16 + 1024);  // engine tile partials
   return b;
 }
 
@@ -264,6 +282,10 @@ extern "C" int impact_b200_case_destroy(impact_b200_case* c) {
   CaseState& s = c->s;
   cudaSetDevice(s.device);
   if (s.stream) cudaStreamSynchronize(s.stream);
+  delete s.e64;
+  delete s.emx;
+  s.e64 = nullptr;
+  s.emx = nullptr;
   for (void* p : s.allocs) cudaFree(p);
   if (s.hscal) cudaFreeHost(s.hscal);
   if (s.scal_host) cudaFreeHost(s.scal_host);
@@ -271,6 +293,19 @@ extern "C" int impact_b200_case_destroy(impact_b200_case* c) {
   if (s.own_stream && s.stream) cudaStreamDestroy(s.stream);
   delete c;
   return 0;
+}
+
+// 1 when the rows of a table (width w, `rows` rows) agree to 1e-12 of its largest entry.  The
+// tables of an equidistant axis differ row to row only by the rounding of the coordinates
+// (about 1e-13 of the largest entry); kernels then use the first row for the whole axis.  This is
+// applied to the multigrid smoother's compact Laplacians and to the FP32 operator of the inner
+// solve, never to the FP64 operator A that defines the residual.
+static int rows_uniform(const double* t, size_t rows, int w) {
+  double mx = 0.0, dev = 0.0;
+  for (size_t q = 0; q < rows * w; ++q) mx = std::fmax(mx, std::fabs(t[q]));
+  for (size_t r = 1; r < rows; ++r)
+    for (int l = 0; l < w; ++l) dev = std::fmax(dev, std::fabs(t[r * w + l] - t[l]));
+  return dev <= 1e-12 * mx ? 1 : 0;
 }
 
 extern "C" int impact_b200_case_create(const impact_b200_case_desc* desc, const impact_b200_coeffs* co,
@@ -366,6 +401,37 @@ extern "C" int impact_b200_case_create(const impact_b200_case_desc* desc, const 
     s.dt.spp[a] = b + offs[a][12];
     s.dt.sp1[a] = b + offs[a][13];
   }
+  // ---- collapsed operator weights of product_div_grad ----
+  {
+    std::vector<double> w[3];
+    size_t tot = 0;
+    for (int a = 0; a < 3; ++a) {
+      collapse_divgrad(Nax[a], co->axis[a]->cG, co->axis[a]->cD, w[a]);
+      tot += w[a].size();
+    }
+    double* d64 = nullptr;
+    float* d32 = nullptr;
+    rc |= case_alloc(s, (void**)&d64, tot * sizeof(double));
+    rc |= case_alloc(s, (void**)&d32, tot * sizeof(float));
+    if (rc) {
+      impact_b200_case_destroy(c);
+      return -1;
+    }
+    std::vector<double> all;
+    all.reserve(tot);
+    for (int a = 0; a < 3; ++a) {
+      s.W64[a] = d64 + all.size();
+      s.W32[a] = d32 + all.size();
+      all.insert(all.end(), w[a].begin(), w[a].end());
+    }
+    // uniform z spacing: all z rows equal up to rounding of the table construction (1e-14 of the
+    // largest weight), then the kernels keep one row in registers
+    s.zuni = rows_uniform(w[2].data(), w[2].size() / AXW, AXW);
+    s.cdg_zuni = rows_uniform(co->axis[2]->cdg, (size_t)(desc->N3 - 1), 3);
+    std::vector<float> all32(all.begin(), all.end());
+    cudaMemcpy(d64, all.data(), tot * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(d32, all32.data(), tot * sizeof(float), cudaMemcpyHostToDevice);
+  }
   // ---- fields ----
   const size_t fb = (size_t)g.nfield * sizeof(double);
   for (int q = 0; q < IMPACT_B200_NFIELDS; ++q) rc |= case_alloc(s, (void**)&s.f[q], fb);
@@ -441,6 +507,7 @@ extern "C" int impact_b200_case_create(const impact_b200_case_desc* desc, const 
         b.cI[m] = d32 + o_cI[g * 3 + m];
         a.ratio[m] = b.ratio[m] = lv[g].ratio[m];
       }
+      a.zuni = b.zuni = rows_uniform(lv[g].cdg[2].data(), (size_t)(lv[g].M[2] - 1), 3);
       a.A = a.B = a.C = nullptr;
       b.A = b.B = b.C = nullptr;
       if (g == 0) continue;
@@ -528,53 +595,122 @@ extern "C" double* impact_b200_case_field_ptr(impact_b200_case* c, int field) {
 }
 extern "C" void* impact_b200_case_stream(impact_b200_case* c) { return c ? (void*)c->s.stream : nullptr; }
 
-static SolverOpts to_opts(const impact_b200_solver_params* p) {
-  SolverOpts o{};
-  o.precond = p->precond;
-  o.mg = nullptr;
-  o.tol_rel = p->tol_rel;
-  o.tol_abs_inf = p->tol_abs_inf;
-  o.max_it = p->max_it;
-  o.n_sweeps = p->n_sweeps;
-  o.omega = p->omega;
-  o.init_yes = p->init_yes;
-  o.check_every = p->check_every > 0 ? p->check_every : 1;
-  return o;
+static EngineParams engine_params(const CaseState& s, const impact_b200_solver_params* p) {
+  EngineParams ep;
+  ep.precond = p->precond;
+  ep.n_sweeps = p->n_sweeps;
+  ep.mg_down = p->mg_down > 0 ? p->mg_down : 4;
+  ep.mg_up = p->mg_up > 0 ? p->mg_up : 4;
+  ep.mg_bottom = p->mg_bottom > 0 ? p->mg_bottom : 4;
+  ep.omega = p->omega;
+  ep.check_every = p->check_every > 0 ? p->check_every : 1;
+  const char* kc = std::getenv("IMPACT_B200_KC");
+  ep.kc = kc ? std::atoi(kc) : 16;
+  ep.kc = ep.kc < 1 ? 1 : (ep.kc > KC_MAX ? KC_MAX : ep.kc);
+  ep.use_graph = std::getenv("IMPACT_B200_NO_GRAPH") ? 0 : 1;
+  (void)s;
+  return ep;
+}
+
+// build (or rebuild) the case's own engine for these parameters and fields
+static int ensure_engine(CaseState& s, const double* b, double* x, const EngineParams& ep) {
+  if (s.precision == 0) {
+    if (!s.e64) s.e64 = new Engine<double>();
+    if (s.e64->built() && s.e64->params() == ep && s.eng_b == b && s.eng_x == x) return 0;
+    EngineCase<double> ec{};
+    ec.g = s.g;
+    for (int m = 0; m < 3; ++m) {
+      ec.W[m] = s.W64[m];
+      ec.cdg[m] = s.c64.cdg[m];
+    }
+    ec.zuni = s.zuni;
+    ec.cdg_zuni = s.cdg_zuni;
+    ec.mg = s.mg_levels ? &s.mg64 : nullptr;
+    ec.bb = b;
+    ec.phi = x;
+    const KrylovWork<double>& w = s.kw64;
+    ec.rr = w.rr;
+    ec.rh = w.rh;
+    ec.pp = w.pp;
+    ec.Ap = w.Ap;
+    ec.Ar = w.Ar;
+    ec.z1 = w.z1;
+    ec.z2 = w.z2;
+    ec.comp = w.comp;
+    int rc = s.e64->build({ec}, ep, s.stream);
+    if (rc) return rc;
+  } else {
+    if (!s.emx) s.emx = new MixedEngine();
+    if (s.emx->built() && s.emx->params() == ep && s.eng_b == b && s.eng_x == x) return 0;
+    MixedEngine::Case mc{};
+    mc.g = s.g;
+    for (int m = 0; m < 3; ++m) mc.W64[m] = s.W64[m];
+    mc.zuni = s.zuni;
+    mc.bb = b;
+    mc.x = x;
+    mc.r64 = s.mw.r64;
+    mc.r32 = s.mw.r32;
+    mc.e32 = s.mw.e32;
+    EngineCase<float>& ec = mc.inner;
+    ec.g = s.g;
+    for (int m = 0; m < 3; ++m) {
+      ec.W[m] = s.W32[m];
+      ec.cdg[m] = s.c32.cdg[m];
+    }
+    ec.zuni = s.zuni;
+    ec.cdg_zuni = s.cdg_zuni;
+    ec.mg = s.mg_levels ? &s.mg32 : nullptr;
+    ec.bb = s.mw.r32;
+    ec.phi = s.mw.e32;
+    const KrylovWork<float>& w = s.mw.inner;
+    ec.rr = w.rr;
+    ec.rh = w.rh;
+    ec.pp = w.pp;
+    ec.Ap = w.Ap;
+    ec.Ar = w.Ar;
+    ec.z1 = w.z1;
+    ec.z2 = w.z2;
+    ec.comp = w.comp;
+    int rc = s.emx->build({mc}, ep, s.stream);
+    if (rc) return rc;
+  }
+  s.eng_b = b;
+  s.eng_x = x;
+  return 0;
 }
 
 static int run_poisson(CaseState& s, const double* b, double* x, const impact_b200_solver_params* p,
                        impact_b200_solver_result* r) {
-  SolverResult res{};
-  int inner = 0;
-  int rc;
   if (p->precond == 1 && s.mg_levels == 0)
     return impact_set_error_msg(-1, "multigrid preconditioner requested but the case was created without coordinates");
-  auto set_mg = [&](auto& mgd) {
-    mgd.n_down = p->mg_down > 0 ? p->mg_down : 4;
-    mgd.n_up = p->mg_up > 0 ? p->mg_up : 4;
-    mgd.n_bottom = p->mg_bottom > 0 ? p->mg_bottom : 4;
-    mgd.omega = p->omega;
-  };
-  set_mg(s.mg64);
-  set_mg(s.mg32);
-  if (s.precision == 0) {
-    SolverOpts o = to_opts(p);
-    if (o.precond == 1) o.mg = &s.mg64;
-    rc = bicgstab<double>(s.g, s.c64, o, b, x, s.kw64, s.stream, &res);
-  } else {
-    SolverOpts outer = to_opts(p);
-    SolverOpts in = to_opts(p);
-    if (in.precond == 1) in.mg = &s.mg32;
-    in.tol_rel = p->inner_tol_rel > 0 ? p->inner_tol_rel : 1e-4;
-    in.tol_abs_inf = 0.0;
-    in.max_it = p->inner_max_it > 0 ? p->inner_max_it : p->max_it * 4;
-    outer.max_it = p->max_it;
-    if (p->init_yes) {
-      cudaMemsetAsync(x, 0, (size_t)s.g.nfield * sizeof(double), s.stream);
-    }
-    rc = mixed_solve(s.g, s.c64, s.c32, outer, in, b, x, s.mw, s.stream, &res, &inner);
-  }
+  const EngineParams ep = engine_params(s, p);
+  int rc = ensure_engine(s, b, x, ep);
   if (rc) return rc;
+  SolverResult res{};
+  int inner = 0;
+  if (s.precision == 0) {
+    SolverScalars init{};
+    init.tol_rel = p->tol_rel;
+    init.tol_abs_inf = p->tol_abs_inf;
+    init.max_it = p->max_it;
+    std::vector<SolverResult> out;
+    rc = s.e64->solve({init}, p->init_yes, out);
+    if (rc) return rc;
+    res = out[0];
+  } else {
+    SolverScalars outer{};
+    outer.tol_rel = p->tol_rel;
+    outer.tol_abs_inf = p->tol_abs_inf;
+    outer.max_it = p->max_it;
+    const double itol = p->inner_tol_rel > 0 ? p->inner_tol_rel : 1e-4;
+    const int imax = p->inner_max_it > 0 ? p->inner_max_it : p->max_it * 4;
+    std::vector<SolverResult> out;
+    std::vector<int> its;
+    rc = s.emx->solve({outer}, itol, imax, p->init_yes, out, its);
+    if (rc) return rc;
+    res = out[0];
+    inner = its[0];
+  }
   if (r) {
     r->iterations = res.iterations;
     r->inner_iterations = inner;
@@ -584,6 +720,21 @@ static int run_poisson(CaseState& s, const double* b, double* x, const impact_b2
     r->b_two = res.b_two;
   }
   return 0;
+}
+
+// measurement entry: `iters` launches of one engine kernel kind on the case's resident fields in
+// its solve precision (FP64, or FP32 for the inner solve of a mixed case); see Engine::bench
+extern "C" int impact_b200_case_engine_bench(impact_b200_case* c, int kind, int iters,
+                                             const impact_b200_solver_params* p, double* ms, double* bytes) {
+  if (!c || !p || iters < 1 || !ms || !bytes) return impact_set_error_msg(-1, "impact_b200_case_engine_bench: bad arguments");
+  CaseState& s = c->s;
+  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  if (p->precond == 1 && s.mg_levels == 0) return impact_set_error_msg(-1, "engine bench: no multigrid hierarchy");
+  EngineParams ep = engine_params(s, p);
+  int rc = ensure_engine(s, s.f[IMPACT_B200_RES], s.f[IMPACT_B200_PRE], ep);
+  if (rc) return rc;
+  rc = s.precision == 0 ? s.e64->bench(kind, iters, ms, bytes) : s.emx->inner().bench(kind, iters, ms, bytes);
+  return rc;
 }
 
 extern "C" int impact_b200_case_poisson(impact_b200_case* c, int field_b, int field_x,
@@ -611,32 +762,73 @@ extern "C" int impact_b200_case_precond(impact_b200_case* c, int field_in, int f
   CaseState& s = c->s;
   if (s.precision != 0) return impact_set_error_msg(-1, "impact_b200_case_precond: FP64 cases only");
   IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
-  if (p->precond == 1) {
-    if (s.mg_levels == 0) return impact_set_error_msg(-1, "impact_b200_case_precond: case has no multigrid hierarchy");
-    s.mg64.n_down = p->mg_down > 0 ? p->mg_down : 4;
-    s.mg64.n_up = p->mg_up > 0 ? p->mg_up : 4;
-    s.mg64.n_bottom = p->mg_bottom > 0 ? p->mg_bottom : 4;
-    s.mg64.omega = p->omega;
-    mg_vcycle<double>(s.mg64, nullptr, s.f[field_in], s.f[field_out], s.kw64.comp, s.stream);
-  } else {
-    // n_sweeps sweeps from zero (single-level multigridV)
-    if (p->n_sweeps < 1) return impact_set_error_msg(-1, "impact_b200_case_precond: n_sweeps must be >= 1");
-    MGData<double> one{};
-    one.n = 1;
-    one.lv[0] = s.mg_levels ? s.mg64.lv[0] : MGLevel<double>{};
-    if (!s.mg_levels) {
-      one.lv[0].g = s.g;
-      for (int m = 0; m < 3; ++m) one.lv[0].cdg[m] = s.c64.cdg[m];
-    }
-    one.n_down = one.n_up = 0;
-    one.n_bottom = p->n_sweeps;  // relax_bottom runs the init sweep set and a second set
-    one.omega = p->omega;
-    // single level: relax_bottom does n_bottom sweeps from zero then n_bottom more; use half
-    if (p->n_sweeps % 2 != 0) return impact_set_error_msg(-1, "impact_b200_case_precond: use an even n_sweeps");
-    one.n_bottom = p->n_sweeps / 2;
-    mg_vcycle<double>(one, nullptr, s.f[field_in], s.f[field_out], s.kw64.comp, s.stream);
+  if (p->precond == 1 && s.mg_levels == 0)
+    return impact_set_error_msg(-1, "impact_b200_case_precond: case has no multigrid hierarchy");
+  if (p->precond != 1 && p->n_sweeps < 1)
+    return impact_set_error_msg(-1, "impact_b200_case_precond: n_sweeps must be >= 1");
+  // one application of the preconditioner: field_out = M field_in
+  EngineParams ep = engine_params(s, p);
+  ep.use_graph = 0;
+  EngineCase<double> ec{};
+  ec.g = s.g;
+  for (int m = 0; m < 3; ++m) {
+    ec.W[m] = s.W64[m];
+    ec.cdg[m] = s.c64.cdg[m];
   }
+  ec.zuni = s.zuni;
+  ec.cdg_zuni = s.cdg_zuni;
+  ec.mg = s.mg_levels ? &s.mg64 : nullptr;
+  const KrylovWork<double>& w = s.kw64;
+  ec.bb = s.f[field_in];
+  ec.phi = w.Ar;
+  ec.rr = w.rr;
+  ec.rh = w.rh;
+  ec.pp = s.f[field_in];
+  ec.Ap = w.Ap;
+  ec.Ar = w.Ar;
+  ec.z1 = s.f[field_out];
+  ec.z2 = w.z2;
+  ec.comp = w.comp;
+  Engine<double> e;
+  int rc = e.build({ec}, ep, s.stream);
+  if (!rc) rc = e.apply_precond();
+  if (rc) return rc;
   IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
+  IMPACT_CUDA_CHECK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int impact_b200_case_apply(impact_b200_case* c, int op, int field_in, int field_out) {
+  if (!c || field_in < 0 || field_out < 0 || field_in >= IMPACT_B200_NFIELDS || field_out >= IMPACT_B200_NFIELDS ||
+      field_in == field_out || op != 0)
+    return impact_set_error_msg(-1, "impact_b200_case_apply: bad arguments");
+  CaseState& s = c->s;
+  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  impact_b200_solver_params p{};
+  p.precond = 0;
+  p.omega = 0.8;
+  EngineParams ep = engine_params(s, &p);
+  ep.use_graph = 0;
+  EngineCase<double> ec{};
+  ec.g = s.g;
+  for (int m = 0; m < 3; ++m) {
+    ec.W[m] = s.W64[m];
+    ec.cdg[m] = s.c64.cdg[m];
+  }
+  ec.zuni = s.zuni;
+  ec.cdg_zuni = s.cdg_zuni;
+  ec.mg = nullptr;
+  // field_out = A field_in (product_div_grad); the Krylov work fields of an FP64 case or the
+  // library's own fields serve as unused slots
+  double* spare = s.work[0];
+  ec.bb = s.f[field_in];
+  ec.phi = s.f[field_in];
+  ec.rr = s.f[field_out];
+  ec.rh = ec.pp = ec.Ap = ec.Ar = ec.z1 = ec.z2 = ec.comp = spare;
+  Engine<double> e;
+  int rc = e.build({ec}, ep, s.stream);
+  if (!rc) rc = e.apply_operator();
+  if (rc) return rc;
   IMPACT_CUDA_CHECK(cudaGetLastError());
   return 0;
 }
@@ -668,86 +860,317 @@ static void stability_limits(double* lim) {
   }
 }
 
-extern "C" int impact_b200_case_step(impact_b200_case* c, const impact_b200_step_params* p,
-                                     impact_b200_step_state* st, int nsteps) {
-  if (!c || !p || !st || nsteps < 0) return impact_set_error_msg(-1, "impact_b200_case_step: bad arguments");
-  CaseState& s = c->s;
-  const Geom& g = s.g;
-  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+// ---- phases of one time step of one case, on stream st (shared by single cases and batches) ----
+static int upload_stab(cudaStream_t st) {
   if (!stab_ready) {
     stability_limits(stab_host);
     stab_ready = true;
   }
-  IMPACT_CUDA_CHECK(cudaMemcpyToSymbolAsync(c_stab, stab_host, sizeof(stab_host), 0, cudaMemcpyHostToDevice, s.stream));
+  IMPACT_CUDA_CHECK(cudaMemcpyToSymbolAsync(c_stab, stab_host, sizeof(stab_host), 0, cudaMemcpyHostToDevice, st));
+  return 0;
+}
+
+// get_dtime: the CFL bound beta of the case lands in s.dscal[0]
+static void step_beta(CaseState& s, const impact_b200_step_params* p, cudaStream_t st) {
+  const Geom& g = s.g;
+  k_dtime<<<grid3(g), dim3(BX, BY), 0, st>>>(g, s.c64, s.dt, p->Re, s.f[IMPACT_B200_VEL1], s.f[IMPACT_B200_VEL2],
+                                             s.f[IMPACT_B200_VEL3], s.partial);
+  k_reduce_partials<<<1, 1024, 0, st>>>(s.partial, nblocks(g), 1, s.dscal);
+  prof::count(2);
+}
+
+static double dt_from_beta(double beta1, const impact_b200_step_params* p, const impact_b200_step_state* stt) {
+  double dt;
+  const double dinv = beta1 / p->CFL;
+  if (std::fabs(dinv) < 1.0 / p->dtime_max)
+    dt = p->dtime_max;
+  else
+    dt = 1.0 / dinv;
+  if (stt->timestep == 0 && dt > p->dtime0) dt = p->dtime0;
+  return dt;
+}
+
+// rhs_vel and the right-hand side of the pressure equation of substep sub
+static void substep_rhs(CaseState& s, const impact_b200_step_params* p, double dt, int sub, cudaStream_t st) {
+  const Geom& g = s.g;
   const dim3 gr = grid3(g), bl(BX, BY);
-  const long long nb = nblocks(g);
   const double cells = (double)g.n1 * g.n2 * g.n3;
   double* vel[3] = {s.f[IMPACT_B200_VEL1], s.f[IMPACT_B200_VEL2], s.f[IMPACT_B200_VEL3]};
   double* nl[3] = {s.f[IMPACT_B200_NL1], s.f[IMPACT_B200_NL2], s.f[IMPACT_B200_NL3]};
   double* rhs[3] = {s.f[IMPACT_B200_RHS1], s.f[IMPACT_B200_RHS2], s.f[IMPACT_B200_RHS3]};
-  double* pre = s.f[IMPACT_B200_PRE];
-  double* res = s.f[IMPACT_B200_RES];
   const double multL = 1.0 / p->Re;
+  k_interp_vel3<<<gr, bl, 0, st>>>(g, s.c64, vel[0], vel[1], vel[2], s.work[0], s.work[1], s.work[2]);
+  prof::count(1);
+  const double mb = dt * bRK[sub], ma = dt * aRK[sub];
+  const int use_old = sub != 0;
+  const double nlb = (use_old ? 7.0 : 6.0) * 8.0 * cells;
+  IMPACT_PROF(prof::K_NL_RHS, nlb, st, k_nl_rhs<0><<<gr, bl, 0, st>>>(g, s.c64, multL, mb, ma, use_old, vel[0], s.work[0], s.work[1], s.work[2], nl[0], rhs[0]));
+  IMPACT_PROF(prof::K_NL_RHS, nlb, st, k_nl_rhs<1><<<gr, bl, 0, st>>>(g, s.c64, multL, mb, ma, use_old, vel[1], s.work[0], s.work[1], s.work[2], nl[1], rhs[1]));
+  IMPACT_PROF(prof::K_NL_RHS, nlb, st, k_nl_rhs<2><<<gr, bl, 0, st>>>(g, s.c64, multL, mb, ma, use_old, vel[2], s.work[0], s.work[1], s.work[2], nl[2], rhs[2]));
+  const double ab = aRK[sub] + bRK[sub];
+  k_scale_pre<<<gr, bl, 0, st>>>(g, ab, dt, 0, s.f[IMPACT_B200_PRE]);
+  prof::count(1);
+  IMPACT_PROF(prof::K_DIV2, 4.0 * 8.0 * cells, st,
+              launch_divergence2<double>(g, s.c64.cD[0], s.c64.cD[1], s.c64.cD[2], rhs[0], rhs[1], rhs[2],
+                                         s.f[IMPACT_B200_RES], st));
+}
+
+// projection vel = rhs - G pre and the pressure scaling back (mod_timeint.f90:372)
+static void substep_project(CaseState& s, double dt, int sub, cudaStream_t st) {
+  const Geom& g = s.g;
+  const dim3 gr = grid3(g), bl(BX, BY);
+  const double cells = (double)g.n1 * g.n2 * g.n3;
+  double* pre = s.f[IMPACT_B200_PRE];
+  IMPACT_PROF(prof::K_PROJECT, 7.0 * 8.0 * cells, st,
+              k_project<<<gr, bl, 0, st>>>(g, s.c64, pre, s.f[IMPACT_B200_RHS1], s.f[IMPACT_B200_RHS2],
+                                           s.f[IMPACT_B200_RHS3], s.f[IMPACT_B200_VEL1], s.f[IMPACT_B200_VEL2],
+                                           s.f[IMPACT_B200_VEL3]));
+  k_scale_pre<<<gr, bl, 0, st>>>(g, aRK[sub] + bRK[sub], dt, 1, pre);
+  prof::count(1);
+}
+
+// end of the step: mask forcing at the new time, level_pressure
+static void step_finish(CaseState& s, const impact_b200_step_params* p, impact_b200_step_state* stt, double dt,
+                        cudaStream_t st) {
+  const Geom& g = s.g;
+  const dim3 gr = grid3(g), bl(BX, BY);
+  stt->timestep += 1;
+  stt->time += dt;
+  const double u_in = p->U0 * (1.0 + 0.5 * std::sin(2.0 * 3.14159265358979323846 * stt->time / p->T_pulse));
+  k_mask<<<gr, bl, 0, st>>>(g, s.label, u_in, s.f[IMPACT_B200_VEL1], s.f[IMPACT_B200_VEL2], s.f[IMPACT_B200_VEL3]);
+  prof::count(1);
+  if (p->level_pressure) {
+    k_sum<<<gr, bl, 0, st>>>(g, s.f[IMPACT_B200_PRE], s.partial);
+    k_reduce_partials<<<1, 1024, 0, st>>>(s.partial, nblocks(g), 0, s.dscal + 1);
+    k_sub_mean<<<gr, bl, 0, st>>>(g, s.dscal + 1, s.f[IMPACT_B200_PRE]);
+    prof::count(3);
+  }
+}
+
+static void record_solve(impact_b200_step_state* stt, int sub, const impact_b200_solver_result& r) {
+  stt->poisson_iterations[sub] = r.iterations;
+  stt->inner_iterations[sub] = r.inner_iterations;
+  stt->poisson_status[sub] = r.status;
+  stt->poisson_res_rel[sub] = r.b_two > 0.0 ? r.res_two / r.b_two : 0.0;
+}
+
+extern "C" int impact_b200_case_step(impact_b200_case* c, const impact_b200_step_params* p,
+                                     impact_b200_step_state* st, int nsteps) {
+  if (!c || !p || !st || nsteps < 0) return impact_set_error_msg(-1, "impact_b200_case_step: bad arguments");
+  CaseState& s = c->s;
+  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  if (upload_stab(s.stream)) return -1;
   for (int step = 0; step < nsteps; ++step) {
-    // ---- get_dtime ----
-    k_dtime<<<gr, bl, 0, s.stream>>>(g, s.c64, s.dt, p->Re, vel[0], vel[1], vel[2], s.partial);
-    k_reduce_partials<<<1, 1024, 0, s.stream>>>(s.partial, nb, 1, s.dscal);
-    prof::count(2);
+    step_beta(s, p, s.stream);
     IMPACT_CUDA_CHECK(cudaMemcpyAsync(s.hscal, s.dscal, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
-    const double beta1 = s.hscal[0];
-    double dt;
-    const double dinv = beta1 / p->CFL;
-    if (std::fabs(dinv) < 1.0 / p->dtime_max)
-      dt = p->dtime_max;
-    else
-      dt = 1.0 / dinv;
-    if (st->timestep == 0 && dt > p->dtime0) dt = p->dtime0;
+    const double dt = dt_from_beta(s.hscal[0], p, st);
     st->dtime = dt;
-    // ---- three RK substeps ----
     for (int sub = 0; sub < 3; ++sub) {
-      k_interp_vel3<<<gr, bl, 0, s.stream>>>(g, s.c64, vel[0], vel[1], vel[2], s.work[0], s.work[1], s.work[2]);
-      prof::count(1);
-      const double mb = dt * bRK[sub], ma = dt * aRK[sub];
-      const int use_old = sub != 0;
-      const double nlb = (use_old ? 7.0 : 6.0) * 8.0 * cells;
-      IMPACT_PROF(prof::K_NL_RHS, nlb, s.stream, k_nl_rhs<0><<<gr, bl, 0, s.stream>>>(g, s.c64, multL, mb, ma, use_old, vel[0], s.work[0], s.work[1], s.work[2], nl[0], rhs[0]));
-      IMPACT_PROF(prof::K_NL_RHS, nlb, s.stream, k_nl_rhs<1><<<gr, bl, 0, s.stream>>>(g, s.c64, multL, mb, ma, use_old, vel[1], s.work[0], s.work[1], s.work[2], nl[1], rhs[1]));
-      IMPACT_PROF(prof::K_NL_RHS, nlb, s.stream, k_nl_rhs<2><<<gr, bl, 0, s.stream>>>(g, s.c64, multL, mb, ma, use_old, vel[2], s.work[0], s.work[1], s.work[2], nl[2], rhs[2]));
-      const double ab = aRK[sub] + bRK[sub];
-      k_scale_pre<<<gr, bl, 0, s.stream>>>(g, ab, dt, 0, pre);
-      prof::count(1);
-      IMPACT_PROF(prof::K_DIV2, 4.0 * 8.0 * cells, s.stream,
-                  launch_divergence2<double>(g, s.c64.cD[0], s.c64.cD[1], s.c64.cD[2], rhs[0], rhs[1], rhs[2], res, s.stream));
+      substep_rhs(s, p, dt, sub, s.stream);
       impact_b200_solver_result r{};
-      int rc = run_poisson(s, res, pre, &p->poisson, &r);
+      int rc = run_poisson(s, s.f[IMPACT_B200_RES], s.f[IMPACT_B200_PRE], &p->poisson, &r);
       if (rc) return rc;
-      st->poisson_iterations[sub] = r.iterations;
-      st->inner_iterations[sub] = r.inner_iterations;
-      st->poisson_status[sub] = r.status;
-      st->poisson_res_rel[sub] = r.b_two > 0.0 ? r.res_two / r.b_two : 0.0;
-      IMPACT_PROF(prof::K_PROJECT, 7.0 * 8.0 * cells, s.stream,
-                  k_project<<<gr, bl, 0, s.stream>>>(g, s.c64, pre, rhs[0], rhs[1], rhs[2], vel[0], vel[1], vel[2]));
-      k_scale_pre<<<gr, bl, 0, s.stream>>>(g, ab, dt, 1, pre);
-      prof::count(1);
+      record_solve(st, sub, r);
+      substep_project(s, dt, sub, s.stream);
     }
-    st->timestep += 1;
-    st->time += dt;
-    const double u_in = p->U0 * (1.0 + 0.5 * std::sin(2.0 * 3.14159265358979323846 * st->time / p->T_pulse));
-    k_mask<<<gr, bl, 0, s.stream>>>(g, s.label, u_in, vel[0], vel[1], vel[2]);
-    prof::count(1);
-    if (p->level_pressure) {
-      k_sum<<<gr, bl, 0, s.stream>>>(g, pre, s.partial);
-      k_reduce_partials<<<1, 1024, 0, s.stream>>>(s.partial, nb, 0, s.dscal + 1);
-      k_sub_mean<<<gr, bl, 0, s.stream>>>(g, s.dscal + 1, pre);
-      prof::count(3);
-    }
+    step_finish(s, p, st, dt, s.stream);
   }
   IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
   IMPACT_CUDA_CHECK(cudaGetLastError());
   prof::flush();
   return 0;
 }
+
+// =========================================================================================
+// batches: several cases of one device and precision advanced together; every kernel of the
+// pressure solve is one launch over all cases, the explicit parts run per case on the batch
+// stream
+// =========================================================================================
+struct impact_b200_batch {
+  std::vector<impact_b200_case*> cases;
+  int device = 0, precision = 0;
+  cudaStream_t stream = nullptr;
+  Engine<double> e64;
+  MixedEngine emx;
+  double* hbeta = nullptr;  // pinned, one per case
+};
+
+extern "C" int impact_b200_batch_destroy(impact_b200_batch* b) {
+  if (!b) return 0;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  b->e64.release();
+  b->emx.release();
+  if (b->hbeta) cudaFreeHost(b->hbeta);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return 0;
+}
+
+extern "C" int impact_b200_batch_create(impact_b200_case* const* cases, int ncases, impact_b200_batch** out) {
+  if (!cases || ncases < 1 || !out) return impact_set_error_msg(-1, "impact_b200_batch_create: bad arguments");
+  *out = nullptr;
+  for (int c = 0; c < ncases; ++c) {
+    if (!cases[c]) return impact_set_error_msg(-1, "impact_b200_batch_create: null case");
+    if (cases[c]->s.device != cases[0]->s.device || cases[c]->s.precision != cases[0]->s.precision)
+      return impact_set_error_msg(-1, "impact_b200_batch_create: cases differ in device or precision");
+    for (int d = 0; d < c; ++d)
+      if (cases[d] == cases[c]) return impact_set_error_msg(-1, "impact_b200_batch_create: a case appears twice");
+  }
+  IMPACT_CUDA_CHECK(cudaSetDevice(cases[0]->s.device));
+  impact_b200_batch* b = new impact_b200_batch();
+  b->cases.assign(cases, cases + ncases);
+  b->device = cases[0]->s.device;
+  b->precision = cases[0]->s.precision;
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&b->hbeta, ncases * sizeof(double));
+  if (e != cudaSuccess) {
+    impact_b200_batch_destroy(b);
+    return impact_set_error(e, "impact_b200_batch_create", __FILE__, __LINE__);
+  }
+  *out = b;
+  return 0;
+}
+
+// (re)build the batch engine when the solver parameters change
+static int batch_engine(impact_b200_batch* b, const impact_b200_solver_params* p) {
+  const int n = (int)b->cases.size();
+  const EngineParams ep = engine_params(b->cases[0]->s, p);
+  if (p->precond == 1)
+    for (auto* c : b->cases)
+      if (c->s.mg_levels == 0)
+        return impact_set_error_msg(-1, "batch: multigrid requested but a case was created without coordinates");
+  if (b->precision == 0) {
+    if (b->e64.built() && b->e64.params() == ep) return 0;
+    std::vector<EngineCase<double>> ec(n);
+    for (int c = 0; c < n; ++c) {
+      CaseState& s = b->cases[c]->s;
+      EngineCase<double>& E = ec[c];
+      E = EngineCase<double>{};
+      E.g = s.g;
+      for (int m = 0; m < 3; ++m) {
+        E.W[m] = s.W64[m];
+        E.cdg[m] = s.c64.cdg[m];
+      }
+      E.zuni = s.zuni;
+      E.cdg_zuni = s.cdg_zuni;
+      E.mg = s.mg_levels ? &s.mg64 : nullptr;
+      E.bb = s.f[IMPACT_B200_RES];
+      E.phi = s.f[IMPACT_B200_PRE];
+      const KrylovWork<double>& w = s.kw64;
+      E.rr = w.rr;
+      E.rh = w.rh;
+      E.pp = w.pp;
+      E.Ap = w.Ap;
+      E.Ar = w.Ar;
+      E.z1 = w.z1;
+      E.z2 = w.z2;
+      E.comp = w.comp;
+    }
+    return b->e64.build(ec, ep, b->stream);
+  }
+  if (b->emx.built() && b->emx.params() == ep) return 0;
+  std::vector<MixedEngine::Case> mc(n);
+  for (int c = 0; c < n; ++c) {
+    CaseState& s = b->cases[c]->s;
+    MixedEngine::Case& M = mc[c];
+    M = MixedEngine::Case{};
+    M.g = s.g;
+    for (int m = 0; m < 3; ++m) M.W64[m] = s.W64[m];
+    M.zuni = s.zuni;
+    M.bb = s.f[IMPACT_B200_RES];
+    M.x = s.f[IMPACT_B200_PRE];
+    M.r64 = s.mw.r64;
+    M.r32 = s.mw.r32;
+    M.e32 = s.mw.e32;
+    EngineCase<float>& E = M.inner;
+    E.g = s.g;
+    for (int m = 0; m < 3; ++m) {
+      E.W[m] = s.W32[m];
+      E.cdg[m] = s.c32.cdg[m];
+    }
+    E.zuni = s.zuni;
+    E.cdg_zuni = s.cdg_zuni;
+    E.mg = s.mg_levels ? &s.mg32 : nullptr;
+    E.bb = s.mw.r32;
+    E.phi = s.mw.e32;
+    const KrylovWork<float>& w = s.mw.inner;
+    E.rr = w.rr;
+    E.rh = w.rh;
+    E.pp = w.pp;
+    E.Ap = w.Ap;
+    E.Ar = w.Ar;
+    E.z1 = w.z1;
+    E.z2 = w.z2;
+    E.comp = w.comp;
+  }
+  return b->emx.build(mc, ep, b->stream);
+}
+
+extern "C" int impact_b200_batch_step(impact_b200_batch* b, const impact_b200_step_params* p,
+                                      impact_b200_step_state* st, int nsteps) {
+  if (!b || !p || !st || nsteps < 0) return impact_set_error_msg(-1, "impact_b200_batch_step: bad arguments");
+  const int n = (int)b->cases.size();
+  IMPACT_CUDA_CHECK(cudaSetDevice(b->device));
+  cudaStream_t bs = b->stream;
+  for (auto* c : b->cases) IMPACT_CUDA_CHECK(cudaStreamSynchronize(c->s.stream));
+  int rc = batch_engine(b, &p[0].poisson);
+  if (rc) return rc;
+  if (upload_stab(bs)) return -1;
+  std::vector<double> dt(n);
+  std::vector<SolverScalars> init(n);
+  std::vector<SolverResult> res;
+  std::vector<int> its;
+  for (int step = 0; step < nsteps; ++step) {
+    for (int c = 0; c < n; ++c) {
+      step_beta(b->cases[c]->s, &p[c], bs);
+      IMPACT_CUDA_CHECK(cudaMemcpyAsync(b->hbeta + c, b->cases[c]->s.dscal, sizeof(double), cudaMemcpyDeviceToHost, bs));
+    }
+    IMPACT_CUDA_CHECK(cudaStreamSynchronize(bs));
+    for (int c = 0; c < n; ++c) {
+      dt[c] = dt_from_beta(b->hbeta[c], &p[c], &st[c]);
+      st[c].dtime = dt[c];
+    }
+    for (int sub = 0; sub < 3; ++sub) {
+      for (int c = 0; c < n; ++c) substep_rhs(b->cases[c]->s, &p[c], dt[c], sub, bs);
+      for (int c = 0; c < n; ++c) {
+        init[c] = SolverScalars{};
+        init[c].tol_rel = p[c].poisson.tol_rel;
+        init[c].tol_abs_inf = p[c].poisson.tol_abs_inf;
+        init[c].max_it = p[c].poisson.max_it;
+      }
+      if (b->precision == 0) {
+        rc = b->e64.solve(init, p[0].poisson.init_yes, res);
+        its.assign(n, 0);
+      } else {
+        const double itol = p[0].poisson.inner_tol_rel > 0 ? p[0].poisson.inner_tol_rel : 1e-4;
+        const int imax = p[0].poisson.inner_max_it > 0 ? p[0].poisson.inner_max_it : p[0].poisson.max_it * 4;
+        rc = b->emx.solve(init, itol, imax, p[0].poisson.init_yes, res, its);
+      }
+      if (rc) return rc;
+      for (int c = 0; c < n; ++c) {
+        impact_b200_solver_result r{};
+        r.iterations = res[c].iterations;
+        r.inner_iterations = its[c];
+        r.status = res[c].status;
+        r.res_inf = res[c].res_inf;
+        r.res_two = res[c].res_two;
+        r.b_two = res[c].b_two;
+        record_solve(&st[c], sub, r);
+        substep_project(b->cases[c]->s, dt[c], sub, bs);
+      }
+    }
+    for (int c = 0; c < n; ++c) step_finish(b->cases[c]->s, &p[c], &st[c], dt[c], bs);
+  }
+  IMPACT_CUDA_CHECK(cudaStreamSynchronize(bs));
+  IMPACT_CUDA_CHECK(cudaGetLastError());
+  prof::flush();
+  return 0;
+}
+
+extern "C" int impact_b200_batch_size(impact_b200_batch* b) { return b ? (int)b->cases.size() : 0; }
+extern "C" void* impact_b200_batch_stream(impact_b200_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 // ---------------------------------------------------------------------------------------
 // measurement entry: launch one hot kernel `iters` times on the case's resident fields

@@ -105,6 +105,12 @@ def lib():
         "impact_b200_case_poisson": (i, [_vp, i, i, P(SolverParams), P(SolverResult)]),
         "impact_b200_case_step": (i, [_vp, P(StepParams), P(StepState), i]),
         "impact_b200_case_precond": (i, [_vp, i, i, P(SolverParams)]),
+        "impact_b200_case_apply": (i, [_vp, i, i, i]),
+        "impact_b200_batch_create": (i, [C.POINTER(_vp), i, C.POINTER(_vp)]),
+        "impact_b200_batch_destroy": (i, [_vp]),
+        "impact_b200_batch_step": (i, [_vp, C.POINTER(StepParams), C.POINTER(StepState), i]),
+        "impact_b200_batch_size": (i, [_vp]),
+        "impact_b200_batch_stream": (_vp, [_vp]),
         "impact_b200_case_mg_levels": (i, [_vp]),
         "impact_b200_jacobi_solve": (i, [i, i, i, i, i, i, d, _dp, _dp, _dp, _dp, _dp, i, d, i, _ip, _dp]),
         "impact_b200_product_scalar": (i, [i, i, i, _vp, _vp, _dp]),
@@ -114,6 +120,7 @@ def lib():
         "impact_b200_profile_read": (i, [i, P(C.c_longlong), _dp, _dp, P(C.c_char_p)]),
         "impact_b200_launch_count": (C.c_longlong, []),
         "impact_b200_case_kernel_bench": (i, [_vp, i, i, _dp]),
+        "impact_b200_case_engine_bench": (i, [_vp, i, i, P(SolverParams), _dp, _dp]),
         # reference launcher FFI (every argument by reference)
         "gradient_launcher_": (None, [_ip] * 6 + [_PP] * 3),
         "divergence_launcher_": (None, [_ip] * 6 + [_PP] * 3),
@@ -142,8 +149,12 @@ def last_error() -> str:
 
 
 def check(rc: int, what: str = ""):
+    """Raise ImpactError with the library's message when rc != 0 (the message is then cleared,
+    so that later calls do not report it again)."""
     if rc != 0:
-        raise ImpactError(f"{what}: {last_error()} (rc={rc})")
+        msg = last_error()
+        lib().impact_b200_clear_error()
+        raise ImpactError(f"{what}: {msg} (rc={rc})")
 
 
 def _ptr(a: np.ndarray):
@@ -290,6 +301,20 @@ class Case:
         fo = FIELDS[field_out] if isinstance(field_out, str) else field_out
         check(lib().impact_b200_case_precond(self._h, fi, fo, C.byref(params)), "case_precond")
 
+    def engine_bench(self, kind: int, iters: int = 10, params: SolverParams | None = None):
+        """(ms per launch, algorithmic bytes per launch) of one Poisson-engine kernel kind"""
+        params = solver_params(precond=1) if params is None else params
+        ms, by = C.c_double(), C.c_double()
+        check(lib().impact_b200_case_engine_bench(self._h, kind, iters, C.byref(params), C.byref(ms), C.byref(by)),
+              "engine_bench")
+        return ms.value, by.value
+
+    def apply(self, field_in="pre", field_out="res", op: int = 0):
+        """field_out = A field_in; op 0: product_div_grad in FP64"""
+        fi = FIELDS[field_in] if isinstance(field_in, str) else field_in
+        fo = FIELDS[field_out] if isinstance(field_out, str) else field_out
+        check(lib().impact_b200_case_apply(self._h, op, fi, fo), "case_apply")
+
     def kernel_bench(self, kid: int, iters: int = 10) -> float:
         """average ms of one hot kernel launched iters times on the resident fields"""
         ms = C.c_double()
@@ -301,7 +326,46 @@ class Case:
         return self.state
 
 
-PROFILE_KERNELS = 9
+class Batch:
+    """Several cases of one device and precision advanced together (impact_b200_batch_*): one
+    launch per operator of the pressure solve over all cases, graph-replayed iteration chunks.
+    Each case keeps its own StepState (case.state), which the batch updates."""
+
+    def __init__(self, cases):
+        self.cases = list(cases)
+        arr = (_vp * len(self.cases))(*[c._h for c in self.cases])
+        h = _vp()
+        check(lib().impact_b200_batch_create(arr, len(self.cases), C.byref(h)), "batch_create")
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().impact_b200_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, params, nsteps: int = 1):
+        """params: one StepParams for all cases, or a list with one per case"""
+        n = len(self.cases)
+        plist = list(params) if isinstance(params, (list, tuple)) else [params] * n
+        pa = (StepParams * n)(*plist)
+        sa = (StepState * n)(*[c.state for c in self.cases])
+        check(lib().impact_b200_batch_step(self._h, pa, sa, nsteps), "batch_step")
+        for c, s in zip(self.cases, sa):
+            C.memmove(C.byref(c.state), C.byref(s), C.sizeof(StepState))
+        return [c.state for c in self.cases]
+
+    @property
+    def stream(self):
+        return lib().impact_b200_batch_stream(self._h)
+
+
+PROFILE_KERNELS = 13
 
 
 def profile(enable: bool = True, reset: bool = True):

@@ -190,6 +190,9 @@ int impact_b200_case_poisson(impact_b200_case* c, int field_b, int field_x, cons
 
 /* Apply the preconditioner of p once: field_out = M field_in (FP64 cases). */
 int impact_b200_case_precond(impact_b200_case* c, int field_in, int field_out, const impact_b200_solver_params* p);
+/* field_out = A field_in for op 0: product_div_grad (mod_laplace.f90:38-197), the operator of the
+ * pressure Poisson solve, in FP64 on the resident fields. */
+int impact_b200_case_apply(impact_b200_case* c, int op, int field_in, int field_out);
 /* levels of the multigrid hierarchy of the case (0 when it has none) */
 int impact_b200_case_mg_levels(impact_b200_case* c);
 
@@ -212,6 +215,22 @@ typedef struct {
 /* nsteps RK3 time steps (mod_timeint.f90:242-578) on the resident fields. */
 int impact_b200_case_step(impact_b200_case* c, const impact_b200_step_params* p, impact_b200_step_state* st,
                           int nsteps);
+
+/* ---- batches (no counterpart in the reference) ------------------------------------------
+ * A batch advances several cases of one device and one precision together, each with its own
+ * grid size, parameters and time step: every kernel of the pressure solve is one launch over
+ * the tiles of all cases (converged cases drop out on the device), and each chunk of solver
+ * iterations is replayed as a captured CUDA graph.  The solver structure (preconditioner,
+ * sweeps, omega, check_every) comes from p[0].poisson; tolerances and max_it from each p[c].
+ * A case must not be stepped on its own while it belongs to a batch that is stepping. */
+typedef struct impact_b200_batch impact_b200_batch;
+int impact_b200_batch_create(impact_b200_case* const* cases, int ncases, impact_b200_batch** out);
+int impact_b200_batch_destroy(impact_b200_batch* b);
+/* nsteps RK3 steps of every case; p and st hold one entry per case, in creation order. */
+int impact_b200_batch_step(impact_b200_batch* b, const impact_b200_step_params* p, impact_b200_step_state* st,
+                           int nsteps);
+int impact_b200_batch_size(impact_b200_batch* b);
+void* impact_b200_batch_stream(impact_b200_batch* b);
 
 /* ---- device_jacobi_solver (jacobi_solver_host_v4.f90:5) replacement -------------------
  * Host arrays rel (in/out) and bb in the reference layout.  Deterministic out-of-place JOR
@@ -253,6 +272,14 @@ long long impact_b200_launch_count(void);
  * init + sweep, 2 A x with a fused inner product, 3 A x, 4 one-thread-per-point Jacobi sweep), in
  * the case's precision; *ms_per_launch = average device time (CUDA events on the case stream) */
 int impact_b200_case_kernel_bench(impact_b200_case* c, int kid, int iters, double* ms_per_launch);
+/* Measurement: iters launches of one kernel of the Poisson engine on the case's finest level, in
+ * the solve precision (FP64, or FP32 for the inner solve of a mixed case), the engine built with
+ * the solver parameters p.  kind: 0 sweep, 1 init sweep, 2 residual, 3 prolongation,
+ * 4 restriction, 5 A x + inner product, 6 A x + two inner products, 7 x update, 8 p update,
+ * 9 r update, 10 one V-cycle, 11 one BiCGstab iteration.  Returns the average ms per launch
+ * (CUDA events on the case stream) and the algorithmic bytes of one launch (0 for 10, 11). */
+int impact_b200_case_engine_bench(impact_b200_case* c, int kind, int iters, const impact_b200_solver_params* p,
+                                  double* ms, double* bytes);
 
 #ifdef __cplusplus
 }
