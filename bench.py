@@ -6,8 +6,10 @@ Workload (default, the mixed-precision single case of the benchmark suite): sten
 384 x 384 x 768 periodic box (L = 1 x 1 x 2, uniform spacing); cylinder of radius 0.25 L1 with a
 Gaussian constriction at mid-length (60 % area reduction, sigma = 0.5 R); pulsatile plug inflow
 u_z = U0 (1 + 0.5 sin(2 pi t / T)), U0 = 1, T = 1, on the label-5 buffer; Re = 500; dt = 0.2 x the
-RK3 stability limit (get_dtime with CFL = 0.2); every Poisson solve is BiCGstab with a 4-sweep
-JOR (omega = 0.8) preconditioner to ||b - A x||_2 <= 1e-8 ||b||_2.  Starts from rest.  One
+RK3 stability limit (get_dtime with CFL = 0.2); every Poisson solve is BiCGstab with the
+multigrid V-cycle preconditioner (damped Jacobi, omega = 0.8, 4/4/4 sweeps) to
+||b - A x||_2 <= 1e-8 ||b||_2: FP32 inner solve with FP64 refinement (the line), plain FP64
+beside it.  Starts from rest.  One
 "step" is one RK3 time step (3 substeps, 3 Poisson solves).  Fields are ~0.95 GB each, far
 larger than L2, so no flush is needed between steps.
 
@@ -50,6 +52,13 @@ def parse():
     ap.add_argument("--inner-tol", type=float, default=1e-4)
     ap.add_argument("--precond", type=int, default=1, help="0: JOR sweeps, 1: multigrid V-cycle (default)")
     ap.add_argument("--check-every", type=int, default=2)
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve"],
+                    help="single: the 384 mixed case (default line, with short batch and serve samples); "
+                         "batch / serve: the full batched or serving workload as the line")
+    ap.add_argument("--no-extra", action="store_true", help="skip the batch and serve samples of the default line")
+    ap.add_argument("--cases", type=int, default=48, help="batch: number of cases")
+    ap.add_argument("--requests", type=int, default=16, help="serve: number of requests")
+    ap.add_argument("--case-steps", type=int, default=0, help="batch / serve: time steps per case (0: the spec's)")
     return ap.parse_args()
 
 
@@ -315,6 +324,143 @@ def _iters_estimate(n, precond=1):
     return 8 if precond == 1 else int(round(1.6 * n))
 
 
+# ---------------------------------------------------------------------------------------------
+# batched uneven cases and the serving stream
+# ---------------------------------------------------------------------------------------------
+def batch_specs(n_cases, seed=7):
+    """Uneven vessel cases: n log-uniform in [32, 160] (n x n x 2n cells, rounded to a multiple of 8
+    so that the multigrid hierarchy coarsens at least three times), straight cylinder of radius
+    U[0.15, 0.3], 0-2 Gaussian stenoses of 30-70 % area reduction at random z (sigma = 0.5 R),
+    U0 in U[0.5, 1.5], Re in U[100, 800]."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_cases):
+        n = int(max(32, min(160, round(float(np.exp(rng.uniform(np.log(32), np.log(160)))) / 8) * 8)))
+        radius = float(rng.uniform(0.15, 0.3))
+        sten = [(float(rng.uniform(0.3, 1.7)), float(rng.uniform(0.3, 0.7)), 0.5 * radius)
+                for _ in range(int(rng.integers(0, 3)))]
+        out.append({"n": n, "radius": radius, "stenoses": sten, "U0": float(rng.uniform(0.5, 1.5)),
+                    "Re": float(rng.uniform(100, 800))})
+    return out
+
+
+def _case_params(spec, precision, args):
+    import impact_b200 as I
+    return I.step_params(Re=spec["Re"], CFL=0.2, dtime_max=1.0, dtime0=1e9, U0=spec["U0"], T_pulse=1.0,
+                         level_pressure=1, tol_rel=1e-8, max_it=200 if precision == 0 else 40, omega=0.8,
+                         init_yes=0, check_every=args.check_every, inner_tol_rel=args.inner_tol, inner_max_it=400,
+                         precond=1, mg_down=4, mg_up=4, mg_bottom=4)
+
+
+def _make_case(spec, precision, device, labels=None):
+    import impact_b200 as I
+    from impact_b200 import geometry as G
+    n = spec["n"]
+    g = I.Grid((n + 1, n + 1, 2 * n + 1), (1.0, 1.0, 2.0))
+    c = I.Case(g, precision=precision, device=device)
+    c.set_labels(labels(g) if labels else G.straight_vessel(g, radius_frac=spec["radius"] / g.L[0],
+                                                            stenoses=spec["stenoses"]))
+    return c
+
+
+def batch_bench(args, device, n_cases, steps):
+    """48 uneven cases x `steps` mixed-precision steps advanced as one batch, against the same
+    cases run one after another in plain FP64 (each case alone, the drop-in's way).  Device time
+    from CUDA events on the batch stream / on each case's stream; one untimed warm-up step."""
+    import torch
+
+    import impact_b200 as I
+    specs = batch_specs(n_cases)
+    cells = [s["n"] * s["n"] * 2 * s["n"] for s in specs]
+    out = {"workload": f"batched-vessels-{n_cases}", "cases": n_cases, "steps_per_case": steps,
+           "cells_total": sum(cells), "n_range": [min(s["n"] for s in specs), max(s["n"] for s in specs)]}
+    # mixed, batched
+    cases = [_make_case(s, 1, device) for s in specs]
+    params = [_case_params(s, 1, args) for s in specs]
+    batch = I.Batch(cases)
+    launches0 = I.launch_count()
+    batch.step(params, 1)
+    stream = torch.cuda.ExternalStream(batch.stream, device=device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        st = batch.step(params, 1)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    out["mixed_batched"] = {"value": round(sum(cells) * steps / (ms / 1e3) / 1e6, 3), "unit": UNIT,
+                            "ms_per_step": ms / steps, "launches_per_step": (I.launch_count() - launches0) / (steps + 1),
+                            "status_ok": all(all(x == 0 for x in s.poisson_status) for s in st)}
+    batch.close()
+    for c in cases:
+        c.close()
+    del cases
+    torch.cuda.empty_cache()
+    # plain FP64, one case after another
+    total = 0.0
+    for s in specs:
+        c = _make_case(s, 0, device)
+        p = _case_params(s, 0, args)
+        c.step(p, 1)
+        cs = torch.cuda.ExternalStream(c.stream, device=device)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(cs)
+        c.step(p, steps)
+        b.record(cs)
+        b.synchronize()
+        total += a.elapsed_time(b)
+        c.close()
+    out["fp64_sequential"] = {"value": round(sum(cells) * steps / (total / 1e3) / 1e6, 3), "unit": UNIT,
+                              "ms_per_step": total / steps}
+    out["batched_mixed_over_sequential_fp64"] = round(out["mixed_batched"]["value"] / out["fp64_sequential"]["value"], 3)
+    torch.cuda.empty_cache()
+    return out
+
+
+def serve_bench(args, device, n_req, steps, budget_gb=160.0, rate=20.0):
+    """Poisson arrivals (mean `rate` / s) of curved-tube vessel cases, n log-uniform in [64, 256]
+    (n x n x 2n, multiple of 8), radius U[0.15, 0.3], 0-2 stenoses; admission by an HBM budget,
+    mixed precision at 1e-8, `steps` steps per case; throughput and p50 / p99 completion latency
+    on the loop's host clock."""
+    import numpy as np
+    import torch
+
+    from impact_b200 import geometry as G
+    from impact_b200 import serve as S
+    rng = np.random.default_rng(11)
+    arrivals = S.poisson_arrivals(n_req, rate, rng)
+    reqs = []
+    cells = 0
+    for r in range(n_req):
+        n = int(max(64, min(256, round(float(np.exp(rng.uniform(np.log(64), np.log(256)))) / 8) * 8)))
+        radius = float(rng.uniform(0.15, 0.3))
+        sten = [(float(rng.uniform(0.3, 1.7)), float(rng.uniform(0.3, 0.7)), 0.5 * radius)
+                for _ in range(int(rng.integers(0, 3)))]
+        seed = int(rng.integers(1 << 30))
+        spec = {"n": n, "radius": radius, "stenoses": sten, "U0": float(rng.uniform(0.5, 1.5)),
+                "Re": float(rng.uniform(100, 800))}
+
+        def labels(g, seed=seed, radius=radius, sten=sten):
+            return G.curved_tube(g, np.random.default_rng(seed), radius, stenoses=sten)
+
+        reqs.append(S.Request(r, (n + 1, n + 1, 2 * n + 1), (1.0, 1.0, 2.0), labels, _case_params(spec, 1, args),
+                              steps, float(arrivals[r])))
+        cells += n * n * 2 * n
+    srv = S.Server(int(budget_gb * 1e9), precision=1, device=device, keep=())
+    t0 = time.perf_counter()
+    done = srv.run(reqs)
+    wall = time.perf_counter() - t0
+    torch.cuda.synchronize(device)
+    stats = S.summarize(done, wall)
+    stats.update({"workload": f"serving-{n_req}-requests", "arrival_rate_per_s": rate, "steps_per_case": steps,
+                  "hbm_budget_gb": budget_gb, "peak_cases": srv.peak_cases, "peak_gb": round(srv.peak_bytes / 1e9, 2),
+                  "batch_rebuilds": srv.batch_rebuilds, "rounds": srv.rounds,
+                  "status_ok": all(all(x == 0 for x in d.status) for d in done),
+                  "clock": "host wall clock of the request loop (latency = completion - arrival)"})
+    return stats
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -336,6 +482,9 @@ def main():
     else:
         torch.cuda.set_device(0)
     device = local if world > 1 else 0
+    if args.workload != "single":
+        extra_main(args, device, rank, world, dist)
+        return
     mixed, fields, grid, lab = run_arm(args, 1, device, rank, world, dist, profile_on=True, e2e_on=True)
     fp64 = None
     if not args.no_fp64:
@@ -381,12 +530,41 @@ def main():
         line["fp64"] = {"value": round(v64, 3), "unit": UNIT, "ms_per_step": fp64["ms_dev"] / K,
                         "iterations_per_substep": fp64["iterations"], "status": fp64["status"]}
         line["mixed_over_fp64"] = round(value / v64, 3)
+    if not args.no_extra and world == 1:
+        line["batch"] = batch_bench(args, device, min(args.cases, 48), args.case_steps or 5)
+        line["serve"] = serve_bench(args, device, args.requests, args.case_steps or 10)
     if world == 1 and not args.no_cpu:
         its = fp64["iterations"][-1] if fp64 is not None else [_iters_estimate(args.size, args.precond)] * 3
         try:
             line["cpu_baseline"] = cpu_baseline(args, fields, lab, its)
         except Exception as ex:  # the CPU sample must never hide the device number
             line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
+    print(json.dumps(line), flush=True)
+
+
+def extra_main(args, device, rank, world, dist):
+    """--workload batch | serve: the batched or serving workload as the benchmark line (every rank
+    runs its own replica; value = whole-job aggregate)."""
+    import torch
+    if args.workload == "batch":
+        r = batch_bench(args, device, args.cases, args.case_steps or 50)
+        v = r["mixed_batched"]["value"]
+        ms = r["mixed_batched"]["ms_per_step"]
+    else:
+        r = serve_bench(args, device, args.requests, args.case_steps or 200)
+        v = r["throughput_mcell_steps_s"]
+        ms = 1e3 * r["wall_s"]
+    if dist is not None:
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        v = float(t[0]) * world
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": world, "steps": args.case_steps or 0,
+            "warmup": 1, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 inner solve / f64 residual+RHS", "data": "synthetic", "config": r}
     print(json.dumps(line), flush=True)
 
 

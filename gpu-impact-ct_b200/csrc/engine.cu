@@ -496,7 +496,7 @@ constexpr int AX_PER = (AX_TE + ENT - 1) / ENT;  // staged elements per thread a
 // ring depth: planes k .. k+5 are read at plane k, the rest of the ring is in flight
 template <typename T>
 struct AxRing {
-  static constexpr int R = sizeof(T) == 4 ? 12 : 10;
+  static constexpr int R = sizeof(T) == 4 ? 16 : 8;  // a power of two: slots by masking
 };
 template <typename T>
 constexpr size_t ax_smem_bytes() {
@@ -558,7 +558,7 @@ __global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict
     // plane kk (k0-5 <= kk <= k1+5) into its ring slot; the partner only for kk in k0..k1
     auto stage = [&](int kk) {
       if (kk <= k1 + 5) {
-        const int sl = (kk - k0 + AX_R * 8) % AX_R;
+        const int sl = (kk - k0) & (AX_R - 1);
         T* slot = &ring[sl][0][0];
         const T* src = x + zoff(kk);
 #pragma unroll
@@ -579,11 +579,12 @@ __global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict
 #pragma unroll
     for (int l = 0; l < AX_R - 1; ++l) stage(k0 + l);
     double v0 = 0.0, v1 = 0.0;
-    for (int k = k0; k <= k1; ++k) {
+    T* __restrict__ op = out + (long long)(k0 + 3) * nxy + own;  // tile planes never wrap
+    for (int k = k0; k <= k1; ++k, op += nxy) {
       cp_wait<AX_R - 7>();  // this thread's copies of planes k .. k+5 have landed
       __syncthreads();      // everybody's have; the slot of plane k-1 is free again
       stage(k + AX_R - 1);
-      const int sl = (k - k0) % AX_R;
+      const int sl = (k - k0) & (AX_R - 1);
       const T (*sp)[AX_TW] = ring[sl];
       if (in) {
         const T c = sp[ty + 5][tx + 5];
@@ -599,9 +600,9 @@ __global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict
         for (int l = 1; l < 5; ++l) az += wz[l] * zp[l];
         az += wz[5] * c;
 #pragma unroll
-        for (int l = 6; l < AXW; ++l) az += wz[l] * ring[(sl + l - 5) % AX_R][ty + 5][tx + 5];
+        for (int l = 6; l < AXW; ++l) az += wz[l] * ring[(sl + l - 5) & (AX_R - 1)][ty + 5][tx + 5];
         const T r = ax + ay + az;
-        out[zoff(k) + own] = r;
+        *op = r;
         if (MODE == 1) v0 += (double)r * (double)dring[sl][tid];
         if (MODE == 2) {
           v0 += (double)r * (double)dring[sl][tid];
@@ -1268,6 +1269,7 @@ template <typename T>
 void Engine<T>::release() {
   if (graph_) cudaGraphExecDestroy(graph_);
   graph_ = nullptr;
+  prof::graph_release(gpairs_);
   arena_.release();
   if (partial_) cudaFree(partial_);
   if (scal_) cudaFree(scal_);
@@ -1608,12 +1610,19 @@ int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::
   k_efin<<<n, 256, 0, s_>>>(K.ts, partial_, 4, 1, EFIN_INIT, scal_, nullptr);
   prof::count(2);
   const int chunk = p_.check_every > 0 ? p_.check_every : 1;
-  const bool graphs = p_.use_graph && !prof::enabled();
-  if (graphs && !graph_) {
+  const bool profiling = prof::enabled();
+  if (graph_ && graph_prof_ != profiling) {  // the profiler was switched: capture again
+    cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+    prof::graph_release(gpairs_);
+  }
+  if (p_.use_graph && !graph_) {
     cudaGraph_t gr = nullptr;
     e = cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
+      if (profiling) prof::capture_begin();
       for (int t = 0; t < chunk; ++t) enqueue_iteration();
+      if (profiling) gpairs_ = prof::capture_end();
       e = cudaStreamEndCapture(s_, &gr);
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&graph_, gr, 0);
@@ -1621,13 +1630,15 @@ int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::
     if (e != cudaSuccess) {  // capture unavailable on this stream: launch directly from now on
       cudaGetLastError();
       graph_ = nullptr;
+      prof::graph_release(gpairs_);
       p_.use_graph = 0;
     }
+    graph_prof_ = profiling;
     prof::count(-(long long)chunk * launches_iter_);  // the capture counted launches that did not run
   }
   int launched = 0;
   for (;;) {
-    if (graph_ && p_.use_graph && !prof::enabled()) {
+    if (graph_) {
       e = cudaGraphLaunch(graph_, s_);
       if (e != cudaSuccess) return impact_set_error(e, "engine graph launch", __FILE__, __LINE__);
       prof::count((long long)chunk * launches_iter_);
@@ -1638,6 +1649,7 @@ int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::
     bool all_done = false;
     int rc = poll(all_done);
     if (rc) return rc;
+    if (graph_ && graph_prof_) prof::graph_account(gpairs_);  // the replay has completed
     bool reset = false;
     for (int c = 0; c < n; ++c)
       if (scal_host_[c].status == 4) reset = true;

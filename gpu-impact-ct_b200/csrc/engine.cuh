@@ -17,6 +17,7 @@
 
 #include "common.cuh"
 #include "mg.cuh"
+#include "prof.cuh"
 #include "solver.cuh"
 
 namespace impact {
@@ -180,6 +181,8 @@ class Engine {
   SolverScalars* scal_ = nullptr;
   SolverScalars* scal_host_ = nullptr;
   cudaGraphExec_t graph_ = nullptr;
+  bool graph_prof_ = false;          // the graph holds profiler event nodes
+  std::vector<prof::Pair> gpairs_;   // those nodes' events
   long long launches_iter_ = 0;
   // per list: cells of its grids, of the next finer and of the next coarser grids (bytes for
   // the profiler)

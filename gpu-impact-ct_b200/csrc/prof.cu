@@ -10,13 +10,11 @@ namespace impact {
 namespace prof {
 
 namespace {
-struct Pending {
-  int kid;
-  double bytes;
-  cudaEvent_t a, b;
-};
+using Pending = Pair;
 std::mutex mu;
 bool on = false;
+bool capturing = false;
+std::vector<Pair> captured;
 std::vector<cudaEvent_t> pool;
 std::vector<Pending> pending;
 std::vector<cudaEvent_t> open_start;  // token -> start event
@@ -46,7 +44,10 @@ int begin(cudaStream_t s) {
   if (!on) return -1;
   std::lock_guard<std::mutex> lk(mu);
   cudaEvent_t e = take();
-  cudaEventRecord(e, s);
+  if (capturing)
+    cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+  else
+    cudaEventRecord(e, s);
   open_start.push_back(e);
   return (int)open_start.size() - 1;
 }
@@ -55,8 +56,11 @@ void end(int token, int kid, double bytes, cudaStream_t s) {
   if (token < 0) return;
   std::lock_guard<std::mutex> lk(mu);
   cudaEvent_t e = take();
-  cudaEventRecord(e, s);
-  pending.push_back({kid, bytes, open_start[token], e});
+  if (capturing)
+    cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+  else
+    cudaEventRecord(e, s);
+  (capturing ? captured : pending).push_back({kid, bytes, open_start[token], e});
   open_start[token] = nullptr;
   // compact the token table once every open pair is closed
   bool all_closed = true;
@@ -89,6 +93,43 @@ void flush() {
 }
 
 void count(long long n) { g_count += n; }
+
+void capture_begin() {
+  std::lock_guard<std::mutex> lk(mu);
+  capturing = true;
+  captured.clear();
+}
+
+std::vector<Pair> capture_end() {
+  std::lock_guard<std::mutex> lk(mu);
+  capturing = false;
+  std::vector<Pair> out;
+  out.swap(captured);
+  return out;
+}
+
+void graph_account(const std::vector<Pair>& pairs) {
+  std::lock_guard<std::mutex> lk(mu);
+  for (const Pair& p : pairs) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    launches[p.kid] += 1;
+    total_ms[p.kid] += ms;
+    total_bytes[p.kid] += p.bytes;
+  }
+}
+
+void graph_release(std::vector<Pair>& pairs) {
+  std::lock_guard<std::mutex> lk(mu);
+  for (const Pair& p : pairs) {
+    pool.push_back(p.a);
+    pool.push_back(p.b);
+  }
+  pairs.clear();
+}
 
 }  // namespace prof
 }  // namespace impact

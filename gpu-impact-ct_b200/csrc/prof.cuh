@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 namespace impact {
 namespace prof {
 
@@ -30,6 +32,19 @@ void end(int token, int kid, double bytes, cudaStream_t s);
 // resolve every recorded pair whose stream has been synchronised
 void flush();
 void count(long long n);  // kernel launches issued by the library
+
+// CUDA graphs: between capture_begin() and capture_end() the timed pairs become event-record
+// nodes of the graph being captured; after every replay of that graph has completed,
+// graph_account() adds their times, and graph_release() returns the events.
+struct Pair {
+  int kid;
+  double bytes;
+  cudaEvent_t a, b;
+};
+void capture_begin();
+std::vector<Pair> capture_end();
+void graph_account(const std::vector<Pair>& pairs);
+void graph_release(std::vector<Pair>& pairs);
 
 }  // namespace prof
 }  // namespace impact
