@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <type_traits>
 
 #include "engine.cuh"
 #include "prof.cuh"
@@ -491,6 +492,8 @@ __device__ __forceinline__ void cp_wait() {
 //   MODE 0: rr = A phi                 (initial residual)
 //   MODE 1: Ap = A z1, partial rh.Ap   (alpha)
 //   MODE 2: Ar = A z2, partials Ar.rr, Ar.Ar (omega)
+//   MODE 3: FP64 only: r32 = (float)(bb - A phi), partials max|r|, sum r^2, sum bb^2 (the outer
+//           residual of the mixed-precision solve and the right-hand side of its inner solve)
 constexpr int AX_TW = ETX + 10, AX_TH = ETY + 10, AX_TE = AX_TW * AX_TH;
 constexpr int AX_PER = (AX_TE + ENT - 1) / ENT;  // staged elements per thread and plane
 // ring depth: planes k .. k+5 are read at plane k, the rest of the ring is in flight
@@ -527,9 +530,9 @@ __global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict
     tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
     const int i0 = i - tx, j0 = j - ty;
     const bool in = i <= g.n1 && j <= g.n2;
-    const T* __restrict__ x = MODE == 0 ? J.phi : (MODE == 1 ? J.z1 : J.z2);
+    const T* __restrict__ x = (MODE == 0 || MODE == 3) ? J.phi : (MODE == 1 ? J.z1 : J.z2);
     T* __restrict__ out = MODE == 0 ? J.rr : (MODE == 1 ? J.Ap : J.Ar);
-    const T* __restrict__ d1 = MODE == 1 ? J.rh : J.rr;
+    const T* __restrict__ d1 = MODE == 1 ? J.rh : (MODE == 3 ? J.bb : J.rr);
     const long long nxy = g.nxy;
     // weights of the tile: z rows of its planes, y rows of its 8 rows, x rows of its 32 columns
     const int nzw = (k1 - k0 + 1) * AXW;
@@ -569,18 +572,28 @@ __global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict
       cp_commit();
     };
     __syncthreads();  // weights visible
-    T wx[AXW];
+    T wx[AXW], wyr[AXW], wzr[AXW];
+    // FP32: the y weights of the row, and on uniform z the z weights, stay in registers
+    const bool zu = sizeof(T) == 4 && J.zuni != 0;
 #pragma unroll
-    for (int l = 0; l < AXW; ++l) wx[l] = wxs[l][tx];
+    for (int l = 0; l < AXW; ++l) {
+      wx[l] = wxs[l][tx];
+      wyr[l] = wys[ty][l];
+      wzr[l] = wzs[0][l];
+    }
     // the past z values x(k0-5 .. k0-1) of the column, then the ring from plane k0
     T zp[5];
 #pragma unroll
     for (int l = 0; l < 5; ++l) zp[l] = in ? x[zoff(k0 - 5 + l) + own] : T(0);
 #pragma unroll
     for (int l = 0; l < AX_R - 1; ++l) stage(k0 + l);
-    double v0 = 0.0, v1 = 0.0;
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0;
     T* __restrict__ op = out + (long long)(k0 + 3) * nxy + own;  // tile planes never wrap
-    for (int k = k0; k <= k1; ++k, op += nxy) {
+    float* __restrict__ op32 = MODE == 3 ? J.r32 + (long long)(k0 + 3) * nxy + own : nullptr;
+    auto walk = [&](auto zreg) {
+    constexpr bool ZR = decltype(zreg)::value;
+    constexpr bool YR = sizeof(T) == 4;
+    for (int k = k0; k <= k1; ++k, op += nxy, op32 += (MODE == 3 ? nxy : 0)) {
       cp_wait<AX_R - 7>();  // this thread's copies of planes k .. k+5 have landed
       __syncthreads();      // everybody's have; the slot of plane k-1 is free again
       stage(k + AX_R - 1);
@@ -591,18 +604,28 @@ __global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict
         T ax = wx[0] * sp[ty + 5][tx];
 #pragma unroll
         for (int l = 1; l < AXW; ++l) ax += wx[l] * (l == 5 ? c : sp[ty + 5][tx + l]);
-        T ay = wys[ty][0] * sp[ty][tx + 5];
+        T ay = (YR ? wyr[0] : wys[ty][0]) * sp[ty][tx + 5];
 #pragma unroll
-        for (int l = 1; l < AXW; ++l) ay += wys[ty][l] * (l == 5 ? c : sp[ty + l][tx + 5]);
+        for (int l = 1; l < AXW; ++l) ay += (YR ? wyr[l] : wys[ty][l]) * (l == 5 ? c : sp[ty + l][tx + 5]);
         const T* wz = wzs[k - k0];
-        T az = wz[0] * zp[0];
+        T az = (ZR ? wzr[0] : wz[0]) * zp[0];
 #pragma unroll
-        for (int l = 1; l < 5; ++l) az += wz[l] * zp[l];
-        az += wz[5] * c;
+        for (int l = 1; l < 5; ++l) az += (ZR ? wzr[l] : wz[l]) * zp[l];
+        az += (ZR ? wzr[5] : wz[5]) * c;
 #pragma unroll
-        for (int l = 6; l < AXW; ++l) az += wz[l] * ring[(sl + l - 5) & (AX_R - 1)][ty + 5][tx + 5];
+        for (int l = 6; l < AXW; ++l)
+          az += (ZR ? wzr[l] : wz[l]) * ring[(sl + l - 5) & (AX_R - 1)][ty + 5][tx + 5];
         const T r = ax + ay + az;
-        *op = r;
+        if (MODE == 3) {
+          const double bv = (double)dring[sl][tid];
+          const double res = bv - (double)r;
+          *op32 = (float)res;
+          v0 = fmax(v0, fabs(res));
+          v1 += res * res;
+          v2 += bv * bv;
+        } else {
+          *op = r;
+        }
         if (MODE == 1) v0 += (double)r * (double)dring[sl][tid];
         if (MODE == 2) {
           v0 += (double)r * (double)dring[sl][tid];
@@ -613,6 +636,11 @@ __global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict
         zp[4] = c;
       }
     }
+    };
+    if (zu)
+      walk(std::true_type{});
+    else
+      walk(std::false_type{});
     cp_wait<0>();
     if (MODE == 1) {
       double v[1] = {v0};
@@ -620,6 +648,9 @@ __global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict
     } else if (MODE == 2) {
       double v[2] = {v0, v1};
       tile_partials<2, 0>(v, partial + (long long)b * 4);
+    } else if (MODE == 3) {
+      double v[3] = {v0, v1, v2};
+      tile_partials<3, 1>(v, partial + (long long)b * 4);
     } else {
       __syncthreads();  // the ring and the weights are rewritten by the next tile
     }
@@ -912,6 +943,28 @@ __global__ void __launch_bounds__(ENT) k_lv_smooth(const LevelJob<T>* __restrict
   }
 }
 
+// The common case as its own kernel, for lists whose every job has several columns per thread
+// and uniform z: only the vectorised walk is compiled, which keeps the register count (and so
+// the occupancy) of the streaming loop low.  OP 0: sweep (flip as in k_lv_smooth), 1: residual.
+template <typename T, int OP, int U, int MINB>
+__global__ void __launch_bounds__(ENT, MINB) k_lv_fast(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+                                                       int nj, int ntiles, T omega, int flip) {
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const LevelJob<T>& J = jobs[q];
+    if (e_halted(J.sc)) continue;
+    const Geom g = J.g;
+    int i, j, k0, k1;
+    tile_at(g, J.kc, b - ts[q], i, j, k0, k1, VecT<T>::W);
+    const bool act = i <= g.n1 && j <= g.n2;
+    if (OP == 0)
+      march7v<T, 0, U, true>(g, i, j, k0, k1, act, J.cdg[0], J.cdg[1], J.cdg[2], omega, J.A, flip ? J.C : J.B,
+                             flip ? J.B : J.C);
+    else
+      march7v<T, 1, U, true>(g, i, j, k0, k1, act, J.cdg[0], J.cdg[1], J.cdg[2], T(0), J.A, J.B, J.C);
+  }
+}
+
 // C = A - cdg(B): the residual that restrict forms as fine1 - fine2 (fine2 = product_div_grad_relax)
 template <typename T>
 __global__ void __launch_bounds__(ENT) k_lv_resid(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
@@ -1070,9 +1123,88 @@ __device__ __forceinline__ void prolong_cols(const LevelJob<T>& J, const Geom& g
   }
 }
 
+// The same for V > 1 fine columns i .. i+V-1 (i odd) when x is coarsened by 2: they span only
+// V/2 + 1 coarse columns, so each coarse plane costs (V/2 + 1) x 2 loads instead of 4 V; every
+// fine point sees the same operations in the same order as in prolong_cols.
+template <typename T, int V>
+__device__ __forceinline__ void prolong_cols_x2(const LevelJob<T>& J, const Geom& g, int i, int j, int k0, int k1) {
+  constexpr int NC = V / 2 + 1;
+  const Geom gc = J.gc;
+  const T* __restrict__ cI3 = J.cI[2];
+  T* __restrict__ fine = J.B;
+  int yl, yh;
+  bool my;
+  bracket(j, J.rc[1], gc.n2, yl, yh, my);
+  const T wy0 = J.cI[1][2 * j], wy1 = J.cI[1][2 * j + 1];
+  T wx0[V], wx1[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    wx0[v] = J.cI[0][2 * (i + v)];
+    wx1[v] = J.cI[0][2 * (i + v) + 1];
+  }
+  const int a = (i + 1) / 2;  // coarse column of fine column i
+  int oc[NC][2];
+#pragma unroll
+  for (int m = 0; m < NC; ++m) {
+    const int cx = a + m > gc.n1 ? a + m - gc.n1 : a + m;
+    oc[m][0] = cx + gc.nx * yl;
+    oc[m][1] = cx + gc.nx * yh;
+  }
+  const T* __restrict__ c0 = J.Bc + off(gc, 0, 0, 0);
+  int zcur = -1;
+  bool have1 = false;
+  T P0[NC][2], P1[NC][2];
+  auto load = [&](int z, T (&w)[NC][2]) {
+    const T* __restrict__ cz = c0 + (long long)z * gc.nxy;
+#pragma unroll
+    for (int m = 0; m < NC; ++m) {
+      w[m][0] = cz[oc[m][0]];
+      w[m][1] = cz[oc[m][1]];
+    }
+  };
+  long long p = off(g, i, j, k0);
+  for (int k = k0; k <= k1; ++k, p += g.nxy) {
+    int zl, zh;
+    bool mz;
+    bracket(k, J.rc[2], gc.n3, zl, zh, mz);
+    if (zl != zcur) {
+      const int nxt = zcur + 1 > gc.n3 ? 1 : zcur + 1;
+      if (zcur >= 0 && have1 && zl == nxt) {
+#pragma unroll
+        for (int m = 0; m < NC; ++m) {
+          P0[m][0] = P1[m][0];
+          P0[m][1] = P1[m][1];
+        }
+      } else {
+        load(zl, P0);
+      }
+      zcur = zl;
+      have1 = false;
+    }
+    if (mz && !have1) {
+      load(zh, P1);
+      have1 = true;
+    }
+    const T wz0 = cI3[2 * k], wz1 = cI3[2 * k + 1];
+    T Y[NC];
+#pragma unroll
+    for (int m = 0; m < NC; ++m) {
+      const T Zl = mz ? wz0 * P0[m][0] + wz1 * P1[m][0] : P0[m][0];
+      const T Zh = mz ? wz0 * P0[m][1] + wz1 * P1[m][1] : P0[m][1];
+      Y[m] = my ? wy0 * Zl + wy1 * Zh : Zl;
+    }
+    T f[V];
+    vload(fine + p, f);
+#pragma unroll
+    for (int v = 0; v < V; ++v)  // even v: coincident with coarse column v/2; odd v: between two
+      f[v] = f[v] + ((v & 1) ? wx0[v] * Y[(v - 1) / 2] + wx1[v] * Y[(v + 1) / 2] : Y[v / 2]);
+    vstore(fine + p, f);
+  }
+}
+
 // this (fine) level: B += P Bc (interpolate, mod_solvers.f90:955-1141)
 template <typename T>
-__global__ void __launch_bounds__(ENT) k_lv_prolong(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+__global__ void __launch_bounds__(ENT, 2) k_lv_prolong(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
                                                     int nj, int ntiles) {
   for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
     const int q = find_job(ts, nj, b);
@@ -1082,64 +1214,18 @@ __global__ void __launch_bounds__(ENT) k_lv_prolong(const LevelJob<T>* __restric
     int i, j, k0, k1;
     tile_at(g, J.kc, b - ts[q], i, j, k0, k1, J.vw);
     if (i > g.n1 || j > g.n2) continue;
-    if (J.vw > 1)
-      prolong_cols<T, VecT<T>::W>(J, g, i, j, k0, k1);
-    else
-      prolong_cols<T, 1>(J, g, i, j, k0, k1);
+    if (J.vw > 1 && J.rc[0] == 2) {
+      prolong_cols_x2<T, VecT<T>::W>(J, g, i, j, k0, k1);
+    } else {
+      for (int v = 0; v < J.vw; ++v) prolong_cols<T, 1>(J, g, i + v, j, k0, k1);
+    }
   }
 }
 
 // ------------------------------------------------------------------------------------------
 // mixed precision: FP64 residual / conversion / correction over the MixJob list
 // ------------------------------------------------------------------------------------------
-// r64 = bb - r64 (r64 = A x on entry); partials [max|r|, sum r^2, sum bb^2]
-__global__ void __launch_bounds__(ENT) k_mx_res(const MixJob* __restrict__ jobs, const int* __restrict__ ts, int nj,
-                                                int ntiles, const SolverScalars* __restrict__ osc,
-                                                double* __restrict__ partial) {
-  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
-    const int q = find_job(ts, nj, b);
-    if (osc[q].done) continue;
-    const MixJob& J = jobs[q];
-    const Geom g = J.g;
-    int i, j, k0, k1;
-    tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
-    double v[3] = {0.0, 0.0, 0.0};
-    if (i <= g.n1 && j <= g.n2) {
-      const double* __restrict__ bb = J.bb;
-      double* __restrict__ r64 = J.r64;
-      long long p = off(g, i, j, k0);
-      for (int k = k0; k <= k1; ++k, p += g.nxy) {
-        const double bv = bb[p];
-        const double r = bv - r64[p];
-        r64[p] = r;
-        v[0] = fmax(v[0], fabs(r));
-        v[1] += r * r;
-        v[2] += bv * bv;
-      }
-    }
-    tile_partials<3, 1>(v, partial + (long long)b * 4);
-  }
-}
-// r32 = (float)(r64 / |r|_inf): the inner right-hand side normalised to |r|_inf = 1
-__global__ void __launch_bounds__(ENT) k_mx_tof32(const MixJob* __restrict__ jobs, const int* __restrict__ ts, int nj,
-                                                  int ntiles, const SolverScalars* __restrict__ osc) {
-  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
-    const int q = find_job(ts, nj, b);
-    if (osc[q].done) continue;
-    const MixJob& J = jobs[q];
-    const Geom g = J.g;
-    int i, j, k0, k1;
-    tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
-    if (i > g.n1 || j > g.n2) continue;
-    const double scale = 1.0 / J.q[0];
-    const double* __restrict__ r64 = J.r64;
-    float* __restrict__ r32 = J.r32;
-    long long p = off(g, i, j, k0);
-#pragma unroll 4
-    for (int k = k0; k <= k1; ++k, p += g.nxy) r32[p] = (float)(r64[p] * scale);
-  }
-}
-// x += |r|_inf e for the cases whose inner solve ended with status 0 or 1
+// x += e for the cases whose inner solve ended with status 0 or 1
 __global__ void __launch_bounds__(ENT) k_mx_apply(const MixJob* __restrict__ jobs, const int* __restrict__ ts, int nj,
                                                   int ntiles, const SolverScalars* __restrict__ osc) {
   for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
@@ -1152,12 +1238,11 @@ __global__ void __launch_bounds__(ENT) k_mx_apply(const MixJob* __restrict__ job
     int i, j, k0, k1;
     tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
     if (i > g.n1 || j > g.n2) continue;
-    const double unscale = J.q[0];
     const float* __restrict__ e = J.e32;
     double* __restrict__ x = J.x;
     long long p = off(g, i, j, k0);
 #pragma unroll 4
-    for (int k = k0; k <= k1; ++k, p += g.nxy) x[p] = x[p] + unscale * (double)e[p];
+    for (int k = k0; k <= k1; ++k, p += g.nxy) x[p] = x[p] + (double)e[p];
   }
 }
 
@@ -1174,6 +1259,7 @@ void ax_attributes() {
   cudaFuncSetAttribute(k_kr_ax<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
   cudaFuncSetAttribute(k_kr_ax<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
   cudaFuncSetAttribute(k_kr_ax<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
+  cudaFuncSetAttribute(k_kr_ax<double, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
   done[dev] = true;
 }
 
@@ -1282,6 +1368,7 @@ void Engine<T>::release() {
   cells_.clear();
   cells_f_.clear();
   cells_c_.clear();
+  fast_.clear();
   cs_.clear();
   built_ = false;
 }
@@ -1405,13 +1492,15 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
     return J;
   };
   auto vol = [](const Geom& g) { return (double)g.n1 * g.n2 * g.n3; };
-  auto note = [&](int list, double c, double f, double cc) {
+  auto note = [&](int list, double c, double f, double cc, bool fast = false) {
     cells_.resize(list + 1, 0.0);
     cells_f_.resize(list + 1, 0.0);
     cells_c_.resize(list + 1, 0.0);
+    fast_.resize(list + 1, 0);
     cells_[list] = c;
     cells_f_[list] = f;
     cells_c_[list] = cc;
+    fast_[list] = fast ? 1 : 0;
   };
   {
     double c = 0.0;
@@ -1424,6 +1513,7 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
     std::vector<LevelJob<T>> jobs;
     std::vector<int> tiles;
     double c = 0.0, f = 0.0, cc = 0.0;
+    bool fast = !members.empty();
     for (auto& m : members) {
       jobs.push_back(lvjob(m.first, m.second, variant));
       if (!vec) jobs.back().vw = 1;
@@ -1432,9 +1522,10 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
       c += vol(J.g);
       if (J.Cf) f += vol(J.gf);
       if (J.Bc) cc += vol(J.gc);
+      fast = fast && J.vw == VecT<T>::W && J.zuni;
     }
     const int id = arena_.add(jobs, tiles);
-    note(id, c, f, cc);
+    note(id, c, f, cc, fast);
     return id;
   };
   std::vector<int> nlev(n, 1);
@@ -1523,13 +1614,19 @@ void Engine<T>::enqueue_phase(const Phase& ph) {
       IMPACT_PROF(prof::K_MG_INIT, 2 * sz * c, s, (k_lv_smooth<T, 1><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles, om, ph.flip)));
       break;
     case PH_SWEEP:
-      IMPACT_PROF(prof::K_MG_SWEEP, 3 * sz * c, s, (k_lv_smooth<T, 0><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles, om, ph.flip)));
+      if (fast_[ph.list])
+        IMPACT_PROF(prof::K_MG_SWEEP, 3 * sz * c, s, (k_lv_fast<T, 0, 2, 1><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles, om, ph.flip)));
+      else
+        IMPACT_PROF(prof::K_MG_SWEEP, 3 * sz * c, s, (k_lv_smooth<T, 0><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles, om, ph.flip)));
       break;
     case PH_COPY:
       IMPACT_PROF(prof::K_MG_OTHER, 2 * sz * c, s, (k_lv_smooth<T, 2><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles, om, 0)));
       break;
     case PH_RESID:
-      IMPACT_PROF(prof::K_MG_RESID, 3 * sz * c, s, (k_lv_resid<T><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles)));
+      if (fast_[ph.list])
+        IMPACT_PROF(prof::K_MG_RESID, 3 * sz * c, s, (k_lv_fast<T, 1, 2, 1><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles, om, 0)));
+      else
+        IMPACT_PROF(prof::K_MG_RESID, 3 * sz * c, s, (k_lv_resid<T><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles)));
       break;
     case PH_RESTRICT:
       IMPACT_PROF(prof::K_MG_OTHER, sz * (c + cf), s, (k_lv_restrict<T><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles)));
@@ -1845,7 +1942,9 @@ int MixedEngine::build(const std::vector<Case>& cs, const EngineParams& p, cudaS
     for (int m = 0; m < 3; ++m) A.W[m] = C.W64[m];
     A.zuni = C.zuni;
     A.phi = C.x;
+    A.bb = C.bb;
     A.rr = C.r64;
+    A.r32 = C.r32;
     A.sc = oscal_ + c;
     MixJob& M = mj[c];
     M = MixJob{};
@@ -1873,7 +1972,7 @@ int MixedEngine::build(const std::vector<Case>& cs, const EngineParams& p, cudaS
 
 // Iterative refinement (no counterpart in mod_solvers.f90; the FP64 outer loop wraps the
 // reference's BiCGstab run in FP32): r = b - A x in FP64, e ~ A^-1 r by the FP32 engine on the
-// normalised r, x += |r|_inf e.  A case whose inner solve breaks down or turns non-finite has
+// FP32 image of r, x += e.  A case whose inner solve breaks down or turns non-finite has
 // its correction discarded and is retried with a looser tolerance (twice at most).
 int MixedEngine::solve(const std::vector<SolverScalars>& outer, double inner_tol, int inner_max_it, int zero_x,
                        std::vector<SolverResult>& res, std::vector<int>& inner_its) {
@@ -1909,11 +2008,11 @@ int MixedEngine::solve(const std::vector<SolverScalars>& outer, double inner_tol
   for (;;) {
     int rc = push_flags();
     if (rc) return rc;
-    // r = b - A x  (FP64, the reference operator)
-    k_kr_ax<double, 0><<<grid, kBlock, ax_smem_bytes<double>(), s_>>>(AJ, AL.ts, n, AL.ntiles, partial_);
-    k_mx_res<<<grid, kBlock, 0, s_>>>(MJ, ML.ts, n, ML.ntiles, oscal_, partial_);
-    k_efin<<<n, 256, 0, s_>>>(ML.ts, partial_, 3, 1, EFIN_RAW, nullptr, q_);
-    prof::count(3);
+    // r = b - A x in FP64 (the reference operator), stored as the FP32 right-hand side of the
+    // inner solve, with its norms
+    k_kr_ax<double, 3><<<grid, kBlock, ax_smem_bytes<double>(), s_>>>(AJ, AL.ts, n, AL.ntiles, partial_);
+    k_efin<<<n, 256, 0, s_>>>(AL.ts, partial_, 3, 1, EFIN_RAW, nullptr, q_);
+    prof::count(2);
     cudaError_t e = cudaMemcpyAsync(q_host_, q_, (size_t)n * 4 * sizeof(double), cudaMemcpyDeviceToHost, s_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s_);
     if (e != cudaSuccess) return impact_set_error(e, "mixed engine residual", __FILE__, __LINE__);
@@ -1967,8 +2066,6 @@ int MixedEngine::solve(const std::vector<SolverScalars>& outer, double inner_tol
     if (!any) break;
     rc = push_flags();
     if (rc) return rc;
-    k_mx_tof32<<<grid, kBlock, 0, s_>>>(MJ, ML.ts, n, ML.ntiles, oscal_);
-    prof::count(1);
     rc = inner_.solve(init, 1, ir);
     if (rc) return rc;
     for (int c = 0; c < n; ++c) {

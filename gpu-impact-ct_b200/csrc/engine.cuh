@@ -64,6 +64,7 @@ struct KrylovJob {
   const T* bb;
   T* phi;
   T *rr, *rh, *pp, *Ap, *Ar, *z1, *z2;
+  float* r32;  // mixed precision: FP32 image of the FP64 outer residual
   SolverScalars* sc;
 };
 
@@ -187,6 +188,7 @@ class Engine {
   // per list: cells of its grids, of the next finer and of the next coarser grids (bytes for
   // the profiler)
   std::vector<double> cells_, cells_f_, cells_c_;
+  std::vector<char> fast_;  // per list: every job vectorised with uniform z (k_lv_fast)
 };
 
 // Mixed precision: FP64 residual and correction around the FP32 engine.

@@ -39,6 +39,57 @@ __device__ __forceinline__ int crd(int a, int i, int j, int k) { return a == 0 ?
 __device__ __forceinline__ int ext(const Geom& g, int a) { return a == 0 ? g.n1 : (a == 1 ? g.n2 : g.n3); }
 __device__ __forceinline__ long long strd(const Geom& g, int a) { return a == 0 ? 1LL : (a == 1 ? (long long)g.nx : g.nxy); }
 
+// WRAP = false: the whole block lies at least 3 points inside the periodic box, so the stencil
+// points are p + l * stride without any index wrapping (same values, same operation order)
+template <int LO, int CNT, bool WRAP>
+__device__ __forceinline__ double st1w(const double* __restrict__ c, const double* __restrict__ f, const Geom& g, int a,
+                                       int i, int j, int k, long long p) {
+  if (WRAP) {
+    const int q = crd(a, i, j, k), n = ext(g, a);
+    const long long s = strd(g, a);
+    const long long base = p - (long long)q * s;
+    const double* cr = c + (long long)q * CNT;
+    double v = cr[0] * __ldg(f + base + (long long)wrapi(q + LO, n) * s);
+#pragma unroll
+    for (int l = 1; l < CNT; ++l) v = v + cr[l] * __ldg(f + base + (long long)wrapi(q + LO + l, n) * s);
+    return v;
+  }
+  const int q = crd(a, i, j, k);
+  const long long s = strd(g, a);
+  const double* cr = c + (long long)q * CNT;
+  const double* fp = f + p + (long long)LO * s;
+  double v = cr[0] * __ldg(fp);
+#pragma unroll
+  for (int l = 1; l < CNT; ++l) v = v + cr[l] * __ldg(fp + l * s);
+  return v;
+}
+template <int LO, int CNT, bool WRAP>
+__device__ __forceinline__ double st1w_acc(double v, const double* __restrict__ c, const double* __restrict__ f,
+                                           const Geom& g, int a, int i, int j, int k, long long p) {
+  if (WRAP) {
+    const int q = crd(a, i, j, k), n = ext(g, a);
+    const long long s = strd(g, a);
+    const long long base = p - (long long)q * s;
+    const double* cr = c + (long long)q * CNT;
+#pragma unroll
+    for (int l = 0; l < CNT; ++l) v = v + cr[l] * __ldg(f + base + (long long)wrapi(q + LO + l, n) * s);
+    return v;
+  }
+  const int q = crd(a, i, j, k);
+  const long long s = strd(g, a);
+  const double* cr = c + (long long)q * CNT;
+  const double* fp = f + p + (long long)LO * s;
+#pragma unroll
+  for (int l = 0; l < CNT; ++l) v = v + cr[l] * __ldg(fp + l * s);
+  return v;
+}
+// the block's points and their 3-point halos stay inside 1..n on every axis
+__device__ __forceinline__ bool block_interior(const Geom& g, int k) {
+  const int i0 = blockIdx.x * BX + 1, j0 = blockIdx.y * BY + 1;
+  return i0 - 3 >= 1 && i0 + BX - 1 + 3 <= g.n1 && j0 - 3 >= 1 && j0 + BY - 1 + 3 <= g.n2 && k - 3 >= 1 &&
+         k + 3 <= g.n3;
+}
+
 template <int LO, int CNT>
 __device__ __forceinline__ double st1(const double* __restrict__ c, const double* __restrict__ f, const Geom& g, int a,
                                       int i, int j, int k, long long p) {
@@ -68,36 +119,52 @@ __global__ void __launch_bounds__(NT) k_interp_vel3(Geom g, Coeffs<double> c, co
                                                     const double* __restrict__ v, const double* __restrict__ w,
                                                     double* __restrict__ w1, double* __restrict__ w2,
                                                     double* __restrict__ w3) {
+  const bool wrap = !block_interior(g, blockIdx.z + 1);
   PT
-  w1[p] = st1<D_LO, ND>(c.cIup[0], u, g, 0, i, j, k, p);
-  w2[p] = st1<D_LO, ND>(c.cIup[1], v, g, 1, i, j, k, p);
-  w3[p] = st1<D_LO, ND>(c.cIup[2], w, g, 2, i, j, k, p);
+  if (wrap) {
+    w1[p] = st1w<D_LO, ND, true>(c.cIup[0], u, g, 0, i, j, k, p);
+    w2[p] = st1w<D_LO, ND, true>(c.cIup[1], v, g, 1, i, j, k, p);
+    w3[p] = st1w<D_LO, ND, true>(c.cIup[2], w, g, 2, i, j, k, p);
+  } else {
+    w1[p] = st1w<D_LO, ND, false>(c.cIup[0], u, g, 0, i, j, k, p);
+    w2[p] = st1w<D_LO, ND, false>(c.cIup[1], v, g, 1, i, j, k, p);
+    w3[p] = st1w<D_LO, ND, false>(c.cIup[2], w, g, 2, i, j, k, p);
+  }
 }
 
 // rhs_vel (mod_rhs.f90:35-140) for component m: nonlinear (upwind) + Helmholtz_explicit + RK update
+template <int M, bool WRAP>
+__device__ __forceinline__ double nl_point(const Geom& g, const Coeffs<double>& c, double multL,
+                                           const double* __restrict__ vel, const double* const (&wk)[3], int i, int j,
+                                           int k, long long p) {
+  double acc = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    // pp = interpolate2_pre_vel(M, work_a): along axis M
+    const double pp = st1w<G_LO, NG, WRAP>(c.cIpu[M], wk[a], g, M, i, j, k, p);
+    const double* cU = (a == M) ? c.cNuU[a] : c.cNpU[a];
+    const double* cDn = (a == M) ? c.cNuD[a] : c.cNpD[a];
+    const double dd = st1w<B_LO, NB, WRAP>(pp >= 0.0 ? cU : cDn, vel, g, a, i, j, k, p);
+    acc = (a == 0) ? dd * pp : acc + dd * pp;
+  }
+  // Helmholtz_explicit: x, y, z second derivatives of vel_M
+  double lap = st1w<B_LO, NB, WRAP>(M == 0 ? c.cuu[0] : c.cpp[0], vel, g, 0, i, j, k, p);
+  lap = st1w_acc<B_LO, NB, WRAP>(lap, M == 1 ? c.cuu[1] : c.cpp[1], vel, g, 1, i, j, k, p);
+  lap = st1w_acc<B_LO, NB, WRAP>(lap, M == 2 ? c.cuu[2] : c.cpp[2], vel, g, 2, i, j, k, p);
+  return acc - multL * lap;
+}
+
 template <int M>
 __global__ void __launch_bounds__(NT) k_nl_rhs(Geom g, Coeffs<double> c, double multL, double mult_b, double mult_a,
                                                int use_old, const double* __restrict__ vel,
                                                const double* __restrict__ work1, const double* __restrict__ work2,
                                                const double* __restrict__ work3, double* __restrict__ nl,
                                                double* __restrict__ rhs) {
+  const bool wrap = !block_interior(g, blockIdx.z + 1);
   PT
-  const double* wk[3] = {work1, work2, work3};
-  double acc = 0.0;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    // pp = interpolate2_pre_vel(M, work_a): along axis M
-    const double pp = st1<G_LO, NG>(c.cIpu[M], wk[a], g, M, i, j, k, p);
-    const double* cU = (a == M) ? c.cNuU[a] : c.cNpU[a];
-    const double* cDn = (a == M) ? c.cNuD[a] : c.cNpD[a];
-    const double dd = st1<B_LO, NB>(pp >= 0.0 ? cU : cDn, vel, g, a, i, j, k, p);
-    acc = (a == 0) ? dd * pp : acc + dd * pp;
-  }
-  // Helmholtz_explicit: x, y, z second derivatives of vel_M
-  double lap = st1<B_LO, NB>(M == 0 ? c.cuu[0] : c.cpp[0], vel, g, 0, i, j, k, p);
-  lap = st1_acc<B_LO, NB>(lap, M == 1 ? c.cuu[1] : c.cpp[1], vel, g, 1, i, j, k, p);
-  lap = st1_acc<B_LO, NB>(lap, M == 2 ? c.cuu[2] : c.cpp[2], vel, g, 2, i, j, k, p);
-  const double nln = acc - multL * lap;
+  const double* const wk[3] = {work1, work2, work3};
+  const double nln = wrap ? nl_point<M, true>(g, c, multL, vel, wk, i, j, k, p)
+                          : nl_point<M, false>(g, c, multL, vel, wk, i, j, k, p);
   double r = vel[p];
   if (use_old) r = r - mult_b * nl[p];
   r = r - mult_a * nln;
@@ -116,10 +183,17 @@ __global__ void __launch_bounds__(NT) k_project(Geom g, Coeffs<double> c, const 
                                                 const double* __restrict__ r1, const double* __restrict__ r2,
                                                 const double* __restrict__ r3, double* __restrict__ u,
                                                 double* __restrict__ v, double* __restrict__ w) {
+  const bool wrap = !block_interior(g, blockIdx.z + 1);
   PT
-  u[p] = 1.0 * r1[p] + (-1.0) * st1<G_LO, NG>(c.cG[0], pre, g, 0, i, j, k, p);
-  v[p] = 1.0 * r2[p] + (-1.0) * st1<G_LO, NG>(c.cG[1], pre, g, 1, i, j, k, p);
-  w[p] = 1.0 * r3[p] + (-1.0) * st1<G_LO, NG>(c.cG[2], pre, g, 2, i, j, k, p);
+  if (wrap) {
+    u[p] = 1.0 * r1[p] + (-1.0) * st1w<G_LO, NG, true>(c.cG[0], pre, g, 0, i, j, k, p);
+    v[p] = 1.0 * r2[p] + (-1.0) * st1w<G_LO, NG, true>(c.cG[1], pre, g, 1, i, j, k, p);
+    w[p] = 1.0 * r3[p] + (-1.0) * st1w<G_LO, NG, true>(c.cG[2], pre, g, 2, i, j, k, p);
+  } else {
+    u[p] = 1.0 * r1[p] + (-1.0) * st1w<G_LO, NG, false>(c.cG[0], pre, g, 0, i, j, k, p);
+    v[p] = 1.0 * r2[p] + (-1.0) * st1w<G_LO, NG, false>(c.cG[1], pre, g, 1, i, j, k, p);
+    w[p] = 1.0 * r3[p] + (-1.0) * st1w<G_LO, NG, false>(c.cG[2], pre, g, 2, i, j, k, p);
+  }
 }
 
 // get_dtime (mod_lib.f90:46-250), timeint_mode 1: block max of radius / stabilitylimit(angle)
@@ -605,7 +679,7 @@ static EngineParams engine_params(const CaseState& s, const impact_b200_solver_p
   ep.omega = p->omega;
   ep.check_every = p->check_every > 0 ? p->check_every : 1;
   const char* kc = std::getenv("IMPACT_B200_KC");
-  ep.kc = kc ? std::atoi(kc) : 16;
+  ep.kc = p->tile_kc > 0 ? p->tile_kc : (kc ? std::atoi(kc) : 32);
   ep.kc = ep.kc < 1 ? 1 : (ep.kc > KC_MAX ? KC_MAX : ep.kc);
   ep.use_graph = std::getenv("IMPACT_B200_NO_GRAPH") ? 0 : 1;
   (void)s;
@@ -800,10 +874,19 @@ extern "C" int impact_b200_case_precond(impact_b200_case* c, int field_in, int f
 
 extern "C" int impact_b200_case_apply(impact_b200_case* c, int op, int field_in, int field_out) {
   if (!c || field_in < 0 || field_out < 0 || field_in >= IMPACT_B200_NFIELDS || field_out >= IMPACT_B200_NFIELDS ||
-      field_in == field_out || op != 0)
+      field_in == field_out || op < 0 || op > 1)
     return impact_set_error_msg(-1, "impact_b200_case_apply: bad arguments");
   CaseState& s = c->s;
   IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  if (op == 1) {  // field_out = divergence2 of the velocity (field_in unused)
+    if (field_out <= IMPACT_B200_VEL3) return impact_set_error_msg(-1, "impact_b200_case_apply: output overlaps the velocity");
+    launch_divergence2<double>(s.g, s.c64.cD[0], s.c64.cD[1], s.c64.cD[2], s.f[IMPACT_B200_VEL1], s.f[IMPACT_B200_VEL2],
+                               s.f[IMPACT_B200_VEL3], s.f[field_out], s.stream);
+    prof::count(1);
+    IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
+    IMPACT_CUDA_CHECK(cudaGetLastError());
+    return 0;
+  }
   impact_b200_solver_params p{};
   p.precond = 0;
   p.omega = 0.8;

@@ -51,7 +51,8 @@ class SolverParams(C.Structure):
     _fields_ = [("tol_rel", C.c_double), ("tol_abs_inf", C.c_double), ("max_it", C.c_int),
                 ("n_sweeps", C.c_int), ("omega", C.c_double), ("init_yes", C.c_int),
                 ("check_every", C.c_int), ("inner_tol_rel", C.c_double), ("inner_max_it", C.c_int),
-                ("precond", C.c_int), ("mg_down", C.c_int), ("mg_up", C.c_int), ("mg_bottom", C.c_int)]
+                ("precond", C.c_int), ("mg_down", C.c_int), ("mg_up", C.c_int), ("mg_bottom", C.c_int),
+                ("tile_kc", C.c_int)]
 
 
 class SolverResult(C.Structure):
@@ -221,11 +222,12 @@ class Grid:
 
 
 def solver_params(tol_rel=1e-8, tol_abs_inf=0.0, max_it=2000, n_sweeps=4, omega=0.8, init_yes=0,
-                  check_every=4, inner_tol_rel=1e-4, inner_max_it=0, precond=0, mg_down=4, mg_up=4,
-                  mg_bottom=4) -> SolverParams:
-    """precond 0: n_sweeps damped-Jacobi sweeps; 1: multigrid V-cycle (mg_down/up/bottom sweeps)."""
+                  check_every=4, inner_tol_rel=1e-3, inner_max_it=0, precond=0, mg_down=4, mg_up=4,
+                  mg_bottom=4, tile_kc=0) -> SolverParams:
+    """precond 0: n_sweeps damped-Jacobi sweeps; 1: multigrid V-cycle (mg_down/up/bottom sweeps).
+    tile_kc: z-planes per tile of the solver kernels (0: library default)."""
     return SolverParams(tol_rel, tol_abs_inf, max_it, n_sweeps, omega, init_yes, check_every,
-                        inner_tol_rel, inner_max_it, precond, mg_down, mg_up, mg_bottom)
+                        inner_tol_rel, inner_max_it, precond, mg_down, mg_up, mg_bottom, tile_kc)
 
 
 def step_params(Re=200.0, CFL=0.2, dtime_max=1e-2, dtime0=1e9, U0=1.0, T_pulse=1.0, level_pressure=1,
@@ -310,7 +312,7 @@ class Case:
         return ms.value, by.value
 
     def apply(self, field_in="pre", field_out="res", op: int = 0):
-        """field_out = A field_in; op 0: product_div_grad in FP64"""
+        """op 0: field_out = A field_in (product_div_grad); op 1: field_out = div(velocity)"""
         fi = FIELDS[field_in] if isinstance(field_in, str) else field_in
         fo = FIELDS[field_out] if isinstance(field_out, str) else field_out
         check(lib().impact_b200_case_apply(self._h, op, fi, fo), "case_apply")

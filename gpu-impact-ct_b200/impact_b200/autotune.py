@@ -1,0 +1,64 @@
+"""Autotuner of the pressure solve: tile depth of the solver kernels and multigrid sweep schedule.
+
+The kernels of the Poisson engine cut every grid into tiles of 32 x 8 columns and `tile_kc`
+z-planes; deeper tiles stream longer columns (fewer tile start-ups), shallower ones give more
+tiles to fill the 148 SMs on small grids and coarse levels.  The V-cycle's sweep counts trade
+the cost of one preconditioner application against the number of BiCGstab iterations.  Both are
+chosen here by timing complete Poisson solves of the case's own current right-hand side to the
+requested tolerance, one per candidate, on the device, and keeping the fastest candidate that
+converged.  Results are cached per (grid, precision, device) for the life of the process.
+"""
+from __future__ import annotations
+
+import copy
+import time
+
+from . import Case, SolverParams
+
+TILE_KC = (8, 16, 32, 64)
+SWEEPS = ((2, 2, 2), (3, 3, 3), (4, 4, 4))
+
+_cache: dict = {}
+
+
+def _with(base: SolverParams, kc: int, sw) -> SolverParams:
+    p = copy.copy(base)
+    p.tile_kc = kc
+    p.mg_down, p.mg_up, p.mg_bottom = sw
+    return p
+
+
+def tune(case: Case, base: SolverParams, tile_kc=TILE_KC, sweeps=SWEEPS, rhs="res", scratch="rhs1",
+         repeats: int = 1, use_cache: bool = True):
+    """Time Poisson solves A x = rhs (x from zero, written into `scratch`, which the next time step
+    recomputes anyway) for every candidate and return (best SolverParams, report).  The case should
+    hold a realistic right-hand side, e.g. after one time step.  Multigrid candidates only when
+    base.precond == 1; otherwise only the tile depth is tuned."""
+    key = (tuple(case.grid.N), case.precision, base.precond, base.tol_rel, base.omega)
+    if use_cache and key in _cache:
+        return _cache[key]
+    cands = [(kc, sw) for kc in tile_kc for sw in (sweeps if base.precond == 1 else [(base.mg_down, base.mg_up,
+                                                                                       base.mg_bottom)])]
+    report = []
+    best = None
+    for kc, sw in cands:
+        p = _with(base, kc, sw)
+        p.init_yes = 1
+        case.poisson(rhs, scratch, p)  # builds the engine and its graphs
+        t0 = time.perf_counter()
+        for _ in range(repeats):
+            r = case.poisson(rhs, scratch, p)  # returns after the device has finished
+        ms = 1e3 * (time.perf_counter() - t0) / repeats
+        ok = r.status == 0
+        report.append({"tile_kc": kc, "sweeps": list(sw), "ms": round(ms, 3), "iterations": r.iterations,
+                       "inner_iterations": r.inner_iterations, "converged": ok})
+        if ok and (best is None or ms < best[0]):
+            best = (ms, kc, sw)
+    if best is None:
+        chosen = copy.copy(base)
+    else:
+        chosen = _with(base, best[1], best[2])
+    out = (chosen, report)
+    if use_cache:
+        _cache[key] = out
+    return out

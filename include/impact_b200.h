@@ -174,6 +174,8 @@ typedef struct {
   int precond;         /* 0: n_sweeps damped-Jacobi sweeps; 1: multigrid V-cycle (multigridV,
                           mod_solvers.f90:456-585; needs the coordinates at case creation) */
   int mg_down, mg_up, mg_bottom; /* V-cycle sweeps (n_relax_down / _up / _bottom), relaxation omega */
+  int tile_kc;         /* z-planes per tile of the solver kernels (0: library default); chosen by
+                          the autotuner of the Python package, no counterpart in the reference */
 } impact_b200_solver_params;
 
 typedef struct {
@@ -190,8 +192,9 @@ int impact_b200_case_poisson(impact_b200_case* c, int field_b, int field_x, cons
 
 /* Apply the preconditioner of p once: field_out = M field_in (FP64 cases). */
 int impact_b200_case_precond(impact_b200_case* c, int field_in, int field_out, const impact_b200_solver_params* p);
-/* field_out = A field_in for op 0: product_div_grad (mod_laplace.f90:38-197), the operator of the
- * pressure Poisson solve, in FP64 on the resident fields. */
+/* op 0: field_out = A field_in, product_div_grad (mod_laplace.f90:38-197), the operator of the
+ * pressure Poisson solve; op 1: field_out = divergence2 of the resident velocity (mod_diff.f90:
+ * 130-215; field_in unused).  FP64, on the resident fields. */
 int impact_b200_case_apply(impact_b200_case* c, int op, int field_in, int field_out);
 /* levels of the multigrid hierarchy of the case (0 when it has none) */
 int impact_b200_case_mg_levels(impact_b200_case* c);

@@ -1,0 +1,35 @@
+"""The solver autotuner: every candidate (tile depth x multigrid sweep schedule) is timed on a
+complete Poisson solve of the case's own right-hand side, the fastest converged one is returned,
+and it leaves the case's state untouched (the next step equals a run without tuning)."""
+import numpy as np
+import pytest
+
+import impact_b200 as I
+from impact_b200 import autotune as A
+from impact_b200 import geometry as G
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(precision):
+    g = I.Grid((33, 33, 65), (1.0, 1.0, 2.0))
+    c = I.Case(g, precision=precision)
+    c.set_labels(G.straight_vessel(g, stenoses=[(1.0, 0.5, 0.125)]))
+    return c
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
+def test_autotune_picks_a_converged_candidate(precision):
+    p = I.step_params(Re=300.0, tol_rel=1e-8, omega=0.8, precond=1, max_it=200 if precision == 0 else 40)
+    ref = _case(precision)
+    ref.step(p, 2)
+    c = _case(precision)
+    c.step(p, 1)
+    best, report = A.tune(c, p.poisson, tile_kc=(8, 32), sweeps=((2, 2, 2), (4, 4, 4)), use_cache=False)
+    assert len(report) == 4 and all(r["converged"] for r in report)
+    fastest = min(report, key=lambda r: r["ms"])
+    assert (best.tile_kc, [best.mg_down, best.mg_up, best.mg_bottom]) == (fastest["tile_kc"], fastest["sweeps"])
+    # tuning only wrote the scratch field: the next step matches the untuned run
+    c.step(p, 1)
+    for f in ("vel1", "vel2", "vel3", "pre"):
+        assert np.array_equal(c.download(f), ref.download(f))

@@ -65,3 +65,16 @@ def test_step_mixed_matches_oracle(precond):
     umax = max(np.abs(og.interior(vel[m])).max() for m in range(3))
     for m in range(3):
         assert np.abs(og.interior(got[m]) - og.interior(vel[m])).max() <= 1e-6 * umax
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
+def test_step_wide_grid_matches_oracle(precision):
+    """A grid wide enough for thread blocks whose 3-point halos stay inside the box (the kernels'
+    unwrapped fast path) next to blocks at the periodic boundary (the wrapped path)."""
+    og, vel, pre, hist, case, got, dh = _run(precision, nsteps=2, N=(97, 25, 33), L=(4.0, 1.0, 1.0), precond=1)
+    for (dt_o, _), (dt_g, _, stat) in zip(hist, dh):
+        assert abs(dt_g - dt_o) <= 1e-9 * dt_o
+        assert all(s == 0 for s in stat)
+    umax = max(np.abs(og.interior(vel[m])).max() for m in range(3))
+    for m in range(3):
+        assert np.abs(og.interior(got[m]) - og.interior(vel[m])).max() <= 1e-6 * umax
