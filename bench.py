@@ -7,11 +7,11 @@ Workload (default, the mixed-precision single case of the benchmark suite): sten
 Gaussian constriction at mid-length (60 % area reduction, sigma = 0.5 R); pulsatile plug inflow
 u_z = U0 (1 + 0.5 sin(2 pi t / T)), U0 = 1, T = 1, on the label-5 buffer; Re = 500; dt = 0.2 x the
 RK3 stability limit (get_dtime with CFL = 0.2); every Poisson solve is BiCGstab with the
-multigrid V-cycle preconditioner (damped Jacobi, omega = 0.8, 4/4/4 sweeps) to
-||b - A x||_2 <= 1e-8 ||b||_2: FP32 inner solve with FP64 refinement (the line), plain FP64
-beside it.  Starts from rest.  One
-"step" is one RK3 time step (3 substeps, 3 Poisson solves).  Fields are ~0.95 GB each, far
-larger than L2, so no flush is needed between steps.
+multigrid V-cycle preconditioner (damped Jacobi, omega = 0.8; sweeps and tile depth chosen by the
+autotuner during warm-up) to ||b - A x||_2 <= 1e-8 ||b||_2: FP32 inner solve with FP64 refinement
+(the line), plain FP64 beside it.  Starts from rest.  One "step" is one RK3 time step (3
+substeps, 3 Poisson solves).  Fields are ~0.95 GB each, far larger than L2, so no flush is
+needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size n]
 
@@ -52,10 +52,15 @@ def parse():
     ap.add_argument("--inner-tol", type=float, default=1e-3)
     ap.add_argument("--precond", type=int, default=1, help="0: JOR sweeps, 1: multigrid V-cycle (default)")
     ap.add_argument("--check-every", type=int, default=2)
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "kernels"],
                     help="single: the 384 mixed case (default line, with short batch and serve samples); "
-                         "batch / serve: the full batched or serving workload as the line")
+                         "batch / serve: the full batched or serving workload as the line; kernels: per-kernel "
+                         "micro-benchmark on resident random fields (the small case for profilers)")
+    ap.add_argument("--kernels", default="all", help="kernels: comma-separated names to run (default all)")
+    ap.add_argument("--iters", type=int, default=20, help="kernels: timed launches per kernel")
     ap.add_argument("--no-extra", action="store_true", help="skip the batch and serve samples of the default line")
+    ap.add_argument("--no-tune", action="store_true", help="keep tile depth 32 and 4/4/4 sweeps (no autotuning)")
+    ap.add_argument("--no-profile", action="store_true", help="no per-kernel events in the timed steps (no roofline)")
     ap.add_argument("--cases", type=int, default=48, help="batch: number of cases")
     ap.add_argument("--requests", type=int, default=16, help="serve: number of requests")
     ap.add_argument("--case-steps", type=int, default=0, help="batch / serve: time steps per case (0: the spec's)")
@@ -66,7 +71,8 @@ def workload(n):
     return {"workload": f"stenosed-vessel-{n}x{n}x{2 * n}", "cells": n * n * 2 * n, "box": [1.0, 1.0, 2.0],
             "radius": 0.25, "stenosis": {"z": 1.0, "area_reduction": 0.6, "sigma": 0.125}, "Re": 500.0,
             "inflow": "U0 (1 + 0.5 sin(2 pi t / T)), U0 = 1, T = 1", "dt": "0.2 x CFL limit",
-            "poisson": "BiCGstab + multigrid V-cycle (damped-Jacobi omega=0.8, 4/4/4 sweeps) to 1e-8 relative", "start": "rest",
+            "poisson": "BiCGstab + multigrid V-cycle (damped Jacobi, omega 0.8, sweeps and tile depth autotuned) to 1e-8 "
+                       "relative", "start": "rest",
             "l2_flush": "not needed: every field (0.95 GB at 384) exceeds the 126 MB L2"}
 
 
@@ -179,8 +185,17 @@ def run_arm(args, precision, device, rank, world, dist, profile_on, e2e_on):
 
     grid, lab, case = build_case(args.size, precision, device)
     sp = step_params(args, precision)
-    for _ in range(args.warmup):
+    tuning = None
+    for w in range(args.warmup):
         case.step(sp)
+        # from rest the first step's Poisson right-hand side is zero: tune on the second one's
+        if w == min(1, args.warmup - 1) and not args.no_tune:
+            # tile depth and V-cycle sweeps by timing whole Poisson solves of this case (untimed)
+            from impact_b200 import autotune
+            best, report = autotune.tune(case, sp.poisson, tile_kc=(16, 32, 64), sweeps=((2, 2, 2), (3, 3, 3), (4, 4, 4)))
+            sp.poisson = best
+            tuning = {"chosen": {"tile_kc": best.tile_kc, "sweeps": [best.mg_down, best.mg_up, best.mg_bottom]},
+                      "candidates": report}
     stream = torch.cuda.ExternalStream(case.stream, device=device)
     # pinned host copies of the state the Fortran host owns between steps (velocity, pressure,
     # nonlinear term): uploaded before and downloaded after every step, as a drop-in call would
@@ -192,10 +207,8 @@ def run_arm(args, precision, device, rank, world, dist, profile_on, e2e_on):
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize(device)
-    if profile_on:
-        I.profile(True)
     launches0 = I.launch_count()
-    sampler = ClockSampler(device) if rank == 0 and profile_on else None
+    sampler = ClockSampler(device) if rank == 0 and e2e_on else None
     t_dev, t_e2e, its, inner, stats = 0.0, 0.0, [], [], []
     for _ in range(args.steps):
         e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
@@ -217,19 +230,35 @@ def run_arm(args, precision, device, rank, world, dist, profile_on, e2e_on):
     torch.cuda.synchronize(device)
     launches = I.launch_count() - launches0
     clocks = sampler.stop() if sampler else None
-    prof = I.profile_read() if profile_on else None
-    if profile_on:
-        I.profile(False)
     if dist is not None:
         t_dev, t_e2e = max_over_ranks(dist, [t_dev, t_e2e], f"cuda:{device}")
     out = {"ms_dev": t_dev, "ms_e2e": t_e2e, "iterations": its, "inner_iterations": inner, "status": stats,
-           "launches": launches, "clocks": clocks, "prof": prof, "bytes_in": bytes_in, "bytes_out": bytes_out,
+           "tuning": tuning,
+           "launches": launches, "clocks": clocks, "prof": None, "bytes_in": bytes_in, "bytes_out": bytes_out,
            "dt": st.dtime, "time": st.time}
     fields = None
     if rank == 0:
         fields = {f: case.download(f) for f in ("vel1", "vel2", "vel3", "pre", "nl1", "nl2", "nl3")}
         case.apply("vel1", "res", op=1)  # discrete divergence of the final velocity
         fields["div"] = case.download("res")
+    if profile_on:
+        # per-kernel device times over K further steps of the same case: the events around every
+        # launch (event nodes inside the replayed graphs) slow a step down by about a sixth, so
+        # the timed steps above run without them
+        torch.cuda.synchronize(device)
+        I.profile(True)
+        t_prof = 0.0
+        for _ in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            case.step(sp)
+            b.record(stream)
+            b.synchronize()
+            t_prof += a.elapsed_time(b)
+        torch.cuda.synchronize(device)
+        out["prof"] = I.profile_read()
+        out["ms_prof"] = t_prof
+        I.profile(False)
     case.close()
     del case
     torch.cuda.empty_cache()
@@ -504,10 +533,18 @@ def main():
     else:
         torch.cuda.set_device(0)
     device = local if world > 1 else 0
+    if args.workload == "kernels":
+        if rank == 0:
+            kernels_main(args, device)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.workload != "single":
         extra_main(args, device, rank, world, dist)
         return
-    mixed, fields, grid, lab = run_arm(args, 1, device, rank, world, dist, profile_on=True, e2e_on=True)
+    mixed, fields, grid, lab = run_arm(args, 1, device, rank, world, dist, profile_on=not args.no_profile,
+                                       e2e_on=True)
     fp64 = None
     if not args.no_fp64:
         fp64, fields64, _, _ = run_arm(args, 0, device, rank, world, dist, profile_on=False, e2e_on=False)
@@ -533,7 +570,10 @@ def main():
                 "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peak_note,
                 "traffic": (tpc * cells) if tpc else None, "algorithmic_bytes_per_launch": per_launch_bytes,
                 "launches": launches, "avg_launch_ms": ms / launches,
-                "share_of_step": round(ms / mixed["ms_dev"], 3),
+                "share_of_step": round(ms / mixed["ms_prof"], 3),
+                "measured_over": (f"{K} further steps of the same case after the timed ones, CUDA events around every "
+                                  f"launch on the case stream ({mixed['ms_prof'] / K:.1f} ms per step with the events, "
+                                  f"{mixed['ms_dev'] / K:.1f} ms without)"),
                 "all_kernels": {k: {"launches": v[0], "ms": round(v[1], 2),
                                     "GB/s": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] > 0 else None}
                                 for k, v in prof.items() if v[0] > 0}}
@@ -546,12 +586,13 @@ def main():
                     "d2h_bytes_per_step": mixed["bytes_out"]},
             "gpu_launches": mixed["launches"], "clocks": mixed["clocks"], "roofline": roof,
             "solver": {"mixed_outer_per_substep": mixed["iterations"], "mixed_inner_per_substep": mixed["inner_iterations"],
-                       "status": mixed["status"], "dt": mixed["dt"]}}
+                       "status": mixed["status"], "dt": mixed["dt"], "autotune": mixed["tuning"]}}
     if fp64 is not None:
         import numpy as np
         v64 = world * cells * K / (fp64["ms_dev"] / 1e3) / 1e6
         line["fp64"] = {"value": round(v64, 3), "unit": UNIT, "ms_per_step": fp64["ms_dev"] / K,
-                        "iterations_per_substep": fp64["iterations"], "status": fp64["status"]}
+                        "iterations_per_substep": fp64["iterations"], "status": fp64["status"],
+                        "autotune": (fp64["tuning"] or {}).get("chosen")}
         line["mixed_over_fp64"] = round(value / v64, 3)
         if fields is not None and fields64 is not None:
             sl = (slice(4, -4), slice(4, -4), slice(4, -4))  # interior points
@@ -575,6 +616,52 @@ def main():
         except Exception as ex:  # the CPU sample must never hide the device number
             line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
     print(json.dumps(line), flush=True)
+
+
+# kernel micro-benchmark: (name, precision, entry, id, algorithmic bytes per cell at that precision)
+# entry "step": impact_b200_case_kernel_bench (FP64 passes of the time step); "engine":
+# impact_b200_case_engine_bench on the finest level (FP64, or FP32 = the inner solve of a mixed case)
+KERNELS = [("rhs_vel_1", 0, "step", 10, 56), ("rhs_vel_2", 0, "step", 11, 56), ("rhs_vel_3", 0, "step", 12, 56),
+           ("interpolate_vel", 0, "step", 13, 48), ("project", 0, "step", 14, 56), ("divergence2", 0, "step", 15, 32)]
+ENGINE = [("mg_sweep", 0), ("mg_init", 1), ("mg_residual", 2), ("mg_prolong", 3), ("mg_restrict", 4), ("ax_dot", 5),
+          ("ax_dot2", 6), ("x_update", 7), ("p_update", 8), ("r_update", 9), ("vcycle", 10), ("bicgstab_iteration", 11)]
+for _nm, _k in ENGINE:
+    KERNELS += [(_nm + "_f64", 0, "engine", _k, None), (_nm + "_f32", 1, "engine", _k, None)]
+
+
+def kernels_main(args, device):
+    """Average device time of every hot kernel (or of the --kernels subset), --iters launches each
+    on resident seeded U[-1, 1] fields of the --size grid, CUDA events on the case stream."""
+    import numpy as np
+
+    import impact_b200 as I
+    want = None if args.kernels == "all" else set(args.kernels.split(","))
+    sel = [k for k in KERNELS if want is None or k[0] in want]
+    n = args.size
+    cells = n * n * 2 * n
+    out = {}
+    for prec in (0, 1):
+        todo = [k for k in sel if k[1] == prec]
+        if not todo:
+            continue
+        grid = I.Grid((n + 1, n + 1, 2 * n + 1), (1.0, 1.0, 2.0))
+        case = I.Case(grid, precision=prec, device=device)
+        rng = np.random.default_rng(5)
+        for f in ("vel1", "vel2", "vel3", "pre", "nl1", "nl2", "nl3", "res"):
+            case.upload(f, rng.uniform(-1.0, 1.0, grid.shape))
+        if any(k[2] == "step" for k in todo):
+            case.kernel_bench(13, 1)  # interpolated velocities for the rhs_vel passes
+        sp = I.solver_params(precond=1, omega=0.8, tile_kc=32)
+        for name, _, entry, kid, bpc in todo:
+            if entry == "step":
+                ms = case.kernel_bench(kid, args.iters)
+                byts = bpc * cells
+            else:
+                ms, byts = case.engine_bench(kid, args.iters, sp)
+            out[name] = {"ms": round(ms, 4), "GB/s": round(byts / (ms / 1e3) / 1e9, 1) if byts else None}
+        case.close()
+    print(json.dumps({"workload": f"kernels-{n}x{n}x{2 * n}", "cells": cells, "iters": args.iters,
+                      "fields": "seeded U[-1, 1]", "kernels": out}), flush=True)
 
 
 def extra_main(args, device, rank, world, dist):

@@ -1,0 +1,281 @@
+// rhs.cu -- rhs_vel of one velocity component as a z-marching shared-memory stencil pass.
+//
+// rhs_vel (mod_rhs.f90:35-140) for component m forms, at every u_m point,
+//   pp_a  = interpolate2_pre_vel(m, work_a)            (6-point, along axis m; mod_diff.f90:1567-1648)
+//   nl_m  = sum_a pp_a * D^{up/down}_a vel_m           (7-point upwind-biased set chosen by the sign
+//                                                       of pp_a; mod_diff.f90:784-1424)
+//         - (1/Re) sum_a D2_a vel_m                    (Helmholtz_explicit, mod_diff.f90:549-762)
+//   rhs_m = vel_m - dt bRK nl_m(old) - dt aRK nl_m(new)
+// with the reference's operation order per point (each stencil sums its terms in table order;
+// the advective terms and the three second derivatives accumulate axis by axis).
+//
+// A block owns TX x TY = 32 x 8 columns and walks them along z over KZ planes.  Every plane of
+// vel_m (with its 3-wide x/y halo, periodic images) and of the three work fields (with the
+// halo of the interpolation along axis m) is staged into a ring of R shared-memory slots by
+// cp.async, R-4 planes ahead of its use.  The x and y neighbours come from the ring, the z
+// values of the column from register windows: vel_m at k-3..k+3 and, for m = 3, work_a at
+// k-2..k+3.  x coefficient rows (one per thread column) are staged once per block, transposed;
+// y rows are warp-uniform and z rows block-uniform, read through the read-only cache.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "rhs.cuh"
+
+namespace impact {
+namespace {
+
+constexpr int RTX = 32, RTY = 8, RNT = RTX * RTY;
+constexpr int RR = 7;                                 // ring slots: planes c .. c+3 resident, 3 in flight
+constexpr int VW = RTX + 6, VH = RTY + 6, VE = VW * VH;  // vel tile with the 3-wide halo
+constexpr int NXR = 27;                               // x coefficient rows: U 7, D 7, D2 7, I 6
+
+template <int M>
+struct WTile {  // work tile of one field: halo -2..3 along axis M only
+  static constexpr int W = M == 0 ? RTX + 5 : RTX;
+  static constexpr int H = M == 1 ? RTY + 5 : RTY;
+  static constexpr int E = W * H;
+};
+template <int M>
+constexpr int slot_elems() { return VE + 3 * WTile<M>::E; }
+template <int M>
+constexpr size_t rhs_smem_bytes() { return sizeof(double) * ((size_t)RR * slot_elems<M>() + (size_t)NXR * RTX); }
+
+// periodic image of index i in 1..n, for any integer i
+__device__ __forceinline__ int wrapg(int i, int n) {
+  int r = (i - 1) % n;
+  if (r < 0) r += n;
+  return r + 1;
+}
+
+__device__ __forceinline__ void cpa8(double* smem, const double* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <int M>
+__global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, double multL, double mult_b,
+                                                      double mult_a, int use_old, int kz,
+                                                      const double* __restrict__ vel, const double* __restrict__ wk0,
+                                                      const double* __restrict__ wk1, const double* __restrict__ wk2,
+                                                      double* __restrict__ nl, double* __restrict__ rhs) {
+  using WT = WTile<M>;
+  constexpr int SE = slot_elems<M>();
+  constexpr int VPER = (VE + RNT - 1) / RNT;
+  constexpr int WPER = (3 * WT::E + RNT - 1) / RNT;
+  extern __shared__ __align__(16) double rsm[];
+  double* ring = rsm;                      // RR slots of SE doubles: vel tile, then work tiles 0..2
+  double* sx = rsm + (size_t)RR * SE;      // NXR x RTX transposed x rows
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + RTX * ty;
+  const int i0 = blockIdx.x * RTX + 1, j0 = blockIdx.y * RTY + 1;
+  const int k0 = blockIdx.z * kz + 1;
+  const int k1 = min(k0 + kz - 1, g.n3);
+  const int i = i0 + tx, j = j0 + ty;
+  const bool in = i <= g.n1 && j <= g.n2;
+  const int jr = wrapg(j, g.n2);  // y coefficient row (valid for idle threads too)
+
+  // x rows of this block's columns, transposed: sx[l][tx]
+  {
+    const double* xU = M == 0 ? c.cNuU[0] : c.cNpU[0];
+    const double* xD = M == 0 ? c.cNuD[0] : c.cNpD[0];
+    const double* xH = M == 0 ? c.cuu[0] : c.cpp[0];
+    for (int t = tid; t < NXR * RTX; t += RNT) {
+      const int l = t / RTX, col = t % RTX;
+      const int row = wrapg(i0 + col, g.n1);
+      double v;
+      if (l < 7) v = xU[row * NB + l];
+      else if (l < 14) v = xD[row * NB + (l - 7)];
+      else if (l < 21) v = xH[row * NB + (l - 14)];
+      else v = M == 0 ? c.cIpu[0][row * NG + (l - 21)] : 0.0;
+      sx[t] = v;
+    }
+  }
+  // in-plane source offsets of this thread's staged elements (periodic images)
+  int vo[VPER];
+#pragma unroll
+  for (int e = 0; e < VPER; ++e) {
+    const int t = tid + e * RNT;
+    const int r = t / VW, col = t % VW;
+    vo[e] = t < VE ? (wrapg(i0 - 3 + col, g.n1) + 3) + g.nx * (wrapg(j0 - 3 + r, g.n2) + 3) : -1;
+  }
+  const double* wsrc[WPER];
+  int wdst[WPER];
+#pragma unroll
+  for (int e = 0; e < WPER; ++e) {
+    const int t = tid + e * RNT;
+    const int f = t / WT::E, u = t % WT::E;
+    const int r = u / WT::W, col = u % WT::W;
+    const int gi = wrapg(i0 + col - (M == 0 ? 2 : 0), g.n1), gj = wrapg(j0 + r - (M == 1 ? 2 : 0), g.n2);
+    const double* base = f == 0 ? wk0 : (f == 1 ? wk1 : wk2);
+    wsrc[e] = t < 3 * WT::E ? base + (gi + 3) + (long long)g.nx * (gj + 3) : nullptr;
+    wdst[e] = VE + t;
+  }
+  const int nq = (k1 - k0 + 1) + 6;  // planes k0-3 .. k1+3
+  auto zoff = [&](int q) -> long long { return (long long)(wrapg(k0 - 3 + q, g.n3) + 3) * g.nxy; };
+  auto stage = [&](int q) {
+    if (q < nq) {
+      double* slot = ring + (size_t)(q % RR) * SE;
+      const long long zo = zoff(q);
+#pragma unroll
+      for (int e = 0; e < VPER; ++e)
+        if (vo[e] >= 0) cpa8(slot + tid + e * RNT, vel + zo + vo[e]);
+#pragma unroll
+      for (int e = 0; e < WPER; ++e)
+        if (wsrc[e]) cpa8(slot + wdst[e], wsrc[e] + zo);
+    }
+    cpa_commit();
+  };
+#pragma unroll
+  for (int q = 0; q < RR - 4; ++q) stage(q);
+
+  double vq[7];                                    // vel of the column, planes c-3 .. c+3
+  double wq[3][6];                                 // m = 3: work_a of the column, planes c-2 .. c+3
+#pragma unroll
+  for (int l = 0; l < 7; ++l) vq[l] = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int l = 0; l < 6; ++l) wq[a][l] = 0.0;
+
+  const double* yU = M == 1 ? c.cNuU[1] : c.cNpU[1];
+  const double* yD = M == 1 ? c.cNuD[1] : c.cNpD[1];
+  const double* yH = M == 1 ? c.cuu[1] : c.cpp[1];
+  const double* zU = M == 2 ? c.cNuU[2] : c.cNpU[2];
+  const double* zD = M == 2 ? c.cNuD[2] : c.cNpD[2];
+  const double* zH = M == 2 ? c.cuu[2] : c.cpp[2];
+  const int own = (tx + 3) + VW * (ty + 3);
+
+  for (int t = 0; t < nq; ++t) {
+    cpa_wait<RR - 5>();   // this thread's copies of plane t have landed
+    __syncthreads();      // everybody's have; the slot of plane t-4 is free again
+    stage(t + RR - 4);
+    const double* slot = ring + (size_t)(t % RR) * SE;
+#pragma unroll
+    for (int l = 0; l < 6; ++l) vq[l] = vq[l + 1];
+    vq[6] = slot[own];
+    if (M == 2) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int l = 0; l < 5; ++l) wq[a][l] = wq[a][l + 1];
+        wq[a][5] = slot[VE + a * WT::E + tid];
+      }
+    }
+    if (t < 6 || !in) continue;
+    const int k = k0 + t - 6;
+    const double* cs = ring + (size_t)((t - 3) % RR) * SE;  // plane k
+    const long long p = off(g, i, j, k);
+    const double nlo = use_old ? nl[p] : 0.0;
+    // vel_m neighbours along x and y (plane k), z (register window)
+    double xv[7], yv[7];
+#pragma unroll
+    for (int l = 0; l < 7; ++l) {
+      xv[l] = cs[(ty + 3) * VW + tx + l];
+      yv[l] = cs[(ty + l) * VW + tx + 3];
+    }
+    double acc = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      // pp = interpolate2_pre_vel(m, work_a) along axis m
+      double pp;
+      if (M == 0) {
+        const double* w = cs + VE + a * WT::E + ty * WT::W + tx;
+        pp = sx[21 * RTX + tx] * w[0];
+#pragma unroll
+        for (int l = 1; l < 6; ++l) pp = pp + sx[(21 + l) * RTX + tx] * w[l];
+      } else if (M == 1) {
+        const double* w = cs + VE + a * WT::E + ty * WT::W + tx;
+        const double* cr = c.cIpu[1] + jr * NG;
+        pp = __ldg(cr) * w[0];
+#pragma unroll
+        for (int l = 1; l < 6; ++l) pp = pp + __ldg(cr + l) * w[l * WT::W];
+      } else {
+        const double* cr = c.cIpu[2] + k * NG;
+        pp = __ldg(cr) * wq[a][0];
+#pragma unroll
+        for (int l = 1; l < 6; ++l) pp = pp + __ldg(cr + l) * wq[a][l];
+      }
+      double dd;
+      if (a == 0) {
+        const double* cr = sx + (pp >= 0.0 ? 0 : 7) * RTX + tx;
+        dd = cr[0] * xv[0];
+#pragma unroll
+        for (int l = 1; l < 7; ++l) dd = dd + cr[l * RTX] * xv[l];
+      } else if (a == 1) {
+        const double* cr = (pp >= 0.0 ? yU : yD) + jr * NB;
+        dd = __ldg(cr) * yv[0];
+#pragma unroll
+        for (int l = 1; l < 7; ++l) dd = dd + __ldg(cr + l) * yv[l];
+      } else {
+        const double* cr = (pp >= 0.0 ? zU : zD) + k * NB;
+        dd = __ldg(cr) * vq[0];
+#pragma unroll
+        for (int l = 1; l < 7; ++l) dd = dd + __ldg(cr + l) * vq[l];
+      }
+      acc = (a == 0) ? dd * pp : acc + dd * pp;
+    }
+    // Helmholtz_explicit: x, y, z second derivatives of vel_m
+    double lap = sx[14 * RTX + tx] * xv[0];
+#pragma unroll
+    for (int l = 1; l < 7; ++l) lap = lap + sx[(14 + l) * RTX + tx] * xv[l];
+    {
+      const double* cr = yH + jr * NB;
+#pragma unroll
+      for (int l = 0; l < 7; ++l) lap = lap + __ldg(cr + l) * yv[l];
+    }
+    {
+      const double* cr = zH + k * NB;
+#pragma unroll
+      for (int l = 0; l < 7; ++l) lap = lap + __ldg(cr + l) * vq[l];
+    }
+    const double nln = acc - multL * lap;
+    double r = vq[3];
+    if (use_old) r = r - mult_b * nlo;
+    r = r - mult_a * nln;
+    nl[p] = nln;
+    rhs[p] = r;
+  }
+  cpa_wait<0>();
+}
+
+template <int M>
+void launch_m(const Geom& g, const Coeffs<double>& c, double multL, double mult_b, double mult_a, int use_old,
+              const double* vel, const double* const work[3], double* nl, double* rhs, cudaStream_t s) {
+  static unsigned long long attr_set = 0;  // devices on which the shared-memory limit was raised
+  constexpr size_t bytes = rhs_smem_bytes<M>();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !(attr_set >> dev & 1ULL)) {
+    cudaFuncSetAttribute(k_rhs_march<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    attr_set |= 1ULL << dev;
+  }
+  const int kz = rhs_march_kz(g);
+  const dim3 grid((g.n1 + RTX - 1) / RTX, (g.n2 + RTY - 1) / RTY, (g.n3 + kz - 1) / kz);
+  k_rhs_march<M><<<grid, dim3(RTX, RTY), bytes, s>>>(g, c, multL, mult_b, mult_a, use_old, kz, vel, work[0], work[1],
+                                                     work[2], nl, rhs);
+}
+
+}  // namespace
+
+// planes per block: enough blocks for several waves of two blocks per SM, at most 64 planes
+int rhs_march_kz(const Geom& g) {
+  const long long cols = (long long)((g.n1 + RTX - 1) / RTX) * ((g.n2 + RTY - 1) / RTY);
+  long long kz = (cols * g.n3) / (148LL * 2 * 8);
+  kz = kz < 8 ? 8 : (kz > 64 ? 64 : kz);
+  return (int)kz;
+}
+
+void launch_rhs_march(int m, const Geom& g, const Coeffs<double>& c, double multL, double mult_b, double mult_a,
+                      int use_old, const double* vel, const double* const work[3], double* nl, double* rhs,
+                      cudaStream_t s) {
+  if (m == 0)
+    launch_m<0>(g, c, multL, mult_b, mult_a, use_old, vel, work, nl, rhs, s);
+  else if (m == 1)
+    launch_m<1>(g, c, multL, mult_b, mult_a, use_old, vel, work, nl, rhs, s);
+  else
+    launch_m<2>(g, c, multL, mult_b, mult_a, use_old, vel, work, nl, rhs, s);
+}
+
+}  // namespace impact

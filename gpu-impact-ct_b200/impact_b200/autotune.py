@@ -32,8 +32,9 @@ def tune(case: Case, base: SolverParams, tile_kc=TILE_KC, sweeps=SWEEPS, rhs="re
          repeats: int = 1, use_cache: bool = True):
     """Time Poisson solves A x = rhs (x from zero, written into `scratch`, which the next time step
     recomputes anyway) for every candidate and return (best SolverParams, report).  The case should
-    hold a realistic right-hand side, e.g. after one time step.  Multigrid candidates only when
-    base.precond == 1; otherwise only the tile depth is tuned."""
+    hold a realistic right-hand side, e.g. after two time steps from rest (the first step of a
+    flow at rest has a zero right-hand side; with one, nothing is tuned and `base` is returned).
+    Multigrid candidates only when base.precond == 1; otherwise only the tile depth is tuned."""
     key = (tuple(case.grid.N), case.precision, base.precond, base.tol_rel, base.omega)
     if use_cache and key in _cache:
         return _cache[key]
@@ -44,7 +45,11 @@ def tune(case: Case, base: SolverParams, tile_kc=TILE_KC, sweeps=SWEEPS, rhs="re
     for kc, sw in cands:
         p = _with(base, kc, sw)
         p.init_yes = 1
-        case.poisson(rhs, scratch, p)  # builds the engine and its graphs
+        r0 = case.poisson(rhs, scratch, p)  # builds the engine and its graphs
+        if r0.b_two == 0.0:
+            # a zero right-hand side (e.g. a flow still at rest) solves in no iterations: timing
+            # it says nothing about the candidates, so the base parameters stay
+            return copy.copy(base), [{"skipped": "zero right-hand side"}]
         t0 = time.perf_counter()
         for _ in range(repeats):
             r = case.poisson(rhs, scratch, p)  # returns after the device has finished

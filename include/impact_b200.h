@@ -272,8 +272,11 @@ void impact_b200_profile_reset(void);
 int impact_b200_profile_read(int kid, long long* launches, double* total_ms, double* total_bytes, const char** name);
 long long impact_b200_launch_count(void);
 /* launch one hot kernel iters times on the case's resident fields (kid 0 Jacobi sweep, 1 fused
- * init + sweep, 2 A x with a fused inner product, 3 A x, 4 one-thread-per-point Jacobi sweep), in
- * the case's precision; *ms_per_launch = average device time (CUDA events on the case stream) */
+ * init + sweep, 2 A x with a fused inner product, 3 A x, 4 one-thread-per-point Jacobi sweep, in
+ * the case's precision; FP64 passes of the time step: 10..12 rhs_vel of component 1..3 (reads
+ * vel_m, work1..3, nl_m; writes nl_m, rhs_m; 1/Re = 2e-3, dt bRK = -0.01, dt aRK = 0.02), 13 interpolate_vel (vel -> work), 14 projection
+ * (vel = rhs - G pre), 15 divergence2 of rhs into res); *ms_per_launch = average device time
+ * (CUDA events on the case stream) */
 int impact_b200_case_kernel_bench(impact_b200_case* c, int kid, int iters, double* ms_per_launch);
 /* Measurement: iters launches of one kernel of the Poisson engine on the case's finest level, in
  * the solve precision (FP64, or FP32 for the inner solve of a mixed case), the engine built with
