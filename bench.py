@@ -624,7 +624,8 @@ def main():
 KERNELS = [("rhs_vel_1", 0, "step", 10, 56), ("rhs_vel_2", 0, "step", 11, 56), ("rhs_vel_3", 0, "step", 12, 56),
            ("interpolate_vel", 0, "step", 13, 48), ("project", 0, "step", 14, 56), ("divergence2", 0, "step", 15, 32)]
 ENGINE = [("mg_sweep", 0), ("mg_init", 1), ("mg_residual", 2), ("mg_prolong", 3), ("mg_restrict", 4), ("ax_dot", 5),
-          ("ax_dot2", 6), ("x_update", 7), ("p_update", 8), ("r_update", 9), ("vcycle", 10), ("bicgstab_iteration", 11)]
+          ("ax_dot2", 6), ("x_update", 7), ("p_update", 8), ("r_update", 9), ("vcycle", 10), ("bicgstab_iteration", 11),
+          ("mg_pre_smooth", 12), ("mg_post_smooth", 13)]
 for _nm, _k in ENGINE:
     KERNELS += [(_nm + "_f64", 0, "engine", _k, None), (_nm + "_f32", 1, "engine", _k, None)]
 
@@ -651,7 +652,7 @@ def kernels_main(args, device):
             case.upload(f, rng.uniform(-1.0, 1.0, grid.shape))
         if any(k[2] == "step" for k in todo):
             case.kernel_bench(13, 1)  # interpolated velocities for the rhs_vel passes
-        sp = I.solver_params(precond=1, omega=0.8, tile_kc=32)
+        sp = I.solver_params(precond=1, omega=0.8, tile_kc=32, mg_down=3, mg_up=3, mg_bottom=3)
         for name, _, entry, kid, bpc in todo:
             if entry == "step":
                 ms = case.kernel_bench(kid, args.iters)

@@ -660,6 +660,50 @@ __global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict
 // ------------------------------------------------------------------------------------------
 // multigrid kernels over level job lists
 // ------------------------------------------------------------------------------------------
+// The point operations of the damped-Jacobi sweep, the init sweep and the residual of the
+// compact operator, with every rounding spelled out (fused multiply-adds and products by
+// intrinsic, so the compiler contracts nothing on its own), so that the one-sweep kernels and
+// the fused smoothing kernels produce the same bits.
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float mulT(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mulT(double a, double b) { return __dmul_rn(a, b); }
+// bv - a0 w - a2 e - b0 s - b2 n - cm zm - cp zp
+template <typename T>
+__device__ __forceinline__ T jres(T bv, T a0, T w, T a2, T e, T b0, T s, T b2, T n, T cm, T zm, T cp, T zp) {
+  T r = fmaT(-a0, w, bv);
+  r = fmaT(-a2, e, r);
+  r = fmaT(-b0, s, r);
+  r = fmaT(-b2, n, r);
+  r = fmaT(-cm, zm, r);
+  return fmaT(-cp, zp, r);
+}
+// damped-Jacobi update of centre value zc from r: omega r / diag + (1 - omega) zc; on uniform z
+// r (omega / diag) with inv = omega / diag formed once per column
+template <typename T>
+__device__ __forceinline__ T jsweep(T r, T zc, T omega, bool zu, T inv, T diag) {
+  const T q = zu ? mulT(r, inv) : mulT(omega, r) / diag;
+  return fmaT(T(1) - omega, zc, q);
+}
+// init sweep omega v / diag (uniform z: v inv)
+template <typename T>
+__device__ __forceinline__ T jinit(T v, T omega, bool zu, T inv, T diag) {
+  return zu ? mulT(v, inv) : mulT(omega, v) / diag;
+}
+// residual bv - (a0 w + a2 e + b0 s + b2 n + cm zm + cp zp + diag zc)
+template <typename T>
+__device__ __forceinline__ T jresid(T bv, T a0, T w, T a2, T e, T b0, T s, T b2, T n, T cm, T zm, T cp, T zp, T diag,
+                                    T zc) {
+  T l = mulT(a0, w);
+  l = fmaT(a2, e, l);
+  l = fmaT(b0, s, l);
+  l = fmaT(b2, n, l);
+  l = fmaT(cm, zm, l);
+  l = fmaT(cp, zp, l);
+  l = fmaT(diag, zc, l);
+  return bv - l;
+}
+
 // One column (i, j), planes k0..k1, of the compact 7-point operator cdg.  The column is walked
 // in blocks of U planes: all loads of a block (the next planes' centres, the right-hand side
 // and the four lateral neighbours) are issued before its stores, so that every thread keeps
@@ -691,11 +735,10 @@ __device__ __forceinline__ void march7(const Geom& g, int i, int j, int k0, int 
     const T cc = ZU ? zcc : cz[3 * (k - 1) + 1];
     const T cp = ZU ? zcp : cz[3 * (k - 1) + 2];
     if (OP == 0) {
-      const T r = bv - a0 * w - a2 * e - b0 * s - b2 * n - cm * zm - cp * zp;
-      out[q] = (ZU ? r * inv : omega * r / (a1 + b1 + cc)) + (T(1) - omega) * zc;
+      const T r = jres(bv, a0, w, a2, e, b0, s, b2, n, cm, zm, cp, zp);
+      out[q] = jsweep(r, zc, omega, ZU, inv, ZU ? dg : a1 + b1 + cc);
     } else {
-      const T lap = a0 * w + a2 * e + b0 * s + b2 * n + cm * zm + cp * zp + (ZU ? dg : a1 + b1 + cc) * zc;
-      out[q] = bv - lap;
+      out[q] = jresid(bv, a0, w, a2, e, b0, s, b2, n, cm, zm, cp, zp, ZU ? dg : a1 + b1 + cc, zc);
     }
   };
   int k = k0;
@@ -807,12 +850,11 @@ __device__ __forceinline__ void march7v(const Geom& g, int i, int j, int k0, int
           const T w = v == 0 ? (lw ? ws[u] : wsh) : zc[v - 1];
           const T e = v == V - 1 ? (le ? es[u] : esh) : zc[v + 1];
           if (OP == 0) {
-            const T r = bv[u][v] - a0[v] * w - a2[v] * e - b0 * sv[u][v] - b2 * nv[u][v] - cm * zm[v] - cp * xn[u][v];
-            ov[v] = (ZU ? r * inv[v] : omega * r / (a1[v] + b1 + cc)) + (T(1) - omega) * zc[v];
+            const T r = jres(bv[u][v], a0[v], w, a2[v], e, b0, sv[u][v], b2, nv[u][v], cm, zm[v], cp, xn[u][v]);
+            ov[v] = jsweep(r, zc[v], omega, ZU, inv[v], a1[v] + b1 + cc);
           } else {
-            const T lap = a0[v] * w + a2[v] * e + b0 * sv[u][v] + b2 * nv[u][v] + cm * zm[v] + cp * xn[u][v] +
-                          (a1[v] + b1 + cc) * zc[v];
-            ov[v] = bv[u][v] - lap;
+            ov[v] = jresid(bv[u][v], a0[v], w, a2[v], e, b0, sv[u][v], b2, nv[u][v], cm, zm[v], cp, xn[u][v],
+                           a1[v] + b1 + cc, zc[v]);
           }
         }
         if (act) vstore(out + p + u * nxy, ov);
@@ -915,7 +957,7 @@ __global__ void __launch_bounds__(ENT) k_lv_smooth(const LevelJob<T>* __restrict
         for (int u = 0; u < 4; ++u) {
 #pragma unroll
           for (int c = 0; c < V; ++c)
-            v[u][c] = zu ? v[u][c] * inv[c] : omega * v[u][c] / (a1[c] + b1 + c3[3 * (k + u - 1) + 1]);
+            v[u][c] = jinit(v[u][c], omega, zu, inv[c], a1[c] + b1 + c3[3 * (k + u - 1) + 1]);
           vstore(dst + p + u * nxy, v[u]);
         }
       }
@@ -923,7 +965,7 @@ __global__ void __launch_bounds__(ENT) k_lv_smooth(const LevelJob<T>* __restrict
         T v[V];
         vload(bb + p, v);
 #pragma unroll
-        for (int c = 0; c < V; ++c) v[c] = zu ? v[c] * inv[c] : omega * v[c] / (a1[c] + b1 + c3[3 * (k - 1) + 1]);
+        for (int c = 0; c < V; ++c) v[c] = jinit(v[c], omega, zu, inv[c], a1[c] + b1 + c3[3 * (k - 1) + 1]);
         vstore(dst + p, v);
       }
       continue;
@@ -937,9 +979,9 @@ __global__ void __launch_bounds__(ENT) k_lv_smooth(const LevelJob<T>* __restrict
       for (int u = 0; u < 2 * U; ++u) v[u] = bb[p + u * nxy];
 #pragma unroll
       for (int u = 0; u < 2 * U; ++u)
-        dst[p + u * nxy] = zu ? v[u] * inv : omega * v[u] / (a1 + b1 + c3[3 * (k + u - 1) + 1]);
+        dst[p + u * nxy] = jinit(v[u], omega, zu, inv, a1 + b1 + c3[3 * (k + u - 1) + 1]);
     }
-    for (; k <= k1; ++k, p += nxy) dst[p] = zu ? bb[p] * inv : omega * bb[p] / (a1 + b1 + c3[3 * (k - 1) + 1]);
+    for (; k <= k1; ++k, p += nxy) dst[p] = jinit(bb[p], omega, zu, inv, a1 + b1 + c3[3 * (k - 1) + 1]);
   }
 }
 
@@ -1044,11 +1086,12 @@ __device__ __forceinline__ void bracket(int q, int r, int nc, int& lo, int& hi, 
 // corner values of the two most recent coarse planes in registers, so consecutive fine planes
 // reuse them; with V > 1 the fine values move as 16-byte vectors.
 template <typename T, int V>
-__device__ __forceinline__ void prolong_cols(const LevelJob<T>& J, const Geom& g, int i, int j, int k0, int k1) {
+__device__ __forceinline__ void prolong_cols(const LevelJob<T>& J, const Geom& g, int i, int j, int k0, int k1,
+                                             T* __restrict__ dst) {
   const Geom gc = J.gc;
   const T* __restrict__ coarse = J.Bc;
   const T* __restrict__ cI3 = J.cI[2];
-  T* __restrict__ fine = J.B;
+  const T* __restrict__ fine = J.B;
   int yl, yh;
   bool my;
   bracket(j, J.rc[1], gc.n2, yl, yh, my);
@@ -1117,9 +1160,9 @@ __device__ __forceinline__ void prolong_cols(const LevelJob<T>& J, const Geom& g
       f[v] = f[v] + (mx[v] ? wx0[v] * Yl + wx1[v] * Yh : Yl);
     }
     if constexpr (V > 1)
-      vstore(fine + p, f);
+      vstore(dst + p, f);
     else
-      fine[p] = f[0];
+      dst[p] = f[0];
   }
 }
 
@@ -1127,11 +1170,12 @@ __device__ __forceinline__ void prolong_cols(const LevelJob<T>& J, const Geom& g
 // V/2 + 1 coarse columns, so each coarse plane costs (V/2 + 1) x 2 loads instead of 4 V; every
 // fine point sees the same operations in the same order as in prolong_cols.
 template <typename T, int V>
-__device__ __forceinline__ void prolong_cols_x2(const LevelJob<T>& J, const Geom& g, int i, int j, int k0, int k1) {
+__device__ __forceinline__ void prolong_cols_x2(const LevelJob<T>& J, const Geom& g, int i, int j, int k0, int k1,
+                                                T* __restrict__ dst) {
   constexpr int NC = V / 2 + 1;
   const Geom gc = J.gc;
   const T* __restrict__ cI3 = J.cI[2];
-  T* __restrict__ fine = J.B;
+  const T* __restrict__ fine = J.B;
   int yl, yh;
   bool my;
   bracket(j, J.rc[1], gc.n2, yl, yh, my);
@@ -1198,14 +1242,15 @@ __device__ __forceinline__ void prolong_cols_x2(const LevelJob<T>& J, const Geom
 #pragma unroll
     for (int v = 0; v < V; ++v)  // even v: coincident with coarse column v/2; odd v: between two
       f[v] = f[v] + ((v & 1) ? wx0[v] * Y[(v - 1) / 2] + wx1[v] * Y[(v + 1) / 2] : Y[v / 2]);
-    vstore(fine + p, f);
+    vstore(dst + p, f);
   }
 }
 
-// this (fine) level: B += P Bc (interpolate, mod_solvers.f90:955-1141)
+// this (fine) level: B += P Bc (interpolate, mod_solvers.f90:955-1141); with flip, C = B + P Bc
+// (B unchanged) for the fused smoothing that follows
 template <typename T>
 __global__ void __launch_bounds__(ENT, 2) k_lv_prolong(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
-                                                    int nj, int ntiles) {
+                                                    int nj, int ntiles, int flip) {
   for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
     const int q = find_job(ts, nj, b);
     const LevelJob<T>& J = jobs[q];
@@ -1214,11 +1259,230 @@ __global__ void __launch_bounds__(ENT, 2) k_lv_prolong(const LevelJob<T>* __rest
     int i, j, k0, k1;
     tile_at(g, J.kc, b - ts[q], i, j, k0, k1, J.vw);
     if (i > g.n1 || j > g.n2) continue;
+    T* dst = flip ? J.C : J.B;
     if (J.vw > 1 && J.rc[0] == 2) {
-      prolong_cols_x2<T, VecT<T>::W>(J, g, i, j, k0, k1);
+      prolong_cols_x2<T, VecT<T>::W>(J, g, i, j, k0, k1, dst);
     } else {
-      for (int v = 0; v < J.vw; ++v) prolong_cols<T, 1>(J, g, i + v, j, k0, k1);
+      for (int v = 0; v < J.vw; ++v) prolong_cols<T, 1>(J, g, i + v, j, k0, k1, dst);
     }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// fused V-cycle smoothing: the sweeps of one smoothing phase (and the residual after them) in
+// one z-march
+// ------------------------------------------------------------------------------------------
+// Stage 0 is the start iterate x0 (INIT: the init sweep omega A / diag, computed from A; else
+// read from C), stages 1..NSW are damped-Jacobi sweeps and, with RES, stage NSW + 1 is the
+// residual A - cdg(x_NSW).  A block covers an input region of W0 x H0 = 16 V x 32 columns
+// (V = 16 bytes / element size): each half-warp is one row, thread (l, ty) owning the V
+// consecutive columns x = V (l mod 16) .. + V-1 of row y = 2 ty + l / 16 for the whole march
+// (MNT = 512 threads: 32 rows).
+// With S stencil stages the outputs are the X x Y = (W0 - 2S) x (H0 - 2S) interior columns
+// (stage s is valid on the region shrunk by s on every side).  At each step the block takes one
+// new plane of A (and of C) -- staged by cp.async MPF planes ahead, each thread its own columns
+// -- and advances every stage by one plane, stage s lagging s planes behind the newest: stage s
+// at plane k needs stage s-1 at k-1..k+1 of its own columns (register windows), at k of the x
+// neighbours (its own registers, or the next lane's by a shuffle) and of the y neighbours
+// (16-byte rows published in shared memory one step earlier), so one barrier per step suffices.
+// Every point is evaluated with the operations of the one-sweep kernels (jres / jsweep / jinit
+// / jresid), so the fused phase gives the same iterate bit for bit.
+// Outputs: PRE (INIT, RES): B = x_NSW and C = residual; POST: B = x_NSW.
+constexpr int MPF = 2;  // planes staged ahead of the newest one in use
+const dim3 kMBlock(32, MNT / 32);
+
+template <typename T, int S, bool INIT>
+struct MLayout {
+  static constexpr int V = VecT<T>::W;
+  static constexpr int W0 = 16 * V, H0 = 2 * MNT / 32, R0 = W0 * H0;
+  static constexpr int NBR = S + 1 + MPF;  // A ring: planes t-S .. t+MPF
+  static constexpr int NCR = MPF + 1;      // C ring (POST): planes t .. t+MPF
+  static constexpr int pub() { return 0; }                   // 2 slots x S stages x R0
+  static constexpr int rhs() { return 2 * S * R0; }         // NBR x R0
+  static constexpr int cin() { return rhs() + NBR * R0; }   // NCR x R0 (POST only)
+  static constexpr int total() { return cin() + (INIT ? 0 : NCR * R0); }
+};
+template <typename T, int NSW, bool INIT, bool RES>
+constexpr size_t multi_smem_bytes() {
+  return sizeof(T) * (size_t)MLayout<T, NSW + (RES ? 1 : 0), INIT>::total();
+}
+
+// periodic image of index i in 1..n, for any integer i
+__device__ __forceinline__ int wrapn(int i, int n) {
+  int r = (i - 1) % n;
+  if (r < 0) r += n;
+  return r + 1;
+}
+// 16-byte shared-memory vectors
+template <typename T>
+__device__ __forceinline__ void sload(const T* p, T (&o)[VecT<T>::W]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+    o[3] = v.w;
+  } else {
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    o[0] = v.x;
+    o[1] = v.y;
+  }
+}
+
+template <typename T, int NSW, bool INIT, bool RES>
+__global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+                                                     int nj, int ntiles, T omega) {
+  constexpr int S = NSW + (RES ? 1 : 0);
+  using LY = MLayout<T, S, INIT>;
+  constexpr int V = LY::V;
+  constexpr int W0 = LY::W0, H0 = LY::H0, R0 = LY::R0, NBR = LY::NBR, NCR = LY::NCR;
+  constexpr int X = W0 - 2 * S, Y = H0 - 2 * S;
+  extern __shared__ __align__(16) unsigned char lm_raw[];
+  T* const sm = reinterpret_cast<T*>(lm_raw);
+  T* const pub = sm + LY::pub();  // pub[(slot * S + s) * R0 + y * W0 + x]
+  T* const br = sm + LY::rhs();
+  T* const cr = sm + LY::cin();
+  const int x0 = V * (threadIdx.x & 15);               // this thread's first column in the region
+  const int y = 2 * threadIdx.y + (threadIdx.x >> 4);  // and its row
+  const int e0 = y * W0 + x0;
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const LevelJob<T>& J = jobs[q];
+    if (e_halted(J.sc)) continue;
+    const Geom g = J.g;
+    const int kc = J.kc;
+    const int ntx = (g.n1 + X - 1) / X, nty = (g.n2 + Y - 1) / Y;
+    const int t0 = b - ts[q];
+    const int ta = t0 % ntx, tr = t0 / ntx, tc = tr / nty;
+    const int i0 = ta * X + 1, j0 = (tr - tc * nty) * Y + 1;  // first output column of the tile
+    const int k0 = tc * kc + 1, k1 = min(g.n3, k0 + kc - 1);
+    const int nq = (k1 - k0 + 1) + 2 * S;  // planes k0-S .. k1+S
+    const T* __restrict__ cz = J.cdg[2];
+    const bool zu = J.zuni != 0;
+    T a0[V], a1[V], a2[V], inv[V];
+    int xo[V];
+#pragma unroll
+    for (int c = 0; c < V; ++c) {
+      const int gi = wrapn(i0 - S + x0 + c, g.n1);
+      a0[c] = J.cdg[0][3 * (gi - 1)];
+      a1[c] = J.cdg[0][3 * (gi - 1) + 1];
+      a2[c] = J.cdg[0][3 * (gi - 1) + 2];
+      xo[c] = gi + 3;
+    }
+    const int gj = wrapn(j0 - S + y, g.n2);
+    const T b0 = J.cdg[1][3 * (gj - 1)], b1 = J.cdg[1][3 * (gj - 1) + 1], b2 = J.cdg[1][3 * (gj - 1) + 2];
+    const int yo = g.nx * (gj + 3);
+    const T zcm = cz[0], zcc = cz[1], zcp = cz[2];  // the z row of a uniform z axis
+#pragma unroll
+    for (int c = 0; c < V; ++c) inv[c] = zu ? omega / (a1[c] + b1 + zcc) : T(0);
+    // outputs of this thread: columns i = i0 + x0 - S + c of row j = j0 + y - S
+    const int io = i0 + x0 - S, jo = j0 + y - S;
+    const bool rowout = y >= S && y < H0 - S && jo <= g.n2;
+    const long long obase = (long long)(io + 3) + (long long)g.nx * (jo + 3);
+    const T* __restrict__ A = J.A;
+    const T* __restrict__ Cin = J.C;
+    auto stage_in = [&](int qq) {  // plane qq of A (and of C) at this thread's columns
+      if (qq < nq) {
+        const long long zo = (long long)(wrapn(k0 - S + qq, g.n3) + 3) * g.nxy + yo;
+        T* bd = br + (qq % NBR) * R0 + e0;
+        T* cd = cr + (qq % NCR) * R0 + e0;
+#pragma unroll
+        for (int c = 0; c < V; ++c) {
+          cp_async1(bd + c, A + zo + xo[c]);
+          if (!INIT) cp_async1(cd + c, Cin + zo + xo[c]);
+        }
+      }
+      cp_commit();
+    };
+#pragma unroll
+    for (int qq = 0; qq < MPF; ++qq) stage_in(qq);
+    // register windows: stage s at plane p of column x0 + c lives in Qz[s][c][p % 3]
+    T Qz[S][V][3];
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+#pragma unroll
+      for (int c = 0; c < V; ++c) Qz[s][c][0] = Qz[s][c][1] = Qz[s][c][2] = T(0);
+    // one step; R = t % 3 at compile time, so that every window slot is a fixed register
+    auto step = [&](int t, auto rt) {
+      constexpr int R = decltype(rt)::value;
+      cp_wait<MPF - 1>();  // this thread's copies of plane t have landed (only it reads them)
+      __syncthreads();     // the rows published at step t-1 are visible; slot t%2 is free again
+      stage_in(t + MPF);
+      const int wslot = t & 1, rslot = wslot ^ 1;
+      {  // stage 0 at plane t
+        const T cc = zu ? zcc : cz[3 * (wrapn(k0 - S + t, g.n3) - 1) + 1];
+        T v[V];
+        sload(INIT ? br + (t % NBR) * R0 + e0 : cr + (t % NCR) * R0 + e0, v);
+#pragma unroll
+        for (int c = 0; c < V; ++c) {
+          if (INIT) v[c] = jinit(v[c], omega, zu, inv[c], a1[c] + b1 + cc);
+          Qz[0][c][R] = v[c];
+        }
+        vstore(pub + (wslot * S + 0) * R0 + e0, v);
+      }
+#pragma unroll
+      for (int s = 1; s <= S; ++s) {
+        const int qs = t - s;  // plane of stage s at this step (block-uniform)
+        // window slots of stage s-1 at planes qs-1, qs, qs+1 and of stage s at qs
+        const int sm1 = ((R - s - 1) % 3 + 3) % 3, s0 = ((R - s) % 3 + 3) % 3, sp1 = ((R - s + 1) % 3 + 3) % 3;
+        if (qs >= s) {
+          const bool rowin = y >= s && y < H0 - s;  // the row lies inside stage s's region
+          const T* pr = pub + (rslot * S + (s - 1)) * R0;  // stage s-1 at plane qs (published at t-1)
+          const int kk = k0 - S + qs;  // unwrapped; the outputs (s == S) lie in k0..k1
+          const int k3 = zu ? 0 : 3 * (wrapn(kk, g.n3) - 1);
+          const T cm = zu ? zcm : cz[k3];
+          const T cc = zu ? zcc : cz[k3 + 1];
+          const T cp = zu ? zcp : cz[k3 + 2];
+          // x neighbours across vectors: every lane takes part in the shuffles
+          const T wl = __shfl_up_sync(0xffffffffu, Qz[s - 1][V - 1][s0], 1, 16);  // column x0 - 1
+          const T er = __shfl_down_sync(0xffffffffu, Qz[s - 1][0][s0], 1, 16);    // column x0 + V
+          T ov[V];
+#pragma unroll
+          for (int c = 0; c < V; ++c) ov[c] = T(0);
+          if (rowin) {
+            T so[V], no[V], bv[V];
+            sload(pr + e0 - W0, so);
+            sload(pr + e0 + W0, no);
+            sload(br + (qs % NBR) * R0 + e0, bv);
+            const long long ob = obase + (long long)g.nxy * (kk + 3);
+#pragma unroll
+            for (int c = 0; c < V; ++c) {
+              const T zm = Qz[s - 1][c][sm1], zc = Qz[s - 1][c][s0], zp = Qz[s - 1][c][sp1];
+              const T w = c == 0 ? wl : Qz[s - 1][c - 1][s0];
+              const T ea = c == V - 1 ? er : Qz[s - 1][c + 1][s0];
+              const bool out = s == S && rowout && x0 + c >= S && x0 + c < W0 - S && io + c <= g.n1;
+              if (RES && s == S) {
+                const T res = jresid(bv[c], a0[c], w, a2[c], ea, b0, so[c], b2, no[c], cm, zm, cp, zp,
+                                     a1[c] + b1 + cc, zc);
+                if (out) {
+                  J.C[ob + c] = res;
+                  J.B[ob + c] = zc;
+                }
+              } else {
+                const T rr = jres(bv[c], a0[c], w, a2[c], ea, b0, so[c], b2, no[c], cm, zm, cp, zp);
+                ov[c] = jsweep(rr, zc, omega, zu, inv[c], a1[c] + b1 + cc);
+                if (s == S && out) J.B[ob + c] = ov[c];
+              }
+            }
+          }
+          if (s < S) {
+#pragma unroll
+            for (int c = 0; c < V; ++c) Qz[s][c][s0] = ov[c];
+            vstore(pub + (wslot * S + s) * R0 + e0, ov);
+          }
+        }
+      }
+    };
+    int t = 0;
+    for (; t + 2 < nq; t += 3) {
+      step(t, std::integral_constant<int, 0>{});
+      step(t + 1, std::integral_constant<int, 1>{});
+      step(t + 2, std::integral_constant<int, 2>{});
+    }
+    if (t < nq) step(t, std::integral_constant<int, 0>{});
+    if (t + 1 < nq) step(t + 1, std::integral_constant<int, 1>{});
+    cp_wait<0>();
+    __syncthreads();  // the rings are rewritten by the next tile
   }
 }
 
@@ -1260,6 +1524,17 @@ void ax_attributes() {
   cudaFuncSetAttribute(k_kr_ax<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
   cudaFuncSetAttribute(k_kr_ax<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
   cudaFuncSetAttribute(k_kr_ax<double, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
+#define IMPACT_MULTI_ATTR(T, N, I, R) \
+  cudaFuncSetAttribute(k_lv_multi<T, N, I, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)multi_smem_bytes<T, N, I, R>())
+  IMPACT_MULTI_ATTR(float, 1, true, true);
+  IMPACT_MULTI_ATTR(float, 2, true, true);
+  IMPACT_MULTI_ATTR(float, 2, false, false);
+  IMPACT_MULTI_ATTR(float, 3, false, false);
+  IMPACT_MULTI_ATTR(double, 1, true, true);
+  IMPACT_MULTI_ATTR(double, 2, true, true);
+  IMPACT_MULTI_ATTR(double, 2, false, false);
+  IMPACT_MULTI_ATTR(double, 3, false, false);
+#undef IMPACT_MULTI_ATTR
   done[dev] = true;
 }
 
@@ -1275,6 +1550,8 @@ inline int grid_for(int ntiles) {
   return ntiles < cap ? ntiles : cap;
 }
 const dim3 kBlock(ETX, ETY);
+// the fused smoothing kernel runs one block per tile (one block per SM at a time)
+inline int grid_multi(int ntiles) { return ntiles; }
 
 }  // namespace
 
@@ -1365,6 +1642,7 @@ void Engine<T>::release() {
   scal_host_ = nullptr;
   vc_[0].clear();
   vc_[1].clear();
+  pre0_ = post0_ = -1;
   cells_.clear();
   cells_f_.clear();
   cells_c_.clear();
@@ -1508,8 +1786,10 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
     note(kr_list_, c, 0.0, 0.0);
   }
   // vec: allow several columns per thread (lists walked by the smoothing and residual kernels);
-  // the restriction lists keep one column per thread
-  auto add_list = [&](const std::vector<std::pair<int, int>>& members, int variant, bool vec = true) {
+  // the restriction lists keep one column per thread.  fusedS > 0: a list of the fused smoothing
+  // kernel with S stencil stages (its own tile shape; tile depth per job, deep enough to stream,
+  // shallow enough to give every SM a few tiles)
+  auto add_list = [&](const std::vector<std::pair<int, int>>& members, int variant, bool vec = true, int fusedS = 0) {
     std::vector<LevelJob<T>> jobs;
     std::vector<int> tiles;
     double c = 0.0, f = 0.0, cc = 0.0;
@@ -1517,8 +1797,14 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
     for (auto& m : members) {
       jobs.push_back(lvjob(m.first, m.second, variant));
       if (!vec) jobs.back().vw = 1;
+      if (fusedS > 0) {
+        LevelJob<T>& Jm = jobs.back();
+        int kcm = KC_MAX;
+        while (kcm > 8 && tiles_multi(Jm.g, kcm, (int)sizeof(T), fusedS) < 2 * 148) kcm /= 2;
+        Jm.kc = kcm;
+      }
       const LevelJob<T>& J = jobs.back();
-      tiles.push_back(tiles_of(J.g, kc, J.vw));
+      tiles.push_back(fusedS > 0 ? tiles_multi(J.g, J.kc, (int)sizeof(T), fusedS) : tiles_of(J.g, kc, J.vw));
       c += vol(J.g);
       if (J.Cf) f += vol(J.gf);
       if (J.Bc) cc += vol(J.gc);
@@ -1535,13 +1821,18 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
     gmax = std::max(gmax, nlev[c]);
   }
   if (use_mg) {
+    // fused smoothing phases for the sweep counts that have kernels
+    const int spre = (p_.fuse && p_.mg_down >= 2 && p_.mg_down <= 3) ? p_.mg_down : 0;
+    const int spost = (p_.fuse && p_.mg_up >= 2 && p_.mg_up <= 3) ? p_.mg_up : 0;
     // level >= 1 lists are shared by both schedules
-    std::vector<int> down(gmax, -1), rs(gmax, -1);
+    std::vector<int> down(gmax, -1), rs(gmax, -1), dpre(gmax, -1), dpost(gmax, -1);
     for (int g = 1; g + 1 < gmax; ++g) {
       std::vector<std::pair<int, int>> m;
       for (int c = 0; c < n; ++c)
         if (nlev[c] >= g + 2) m.push_back({c, g});
       down[g] = add_list(m, 0);
+      if (spre) dpre[g] = add_list(m, 0, true, spre);
+      if (spost) dpost[g] = add_list(m, 0, true, spost);
     }
     for (int g = 1; g < gmax; ++g) {
       std::vector<std::pair<int, int>> m;
@@ -1557,23 +1848,36 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
       }
       const int down0 = add_list(m0, v);
       const int botl = add_list(bot, v);
+      if (spre) dpre[0] = add_list(m0, v, true, spre);
+      if (spost) dpost[0] = add_list(m0, v, true, spost);
       if (v == 0) {
         down0_ = down0;
         rs1_ = gmax > 1 ? rs[1] : -1;
+        pre0_ = dpre[0];
+        post0_ = dpost[0];
       }
       std::vector<Phase>& sch = vc_[v];
       for (int g = 0; g + 1 < gmax; ++g) {  // relax_restrict
         const int D = g == 0 ? down0 : down[g];
-        smooth(sch, D, 1, p_.mg_down);
-        sch.push_back({PH_RESID, D, 0});
+        if (spre) {
+          sch.push_back({PH_PRE, dpre[g], 0});
+        } else {
+          smooth(sch, D, 1, p_.mg_down);
+          sch.push_back({PH_RESID, D, 0});
+        }
         sch.push_back({PH_RESTRICT, rs[g + 1], 0});
       }
       smooth(sch, botl, 1, p_.mg_bottom);  // relax_bottom
       smooth(sch, botl, 0, p_.mg_bottom);
       for (int g = gmax - 2; g >= 0; --g) {  // interpolate_relax
         const int D = g == 0 ? down0 : down[g];
-        sch.push_back({PH_PROLONG, D, 0});
-        smooth(sch, D, 0, p_.mg_up);
+        if (spost) {
+          sch.push_back({PH_PROLONG, D, 1});
+          sch.push_back({PH_POST, dpost[g], 0});
+        } else {
+          sch.push_back({PH_PROLONG, D, 0});
+          smooth(sch, D, 0, p_.mg_up);
+        }
       }
     }
   } else if (p_.n_sweeps > 0) {
@@ -1632,7 +1936,19 @@ void Engine<T>::enqueue_phase(const Phase& ph) {
       IMPACT_PROF(prof::K_MG_OTHER, sz * (c + cf), s, (k_lv_restrict<T><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles)));
       break;
     case PH_PROLONG:
-      IMPACT_PROF(prof::K_MG_OTHER, sz * (2 * c + cc), s, (k_lv_prolong<T><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles)));
+      IMPACT_PROF(prof::K_MG_OTHER, sz * (2 * c + cc), s, (k_lv_prolong<T><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles, ph.flip)));
+      break;
+    case PH_PRE:  // mg_down 2 or 3
+      if (p_.mg_down == 2)
+        IMPACT_PROF(prof::K_MG_PRE, 3 * sz * c, s, (k_lv_multi<T, 1, true, true><<<grid_multi(L.ntiles), kMBlock, multi_smem_bytes<T, 1, true, true>(), s>>>(J, L.ts, L.njobs, L.ntiles, om)));
+      else
+        IMPACT_PROF(prof::K_MG_PRE, 3 * sz * c, s, (k_lv_multi<T, 2, true, true><<<grid_multi(L.ntiles), kMBlock, multi_smem_bytes<T, 2, true, true>(), s>>>(J, L.ts, L.njobs, L.ntiles, om)));
+      break;
+    case PH_POST:  // mg_up 2 or 3
+      if (p_.mg_up == 2)
+        IMPACT_PROF(prof::K_MG_POST, 3 * sz * c, s, (k_lv_multi<T, 2, false, false><<<grid_multi(L.ntiles), kMBlock, multi_smem_bytes<T, 2, false, false>(), s>>>(J, L.ts, L.njobs, L.ntiles, om)));
+      else
+        IMPACT_PROF(prof::K_MG_POST, 3 * sz * c, s, (k_lv_multi<T, 3, false, false><<<grid_multi(L.ntiles), kMBlock, multi_smem_bytes<T, 3, false, false>(), s>>>(J, L.ts, L.njobs, L.ntiles, om)));
       break;
     default:
       break;
@@ -1863,6 +2179,15 @@ int Engine<T>::bench(int kind, int iters, double* ms, double* bytes) {
     case 10:
       f = [this]() { enqueue_precond(0); };
       break;
+    case 12:
+    case 13: {
+      const int l = kind == 12 ? pre0_ : post0_;
+      if (!need(l)) return impact_set_error_msg(-1, "engine bench: no fused smoothing list (sweep count 2..4, fusion on)");
+      const Phase ph{kind == 12 ? PH_PRE : PH_POST, l, 0};
+      by = 3 * sz * cells_[l];
+      f = [this, ph]() { enqueue_phase(ph); };
+      break;
+    }
     case 11:
       f = [this]() { enqueue_iteration(); };
       break;

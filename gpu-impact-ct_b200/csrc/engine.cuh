@@ -30,6 +30,15 @@ inline int tiles_xy(const Geom& g) { return ((g.n1 + ETX - 1) / ETX) * ((g.n2 + 
 inline int tiles_of(const Geom& g, int kc, int vw = 1) {
   return ((g.n1 + ETX * vw - 1) / (ETX * vw)) * ((g.n2 + ETY - 1) / ETY) * ((g.n3 + kc - 1) / kc);
 }
+// Tile geometry of the fused smoothing kernel k_lv_multi (MNT threads): a block's input region
+// is 16 V x (MNT / 16) columns (V = 16 bytes / element size consecutive columns per thread, one
+// row per half-warp); with S stencil stages it yields (16 V - 2S) x (MNT / 16 - 2S) output
+// columns, kc planes deep.
+constexpr int MNT = 512;
+inline int tiles_multi(const Geom& g, int kc, int sz, int S) {
+  const int X = 16 * (16 / sz) - 2 * S, Y = MNT / 16 - 2 * S;
+  return ((g.n1 + X - 1) / X) * ((g.n2 + Y - 1) / Y) * ((g.n3 + kc - 1) / kc);
+}
 
 // one multigrid level of one case
 template <typename T>
@@ -109,10 +118,11 @@ struct EngineParams {
   int check_every = 2;
   int kc = 16;       // z-planes per tile
   int use_graph = 1; // replay each chunk of iterations as a captured CUDA graph
+  int fuse = 1;      // V-cycle smoothing phases as fused multi-sweep kernels
   bool operator==(const EngineParams& o) const {
     return precond == o.precond && n_sweeps == o.n_sweeps && mg_down == o.mg_down && mg_up == o.mg_up &&
            mg_bottom == o.mg_bottom && omega == o.omega && check_every == o.check_every && kc == o.kc &&
-           use_graph == o.use_graph;
+           use_graph == o.use_graph && fuse == o.fuse;
   }
 };
 
@@ -121,7 +131,9 @@ struct Phase {
   int list;
   int flip;
 };
-enum { PH_INIT = 0, PH_SWEEP, PH_COPY, PH_RESID, PH_RESTRICT, PH_PROLONG };
+// PH_PRE: init + (mg_down - 1) sweeps + residual in one kernel; PH_POST: mg_up sweeps in one
+// kernel (after a PH_PROLONG with flip = 1, which writes its result into C); for 2 or 3 sweeps
+enum { PH_INIT = 0, PH_SWEEP, PH_COPY, PH_RESID, PH_RESTRICT, PH_PROLONG, PH_PRE, PH_POST };
 
 // device arena of job lists built on the host
 struct ListArena {
@@ -154,7 +166,8 @@ class Engine {
   // measurement: `iters` launches of one kernel kind on the finest level of every case
   // (0 sweep, 1 init, 2 residual, 3 prolongation, 4 restriction to level 2, 5 A x + dot,
   //  6 A x + 2 dots, 7 x update, 8 p update, 9 r update, 10 one V-cycle, 11 one BiCGstab
-  //  iteration); returns ms per launch and the algorithmic bytes of one launch
+  //  iteration, 12 fused pre-smoothing + residual, 13 fused post-smoothing); returns ms per
+  //  launch and the algorithmic bytes of one launch
   int bench(int kind, int iters, double* ms, double* bytes);
   int ncases() const { return (int)cs_.size(); }
   const EngineParams& params() const { return p_; }
@@ -177,6 +190,7 @@ class Engine {
   ListArena arena_;
   int kr_list_ = -1;
   int down0_ = -1, rs1_ = -1;  // finest-level list of the first schedule, restriction to level 2
+  int pre0_ = -1, post0_ = -1; // its fused pre- and post-smoothing lists (-1: not fused)
   std::vector<Phase> vc_[2];  // preconditioner schedules: z1 = M pp, z2 = M rr
   double* partial_ = nullptr;
   SolverScalars* scal_ = nullptr;

@@ -22,6 +22,8 @@ enum Kid {
   K_MG_INIT,       // multigrid init sweep
   K_MG_RESID,      // multigrid residual
   K_MG_OTHER,      // restriction, prolongation, copies
+  K_MG_PRE,        // fused init + sweeps + residual of one V-cycle level
+  K_MG_POST,       // fused sweeps after the prolongation
   K_COUNT
 };
 

@@ -644,6 +644,7 @@ static EngineParams engine_params(const CaseState& s, const impact_b200_solver_p
   ep.kc = p->tile_kc > 0 ? p->tile_kc : (kc ? std::atoi(kc) : 32);
   ep.kc = ep.kc < 1 ? 1 : (ep.kc > KC_MAX ? KC_MAX : ep.kc);
   ep.use_graph = std::getenv("IMPACT_B200_NO_GRAPH") ? 0 : 1;
+  ep.fuse = p->smooth_unfused ? 0 : 1;
   (void)s;
   return ep;
 }

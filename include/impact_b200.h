@@ -176,6 +176,10 @@ typedef struct {
   int mg_down, mg_up, mg_bottom; /* V-cycle sweeps (n_relax_down / _up / _bottom), relaxation omega */
   int tile_kc;         /* z-planes per tile of the solver kernels (0: library default); chosen by
                           the autotuner of the Python package, no counterpart in the reference */
+  int smooth_unfused;  /* 0 (default): the sweeps of each V-cycle smoothing phase (and, before a
+                          restriction, the residual after them) run as one z-marching kernel;
+                          1: one sweep per launch.  Same results bit for bit; no counterpart in
+                          the reference */
 } impact_b200_solver_params;
 
 typedef struct {
@@ -264,8 +268,9 @@ int impact_b200_product_scalar_noalloc(int N1, int N2, int N3, const double* a_d
 /* ---- measurement hooks -----------------------------------------------------------------
  * When enabled, the library records CUDA events on the launching stream around its hot kernels
  * and accumulates, per kernel kind kid (0 jacobi_sweep, 1 jacobi_init2, 2 div_grad_dot,
- * 3 x_update, 4 p_update, 5 r_update, 6 nl_rhs, 7 project, 8 divergence2), the launches, the
- * elapsed milliseconds and the algorithmic bytes moved.  launch_count counts every kernel
+ * 3 x_update, 4 p_update, 5 r_update, 6 nl_rhs, 7 project, 8 divergence2, 9 mg_sweep,
+ * 10 mg_init, 11 mg_residual, 12 mg_transfer, 13 mg_pre_smooth, 14 mg_post_smooth), the
+ * launches, the elapsed milliseconds and the algorithmic bytes moved.  launch_count counts every kernel
  * launch the library has issued since load. */
 void impact_b200_profile_enable(int enable);
 void impact_b200_profile_reset(void);
@@ -282,8 +287,10 @@ int impact_b200_case_kernel_bench(impact_b200_case* c, int kid, int iters, doubl
  * the solve precision (FP64, or FP32 for the inner solve of a mixed case), the engine built with
  * the solver parameters p.  kind: 0 sweep, 1 init sweep, 2 residual, 3 prolongation,
  * 4 restriction, 5 A x + inner product, 6 A x + two inner products, 7 x update, 8 p update,
- * 9 r update, 10 one V-cycle, 11 one BiCGstab iteration.  Returns the average ms per launch
- * (CUDA events on the case stream) and the algorithmic bytes of one launch (0 for 10, 11). */
+ * 9 r update, 10 one V-cycle, 11 one BiCGstab iteration, 12 fused pre-smoothing (init sweep,
+ * mg_down - 1 sweeps and the residual in one kernel), 13 fused post-smoothing (mg_up sweeps).
+ * Returns the average ms per launch (CUDA events on the case stream) and the algorithmic bytes of
+ * one launch (0 for 10, 11). */
 int impact_b200_case_engine_bench(impact_b200_case* c, int kind, int iters, const impact_b200_solver_params* p,
                                   double* ms, double* bytes);
 
