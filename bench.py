@@ -59,7 +59,9 @@ def parse():
     ap.add_argument("--kernels", default="all", help="kernels: comma-separated names to run (default all)")
     ap.add_argument("--iters", type=int, default=20, help="kernels: timed launches per kernel")
     ap.add_argument("--no-extra", action="store_true", help="skip the batch and serve samples of the default line")
-    ap.add_argument("--no-tune", action="store_true", help="keep tile depth 32 and 4/4/4 sweeps (no autotuning)")
+    ap.add_argument("--no-tune", action="store_true", help="keep --tile-kc and --sweeps (no autotuning)")
+    ap.add_argument("--sweeps", type=int, default=4, help="V-cycle sweeps down / up / bottom without autotuning")
+    ap.add_argument("--tile-kc", type=int, default=32, help="tile depth of the solver kernels without autotuning")
     ap.add_argument("--no-profile", action="store_true", help="no per-kernel events in the timed steps (no roofline)")
     ap.add_argument("--cases", type=int, default=48, help="batch: number of cases")
     ap.add_argument("--requests", type=int, default=16, help="serve: number of requests")
@@ -93,7 +95,8 @@ def step_params(args, precision):
                          tol_rel=1e-8, max_it=(5000 if args.precond == 0 else 200) if precision == 0 else 40,
                          n_sweeps=args.n_sweeps, omega=0.8, init_yes=0, check_every=args.check_every,
                          inner_tol_rel=args.inner_tol, inner_max_it=4000 if args.precond == 0 else 400,
-                         precond=args.precond, mg_down=4, mg_up=4, mg_bottom=4)
+                         precond=args.precond, mg_down=args.sweeps, mg_up=args.sweeps, mg_bottom=args.sweeps,
+                         tile_kc=args.tile_kc)
 
 
 class ClockSampler:
@@ -163,16 +166,17 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
 
 
-def traffic_per_cell():
-    """dram bytes per cell and launch of the profiled kernels, from the committed ncu summary."""
+def traffic_ratio():
+    """{kernel kind: measured DRAM bytes / algorithmic bytes} of one launch, from the committed ncu
+    summaries (profiles/traffic_per_cell.txt)."""
     out = {}
     p = os.path.join(ROOT, "profiles", "traffic_per_cell.txt")
     if os.path.exists(p):
         for line in open(p):
             if line.startswith("#") or not line.strip():
                 continue
-            k, v = line.split()[:2]
-            out[k] = float(v)
+            k, dram, alg = line.split()[:3]
+            out[k] = float(dram) / float(alg)
     return out
 
 
@@ -197,10 +201,12 @@ def run_arm(args, precision, device, rank, world, dist, profile_on, e2e_on):
             tuning = {"chosen": {"tile_kc": best.tile_kc, "sweeps": [best.mg_down, best.mg_up, best.mg_bottom]},
                       "candidates": report}
     stream = torch.cuda.ExternalStream(case.stream, device=device)
-    # pinned host copies of the state the Fortran host owns between steps (velocity, pressure,
-    # nonlinear term): uploaded before and downloaded after every step, as a drop-in call would
+    # pinned host copies of the state the Fortran host owns between time steps -- velocity and
+    # pressure (the initial guess of the next Poisson solve); the nonlinear term is not state:
+    # the first substep does not read the previous one (mod_rhs.f90, bRK(1) = 0) -- uploaded
+    # before and downloaded after every step, as a drop-in call would
     host = {f: torch.empty(grid.shape, dtype=torch.float64, pin_memory=True).numpy()
-            for f in ("vel1", "vel2", "vel3", "pre", "nl1", "nl2", "nl3")} if e2e_on else {}
+            for f in ("vel1", "vel2", "vel3", "pre")} if e2e_on else {}
     for f, a in host.items():
         case.download(f, a)
     bytes_in = bytes_out = sum(a.nbytes for a in host.values())
@@ -565,10 +571,13 @@ def main():
         name, (launches, ms, byts) = dom
         per_launch_bytes = byts / launches
         achieved = per_launch_bytes / (ms / launches / 1e3) / 1e9
-        tpc = traffic_per_cell().get(name)
+        ratio = traffic_ratio().get(name)
         roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peak_note,
-                "traffic": (tpc * cells) if tpc else None, "algorithmic_bytes_per_launch": per_launch_bytes,
+                "traffic": round(ratio * per_launch_bytes) if ratio else None,
+                "traffic_source": "ncu dram bytes / algorithmic bytes of one finest-level launch (profiles/), "
+                                  "times the algorithmic bytes per launch" if ratio else None,
+                "algorithmic_bytes_per_launch": per_launch_bytes,
                 "launches": launches, "avg_launch_ms": ms / launches,
                 "share_of_step": round(ms / mixed["ms_prof"], 3),
                 "measured_over": (f"{K} further steps of the same case after the timed ones, CUDA events around every "
