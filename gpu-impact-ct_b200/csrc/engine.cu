@@ -476,6 +476,11 @@ __device__ __forceinline__ void cp_async1(T* smem, const T* gmem) {
   else
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+// 16 bytes (both addresses 16-byte aligned), L2 only
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() {
@@ -1329,14 +1334,20 @@ __device__ __forceinline__ void sload(const T* p, T (&o)[VecT<T>::W]) {
   }
 }
 
-template <typename T, int NSW, bool INIT, bool RES>
+// FAST: every job of the list has n1 divisible by V and uniform z.  The region then starts HX =
+// S rounded up to V columns left of the tile, so that every thread's V columns are one aligned
+// 16-byte vector of the field (a periodic wrap never splits it): one 16-byte cp.async per plane
+// and vector stores of the outputs; the z coefficients are constants.  Otherwise HX = S and
+// every column moves on its own.
+template <typename T, int NSW, bool INIT, bool RES, bool FAST>
 __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
                                                      int nj, int ntiles, T omega) {
   constexpr int S = NSW + (RES ? 1 : 0);
   using LY = MLayout<T, S, INIT>;
   constexpr int V = LY::V;
   constexpr int W0 = LY::W0, H0 = LY::H0, R0 = LY::R0, NBR = LY::NBR, NCR = LY::NCR;
-  constexpr int X = W0 - 2 * S, Y = H0 - 2 * S;
+  constexpr int HX = FAST ? (S + V - 1) / V * V : S;  // x halo of the region
+  constexpr int X = W0 - 2 * HX, Y = H0 - 2 * S;
   extern __shared__ __align__(16) unsigned char lm_raw[];
   T* const sm = reinterpret_cast<T*>(lm_raw);
   T* const pub = sm + LY::pub();  // pub[(slot * S + s) * R0 + y * W0 + x]
@@ -1358,12 +1369,12 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
     const int k0 = tc * kc + 1, k1 = min(g.n3, k0 + kc - 1);
     const int nq = (k1 - k0 + 1) + 2 * S;  // planes k0-S .. k1+S
     const T* __restrict__ cz = J.cdg[2];
-    const bool zu = J.zuni != 0;
+    const bool zu = FAST || J.zuni != 0;
     T a0[V], a1[V], a2[V], inv[V];
     int xo[V];
 #pragma unroll
     for (int c = 0; c < V; ++c) {
-      const int gi = wrapn(i0 - S + x0 + c, g.n1);
+      const int gi = wrapn(i0 - HX + x0 + c, g.n1);
       a0[c] = J.cdg[0][3 * (gi - 1)];
       a1[c] = J.cdg[0][3 * (gi - 1) + 1];
       a2[c] = J.cdg[0][3 * (gi - 1) + 2];
@@ -1375,21 +1386,28 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
     const T zcm = cz[0], zcc = cz[1], zcp = cz[2];  // the z row of a uniform z axis
 #pragma unroll
     for (int c = 0; c < V; ++c) inv[c] = zu ? omega / (a1[c] + b1 + zcc) : T(0);
-    // outputs of this thread: columns i = i0 + x0 - S + c of row j = j0 + y - S
-    const int io = i0 + x0 - S, jo = j0 + y - S;
+    // outputs of this thread: columns i = io + c of row jo, when its vector lies in the tile interior
+    const int io = i0 + x0 - HX, jo = j0 + y - S;
     const bool rowout = y >= S && y < H0 - S && jo <= g.n2;
     const long long obase = (long long)(io + 3) + (long long)g.nx * (jo + 3);
-    const T* __restrict__ A = J.A;
-    const T* __restrict__ Cin = J.C;
+    const T* __restrict__ Ab = J.A + yo + (FAST ? xo[0] : 0);
+    const T* __restrict__ Cb = J.C + yo + (FAST ? xo[0] : 0);
+    int kin = wrapn(k0 - S, g.n3);  // wrapped plane of the next stage_in
     auto stage_in = [&](int qq) {  // plane qq of A (and of C) at this thread's columns
       if (qq < nq) {
-        const long long zo = (long long)(wrapn(k0 - S + qq, g.n3) + 3) * g.nxy + yo;
+        const long long zo = (long long)(kin + 3) * g.nxy;
+        kin = kin == g.n3 ? 1 : kin + 1;
         T* bd = br + (qq % NBR) * R0 + e0;
         T* cd = cr + (qq % NCR) * R0 + e0;
+        if constexpr (FAST) {
+          cp_async16(bd, Ab + zo);
+          if (!INIT) cp_async16(cd, Cb + zo);
+        } else {
 #pragma unroll
-        for (int c = 0; c < V; ++c) {
-          cp_async1(bd + c, A + zo + xo[c]);
-          if (!INIT) cp_async1(cd + c, Cin + zo + xo[c]);
+          for (int c = 0; c < V; ++c) {
+            cp_async1(bd + c, Ab + zo + xo[c]);
+            if (!INIT) cp_async1(cd + c, Cb + zo + xo[c]);
+          }
         }
       }
       cp_commit();
@@ -1429,10 +1447,13 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
           const bool rowin = y >= s && y < H0 - s;  // the row lies inside stage s's region
           const T* pr = pub + (rslot * S + (s - 1)) * R0;  // stage s-1 at plane qs (published at t-1)
           const int kk = k0 - S + qs;  // unwrapped; the outputs (s == S) lie in k0..k1
-          const int k3 = zu ? 0 : 3 * (wrapn(kk, g.n3) - 1);
-          const T cm = zu ? zcm : cz[k3];
-          const T cc = zu ? zcc : cz[k3 + 1];
-          const T cp = zu ? zcp : cz[k3 + 2];
+          T cm = zcm, cc = zcc, cp = zcp;
+          if (!zu) {
+            const int k3 = 3 * (wrapn(kk, g.n3) - 1);
+            cm = cz[k3];
+            cc = cz[k3 + 1];
+            cp = cz[k3 + 2];
+          }
           // x neighbours across vectors: every lane takes part in the shuffles
           const T wl = __shfl_up_sync(0xffffffffu, Qz[s - 1][V - 1][s0], 1, 16);  // column x0 - 1
           const T er = __shfl_down_sync(0xffffffffu, Qz[s - 1][0][s0], 1, 16);    // column x0 + V
@@ -1444,24 +1465,34 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
             sload(pr + e0 - W0, so);
             sload(pr + e0 + W0, no);
             sload(br + (qs % NBR) * R0 + e0, bv);
-            const long long ob = obase + (long long)g.nxy * (kk + 3);
+            T rv[V];
 #pragma unroll
             for (int c = 0; c < V; ++c) {
               const T zm = Qz[s - 1][c][sm1], zc = Qz[s - 1][c][s0], zp = Qz[s - 1][c][sp1];
               const T w = c == 0 ? wl : Qz[s - 1][c - 1][s0];
               const T ea = c == V - 1 ? er : Qz[s - 1][c + 1][s0];
-              const bool out = s == S && rowout && x0 + c >= S && x0 + c < W0 - S && io + c <= g.n1;
               if (RES && s == S) {
-                const T res = jresid(bv[c], a0[c], w, a2[c], ea, b0, so[c], b2, no[c], cm, zm, cp, zp,
-                                     a1[c] + b1 + cc, zc);
-                if (out) {
-                  J.C[ob + c] = res;
-                  J.B[ob + c] = zc;
-                }
+                rv[c] = jresid(bv[c], a0[c], w, a2[c], ea, b0, so[c], b2, no[c], cm, zm, cp, zp, a1[c] + b1 + cc, zc);
+                ov[c] = zc;
               } else {
                 const T rr = jres(bv[c], a0[c], w, a2[c], ea, b0, so[c], b2, no[c], cm, zm, cp, zp);
                 ov[c] = jsweep(rr, zc, omega, zu, inv[c], a1[c] + b1 + cc);
-                if (s == S && out) J.B[ob + c] = ov[c];
+              }
+            }
+            if (s == S && rowout) {  // the outputs: B = the last sweep (or x_NSW), C = the residual
+              const long long ob = obase + (long long)g.nxy * (kk + 3);
+              if constexpr (FAST) {
+                if (x0 >= HX && x0 < W0 - HX && io <= g.n1) {
+                  vstore(J.B + ob, ov);
+                  if (RES) vstore(J.C + ob, rv);
+                }
+              } else {
+#pragma unroll
+                for (int c = 0; c < V; ++c)
+                  if (x0 + c >= HX && x0 + c < W0 - HX && io + c <= g.n1) {
+                    J.B[ob + c] = ov[c];
+                    if (RES) J.C[ob + c] = rv[c];
+                  }
               }
             }
           }
@@ -1524,8 +1555,11 @@ void ax_attributes() {
   cudaFuncSetAttribute(k_kr_ax<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
   cudaFuncSetAttribute(k_kr_ax<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
   cudaFuncSetAttribute(k_kr_ax<double, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
-#define IMPACT_MULTI_ATTR(T, N, I, R) \
-  cudaFuncSetAttribute(k_lv_multi<T, N, I, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)multi_smem_bytes<T, N, I, R>())
+#define IMPACT_MULTI_ATTR(T, N, I, R)                                                                           \
+  cudaFuncSetAttribute(k_lv_multi<T, N, I, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,               \
+                       (int)multi_smem_bytes<T, N, I, R>());                                                    \
+  cudaFuncSetAttribute(k_lv_multi<T, N, I, R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,              \
+                       (int)multi_smem_bytes<T, N, I, R>())
   IMPACT_MULTI_ATTR(float, 1, true, true);
   IMPACT_MULTI_ATTR(float, 2, true, true);
   IMPACT_MULTI_ATTR(float, 2, false, false);
@@ -1794,17 +1828,22 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
     std::vector<int> tiles;
     double c = 0.0, f = 0.0, cc = 0.0;
     bool fast = !members.empty();
+    bool mfast = true;  // fused lists: every job vectorisable with uniform z (the kernel's FAST path)
+    for (auto& m : members) {
+      const LevelJob<T> Jt = lvjob(m.first, m.second, variant);
+      mfast = mfast && Jt.vw == VecT<T>::W && Jt.zuni;
+    }
     for (auto& m : members) {
       jobs.push_back(lvjob(m.first, m.second, variant));
       if (!vec) jobs.back().vw = 1;
       if (fusedS > 0) {
         LevelJob<T>& Jm = jobs.back();
         int kcm = KC_MAX;
-        while (kcm > 8 && tiles_multi(Jm.g, kcm, (int)sizeof(T), fusedS) < 2 * 148) kcm /= 2;
+        while (kcm > 8 && tiles_multi(Jm.g, kcm, (int)sizeof(T), fusedS, mfast) < 2 * 148) kcm /= 2;
         Jm.kc = kcm;
       }
       const LevelJob<T>& J = jobs.back();
-      tiles.push_back(fusedS > 0 ? tiles_multi(J.g, J.kc, (int)sizeof(T), fusedS) : tiles_of(J.g, kc, J.vw));
+      tiles.push_back(fusedS > 0 ? tiles_multi(J.g, J.kc, (int)sizeof(T), fusedS, mfast) : tiles_of(J.g, kc, J.vw));
       c += vol(J.g);
       if (J.Cf) f += vol(J.gf);
       if (J.Bc) cc += vol(J.gc);
@@ -1904,6 +1943,31 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
   return 0;
 }
 
+// fused smoothing launches: pre-smoothing with mg_down sweeps, post-smoothing with mg_up sweeps
+template <typename T, int NSW, bool INIT, bool RES>
+void launch_multi(bool fast, const LevelJob<T>* J, const DevList& L, T om, cudaStream_t s) {
+  if (fast)
+    k_lv_multi<T, NSW, INIT, RES, true><<<grid_multi(L.ntiles), kMBlock, multi_smem_bytes<T, NSW, INIT, RES>(), s>>>(
+        J, L.ts, L.njobs, L.ntiles, om);
+  else
+    k_lv_multi<T, NSW, INIT, RES, false><<<grid_multi(L.ntiles), kMBlock, multi_smem_bytes<T, NSW, INIT, RES>(), s>>>(
+        J, L.ts, L.njobs, L.ntiles, om);
+}
+template <typename T>
+void launch_multi_pre(int sweeps, bool fast, const LevelJob<T>* J, const DevList& L, T om, cudaStream_t s) {
+  if (sweeps == 2)
+    launch_multi<T, 1, true, true>(fast, J, L, om, s);
+  else
+    launch_multi<T, 2, true, true>(fast, J, L, om, s);
+}
+template <typename T>
+void launch_multi_post(int sweeps, bool fast, const LevelJob<T>* J, const DevList& L, T om, cudaStream_t s) {
+  if (sweeps == 2)
+    launch_multi<T, 2, false, false>(fast, J, L, om, s);
+  else
+    launch_multi<T, 3, false, false>(fast, J, L, om, s);
+}
+
 template <typename T>
 void Engine<T>::enqueue_phase(const Phase& ph) {
   const DevList& L = arena_.lists[ph.list];
@@ -1939,16 +2003,10 @@ void Engine<T>::enqueue_phase(const Phase& ph) {
       IMPACT_PROF(prof::K_MG_OTHER, sz * (2 * c + cc), s, (k_lv_prolong<T><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles, ph.flip)));
       break;
     case PH_PRE:  // mg_down 2 or 3
-      if (p_.mg_down == 2)
-        IMPACT_PROF(prof::K_MG_PRE, 3 * sz * c, s, (k_lv_multi<T, 1, true, true><<<grid_multi(L.ntiles), kMBlock, multi_smem_bytes<T, 1, true, true>(), s>>>(J, L.ts, L.njobs, L.ntiles, om)));
-      else
-        IMPACT_PROF(prof::K_MG_PRE, 3 * sz * c, s, (k_lv_multi<T, 2, true, true><<<grid_multi(L.ntiles), kMBlock, multi_smem_bytes<T, 2, true, true>(), s>>>(J, L.ts, L.njobs, L.ntiles, om)));
+      IMPACT_PROF(prof::K_MG_PRE, 3 * sz * c, s, launch_multi_pre<T>(p_.mg_down, fast_[ph.list] != 0, J, L, om, s));
       break;
     case PH_POST:  // mg_up 2 or 3
-      if (p_.mg_up == 2)
-        IMPACT_PROF(prof::K_MG_POST, 3 * sz * c, s, (k_lv_multi<T, 2, false, false><<<grid_multi(L.ntiles), kMBlock, multi_smem_bytes<T, 2, false, false>(), s>>>(J, L.ts, L.njobs, L.ntiles, om)));
-      else
-        IMPACT_PROF(prof::K_MG_POST, 3 * sz * c, s, (k_lv_multi<T, 3, false, false><<<grid_multi(L.ntiles), kMBlock, multi_smem_bytes<T, 3, false, false>(), s>>>(J, L.ts, L.njobs, L.ntiles, om)));
+      IMPACT_PROF(prof::K_MG_POST, 3 * sz * c, s, launch_multi_post<T>(p_.mg_up, fast_[ph.list] != 0, J, L, om, s));
       break;
     default:
       break;

@@ -35,8 +35,11 @@ inline int tiles_of(const Geom& g, int kc, int vw = 1) {
 // row per half-warp); with S stencil stages it yields (16 V - 2S) x (MNT / 16 - 2S) output
 // columns, kc planes deep.
 constexpr int MNT = 512;
-inline int tiles_multi(const Geom& g, int kc, int sz, int S) {
-  const int X = 16 * (16 / sz) - 2 * S, Y = MNT / 16 - 2 * S;
+// fast: the aligned path (every job with n1 divisible by V = 16 / sz and uniform z), whose x halo
+// is S rounded up to V
+inline int tiles_multi(const Geom& g, int kc, int sz, int S, bool fast) {
+  const int V = 16 / sz, HX = fast ? (S + V - 1) / V * V : S;
+  const int X = 16 * V - 2 * HX, Y = MNT / 16 - 2 * S;
   return ((g.n1 + X - 1) / X) * ((g.n2 + Y - 1) / Y) * ((g.n3 + kc - 1) / kc);
 }
 
