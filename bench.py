@@ -60,8 +60,10 @@ def parse():
     ap.add_argument("--iters", type=int, default=20, help="kernels: timed launches per kernel")
     ap.add_argument("--no-extra", action="store_true", help="skip the batch and serve samples of the default line")
     ap.add_argument("--no-tune", action="store_true", help="keep --tile-kc and --sweeps (no autotuning)")
-    ap.add_argument("--sweeps", type=int, default=4, help="V-cycle sweeps down / up / bottom without autotuning")
-    ap.add_argument("--tile-kc", type=int, default=32, help="tile depth of the solver kernels without autotuning")
+    ap.add_argument("--sweeps", type=int, default=3,
+                    help="V-cycle sweeps down / up / bottom of the batch and serve cases, and of the single case "
+                         "with --no-tune (default: the autotuner's choice on the 384 case)")
+    ap.add_argument("--tile-kc", type=int, default=64, help="tile depth of the solver kernels, as --sweeps")
     ap.add_argument("--no-profile", action="store_true", help="no per-kernel events in the timed steps (no roofline)")
     ap.add_argument("--cases", type=int, default=48, help="batch: number of cases")
     ap.add_argument("--requests", type=int, default=16, help="serve: number of requests")
@@ -402,7 +404,8 @@ def _case_params(spec, precision, args):
     return I.step_params(Re=spec["Re"], CFL=0.2, dtime_max=1.0, dtime0=1e9, U0=spec["U0"], T_pulse=1.0,
                          level_pressure=1, tol_rel=1e-8, max_it=200 if precision == 0 else 40, omega=0.8,
                          init_yes=0, check_every=args.check_every, inner_tol_rel=args.inner_tol, inner_max_it=400,
-                         precond=1, mg_down=4, mg_up=4, mg_bottom=4)
+                         precond=1, mg_down=args.sweeps, mg_up=args.sweeps, mg_bottom=args.sweeps,
+                         tile_kc=args.tile_kc)
 
 
 def _make_case(spec, precision, device, labels=None):

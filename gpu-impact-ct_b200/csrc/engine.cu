@@ -106,9 +106,9 @@ __device__ __forceinline__ void vstore(T* p, const T (&o)[VecT<T>::W]) {
 }
 
 // NQ block-wide partials of one tile into out[0..NQ-1]; bit q of MAXMASK: max instead of sum
-template <int NQ, int MAXMASK>
+template <int NQ, int MAXMASK, int NTH = ENT>
 __device__ __forceinline__ void tile_partials(double (&v)[NQ], double* __restrict__ out) {
-  __shared__ double sh[NQ][ENT / 32];
+  __shared__ double sh[NQ][NTH / 32];
   const int tid = threadIdx.x + ETX * threadIdx.y;
   const int lane = tid & 31, w = tid >> 5;
 #pragma unroll
@@ -121,7 +121,7 @@ __device__ __forceinline__ void tile_partials(double (&v)[NQ], double* __restric
   if (w == 0) {
 #pragma unroll
     for (int q = 0; q < NQ; ++q) {
-      double x = lane < ENT / 32 ? sh[q][lane] : 0.0;
+      double x = lane < NTH / 32 ? sh[q][lane] : 0.0;
       x = ((MAXMASK >> q) & 1) ? e_wmax(x) : e_wsum(x);
       if (lane == 0) out[q] = x;
     }
@@ -488,19 +488,23 @@ __device__ __forceinline__ void cp_wait() {
 }
 
 // A x = sum_m D_m G_m x with the two 6-point stencils of each axis collapsed into one 11-point
-// stencil W_m (weights formed once on the host in FP64).  A block owns 32 x 8 columns over kc
-// planes.  Each plane of the tile with its 5-wide x/y halo (42 x 18 elements, periodic images),
-// and the inner-product partner of the plane, are staged by cp.async into a ring of R shared-
-// memory slots R-1 planes ahead of their use, so that about R planes of DRAM traffic are in
-// flight per block.  x and y neighbours and the z values k..k+5 of the column are read from
-// the ring; the z values k-5..k-1 stay in a register window.
+// stencil W_m (weights formed once on the host in FP64).  A block of 32 x 4 threads owns one
+// 32 x 8-column tile over kc planes; each thread computes the two adjacent rows ya = 2 ty and
+// ya + 1 of its column, so that the 12 staged rows ya-5 .. ya+6 serve both y stencils.  Each
+// plane of the tile with its 5-wide x/y halo (42 x 18 elements, periodic images), and the
+// inner-product partner of the plane, are staged by cp.async into a ring of R shared-memory slots
+// R-1 planes ahead of their use.  x and y neighbours come from the ring; the z values k-5 .. k+5
+// of the two points stay in register windows, each step adding plane k+5 from the ring.  The y
+// weights of the two rows and, on uniform z, the z weights are registers in FP32 and
+// warp-broadcast shared-memory reads in FP64.
 //   MODE 0: rr = A phi                 (initial residual)
 //   MODE 1: Ap = A z1, partial rh.Ap   (alpha)
 //   MODE 2: Ar = A z2, partials Ar.rr, Ar.Ar (omega)
 //   MODE 3: FP64 only: r32 = (float)(bb - A phi), partials max|r|, sum r^2, sum bb^2 (the outer
 //           residual of the mixed-precision solve and the right-hand side of its inner solve)
+constexpr int AXTY = ETY / 2, AXNT = ETX * AXTY;  // 32 x 4 threads, two rows each
 constexpr int AX_TW = ETX + 10, AX_TH = ETY + 10, AX_TE = AX_TW * AX_TH;
-constexpr int AX_PER = (AX_TE + ENT - 1) / ENT;  // staged elements per thread and plane
+constexpr int AX_PER = (AX_TE + AXNT - 1) / AXNT;  // staged elements per thread and plane
 // ring depth: planes k .. k+5 are read at plane k, the rest of the ring is in flight
 template <typename T>
 struct AxRing {
@@ -513,9 +517,10 @@ constexpr size_t ax_smem_bytes() {
 }
 
 template <typename T, int MODE>
-__global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts,
-                                                  int nj, int ntiles, double* __restrict__ partial) {
+__global__ void __launch_bounds__(AXNT, 3) k_kr_ax(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+                                                   int nj, int ntiles, double* __restrict__ partial) {
   constexpr int AX_R = AxRing<T>::R;
+  constexpr bool REG = sizeof(T) == 4;  // y and z weights in registers
   extern __shared__ __align__(16) unsigned char ax_smem[];
   T(*ring)[AX_TH][AX_TW] = reinterpret_cast<T(*)[AX_TH][AX_TW]>(ax_smem);
   T(*dring)[ENT] = reinterpret_cast<T(*)[ENT]>(ax_smem + sizeof(T) * AX_R * AX_TE);
@@ -523,30 +528,34 @@ __global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict
   T(*wys)[AXW] = reinterpret_cast<T(*)[AXW]>(ax_smem + sizeof(T) * (AX_R * AX_TE + AX_R * ENT + KC_MAX * AXW));
   T(*wxs)[ETX] =
       reinterpret_cast<T(*)[ETX]>(ax_smem + sizeof(T) * (AX_R * AX_TE + AX_R * ENT + KC_MAX * AXW + ETY * AXW));
-  const int tid = threadIdx.x + ETX * threadIdx.y;
   const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + ETX * ty;
+  const int ya = 2 * ty;  // tile rows ya and ya + 1 of this thread
   for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
     const int q = find_job(ts, nj, b);
     const KrylovJob<T>& J = jobs[q];
     const SolverScalars* sc = J.sc;
     if (MODE == 0 ? (sc->done != 0) : e_halted(sc)) continue;
     const Geom g = J.g;
-    int i, j, k0, k1;
-    tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
-    const int i0 = i - tx, j0 = j - ty;
-    const bool in = i <= g.n1 && j <= g.n2;
+    const int ntx = (g.n1 + ETX - 1) / ETX, nty = (g.n2 + ETY - 1) / ETY;
+    const int t0 = b - ts[q];
+    const int ta = t0 % ntx, tr = t0 / ntx, tc = tr / nty;
+    const int i0 = ta * ETX + 1, j0 = (tr - tc * nty) * ETY + 1;
+    const int k0 = tc * J.kc + 1, k1 = min(g.n3, k0 + J.kc - 1);
+    const int i = i0 + tx;
+    const bool in0 = i <= g.n1 && j0 + ya <= g.n2, in1 = i <= g.n1 && j0 + ya + 1 <= g.n2;
     const T* __restrict__ x = (MODE == 0 || MODE == 3) ? J.phi : (MODE == 1 ? J.z1 : J.z2);
     T* __restrict__ out = MODE == 0 ? J.rr : (MODE == 1 ? J.Ap : J.Ar);
     const T* __restrict__ d1 = MODE == 1 ? J.rh : (MODE == 3 ? J.bb : J.rr);
     const long long nxy = g.nxy;
     // weights of the tile: z rows of its planes, y rows of its 8 rows, x rows of its 32 columns
     const int nzw = (k1 - k0 + 1) * AXW;
-    for (int t = tid; t < nzw; t += ENT) wzs[t / AXW][t % AXW] = J.W[2][(k0 - 1) * AXW + t];
-    for (int t = tid; t < ETY * AXW; t += ENT) {
+    for (int t = tid; t < nzw; t += AXNT) wzs[t / AXW][t % AXW] = J.W[2][(k0 - 1) * AXW + t];
+    for (int t = tid; t < ETY * AXW; t += AXNT) {
       const int jj = j0 + t / AXW;
       wys[t / AXW][t % AXW] = jj <= g.n2 ? J.W[1][(jj - 1) * AXW + t % AXW] : T(0);
     }
-    for (int t = tid; t < ETX * AXW; t += ENT) {
+    for (int t = tid; t < ETX * AXW; t += AXNT) {
       const int ii = i0 + t / AXW;
       wxs[t % AXW][t / AXW] = ii <= g.n1 ? J.W[0][(ii - 1) * AXW + t % AXW] : T(0);
     }
@@ -554,12 +563,15 @@ __global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict
     int eo[AX_PER];
 #pragma unroll
     for (int e = 0; e < AX_PER; ++e) {
-      const int t = tid + e * ENT;
+      const int t = tid + e * AXNT;
       const int r = t / AX_TW, c = t % AX_TW;
       const int gi = wrapi(i0 - 5 + c, g.n1), gj = wrapi(j0 - 5 + r, g.n2);
       eo[e] = t < AX_TE ? (gi + 3) + g.nx * (gj + 3) : -1;
     }
-    const int own = (in ? i + 3 : 4) + g.nx * ((in ? j : 1) + 3);  // the column's in-plane offset
+    // the two points' in-plane offsets (an idle point reads a valid column and stores nothing)
+    const int own0 = (in0 ? i + 3 : 4) + g.nx * ((in0 ? j0 + ya : 1) + 3);
+    const int own1 = (in1 ? i + 3 : 4) + g.nx * ((in1 ? j0 + ya + 1 : 1) + 3);
+    const int pa = ya * ETX + tx, pb = pa + ETX;  // the points' slots in the partner ring
     auto zoff = [&](int k) -> long long {  // plane k (periodic) + 3 ghost planes
       return (long long)((k < 1 ? k + g.n3 : (k > g.n3 ? k - g.n3 : k)) + 3) * nxy;
     };
@@ -571,91 +583,139 @@ __global__ void __launch_bounds__(ENT, 2) k_kr_ax(const KrylovJob<T>* __restrict
         const T* src = x + zoff(kk);
 #pragma unroll
         for (int e = 0; e < AX_PER; ++e)
-          if (eo[e] >= 0) cp_async1(slot + tid + e * ENT, src + eo[e]);
-        if (MODE != 0 && kk >= k0 && kk <= k1 && in) cp_async1(&dring[sl][tid], d1 + zoff(kk) + own);
+          if (eo[e] >= 0) cp_async1(slot + tid + e * AXNT, src + eo[e]);
+        if (MODE != 0 && kk >= k0 && kk <= k1) {
+          if (in0) cp_async1(&dring[sl][pa], d1 + zoff(kk) + own0);
+          if (in1) cp_async1(&dring[sl][pb], d1 + zoff(kk) + own1);
+        }
       }
       cp_commit();
     };
     __syncthreads();  // weights visible
-    T wx[AXW], wyr[AXW], wzr[AXW];
-    // FP32: the y weights of the row, and on uniform z the z weights, stay in registers
-    const bool zu = sizeof(T) == 4 && J.zuni != 0;
+    const bool zu = J.zuni != 0;
+    T wx[AXW], wya[AXW], wyb[AXW], wzr[AXW];
 #pragma unroll
     for (int l = 0; l < AXW; ++l) {
       wx[l] = wxs[l][tx];
-      wyr[l] = wys[ty][l];
-      wzr[l] = wzs[0][l];
+      wya[l] = REG ? wys[ya][l] : T(0);
+      wyb[l] = REG ? wys[ya + 1][l] : T(0);
+      wzr[l] = REG ? wzs[0][l] : T(0);
     }
-    // the past z values x(k0-5 .. k0-1) of the column, then the ring from plane k0
-    T zp[5];
+    // z windows: planes k-5 .. k+5 of the two points; the past ones now, the rest from the ring
+    T za[AXW], zb[AXW];
 #pragma unroll
-    for (int l = 0; l < 5; ++l) zp[l] = in ? x[zoff(k0 - 5 + l) + own] : T(0);
+    for (int l = 0; l < 5; ++l) {
+      za[l] = x[zoff(k0 - 5 + l) + own0];
+      zb[l] = x[zoff(k0 - 5 + l) + own1];
+    }
+#pragma unroll
+    for (int l = 5; l < AXW; ++l) za[l] = zb[l] = T(0);
 #pragma unroll
     for (int l = 0; l < AX_R - 1; ++l) stage(k0 + l);
     double v0 = 0.0, v1 = 0.0, v2 = 0.0;
-    T* __restrict__ op = out + (long long)(k0 + 3) * nxy + own;  // tile planes never wrap
-    float* __restrict__ op32 = MODE == 3 ? J.r32 + (long long)(k0 + 3) * nxy + own : nullptr;
+    const long long ob0 = (long long)(k0 + 3) * nxy + own0, ob1 = (long long)(k0 + 3) * nxy + own1;
     auto walk = [&](auto zreg) {
-    constexpr bool ZR = decltype(zreg)::value;
-    constexpr bool YR = sizeof(T) == 4;
-    for (int k = k0; k <= k1; ++k, op += nxy, op32 += (MODE == 3 ? nxy : 0)) {
-      cp_wait<AX_R - 7>();  // this thread's copies of planes k .. k+5 have landed
-      __syncthreads();      // everybody's have; the slot of plane k-1 is free again
-      stage(k + AX_R - 1);
-      const int sl = (k - k0) & (AX_R - 1);
-      const T (*sp)[AX_TW] = ring[sl];
-      if (in) {
-        const T c = sp[ty + 5][tx + 5];
-        T ax = wx[0] * sp[ty + 5][tx];
+      constexpr bool ZR = decltype(zreg)::value;
+      for (int k = k0; k <= k1; ++k) {
+        cp_wait<AX_R - 7>();  // this thread's copies of planes k .. k+5 have landed
+        __syncthreads();      // everybody's have; the slot of plane k-1 is free again
+        stage(k + AX_R - 1);
+        const int sl = (k - k0) & (AX_R - 1);
+        const T (*sp)[AX_TW] = ring[sl];
+        if (k == k0) {  // the windows' planes k0 .. k0+5
 #pragma unroll
-        for (int l = 1; l < AXW; ++l) ax += wx[l] * (l == 5 ? c : sp[ty + 5][tx + l]);
-        T ay = (YR ? wyr[0] : wys[ty][0]) * sp[ty][tx + 5];
-#pragma unroll
-        for (int l = 1; l < AXW; ++l) ay += (YR ? wyr[l] : wys[ty][l]) * (l == 5 ? c : sp[ty + l][tx + 5]);
-        const T* wz = wzs[k - k0];
-        T az = (ZR ? wzr[0] : wz[0]) * zp[0];
-#pragma unroll
-        for (int l = 1; l < 5; ++l) az += (ZR ? wzr[l] : wz[l]) * zp[l];
-        az += (ZR ? wzr[5] : wz[5]) * c;
-#pragma unroll
-        for (int l = 6; l < AXW; ++l)
-          az += (ZR ? wzr[l] : wz[l]) * ring[(sl + l - 5) & (AX_R - 1)][ty + 5][tx + 5];
-        const T r = ax + ay + az;
-        if (MODE == 3) {
-          const double bv = (double)dring[sl][tid];
-          const double res = bv - (double)r;
-          *op32 = (float)res;
-          v0 = fmax(v0, fabs(res));
-          v1 += res * res;
-          v2 += bv * bv;
+          for (int l = 0; l < 6; ++l) {
+            za[5 + l] = ring[(sl + l) & (AX_R - 1)][ya + 5][tx + 5];
+            zb[5 + l] = ring[(sl + l) & (AX_R - 1)][ya + 6][tx + 5];
+          }
         } else {
-          *op = r;
-        }
-        if (MODE == 1) v0 += (double)r * (double)dring[sl][tid];
-        if (MODE == 2) {
-          v0 += (double)r * (double)dring[sl][tid];
-          v1 += (double)r * (double)r;
-        }
 #pragma unroll
-        for (int l = 0; l < 4; ++l) zp[l] = zp[l + 1];
-        zp[4] = c;
+          for (int l = 0; l < AXW - 1; ++l) {
+            za[l] = za[l + 1];
+            zb[l] = zb[l + 1];
+          }
+          za[AXW - 1] = ring[(sl + 5) & (AX_R - 1)][ya + 5][tx + 5];
+          zb[AXW - 1] = ring[(sl + 5) & (AX_R - 1)][ya + 6][tx + 5];
+        }
+        const T ca = za[5], cb = zb[5];
+        // x stencils of both rows
+        T axa = wx[0] * sp[ya + 5][tx], axb = wx[0] * sp[ya + 6][tx];
+#pragma unroll
+        for (int l = 1; l < AXW; ++l) {
+          axa += wx[l] * (l == 5 ? ca : sp[ya + 5][tx + l]);
+          axb += wx[l] * (l == 5 ? cb : sp[ya + 6][tx + l]);
+        }
+        // y stencils: staged rows ya .. ya+11 (ya+5, ya+6 are the centres) serve both points
+        T yv[AXW + 1];
+#pragma unroll
+        for (int r = 0; r < AXW + 1; ++r) yv[r] = r == 5 ? ca : (r == 6 ? cb : sp[ya + r][tx + 5]);
+        T aya = (REG ? wya[0] : wys[ya][0]) * yv[0], ayb = (REG ? wyb[0] : wys[ya + 1][0]) * yv[1];
+#pragma unroll
+        for (int l = 1; l < AXW; ++l) {
+          aya += (REG ? wya[l] : wys[ya][l]) * yv[l];
+          ayb += (REG ? wyb[l] : wys[ya + 1][l]) * yv[l + 1];
+        }
+        // z stencils from the windows
+        const T* wz = wzs[k - k0];
+        T aza = (ZR ? wzr[0] : wz[0]) * za[0], azb = (ZR ? wzr[0] : wz[0]) * zb[0];
+#pragma unroll
+        for (int l = 1; l < AXW; ++l) {
+          aza += (ZR ? wzr[l] : wz[l]) * za[l];
+          azb += (ZR ? wzr[l] : wz[l]) * zb[l];
+        }
+        const T ra = axa + aya + aza, rb = axb + ayb + azb;
+        const long long dz = (long long)(k - k0) * nxy;
+        if (MODE == 3) {
+          if (in0) {
+            const double bv = (double)dring[sl][pa];
+            const double res = bv - (double)ra;
+            J.r32[ob0 + dz] = (float)res;
+            v0 = fmax(v0, fabs(res));
+            v1 += res * res;
+            v2 += bv * bv;
+          }
+          if (in1) {
+            const double bv = (double)dring[sl][pb];
+            const double res = bv - (double)rb;
+            J.r32[ob1 + dz] = (float)res;
+            v0 = fmax(v0, fabs(res));
+            v1 += res * res;
+            v2 += bv * bv;
+          }
+        } else {
+          if (in0) out[ob0 + dz] = ra;
+          if (in1) out[ob1 + dz] = rb;
+          if (MODE == 1) {
+            if (in0) v0 += (double)ra * (double)dring[sl][pa];
+            if (in1) v0 += (double)rb * (double)dring[sl][pb];
+          }
+          if (MODE == 2) {
+            if (in0) {
+              v0 += (double)ra * (double)dring[sl][pa];
+              v1 += (double)ra * (double)ra;
+            }
+            if (in1) {
+              v0 += (double)rb * (double)dring[sl][pb];
+              v1 += (double)rb * (double)rb;
+            }
+          }
+        }
       }
-    }
     };
-    if (zu)
+    if (REG && zu)
       walk(std::true_type{});
     else
       walk(std::false_type{});
     cp_wait<0>();
     if (MODE == 1) {
       double v[1] = {v0};
-      tile_partials<1, 0>(v, partial + (long long)b * 4);
+      tile_partials<1, 0, AXNT>(v, partial + (long long)b * 4);
     } else if (MODE == 2) {
       double v[2] = {v0, v1};
-      tile_partials<2, 0>(v, partial + (long long)b * 4);
+      tile_partials<2, 0, AXNT>(v, partial + (long long)b * 4);
     } else if (MODE == 3) {
       double v[3] = {v0, v1, v2};
-      tile_partials<3, 1>(v, partial + (long long)b * 4);
+      tile_partials<3, 1, AXNT>(v, partial + (long long)b * 4);
     } else {
       __syncthreads();  // the ring and the weights are rewritten by the next tile
     }
@@ -1584,6 +1644,7 @@ inline int grid_for(int ntiles) {
   return ntiles < cap ? ntiles : cap;
 }
 const dim3 kBlock(ETX, ETY);
+const dim3 kAxBlock(ETX, AXTY);  // k_kr_ax: two rows per thread
 // the fused smoothing kernel runs one block per tile (one block per SM at a time)
 inline int grid_multi(int ntiles) { return ntiles; }
 
@@ -2030,11 +2091,11 @@ void Engine<T>::enqueue_iteration() {
   prof::count(1);
   IMPACT_PROF(prof::K_P_UPDATE, 4 * fb, s, (k_kr_p<T><<<grid, kBlock, 0, s>>>(J, K.ts, n, K.ntiles)));
   enqueue_precond(0);
-  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (k_kr_ax<T, 1><<<grid, kBlock, ax_smem_bytes<T>(), s>>>(J, K.ts, n, K.ntiles, partial_)));
+  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (k_kr_ax<T, 1><<<grid, kAxBlock, ax_smem_bytes<T>(), s>>>(J, K.ts, n, K.ntiles, partial_)));
   k_efin<<<n, 256, 0, s>>>(K.ts, partial_, 1, 0, EFIN_ALPHA, scal_, nullptr);
   IMPACT_PROF(prof::K_R_UPDATE, 3 * fb, s, (k_kr_r<T><<<grid, kBlock, 0, s>>>(J, K.ts, n, K.ntiles)));
   enqueue_precond(1);
-  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (k_kr_ax<T, 2><<<grid, kBlock, ax_smem_bytes<T>(), s>>>(J, K.ts, n, K.ntiles, partial_)));
+  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (k_kr_ax<T, 2><<<grid, kAxBlock, ax_smem_bytes<T>(), s>>>(J, K.ts, n, K.ntiles, partial_)));
   k_efin<<<n, 256, 0, s>>>(K.ts, partial_, 2, 0, EFIN_OMEGA, scal_, nullptr);
   IMPACT_PROF(prof::K_X_UPDATE, 8 * fb, s, (k_kr_x<T><<<grid, kBlock, 0, s>>>(J, K.ts, n, K.ntiles, partial_)));
   k_efin<<<n, 256, 0, s>>>(K.ts, partial_, 3, 1, EFIN_NORMS, scal_, nullptr);
@@ -2074,7 +2135,7 @@ int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::
   const KrylovJob<T>* J = static_cast<const KrylovJob<T>*>(K.jobs);
   const int grid = grid_for(K.ntiles);
   if (!zero_phi) {
-    k_kr_ax<T, 0><<<grid, kBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_);
+    k_kr_ax<T, 0><<<grid, kAxBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_);
     prof::count(1);
   }
   k_kr_init<T><<<grid, kBlock, 0, s_>>>(J, K.ts, n, K.ntiles, zero_phi, partial_);
@@ -2168,7 +2229,7 @@ int Engine<T>::apply_operator() {
   if (e != cudaSuccess) return impact_set_error(e, "engine scalars", __FILE__, __LINE__);
   const DevList& K = arena_.lists[kr_list_];
   const KrylovJob<T>* J = static_cast<const KrylovJob<T>*>(K.jobs);
-  k_kr_ax<T, 0><<<grid_for(K.ntiles), kBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_);
+  k_kr_ax<T, 0><<<grid_for(K.ntiles), kAxBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_);
   prof::count(1);
   e = cudaStreamSynchronize(s_);
   if (e != cudaSuccess) return impact_set_error(e, "engine operator", __FILE__, __LINE__);
@@ -2216,11 +2277,11 @@ int Engine<T>::bench(int kind, int iters, double* ms, double* bytes) {
     }
     case 5:
       by = 3 * sz * fc;
-      f = [&]() { k_kr_ax<T, 1><<<grid, kBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_); };
+      f = [&]() { k_kr_ax<T, 1><<<grid, kAxBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_); };
       break;
     case 6:
       by = 3 * sz * fc;
-      f = [&]() { k_kr_ax<T, 2><<<grid, kBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_); };
+      f = [&]() { k_kr_ax<T, 2><<<grid, kAxBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_); };
       break;
     case 7:
       by = 8 * sz * fc;
@@ -2393,7 +2454,7 @@ int MixedEngine::solve(const std::vector<SolverScalars>& outer, double inner_tol
     if (rc) return rc;
     // r = b - A x in FP64 (the reference operator), stored as the FP32 right-hand side of the
     // inner solve, with its norms
-    k_kr_ax<double, 3><<<grid, kBlock, ax_smem_bytes<double>(), s_>>>(AJ, AL.ts, n, AL.ntiles, partial_);
+    k_kr_ax<double, 3><<<grid, kAxBlock, ax_smem_bytes<double>(), s_>>>(AJ, AL.ts, n, AL.ntiles, partial_);
     k_efin<<<n, 256, 0, s_>>>(AL.ts, partial_, 3, 1, EFIN_RAW, nullptr, q_);
     prof::count(2);
     cudaError_t e = cudaMemcpyAsync(q_host_, q_, (size_t)n * 4 * sizeof(double), cudaMemcpyDeviceToHost, s_);
