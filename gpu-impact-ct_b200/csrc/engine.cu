@@ -1131,6 +1131,13 @@ __global__ void __launch_bounds__(ENT) k_lv_restrict(const LevelJob<T>* __restri
   }
 }
 
+// one linear-interpolation pass of the prolongation: m ? w0 a + w1 b : a, with every rounding
+// spelled out (the same bits in every prolongation kernel)
+template <typename T>
+__device__ __forceinline__ T pmix(bool m, T w0, T a, T w1, T b) {
+  return m ? fmaT(w1, b, mulT(w0, a)) : a;
+}
+
 // coarse indices bracketing fine index q (lo == hi for coincident points)
 __device__ __forceinline__ void bracket(int q, int r, int nc, int& lo, int& hi, bool& mid) {
   if (r == 1) {
@@ -1219,10 +1226,10 @@ __device__ __forceinline__ void prolong_cols(const LevelJob<T>& J, const Geom& g
     for (int v = 0; v < V; ++v) {
       T Z[4];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) Z[c] = mz ? wz0 * P0[v][c] + wz1 * P1[v][c] : P0[v][c];
-      const T Yl = my ? wy0 * Z[0] + wy1 * Z[1] : Z[0];  // x = xl
-      const T Yh = my ? wy0 * Z[2] + wy1 * Z[3] : Z[2];  // x = xh
-      f[v] = f[v] + (mx[v] ? wx0[v] * Yl + wx1[v] * Yh : Yl);
+      for (int c = 0; c < 4; ++c) Z[c] = pmix(mz, wz0, P0[v][c], wz1, P1[v][c]);
+      const T Yl = pmix(my, wy0, Z[0], wy1, Z[1]);  // x = xl
+      const T Yh = pmix(my, wy0, Z[2], wy1, Z[3]);  // x = xh
+      f[v] = f[v] + pmix(mx[v], wx0[v], Yl, wx1[v], Yh);
     }
     if constexpr (V > 1)
       vstore(dst + p, f);
@@ -1271,43 +1278,54 @@ __device__ __forceinline__ void prolong_cols_x2(const LevelJob<T>& J, const Geom
       w[m][1] = cz[oc[m][1]];
     }
   };
+  // blocks of U planes: the fine vectors of the block are loaded before any store, so that each
+  // thread keeps several DRAM requests in flight
+  constexpr int U = 4;
   long long p = off(g, i, j, k0);
-  for (int k = k0; k <= k1; ++k, p += g.nxy) {
-    int zl, zh;
-    bool mz;
-    bracket(k, J.rc[2], gc.n3, zl, zh, mz);
-    if (zl != zcur) {
-      const int nxt = zcur + 1 > gc.n3 ? 1 : zcur + 1;
-      if (zcur >= 0 && have1 && zl == nxt) {
+  for (int kb = k0; kb <= k1; kb += U, p += U * g.nxy) {
+    const int nk = min(U, k1 - kb + 1);
+    T f[U][V];
 #pragma unroll
-        for (int m = 0; m < NC; ++m) {
-          P0[m][0] = P1[m][0];
-          P0[m][1] = P1[m][1];
+    for (int u = 0; u < U; ++u)
+      if (u < nk) vload(fine + p + u * g.nxy, f[u]);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (u >= nk) continue;
+      const int k = kb + u;
+      int zl, zh;
+      bool mz;
+      bracket(k, J.rc[2], gc.n3, zl, zh, mz);
+      if (zl != zcur) {
+        const int nxt = zcur + 1 > gc.n3 ? 1 : zcur + 1;
+        if (zcur >= 0 && have1 && zl == nxt) {
+#pragma unroll
+          for (int m = 0; m < NC; ++m) {
+            P0[m][0] = P1[m][0];
+            P0[m][1] = P1[m][1];
+          }
+        } else {
+          load(zl, P0);
         }
-      } else {
-        load(zl, P0);
+        zcur = zl;
+        have1 = false;
       }
-      zcur = zl;
-      have1 = false;
-    }
-    if (mz && !have1) {
-      load(zh, P1);
-      have1 = true;
-    }
-    const T wz0 = cI3[2 * k], wz1 = cI3[2 * k + 1];
-    T Y[NC];
+      if (mz && !have1) {
+        load(zh, P1);
+        have1 = true;
+      }
+      const T wz0 = cI3[2 * k], wz1 = cI3[2 * k + 1];
+      T Y[NC];
 #pragma unroll
-    for (int m = 0; m < NC; ++m) {
-      const T Zl = mz ? wz0 * P0[m][0] + wz1 * P1[m][0] : P0[m][0];
-      const T Zh = mz ? wz0 * P0[m][1] + wz1 * P1[m][1] : P0[m][1];
-      Y[m] = my ? wy0 * Zl + wy1 * Zh : Zl;
-    }
-    T f[V];
-    vload(fine + p, f);
+      for (int m = 0; m < NC; ++m) {
+        const T Zl = pmix(mz, wz0, P0[m][0], wz1, P1[m][0]);
+        const T Zh = pmix(mz, wz0, P0[m][1], wz1, P1[m][1]);
+        Y[m] = pmix(my, wy0, Zl, wy1, Zh);
+      }
 #pragma unroll
-    for (int v = 0; v < V; ++v)  // even v: coincident with coarse column v/2; odd v: between two
-      f[v] = f[v] + ((v & 1) ? wx0[v] * Y[(v - 1) / 2] + wx1[v] * Y[(v + 1) / 2] : Y[v / 2]);
-    vstore(dst + p, f);
+      for (int v = 0; v < V; ++v)  // even v: coincident with coarse column v/2; odd v: between two
+        f[u][v] = f[u][v] + ((v & 1) ? pmix(true, wx0[v], Y[(v - 1) / 2], wx1[v], Y[(v + 1) / 2]) : Y[v / 2]);
+      vstore(dst + p + u * g.nxy, f[u]);
+    }
   }
 }
 
