@@ -2452,6 +2452,8 @@ int MixedEngine::solve(const std::vector<SolverScalars>& outer, double inner_tol
   }
   const DevList& AL = arena_.lists[ax_list_];
   const DevList& ML = arena_.lists[mix_list_];
+  double cells = 0.0;  // algorithmic bytes of both kernels: 20 per cell (x, b or e, r32 or x)
+  for (const auto& c : cs_) cells += (double)c.g.n1 * c.g.n2 * c.g.n3;
   const KrylovJob<double>* AJ = static_cast<const KrylovJob<double>*>(AL.jobs);
   const MixJob* MJ = static_cast<const MixJob*>(ML.jobs);
   const int grid = grid_for(ML.ntiles);
@@ -2472,9 +2474,10 @@ int MixedEngine::solve(const std::vector<SolverScalars>& outer, double inner_tol
     if (rc) return rc;
     // r = b - A x in FP64 (the reference operator), stored as the FP32 right-hand side of the
     // inner solve, with its norms
-    k_kr_ax<double, 3><<<grid, kAxBlock, ax_smem_bytes<double>(), s_>>>(AJ, AL.ts, n, AL.ntiles, partial_);
+    IMPACT_PROF(prof::K_MX_RESID, 20.0 * cells, s_,
+                (k_kr_ax<double, 3><<<grid, kAxBlock, ax_smem_bytes<double>(), s_>>>(AJ, AL.ts, n, AL.ntiles, partial_)));
     k_efin<<<n, 256, 0, s_>>>(AL.ts, partial_, 3, 1, EFIN_RAW, nullptr, q_);
-    prof::count(2);
+    prof::count(1);
     cudaError_t e = cudaMemcpyAsync(q_host_, q_, (size_t)n * 4 * sizeof(double), cudaMemcpyDeviceToHost, s_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s_);
     if (e != cudaSuccess) return impact_set_error(e, "mixed engine residual", __FILE__, __LINE__);
@@ -2548,8 +2551,7 @@ int MixedEngine::solve(const std::vector<SolverScalars>& outer, double inner_tol
     }
     rc = push_flags();
     if (rc) return rc;
-    k_mx_apply<<<grid, kBlock, 0, s_>>>(MJ, ML.ts, n, ML.ntiles, oscal_);
-    prof::count(1);
+    IMPACT_PROF(prof::K_MX_APPLY, 20.0 * cells, s_, (k_mx_apply<<<grid, kBlock, 0, s_>>>(MJ, ML.ts, n, ML.ntiles, oscal_)));
   }
   for (int c = 0; c < n; ++c) res[c].iterations = outer_it[c];
   return 0;

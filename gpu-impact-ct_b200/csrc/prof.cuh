@@ -24,6 +24,8 @@ enum Kid {
   K_MG_OTHER,      // restriction, prolongation, copies
   K_MG_PRE,        // fused init + sweeps + residual of one V-cycle level
   K_MG_POST,       // fused sweeps after the prolongation
+  K_MX_RESID,      // mixed precision: FP64 outer residual b - A x and its FP32 image
+  K_MX_APPLY,      // mixed precision: x += e in FP64
   K_COUNT
 };
 

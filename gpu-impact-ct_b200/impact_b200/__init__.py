@@ -368,7 +368,7 @@ class Batch:
         return lib().impact_b200_batch_stream(self._h)
 
 
-PROFILE_KERNELS = 15
+PROFILE_KERNELS = 17
 
 
 def profile(enable: bool = True, reset: bool = True):

@@ -20,7 +20,7 @@ def test_profiler_counts_graph_replays():
     prof = I.profile_read()
     I.profile(False)
     assert I.launch_count() > n0
-    for k in ("mg_sweep", "div_grad_dot", "x_update", "nl_rhs"):
+    for k in ("mg_sweep", "div_grad_dot", "x_update", "nl_rhs", "mx_residual", "mx_apply"):
         launches, ms, byts = prof[k]
         assert launches > 0 and ms > 0 and byts > 0, k
     I.profile(False, reset=True)
