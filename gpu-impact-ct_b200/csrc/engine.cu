@@ -1915,14 +1915,23 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
     for (auto& m : members) {
       jobs.push_back(lvjob(m.first, m.second, variant));
       if (!vec) jobs.back().vw = 1;
-      if (fusedS > 0) {
-        LevelJob<T>& Jm = jobs.back();
-        int kcm = KC_MAX;
-        while (kcm > 8 && tiles_multi(Jm.g, kcm, (int)sizeof(T), fusedS, mfast) < 2 * 148) kcm /= 2;
-        Jm.kc = kcm;
-      }
-      const LevelJob<T>& J = jobs.back();
-      tiles.push_back(fusedS > 0 ? tiles_multi(J.g, J.kc, (int)sizeof(T), fusedS, mfast) : tiles_of(J.g, kc, J.vw));
+    }
+    auto tiles_at_kc = [&](const LevelJob<T>& J, int kcj) {
+      return fusedS > 0 ? tiles_multi(J.g, kcj, (int)sizeof(T), fusedS, mfast) : tiles_of(J.g, kcj, J.vw);
+    };
+    // tile depth of the list: the engine's (the deepest for the fused kernels), halved while the
+    // list has fewer than two tiles per SM, so that the small coarse levels march short columns
+    // on many SMs instead of long ones on a few
+    int kcl = fusedS > 0 ? KC_MAX : kc;
+    for (;;) {
+      long long tot = 0;
+      for (const auto& J : jobs) tot += tiles_at_kc(J, kcl);
+      if (tot >= 2 * 148 || kcl <= 1) break;
+      kcl /= 2;
+    }
+    for (auto& J : jobs) {
+      J.kc = kcl;
+      tiles.push_back(tiles_at_kc(J, kcl));
       c += vol(J.g);
       if (J.Cf) f += vol(J.gf);
       if (J.Bc) cc += vol(J.gc);
