@@ -1,4 +1,5 @@
-"""Autotuner of the pressure solve: tile depth of the solver kernels and multigrid sweep schedule.
+"""Autotuner of the pressure solve: tile depth of the solver kernels, multigrid sweep schedule and,
+for mixed precision, the tolerance of each FP32 inner solve.
 
 The kernels of the Poisson engine cut every grid into tiles of 32 x 8 columns and `tile_kc`
 z-planes; deeper tiles stream longer columns (fewer tile start-ups), shallower ones give more
@@ -6,7 +7,9 @@ tiles to fill the 148 SMs on small grids and coarse levels.  The V-cycle's sweep
 the cost of one preconditioner application against the number of BiCGstab iterations.  Both are
 chosen here by timing complete Poisson solves of the case's own current right-hand side to the
 requested tolerance, one per candidate, on the device, and keeping the fastest candidate that
-converged.  Results are cached per (grid, precision, device) for the life of the process.
+converged.  In mixed precision a looser inner tolerance means cheaper inner solves and more FP64
+refinement passes; the best balance depends on the case, so it is one more tuned dimension.
+Results are cached per (grid, precision, device) for the life of the process.
 """
 from __future__ import annotations
 
@@ -17,33 +20,39 @@ from . import Case, SolverParams
 
 TILE_KC = (8, 16, 32, 64)
 SWEEPS = ((2, 2, 2), (3, 3, 3), (4, 4, 4))
+INNER_TOL = (1e-3, 3e-3, 1e-2)
 
 _cache: dict = {}
 
 
-def _with(base: SolverParams, kc: int, sw) -> SolverParams:
+def _with(base: SolverParams, kc: int, sw, itol=None) -> SolverParams:
     p = copy.copy(base)
     p.tile_kc = kc
     p.mg_down, p.mg_up, p.mg_bottom = sw
+    if itol is not None:
+        p.inner_tol_rel = itol
     return p
 
 
 def tune(case: Case, base: SolverParams, tile_kc=TILE_KC, sweeps=SWEEPS, rhs="res", scratch="rhs1",
-         repeats: int = 1, use_cache: bool = True):
+         repeats: int = 1, use_cache: bool = True, inner_tol=INNER_TOL):
     """Time Poisson solves A x = rhs (x from zero, written into `scratch`, which the next time step
     recomputes anyway) for every candidate and return (best SolverParams, report).  The case should
     hold a realistic right-hand side, e.g. after two time steps from rest (the first step of a
     flow at rest has a zero right-hand side; with one, nothing is tuned and `base` is returned).
-    Multigrid candidates only when base.precond == 1; otherwise only the tile depth is tuned."""
+    Multigrid candidates only when base.precond == 1; otherwise only the tile depth is tuned.
+    inner_tol: candidate inner tolerances of a mixed-precision case (ignored in FP64; () keeps
+    base.inner_tol_rel)."""
     key = (tuple(case.grid.N), case.precision, base.precond, base.tol_rel, base.omega)
     if use_cache and key in _cache:
         return _cache[key]
-    cands = [(kc, sw) for kc in tile_kc for sw in (sweeps if base.precond == 1 else [(base.mg_down, base.mg_up,
-                                                                                       base.mg_bottom)])]
+    sws = sweeps if base.precond == 1 else [(base.mg_down, base.mg_up, base.mg_bottom)]
+    itols = list(inner_tol) if (case.precision == 1 and inner_tol) else [None]
+    cands = [(kc, sw, it) for kc in tile_kc for sw in sws for it in itols]
     report = []
     best = None
-    for kc, sw in cands:
-        p = _with(base, kc, sw)
+    for kc, sw, it in cands:
+        p = _with(base, kc, sw, it)
         p.init_yes = 1
         r0 = case.poisson(rhs, scratch, p)  # builds the engine and its graphs
         if r0.b_two == 0.0:
@@ -55,14 +64,14 @@ def tune(case: Case, base: SolverParams, tile_kc=TILE_KC, sweeps=SWEEPS, rhs="re
             r = case.poisson(rhs, scratch, p)  # returns after the device has finished
         ms = 1e3 * (time.perf_counter() - t0) / repeats
         ok = r.status == 0
-        report.append({"tile_kc": kc, "sweeps": list(sw), "ms": round(ms, 3), "iterations": r.iterations,
-                       "inner_iterations": r.inner_iterations, "converged": ok})
+        report.append({"tile_kc": kc, "sweeps": list(sw), "inner_tol": it, "ms": round(ms, 3),
+                       "iterations": r.iterations, "inner_iterations": r.inner_iterations, "converged": ok})
         if ok and (best is None or ms < best[0]):
-            best = (ms, kc, sw)
+            best = (ms, kc, sw, it)
     if best is None:
         chosen = copy.copy(base)
     else:
-        chosen = _with(base, best[1], best[2])
+        chosen = _with(base, best[1], best[2], best[3])
     out = (chosen, report)
     if use_cache:
         _cache[key] = out

@@ -1,6 +1,7 @@
-"""The solver autotuner: every candidate (tile depth x multigrid sweep schedule) is timed on a
-complete Poisson solve of the case's own right-hand side, the fastest converged one is returned,
-and it leaves the case's state untouched (the next step equals a run without tuning)."""
+"""The solver autotuner: every candidate (tile depth x multigrid sweep schedule x, in mixed
+precision, inner tolerance) is timed on a complete Poisson solve of the case's own right-hand
+side, the fastest converged one is returned, and it leaves the case's state untouched (the next
+step equals a run without tuning)."""
 import numpy as np
 import pytest
 
@@ -25,11 +26,15 @@ def test_autotune_picks_a_converged_candidate(precision):
     ref.step(p, 3)
     c = _case(precision)
     c.step(p, 2)  # the first step from rest leaves a zero right-hand side
-    best, report = A.tune(c, p.poisson, tile_kc=(8, 32), sweeps=((2, 2, 2), (4, 4, 4)), use_cache=False)
-    assert len(report) == 4 and all(r["converged"] for r in report)
+    itols = (1e-3, 1e-2) if precision == 1 else ()  # inner tolerances: mixed precision only
+    best, report = A.tune(c, p.poisson, tile_kc=(8, 32), sweeps=((2, 2, 2), (4, 4, 4)), use_cache=False,
+                          inner_tol=itols)
+    assert len(report) == 4 * max(1, len(itols)) and all(r["converged"] for r in report)
     assert all(r["iterations"] > 0 for r in report)
     fastest = min(report, key=lambda r: r["ms"])
     assert (best.tile_kc, [best.mg_down, best.mg_up, best.mg_bottom]) == (fastest["tile_kc"], fastest["sweeps"])
+    if precision == 1:
+        assert best.inner_tol_rel == fastest["inner_tol"]
     # tuning only wrote the scratch field: the next step matches the untuned run
     c.step(p, 1)
     for f in ("vel1", "vel2", "vel3", "pre"):
