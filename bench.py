@@ -65,6 +65,8 @@ def parse():
                     help="V-cycle sweeps down / up / bottom of the batch and serve cases, and of the single case "
                          "with --no-tune (default: the autotuner's choice on the 384 case)")
     ap.add_argument("--tile-kc", type=int, default=64, help="tile depth of the solver kernels, as --sweeps")
+    ap.add_argument("--copy-chunks", type=int, default=8,
+                    help="element ranges per field of the end-to-end copies (download and next upload pipeline)")
     ap.add_argument("--no-profile", action="store_true", help="no per-kernel events in the timed steps (no roofline)")
     ap.add_argument("--cases", type=int, default=48, help="batch: number of cases")
     ap.add_argument("--requests", type=int, default=16, help="serve: number of requests")
@@ -220,23 +222,43 @@ def run_arm(args, precision, device, rank, world, dist, profile_on, e2e_on):
     launches0 = I.launch_count()
     sampler = ClockSampler(device) if rank == 0 and e2e_on else None
     t_dev, t_e2e, its, inner, stats = 0.0, 0.0, [], [], []
+    # every step uploads its inputs on a copy-in stream, runs on the case stream once they have
+    # landed, and downloads its results on a copy-out stream.  Each field moves in --copy-chunks element
+    # ranges, and the upload of a range for the next step waits only for the download of the same
+    # range, so the two copy directions run side by side, one range apart
+    up_s, dn_s = torch.cuda.Stream(device), torch.cuda.Stream(device)
+    ranges = [(f, a, j * a.size // args.copy_chunks,
+               (j + 1) * a.size // args.copy_chunks - j * a.size // args.copy_chunks)
+              for f, a in host.items() for j in range(args.copy_chunks)]
+    done = [None] * len(ranges)  # download of each host range enqueued last
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_start.record(up_s)
     for _ in range(args.steps):
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-        e[0].record(stream)
-        for f, a in host.items():
-            case.upload(f, a)
-        e[1].record(stream)
+        for i, (f, a, first, count) in enumerate(ranges):
+            if done[i] is not None:
+                up_s.wait_event(done[i])
+            case.upload_async(f, a, up_s.cuda_stream, first, count)
+        if host:
+            landed = torch.cuda.Event()
+            landed.record(up_s)
+            stream.wait_event(landed)
+        e1, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e1.record(stream)
         st = case.step(sp)
-        e[2].record(stream)
-        for f, a in host.items():
-            case.download(f, a)
-        e[3].record(stream)
-        e[3].synchronize()
-        t_dev += e[1].elapsed_time(e[2])
-        t_e2e += e[0].elapsed_time(e[3])
+        e2.record(stream)
+        dn_s.wait_event(e2)
+        for i, (f, a, first, count) in enumerate(ranges):
+            case.download_async(f, a, dn_s.cuda_stream, first, count)
+            done[i] = torch.cuda.Event()
+            done[i].record(dn_s)
+        e2.synchronize()
+        t_dev += e1.elapsed_time(e2)
         its.append(list(st.poisson_iterations))
         inner.append(list(st.inner_iterations))
         stats.append(list(st.poisson_status))
+    t_end.record(dn_s)
+    t_end.synchronize()
+    t_e2e = t_start.elapsed_time(t_end)
     torch.cuda.synchronize(device)
     launches = I.launch_count() - launches0
     clocks = sampler.stop() if sampler else None
@@ -488,6 +510,7 @@ def serve_bench(args, device, n_req, steps, budget_gb=160.0, rate=20.0):
     import numpy as np
     import torch
 
+    import impact_b200 as I
     from impact_b200 import geometry as G
     from impact_b200 import serve as S
     rng = np.random.default_rng(11)
@@ -503,11 +526,10 @@ def serve_bench(args, device, n_req, steps, budget_gb=160.0, rate=20.0):
         spec = {"n": n, "radius": radius, "stenoses": sten, "U0": float(rng.uniform(0.5, 1.5)),
                 "Re": float(rng.uniform(100, 800))}
 
-        def labels(g, seed=seed, radius=radius, sten=sten):
-            return G.curved_tube(g, np.random.default_rng(seed), radius, stenoses=sten)
-
-        reqs.append(S.Request(r, (n + 1, n + 1, 2 * n + 1), (1.0, 1.0, 2.0), labels, _case_params(spec, 1, args),
-                              steps, float(arrivals[r])))
+        # the client submits its label mask with the request: built here, before the stream starts
+        N = (n + 1, n + 1, 2 * n + 1)
+        labels = G.curved_tube(I.Grid(N, (1.0, 1.0, 2.0)), np.random.default_rng(seed), radius, stenoses=sten)
+        reqs.append(S.Request(r, N, (1.0, 1.0, 2.0), labels, _case_params(spec, 1, args), steps, float(arrivals[r])))
         cells += n * n * 2 * n
     srv = S.Server(int(budget_gb * 1e9), precision=1, device=device, keep=())
     t0 = time.perf_counter()
@@ -518,6 +540,7 @@ def serve_bench(args, device, n_req, steps, budget_gb=160.0, rate=20.0):
     stats.update({"workload": f"serving-{n_req}-requests", "arrival_rate_per_s": rate, "steps_per_case": steps,
                   "hbm_budget_gb": budget_gb, "peak_cases": srv.peak_cases, "peak_gb": round(srv.peak_bytes / 1e9, 2),
                   "batch_rebuilds": srv.batch_rebuilds, "rounds": srv.rounds,
+                  "host_seconds": {k: round(v, 3) for k, v in srv.seconds.items()},
                   "status_ok": all(all(x == 0 for x in d.status) for d in done),
                   "clock": "host wall clock of the request loop (latency = completion - arrival)"})
     return stats
@@ -597,7 +620,9 @@ def main():
             "config": dict(workload(args.size), parallelism=f"replicas x{world}" if world > 1 else "single GPU",
                            precision="mixed"),
             "e2e": {"value": round(e2e, 3), "unit": UNIT, "h2d_bytes_per_step": mixed["bytes_in"],
-                    "d2h_bytes_per_step": mixed["bytes_out"]},
+                    "d2h_bytes_per_step": mixed["bytes_out"], "ms_per_step": mixed["ms_e2e"] / K,
+                    "copies": f"pinned host, vel1-3 + pre, {args.copy_chunks} ranges per field each way on "
+                              "copy-in / copy-out streams"},
             "gpu_launches": mixed["launches"], "clocks": mixed["clocks"], "roofline": roof,
             "solver": {"mixed_outer_per_substep": mixed["iterations"], "mixed_inner_per_substep": mixed["inner_iterations"],
                        "status": mixed["status"], "dt": mixed["dt"], "autotune": mixed["tuning"]}}

@@ -617,6 +617,34 @@ extern "C" int impact_b200_case_download(impact_b200_case* c, int field, double*
   IMPACT_CUDA_CHECK(cudaStreamSynchronize(s.stream));
   return 0;
 }
+// the same copies enqueued on `stream` (the case stream when null) without waiting for them
+// Element range [first, first + count) of a field; `host` is the base of the whole host field.
+static int range_ok(const impact_b200_case* c, int field, const void* host, size_t first, size_t count) {
+  return c && host && field >= 0 && field < IMPACT_B200_NFIELDS && first <= (size_t)c->s.g.nfield &&
+         count <= (size_t)c->s.g.nfield - first;
+}
+extern "C" int impact_b200_case_upload_async(impact_b200_case* c, int field, const double* host, size_t first,
+                                             size_t count, void* stream) {
+  if (!range_ok(c, field, host, first, count))
+    return impact_set_error_msg(-1, "impact_b200_case_upload_async: bad arguments");
+  CaseState& s = c->s;
+  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s.stream;
+  if (count)
+    IMPACT_CUDA_CHECK(cudaMemcpyAsync(s.f[field] + first, host + first, count * sizeof(double), cudaMemcpyHostToDevice, st));
+  return 0;
+}
+extern "C" int impact_b200_case_download_async(impact_b200_case* c, int field, double* host, size_t first,
+                                               size_t count, void* stream) {
+  if (!range_ok(c, field, host, first, count))
+    return impact_set_error_msg(-1, "impact_b200_case_download_async: bad arguments");
+  CaseState& s = c->s;
+  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s.stream;
+  if (count)
+    IMPACT_CUDA_CHECK(cudaMemcpyAsync(host + first, s.f[field] + first, count * sizeof(double), cudaMemcpyDeviceToHost, st));
+  return 0;
+}
 extern "C" int impact_b200_case_set_labels(impact_b200_case* c, const uint8_t* host) {
   if (!c || !host) return impact_set_error_msg(-1, "impact_b200_case_set_labels: bad arguments");
   CaseState& s = c->s;

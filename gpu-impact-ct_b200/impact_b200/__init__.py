@@ -100,6 +100,8 @@ def lib():
         "impact_b200_case_bytes": (C.c_longlong, [i, i, i, i]),
         "impact_b200_case_upload": (i, [_vp, i, _dp]),
         "impact_b200_case_download": (i, [_vp, i, _dp]),
+        "impact_b200_case_upload_async": (i, [_vp, i, _dp, C.c_size_t, C.c_size_t, _vp]),
+        "impact_b200_case_download_async": (i, [_vp, i, _dp, C.c_size_t, C.c_size_t, _vp]),
         "impact_b200_case_set_labels": (i, [_vp, _u8p]),
         "impact_b200_case_field_ptr": (_vp, [_vp, i]),
         "impact_b200_case_stream": (_vp, [_vp]),
@@ -272,6 +274,32 @@ class Case:
         out = self.grid.zeros() if out is None else out
         check(lib().impact_b200_case_download(self._h, f, _ptr(out)), "case_download")
         return out
+
+    def _range(self, what, a, first, count):
+        if not (a.flags["C_CONTIGUOUS"] and a.dtype == np.float64 and a.shape == self.grid.shape):
+            raise ValueError(what + ": host array must be C-contiguous float64 of the grid's shape")
+        count = a.size - first if count is None else count
+        if first < 0 or count < 0 or first + count > a.size:
+            raise ValueError(what + ": element range outside the field")
+        return first, count
+
+    def upload_async(self, field, host: np.ndarray, stream: int = 0, first: int = 0, count: int | None = None):
+        """Enqueue the copy of elements [first, first + count) (default: all) of `host` (C-contiguous
+        float64 of the grid's shape, pinned for overlap) into the field on the CUDA stream handle
+        `stream` (0: the case stream) and return at once; that range of `host` must stay alive and
+        unchanged until the copy has completed."""
+        f = FIELDS[field] if isinstance(field, str) else field
+        first, count = self._range("upload_async", host, first, count)
+        check(lib().impact_b200_case_upload_async(self._h, f, _ptr(host), first, count, C.c_void_p(stream or None)),
+              "case_upload_async")
+
+    def download_async(self, field, out: np.ndarray, stream: int = 0, first: int = 0, count: int | None = None):
+        """Enqueue the copy of the field's elements [first, first + count) into `out` (as
+        upload_async) and return at once."""
+        f = FIELDS[field] if isinstance(field, str) else field
+        first, count = self._range("download_async", out, first, count)
+        check(lib().impact_b200_case_download_async(self._h, f, _ptr(out), first, count, C.c_void_p(stream or None)),
+              "case_download_async")
 
     def set_labels(self, labels: np.ndarray):
         lb = np.ascontiguousarray(labels, dtype=np.uint8)

@@ -69,6 +69,9 @@ class Server:
         self.batch_rebuilds = 0
         self.peak_bytes = 0
         self.peak_cases = 0
+        # host seconds spent per activity of the loop (admission: case allocation + labels;
+        # build: batch construction; step: batched time steps; finish: download + free)
+        self.seconds = {"admit": 0.0, "build": 0.0, "step": 0.0, "finish": 0.0}
 
     def run(self, requests, clock=time.perf_counter, sleep=time.sleep):
         pending = sorted(requests, key=lambda r: r.arrival)
@@ -90,11 +93,13 @@ class Server:
                 r = waiting[q]
                 need = case_bytes(r.N, self.precision)
                 if used + need <= self.budget:
+                    ta = clock()
                     g = Grid(r.N, r.L, r.kinds)
                     c = Case(g, precision=self.precision, device=self.device)
                     lab = r.labels(g) if callable(r.labels) else r.labels
                     c.set_labels(lab)
                     active.append({"req": r, "case": c, "bytes": need, "steps": 0, "admitted": clock() - t0})
+                    self.seconds["admit"] += clock() - ta
                     used += need
                     waiting.pop(q)
                     changed = True
@@ -111,13 +116,18 @@ class Server:
                     sleep(max(0.0, pending[0].arrival - (clock() - t0)))
                 continue
             if changed or batch is None:
+                tb = clock()
                 if batch is not None:
                     batch.close()
                 batch = Batch([a["case"] for a in active])
                 self.batch_rebuilds += 1
                 changed = False
+                self.seconds["build"] += clock() - tb
+            ts = clock()
             batch.step([a["req"].params for a in active], 1)
             self.rounds += 1
+            tf = clock()
+            self.seconds["step"] += tf - ts
             keep_active = []
             for a in active:
                 a["steps"] += 1
@@ -139,6 +149,7 @@ class Server:
                     if a not in keep_active:
                         a["case"].close()
             active = keep_active
+            self.seconds["finish"] += clock() - tf
         if batch is not None:
             batch.close()
         return done

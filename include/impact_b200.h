@@ -156,6 +156,17 @@ long long impact_b200_case_bytes(int N1, int N2, int N3, int precision);
 /* whole padded field (nx*ny*nz doubles, reference layout) host <-> device, on the case stream */
 int impact_b200_case_upload(impact_b200_case* c, int field, const double* host);
 int impact_b200_case_download(impact_b200_case* c, int field, double* host);
+/* Elements [first, first + count) of the field (linear index of the padded layout; `host` is the
+ * base of the whole host field) copied on `stream` (a cudaStream_t; NULL: the case stream), the
+ * call returning at once: with pinned host memory the copies overlap other copies and kernels, and
+ * ranges of one field let its download and the next upload pipeline against each other.  Ordering
+ * against the case stream (its time steps) is the caller's, by events; the host range must stay
+ * untouched until the copy has completed.  No counterpart in the reference (its wrappers copy
+ * whole fields synchronously). */
+int impact_b200_case_upload_async(impact_b200_case* c, int field, const double* host, size_t first, size_t count,
+                                  void* stream);
+int impact_b200_case_download_async(impact_b200_case* c, int field, double* host, size_t first, size_t count,
+                                    void* stream);
 /* voxel labels (padded layout, one byte per point): 0 solid, 1 fluid, 5 inflow, 7 wall, 9/11 outlets */
 int impact_b200_case_set_labels(impact_b200_case* c, const uint8_t* host_labels);
 double* impact_b200_case_field_ptr(impact_b200_case* c, int field);
