@@ -2,7 +2,7 @@
 // damped-Jacobi sweeps) as preconditioner, every kernel over a job list of cases / levels.
 //
 //   BiCGstab_orig           mod_solvers.f90:1509-1935   k_kr_* and the scalar finalisation
-//   product_div_grad        mod_laplace.f90:38-197      k_kr_ax (collapsed 11-point form, z-march)
+//   product_div_grad        mod_laplace.f90:38-197      k_kr_ax / k_kr_ax32 (collapsed 11-point form, z-march)
 //   multigridV              mod_solvers.f90:456-585     schedule built in Engine::build
 //   relaxation_div_grad     mod_laplace.f90:339-613     k_lv_smooth
 //   product_div_grad_relax  mod_laplace.f90:216-327     k_lv_resid (fused with the subtraction)
@@ -502,6 +502,7 @@ __device__ __forceinline__ void cp_wait() {
 //   MODE 2: Ar = A z2, partials Ar.rr, Ar.Ar (omega)
 //   MODE 3: FP64 only: r32 = (float)(bb - A phi), partials max|r|, sum r^2, sum bb^2 (the outer
 //           residual of the mixed-precision solve and the right-hand side of its inner solve)
+// The FP32 lists run k_kr_ax32 below (same operator and operation order per point).
 constexpr int AXTY = ETY / 2, AXNT = ETX * AXTY;  // 32 x 4 threads, two rows each
 constexpr int AX_TW = ETX + 10, AX_TH = ETY + 10, AX_TE = AX_TW * AX_TH;
 constexpr int AX_PER = (AX_TE + AXNT - 1) / AXNT;  // staged elements per thread and plane
@@ -733,6 +734,291 @@ __device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf
 __device__ __forceinline__ double fmaT(double a, double b, double c) { return __fma_rn(a, b, c); }
 __device__ __forceinline__ float mulT(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double mulT(double a, double b) { return __dmul_rn(a, b); }
+// ------------------------------------------------------------------------------------------
+// The FP32 operator of the Krylov list (the inner solve of the mixed-precision Poisson solve):
+// the same collapsed 11-point product_div_grad and the same operation order per point as
+// k_kr_ax, with the plane ring staged in 16-byte chunks and the z march taken AXB planes at a
+// time.
+//
+// Staged plane: AXA_H = 18 rows (y halo 5) of AXA_W = 48 columns whose first column is the
+// 16-byte aligned element 8 left of the tile (the 5-wide x halo rounded out to whole chunks).
+// Each thread stages up to AXA_PER chunks of a plane; a chunk is one 16-byte cp.async when its
+// needed elements are interior points of the row and the field's rows are 16-byte aligned
+// (nx a multiple of 4), else its needed elements one by one from their periodic images.
+// Chunks no point of the tile reads are not staged.
+//
+// z march: the ring holds AXA_R = AXB * AXA_G planes in AXA_G groups of AXB planes, one
+// cp.async group each.  A step outputs planes t .. t+AXB-1 of the tile; it needs planes up to
+// t+AXB+4 in the ring, waits for them with one barrier, refills the group freed by the previous
+// step, adds planes t+5 .. t+AXB+4 to the register windows (z values k-5 .. k+AXB+4 of the two
+// points of the thread) and moves the windows on by AXB after the step, so a window value is
+// moved once per AXB planes.  The inner-product partner of the step's points is loaded from
+// global memory one step ahead.
+constexpr int AXB = 4;                                     // planes per step
+constexpr int AXA_G = 5;                                   // groups of AXB planes in the ring
+constexpr int AXA_R = AXB * AXA_G;                         // ring slots
+constexpr int AXA_V = 4;                                   // floats per 16-byte chunk
+constexpr int AXA_HX = 8;                                  // staged columns left of the tile
+constexpr int AXA_W = 48;                                  // staged row: 8 + 32 + 5, whole chunks
+constexpr int AXA_H = ETY + 10;                            // staged rows
+constexpr int AXA_CR = AXA_W / AXA_V;                      // chunks per row
+constexpr int AXA_NCH = AXA_CR * AXA_H;                    // chunks per plane
+constexpr int AXA_PER = (AXA_NCH + AXNT - 1) / AXNT;       // chunks per thread and plane
+constexpr int AXA_PLANE = AXA_W * AXA_H;                   // floats per slot
+constexpr int AXA_ZW = AXB + 10;                           // z window per point
+static_assert((AXA_PLANE * 4) % 16 == 0, "slots must keep 16-byte alignment");
+static_assert(AXB >= 1 && AXB <= 5, "group bookkeeping below assumes 4 / AXB <= 4");
+constexpr int AXA_NEED = 1 + 4 / AXB;                      // groups beyond the step's own that it reads
+constexpr int AXA_WAIT = AXA_G - 2 - AXA_NEED;             // groups left in flight at the wait
+static_assert(AXA_WAIT >= 0, "ring too shallow for the step");
+
+constexpr size_t axa_smem_bytes() {
+  return sizeof(float) * ((size_t)AXA_R * AXA_PLANE + (size_t)KC_MAX * AXW + ETY * AXW + AXW * ETX);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(AXNT, 3) k_kr_ax32(const KrylovJob<float>* __restrict__ jobs,
+                                                     const int* __restrict__ ts, int nj, int ntiles,
+                                                     double* __restrict__ partial) {
+  static_assert(MODE >= 0 && MODE <= 2, "FP32 operator modes: 0 residual, 1 alpha, 2 omega");
+  extern __shared__ __align__(16) unsigned char ax_smem[];
+  float* ring = reinterpret_cast<float*>(ax_smem);
+  float(*wzs)[AXW] = reinterpret_cast<float(*)[AXW]>(ax_smem + sizeof(float) * AXA_R * AXA_PLANE);
+  float(*wys)[AXW] = reinterpret_cast<float(*)[AXW]>(ax_smem + sizeof(float) * (AXA_R * AXA_PLANE + KC_MAX * AXW));
+  float(*wxs)[ETX] =
+      reinterpret_cast<float(*)[ETX]>(ax_smem + sizeof(float) * (AXA_R * AXA_PLANE + KC_MAX * AXW + ETY * AXW));
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + ETX * ty;
+  const int ya = 2 * ty;
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const KrylovJob<float>& J = jobs[q];
+    const SolverScalars* sc = J.sc;
+    if (MODE == 0 ? (sc->done != 0) : e_halted(sc)) continue;
+    const Geom g = J.g;
+    const int ntx = (g.n1 + ETX - 1) / ETX, nty = (g.n2 + ETY - 1) / ETY;
+    const int t0 = b - ts[q];
+    const int ta = t0 % ntx, tr = t0 / ntx, tc = tr / nty;
+    const int i0 = ta * ETX + 1, j0 = (tr - tc * nty) * ETY + 1;
+    const int k0 = tc * J.kc + 1, k1 = min(g.n3, k0 + J.kc - 1);
+    const int nk = k1 - k0 + 1;
+    const int i = i0 + tx;
+    const bool in0 = i <= g.n1 && j0 + ya <= g.n2, in1 = i <= g.n1 && j0 + ya + 1 <= g.n2;
+    const float* __restrict__ x = MODE == 0 ? J.phi : (MODE == 1 ? J.z1 : J.z2);
+    float* __restrict__ out = MODE == 0 ? J.rr : (MODE == 1 ? J.Ap : J.Ar);
+    const float* __restrict__ d1 = MODE == 1 ? J.rh : J.rr;
+    const long long nxy = g.nxy;
+    const int nzw = nk * AXW;
+    for (int t = tid; t < nzw; t += AXNT) wzs[t / AXW][t % AXW] = J.W[2][(k0 - 1) * AXW + t];
+    for (int t = tid; t < ETY * AXW; t += AXNT) {
+      const int jj = j0 + t / AXW;
+      wys[t / AXW][t % AXW] = jj <= g.n2 ? J.W[1][(jj - 1) * AXW + t % AXW] : 0.f;
+    }
+    for (int t = tid; t < ETX * AXW; t += AXNT) {
+      const int ii = i0 + t / AXW;
+      wxs[t % AXW][t / AXW] = ii <= g.n1 ? J.W[0][(ii - 1) * AXW + t % AXW] : 0.f;
+    }
+    // this thread's chunks: in-plane source offsets (go[e][0] alone for a 16-byte chunk, one per
+    // element otherwise, -1 where nothing is staged); columns and rows that a point of the tile
+    // reads: i0-5 .. min(i0+31, n1)+5 and j0-5 .. min(j0+7, n2)+5
+    const int ilast = min(i0 + ETX - 1, g.n1) + 5, jlast = min(j0 + ETY - 1, g.n2) + 5;
+    const bool rows16 = (g.nx & (AXA_V - 1)) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+    int go[AXA_PER][AXA_V];
+    unsigned vec = 0;
+#pragma unroll
+    for (int e = 0; e < AXA_PER; ++e) {
+      const int cq = tid + e * AXNT;
+      const int r = cq / AXA_CR, c0 = (cq % AXA_CR) * AXA_V;
+      const int jj = j0 - 5 + r;
+      const bool row_ok = cq < AXA_NCH && jj <= jlast;
+      const int rowoff = g.nx * (wrapi(row_ok ? jj : 1, g.n2) + 3);
+      bool v16 = row_ok && rows16, any = false;
+#pragma unroll
+      for (int v = 0; v < AXA_V; ++v) {
+        const int ii = i0 - AXA_HX + c0 + v;
+        const bool need = row_ok && ii >= i0 - 5 && ii <= ilast;
+        any |= need;
+        if (need && (ii < 1 || ii > g.n1)) v16 = false;
+        if (ii < -3 || ii > g.n1 + 4) v16 = false;  // the chunk must lie inside the padded row
+        go[e][v] = need ? (wrapi(ii, g.n1) + 3) + rowoff : -1;
+      }
+      if (v16 && any) {
+        go[e][0] = (i0 - AXA_HX + c0 + 3) + rowoff;
+        vec |= 1u << e;
+      }
+    }
+    const int own0 = (in0 ? i + 3 : 4) + g.nx * ((in0 ? j0 + ya : 1) + 3);
+    const int own1 = (in1 ? i + 3 : 4) + g.nx * ((in1 ? j0 + ya + 1 : 1) + 3);
+    auto zoff = [&](int k) -> long long {
+      return (long long)((k < 1 ? k + g.n3 : (k > g.n3 ? k - g.n3 : k)) + 3) * nxy;
+    };
+    // group gi: planes t = gi*AXB .. gi*AXB+AXB-1 of the tile (t < nk + 5) into their slots
+    auto stage_group = [&](int gi) {
+#pragma unroll
+      for (int u = 0; u < AXB; ++u) {
+        const int t = gi * AXB + u;
+        if (t < nk + 5) {
+          const float* src = x + zoff(k0 + t);
+          float* dst = ring + (size_t)(t % AXA_R) * AXA_PLANE + tid * AXA_V;
+#pragma unroll
+          for (int e = 0; e < AXA_PER; ++e) {
+            float* d = dst + e * AXNT * AXA_V;
+            if ((vec >> e) & 1u) {
+              cp_async16(d, src + go[e][0]);
+            } else {
+#pragma unroll
+              for (int v = 0; v < AXA_V; ++v)
+                if (go[e][v] >= 0) cp_async1(d + v, src + go[e][v]);
+            }
+          }
+        }
+      }
+      cp_commit();
+    };
+    __syncthreads();  // weights visible; the ring is free
+    const bool zu = J.zuni != 0;
+    float wx[AXW], wya[AXW], wyb[AXW], wzr[AXW];
+#pragma unroll
+    for (int l = 0; l < AXW; ++l) {
+      wx[l] = wxs[l][tx];
+      wya[l] = wys[ya][l];
+      wyb[l] = wys[ya + 1][l];
+      wzr[l] = wzs[0][l];
+    }
+    float za[AXA_ZW], zb[AXA_ZW];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+      za[l] = x[zoff(k0 - 5 + l) + own0];
+      zb[l] = x[zoff(k0 - 5 + l) + own1];
+    }
+#pragma unroll
+    for (int l = 5; l < AXA_ZW; ++l) za[l] = zb[l] = 0.f;
+#pragma unroll
+    for (int gi = 0; gi < AXA_G - 1; ++gi) stage_group(gi);
+    // partners of the first step
+    float pa[AXB], pb[AXB];
+#pragma unroll
+    for (int u = 0; u < AXB; ++u) {
+      pa[u] = pb[u] = 0.f;
+      if (MODE != 0 && u < nk) {
+        if (in0) pa[u] = d1[zoff(k0 + u) + own0];
+        if (in1) pb[u] = d1[zoff(k0 + u) + own1];
+      }
+    }
+    double v0 = 0.0, v1 = 0.0;
+    float* o0 = out + (long long)(k0 + 3) * nxy + own0;
+    float* o1 = out + (long long)(k0 + 3) * nxy + own1;
+    const int cx = tx + AXA_HX;  // the thread's column in the staged plane
+    auto walk = [&](auto zreg) {
+      constexpr bool ZR = decltype(zreg)::value;
+      const int nsteps = (nk + AXB - 1) / AXB;
+      for (int s = 0; s < nsteps; ++s) {
+        const int tb = s * AXB;
+        cp_wait<AXA_WAIT>();  // this thread's copies of planes up to tb+AXB+4 have landed
+        __syncthreads();      // everybody's have; the previous step's group is free
+        stage_group(s + AXA_G - 1);
+        // partners of the next step
+        float na[AXB], nb[AXB];
+#pragma unroll
+        for (int u = 0; u < AXB; ++u) {
+          na[u] = nb[u] = 0.f;
+          if (MODE != 0 && tb + AXB + u < nk) {
+            const long long zo = zoff(k0 + tb + AXB + u);
+            if (in0) na[u] = d1[zo + own0];
+            if (in1) nb[u] = d1[zo + own1];
+          }
+        }
+        if (s == 0) {  // window planes 0 .. 4 of the tile
+#pragma unroll
+          for (int l = 0; l < 5; ++l) {
+            za[5 + l] = ring[(size_t)l * AXA_PLANE + (ya + 5) * AXA_W + cx];
+            zb[5 + l] = ring[(size_t)l * AXA_PLANE + (ya + 6) * AXA_W + cx];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < AXB; ++u) {  // window planes tb+5 .. tb+AXB+4
+          const float* sp = ring + (size_t)((tb + 5 + u) % AXA_R) * AXA_PLANE;
+          za[10 + u] = sp[(ya + 5) * AXA_W + cx];
+          zb[10 + u] = sp[(ya + 6) * AXA_W + cx];
+        }
+#pragma unroll
+        for (int u = 0; u < AXB; ++u) {
+          const int t = tb + u;
+          if (t < nk) {
+            const float(*sp)[AXA_W] = reinterpret_cast<const float(*)[AXA_W]>(ring + (size_t)(t % AXA_R) * AXA_PLANE);
+            const float ca = za[5 + u], cb = zb[5 + u];
+            float axa = mulT(wx[0], sp[ya + 5][cx - 5]), axb = mulT(wx[0], sp[ya + 6][cx - 5]);
+#pragma unroll
+            for (int l = 1; l < AXW; ++l) {
+              axa = fmaT(wx[l], l == 5 ? ca : sp[ya + 5][cx - 5 + l], axa);
+              axb = fmaT(wx[l], l == 5 ? cb : sp[ya + 6][cx - 5 + l], axb);
+            }
+            float yv[AXW + 1];
+#pragma unroll
+            for (int r = 0; r < AXW + 1; ++r) yv[r] = r == 5 ? ca : (r == 6 ? cb : sp[ya + r][cx]);
+            float aya = mulT(wya[0], yv[0]), ayb = mulT(wyb[0], yv[1]);
+#pragma unroll
+            for (int l = 1; l < AXW; ++l) {
+              aya = fmaT(wya[l], yv[l], aya);
+              ayb = fmaT(wyb[l], yv[l + 1], ayb);
+            }
+            const float* wz = wzs[t];
+            float aza = mulT(ZR ? wzr[0] : wz[0], za[u]), azb = mulT(ZR ? wzr[0] : wz[0], zb[u]);
+#pragma unroll
+            for (int l = 1; l < AXW; ++l) {
+              aza = fmaT(ZR ? wzr[l] : wz[l], za[u + l], aza);
+              azb = fmaT(ZR ? wzr[l] : wz[l], zb[u + l], azb);
+            }
+            const float ra = __fadd_rn(__fadd_rn(axa, aya), aza), rb = __fadd_rn(__fadd_rn(axb, ayb), azb);
+            if (in0) *o0 = ra;
+            if (in1) *o1 = rb;
+            if (MODE == 1) {
+              if (in0) v0 += (double)ra * (double)pa[u];
+              if (in1) v0 += (double)rb * (double)pb[u];
+            }
+            if (MODE == 2) {
+              if (in0) {
+                v0 += (double)ra * (double)pa[u];
+                v1 += (double)ra * (double)ra;
+              }
+              if (in1) {
+                v0 += (double)rb * (double)pb[u];
+                v1 += (double)rb * (double)rb;
+              }
+            }
+            o0 += nxy;
+            o1 += nxy;
+          }
+        }
+#pragma unroll
+        for (int l = 0; l < 10; ++l) {
+          za[l] = za[l + AXB];
+          zb[l] = zb[l + AXB];
+        }
+#pragma unroll
+        for (int u = 0; u < AXB; ++u) {
+          pa[u] = na[u];
+          pb[u] = nb[u];
+        }
+      }
+    };
+    if (zu)
+      walk(std::true_type{});
+    else
+      walk(std::false_type{});
+    cp_wait<0>();
+    if (MODE == 1) {
+      double v[1] = {v0};
+      tile_partials<1, 0, AXNT>(v, partial + (long long)b * 4);
+    } else if (MODE == 2) {
+      double v[2] = {v0, v1};
+      tile_partials<2, 0, AXNT>(v, partial + (long long)b * 4);
+    } else {
+      __syncthreads();  // the ring and the weights are rewritten by the next tile
+    }
+  }
+}
+
 // bv - a0 w - a2 e - b0 s - b2 n - cm zm - cp zp
 template <typename T>
 __device__ __forceinline__ T jres(T bv, T a0, T w, T a2, T e, T b0, T s, T b2, T n, T cm, T zm, T cp, T zp) {
@@ -1626,13 +1912,13 @@ void ax_attributes() {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64 || done[dev]) return;
-  cudaFuncSetAttribute(k_kr_ax<float, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<float>());
-  cudaFuncSetAttribute(k_kr_ax<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<float>());
-  cudaFuncSetAttribute(k_kr_ax<float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<float>());
   cudaFuncSetAttribute(k_kr_ax<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
   cudaFuncSetAttribute(k_kr_ax<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
   cudaFuncSetAttribute(k_kr_ax<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
   cudaFuncSetAttribute(k_kr_ax<double, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ax_smem_bytes<double>());
+  cudaFuncSetAttribute(k_kr_ax32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axa_smem_bytes());
+  cudaFuncSetAttribute(k_kr_ax32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axa_smem_bytes());
+  cudaFuncSetAttribute(k_kr_ax32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axa_smem_bytes());
 #define IMPACT_MULTI_ATTR(T, N, I, R)                                                                           \
   cudaFuncSetAttribute(k_lv_multi<T, N, I, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,               \
                        (int)multi_smem_bytes<T, N, I, R>());                                                    \
@@ -1663,6 +1949,14 @@ inline int grid_for(int ntiles) {
 }
 const dim3 kBlock(ETX, ETY);
 const dim3 kAxBlock(ETX, AXTY);  // k_kr_ax: two rows per thread
+// the operator over a Krylov list: FP32 by the 16-byte staged, stepped kernel
+template <typename T, int MODE>
+void launch_ax(int grid, const KrylovJob<T>* J, const int* ts, int n, int ntiles, double* partial, cudaStream_t s) {
+  if constexpr (std::is_same<T, float>::value && MODE <= 2)
+    k_kr_ax32<MODE><<<grid, kAxBlock, axa_smem_bytes(), s>>>(J, ts, n, ntiles, partial);
+  else
+    k_kr_ax<T, MODE><<<grid, kAxBlock, ax_smem_bytes<T>(), s>>>(J, ts, n, ntiles, partial);
+}
 // the fused smoothing kernel runs one block per tile (one block per SM at a time)
 inline int grid_multi(int ntiles) { return ntiles; }
 
@@ -2118,11 +2412,11 @@ void Engine<T>::enqueue_iteration() {
   prof::count(1);
   IMPACT_PROF(prof::K_P_UPDATE, 4 * fb, s, (k_kr_p<T><<<grid, kBlock, 0, s>>>(J, K.ts, n, K.ntiles)));
   enqueue_precond(0);
-  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (k_kr_ax<T, 1><<<grid, kAxBlock, ax_smem_bytes<T>(), s>>>(J, K.ts, n, K.ntiles, partial_)));
+  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (launch_ax<T, 1>(grid, J, K.ts, n, K.ntiles, partial_, s)));
   k_efin<<<n, 256, 0, s>>>(K.ts, partial_, 1, 0, EFIN_ALPHA, scal_, nullptr);
   IMPACT_PROF(prof::K_R_UPDATE, 3 * fb, s, (k_kr_r<T><<<grid, kBlock, 0, s>>>(J, K.ts, n, K.ntiles)));
   enqueue_precond(1);
-  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (k_kr_ax<T, 2><<<grid, kAxBlock, ax_smem_bytes<T>(), s>>>(J, K.ts, n, K.ntiles, partial_)));
+  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (launch_ax<T, 2>(grid, J, K.ts, n, K.ntiles, partial_, s)));
   k_efin<<<n, 256, 0, s>>>(K.ts, partial_, 2, 0, EFIN_OMEGA, scal_, nullptr);
   IMPACT_PROF(prof::K_X_UPDATE, 8 * fb, s, (k_kr_x<T><<<grid, kBlock, 0, s>>>(J, K.ts, n, K.ntiles, partial_)));
   k_efin<<<n, 256, 0, s>>>(K.ts, partial_, 3, 1, EFIN_NORMS, scal_, nullptr);
@@ -2162,7 +2456,7 @@ int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::
   const KrylovJob<T>* J = static_cast<const KrylovJob<T>*>(K.jobs);
   const int grid = grid_for(K.ntiles);
   if (!zero_phi) {
-    k_kr_ax<T, 0><<<grid, kAxBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_);
+    launch_ax<T, 0>(grid, J, K.ts, n, K.ntiles, partial_, s_);
     prof::count(1);
   }
   k_kr_init<T><<<grid, kBlock, 0, s_>>>(J, K.ts, n, K.ntiles, zero_phi, partial_);
@@ -2256,7 +2550,7 @@ int Engine<T>::apply_operator() {
   if (e != cudaSuccess) return impact_set_error(e, "engine scalars", __FILE__, __LINE__);
   const DevList& K = arena_.lists[kr_list_];
   const KrylovJob<T>* J = static_cast<const KrylovJob<T>*>(K.jobs);
-  k_kr_ax<T, 0><<<grid_for(K.ntiles), kAxBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_);
+  launch_ax<T, 0>(grid_for(K.ntiles), J, K.ts, n, K.ntiles, partial_, s_);
   prof::count(1);
   e = cudaStreamSynchronize(s_);
   if (e != cudaSuccess) return impact_set_error(e, "engine operator", __FILE__, __LINE__);
@@ -2304,11 +2598,11 @@ int Engine<T>::bench(int kind, int iters, double* ms, double* bytes) {
     }
     case 5:
       by = 3 * sz * fc;
-      f = [&]() { k_kr_ax<T, 1><<<grid, kAxBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_); };
+      f = [&]() { launch_ax<T, 1>(grid, J, K.ts, n, K.ntiles, partial_, s_); };
       break;
     case 6:
       by = 3 * sz * fc;
-      f = [&]() { k_kr_ax<T, 2><<<grid, kAxBlock, ax_smem_bytes<T>(), s_>>>(J, K.ts, n, K.ntiles, partial_); };
+      f = [&]() { launch_ax<T, 2>(grid, J, K.ts, n, K.ntiles, partial_, s_); };
       break;
     case 7:
       by = 8 * sz * fc;

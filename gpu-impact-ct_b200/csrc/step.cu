@@ -8,6 +8,7 @@
 //                                        rhs.cu)
 //   explicit         -> divergence2 of rhs, Poisson solve, k_project (vel = rhs - G pre, 3 comps)
 // Every pass keeps the reference's order of floating-point operations per point.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -226,6 +227,15 @@ __global__ void __launch_bounds__(1024) k_reduce_partials(const double* __restri
 }
 
 // sum of pre over the unique points, block partials (level_pressure, mod_lib.f90:507-537)
+// FP64 -> FP32 and back, whole padded fields
+__global__ void k_narrow(const double* __restrict__ a, float* __restrict__ b, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    b[q] = (float)a[q];
+}
+__global__ void k_widen(const float* __restrict__ a, double* __restrict__ b, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    b[q] = (double)a[q];
+}
 __global__ void __launch_bounds__(NT) k_sum(Geom g, const double* __restrict__ a, double* __restrict__ partial) {
   const int i = blockIdx.x * BX + threadIdx.x + 1;
   const int j = blockIdx.y * BY + threadIdx.y + 1;
@@ -865,7 +875,7 @@ extern "C" int impact_b200_case_precond(impact_b200_case* c, int field_in, int f
 
 extern "C" int impact_b200_case_apply(impact_b200_case* c, int op, int field_in, int field_out) {
   if (!c || field_in < 0 || field_out < 0 || field_in >= IMPACT_B200_NFIELDS || field_out >= IMPACT_B200_NFIELDS ||
-      field_in == field_out || op < 0 || op > 1)
+      field_in == field_out || op < 0 || op > 2)
     return impact_set_error_msg(-1, "impact_b200_case_apply: bad arguments");
   CaseState& s = c->s;
   IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
@@ -883,6 +893,39 @@ extern "C" int impact_b200_case_apply(impact_b200_case* c, int op, int field_in,
   p.omega = 0.8;
   EngineParams ep = engine_params(s, &p);
   ep.use_graph = 0;
+  if (op == 2) {  // field_out = A field_in in FP32 (the operator of the mixed solve's inner solve)
+    const long long nf = s.g.nfield;
+    float* buf = nullptr;  // input, output, unused Krylov slots
+    IMPACT_CUDA_CHECK(cudaMalloc((void**)&buf, 3 * nf * sizeof(float)));
+    const int nb = (int)std::min<long long>((nf + 255) / 256, 148LL * 32);
+    k_narrow<<<nb, 256, 0, s.stream>>>(s.f[field_in], buf, nf);
+    EngineCase<float> ef{};
+    ef.g = s.g;
+    for (int m = 0; m < 3; ++m) {
+      ef.W[m] = s.W32[m];
+      ef.cdg[m] = s.c32.cdg[m];
+    }
+    ef.zuni = s.zuni;
+    ef.cdg_zuni = s.cdg_zuni;
+    ef.mg = nullptr;
+    ef.bb = ef.phi = buf;
+    ef.rr = buf + nf;
+    ef.rh = ef.pp = ef.Ap = ef.Ar = ef.z1 = ef.z2 = ef.comp = buf + 2 * nf;
+    int rc = 0;
+    {
+      Engine<float> e;
+      rc = e.build({ef}, ep, s.stream);
+      if (!rc) rc = e.apply_operator();
+    }
+    if (!rc) {
+      k_widen<<<nb, 256, 0, s.stream>>>(buf + nf, s.f[field_out], nf);
+      prof::count(2);
+      cudaError_t ce = cudaStreamSynchronize(s.stream);
+      if (ce != cudaSuccess) rc = impact_set_error(ce, "impact_b200_case_apply", __FILE__, __LINE__);
+    }
+    cudaFree(buf);
+    return rc;
+  }
   EngineCase<double> ec{};
   ec.g = s.g;
   for (int m = 0; m < 3; ++m) {

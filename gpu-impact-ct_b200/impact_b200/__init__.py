@@ -341,7 +341,8 @@ class Case:
         return ms.value, by.value
 
     def apply(self, field_in="pre", field_out="res", op: int = 0):
-        """op 0: field_out = A field_in (product_div_grad); op 1: field_out = div(velocity)"""
+        """op 0: field_out = A field_in (product_div_grad); op 1: field_out = div(velocity);
+        op 2: op 0 through the FP32 operator of the mixed solve"""
         fi = FIELDS[field_in] if isinstance(field_in, str) else field_in
         fo = FIELDS[field_out] if isinstance(field_out, str) else field_out
         check(lib().impact_b200_case_apply(self._h, op, fi, fo), "case_apply")

@@ -209,7 +209,9 @@ int impact_b200_case_poisson(impact_b200_case* c, int field_b, int field_x, cons
 int impact_b200_case_precond(impact_b200_case* c, int field_in, int field_out, const impact_b200_solver_params* p);
 /* op 0: field_out = A field_in, product_div_grad (mod_laplace.f90:38-197), the operator of the
  * pressure Poisson solve; op 1: field_out = divergence2 of the resident velocity (mod_diff.f90:
- * 130-215; field_in unused).  FP64, on the resident fields. */
+ * 130-215; field_in unused).  FP64, on the resident fields.  op 2: op 0 in FP32 (field_in
+ * rounded to FP32, the FP32 weights and kernel of the mixed solve's inner iteration, the result
+ * widened to FP64). */
 int impact_b200_case_apply(impact_b200_case* c, int op, int field_in, int field_out);
 /* levels of the multigrid hierarchy of the case (0 when it has none) */
 int impact_b200_case_mg_levels(impact_b200_case* c);
