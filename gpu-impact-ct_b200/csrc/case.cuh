@@ -56,6 +56,7 @@ struct CaseState {
   const double* eng_b = nullptr;
   double* eng_x = nullptr;
   std::vector<void*> allocs;
+  bool pooled = false;  // allocs come from the per-device case pool (freed stream-ordered)
 };
 
 }  // namespace impact

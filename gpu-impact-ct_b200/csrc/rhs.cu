@@ -14,8 +14,9 @@
 // halo of the interpolation along axis m) is staged into a ring of R shared-memory slots by
 // cp.async, R-4 planes ahead of its use.  The x and y neighbours come from the ring, the z
 // values of the column from register windows: vel_m at k-3..k+3 and, for m = 3, work_a at
-// k-2..k+3.  x coefficient rows (one per thread column) are staged once per block, transposed;
-// y rows are warp-uniform and z rows block-uniform, read through the read-only cache.
+// k-2..k+3.  x coefficient rows (one per thread column) are staged once per block, transposed,
+// the y rows of the block's 8 rows once per block (warp-uniform reads), and the z rows of every
+// staged plane into its ring slot with the plane (block-uniform reads).
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -28,6 +29,10 @@ constexpr int RTX = 32, RTY = 8, RNT = RTX * RTY;
 constexpr int RR = 7;                                 // ring slots: planes c .. c+3 resident, 3 in flight
 constexpr int VW = RTX + 6, VH = RTY + 6, VE = VW * VH;  // vel tile with the 3-wide halo
 constexpr int NXR = 27;                               // x coefficient rows: U 7, D 7, D2 7, I 6
+// y / z coefficient row in shared memory: U at 0, D at 8, D2 at 16, I at 24 (7, 7, 7, 6 values),
+// every group 16-byte aligned so that uniform reads take two values per load
+constexpr int NCR = 32;
+constexpr int CU = 0, CD = 8, CH = 16, CI = 24;
 
 template <int M>
 struct WTile {  // work tile of one field: halo -2..3 along axis M only
@@ -36,15 +41,32 @@ struct WTile {  // work tile of one field: halo -2..3 along axis M only
   static constexpr int E = W * H;
 };
 template <int M>
-constexpr int slot_elems() { return VE + 3 * WTile<M>::E; }
+constexpr int slot_elems() { return VE + 3 * WTile<M>::E + NCR; }  // vel tile, work tiles, z row
+static_assert(VE % 2 == 0 && (3 * WTile<0>::E) % 2 == 0 && (3 * WTile<1>::E) % 2 == 0 && (3 * WTile<2>::E) % 2 == 0 &&
+                  (NXR * RTX) % 2 == 0,
+              "z rows and y rows must stay 16-byte aligned");
 template <int M>
-constexpr size_t rhs_smem_bytes() { return sizeof(double) * ((size_t)RR * slot_elems<M>() + (size_t)NXR * RTX); }
+constexpr size_t rhs_smem_bytes() {
+  return sizeof(double) * ((size_t)RR * slot_elems<M>() + (size_t)NXR * RTX + (size_t)RTY * NCR);
+}
 
 // periodic image of index i in 1..n, for any integer i
 __device__ __forceinline__ int wrapg(int i, int n) {
   int r = (i - 1) % n;
   if (r < 0) r += n;
   return r + 1;
+}
+
+// N consecutive doubles from 16-byte aligned shared memory, two per load
+template <int N>
+__device__ __forceinline__ void ld_row(const double* p, double (&o)[N]) {
+#pragma unroll
+  for (int l = 0; l + 1 < N; l += 2) {
+    const double2 v = *reinterpret_cast<const double2*>(p + l);
+    o[l] = v.x;
+    o[l + 1] = v.y;
+  }
+  if (N & 1) o[N - 1] = p[N - 1];
 }
 
 __device__ __forceinline__ void cpa8(double* smem, const double* gmem) {
@@ -66,15 +88,21 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
   constexpr int VPER = (VE + RNT - 1) / RNT;
   constexpr int WPER = (3 * WT::E + RNT - 1) / RNT;
   extern __shared__ __align__(16) double rsm[];
-  double* ring = rsm;                      // RR slots of SE doubles: vel tile, then work tiles 0..2
+  double* ring = rsm;                      // RR slots of SE doubles: vel tile, work tiles 0..2, z row
   double* sx = rsm + (size_t)RR * SE;      // NXR x RTX transposed x rows
+  double* sy = sx + NXR * RTX;             // RTY x NCR y rows of the block's rows
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + RTX * ty;
   const int i0 = blockIdx.x * RTX + 1, j0 = blockIdx.y * RTY + 1;
   const int k0 = blockIdx.z * kz + 1;
   const int k1 = min(k0 + kz - 1, g.n3);
   const int i = i0 + tx, j = j0 + ty;
   const bool in = i <= g.n1 && j <= g.n2;
-  const int jr = wrapg(j, g.n2);  // y coefficient row (valid for idle threads too)
+  const double* yU = M == 1 ? c.cNuU[1] : c.cNpU[1];
+  const double* yD = M == 1 ? c.cNuD[1] : c.cNpD[1];
+  const double* yH = M == 1 ? c.cuu[1] : c.cpp[1];
+  const double* zU = M == 2 ? c.cNuU[2] : c.cNpU[2];
+  const double* zD = M == 2 ? c.cNuD[2] : c.cNpD[2];
+  const double* zH = M == 2 ? c.cuu[2] : c.cpp[2];
 
   // x rows of this block's columns, transposed: sx[l][tx]
   {
@@ -90,6 +118,17 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
       else if (l < 21) v = xH[row * NB + (l - 14)];
       else v = M == 0 ? c.cIpu[0][row * NG + (l - 21)] : 0.0;
       sx[t] = v;
+    }
+    // y rows of the block's rows
+    for (int t = tid; t < RTY * NCR; t += RNT) {
+      const int r = t / NCR, e = t % NCR, grp = e / 8, l = e % 8;
+      const int row = wrapg(j0 + r, g.n2);
+      double v = 0.0;
+      if (grp == 0 && l < 7) v = yU[row * NB + l];
+      else if (grp == 1 && l < 7) v = yD[row * NB + l];
+      else if (grp == 2 && l < 7) v = yH[row * NB + l];
+      else if (grp == 3 && l < 6 && M == 1) v = c.cIpu[1][row * NG + l];
+      sy[t] = v;
     }
   }
   // in-plane source offsets of this thread's staged elements (periodic images)
@@ -113,7 +152,13 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
     wdst[e] = VE + t;
   }
   const int nq = (k1 - k0 + 1) + 6;  // planes k0-3 .. k1+3
-  auto zoff = [&](int q) -> long long { return (long long)(wrapg(k0 - 3 + q, g.n3) + 3) * g.nxy; };
+  auto zwrap = [&](int q) { const int kk = k0 - 3 + q; return kk < 1 ? kk + g.n3 : (kk > g.n3 ? kk - g.n3 : kk); };
+  auto zoff = [&](int q) -> long long { return (long long)(zwrap(q) + 3) * g.nxy; };
+  // z row of a staged plane: thread e < NCR copies element e of the row layout
+  const int zg = tid / 8, zl = tid % 8;
+  const bool zcopy = tid < NCR && (zg < 3 ? zl < 7 : (zl < 6 && M == 2));
+  const double* zsrc = zg == 0 ? zU + zl : (zg == 1 ? zD + zl : (zg == 2 ? zH + zl : c.cIpu[2] + zl));
+  const int zstride = zg < 3 ? NB : NG;
   auto stage = [&](int q) {
     if (q < nq) {
       double* slot = ring + (size_t)(q % RR) * SE;
@@ -124,6 +169,7 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
 #pragma unroll
       for (int e = 0; e < WPER; ++e)
         if (wsrc[e]) cpa8(slot + wdst[e], wsrc[e] + zo);
+      if (zcopy) cpa8(slot + (SE - NCR) + tid, zsrc + zwrap(q) * zstride);
     }
     cpa_commit();
   };
@@ -139,13 +185,9 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
 #pragma unroll
     for (int l = 0; l < 6; ++l) wq[a][l] = 0.0;
 
-  const double* yU = M == 1 ? c.cNuU[1] : c.cNpU[1];
-  const double* yD = M == 1 ? c.cNuD[1] : c.cNpD[1];
-  const double* yH = M == 1 ? c.cuu[1] : c.cpp[1];
-  const double* zU = M == 2 ? c.cNuU[2] : c.cNpU[2];
-  const double* zD = M == 2 ? c.cNuD[2] : c.cNpD[2];
-  const double* zH = M == 2 ? c.cuu[2] : c.cpp[2];
   const int own = (tx + 3) + VW * (ty + 3);
+  const double* cy = sy + ty * NCR;  // this thread's y row (warp-uniform)
+  long long p = off(g, i, j, k0);    // output point of plane k (advanced per plane)
 
   for (int t = 0; t < nq; ++t) {
     cpa_wait<RR - 5>();   // this thread's copies of plane t have landed
@@ -163,10 +205,11 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
         wq[a][5] = slot[VE + a * WT::E + tid];
       }
     }
-    if (t < 6 || !in) continue;
-    const int k = k0 + t - 6;
-    const double* cs = ring + (size_t)((t - 3) % RR) * SE;  // plane k
-    const long long p = off(g, i, j, k);
+    if (t < 6) continue;
+    if (t > 6) p += g.nxy;
+    if (!in) continue;
+    const double* cs = ring + (size_t)((t - 3) % RR) * SE;  // plane k = k0 + t - 6
+    const double* cz = cs + (SE - NCR);                     // its z row (block-uniform)
     const double nlo = use_old ? nl[p] : 0.0;
     // vel_m neighbours along x and y (plane k), z (register window)
     double xv[7], yv[7];
@@ -175,6 +218,14 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
       xv[l] = cs[(ty + 3) * VW + tx + l];
       yv[l] = cs[(ty + l) * VW + tx + 3];
     }
+    // interpolation weights along axis m, shared by the three work fields
+    double ci[6];
+    if (M == 0) {
+#pragma unroll
+      for (int l = 0; l < 6; ++l) ci[l] = sx[(21 + l) * RTX + tx];
+    } else {
+      ld_row((M == 1 ? cy : cz) + CI, ci);
+    }
     double acc = 0.0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -182,20 +233,18 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
       double pp;
       if (M == 0) {
         const double* w = cs + VE + a * WT::E + ty * WT::W + tx;
-        pp = sx[21 * RTX + tx] * w[0];
+        pp = ci[0] * w[0];
 #pragma unroll
-        for (int l = 1; l < 6; ++l) pp = pp + sx[(21 + l) * RTX + tx] * w[l];
+        for (int l = 1; l < 6; ++l) pp = pp + ci[l] * w[l];
       } else if (M == 1) {
         const double* w = cs + VE + a * WT::E + ty * WT::W + tx;
-        const double* cr = c.cIpu[1] + jr * NG;
-        pp = __ldg(cr) * w[0];
+        pp = ci[0] * w[0];
 #pragma unroll
-        for (int l = 1; l < 6; ++l) pp = pp + __ldg(cr + l) * w[l * WT::W];
+        for (int l = 1; l < 6; ++l) pp = pp + ci[l] * w[l * WT::W];
       } else {
-        const double* cr = c.cIpu[2] + k * NG;
-        pp = __ldg(cr) * wq[a][0];
+        pp = ci[0] * wq[a][0];
 #pragma unroll
-        for (int l = 1; l < 6; ++l) pp = pp + __ldg(cr + l) * wq[a][l];
+        for (int l = 1; l < 6; ++l) pp = pp + ci[l] * wq[a][l];
       }
       double dd;
       if (a == 0) {
@@ -204,15 +253,17 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
 #pragma unroll
         for (int l = 1; l < 7; ++l) dd = dd + cr[l * RTX] * xv[l];
       } else if (a == 1) {
-        const double* cr = (pp >= 0.0 ? yU : yD) + jr * NB;
-        dd = __ldg(cr) * yv[0];
+        double cr[7];
+        ld_row(cy + (pp >= 0.0 ? CU : CD), cr);
+        dd = cr[0] * yv[0];
 #pragma unroll
-        for (int l = 1; l < 7; ++l) dd = dd + __ldg(cr + l) * yv[l];
+        for (int l = 1; l < 7; ++l) dd = dd + cr[l] * yv[l];
       } else {
-        const double* cr = (pp >= 0.0 ? zU : zD) + k * NB;
-        dd = __ldg(cr) * vq[0];
+        double cr[7];
+        ld_row(cz + (pp >= 0.0 ? CU : CD), cr);
+        dd = cr[0] * vq[0];
 #pragma unroll
-        for (int l = 1; l < 7; ++l) dd = dd + __ldg(cr + l) * vq[l];
+        for (int l = 1; l < 7; ++l) dd = dd + cr[l] * vq[l];
       }
       acc = (a == 0) ? dd * pp : acc + dd * pp;
     }
@@ -221,14 +272,13 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
 #pragma unroll
     for (int l = 1; l < 7; ++l) lap = lap + sx[(14 + l) * RTX + tx] * xv[l];
     {
-      const double* cr = yH + jr * NB;
+      double ch[7];
+      ld_row(cy + CH, ch);
 #pragma unroll
-      for (int l = 0; l < 7; ++l) lap = lap + __ldg(cr + l) * yv[l];
-    }
-    {
-      const double* cr = zH + k * NB;
+      for (int l = 0; l < 7; ++l) lap = lap + ch[l] * yv[l];
+      ld_row(cz + CH, ch);
 #pragma unroll
-      for (int l = 0; l < 7; ++l) lap = lap + __ldg(cr + l) * vq[l];
+      for (int l = 0; l < 7; ++l) lap = lap + ch[l] * vq[l];
     }
     const double nln = acc - multL * lap;
     double r = vq[3];

@@ -316,10 +316,34 @@ extern "C" long long impact_b200_case_bytes(int N1, int N2, int N3, int precisio
   return b;
 }
 
+// Case memory comes from one stream-ordered pool per device that keeps what cases free (release
+// threshold: never), so that a serving loop which creates and destroys cases reuses device
+// memory without cudaMalloc / cudaFree and the device-wide synchronisation they can cause.
+static cudaMemPool_t case_pool(int dev) {
+  static cudaMemPool_t pools[64] = {};
+  if (dev < 0 || dev >= 64) return nullptr;
+  if (!pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    unsigned long long keep = ~0ULL;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = pool;
+  }
+  return pools[dev];
+}
+
 static int case_alloc(CaseState& s, void** p, size_t bytes) {
-  cudaError_t e = cudaMalloc(p, bytes);
+  cudaMemPool_t pool = case_pool(s.device);
+  cudaError_t e = pool ? cudaMallocFromPoolAsync(p, bytes, pool, s.stream) : cudaMalloc(p, bytes);
+  // usable by any stream and by the synchronous copies of case creation from here on
+  if (e == cudaSuccess && pool) e = cudaStreamSynchronize(s.stream);
   if (e != cudaSuccess) return impact_set_error(e, "cudaMalloc (case)", __FILE__, __LINE__);
   s.allocs.push_back(*p);
+  s.pooled = pool != nullptr;
   return 0;
 }
 
@@ -332,7 +356,12 @@ extern "C" int impact_b200_case_destroy(impact_b200_case* c) {
   delete s.emx;
   s.e64 = nullptr;
   s.emx = nullptr;
-  for (void* p : s.allocs) cudaFree(p);
+  if (s.pooled) {
+    for (void* p : s.allocs) cudaFreeAsync(p, s.stream);
+    cudaStreamSynchronize(s.stream);
+  } else {
+    for (void* p : s.allocs) cudaFree(p);
+  }
   if (s.hscal) cudaFreeHost(s.hscal);
   if (s.scal_host) cudaFreeHost(s.scal_host);
   if (s.mw.scal64_host) cudaFreeHost(s.mw.scal64_host);
