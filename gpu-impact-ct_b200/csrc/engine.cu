@@ -283,24 +283,38 @@ __global__ void __launch_bounds__(ENT) k_kr_init(const KrylovJob<T>* __restrict_
       T* __restrict__ phi = J.phi;
       T* __restrict__ rr = J.rr;
       T* __restrict__ rh = J.rh;
+      const long long nxy = g.nxy;
       long long p = off(g, i, j, k0);
-      for (int k = k0; k <= k1; ++k, p += g.nxy) {
-        const T bv = bb[p];
+      auto point = [&](long long q, T bv, T a) {
         T r;
         if (zero_phi) {
-          phi[p] = T(0);
+          phi[q] = T(0);
           r = bv;
         } else {
-          r = bv - rr[p];
+          r = bv - a;
         }
-        rr[p] = r;
-        rh[p] = r;
+        rr[q] = r;
+        rh[q] = r;
         const double rd = (double)r, bd = (double)bv;
         v[0] = fmax(v[0], fabs(rd));
         v[1] += rd * rd;
         v[2] += rd * rd;
         v[3] += bd * bd;
+      };
+      // blocks of U planes: all loads of a block are issued before its stores
+      constexpr int U = 2 * Ublk<T>::U;
+      int k = k0;
+      for (; k + U - 1 <= k1; k += U, p += U * nxy) {
+        T bv[U], a[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          bv[u] = bb[p + u * nxy];
+          a[u] = zero_phi ? T(0) : rr[p + u * nxy];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) point(p + u * nxy, bv[u], a[u]);
       }
+      for (; k <= k1; ++k, p += nxy) point(p, bb[p], zero_phi ? T(0) : rr[p]);
     }
     tile_partials<4, 1>(v, partial + (long long)b * 4);
   }
