@@ -1580,10 +1580,43 @@ __device__ __forceinline__ void prolong_cols_x2(const LevelJob<T>& J, const Geom
   };
   // blocks of U planes: the fine vectors of the block are loaded before any store, so that each
   // thread keeps several DRAM requests in flight
-  constexpr int U = 4;
+  constexpr int U = 8;
   long long p = off(g, i, j, k0);
   for (int kb = k0; kb <= k1; kb += U, p += U * g.nxy) {
     const int nk = min(U, k1 - kb + 1);
+    if (sizeof(T) == 4 && nk == U && J.rc[2] == 2 && (kb & 1)) {
+      // FP32, a full block starting on a coincident plane: fine planes kb .. kb+U-1 lie on coarse
+      // planes c .. c+U/2 (c = (kb+1)/2, periodic); all of them are loaded with the fine vectors
+      // before any use, so the coarse loads no longer wait on one another (in FP64 the extra
+      // registers cost more than the overlap gains)
+      T f[U][V], Q[U / 2 + 1][NC][2];
+#pragma unroll
+      for (int u = 0; u < U; ++u) vload(fine + p + u * g.nxy, f[u]);
+      const int c = (kb + 1) / 2;
+#pragma unroll
+      for (int m = 0; m <= U / 2; ++m) load(c + m > gc.n3 ? c + m - gc.n3 : c + m, Q[m]);
+      zcur = -1;  // the plane-by-plane path below reloads what it needs
+      have1 = false;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = kb + u;
+        const bool mz = (u & 1) != 0;  // even fine plane: between coarse planes lo and lo + 1
+        const int lo = u / 2;
+        const T wz0 = cI3[2 * k], wz1 = cI3[2 * k + 1];
+        T Y[NC];
+#pragma unroll
+        for (int m = 0; m < NC; ++m) {
+          const T Zl = pmix(mz, wz0, Q[lo][m][0], wz1, Q[lo + 1 <= U / 2 ? lo + 1 : lo][m][0]);
+          const T Zh = pmix(mz, wz0, Q[lo][m][1], wz1, Q[lo + 1 <= U / 2 ? lo + 1 : lo][m][1]);
+          Y[m] = pmix(my, wy0, Zl, wy1, Zh);
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          f[u][v] = f[u][v] + ((v & 1) ? pmix(true, wx0[v], Y[(v - 1) / 2], wx1[v], Y[(v + 1) / 2]) : Y[v / 2]);
+        vstore(dst + p + u * g.nxy, f[u]);
+      }
+      continue;
+    }
     T f[U][V];
 #pragma unroll
     for (int u = 0; u < U; ++u)
@@ -2231,11 +2264,28 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
     // list has fewer than two tiles per SM, so that the small coarse levels march short columns
     // on many SMs instead of long ones on a few
     int kcl = fusedS > 0 ? KC_MAX : kc;
-    for (;;) {
+    auto total_at = [&](int kcj) {
       long long tot = 0;
-      for (const auto& J : jobs) tot += tiles_at_kc(J, kcl);
-      if (tot >= 2 * 148 || kcl <= 1) break;
-      kcl /= 2;
+      for (const auto& J : jobs) tot += tiles_at_kc(J, kcj);
+      return tot;
+    };
+    if (fusedS > 0) {
+      // the fused kernel runs one block per SM and marches kc + 2S planes per tile (plus a few
+      // planes' worth of set-up): pick the depth with the fewest waves x planes per tile
+      int nsm = 0, dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      if (nsm <= 0) nsm = 148;
+      double best = 0.0;
+      for (int kcj = KC_MAX; kcj >= 1; --kcj) {
+        const double cost = (double)((total_at(kcj) + nsm - 1) / nsm) * (kcj + 2 * fusedS + 4);
+        if (kcj == KC_MAX || cost < best) {
+          best = cost;
+          kcl = kcj;
+        }
+      }
+    } else {
+      while (total_at(kcl) < 2 * 148 && kcl > 1) kcl /= 2;
     }
     for (auto& J : jobs) {
       J.kc = kcl;

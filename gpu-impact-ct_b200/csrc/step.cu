@@ -864,7 +864,6 @@ extern "C" int impact_b200_case_precond(impact_b200_case* c, int field_in, int f
       field_in == field_out)
     return impact_set_error_msg(-1, "impact_b200_case_precond: bad arguments");
   CaseState& s = c->s;
-  if (s.precision != 0) return impact_set_error_msg(-1, "impact_b200_case_precond: FP64 cases only");
   IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
   if (p->precond == 1 && s.mg_levels == 0)
     return impact_set_error_msg(-1, "impact_b200_case_precond: case has no multigrid hierarchy");
@@ -873,6 +872,45 @@ extern "C" int impact_b200_case_precond(impact_b200_case* c, int field_in, int f
   // one application of the preconditioner: field_out = M field_in
   EngineParams ep = engine_params(s, p);
   ep.use_graph = 0;
+  if (s.precision == 1) {  // the FP32 preconditioner of the mixed solve's inner iteration
+    const long long nf = s.g.nfield;
+    float* buf = nullptr;  // input, output
+    IMPACT_CUDA_CHECK(cudaMalloc((void**)&buf, 2 * nf * sizeof(float)));
+    const int nb = (int)std::min<long long>((nf + 255) / 256, 148LL * 32);
+    k_narrow<<<nb, 256, 0, s.stream>>>(s.f[field_in], buf, nf);
+    EngineCase<float> ef{};
+    ef.g = s.g;
+    for (int m = 0; m < 3; ++m) {
+      ef.W[m] = s.W32[m];
+      ef.cdg[m] = s.c32.cdg[m];
+    }
+    ef.zuni = s.zuni;
+    ef.cdg_zuni = s.cdg_zuni;
+    ef.mg = s.mg_levels ? &s.mg32 : nullptr;
+    const KrylovWork<float>& w = s.mw.inner;
+    ef.bb = ef.pp = buf;
+    ef.phi = ef.Ar = w.Ar;
+    ef.rr = w.rr;
+    ef.rh = w.rh;
+    ef.Ap = w.Ap;
+    ef.z1 = buf + nf;
+    ef.z2 = w.z2;
+    ef.comp = w.comp;
+    int rc = 0;
+    {
+      Engine<float> e;
+      rc = e.build({ef}, ep, s.stream);
+      if (!rc) rc = e.apply_precond();
+    }
+    if (!rc) {
+      k_widen<<<nb, 256, 0, s.stream>>>(buf + nf, s.f[field_out], nf);
+      prof::count(2);
+      cudaError_t ce = cudaStreamSynchronize(s.stream);
+      if (ce != cudaSuccess) rc = impact_set_error(ce, "impact_b200_case_precond", __FILE__, __LINE__);
+    }
+    cudaFree(buf);
+    return rc;
+  }
   EngineCase<double> ec{};
   ec.g = s.g;
   for (int m = 0; m < 3; ++m) {

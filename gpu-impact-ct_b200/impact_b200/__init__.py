@@ -326,7 +326,8 @@ class Case:
         return lib().impact_b200_case_mg_levels(self._h)
 
     def precond(self, field_in="res", field_out="pre", params: SolverParams | None = None):
-        """field_out = M field_in with the preconditioner of params (FP64 cases)."""
+        """field_out = M field_in with the preconditioner of params (mixed-precision cases: the FP32
+        preconditioner of the inner solve, on the input rounded to FP32)."""
         params = solver_params() if params is None else params
         fi = FIELDS[field_in] if isinstance(field_in, str) else field_in
         fo = FIELDS[field_out] if isinstance(field_out, str) else field_out

@@ -205,7 +205,9 @@ typedef struct {
 int impact_b200_case_poisson(impact_b200_case* c, int field_b, int field_x, const impact_b200_solver_params* p,
                              impact_b200_solver_result* r);
 
-/* Apply the preconditioner of p once: field_out = M field_in (FP64 cases). */
+/* Apply the preconditioner of p once: field_out = M field_in.  FP64 cases: the FP64
+ * preconditioner; mixed-precision cases: the FP32 preconditioner of the inner solve (field_in
+ * rounded to FP32, the result widened to FP64). */
 int impact_b200_case_precond(impact_b200_case* c, int field_in, int field_out, const impact_b200_solver_params* p);
 /* op 0: field_out = A field_in, product_div_grad (mod_laplace.f90:38-197), the operator of the
  * pressure Poisson solve; op 1: field_out = divergence2 of the resident velocity (mod_diff.f90:

@@ -81,3 +81,25 @@ def test_product_div_grad_matches_oracle(N, L, kinds):
     got = case.download("res")
     scale = np.abs(og.interior(want)).max()
     assert np.abs(og.interior(got) - og.interior(want)).max() <= 1e-12 * scale
+
+
+# Grids deep enough that the tile depth of the finest level stays at 16 planes, so that the
+# prolongation runs whole blocks of 8 fine planes (in FP32 with every coarse plane of the block
+# loaded up front); the second one is stretched in z (per-plane interpolation weights).
+DEEP = [((257, 129, 257), (2.0, 1.0, 2.0), (0, 0, 0)), ((257, 129, 193), (2.0, 1.0, 1.5), (0, 0, 1))]
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-5)], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("N,L,kinds", DEEP, ids=["256x128x256", "256x128x192-z"])
+def test_vcycle_deep_tiles_matches_oracle(N, L, kinds, precision, tol):
+    og, ig = O.Grid(N, L, kinds), I.Grid(N, L, kinds)
+    mg = og.multigrid()
+    b = og.random(7)
+    want = mg.vcycle(b.copy(), og.zeros(), 3, 3, 3, 0.8)
+    case = I.Case(ig, precision=precision)
+    case.upload("res", b)
+    case.precond("res", "pre", I.solver_params(precond=1, omega=0.8, mg_down=3, mg_up=3, mg_bottom=3))
+    got = og.interior(case.download("pre"))
+    w = og.interior(want)
+    assert np.abs(got - w).max() <= tol * np.abs(w).max()
+    case.close()
