@@ -1401,6 +1401,22 @@ __global__ void __launch_bounds__(ENT) k_lv_resid(const LevelJob<T>* __restrict_
 }
 
 // this (coarse) level: A(ii,jj,kk) = (1.5 d(c) + sum over the six fine neighbours of 1/4 d) / 3
+// the restriction of the fine residual to one coarse point (restrict, mod_solvers.f90:588-808):
+// weights 1/4, 2/4, 1/4 per axis, the centre's three halves summed first, every rounding spelled
+// out (the same bits in every restriction kernel)
+template <typename T>
+__device__ __forceinline__ T restrict7(T dc, T xm, T xp, T ym, T yp, T zm, T zp) {
+  const T cm = T(1) / T(4), c0 = T(2) / T(4), cp = T(1) / T(4);
+  T v = mulT(c0 + c0 + c0, dc);
+  v = fmaT(cm, xm, v);
+  v = fmaT(cp, xp, v);
+  v = fmaT(cm, ym, v);
+  v = fmaT(cp, yp, v);
+  v = fmaT(cm, zm, v);
+  v = fmaT(cp, zp, v);
+  return v / T(3);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(ENT) k_lv_restrict(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
                                                      int nj, int ntiles) {
@@ -1419,13 +1435,11 @@ __global__ void __launch_bounds__(ENT) k_lv_restrict(const LevelJob<T>* __restri
     const int fi = J.rf[0] * (i - 1) + 1, fj = J.rf[1] * (j - 1) + 1;
     const int fim = wrapi(fi - 1, gf.n1), fip = wrapi(fi + 1, gf.n1);
     const int fjm = wrapi(fj - 1, gf.n2), fjp = wrapi(fj + 1, gf.n2);
-    const T cm = T(1) / T(4), c0 = T(2) / T(4), cp = T(1) / T(4);
     for (int k = k0; k <= k1; ++k) {
       const int fk = J.rf[2] * (k - 1) + 1;
-      const T v = (c0 + c0 + c0) * d[off(gf, fi, fj, fk)] + cm * d[off(gf, fim, fj, fk)] + cp * d[off(gf, fip, fj, fk)] +
-                  cm * d[off(gf, fi, fjm, fk)] + cp * d[off(gf, fi, fjp, fk)] +
-                  cm * d[off(gf, fi, fj, wrapi(fk - 1, gf.n3))] + cp * d[off(gf, fi, fj, wrapi(fk + 1, gf.n3))];
-      coarse[off(g, i, j, k)] = v / T(3);
+      coarse[off(g, i, j, k)] = restrict7(d[off(gf, fi, fj, fk)], d[off(gf, fim, fj, fk)], d[off(gf, fip, fj, fk)],
+                                          d[off(gf, fi, fjm, fk)], d[off(gf, fi, fjp, fk)],
+                                          d[off(gf, fi, fj, wrapi(fk - 1, gf.n3))], d[off(gf, fi, fj, wrapi(fk + 1, gf.n3))]);
     }
     }
   }
@@ -1929,6 +1943,183 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
 }
 
 // ------------------------------------------------------------------------------------------
+// coarse tail of the V-cycle in one block per case
+// ------------------------------------------------------------------------------------------
+// The coarsest levels of a case (lt .. lt + nl - 1, every field of them together within
+// TAIL_BYTES of shared memory) run their whole part of the V-cycle in one block: the
+// right-hand side of level lt comes from global memory (the restriction into it), every later
+// phase -- init sweep, sweeps and residual of each level, the restriction to the next, the
+// bottom sweeps, the prolongation back and the sweeps after it -- works on shared-memory copies,
+// one barrier per phase, and the final iterate of level lt goes back to global memory for the
+// prolongation into level lt - 1.  On a 384 x 384 x 768 case these levels are 12 x 12 x 24 and
+// smaller, whose one-launch-per-phase schedule is some 25 launches of a few microseconds each.
+// Every point sees the operations of the per-level kernels (jinit / jres / jsweep / jresid,
+// restrict7, pmix), so the V-cycle is the same bit for bit.
+constexpr int TNT = 512;
+constexpr size_t TAIL_BYTES = 110 * 1024;
+template <typename T>
+struct TailJob {
+  int nl;                          // levels in the tail (>= 2)
+  LevelJob<T> lv[MG_MAX_LEVELS];   // their level jobs; lv[0].A / lv[0].B are the global fields
+};
+
+template <typename T>
+__global__ void __launch_bounds__(TNT, 1) k_lv_tail(const TailJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+                                                    int nj, int ntiles, T omega, int n_down, int n_up, int n_bottom) {
+  extern __shared__ __align__(16) unsigned char tl_raw[];
+  T* const sm = reinterpret_cast<T*>(tl_raw);
+  const int tid = threadIdx.x;
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q0 = find_job(ts, nj, b);
+    const TailJob<T>& TJ = jobs[q0];
+    if (e_halted(TJ.lv[0].sc)) continue;
+    const int nl = TJ.nl;
+    // shared-memory arrays of level q: A, X0, X1 (compact, i fastest)
+    T* Aq[MG_MAX_LEVELS];
+    T* X0[MG_MAX_LEVELS];
+    T* X1[MG_MAX_LEVELS];
+    int cur[MG_MAX_LEVELS];  // which of X0 / X1 holds the level's iterate
+    {
+      size_t o = 0;
+      for (int q = 0; q < nl; ++q) {
+        const Geom& g = TJ.lv[q].g;
+        const size_t m = (size_t)g.n1 * g.n2 * g.n3;
+        Aq[q] = sm + o;
+        X0[q] = sm + o + m;
+        X1[q] = sm + o + 2 * m;
+        o += 3 * m;
+        cur[q] = 0;
+      }
+    }
+    auto X = [&](int q, int which) { return which ? X1[q] : X0[q]; };
+    // right-hand side of the first level from global memory
+    {
+      const Geom& g = TJ.lv[0].g;
+      const int m = g.n1 * g.n2 * g.n3;
+      for (int idx = tid; idx < m; idx += TNT) {
+        const int i = idx % g.n1 + 1, r = idx / g.n1, j = r % g.n2 + 1, k = r / g.n2 + 1;
+        Aq[0][idx] = TJ.lv[0].A[off(g, i, j, k)];
+      }
+    }
+    __syncthreads();
+    // OP 0: dst = init(A); 1: dst = sweep(A, src); 2: dst = A - cdg(src)
+    auto relax = [&](int q, int op, const T* src, T* dst) {
+      const LevelJob<T>& J = TJ.lv[q];
+      const Geom& g = J.g;
+      const int m = g.n1 * g.n2 * g.n3;
+      const bool zu = J.zuni != 0;
+      const T* __restrict__ cz = J.cdg[2];
+      const T* a = Aq[q];
+      for (int idx = tid; idx < m; idx += TNT) {
+        const int i = idx % g.n1 + 1, r = idx / g.n1, j = r % g.n2 + 1, k = r / g.n2 + 1;
+        const T a0 = J.cdg[0][3 * (i - 1)], a1 = J.cdg[0][3 * (i - 1) + 1], a2 = J.cdg[0][3 * (i - 1) + 2];
+        const T b0 = J.cdg[1][3 * (j - 1)], b1 = J.cdg[1][3 * (j - 1) + 1], b2 = J.cdg[1][3 * (j - 1) + 2];
+        const T cm = zu ? cz[0] : cz[3 * (k - 1)], cc = zu ? cz[1] : cz[3 * (k - 1) + 1],
+                cp = zu ? cz[2] : cz[3 * (k - 1) + 2];
+        const T inv = zu ? omega / (a1 + b1 + cz[1]) : T(0);
+        const T diag = a1 + b1 + cc;
+        if (op == 0) {
+          dst[idx] = jinit(a[idx], omega, zu, inv, diag);
+          continue;
+        }
+        const int im = i == 1 ? idx + g.n1 - 1 : idx - 1, ip = i == g.n1 ? idx - g.n1 + 1 : idx + 1;
+        const int sy = g.n1, sz = g.n1 * g.n2;
+        const int jm = j == 1 ? idx + (g.n2 - 1) * sy : idx - sy, jp = j == g.n2 ? idx - (g.n2 - 1) * sy : idx + sy;
+        const int km = k == 1 ? idx + (g.n3 - 1) * sz : idx - sz, kp = k == g.n3 ? idx - (g.n3 - 1) * sz : idx + sz;
+        const T zc = src[idx];
+        if (op == 1) {
+          const T rr = jres(a[idx], a0, src[im], a2, src[ip], b0, src[jm], b2, src[jp], cm, src[km], cp, src[kp]);
+          dst[idx] = jsweep(rr, zc, omega, zu, inv, diag);
+        } else {
+          dst[idx] = jresid(a[idx], a0, src[im], a2, src[ip], b0, src[jm], b2, src[jp], cm, src[km], cp, src[kp], diag, zc);
+        }
+      }
+      __syncthreads();
+    };
+    // n sweeps of level q (after an init sweep when init): the iterate moves between X0 and X1
+    auto smooth = [&](int q, int init, int n) {
+      for (int w = 0; w < n; ++w) {
+        if (init && w == 0) {
+          relax(q, 0, nullptr, X(q, cur[q]));
+        } else {
+          relax(q, 1, X(q, cur[q]), X(q, cur[q] ^ 1));
+          cur[q] ^= 1;
+        }
+      }
+    };
+    // the residual of level q (in its spare buffer) restricted into the right-hand side of q + 1
+    auto restrict_down = [&](int q) {
+      const LevelJob<T>& C = TJ.lv[q + 1];
+      const Geom& gf = TJ.lv[q].g;
+      const Geom& g = C.g;
+      const T* d = X(q, cur[q] ^ 1);
+      const int m = g.n1 * g.n2 * g.n3;
+      for (int idx = tid; idx < m; idx += TNT) {
+        const int i = idx % g.n1 + 1, r = idx / g.n1, j = r % g.n2 + 1, k = r / g.n2 + 1;
+        const int fi = C.rf[0] * (i - 1) + 1, fj = C.rf[1] * (j - 1) + 1, fk = C.rf[2] * (k - 1) + 1;
+        auto at = [&](int a, int bq, int c) { return d[(a - 1) + gf.n1 * ((bq - 1) + gf.n2 * (c - 1))]; };
+        Aq[q + 1][idx] = restrict7(at(fi, fj, fk), at(wrapi(fi - 1, gf.n1), fj, fk), at(wrapi(fi + 1, gf.n1), fj, fk),
+                                   at(fi, wrapi(fj - 1, gf.n2), fk), at(fi, wrapi(fj + 1, gf.n2), fk),
+                                   at(fi, fj, wrapi(fk - 1, gf.n3)), at(fi, fj, wrapi(fk + 1, gf.n3)));
+      }
+      __syncthreads();
+    };
+    // spare buffer of level q = its iterate + P (iterate of q + 1); then it holds the iterate
+    auto prolong_up = [&](int q) {
+      const LevelJob<T>& J = TJ.lv[q];
+      const Geom& g = J.g;
+      const Geom& gc = TJ.lv[q + 1].g;
+      const T* xf = X(q, cur[q]);
+      const T* xc = X(q + 1, cur[q + 1]);
+      T* out = X(q, cur[q] ^ 1);
+      const int m = g.n1 * g.n2 * g.n3;
+      for (int idx = tid; idx < m; idx += TNT) {
+        const int i = idx % g.n1 + 1, r = idx / g.n1, j = r % g.n2 + 1, k = r / g.n2 + 1;
+        int xl, xh, yl, yh, zl, zh;
+        bool mx, my, mz;
+        bracket(i, J.rc[0], gc.n1, xl, xh, mx);
+        bracket(j, J.rc[1], gc.n2, yl, yh, my);
+        bracket(k, J.rc[2], gc.n3, zl, zh, mz);
+        auto P = [&](int a, int bq, int c) { return xc[(a - 1) + gc.n1 * ((bq - 1) + gc.n2 * (c - 1))]; };
+        const T wz0 = J.cI[2][2 * k], wz1 = J.cI[2][2 * k + 1];
+        const T wy0 = J.cI[1][2 * j], wy1 = J.cI[1][2 * j + 1];
+        const T wx0 = J.cI[0][2 * i], wx1 = J.cI[0][2 * i + 1];
+        const T Z0 = pmix(mz, wz0, P(xl, yl, zl), wz1, P(xl, yl, zh));
+        const T Z1 = pmix(mz, wz0, P(xl, yh, zl), wz1, P(xl, yh, zh));
+        const T Z2 = pmix(mz, wz0, P(xh, yl, zl), wz1, P(xh, yl, zh));
+        const T Z3 = pmix(mz, wz0, P(xh, yh, zl), wz1, P(xh, yh, zh));
+        const T Yl = pmix(my, wy0, Z0, wy1, Z1);
+        const T Yh = pmix(my, wy0, Z2, wy1, Z3);
+        out[idx] = xf[idx] + pmix(mx, wx0, Yl, wx1, Yh);
+      }
+      cur[q] ^= 1;
+      __syncthreads();
+    };
+    for (int q = 0; q + 1 < nl; ++q) {  // relax_restrict
+      smooth(q, 1, n_down);
+      relax(q, 2, X(q, cur[q]), X(q, cur[q] ^ 1));
+      restrict_down(q);
+    }
+    smooth(nl - 1, 1, n_bottom);  // relax_bottom
+    smooth(nl - 1, 0, n_bottom);
+    for (int q = nl - 2; q >= 0; --q) {  // interpolate_relax
+      prolong_up(q);
+      smooth(q, 0, n_up);
+    }
+    {
+      const Geom& g = TJ.lv[0].g;
+      const T* x0 = X(0, cur[0]);
+      const int m = g.n1 * g.n2 * g.n3;
+      for (int idx = tid; idx < m; idx += TNT) {
+        const int i = idx % g.n1 + 1, r = idx / g.n1, j = r % g.n2 + 1, k = r / g.n2 + 1;
+        TJ.lv[0].B[off(g, i, j, k)] = x0[idx];
+      }
+    }
+    __syncthreads();  // shared memory is rewritten by the next case
+  }
+}
+
+// ------------------------------------------------------------------------------------------
 // mixed precision: FP64 residual / conversion / correction over the MixJob list
 // ------------------------------------------------------------------------------------------
 // x += e for the cases whose inner solve ended with status 0 or 1
@@ -1966,6 +2157,8 @@ void ax_attributes() {
   cudaFuncSetAttribute(k_kr_ax32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axa_smem_bytes());
   cudaFuncSetAttribute(k_kr_ax32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axa_smem_bytes());
   cudaFuncSetAttribute(k_kr_ax32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axa_smem_bytes());
+  cudaFuncSetAttribute(k_lv_tail<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_BYTES);
+  cudaFuncSetAttribute(k_lv_tail<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_BYTES);
 #define IMPACT_MULTI_ATTR(T, N, I, R)                                                                           \
   cudaFuncSetAttribute(k_lv_multi<T, N, I, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,               \
                        (int)multi_smem_bytes<T, N, I, R>());                                                    \
@@ -2305,6 +2498,25 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
     nlev[c] = (use_mg && cs[c].mg) ? cs[c].mg->n : 1;
     gmax = std::max(gmax, nlev[c]);
   }
+  // lt[c]: the first level of case c's coarse tail (k_lv_tail), the coarsest level from which
+  // all levels' three fields fit in TAIL_BYTES; -1 without one (one-sweep schedule, no hierarchy,
+  // or fewer than two levels that fit).  Levels from lt[c] on leave the per-level lists.
+  std::vector<int> lt(n, -1);
+  if (use_mg && p_.fuse && p_.mg_down >= 1 && p_.mg_bottom >= 1 && p_.mg_up >= 0) {
+    for (int c = 0; c < n; ++c) {
+      if (nlev[c] < 2) continue;
+      double bytes = 0.0;
+      int first = -1;
+      for (int g = nlev[c] - 1; g >= 0; --g) {
+        const Geom& gg = cs[c].mg->lv[g].g;
+        bytes += 3.0 * sizeof(T) * gg.n1 * gg.n2 * gg.n3;
+        if (bytes > (double)TAIL_BYTES) break;
+        first = g;
+      }
+      if (first >= 0 && nlev[c] - first >= 2) lt[c] = first;
+    }
+  }
+  auto in_lists = [&](int c, int g) { return lt[c] < 0 || g < lt[c]; };
   if (use_mg) {
     // fused smoothing phases for the sweep counts that have kernels
     const int spre = (p_.fuse && p_.mg_down >= 2 && p_.mg_down <= 3) ? p_.mg_down : 0;
@@ -2314,25 +2526,42 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
     for (int g = 1; g + 1 < gmax; ++g) {
       std::vector<std::pair<int, int>> m;
       for (int c = 0; c < n; ++c)
-        if (nlev[c] >= g + 2) m.push_back({c, g});
+        if (nlev[c] >= g + 2 && in_lists(c, g)) m.push_back({c, g});
       down[g] = add_list(m, 0);
       if (spre) dpre[g] = add_list(m, 0, true, spre);
       if (spost) dpost[g] = add_list(m, 0, true, spost);
     }
-    for (int g = 1; g < gmax; ++g) {
+    for (int g = 1; g < gmax; ++g) {  // restriction into level g (into a tail's first level too)
       std::vector<std::pair<int, int>> m;
       for (int c = 0; c < n; ++c)
-        if (nlev[c] >= g + 1) m.push_back({c, g});
+        if (nlev[c] >= g + 1 && (lt[c] < 0 || g <= lt[c])) m.push_back({c, g});
       rs[g] = add_list(m, 0, false);
     }
     for (int v = 0; v < 2; ++v) {
       std::vector<std::pair<int, int>> m0, bot;
+      std::vector<TailJob<T>> tj;
+      std::vector<int> tt;
       for (int c = 0; c < n; ++c) {
-        if (nlev[c] >= 2) m0.push_back({c, 0});
-        bot.push_back({c, nlev[c] - 1});
+        if (nlev[c] >= 2 && in_lists(c, 0)) m0.push_back({c, 0});
+        if (lt[c] < 0) {
+          bot.push_back({c, nlev[c] - 1});
+        } else {
+          TailJob<T> T1{};
+          T1.nl = nlev[c] - lt[c];
+          for (int q = 0; q < T1.nl; ++q) T1.lv[q] = lvjob(c, lt[c] + q, v);
+          tj.push_back(T1);
+          tt.push_back(1);
+        }
       }
       const int down0 = add_list(m0, v);
       const int botl = add_list(bot, v);
+      const int taill = tj.empty() ? -1 : arena_.add(tj, tt);
+      if (taill >= 0) {
+        double tc = 0.0;
+        for (int c = 0; c < n; ++c)
+          if (lt[c] >= 0) tc += vol(cs[c].mg->lv[lt[c]].g);
+        note(taill, tc, 0.0, 0.0);
+      }
       if (spre) dpre[0] = add_list(m0, v, true, spre);
       if (spost) dpost[0] = add_list(m0, v, true, spost);
       if (v == 0) {
@@ -2354,6 +2583,7 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
       }
       smooth(sch, botl, 1, p_.mg_bottom);  // relax_bottom
       smooth(sch, botl, 0, p_.mg_bottom);
+      if (taill >= 0) sch.push_back({PH_TAIL, taill, 0});  // the cases' coarse tails
       for (int g = gmax - 2; g >= 0; --g) {  // interpolate_relax
         const int D = g == 0 ? down0 : down[g];
         if (spost) {
@@ -2453,6 +2683,11 @@ void Engine<T>::enqueue_phase(const Phase& ph) {
       break;
     case PH_POST:  // mg_up 2 or 3
       IMPACT_PROF(prof::K_MG_POST, 3 * sz * c, s, launch_multi_post<T>(p_.mg_up, fast_[ph.list] != 0, J, L, om, s));
+      break;
+    case PH_TAIL:  // one block per case; bytes: read the first level's right-hand side, write its iterate
+      IMPACT_PROF(prof::K_MG_TAIL, 2 * sz * c, s,
+                  (k_lv_tail<T><<<L.ntiles, TNT, TAIL_BYTES, s>>>(static_cast<const TailJob<T>*>(L.jobs), L.ts, L.njobs,
+                                                                  L.ntiles, om, p_.mg_down, p_.mg_up, p_.mg_bottom)));
       break;
     default:
       break;

@@ -136,7 +136,8 @@ struct Phase {
 };
 // PH_PRE: init + (mg_down - 1) sweeps + residual in one kernel; PH_POST: mg_up sweeps in one
 // kernel (after a PH_PROLONG with flip = 1, which writes its result into C); for 2 or 3 sweeps
-enum { PH_INIT = 0, PH_SWEEP, PH_COPY, PH_RESID, PH_RESTRICT, PH_PROLONG, PH_PRE, PH_POST };
+// PH_TAIL: the coarsest levels of every case of the list in one block per case (k_lv_tail)
+enum { PH_INIT = 0, PH_SWEEP, PH_COPY, PH_RESID, PH_RESTRICT, PH_PROLONG, PH_PRE, PH_POST, PH_TAIL };
 
 // device arena of job lists built on the host
 struct ListArena {

@@ -35,7 +35,8 @@ cudaEvent_t take() {
 }
 const char* kNames[K_COUNT] = {"jacobi_sweep", "jacobi_init2", "div_grad_dot", "x_update", "p_update",
                                "r_update", "nl_rhs", "project", "divergence2", "mg_sweep", "mg_init",
-                               "mg_residual", "mg_transfer", "mg_pre_smooth", "mg_post_smooth", "mx_residual", "mx_apply"};
+                               "mg_residual", "mg_transfer", "mg_pre_smooth", "mg_post_smooth", "mx_residual", "mx_apply",
+                               "mg_coarse_tail"};
 }  // namespace
 
 bool enabled() { return on; }

@@ -26,6 +26,7 @@ enum Kid {
   K_MG_POST,       // fused sweeps after the prolongation
   K_MX_RESID,      // mixed precision: FP64 outer residual b - A x and its FP32 image
   K_MX_APPLY,      // mixed precision: x += e in FP64
+  K_MG_TAIL,       // the coarsest levels' part of a V-cycle in one block per case
   K_COUNT
 };
 
