@@ -1963,12 +1963,31 @@ struct TailJob {
   LevelJob<T> lv[MG_MAX_LEVELS];   // their level jobs; lv[0].A / lv[0].B are the global fields
 };
 
+// the cells idx = tid, tid + TNT, ... of an n1 x n2 x n3 level with their 1-based (i, j, k),
+// advanced by carries instead of one division per cell
+template <typename F>
+__device__ __forceinline__ void tail_cells(const Geom& g, F&& f) {
+  const int m = g.n1 * g.n2 * g.n3;
+  int idx = threadIdx.x;
+  int i = idx % g.n1, r = idx / g.n1, j = r % g.n2, k = r / g.n2;
+  const int di = TNT % g.n1, r2 = TNT / g.n1, dj = r2 % g.n2, dk = r2 / g.n2;
+  for (; idx < m; idx += TNT) {
+    f(idx, i + 1, j + 1, k + 1);
+    i += di;
+    const int ci = i >= g.n1;
+    if (ci) i -= g.n1;
+    j += dj + ci;
+    const int cj = j >= g.n2;
+    if (cj) j -= g.n2;
+    k += dk + cj;
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(TNT, 1) k_lv_tail(const TailJob<T>* __restrict__ jobs, const int* __restrict__ ts,
                                                     int nj, int ntiles, T omega, int n_down, int n_up, int n_bottom) {
   extern __shared__ __align__(16) unsigned char tl_raw[];
   T* const sm = reinterpret_cast<T*>(tl_raw);
-  const int tid = threadIdx.x;
   for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
     const int q0 = find_job(ts, nj, b);
     const TailJob<T>& TJ = jobs[q0];
@@ -1995,23 +2014,19 @@ __global__ void __launch_bounds__(TNT, 1) k_lv_tail(const TailJob<T>* __restrict
     // right-hand side of the first level from global memory
     {
       const Geom& g = TJ.lv[0].g;
-      const int m = g.n1 * g.n2 * g.n3;
-      for (int idx = tid; idx < m; idx += TNT) {
-        const int i = idx % g.n1 + 1, r = idx / g.n1, j = r % g.n2 + 1, k = r / g.n2 + 1;
-        Aq[0][idx] = TJ.lv[0].A[off(g, i, j, k)];
-      }
+      T* a0 = Aq[0];
+      const T* src = TJ.lv[0].A;
+      tail_cells(g, [&](int idx, int i, int j, int k) { a0[idx] = src[off(g, i, j, k)]; });
     }
     __syncthreads();
     // OP 0: dst = init(A); 1: dst = sweep(A, src); 2: dst = A - cdg(src)
     auto relax = [&](int q, int op, const T* src, T* dst) {
       const LevelJob<T>& J = TJ.lv[q];
       const Geom& g = J.g;
-      const int m = g.n1 * g.n2 * g.n3;
       const bool zu = J.zuni != 0;
       const T* __restrict__ cz = J.cdg[2];
       const T* a = Aq[q];
-      for (int idx = tid; idx < m; idx += TNT) {
-        const int i = idx % g.n1 + 1, r = idx / g.n1, j = r % g.n2 + 1, k = r / g.n2 + 1;
+      tail_cells(g, [&](int idx, int i, int j, int k) {
         const T a0 = J.cdg[0][3 * (i - 1)], a1 = J.cdg[0][3 * (i - 1) + 1], a2 = J.cdg[0][3 * (i - 1) + 2];
         const T b0 = J.cdg[1][3 * (j - 1)], b1 = J.cdg[1][3 * (j - 1) + 1], b2 = J.cdg[1][3 * (j - 1) + 2];
         const T cm = zu ? cz[0] : cz[3 * (k - 1)], cc = zu ? cz[1] : cz[3 * (k - 1) + 1],
@@ -2020,7 +2035,7 @@ __global__ void __launch_bounds__(TNT, 1) k_lv_tail(const TailJob<T>* __restrict
         const T diag = a1 + b1 + cc;
         if (op == 0) {
           dst[idx] = jinit(a[idx], omega, zu, inv, diag);
-          continue;
+          return;
         }
         const int im = i == 1 ? idx + g.n1 - 1 : idx - 1, ip = i == g.n1 ? idx - g.n1 + 1 : idx + 1;
         const int sy = g.n1, sz = g.n1 * g.n2;
@@ -2033,7 +2048,7 @@ __global__ void __launch_bounds__(TNT, 1) k_lv_tail(const TailJob<T>* __restrict
         } else {
           dst[idx] = jresid(a[idx], a0, src[im], a2, src[ip], b0, src[jm], b2, src[jp], cm, src[km], cp, src[kp], diag, zc);
         }
-      }
+      });
       __syncthreads();
     };
     // n sweeps of level q (after an init sweep when init): the iterate moves between X0 and X1
@@ -2053,15 +2068,14 @@ __global__ void __launch_bounds__(TNT, 1) k_lv_tail(const TailJob<T>* __restrict
       const Geom& gf = TJ.lv[q].g;
       const Geom& g = C.g;
       const T* d = X(q, cur[q] ^ 1);
-      const int m = g.n1 * g.n2 * g.n3;
-      for (int idx = tid; idx < m; idx += TNT) {
-        const int i = idx % g.n1 + 1, r = idx / g.n1, j = r % g.n2 + 1, k = r / g.n2 + 1;
+      T* aq = Aq[q + 1];
+      tail_cells(g, [&](int idx, int i, int j, int k) {
         const int fi = C.rf[0] * (i - 1) + 1, fj = C.rf[1] * (j - 1) + 1, fk = C.rf[2] * (k - 1) + 1;
         auto at = [&](int a, int bq, int c) { return d[(a - 1) + gf.n1 * ((bq - 1) + gf.n2 * (c - 1))]; };
-        Aq[q + 1][idx] = restrict7(at(fi, fj, fk), at(wrapi(fi - 1, gf.n1), fj, fk), at(wrapi(fi + 1, gf.n1), fj, fk),
-                                   at(fi, wrapi(fj - 1, gf.n2), fk), at(fi, wrapi(fj + 1, gf.n2), fk),
-                                   at(fi, fj, wrapi(fk - 1, gf.n3)), at(fi, fj, wrapi(fk + 1, gf.n3)));
-      }
+        aq[idx] = restrict7(at(fi, fj, fk), at(wrapi(fi - 1, gf.n1), fj, fk), at(wrapi(fi + 1, gf.n1), fj, fk),
+                            at(fi, wrapi(fj - 1, gf.n2), fk), at(fi, wrapi(fj + 1, gf.n2), fk),
+                            at(fi, fj, wrapi(fk - 1, gf.n3)), at(fi, fj, wrapi(fk + 1, gf.n3)));
+      });
       __syncthreads();
     };
     // spare buffer of level q = its iterate + P (iterate of q + 1); then it holds the iterate
@@ -2072,9 +2086,7 @@ __global__ void __launch_bounds__(TNT, 1) k_lv_tail(const TailJob<T>* __restrict
       const T* xf = X(q, cur[q]);
       const T* xc = X(q + 1, cur[q + 1]);
       T* out = X(q, cur[q] ^ 1);
-      const int m = g.n1 * g.n2 * g.n3;
-      for (int idx = tid; idx < m; idx += TNT) {
-        const int i = idx % g.n1 + 1, r = idx / g.n1, j = r % g.n2 + 1, k = r / g.n2 + 1;
+      tail_cells(g, [&](int idx, int i, int j, int k) {
         int xl, xh, yl, yh, zl, zh;
         bool mx, my, mz;
         bracket(i, J.rc[0], gc.n1, xl, xh, mx);
@@ -2091,7 +2103,7 @@ __global__ void __launch_bounds__(TNT, 1) k_lv_tail(const TailJob<T>* __restrict
         const T Yl = pmix(my, wy0, Z0, wy1, Z1);
         const T Yh = pmix(my, wy0, Z2, wy1, Z3);
         out[idx] = xf[idx] + pmix(mx, wx0, Yl, wx1, Yh);
-      }
+      });
       cur[q] ^= 1;
       __syncthreads();
     };
@@ -2109,11 +2121,8 @@ __global__ void __launch_bounds__(TNT, 1) k_lv_tail(const TailJob<T>* __restrict
     {
       const Geom& g = TJ.lv[0].g;
       const T* x0 = X(0, cur[0]);
-      const int m = g.n1 * g.n2 * g.n3;
-      for (int idx = tid; idx < m; idx += TNT) {
-        const int i = idx % g.n1 + 1, r = idx / g.n1, j = r % g.n2 + 1, k = r / g.n2 + 1;
-        TJ.lv[0].B[off(g, i, j, k)] = x0[idx];
-      }
+      T* dst = TJ.lv[0].B;
+      tail_cells(g, [&](int idx, int i, int j, int k) { dst[off(g, i, j, k)] = x0[idx]; });
     }
     __syncthreads();  // shared memory is rewritten by the next case
   }
