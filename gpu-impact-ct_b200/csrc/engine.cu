@@ -279,12 +279,14 @@ __global__ void __launch_bounds__(ENT) k_kr_init(const KrylovJob<T>* __restrict_
     tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     if (i <= g.n1 && j <= g.n2) {
-      const T* __restrict__ bb = J.bb;
+      const T* bb = J.bb;  // rh may share bb's buffer: neither is restrict-qualified
       T* __restrict__ phi = J.phi;
       T* __restrict__ rr = J.rr;
-      T* __restrict__ rh = J.rh;
+      T* rh = J.rh;
       const long long nxy = g.nxy;
       long long p = off(g, i, j, k0);
+      // from phi = 0 with rh sharing bb's buffer (the mixed solve's inner solve) rh already holds r
+      const bool write_rh = !(zero_phi && rh == bb);
       auto point = [&](long long q, T bv, T a) {
         T r;
         if (zero_phi) {
@@ -294,7 +296,7 @@ __global__ void __launch_bounds__(ENT) k_kr_init(const KrylovJob<T>* __restrict_
           r = bv - a;
         }
         rr[q] = r;
-        rh[q] = r;
+        if (write_rh) rh[q] = r;
         const double rd = (double)r, bd = (double)bv;
         v[0] = fmax(v[0], fabs(rd));
         v[1] += rd * rd;
@@ -532,7 +534,7 @@ constexpr size_t ax_smem_bytes() {
 }
 
 template <typename T, int MODE>
-__global__ void __launch_bounds__(AXNT, 3) k_kr_ax(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+__global__ void __launch_bounds__(AXNT, 2) k_kr_ax(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts,
                                                    int nj, int ntiles, double* __restrict__ partial) {
   constexpr int AX_R = AxRing<T>::R;
   constexpr bool REG = sizeof(T) == 4;  // y and z weights in registers
@@ -2767,9 +2769,10 @@ int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::
     launch_ax<T, 0>(grid, J, K.ts, n, K.ntiles, partial_, s_);
     prof::count(1);
   }
-  k_kr_init<T><<<grid, kBlock, 0, s_>>>(J, K.ts, n, K.ntiles, zero_phi, partial_);
+  IMPACT_PROF(prof::K_KR_INIT, 4.0 * sizeof(T) * cells_[kr_list_], s_,
+              (k_kr_init<T><<<grid, kBlock, 0, s_>>>(J, K.ts, n, K.ntiles, zero_phi, partial_)));
   k_efin<<<n, 256, 0, s_>>>(K.ts, partial_, 4, 1, EFIN_INIT, scal_, nullptr);
-  prof::count(2);
+  prof::count(1);
   const int chunk = p_.check_every > 0 ? p_.check_every : 1;
   const bool profiling = prof::enabled();
   if (graph_ && graph_prof_ != profiling) {  // the profiler was switched: capture again

@@ -36,7 +36,7 @@ cudaEvent_t take() {
 const char* kNames[K_COUNT] = {"jacobi_sweep", "jacobi_init2", "div_grad_dot", "x_update", "p_update",
                                "r_update", "nl_rhs", "project", "divergence2", "mg_sweep", "mg_init",
                                "mg_residual", "mg_transfer", "mg_pre_smooth", "mg_post_smooth", "mx_residual", "mx_apply",
-                               "mg_coarse_tail"};
+                               "mg_coarse_tail", "kr_init"};
 }  // namespace
 
 bool enabled() { return on; }

@@ -27,6 +27,7 @@ enum Kid {
   K_MX_RESID,      // mixed precision: FP64 outer residual b - A x and its FP32 image
   K_MX_APPLY,      // mixed precision: x += e in FP64
   K_MG_TAIL,       // the coarsest levels' part of a V-cycle in one block per case
+  K_KR_INIT,       // BiCGstab start: r = b - A x (or b), shadow residual, norms
   K_COUNT
 };
 

@@ -768,7 +768,9 @@ static int ensure_engine(CaseState& s, const double* b, double* x, const EngineP
     ec.phi = s.mw.e32;
     const KrylovWork<float>& w = s.mw.inner;
     ec.rr = w.rr;
-    ec.rh = w.rh;
+    // the inner solve starts from e = 0, so its shadow residual is its right-hand side: the two
+    // share the buffer (the outer loop rewrites it before every inner solve)
+    ec.rh = s.mw.r32;
     ec.pp = w.pp;
     ec.Ap = w.Ap;
     ec.Ar = w.Ar;
@@ -1281,7 +1283,7 @@ static int batch_engine(impact_b200_batch* b, const impact_b200_solver_params* p
     E.phi = s.mw.e32;
     const KrylovWork<float>& w = s.mw.inner;
     E.rr = w.rr;
-    E.rh = w.rh;
+    E.rh = s.mw.r32;  // shadow residual = right-hand side (e = 0 at the start), one buffer
     E.pp = w.pp;
     E.Ap = w.Ap;
     E.Ar = w.Ar;

@@ -398,7 +398,7 @@ class Batch:
         return lib().impact_b200_batch_stream(self._h)
 
 
-PROFILE_KERNELS = 18
+PROFILE_KERNELS = 19
 
 
 def profile(enable: bool = True, reset: bool = True):

@@ -285,9 +285,8 @@ int impact_b200_product_scalar_noalloc(int N1, int N2, int N3, const double* a_d
  * and accumulates, per kernel kind kid (0 jacobi_sweep, 1 jacobi_init2, 2 div_grad_dot,
  * 3 x_update, 4 p_update, 5 r_update, 6 nl_rhs, 7 project, 8 divergence2, 9 mg_sweep,
  * 10 mg_init, 11 mg_residual, 12 mg_transfer, 13 mg_pre_smooth, 14 mg_post_smooth,
- * 15 mx_residual, 16 mx_apply, 17 mg_coarse_tail), the launches, the elapsed milliseconds and the
- * algorithmic bytes
- * moved.  launch_count counts every kernel
+ * 15 mx_residual, 16 mx_apply, 17 mg_coarse_tail, 18 kr_init), the launches, the elapsed
+ * milliseconds and the algorithmic bytes moved.  launch_count counts every kernel
  * launch the library has issued since load. */
 void impact_b200_profile_enable(int enable);
 void impact_b200_profile_reset(void);
