@@ -56,6 +56,7 @@ struct CaseState {
   const double* eng_b = nullptr;
   double* eng_x = nullptr;
   std::vector<void*> allocs;
+  cudaEvent_t pre_wait = nullptr;  // the next step waits for it before it first reads the pressure
   bool pooled = false;  // allocs come from the per-device case pool (freed stream-ordered)
 };
 

@@ -684,6 +684,11 @@ extern "C" int impact_b200_case_download_async(impact_b200_case* c, int field, d
     IMPACT_CUDA_CHECK(cudaMemcpyAsync(host + first, s.f[field] + first, count * sizeof(double), cudaMemcpyDeviceToHost, st));
   return 0;
 }
+extern "C" int impact_b200_case_defer_pressure(impact_b200_case* c, void* event) {
+  if (!c || !event) return impact_set_error_msg(-1, "impact_b200_case_defer_pressure: bad arguments");
+  c->s.pre_wait = static_cast<cudaEvent_t>(event);
+  return 0;
+}
 extern "C" int impact_b200_case_set_labels(impact_b200_case* c, const uint8_t* host) {
   if (!c || !host) return impact_set_error_msg(-1, "impact_b200_case_set_labels: bad arguments");
   CaseState& s = c->s;
@@ -1094,6 +1099,10 @@ static void substep_rhs(CaseState& s, const impact_b200_step_params* p, double d
     IMPACT_PROF(prof::K_NL_RHS, nlb, st,
                 launch_rhs_march(m, g, s.c64, multL, mb, ma, use_old, vel[m], s.work, nl[m], rhs[m], st));
   const double ab = aRK[sub] + bRK[sub];
+  if (s.pre_wait) {  // a deferred pressure upload: wait for it here, at the step's first read
+    cudaStreamWaitEvent(st, s.pre_wait, 0);
+    s.pre_wait = nullptr;
+  }
   k_scale_pre<<<gr, bl, 0, st>>>(g, ab, dt, 0, s.f[IMPACT_B200_PRE]);
   prof::count(1);
   IMPACT_PROF(prof::K_DIV2, 4.0 * 8.0 * cells, st,

@@ -102,6 +102,7 @@ def lib():
         "impact_b200_case_download": (i, [_vp, i, _dp]),
         "impact_b200_case_upload_async": (i, [_vp, i, _dp, C.c_size_t, C.c_size_t, _vp]),
         "impact_b200_case_download_async": (i, [_vp, i, _dp, C.c_size_t, C.c_size_t, _vp]),
+        "impact_b200_case_defer_pressure": (i, [_vp, _vp]),
         "impact_b200_case_set_labels": (i, [_vp, _u8p]),
         "impact_b200_case_field_ptr": (_vp, [_vp, i]),
         "impact_b200_case_stream": (_vp, [_vp]),
@@ -300,6 +301,11 @@ class Case:
         first, count = self._range("download_async", out, first, count)
         check(lib().impact_b200_case_download_async(self._h, f, _ptr(out), first, count, C.c_void_p(stream or None)),
               "case_download_async")
+
+    def defer_pressure(self, event: int):
+        """The next step waits for the CUDA event handle `event` (e.g. torch.cuda.Event().cuda_event,
+        recorded after an asynchronous pressure upload) only where it first reads the pressure."""
+        check(lib().impact_b200_case_defer_pressure(self._h, C.c_void_p(event)), "case_defer_pressure")
 
     def set_labels(self, labels: np.ndarray):
         lb = np.ascontiguousarray(labels, dtype=np.uint8)
