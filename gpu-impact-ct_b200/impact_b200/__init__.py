@@ -304,7 +304,8 @@ class Case:
 
     def defer_pressure(self, event: int):
         """The next step waits for the CUDA event handle `event` (e.g. torch.cuda.Event().cuda_event,
-        recorded after an asynchronous pressure upload) only where it first reads the pressure."""
+        recorded after an asynchronous pressure upload) only where it first reads the pressure; the
+        event must stay alive until that step call has returned."""
         check(lib().impact_b200_case_defer_pressure(self._h, C.c_void_p(event)), "case_defer_pressure")
 
     def set_labels(self, labels: np.ndarray):

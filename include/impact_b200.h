@@ -170,8 +170,9 @@ int impact_b200_case_download_async(impact_b200_case* c, int field, double* host
 /* The next time step of the case waits for `event` (a cudaEvent_t the caller recorded, e.g. after
  * an asynchronous upload of the pressure) only where it first reads the pressure -- after the
  * explicit part of its first substep -- instead of before it starts, so that the pressure upload
- * overlaps that part of the step.  The event is consumed by that step.  No counterpart in the
- * reference (its wrappers copy whole fields synchronously). */
+ * overlaps that part of the step.  The event is consumed by that step and must stay valid until
+ * the step call has returned.  No counterpart in the reference (its wrappers copy whole fields
+ * synchronously). */
 int impact_b200_case_defer_pressure(impact_b200_case* c, void* event);
 /* voxel labels (padded layout, one byte per point): 0 solid, 1 fluid, 5 inflow, 7 wall, 9/11 outlets */
 int impact_b200_case_set_labels(impact_b200_case* c, const uint8_t* host_labels);
