@@ -2557,10 +2557,10 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
         if (lt[c] < 0) {
           bot.push_back({c, nlev[c] - 1});
         } else {
-          TailJob<T> T1{};
-          T1.nl = nlev[c] - lt[c];
-          for (int q = 0; q < T1.nl; ++q) T1.lv[q] = lvjob(c, lt[c] + q, v);
-          tj.push_back(T1);
+          TailJob<T> job{};
+          job.nl = nlev[c] - lt[c];
+          for (int q = 0; q < job.nl; ++q) job.lv[q] = lvjob(c, lt[c] + q, v);
+          tj.push_back(job);
           tt.push_back(1);
         }
       }
