@@ -57,6 +57,8 @@ struct CaseState {
   double* eng_x = nullptr;
   std::vector<void*> allocs;
   cudaEvent_t pre_wait = nullptr;  // the next step waits for it before it first reads the pressure
+  // measured inflow waveform (nondimensional time, velocity); empty: the sinusoidal inflow
+  std::vector<double> inflow_t, inflow_u;
   bool pooled = false;  // allocs come from the per-device case pool (freed stream-ordered)
 };
 

@@ -259,7 +259,9 @@ __global__ void __launch_bounds__(NT) k_sub_mean(Geom g, const double* __restric
 }
 
 // apply_CT_forcing (usr_func.f90:909-1049, idealized branch): label 0/7 -> u = 0; 5 -> inflow
-__global__ void __launch_bounds__(NT) k_mask(Geom g, const uint8_t* __restrict__ label, double u_in,
+// inflow_on = 0: the inflow voxels keep their velocity (a measured waveform without an interval
+// that holds the current time, as in apply_CT_forcing)
+__global__ void __launch_bounds__(NT) k_mask(Geom g, const uint8_t* __restrict__ label, double u_in, int inflow_on,
                                              double* __restrict__ u, double* __restrict__ v, double* __restrict__ w) {
   PT
   const uint8_t lb = label[p];
@@ -267,7 +269,7 @@ __global__ void __launch_bounds__(NT) k_mask(Geom g, const uint8_t* __restrict__
     u[p] = 0.0;
     v[p] = 0.0;
     w[p] = 0.0;
-  } else if (lb == 5) {
+  } else if (lb == 5 && inflow_on) {
     w[p] = u_in;
     v[p] = 0.0;
     u[p] = 0.0;
@@ -682,6 +684,20 @@ extern "C" int impact_b200_case_download_async(impact_b200_case* c, int field, d
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s.stream;
   if (count)
     IMPACT_CUDA_CHECK(cudaMemcpyAsync(host + first, s.f[field] + first, count * sizeof(double), cudaMemcpyDeviceToHost, st));
+  return 0;
+}
+extern "C" int impact_b200_case_set_inflow_waveform(impact_b200_case* c, int n, const double* time,
+                                                     const double* velocity) {
+  if (!c || n < 0 || n == 1 || (n > 0 && (!time || !velocity)))
+    return impact_set_error_msg(-1, "impact_b200_case_set_inflow_waveform: bad arguments");
+  for (int i = 0; i < n; ++i) {
+    if (!std::isfinite(time[i]) || !std::isfinite(velocity[i]) || (i > 0 && time[i] < time[i - 1]))
+      return impact_set_error_msg(-1, "impact_b200_case_set_inflow_waveform: times must be finite and non-decreasing");
+  }
+  if (n > 0 && !(time[n - 1] > 0.0))
+    return impact_set_error_msg(-1, "impact_b200_case_set_inflow_waveform: the pulse length (last time) must be positive");
+  c->s.inflow_t.assign(time, time + n);
+  c->s.inflow_u.assign(velocity, velocity + n);
   return 0;
 }
 extern "C" int impact_b200_case_defer_pressure(impact_b200_case* c, void* event) {
@@ -1124,6 +1140,30 @@ static void substep_project(CaseState& s, double dt, int sub, cudaStream_t st) {
   prof::count(1);
 }
 
+// Inflow velocity of the label-5 voxels at nondimensional time t.  With a measured waveform
+// (apply_CT_forcing, usr_func.f90:923-945): t is shifted into the current pulse (pulse length =
+// the last table time, get_pulse_number_and_length :753-760, get_shifted_time_in_pulse
+// :899-906) and the velocity is the value at the start of the last table interval [t_i, t_i+1]
+// that holds it (no such interval: *on = 0, the voxels keep their velocity; the reference's
+// loop also visits a last interval past the table, which is left out here).  Without one:
+// U0 (1 + sin(2 pi t / T) / 2).
+static double inflow_velocity(const CaseState& s, const impact_b200_step_params* p, double t, int* on) {
+  *on = 1;
+  const size_t n = s.inflow_t.size();
+  if (n < 2) return p->U0 * (1.0 + 0.5 * std::sin(2.0 * 3.14159265358979323846 * t / p->T_pulse));
+  const double len = s.inflow_t[n - 1];
+  const double pulse = std::floor(t / len) + 1.0;
+  const double ts = t - (pulse - 1.0) * len;
+  double u = 0.0;
+  *on = 0;
+  for (size_t i = 0; i + 1 < n; ++i)
+    if (ts >= s.inflow_t[i] && ts <= s.inflow_t[i + 1]) {
+      u = s.inflow_u[i];
+      *on = 1;
+    }
+  return u;
+}
+
 // end of the step: mask forcing at the new time, level_pressure
 static void step_finish(CaseState& s, const impact_b200_step_params* p, impact_b200_step_state* stt, double dt,
                         cudaStream_t st) {
@@ -1131,8 +1171,9 @@ static void step_finish(CaseState& s, const impact_b200_step_params* p, impact_b
   const dim3 gr = grid3(g), bl(BX, BY);
   stt->timestep += 1;
   stt->time += dt;
-  const double u_in = p->U0 * (1.0 + 0.5 * std::sin(2.0 * 3.14159265358979323846 * stt->time / p->T_pulse));
-  k_mask<<<gr, bl, 0, st>>>(g, s.label, u_in, s.f[IMPACT_B200_VEL1], s.f[IMPACT_B200_VEL2], s.f[IMPACT_B200_VEL3]);
+  int on = 1;
+  const double u_in = inflow_velocity(s, p, stt->time, &on);
+  k_mask<<<gr, bl, 0, st>>>(g, s.label, u_in, on, s.f[IMPACT_B200_VEL1], s.f[IMPACT_B200_VEL2], s.f[IMPACT_B200_VEL3]);
   prof::count(1);
   if (p->level_pressure) {
     k_sum<<<gr, bl, 0, st>>>(g, s.f[IMPACT_B200_PRE], s.partial);

@@ -103,6 +103,7 @@ def lib():
         "impact_b200_case_upload_async": (i, [_vp, i, _dp, C.c_size_t, C.c_size_t, _vp]),
         "impact_b200_case_download_async": (i, [_vp, i, _dp, C.c_size_t, C.c_size_t, _vp]),
         "impact_b200_case_defer_pressure": (i, [_vp, _vp]),
+        "impact_b200_case_set_inflow_waveform": (i, [_vp, i, _dp, _dp]),
         "impact_b200_case_set_labels": (i, [_vp, _u8p]),
         "impact_b200_case_field_ptr": (_vp, [_vp, i]),
         "impact_b200_case_stream": (_vp, [_vp]),
@@ -307,6 +308,19 @@ class Case:
         recorded after an asynchronous pressure upload) only where it first reads the pressure; the
         event must stay alive until that step call has returned."""
         check(lib().impact_b200_case_defer_pressure(self._h, C.c_void_p(event)), "case_defer_pressure")
+
+    def set_inflow_waveform(self, time=None, velocity=None):
+        """Measured inflow of the label-5 voxels: nondimensional (time, velocity) pairs, times
+        non-decreasing, the last one the pulse length (see impact_b200.ingest); None restores the
+        default sinusoidal inflow."""
+        if time is None:
+            check(lib().impact_b200_case_set_inflow_waveform(self._h, 0, None, None), "case_set_inflow_waveform")
+            return
+        t = np.ascontiguousarray(time, dtype=np.float64)
+        u = np.ascontiguousarray(velocity, dtype=np.float64)
+        if t.ndim != 1 or t.shape != u.shape:
+            raise ValueError("set_inflow_waveform: time and velocity must be 1-D arrays of one length")
+        check(lib().impact_b200_case_set_inflow_waveform(self._h, t.size, _ptr(t), _ptr(u)), "case_set_inflow_waveform")
 
     def set_labels(self, labels: np.ndarray):
         lb = np.ascontiguousarray(labels, dtype=np.uint8)

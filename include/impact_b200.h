@@ -174,6 +174,13 @@ int impact_b200_case_download_async(impact_b200_case* c, int field, double* host
  * the step call has returned.  No counterpart in the reference (its wrappers copy whole fields
  * synchronously). */
 int impact_b200_case_defer_pressure(impact_b200_case* c, void* event);
+/* Measured inflow waveform of the label-5 voxels (read_velocity_waveform / convert_waveform,
+ * usr_func.f90:574-651, as apply_CT_forcing :923-945 uses it): n (time, velocity) pairs in
+ * nondimensional units, times non-decreasing, the last one the pulse length.  At the end of every
+ * step the time is shifted into the current pulse and the inflow voxels take the value at the
+ * start of the last table interval that holds it (none does: they keep their velocity).  n = 0
+ * restores the default inflow U0 (1 + sin(2 pi t / T_pulse) / 2). */
+int impact_b200_case_set_inflow_waveform(impact_b200_case* c, int n, const double* time, const double* velocity);
 /* voxel labels (padded layout, one byte per point): 0 solid, 1 fluid, 5 inflow, 7 wall, 9/11 outlets */
 int impact_b200_case_set_labels(impact_b200_case* c, const uint8_t* host_labels);
 double* impact_b200_case_field_ptr(impact_b200_case* c, int field);
