@@ -57,6 +57,11 @@ struct CaseState {
   double* eng_x = nullptr;
   std::vector<void*> allocs;
   cudaEvent_t pre_wait = nullptr;  // the next step waits for it before it first reads the pressure
+  // snapshot: device copies of fields taken on the case stream, read back on a copy stream
+  double* snap = nullptr;  // snap_cap fields (case pool)
+  int snap_cap = 0;
+  cudaEvent_t snap_taken = nullptr, snap_read = nullptr;
+  bool snap_pending = false;  // snap_read marks the last read-back of the buffer
   // measured inflow waveform (nondimensional time, velocity); empty: the sinusoidal inflow
   std::vector<double> inflow_t, inflow_u;
   bool pooled = false;  // allocs come from the per-device case pool (freed stream-ordered)

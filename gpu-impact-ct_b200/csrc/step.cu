@@ -364,6 +364,8 @@ extern "C" int impact_b200_case_destroy(impact_b200_case* c) {
   } else {
     for (void* p : s.allocs) cudaFree(p);
   }
+  if (s.snap_taken) cudaEventDestroy(s.snap_taken);
+  if (s.snap_read) cudaEventDestroy(s.snap_read);
   if (s.hscal) cudaFreeHost(s.hscal);
   if (s.scal_host) cudaFreeHost(s.scal_host);
   if (s.mw.scal64_host) cudaFreeHost(s.mw.scal64_host);
@@ -698,6 +700,47 @@ extern "C" int impact_b200_case_set_inflow_waveform(impact_b200_case* c, int n, 
     return impact_set_error_msg(-1, "impact_b200_case_set_inflow_waveform: the pulse length (last time) must be positive");
   c->s.inflow_t.assign(time, time + n);
   c->s.inflow_u.assign(velocity, velocity + n);
+  return 0;
+}
+extern "C" int impact_b200_case_snapshot(impact_b200_case* c, int nfields, const int* fields, double* const* host,
+                                         void* stream) {
+  if (!c || nfields < 1 || nfields > IMPACT_B200_NFIELDS || !fields || !host)
+    return impact_set_error_msg(-1, "impact_b200_case_snapshot: bad arguments");
+  for (int q = 0; q < nfields; ++q) {
+    if (fields[q] < 0 || fields[q] >= IMPACT_B200_NFIELDS || !host[q])
+      return impact_set_error_msg(-1, "impact_b200_case_snapshot: bad field or host buffer");
+    for (int r = 0; r < q; ++r)
+      if (fields[r] == fields[q]) return impact_set_error_msg(-1, "impact_b200_case_snapshot: a field appears twice");
+  }
+  CaseState& s = c->s;
+  IMPACT_CUDA_CHECK(cudaSetDevice(s.device));
+  const size_t fb = (size_t)s.g.nfield * sizeof(double);
+  if (!s.snap_taken) {
+    IMPACT_CUDA_CHECK(cudaEventCreateWithFlags(&s.snap_taken, cudaEventDisableTiming));
+    IMPACT_CUDA_CHECK(cudaEventCreateWithFlags(&s.snap_read, cudaEventDisableTiming));
+  }
+  if (s.snap_pending) IMPACT_CUDA_CHECK(cudaStreamWaitEvent(s.stream, s.snap_read, 0));  // buffer free again
+  if (nfields > s.snap_cap) {  // grow (the old buffer stays with the case until it is destroyed)
+    double* p = nullptr;
+    if (case_alloc(s, (void**)&p, (size_t)nfields * fb)) return -1;
+    s.snap = p;
+    s.snap_cap = nfields;
+  }
+  for (int q = 0; q < nfields; ++q)
+    IMPACT_CUDA_CHECK(cudaMemcpyAsync(s.snap + (size_t)q * s.g.nfield, s.f[fields[q]], fb, cudaMemcpyDeviceToDevice, s.stream));
+  IMPACT_CUDA_CHECK(cudaEventRecord(s.snap_taken, s.stream));
+  cudaStream_t cs = stream ? static_cast<cudaStream_t>(stream) : s.stream;
+  IMPACT_CUDA_CHECK(cudaStreamWaitEvent(cs, s.snap_taken, 0));
+  for (int q = 0; q < nfields; ++q)
+    IMPACT_CUDA_CHECK(cudaMemcpyAsync(host[q], s.snap + (size_t)q * s.g.nfield, fb, cudaMemcpyDeviceToHost, cs));
+  IMPACT_CUDA_CHECK(cudaEventRecord(s.snap_read, cs));
+  s.snap_pending = true;
+  return 0;
+}
+extern "C" int impact_b200_case_synchronize(impact_b200_case* c) {
+  if (!c) return impact_set_error_msg(-1, "impact_b200_case_synchronize: bad arguments");
+  IMPACT_CUDA_CHECK(cudaSetDevice(c->s.device));
+  IMPACT_CUDA_CHECK(cudaStreamSynchronize(c->s.stream));
   return 0;
 }
 extern "C" int impact_b200_case_defer_pressure(impact_b200_case* c, void* event) {

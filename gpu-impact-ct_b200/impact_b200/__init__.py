@@ -104,6 +104,8 @@ def lib():
         "impact_b200_case_download_async": (i, [_vp, i, _dp, C.c_size_t, C.c_size_t, _vp]),
         "impact_b200_case_defer_pressure": (i, [_vp, _vp]),
         "impact_b200_case_set_inflow_waveform": (i, [_vp, i, _dp, _dp]),
+        "impact_b200_case_snapshot": (i, [_vp, i, C.POINTER(i), C.POINTER(_dp), _vp]),
+        "impact_b200_case_synchronize": (i, [_vp]),
         "impact_b200_case_set_labels": (i, [_vp, _u8p]),
         "impact_b200_case_field_ptr": (_vp, [_vp, i]),
         "impact_b200_case_stream": (_vp, [_vp]),
@@ -308,6 +310,26 @@ class Case:
         recorded after an asynchronous pressure upload) only where it first reads the pressure; the
         event must stay alive until that step call has returned."""
         check(lib().impact_b200_case_defer_pressure(self._h, C.c_void_p(event)), "case_defer_pressure")
+
+    def snapshot(self, fields, out, stream: int = 0):
+        """Take device copies of `fields` now (in the case stream's order) and read them back into
+        `out` (one C-contiguous float64 array of the grid's shape per field, pinned for overlap) on
+        the CUDA stream handle `stream` (0: the case stream); returns at once.  `out` holds the
+        snapshot once that stream has reached this point."""
+        ids = [FIELDS[f] if isinstance(f, str) else int(f) for f in fields]
+        if len(ids) != len(out):
+            raise ValueError("snapshot: one output array per field")
+        for a in out:
+            if not (a.flags["C_CONTIGUOUS"] and a.dtype == np.float64 and a.shape == self.grid.shape):
+                raise ValueError("snapshot: outputs must be C-contiguous float64 arrays of the grid's shape")
+        fid = (C.c_int * len(ids))(*ids)
+        ptrs = (_dp * len(out))(*[_ptr(a) for a in out])
+        check(lib().impact_b200_case_snapshot(self._h, len(ids), fid, ptrs, C.c_void_p(stream or None)),
+              "case_snapshot")
+
+    def synchronize(self):
+        """Wait until the case stream has finished its work."""
+        check(lib().impact_b200_case_synchronize(self._h), "case_synchronize")
 
     def set_inflow_waveform(self, time=None, velocity=None):
         """Measured inflow of the label-5 voxels: nondimensional (time, velocity) pairs, times

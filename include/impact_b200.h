@@ -167,6 +167,17 @@ int impact_b200_case_upload_async(impact_b200_case* c, int field, const double* 
                                   void* stream);
 int impact_b200_case_download_async(impact_b200_case* c, int field, double* host, size_t first, size_t count,
                                     void* stream);
+/* Snapshot of resident fields (output and restart off the hot path, mod_inout.f90:78-500 without
+ * HDF5): device copies of fields[0..nfields-1] are taken on the case stream at this point of its
+ * work, then read back into host[q] (whole padded fields, pinned for overlap) on `stream` (NULL:
+ * the case stream) while later steps run.  The call returns at once; the host buffers hold the
+ * snapshot once `stream` has reached this point (synchronise it or an event recorded on it).  A
+ * later snapshot of the case waits for the read-back of the previous one.  The copy buffer comes
+ * from the case's memory pool on the first call (and grows to the largest field count asked for).
+ * No counterpart in the reference (its output writes HDF5 from the host arrays). */
+int impact_b200_case_snapshot(impact_b200_case* c, int nfields, const int* fields, double* const* host, void* stream);
+/* wait until the case stream has finished its work */
+int impact_b200_case_synchronize(impact_b200_case* c);
 /* The next time step of the case waits for `event` (a cudaEvent_t the caller recorded, e.g. after
  * an asynchronous upload of the pressure) only where it first reads the pressure -- after the
  * explicit part of its first substep -- instead of before it starts, so that the pressure upload
