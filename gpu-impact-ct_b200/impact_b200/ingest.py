@@ -2,7 +2,7 @@
 waveform, prepared as the reference prepares them before its time loop and handed to a device
 case (Case.set_labels, Case.set_inflow_waveform).
 
-    read_vtk_3D            usr_func.f90:187-555   read_vtk_structured_points + ct_grid
+    read_vtk_3D            usr_func.f90:187-555   read_vtk_structured_points (or read_nifti) + ct_grid
     read_velocity_waveform usr_func.f90:574-596   read_waveform_csv
     convert_waveform       usr_func.f90:599-651   convert_waveform
     apply_CT_forcing       usr_func.f90:909-1049  labels_from_ct_grid (its label tests),
@@ -103,6 +103,49 @@ def read_vtk_structured_points(path) -> VtkVolume:
     if vals.size != npts:
         raise ValueError(f"{path}: {vals.size} values for POINT_DATA {npts}")
     return VtkVolume(dims, spacing or (1.0, 1.0, 1.0), origin or (0.0, 0.0, 0.0), vals, name)
+
+
+_NIFTI_TYPES = {2: "u1", 4: "i2", 8: "i4", 16: "f4", 64: "f8", 256: "i1", 512: "u2", 768: "u4"}
+
+
+def read_nifti(path) -> VtkVolume:
+    """A NIfTI-1 single-file volume (.nii, or gzip-compressed .nii.gz; either byte order) as a
+    VtkVolume: the first three dimensions with x fastest (the point order of a VTK volume), the
+    voxel sizes as spacing, the values scaled by scl_slope / scl_inter when the slope is not 0.
+    CT label volumes prepared for read_vtk_3D are often kept in this format before conversion."""
+    import gzip
+    import struct
+
+    opener = gzip.open if str(path).endswith(".gz") else open
+    with opener(path, "rb") as f:
+        raw = f.read()
+    if len(raw) < 348:
+        raise ValueError(f"{path}: shorter than a NIfTI-1 header")
+    for end in ("<", ">"):
+        if struct.unpack(end + "i", raw[0:4])[0] == 348:
+            break
+    else:
+        raise ValueError(f"{path}: not a NIfTI-1 header (sizeof_hdr is not 348)")
+    if raw[344:347] not in (b"n+1", b"ni1"):
+        raise ValueError(f"{path}: NIfTI magic missing")
+    if raw[344:347] == b"ni1":
+        raise ValueError(f"{path}: a two-file NIfTI pair (.hdr/.img) is not supported")
+    dim = struct.unpack(end + "8h", raw[40:56])
+    if dim[0] < 3 or any(d > 1 for d in dim[4:dim[0] + 1]):
+        raise ValueError(f"{path}: not a single 3-D volume (dim = {dim})")
+    datatype = struct.unpack(end + "h", raw[70:72])[0]
+    if datatype not in _NIFTI_TYPES:
+        raise ValueError(f"{path}: NIfTI datatype {datatype} not supported")
+    pixdim = struct.unpack(end + "8f", raw[76:108])
+    vox_offset = int(struct.unpack(end + "f", raw[108:112])[0])
+    slope, inter = struct.unpack(end + "2f", raw[112:120])
+    n1, n2, n3 = dim[1], dim[2], dim[3]
+    npts = n1 * n2 * n3
+    vals = np.frombuffer(raw, dtype=np.dtype(_NIFTI_TYPES[datatype]).newbyteorder(end), count=npts,
+                         offset=vox_offset).astype(np.float64)
+    if slope != 0.0:
+        vals = vals * float(slope) + float(inter)
+    return VtkVolume((n1, n2, n3), tuple(float(p) for p in pixdim[1:4]), (0.0, 0.0, 0.0), vals, "nifti")
 
 
 def write_vtk_structured_points(path, volume: VtkVolume):

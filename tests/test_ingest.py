@@ -4,7 +4,8 @@ usr_func.f90:283-651, 899-945): the CT grid bit for bit on a synthetic volume wh
 both halves of the inlet plane (the column i = M1 / 2 belongs to the inlet and the first outlet,
 and the outlet fringe overwrites the inlet's), the label mask, the converted waveform and the
 inflow at table times, between them, before the first one and over several pulses; VTK files in
-ASCII and big-endian binary; and the errors for volumes that do not fit.
+ASCII and big-endian binary, NIfTI-1 volumes in either byte order, gzip-compressed and scaled;
+and the errors for volumes that do not fit.
 """
 import math
 import struct
@@ -135,3 +136,43 @@ def test_ingest_rejects_volumes_that_do_not_fit():
     with pytest.raises(ValueError):
         G.labels_from_ct_grid(np.zeros((5, 5, 5)), grid)
     assert math.isclose(G.inlet_radius(2.7, 0.2), math.sqrt(0.0004 / (math.pi * 2.7)) / 0.2)
+
+
+def _nifti_bytes(vals, dims, dtype_code, np_dtype, end, slope=0.0, inter=0.0, pixdim=(0.5, 0.6, 0.7)):
+    hdr = bytearray(352)
+    struct.pack_into(end + "i", hdr, 0, 348)
+    struct.pack_into(end + "8h", hdr, 40, 3, *dims, 1, 1, 1, 1)
+    struct.pack_into(end + "h", hdr, 70, dtype_code)
+    struct.pack_into(end + "h", hdr, 72, np.dtype(np_dtype).itemsize * 8)
+    struct.pack_into(end + "8f", hdr, 76, 1.0, *pixdim, 1.0, 1.0, 1.0, 1.0)
+    struct.pack_into(end + "f", hdr, 108, 352.0)
+    struct.pack_into(end + "2f", hdr, 112, slope, inter)
+    hdr[344:348] = b"n+1\0"
+    return bytes(hdr) + np.asarray(vals, dtype=np.dtype(np_dtype).newbyteorder(end)).tobytes()
+
+
+@pytest.mark.parametrize("end", ["<", ">"])
+@pytest.mark.parametrize("code,np_dtype", [(2, "u1"), (16, "f4"), (64, "f8"), (4, "i2")])
+def test_nifti_volume(tmp_path, end, code, np_dtype):
+    dims = (4, 3, 5)
+    vals = (np.arange(60) % 7).astype(np.float64)
+    p = tmp_path / "ct.nii"
+    p.write_bytes(_nifti_bytes(vals, dims, code, np_dtype, end))
+    v = G.read_nifti(p)
+    assert v.dims == dims and np.array_equal(v.values, vals)
+    assert v.spacing == pytest.approx((0.5, 0.6, 0.7))
+
+
+def test_nifti_gzip_and_scaling(tmp_path):
+    import gzip
+
+    vals = np.arange(24, dtype=np.float64)
+    p = tmp_path / "ct.nii.gz"
+    with gzip.open(p, "wb") as f:
+        f.write(_nifti_bytes(vals, (2, 3, 4), 4, "i2", "<", slope=0.5, inter=1.0))
+    v = G.read_nifti(p)
+    assert np.array_equal(v.values, vals * 0.5 + 1.0)
+    bad = tmp_path / "bad.nii"
+    bad.write_bytes(b"\0" * 400)
+    with pytest.raises(ValueError):
+        G.read_nifti(bad)
