@@ -7,6 +7,8 @@ case (Case.set_labels, Case.set_inflow_waveform).
     convert_waveform       usr_func.f90:599-651   convert_waveform
     apply_CT_forcing       usr_func.f90:909-1049  labels_from_ct_grid (its label tests),
                                                   inflow_velocity (its inflow lookup)
+    get_pressure_waveform_echo_WKM :653-750       windkessel_pressures (inlet / outlet pressure
+                                                  for pressure_bc_launcher_)
 
 Reference grid indices are 1-based and the CT grid is M1 x M2 x M3 (grid points per axis, the
 library's Grid.N); the library's grids are periodic with n = M - 1 unique points, so the label
@@ -317,3 +319,30 @@ def inflow_velocity(time: np.ndarray, velocity: np.ndarray, t: float):
         if time[i] <= ts <= time[i + 1]:
             u = float(velocity[i])
     return u
+
+
+def windkessel_pressures(table: np.ndarray, waveform: Waveform, t: float, r_in=0.78e6, c_in=2.166e-6,
+                         r_out=0.898e6, c_out=2.066e-6, q_max=Q_MAX, outlet_fraction=0.85, p0_mmhg=80.0,
+                         density=BLOOD_DENSITY):
+    """Inlet and outlet pressures at nondimensional time t from the echo waveform and a
+    two-element Windkessel model (get_pressure_waveform_echo_WKM, usr_func.f90:653-750; defaults:
+    the reference's TAVI 000 resistances and compliances).  For each table interval holding the
+    time shifted into the current pulse, starting from p0 = 80 mmHg:
+    p = p (1 - dt / (C R)) - dt / C q with dt the interval's length in seconds and q its start
+    velocity times the inlet area q_max / (peak velocity) (outlet: q_max x 0.85); the result is made
+    nondimensional by density x reference velocity^2 (mmHg -> Pa: 133.322).  These are the values
+    the reference's pressure boundary condition (pressure_bc_launcher_) receives."""
+    t_ms, vel = table[:, 0], table[:, 1]
+    length = float(waveform.time[-1])
+    ts = t - (math.floor(t / length) + 1.0 - 1.0) * length
+    vmax = float(np.max(vel))
+    out = []
+    for r, c, q in ((r_in, c_in, q_max), (r_out, c_out, q_max * outlet_fraction)):
+        area = q / vmax
+        p = p0_mmhg
+        for i in range(len(t_ms) - 1):
+            if waveform.time[i] <= ts <= waveform.time[i + 1]:
+                dt = t_ms[i + 1] / 1000.0 - t_ms[i] / 1000.0
+                p = p * (1.0 - dt / (c * r)) - dt / c * (vel[i] * area)
+        out.append(p / (density * waveform.reference_velocity ** 2.0) * 133.322)
+    return out[0], out[1]

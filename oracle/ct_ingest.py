@@ -11,6 +11,7 @@ checked against the reference's own output.
     converted     convert_waveform       usr_func.f90:599-651
     inflow        apply_CT_forcing       usr_func.f90:929-945, get_shifted_time_in_pulse :899-906,
                   get_pulse_number_and_length :753-760
+    windkessel    get_pressure_waveform_echo_WKM  usr_func.f90:653-750
 """
 from __future__ import annotations
 
@@ -117,3 +118,23 @@ def inflow(times, vels, t):
         if times[i] <= ts <= times[i + 1]:
             u = vels[i]
     return u
+
+
+def windkessel(table, times, u_ref, t):
+    """(pre_inlet, pre_outlet) of get_pressure_waveform_echo_WKM with its TAVI 000 constants."""
+    pulse_length = times[-1]
+    pulse_number = math.floor(t / pulse_length) + 1
+    ts = t - (pulse_number - 1) * pulse_length
+    vel_max = max(v for (_, v) in table)
+    res = []
+    for R, C, q_max in ((0.78 * 1000000., 2.166 / 1000000., 0.0004 * 1.0),
+                        (0.898 * 1000000., 2.066 / 1000000., 0.0004 * 0.85 * 1.0)):
+        inlet_area = q_max / vel_max
+        pre = 80.
+        for i in range(len(table) - 1):
+            if times[i] <= ts <= times[i + 1]:
+                dt = table[i + 1][0] / 1000. - table[i][0] / 1000.
+                q_in = table[i][1] * inlet_area
+                pre = pre * (1. - dt / (C * R)) - dt / C * q_in
+        res.append(pre / (1060. * u_ref ** 2.) * 133.322)
+    return res[0], res[1]

@@ -5,6 +5,7 @@ both halves of the inlet plane (the column i = M1 / 2 belongs to the inlet and t
 and the outlet fringe overwrites the inlet's), the label mask, the converted waveform and the
 inflow at table times, between them, before the first one and over several pulses; VTK files in
 ASCII and big-endian binary, NIfTI-1 volumes in either byte order, gzip-compressed and scaled;
+the Windkessel inlet and outlet pressures of get_pressure_waveform_echo_WKM (usr_func.f90:653-750);
 and the errors for volumes that do not fit.
 """
 import math
@@ -122,6 +123,9 @@ def test_waveform_conversion_and_lookup(tmp_path, idealized):
     assert G.inflow_velocity(w.time, w.velocity, 0.5 * times[0]) is None
     # at a table time the later interval wins
     assert G.inflow_velocity(w.time, w.velocity, times[3]) == vels[3]
+    # Windkessel pressures for the pressure boundary condition (two updates at a table time)
+    for t in probes:
+        assert G.windkessel_pressures(tab, w, t) == R.windkessel([tuple(r) for r in tab], times, u_ref, t), t
 
 
 def test_ingest_rejects_volumes_that_do_not_fit():
