@@ -35,3 +35,26 @@ def test_host_side_calls_without_gpu():
     g = I.Grid((17, 17, 17))
     assert g.tab["cdg"][0].shape == (3 * 17,)
     assert I.Case.bytes_needed((17, 17, 17), 0) > I.Case.bytes_needed((17, 17, 17), 1) > 0
+
+
+def test_case_entry_points_reject_a_null_case_without_touching_the_gpu():
+    """The case entry points added for transfers, snapshots and the inflow waveform validate their
+    arguments before any CUDA call: a null case is an error with a message, never a crash."""
+    import ctypes as C
+
+    L = I.lib()
+    buf = (C.c_double * 4)()
+    fields = (C.c_int * 1)(0)
+    ptrs = (C.POINTER(C.c_double) * 1)(buf)
+    calls = [
+        ("impact_b200_case_upload_async", lambda: L.impact_b200_case_upload_async(None, 0, buf, 0, 1, None)),
+        ("impact_b200_case_download_async", lambda: L.impact_b200_case_download_async(None, 0, buf, 0, 1, None)),
+        ("impact_b200_case_defer_pressure", lambda: L.impact_b200_case_defer_pressure(None, None)),
+        ("impact_b200_case_set_inflow_waveform",
+         lambda: L.impact_b200_case_set_inflow_waveform(None, 2, buf, buf)),
+        ("impact_b200_case_snapshot", lambda: L.impact_b200_case_snapshot(None, 1, fields, ptrs, None)),
+        ("impact_b200_case_synchronize", lambda: L.impact_b200_case_synchronize(None)),
+    ]
+    for name, call in calls:
+        assert call() != 0, name
+        assert name in I.last_error(), (name, I.last_error())
