@@ -65,6 +65,20 @@ struct CaseState {
   // measured inflow waveform (nondimensional time, velocity); empty: the sinusoidal inflow
   std::vector<double> inflow_t, inflow_u;
   bool pooled = false;  // allocs come from the per-device case pool (freed stream-ordered)
+  // global coordinates over -3..N+3 per axis (host copies; empty when the case was created
+  // without them)
+  std::vector<double> xp[3], xu[3];
+  // immersed-boundary markers (impact_b200_case_set_markers), device side
+  struct {
+    int n = 0, cap = 0, type = 0;
+    double reach = 0.0;
+    bool has_skip = false;
+    double* geom = nullptr;   // per axis: xp, xu, dxp, dxu over the points 0..N-1 (0 unused)
+    double* yb = nullptr;     // positions, column-major (cap, 3)
+    uint8_t* skip = nullptr;  // cap flags
+    double* buf = nullptr;    // 4 cap: marker velocities, or forces and node volumes
+    int* flag = nullptr;      // set by a kernel that met a support wider than its limit
+  } ibm;
 };
 
 }  // namespace impact
@@ -72,3 +86,6 @@ struct CaseState {
 struct impact_b200_case {
   impact::CaseState s;
 };
+
+// Device memory owned by the case (freed with it), from the per-device case pool.
+int case_alloc(impact::CaseState& s, void** p, size_t bytes);

@@ -338,7 +338,7 @@ static cudaMemPool_t case_pool(int dev) {
   return pools[dev];
 }
 
-static int case_alloc(CaseState& s, void** p, size_t bytes) {
+int case_alloc(CaseState& s, void** p, size_t bytes) {
   cudaMemPool_t pool = case_pool(s.device);
   cudaError_t e = pool ? cudaMallocFromPoolAsync(p, bytes, pool, s.stream) : cudaMalloc(p, bytes);
   // usable by any stream and by the synchronous copies of case creation from here on
@@ -546,6 +546,10 @@ extern "C" int impact_b200_case_create(const impact_b200_case_desc* desc, const 
   // ---- multigrid hierarchy ----
   if (co->xp[0] && co->xp[1] && co->xp[2] && co->xu[0] && co->xu[1] && co->xu[2]) {
     const int N[3] = {desc->N1, desc->N2, desc->N3};
+    for (int a = 0; a < 3; ++a) {
+      s.xp[a].assign(co->xp[a], co->xp[a] + N[a] + 7);
+      s.xu[a].assign(co->xu[a], co->xu[a] + N[a] + 7);
+    }
     std::vector<MGHostLevel> lv = build_mg_hierarchy(N, co->xp, co->xu, co->L, MG_MAX_LEVELS);
     s.mg_levels = (int)lv.size();
     // tables of every level in one FP64 and one FP32 allocation

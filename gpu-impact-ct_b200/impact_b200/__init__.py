@@ -107,6 +107,9 @@ def lib():
         "impact_b200_case_snapshot": (i, [_vp, i, C.POINTER(i), C.POINTER(_dp), _vp]),
         "impact_b200_case_synchronize": (i, [_vp]),
         "impact_b200_case_set_labels": (i, [_vp, _u8p]),
+        "impact_b200_case_set_markers": (i, [_vp, i, _dp, _u8p, C.c_double, i]),
+        "impact_b200_case_ibm_interpolate": (i, [_vp, _dp]),
+        "impact_b200_case_ibm_spread": (i, [_vp, _dp, _dp, i]),
         "impact_b200_case_field_ptr": (_vp, [_vp, i]),
         "impact_b200_case_stream": (_vp, [_vp]),
         "impact_b200_case_poisson": (i, [_vp, i, i, P(SolverParams), P(SolverResult)]),
@@ -343,6 +346,40 @@ class Case:
         if t.ndim != 1 or t.shape != u.shape:
             raise ValueError("set_inflow_waveform: time and velocity must be 1-D arrays of one length")
         check(lib().impact_b200_case_set_inflow_waveform(self._h, t.size, _ptr(t), _ptr(u)), "case_set_inflow_waveform")
+
+    def set_markers(self, yb, reach, delta_type=2, skip=None):
+        """Immersed-boundary markers at positions yb (n, 3); skip: n flags of excluded markers;
+        delta_type 1 cosine, 2 hat, 3 and 4 piecewise kernels of half-width reach / 2."""
+        y = np.asarray(yb, dtype=np.float64)
+        if y.ndim != 2 or y.shape[1] != 3:
+            raise ValueError("set_markers: positions must be an (n, 3) array")
+        self._markers = y.shape[0]
+        flat = np.ascontiguousarray(y.T)
+        sk = None
+        if skip is not None:
+            sk = np.ascontiguousarray(skip, dtype=np.uint8)
+            if sk.shape != (y.shape[0],):
+                raise ValueError("set_markers: one skip flag per marker")
+            sk = sk.ctypes.data_as(_u8p)
+        check(lib().impact_b200_case_set_markers(self._h, y.shape[0], _ptr(flat), sk, float(reach), int(delta_type)),
+              "case_set_markers")
+
+    def ibm_interpolate(self) -> np.ndarray:
+        """Velocity of the resident fields at the markers, (n, 3)."""
+        n = getattr(self, "_markers", 0)
+        ub = np.zeros((3, n))
+        check(lib().impact_b200_case_ibm_interpolate(self._h, _ptr(ub)), "case_ibm_interpolate")
+        return ub.T.copy()
+
+    def ibm_spread(self, fb, node_vol, into="rhs"):
+        """Force density of the marker forces fb (n, 3) with node volumes node_vol (n,) into the
+        fields rhs1..3 (into="rhs") or nl1..3 (into="nl"); returns the first field's name."""
+        n = getattr(self, "_markers", 0)
+        f = np.ascontiguousarray(np.asarray(fb, dtype=np.float64).reshape(n, 3).T)
+        vol = np.ascontiguousarray(node_vol, dtype=np.float64).reshape(n)
+        first = {"rhs": FIELDS["rhs1"], "nl": FIELDS["nl1"]}[into]
+        check(lib().impact_b200_case_ibm_spread(self._h, _ptr(f), _ptr(vol), first), "case_ibm_spread")
+        return into + "1"
 
     def set_labels(self, labels: np.ndarray):
         lb = np.ascontiguousarray(labels, dtype=np.uint8)

@@ -192,6 +192,24 @@ int impact_b200_case_defer_pressure(impact_b200_case* c, void* event);
  * start of the last table interval that holds it (none does: they keep their velocity).  n = 0
  * restores the default inflow U0 (1 + sin(2 pi t / T_pulse) / 2). */
 int impact_b200_case_set_inflow_waveform(impact_b200_case* c, int n, const double* time, const double* velocity);
+/* Diffuse-interface immersed boundary (mod_ibm.f90).  n Lagrangian markers at positions yb, a
+ * column-major (n, 3) array (all x, then all y, then all z: the reference's yb(1:M_bound, 1:3)),
+ * in the units of the case's coordinates; skip[i] != 0 excludes marker i (its index is listed in
+ * ebcs(:, 1)), skip = NULL excludes none.  delta_type 1..4 and reach are ddf_type and reach of
+ * discrete_delta (mod_ibm.f90:2021-2075); a reach whose vicinity could span more than 16 points
+ * of an axis is rejected.  The case must have been created with coordinates (xp, xu). */
+int impact_b200_case_set_markers(impact_b200_case* c, int n, const double* yb, const uint8_t* skip, double reach,
+                                 int delta_type);
+/* interpolate_vel_to_ib (mod_ibm.f90:589-737): ub (host, column-major (n, 3)) = the velocity of
+ * the resident fields at every marker, the sum of delta * u * cell volume over its vicinity on
+ * each component's staggered grid; skipped markers get 0.  Returns when ub is written. */
+int impact_b200_case_ibm_interpolate(impact_b200_case* c, double* ub);
+/* spread_force_dens_to_vel_grid (mod_ibm.f90:428-583): the three fields field_first..+2
+ * (IMPACT_B200_NL1 or IMPACT_B200_RHS1) are zeroed and receive the force density of the marker
+ * forces fb (host, column-major (n, 3)) times the node volumes node_vol (host, n) spread with the
+ * delta kernel.  The additions of overlapping supports are atomic, so the order of the sum at a
+ * point is not fixed. */
+int impact_b200_case_ibm_spread(impact_b200_case* c, const double* fb, const double* node_vol, int field_first);
 /* voxel labels (padded layout, one byte per point): 0 solid, 1 fluid, 5 inflow, 7 wall, 9/11 outlets */
 int impact_b200_case_set_labels(impact_b200_case* c, const uint8_t* host_labels);
 double* impact_b200_case_field_ptr(impact_b200_case* c, int field);

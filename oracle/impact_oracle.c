@@ -1148,3 +1148,179 @@ void orc_time_step(int N1, int N2, int N3, const orc_coeffs* c, const orc_step_p
   orc_mask_forcing(N1, N2, N3, label, u_in, vel);
   if (p->level_pressure) orc_level_pressure(N1, N2, N3, pre);
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* diffuse-interface immersed boundary transfers (mod_ibm.f90)                            */
+/* ------------------------------------------------------------------------------------ */
+
+/* discrete_delta (mod_ibm.f90:2021-2075).  pi = 2 |acos(0)| (FP64: the reference builds with
+ * -fdefault-real-8).  A distance past the reach -- the reference's sentinel L1*L2*L3 for an
+ * empty vicinity among them -- gives 0. */
+double orc_ibm_delta(int type, double reach, double distance) {
+  const double pi = 2.0 * fabs(acos(0.0));
+  const double ad = fabs(distance);
+  double delta = 0.0;
+  if (type == 1) {
+    if (ad <= reach) delta = (1.0 + cos(pi * ad / reach)) / (2.0 * reach);
+  } else if (type == 2) {
+    if (ad <= reach) delta = (reach - ad) / (reach * reach);
+  } else if (type == 3) {
+    if (ad <= reach / 2.0) {
+      const double q = distance / (reach / 2.0);
+      delta = (1.0 - q * q) / (reach / 2.0);
+    } else if (ad > reach / 2.0 && ad <= reach) {
+      const double q = distance / (reach / 2.0);
+      delta = (2.0 - fabs(3.0 * distance / (reach / 2.0)) + q * q) / (reach / 2.0);
+    }
+  } else if (type == 4) {
+    if (ad <= reach / 2.0) {
+      const double t = ad / (reach / 2.0);
+      delta = (3.0 - 2.0 * ad / (reach / 2.0) + sqrt(1.0 + 4.0 * ad / (reach / 2.0) - 4.0 * (t * t))) / (4.0 * reach);
+    } else if (ad > reach / 2.0 && ad <= reach) {
+      const double t = ad / (reach / 2.0);
+      delta = (5.0 - 2.0 * ad / (reach / 2.0) - sqrt(-7.0 + 12.0 * ad / (reach / 2.0) - 4.0 * (t * t))) / (4.0 * reach);
+    }
+  }
+  return delta;
+}
+
+/* find_vicinity_coordinates (mod_ibm.f90:743-876) along one axis: the first point of S..N
+ * within the reach of y, and the last one before the first point beyond it; -1 / -1 when no
+ * point is within reach.  x is a coordinate array over -3..N+3 (C offset 3). */
+static void ibm_vicinity(const double* x, int S, int N, double y, double reach, int ind[2]) {
+  ind[0] = ind[1] = -1;
+  for (int i = S; i <= N; i++) {
+    if (fabs(y - x[i + 3]) <= reach) {
+      ind[0] = i;
+      for (int j = i; j <= N; j++) {
+        if (x[j + 3] - y > reach) {
+          ind[1] = j - 1;
+          return;
+        } else if (j == N) {
+          ind[1] = j;
+          return;
+        }
+      }
+    }
+  }
+}
+
+/* The cell widths of mod_geometry.f90:193-204 on a periodic axis: dxp(i) = xu(i) - xu(i-1),
+ * dxu(i) = xp(i+1) - xp(i), i = 1..N-1 (index i at offset i). */
+static void ibm_widths(const double* xp, const double* xu, int N, double* dxp, double* dxu) {
+  for (int i = 1; i <= N - 1; i++) {
+    dxp[i] = xu[i + 3] - xu[i - 1 + 3];
+    dxu[i] = xp[i + 1 + 3] - xp[i + 3];
+  }
+}
+
+/* Shared walk of interpolate_vel_to_ib and spread_force_dens_to_vel_grid: for marker m and
+ * velocity component c (0..2) the vicinity of every axis -- on the velocity grid xu along
+ * axis c, on the pressure grid xp along the others -- and the distances yb - x.  Returns 0
+ * when an axis has no point within reach: the reference then loops over the single index -1
+ * with the sentinel distance, whose weight is 0, so every term it adds is a zero (it reads
+ * vel(-1) and dx(-1) there, outside the interior); the restatement skips those terms. */
+typedef struct {
+  int lo[3], hi[3];
+  double* dist[3];
+  const double* dx[3];
+} ibm_walk;
+
+static int ibm_setup(const double* const* xp, const double* const* xu, double* const* dxp, double* const* dxu,
+                     const int* N, double reach, int n, const double* yb, int m, int c, ibm_walk* w) {
+  for (int a = 0; a < 3; a++) {
+    const double* x = (a == c) ? xu[a] : xp[a];
+    int ind[2];
+    const double y = yb[(size_t)a * n + m];
+    ibm_vicinity(x, 1, N[a] - 1, y, reach, ind);
+    if (ind[0] == -1) return 0;
+    w->lo[a] = ind[0];
+    w->hi[a] = ind[1];
+    for (int i = ind[0]; i <= ind[1]; i++) w->dist[a][i - ind[0]] = y - x[i + 3];
+    w->dx[a] = (a == c) ? dxu[a] : dxp[a];
+  }
+  return 1;
+}
+
+static void ibm_alloc(const int* N, double** dxp, double** dxu, double** dist) {
+  for (int a = 0; a < 3; a++) {
+    dxp[a] = (double*)calloc((size_t)N[a] + 1, sizeof(double));
+    dxu[a] = (double*)calloc((size_t)N[a] + 1, sizeof(double));
+    dist[a] = (double*)calloc((size_t)N[a] + 1, sizeof(double));
+  }
+}
+static void ibm_free(double** dxp, double** dxu, double** dist) {
+  for (int a = 0; a < 3; a++) {
+    free(dxp[a]);
+    free(dxu[a]);
+    free(dist[a]);
+  }
+}
+
+/* interpolate_vel_to_ib (mod_ibm.f90:589-737), one block: ub(i, c) = sum over l, k, j of
+ * delta(d1) * delta(d2) * delta(d3) * vel(j, k, l, c) * dx1(j) * dx2(k) * dx3(l), in that order. */
+void orc_ibm_interpolate(int N1, int N2, int N3, const double* const* xp, const double* const* xu,
+                         const double* L, int delta_type, double reach, int n, const double* yb,
+                         const uint8_t* skip, const double* vel, double* ub) {
+  (void)L;
+  dims_t d = mkdims(N1, N2, N3);
+  const size_t fs = field_size(&d);
+  const int N[3] = {N1, N2, N3};
+  double *dxp[3], *dxu[3], *dist[3];
+  ibm_alloc(N, dxp, dxu, dist);
+  for (int a = 0; a < 3; a++) ibm_widths(xp[a], xu[a], N[a], dxp[a], dxu[a]);
+  for (size_t q = 0; q < (size_t)3 * n; q++) ub[q] = 0.0;
+  for (int m = 0; m < n; m++) {
+    if (skip && skip[m]) continue;
+    for (int c = 0; c < 3; c++) {
+      ibm_walk w;
+      for (int a = 0; a < 3; a++) w.dist[a] = dist[a];
+      if (!ibm_setup(xp, xu, dxp, dxu, N, reach, n, yb, m, c, &w)) continue;
+      double* u = &ub[(size_t)c * n + m];
+      for (int l = w.lo[2]; l <= w.hi[2]; l++)
+        for (int k = w.lo[1]; k <= w.hi[1]; k++)
+          for (int j = w.lo[0]; j <= w.hi[0]; j++)
+            *u = *u + orc_ibm_delta(delta_type, reach, w.dist[0][j - w.lo[0]]) *
+                          orc_ibm_delta(delta_type, reach, w.dist[1][k - w.lo[1]]) *
+                          orc_ibm_delta(delta_type, reach, w.dist[2][l - w.lo[2]]) *
+                          vel[(size_t)c * fs + IX(&d, j, k, l)] * w.dx[0][j] * w.dx[1][k] * w.dx[2][l];
+    }
+  }
+  ibm_free(dxp, dxu, dist);
+}
+
+/* spread_force_dens_to_vel_grid (mod_ibm.f90:428-583), one block: fd = 0, then
+ * fd(j, k, l, c) += fb(i, c) * delta(d1) * delta(d2) * delta(d3) * node_vol(i) over the markers in
+ * order.  The exchange_part calls that follow add the ghost planes 0 and N into the planes 1
+ * and N-1 (mod_exchange.f90:1565-1568); those ghost planes hold zeros here (the vicinity search
+ * visits only the points 1..N-1), so they change nothing and are not restated. */
+void orc_ibm_spread(int N1, int N2, int N3, const double* const* xp, const double* const* xu, const double* L,
+                    int delta_type, double reach, int n, const double* yb, const uint8_t* skip,
+                    const double* fb, const double* node_vol, double* fd) {
+  (void)L;
+  dims_t d = mkdims(N1, N2, N3);
+  const size_t fs = field_size(&d);
+  const int N[3] = {N1, N2, N3};
+  double *dxp[3], *dxu[3], *dist[3];
+  ibm_alloc(N, dxp, dxu, dist);
+  for (int a = 0; a < 3; a++) ibm_widths(xp[a], xu[a], N[a], dxp[a], dxu[a]);
+  memset(fd, 0, 3 * fs * sizeof(double));
+  for (int m = 0; m < n; m++) {
+    if (skip && skip[m]) continue;
+    for (int c = 0; c < 3; c++) {
+      ibm_walk w;
+      for (int a = 0; a < 3; a++) w.dist[a] = dist[a];
+      if (!ibm_setup(xp, xu, dxp, dxu, N, reach, n, yb, m, c, &w)) continue;
+      const double f = fb[(size_t)c * n + m];
+      for (int l = w.lo[2]; l <= w.hi[2]; l++)
+        for (int k = w.lo[1]; k <= w.hi[1]; k++)
+          for (int j = w.lo[0]; j <= w.hi[0]; j++) {
+            double* p = &fd[(size_t)c * fs + IX(&d, j, k, l)];
+            *p = *p + f * orc_ibm_delta(delta_type, reach, w.dist[0][j - w.lo[0]]) *
+                          orc_ibm_delta(delta_type, reach, w.dist[1][k - w.lo[1]]) *
+                          orc_ibm_delta(delta_type, reach, w.dist[2][l - w.lo[2]]) * node_vol[m];
+          }
+    }
+  }
+  ibm_free(dxp, dxu, dist);
+}

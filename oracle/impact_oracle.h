@@ -214,6 +214,22 @@ void orc_bicgstab_mg(int N1, int N2, int N3, const orc_coeffs* c, const orc_mg* 
                      int n_down, int n_up, int n_bottom, double* bb, double* phi, double* work,
                      orc_solver_result* res);
 
+/* ---------------- diffuse-interface immersed boundary transfers (mod_ibm.f90), periodic ----------
+ * n Lagrangian markers; yb, ub, fb are column-major (n, 3) arrays (all x, then all y, then all z:
+ * the reference's yb(1:M_bound, 1:3)).  skip[i] != 0 excludes marker i (its index is in
+ * ebcs(:, 1)).  xp / xu are the global coordinates over -3..N+3 per axis, L the box lengths.
+ * delta_type 1..4 and reach as ddf_type and reach of the reference. */
+double orc_ibm_delta(int delta_type, double reach, double distance);
+/* interpolate_vel_to_ib (mod_ibm.f90:589-737): ub = sum of delta * vel * cell volume, per component */
+void orc_ibm_interpolate(int N1, int N2, int N3, const double* const* xp, const double* const* xu,
+                         const double* L, int delta_type, double reach, int n, const double* yb,
+                         const uint8_t* skip, const double* vel, double* ub);
+/* spread_force_dens_to_vel_grid (mod_ibm.f90:428-583): fd (three padded fields) = 0, then the
+ * delta-weighted marker forces times node volumes */
+void orc_ibm_spread(int N1, int N2, int N3, const double* const* xp, const double* const* xu, const double* L,
+                    int delta_type, double reach, int n, const double* yb, const uint8_t* skip,
+                    const double* fb, const double* node_vol, double* fd);
+
 #ifdef __cplusplus
 }
 #endif

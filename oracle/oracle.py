@@ -105,6 +105,9 @@ def lib():
                                        P(OrcSolverResult)]),
             "orc_mask_forcing": (None, [i, i, i, _u8p, d, _dp]),
             "orc_level_pressure": (None, [i, i, i, _dp]),
+            "orc_ibm_delta": (d, [i, d, d]),
+            "orc_ibm_interpolate": (None, [i, i, i, P(_dp), P(_dp), _dp, i, d, i, _dp, _u8p, _dp, _dp]),
+            "orc_ibm_spread": (None, [i, i, i, P(_dp), P(_dp), _dp, i, d, i, _dp, _u8p, _dp, _dp, _dp]),
             "orc_time_step": (None, [i, i, i, P(OrcCoeffs), P(OrcStepParams), _dp, _u8p, _dp,
                                      _dp, _dp, _dp, P(OrcStepState)]),
         }
@@ -241,6 +244,36 @@ class Grid:
         out = self.zeros() if out is None else out
         lib().orc_interpolate_vel_pre(m, *self.N, C.byref(self.c), ptr(phi), ptr(out))
         return out
+
+    # ---- immersed boundary transfers (mod_ibm.f90) ----
+    def _ibm_args(self, yb, skip):
+        yb = np.asfortranarray(yb, dtype=np.float64)
+        n = yb.shape[0]
+        flat = np.ascontiguousarray(yb.T)  # (3, n): all x, then all y, then all z
+        sk = None if skip is None else np.ascontiguousarray(skip, dtype=np.uint8)
+        xp = (_dp * 3)(*[ptr(a) for a in self.xp])
+        xu = (_dp * 3)(*[ptr(a) for a in self.xu])
+        L = np.array(self.L)
+        return n, flat, sk, xp, xu, L
+
+    def ibm_interpolate(self, yb, vel, delta_type, reach, skip=None):
+        """interpolate_vel_to_ib: marker velocities (n, 3) from the velocity fields vel (3, shape)."""
+        n, flat, sk, xp, xu, L = self._ibm_args(yb, skip)
+        vel = np.ascontiguousarray(vel, dtype=np.float64)
+        ub = np.zeros((3, n))
+        lib().orc_ibm_interpolate(*self.N, xp, xu, ptr(L), delta_type, reach, n, ptr(flat),
+                                  None if sk is None else u8ptr(sk), ptr(vel), ptr(ub))
+        return ub.T.copy()
+
+    def ibm_spread(self, yb, fb, node_vol, delta_type, reach, skip=None):
+        """spread_force_dens_to_vel_grid: force density fields (3, shape) from marker forces (n, 3)."""
+        n, flat, sk, xp, xu, L = self._ibm_args(yb, skip)
+        f = np.ascontiguousarray(np.asarray(fb, dtype=np.float64).T)
+        vol = np.ascontiguousarray(node_vol, dtype=np.float64)
+        fd = self.zeros(3)
+        lib().orc_ibm_spread(*self.N, xp, xu, ptr(L), delta_type, reach, n, ptr(flat),
+                             None if sk is None else u8ptr(sk), ptr(f), ptr(vol), ptr(fd))
+        return fd
 
     def nonlinear_upwind(self, cid, pp, vel, nl):
         lib().orc_nonlinear_upwind(cid, *self.N, C.byref(self.c), ptr(pp), ptr(vel), ptr(nl))

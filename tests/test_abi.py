@@ -54,6 +54,9 @@ def test_case_entry_points_reject_a_null_case_without_touching_the_gpu():
          lambda: L.impact_b200_case_set_inflow_waveform(None, 2, buf, buf)),
         ("impact_b200_case_snapshot", lambda: L.impact_b200_case_snapshot(None, 1, fields, ptrs, None)),
         ("impact_b200_case_synchronize", lambda: L.impact_b200_case_synchronize(None)),
+        ("impact_b200_case_set_markers", lambda: L.impact_b200_case_set_markers(None, 1, buf, None, 0.1, 2)),
+        ("impact_b200_case_ibm_interpolate", lambda: L.impact_b200_case_ibm_interpolate(None, buf)),
+        ("impact_b200_case_ibm_spread", lambda: L.impact_b200_case_ibm_spread(None, buf, buf, 8)),
     ]
     for name, call in calls:
         assert call() != 0, name
