@@ -353,7 +353,6 @@ class Case:
         y = np.asarray(yb, dtype=np.float64)
         if y.ndim != 2 or y.shape[1] != 3:
             raise ValueError("set_markers: positions must be an (n, 3) array")
-        self._markers = y.shape[0]
         flat = np.ascontiguousarray(y.T)
         sk = None
         if skip is not None:
@@ -363,6 +362,7 @@ class Case:
             sk = sk.ctypes.data_as(_u8p)
         check(lib().impact_b200_case_set_markers(self._h, y.shape[0], _ptr(flat), sk, float(reach), int(delta_type)),
               "case_set_markers")
+        self._markers = y.shape[0]  # only once the library holds this set
 
     def ibm_interpolate(self) -> np.ndarray:
         """Velocity of the resident fields at the markers, (n, 3)."""

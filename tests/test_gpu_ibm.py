@@ -100,4 +100,6 @@ def test_empty_and_growing_marker_sets():
         case.set_markers(_markers(4, 1), 1.0, 2)  # a window of 2.0 holds all 20 points along z
     with pytest.raises(I.ImpactError):
         case.set_markers(_markers(4, 1), REACH, 5)  # no such delta kernel
+    # a rejected set leaves the previous one in place
+    assert np.array_equal(case.ibm_interpolate(), og.ibm_interpolate(_markers(50, 50), vel, 2, REACH))
     case.close()
