@@ -348,17 +348,23 @@ __global__ void __launch_bounds__(1024) k_jor_check_fin(const double* __restrict
 }
 }  // namespace
 
-extern "C" int impact_b200_jacobi_solve(int N1, int N2, int N3, int M1, int M2, int M3, double omega,
-                                        const double* cdg1, const double* cdg2, const double* cdg3, double* rel,
-                                        const double* bb, int mode_j, double tol_abs_inf, int max_sweeps, int* sweeps,
-                                        double* res_inf) {
-  if (N1 < 9 || N2 < 9 || N3 < 9 || !cdg1 || !cdg2 || !cdg3 || !rel || !bb || mode_j < 1 || max_sweeps < 1)
-    return impact_set_error_msg(-1, "impact_b200_jacobi_solve: bad arguments");
+namespace {
+// Labels and values of the CT pressure boundary condition applied inside the JOR loop.
+struct JorBc {
+  const uint8_t* labels;  // host, padded layout; nullptr: none
+  int k_start_index, t1, t2, t3;
+  double p_in, p_out, p_out2;
+};
+
+int jacobi_solve_impl(int N1, int N2, int N3, int M1, int M2, int M3, double omega, const double* cdg1,
+                      const double* cdg2, const double* cdg3, double* rel, const double* bb, int mode_j,
+                      double tol_abs_inf, int max_sweeps, int* sweeps, double* res_inf, const JorBc& bc) {
   const Geom g = make_geom(N1, N2, N3);
   const size_t fb = (size_t)g.nfield * sizeof(double);
   const dim3 gr((g.n1 + BX - 1) / BX, (g.n2 + BY - 1) / BY, g.n3), bl(BX, BY);
   const long long nb = (long long)gr.x * gr.y * gr.z;
   double *d_rel = nullptr, *d_tmp = nullptr, *d_bb = nullptr, *d_old = nullptr, *d_c = nullptr, *d_part = nullptr;
+  uint8_t* d_lab = nullptr;
   cudaStream_t s = g_stream;
   int rc = 0;
   auto fail = [&](cudaError_t e, const char* w) {
@@ -370,6 +376,7 @@ extern "C" int impact_b200_jacobi_solve(int N1, int N2, int N3, int M1, int M2, 
   if (e == cudaSuccess) e = cudaMalloc(&d_old, fb);
   if (e == cudaSuccess) e = cudaMalloc(&d_c, 3 * sizeof(double) * (N1 + N2 + N3));
   if (e == cudaSuccess) e = cudaMalloc(&d_part, (2 * nb + 8) * sizeof(double));
+  if (e == cudaSuccess && bc.labels) e = cudaMalloc(&d_lab, (size_t)g.nfield);
   if (e != cudaSuccess) fail(e, "impact_b200_jacobi_solve alloc");
   const double pi_ref = 3.1415;  // the constant of the reference's stop test (jacobi_solver_host_v4.f90:383)
   const double thresh =
@@ -384,6 +391,7 @@ extern "C" int impact_b200_jacobi_solve(int N1, int N2, int N3, int M1, int M2, 
     cudaMemcpyAsync(d_c, cdg1, 3 * sizeof(double) * N1, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d_c + 3 * N1, cdg2, 3 * sizeof(double) * N2, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d_c + 3 * (N1 + N2), cdg3, 3 * sizeof(double) * N3, cudaMemcpyHostToDevice, s);
+    if (d_lab) cudaMemcpyAsync(d_lab, bc.labels, (size_t)g.nfield, cudaMemcpyHostToDevice, s);
     const double* c1 = d_c;
     const double* c2 = d_c + 3 * N1;
     const double* c3 = d_c + 3 * (N1 + N2);
@@ -391,6 +399,9 @@ extern "C" int impact_b200_jacobi_solve(int N1, int N2, int N3, int M1, int M2, 
     bool have_old = false;
     double h[2];
     for (int iter = 1; iter <= max_sweeps; ++iter) {
+      // the boundary values first, before the stop test and the sweep of this iteration
+      if (d_lab)
+        launch_pressure_bc(g, bc.t1, bc.t2, bc.t3, bc.k_start_index, bc.p_in, bc.p_out, bc.p_out2, d_lab, d_rel, s);
       if (iter % mode_j == 1 || mode_j == 1) {
         k_jor_check<<<gr, bl, 0, s>>>(g, c1, c2, c3, d_rel, d_bb, d_old, d_part);
         k_jor_check_fin<<<1, 1024, 0, s>>>(d_part, nb, d_part + 2 * nb);
@@ -425,9 +436,36 @@ extern "C" int impact_b200_jacobi_solve(int N1, int N2, int N3, int M1, int M2, 
   cudaFree(d_old);
   cudaFree(d_c);
   cudaFree(d_part);
+  cudaFree(d_lab);
   if (sweeps) *sweeps = done_sweeps;
   if (res_inf) *res_inf = last_res;
   return rc;
+}
+}  // namespace
+
+extern "C" int impact_b200_jacobi_solve(int N1, int N2, int N3, int M1, int M2, int M3, double omega,
+                                        const double* cdg1, const double* cdg2, const double* cdg3, double* rel,
+                                        const double* bb, int mode_j, double tol_abs_inf, int max_sweeps, int* sweeps,
+                                        double* res_inf) {
+  if (N1 < 9 || N2 < 9 || N3 < 9 || !cdg1 || !cdg2 || !cdg3 || !rel || !bb || mode_j < 1 || max_sweeps < 1)
+    return impact_set_error_msg(-1, "impact_b200_jacobi_solve: bad arguments");
+  const JorBc none{nullptr, 0, 0, 0, 0, 0.0, 0.0, 0.0};
+  return jacobi_solve_impl(N1, N2, N3, M1, M2, M3, omega, cdg1, cdg2, cdg3, rel, bb, mode_j, tol_abs_inf, max_sweeps,
+                           sweeps, res_inf, none);
+}
+
+extern "C" int impact_b200_jacobi_solve_bc(int N1, int N2, int N3, int M1, int M2, int M3, double omega,
+                                           const double* cdg1, const double* cdg2, const double* cdg3, double* rel,
+                                           const double* bb, int mode_j, double tol_abs_inf, int max_sweeps,
+                                           int* sweeps, double* res_inf, const uint8_t* labels, int k_start_index,
+                                           int type_id1, int type_id2, int type_id3, double p_inlet,
+                                           double p_outlet, double p_outlet_2) {
+  if (N1 < 9 || N2 < 9 || N3 < 9 || !cdg1 || !cdg2 || !cdg3 || !rel || !bb || mode_j < 1 || max_sweeps < 1 ||
+      !labels)
+    return impact_set_error_msg(-1, "impact_b200_jacobi_solve_bc: bad arguments");
+  const JorBc bc{labels, k_start_index, type_id1, type_id2, type_id3, p_inlet, p_outlet, p_outlet_2};
+  return jacobi_solve_impl(N1, N2, N3, M1, M2, M3, omega, cdg1, cdg2, cdg3, rel, bb, mode_j, tol_abs_inf, max_sweeps,
+                           sweeps, res_inf, bc);
 }
 
 extern "C" int impact_b200_product_scalar(int N1, int N2, int N3, const double* a_dev, const double* b_dev,

@@ -123,6 +123,8 @@ def lib():
         "impact_b200_batch_stream": (_vp, [_vp]),
         "impact_b200_case_mg_levels": (i, [_vp]),
         "impact_b200_jacobi_solve": (i, [i, i, i, i, i, i, d, _dp, _dp, _dp, _dp, _dp, i, d, i, _ip, _dp]),
+        "impact_b200_jacobi_solve_bc": (i, [i, i, i, i, i, i, d, _dp, _dp, _dp, _dp, _dp, i, d, i, _ip, _dp,
+                                            _u8p, i, i, i, i, d, d, d]),
         "impact_b200_product_scalar": (i, [i, i, i, _vp, _vp, _dp]),
         "impact_b200_product_scalar_noalloc": (i, [i, i, i, _vp, _vp, _dp]),
         "impact_b200_profile_enable": (None, [i]),
@@ -523,15 +525,25 @@ def product_scalar_noalloc(N, a_dev: int, b_dev: int) -> float:
 
 
 def jacobi_solve(grid: Grid, rel: np.ndarray, bb: np.ndarray, omega=0.8, mode_j=20, tol_abs_inf=0.0,
-                 max_sweeps=100000, M=None):
-    """device_jacobi_solver replacement on host arrays; returns (sweeps, res_inf)."""
+                 max_sweeps=100000, M=None, labels=None, k_start_index=0, type_ids=(1, 1, 0),
+                 pressures=(0.0, 0.0, 0.0)):
+    """device_jacobi_solver replacement on host arrays; returns (sweeps, res_inf).  With labels,
+    the CT pressure condition of the third substep is applied at the start of every iteration
+    (pressures: inlet, outlet, second outlet, already multiplied by (aRK + bRK) dt)."""
     N1, N2, N3 = grid.N
     M1, M2, M3 = M if M is not None else grid.N
     sw, ri = C.c_int(), C.c_double()
     c = grid.tab["cdg"]
-    check(lib().impact_b200_jacobi_solve(N1, N2, N3, M1, M2, M3, omega, _ptr(c[0]), _ptr(c[1]), _ptr(c[2]),
-                                         _ptr(rel), _ptr(bb), mode_j, tol_abs_inf, max_sweeps, C.byref(sw),
-                                         C.byref(ri)), "jacobi_solve")
+    args = (N1, N2, N3, M1, M2, M3, omega, _ptr(c[0]), _ptr(c[1]), _ptr(c[2]), _ptr(rel), _ptr(bb), mode_j,
+            tol_abs_inf, max_sweeps, C.byref(sw), C.byref(ri))
+    if labels is None:
+        check(lib().impact_b200_jacobi_solve(*args), "jacobi_solve")
+    else:
+        lb = np.ascontiguousarray(labels, dtype=np.uint8)
+        if lb.shape != grid.shape:
+            raise ValueError("jacobi_solve: labels must have the padded field shape")
+        check(lib().impact_b200_jacobi_solve_bc(*args, lb.ctypes.data_as(_u8p), k_start_index, *type_ids,
+                                                *pressures), "jacobi_solve_bc")
     return sw.value, ri.value
 
 

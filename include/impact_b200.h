@@ -306,6 +306,17 @@ void* impact_b200_batch_stream(impact_b200_batch* b);
 int impact_b200_jacobi_solve(int N1, int N2, int N3, int M1, int M2, int M3, double omega, const double* cdg1,
                              const double* cdg2, const double* cdg3, double* rel, const double* bb, int mode_j,
                              double tol_abs_inf, int max_sweeps, int* sweeps, double* res_inf);
+/* The same solve in the third RK substep of a CT case (jacobi_solver_host_v4.f90:302-305): at the
+ * start of every iteration, before its stop test and sweep, the CT pressure condition
+ * (pressure_bc_launcher_) sets rel on the labelled points -- type_id1: label 5 on plane
+ * k_start_index - 1 to p_inlet, type_id2: label 9 on that plane to p_outlet, type_id3: every
+ * label 11 to p_outlet_2 (the reference passes 1, 1, 0 and values already multiplied by
+ * (aRK + bRK) dt).  labels: host, one byte per point in the padded layout. */
+int impact_b200_jacobi_solve_bc(int N1, int N2, int N3, int M1, int M2, int M3, double omega, const double* cdg1,
+                                const double* cdg2, const double* cdg3, double* rel, const double* bb, int mode_j,
+                                double tol_abs_inf, int max_sweeps, int* sweeps, double* res_inf,
+                                const uint8_t* labels, int k_start_index, int type_id1, int type_id2, int type_id3,
+                                double p_inlet, double p_outlet, double p_outlet_2);
 
 /* Deterministic FP64 inner product over the unique periodic points (product_scalar,
  * mod_solvers.f90:2319-2354) of two device fields of a grid with N1 x N2 x N3 points.

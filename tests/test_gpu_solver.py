@@ -106,6 +106,34 @@ def test_jacobi_solve_matches_sweeps():
     assert rel_err(og.interior(got), og.interior(want)) <= 1e-12
 
 
+def test_jacobi_solve_with_ct_pressure_condition():
+    """Every iteration first sets the inlet / outlet planes (jacobi_solver_host_v4.f90:302-305),
+    then sweeps: the oracle's pressure_bc and one JOR sweep, 29 times."""
+    N = (17, 17, 25)
+    og, ig = O.Grid(N), I.Grid(N)
+    b, rel = og.random(9), og.random(10)
+    lab = np.ones(og.shape, dtype=np.uint8)
+    ks = 6
+    lab[ks - 1 + 3, 6:12, 6:12] = 5   # inlet disc on plane ks - 1
+    lab[ks - 1 + 3, 13:16, 4:8] = 9   # first outlet on the same plane
+    lab[20 + 3, 6:10, 6:10] = 11      # second outlet (type_id3 = 1 here)
+    lab[ks + 3, 6:12, 6:12] = 5       # label 5 off the plane: left alone
+    pin, pout, pout2 = 0.31, -0.12, 0.05
+    want = rel.copy()
+    for _ in range(29):
+        og.pressure_bc(lab, ks, pin, pout, pout2, want)
+        want = og.jacobi(b.copy(), want, 1, 0.8, init_yes=False)
+    got = rel.copy()
+    sweeps, _ = I.jacobi_solve(ig, got, b, omega=0.8, mode_j=1000, max_sweeps=29, labels=lab, k_start_index=ks,
+                               type_ids=(1, 1, 1), pressures=(pin, pout, pout2))
+    assert sweeps == 29
+    assert rel_err(og.interior(got), og.interior(want)) <= 1e-12
+    # without the condition the result differs
+    plain = rel.copy()
+    I.jacobi_solve(ig, plain, b, omega=0.8, mode_j=1000, max_sweeps=29)
+    assert rel_err(og.interior(plain), og.interior(want)) > 1e-6
+
+
 def test_jacobi_solve_heuristic_stop_terminates():
     og, ig = O.Grid((17, 17, 17)), I.Grid((17, 17, 17))
     b = _rhs(og, 7)
