@@ -321,6 +321,52 @@ def inflow_velocity(time: np.ndarray, velocity: np.ndarray, t: float):
     return u
 
 
+class AnalyticWindkessel:
+    """Pressure and flow rate of the three branches -- 1 inlet, 2 first outlet, 3 second outlet --
+    from the analytic two-element Windkessel of get_pressure_and_flow_rate_WKM (usr_func.f90:
+    762-855): a half-sine systolic inflow of peak q_peak over the first 0.4 s of a 1 s beat gives
+    the closed-form systolic pressure from 80 mmHg; in diastole the pressure decays from the last
+    systolic value with time constant R C.  Returns nondimensional (p, q): p / (density U_ref^2)
+    in Pa (mmHg x 133.322), q / (L_ref^3 / T_ref).  The last systolic pressure of each branch is
+    state (the reference keeps it in p_end_systole_in / _out / _out_2 and its restart files);
+    pass end_systole to continue from saved values."""
+
+    # (C [m^3/Pa-ish, as the reference divides], R, peak flow) per branch, in the reference's own
+    # arithmetic: C = value / 1e6, R = value * 1e6, peak = 0.0004 x fraction
+    BRANCHES = {1: (1.5496 / 1000000.0, 0.9758 * 1000000.0, 0.0004),
+                2: (1.5 / 1000000.0, 1.12 * 1000000.0, 0.0004 * 0.85),
+                3: (0.059 / 1000000.0, 19.68 * 1000000.0, 0.0004 * 0.05)}
+
+    def __init__(self, reference_time, reference_velocity, reference_length, density=BLOOD_DENSITY,
+                 end_systole=(0.0, 0.0, 0.0)):
+        self.reference_time = float(reference_time)
+        self.reference_velocity = float(reference_velocity)
+        self.reference_length = float(reference_length)
+        self.density = float(density)
+        self.end_systole = {b: float(v) for b, v in zip((1, 2, 3), end_systole)}
+
+    def __call__(self, branch, t):
+        c, r, q_peak = self.BRANCHES[branch]
+        beat = 1.0
+        systole = 0.4 * beat
+        p_dia = 80.0
+        pi = 4.0 * math.atan(1.0)
+        tp = t * self.reference_time
+        den = systole ** 2.0 + c ** 2.0 * pi ** 2.0 * r ** 2.0
+        if tp <= systole:
+            p = ((p_dia + q_peak * systole * r * c * pi * r / den) * math.exp(-1.0 * tp / (r * c))
+                 - (systole * q_peak * r * (c * pi * r * math.cos(pi * tp / systole))
+                    - systole * math.sin(pi * tp / systole)) / den)
+            q = q_peak * math.sin(pi * tp / systole)
+            self.end_systole[branch] = p
+        else:
+            p = self.end_systole[branch] * math.exp(-1.0 * (tp - systole) / (r * c))
+            q = 0.0
+        p = p / (self.density * self.reference_velocity ** 2.0) * 133.322
+        q = q / (self.reference_length ** 3.0 / self.reference_time)
+        return p, q
+
+
 def windkessel_pressures(table: np.ndarray, waveform: Waveform, t: float, r_in=0.78e6, c_in=2.166e-6,
                          r_out=0.898e6, c_out=2.066e-6, q_max=Q_MAX, outlet_fraction=0.85, p0_mmhg=80.0,
                          density=BLOOD_DENSITY):

@@ -12,6 +12,7 @@ checked against the reference's own output.
     inflow        apply_CT_forcing       usr_func.f90:929-945, get_shifted_time_in_pulse :899-906,
                   get_pulse_number_and_length :753-760
     windkessel    get_pressure_waveform_echo_WKM  usr_func.f90:653-750
+    windkessel_wkm  get_pressure_and_flow_rate_WKM  usr_func.f90:762-855
 """
 from __future__ import annotations
 
@@ -138,3 +139,55 @@ def windkessel(table, times, u_ref, t):
                 pre = pre * (1. - dt / (C * R)) - dt / C * q_in
         res.append(pre / (1060. * u_ref ** 2.) * 133.322)
     return res[0], res[1]
+
+
+class windkessel_wkm:
+    """get_pressure_and_flow_rate_WKM(branch_number, p, q) with the module's three end-systolic
+    pressures (p_end_systole_in / _out / _out_2) as state; the reference's `time`,
+    reference_time / _velocity / _length and blood_density = 1060 as inputs."""
+
+    def __init__(self, reference_time, reference_velocity, reference_length):
+        self.reference_time = reference_time
+        self.reference_velocity = reference_velocity
+        self.reference_length = reference_length
+        self.p_end_systole_in = 0.
+        self.p_end_systole_out = 0.
+        self.p_end_systole_out_2 = 0.
+
+    def __call__(self, branch_number, time):
+        pi = 4. * math.atan(1.)
+        T_beat = 1.
+        T_systole = 0.4 * T_beat
+        p_diastole = 80.
+        if branch_number == 1:
+            CWK = 1.5496 / 1000000.
+            RWK = 0.9758 * 1000000.
+            Q_peak_systole = 0.0004
+        elif branch_number == 2:
+            CWK = 1.5 / 1000000.
+            RWK = 1.12 * 1000000.
+            Q_peak_systole = 0.0004 * 0.85
+        else:
+            CWK = 0.059 / 1000000.
+            RWK = 19.68 * 1000000.
+            Q_peak_systole = 0.0004 * 0.05
+        time_phys = time * self.reference_time
+        if time_phys <= T_systole:
+            p = (p_diastole + Q_peak_systole * T_systole * RWK * CWK * pi * RWK / (T_systole ** 2. + CWK ** 2. * pi ** 2. * RWK ** 2.)) \
+                * math.exp(-1. * time_phys / (RWK * CWK)) \
+                - (T_systole * Q_peak_systole * RWK * (CWK * pi * RWK * math.cos(pi * time_phys / T_systole))
+                   - T_systole * math.sin(pi * time_phys / T_systole)) / (T_systole ** 2. + CWK ** 2. * pi ** 2. * RWK ** 2.)
+            q = Q_peak_systole * math.sin(pi * (time_phys) / T_systole)
+            if branch_number == 1:
+                self.p_end_systole_in = p
+            elif branch_number == 2:
+                self.p_end_systole_out = p
+            else:
+                self.p_end_systole_out_2 = p
+        else:
+            p_end = {1: self.p_end_systole_in, 2: self.p_end_systole_out}.get(branch_number, self.p_end_systole_out_2)
+            p = p_end * math.exp(-1. * (time_phys - T_systole) / (RWK * CWK))
+            q = 0.
+        p = p / (1060. * self.reference_velocity ** 2.) * 133.322
+        q = q / (self.reference_length ** 3. / self.reference_time)
+        return p, q

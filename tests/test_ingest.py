@@ -5,7 +5,8 @@ both halves of the inlet plane (the column i = M1 / 2 belongs to the inlet and t
 and the outlet fringe overwrites the inlet's), the label mask, the converted waveform and the
 inflow at table times, between them, before the first one and over several pulses; VTK files in
 ASCII and big-endian binary, NIfTI-1 volumes in either byte order, gzip-compressed and scaled;
-the Windkessel inlet and outlet pressures of get_pressure_waveform_echo_WKM (usr_func.f90:653-750);
+the Windkessel inlet and outlet pressures of get_pressure_waveform_echo_WKM (usr_func.f90:653-750)
+and the analytic branches of get_pressure_and_flow_rate_WKM (:762-855);
 and the errors for volumes that do not fit.
 """
 import math
@@ -126,6 +127,26 @@ def test_waveform_conversion_and_lookup(tmp_path, idealized):
     # Windkessel pressures for the pressure boundary condition (two updates at a table time)
     for t in probes:
         assert G.windkessel_pressures(tab, w, t) == R.windkessel([tuple(r) for r in tab], times, u_ref, t), t
+
+
+def test_analytic_windkessel_branches():
+    """get_pressure_and_flow_rate_WKM: systolic closed form, then the diastolic decay from the
+    branch's last systolic pressure, for the inlet and both outlets, over two beats."""
+    t_ref, u_ref, l_ref = 0.05, 1.3, 0.012
+    got = G.AnalyticWindkessel(t_ref, u_ref, l_ref)
+    want = R.windkessel_wkm(t_ref, u_ref, l_ref)
+    times = [0.0, 0.5, 3.0, 7.999, 8.0, 8.1, 12.0, 19.9]  # x t_ref: systole ends at 0.4 s = t 8
+    for t in times:
+        for b in (1, 2, 3):
+            assert got(b, t) == want(b, t), (b, t)
+    p_sys, q_sys = got(1, 4.0)
+    assert q_sys > 0.0 and p_sys > 0.0
+    p_dia, q_dia = got(1, 12.0)
+    assert q_dia == 0.0 and 0.0 < p_dia < got(1, 8.0)[0]  # decays from the end-systolic value
+    fresh = G.AnalyticWindkessel(t_ref, u_ref, l_ref)
+    assert fresh(2, 12.0) == (0.0, 0.0)  # no systole seen yet: the reference's zero initial state
+    resumed = G.AnalyticWindkessel(t_ref, u_ref, l_ref, end_systole=tuple(got.end_systole[b] for b in (1, 2, 3)))
+    assert resumed(3, 15.0) == got(3, 15.0)
 
 
 def test_ingest_rejects_volumes_that_do_not_fit():
