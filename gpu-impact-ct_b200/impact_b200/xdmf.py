@@ -6,8 +6,9 @@ tables (interpolate2_vel_pre, mod_diff.f90:1740-1825), the pressure is written a
 every field is written on the pressure grid of the unique periodic points 1..N-1, sub-sampled by
 a stride per axis that must divide N - 1.  One XDMF file per output and stride names the
 3DRectMesh (VXVYVZ coordinates y1p, y2p, y3p at the sampled points), the time and the node
-attributes Pressure, Velocity_X, Velocity_Y, Velocity_Z, optionally scaled to physical units
-by Function items (length L_ref, velocity U_ref, pressure rho U_ref^2, time L_ref / U_ref).
+attributes Pressure, Velocity_X, Velocity_Y, Velocity_Z and optionally Lambda_2 (lambda,
+:2827-3008), optionally scaled to physical units by Function items (length L_ref, velocity
+U_ref, pressure rho U_ref^2, time L_ref / U_ref, lambda-2 U_ref / L_ref as the reference writes).
 
 The reference writes its heavy data with parallel HDF5, which this image does not carry; here
 each field is a flat little-endian float64 file read by the XDMF Format="Binary" data item
@@ -20,6 +21,7 @@ Host-side output code: the snapshot that feeds it is taken on the device
 """
 from __future__ import annotations
 
+import math
 import os
 import xml.etree.ElementTree as ET
 from dataclasses import dataclass
@@ -60,6 +62,47 @@ def velocity_at_pressure_points(grid, vel, m):
     return out
 
 
+def lambda2(grid, vel1, vel2, vel3):
+    """The lambda-2 vortex criterion at the pressure points (lambda, mod_inout.f90:2827-3008):
+    the velocity interpolated to the pressure points, its gradient Dvel(m, a) = d u_m / d x_a with
+    the 7-point cp tables (periodic), the symmetric tensor TT of the reference, and the middle
+    eigenvalue from the trigonometric solution of its characteristic cubic (PP / 3 where the
+    discriminant rho <= 1e-5).  Returns the interior-sized array (N3-1, N2-1, N1-1)."""
+    w = [velocity_at_pressure_points(grid, v, m) for m, v in ((1, vel1), (2, vel2), (3, vel3))]
+    D = [[None] * 3 for _ in range(3)]
+    for a in range(3):
+        N = grid.N[a]
+        rows = np.asarray(grid.tab["cp1"][a], dtype=np.float64).reshape(N + 1, 7)[1:N]
+        axis = 2 - a
+        bshape = [1, 1, 1]
+        bshape[axis] = N - 1
+        for m in range(3):
+            acc = None
+            for l in range(-3, 4):
+                shifted = np.roll(w[m], -l, axis=axis)  # u(i + l), periodic
+                term = rows[:, l + 3].reshape(bshape) * shifted
+                acc = term if acc is None else acc + term
+            D[m][a] = acc
+    d = lambda m, a: D[m - 1][a - 1]  # noqa: E731  (Dvel(m, a) of the reference, 1-based)
+    t1 = 2.0 * (d(1, 1) * d(1, 1) + d(1, 2) * d(2, 1) + d(1, 3) * d(3, 1))
+    t2 = 2.0 * (d(2, 1) * d(1, 2) + d(2, 2) * d(2, 2) + d(2, 3) * d(3, 2))
+    t3 = 2.0 * (d(3, 1) * d(1, 3) + d(3, 2) * d(2, 3) + d(3, 3) * d(3, 3))
+    t4 = (d(1, 1) + d(2, 2)) * (d(1, 2) + d(2, 1)) + d(1, 3) * d(3, 2) + d(2, 3) * d(3, 1)
+    t5 = (d(1, 1) + d(3, 3)) * (d(1, 3) + d(3, 1)) + d(1, 2) * d(2, 3) + d(3, 2) * d(2, 1)
+    t6 = (d(2, 2) + d(3, 3)) * (d(2, 3) + d(3, 2)) + d(2, 1) * d(1, 3) + d(3, 1) * d(1, 2)
+    pp = t1 + t2 + t3
+    qq = t1 * t2 + t1 * t3 + t2 * t3 - t4 ** 2 - t5 ** 2 - t6 ** 2
+    rr = t1 * t2 * t3 + 2.0 * t4 * t5 * t6 - t1 * t6 ** 2 - t2 * t5 ** 2 - t3 * t4 ** 2
+    rho = (pp / 3.0) ** 2 - qq / 3.0
+    flat = rho <= 1e-5
+    sr = np.sqrt(np.where(flat, 1.0, rho))
+    q = ((pp / 3.0) ** 3 - qq * (pp / 6.0) + rr / 2.0) / sr ** 3
+    pi = 2.0 * abs(math.acos(0.0))
+    theta = np.where(np.abs(q) < 1.0, np.arccos(np.clip(q, -1.0, 1.0)) / 3.0, np.where(q > 0.0, 0.0, pi / 3.0))
+    lam = np.sort(np.stack([np.cos(theta), np.cos(theta + 2.0 * pi / 3.0), np.cos(theta + 4.0 * pi / 3.0)]), axis=0)
+    return np.where(flat, pp / 3.0, sr * lam[1] + pp / 6.0)
+
+
 def sampled_points(N, stride):
     """Indices (1-based) of the points an output with this stride holds along an axis of N
     points: 1, 1 + stride, ..., (N - 1) / stride of them; the stride must divide N - 1."""
@@ -82,8 +125,10 @@ class XdmfWriter:
     strides: {name: (s1, s2, s3)}, one output per entry (the reference's large / med / small).
     """
 
-    def __init__(self, directory, grid, strides=None, scale: Scale | None = None, base="IMPACT_xdmf3d"):
+    def __init__(self, directory, grid, strides=None, scale: Scale | None = None, base="IMPACT_xdmf3d",
+                 with_lambda2=False):
         self.directory, self.grid, self.scale, self.base = str(directory), grid, scale, base
+        self.with_lambda2 = bool(with_lambda2)  # write_lambda2_yes: also the Lambda_2 attribute
         self.strides = dict(strides or {"large": (1, 1, 1)})
         self.points = {}
         for name, st in self.strides.items():
@@ -105,6 +150,8 @@ class XdmfWriter:
         data = {"pre": np.asarray(fields["pre"], dtype=np.float64)[4:g.N[2] + 3, 4:g.N[1] + 3, 4:g.N[0] + 3]}
         for m, key in enumerate(("velX", "velY", "velZ"), start=1):
             data[key] = velocity_at_pressure_points(g, fields[VELOCITY[m - 1]], m)
+        if self.with_lambda2:
+            data["lamb"] = lambda2(g, *(fields[v] for v in VELOCITY))
         paths = []
         for name in self.strides:
             p1, p2, p3 = self.points[name]
@@ -143,11 +190,12 @@ class XdmfWriter:
             self._item(geo, (n[a],), coords[a], None if sc is None else sc.L_ref)
         t = time if sc is None else time * sc.L_ref / sc.U_ref
         ET.SubElement(grid, "Time", TimeType="Single", Value=repr(float(t)))
-        for attr, key in ATTRIBUTES:
+        attrs = ATTRIBUTES + ((("Lambda_2", "lamb"),) if "lamb" in files else ())
+        for attr, key in attrs:
             a = ET.SubElement(grid, "Attribute", Name=attr, Center="Node")
             factor = None
-            if sc is not None:
-                factor = sc.rho * sc.U_ref ** 2 if key == "pre" else sc.U_ref
+            if sc is not None:  # the reference's factors, U_ref / L_ref for lambda-2 included
+                factor = {"pre": sc.rho * sc.U_ref ** 2, "lamb": sc.U_ref / sc.L_ref}.get(key, sc.U_ref)
             self._item(a, (n[2], n[1], n[0]), files[key], factor)
         path = os.path.join(self.directory, f"{self.base}_{tag}.xmf")
         ET.indent(root)

@@ -3,7 +3,8 @@
 interpolate_vel_pre bit for bit on a stretched grid (ghost values are not read), the strided
 outputs hold the points 1, 1 + s, ... with their coordinates, the XDMF files parse and read back
 to the written data and time, physical scaling multiplies lengths, velocities, pressure and time,
-and a stride that does not divide N - 1 is an error."""
+a stride that does not divide N - 1 is an error, and the lambda-2 field (lambda,
+mod_inout.f90:2827-3008) matches a literal loop restatement to rounding."""
 import xml.etree.ElementTree as ET
 
 import numpy as np
@@ -11,6 +12,7 @@ import pytest
 
 import impact_b200 as I
 import oracle as O
+import output_restatement as R
 from impact_b200 import xdmf as X
 
 N = (17, 13, 25)
@@ -83,3 +85,23 @@ def test_stride_must_divide(tmp_path):
     grid = I.Grid(N, L, KINDS)
     with pytest.raises(ValueError):
         X.XdmfWriter(tmp_path / "out", grid, strides={"bad": (3, 1, 1)})  # 16 % 3 != 0
+
+
+def test_lambda2_matches_restatement(tmp_path):
+    n = (13, 9, 11)
+    grid, og = I.Grid(n, L, KINDS), O.Grid(n, L, KINDS)
+    rng = np.random.default_rng(8)
+    vel = og.zeros(3)
+    for m in range(3):
+        og.interior(vel[m])[...] = rng.uniform(-1.0, 1.0, size=og.interior(vel[m]).shape)
+    got = X.lambda2(grid, vel[0], vel[1], vel[2])
+    want = R.lambda2(og, vel)
+    scale = max(abs(v) for v in want.values())
+    for (i, j, k), v in want.items():
+        assert abs(got[k - 1, j - 1, i - 1] - v) <= 1e-9 * scale, (i, j, k)
+    # the writer's Lambda_2 attribute, scaled by U_ref / L_ref as the reference writes it
+    fields = {f"vel{m + 1}": vel[m] for m in range(3)}
+    fields["pre"] = og.zeros()
+    w = X.XdmfWriter(tmp_path, grid, with_lambda2=True, scale=X.Scale(L_ref=0.5, U_ref=2.0))
+    back = X.read_output(w.write(fields, 1.0)[0])
+    assert np.allclose(back["Lambda_2"], 4.0 * got, rtol=1e-15, atol=0)  # U_ref / L_ref
