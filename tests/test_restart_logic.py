@@ -1,6 +1,7 @@
 """Restart files (impact_b200.restart) with the device case replaced by a stand-in: save writes
 velocity, pressure, time, step count and the grid through Case.snapshot, load uploads the same
-arrays and restores the time and step count, and a file of another grid is refused."""
+arrays and restores the time and step count, a file of another grid is refused, and the
+analytic Windkessel end-systolic state goes along when asked."""
 import numpy as np
 import pytest
 
@@ -49,3 +50,22 @@ def test_save_and_load(tmp_path):
         assert np.array_equal(b.fields[f], a.fields[f])
     with pytest.raises(ValueError):
         restart.load(FakeCase((9, 10, 13)), path)
+
+
+def test_windkessel_state_round_trip(tmp_path):
+    from impact_b200 import ingest
+
+    wk = ingest.AnalyticWindkessel(0.05, 1.3, 0.012)
+    for b in (1, 2, 3):
+        wk(b, 6.0)  # systole: each branch remembers its pressure
+    a = FakeCase((9, 10, 11), seed=3)
+    path = tmp_path / "wk.npz"
+    restart.save(a, path, windkessel=wk)
+    back = ingest.AnalyticWindkessel(0.05, 1.3, 0.012)
+    restart.load(FakeCase((9, 10, 11)), path, windkessel=back)
+    assert back.end_systole == wk.end_systole
+    assert back(2, 14.0) == wk(2, 14.0)  # the same diastolic decay
+    plain = tmp_path / "plain.npz"
+    restart.save(a, plain)
+    with pytest.raises(ValueError):
+        restart.load(FakeCase((9, 10, 11)), plain, windkessel=back)
