@@ -19,10 +19,10 @@ import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-N = (17, 13, 21)
+N = (17, 17, 25)
 L = (1.0, 1.5, 2.0)
 KINDS = (1, 0, 1)
-REACH = 0.25  # two y spacings, about four x and three z spacings
+REACH = 0.25  # about 2.7 y spacings, four x and three z spacings
 
 
 def _markers(n, seed):
@@ -97,7 +97,7 @@ def test_empty_and_growing_marker_sets():
         case.set_markers(yb, REACH, 2)
         assert np.array_equal(case.ibm_interpolate(), og.ibm_interpolate(yb, vel, 2, REACH))
     with pytest.raises(I.ImpactError):
-        case.set_markers(_markers(4, 1), 1.0, 2)  # a window of 2.0 holds all 20 points along z
+        case.set_markers(_markers(4, 1), 1.0, 2)  # a window of 2.0 holds all 24 points along z
     with pytest.raises(I.ImpactError):
         case.set_markers(_markers(4, 1), REACH, 5)  # no such delta kernel
     # a rejected set leaves the previous one in place
