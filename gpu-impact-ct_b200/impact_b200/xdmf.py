@@ -24,11 +24,13 @@ from __future__ import annotations
 import math
 import os
 import xml.etree.ElementTree as ET
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 
 import numpy as np
 
 VELOCITY = ("vel1", "vel2", "vel3")
+_THREADS = max(1, min(16, os.cpu_count() or 1))
 ATTRIBUTES = (("Pressure", "pre"), ("Velocity_X", "velX"), ("Velocity_Y", "velY"), ("Velocity_Z", "velZ"))
 
 
@@ -46,18 +48,47 @@ def velocity_at_pressure_points(grid, vel, m):
     if vel.shape != grid.shape:
         raise ValueError(f"field shape {vel.shape} is not the grid's {grid.shape}")
     N = grid.N[m - 1]
-    periodic = N - 1
     rows = np.asarray(grid.tab["cIup"][m - 1], dtype=np.float64).reshape(N + 1, 6)[1:N]
     axis = 3 - m                       # (k, j, i) storage: m = 1 is the last axis
-    sel = [slice(4, n + 3) for n in (grid.N[2], grid.N[1], grid.N[0])]
+    inner = vel[4:grid.N[2] + 3, 4:grid.N[1] + 3, 4:grid.N[0] + 3]
+    return _periodic_stencil(inner, rows, axis, -3)
+
+
+def _periodic_stencil(u, rows, axis, lo):
+    """sum over l of rows[:, l - lo] * u(i + l) along `axis` of the interior array u, periodic,
+    the terms added in the order of l (the first one not added to zero).  Large arrays are cut
+    into slabs across another axis and done by a thread pool (numpy's arithmetic releases the
+    interpreter lock); every point gets the same operations in the same order either way."""
+    split = 0 if axis != 0 else 1
+    slabs = min(_THREADS, u.shape[split]) if u.size >= (1 << 20) else 1
+    if slabs > 1:
+        edges = np.linspace(0, u.shape[split], slabs + 1).astype(int)
+        out = np.empty(u.shape)
+
+        def work(q):
+            sl = [slice(None)] * 3
+            sl[split] = slice(edges[q], edges[q + 1])
+            out[tuple(sl)] = _stencil_block(u[tuple(sl)], rows, axis, lo)
+
+        with ThreadPoolExecutor(slabs) as ex:
+            list(ex.map(work, range(slabs)))
+        return out
+    return _stencil_block(u, rows, axis, lo)
+
+
+def _stencil_block(u, rows, axis, lo):
+    n = u.shape[axis]
+    width = rows.shape[1]
+    pad = [(0, 0)] * 3
+    pad[axis] = (-lo, width - 1 + lo)
+    wrapped = np.pad(u, pad, mode="wrap")   # u(i + l) at wrapped[i - 1 - lo + l]
     bshape = [1, 1, 1]
-    bshape[axis] = periodic
+    bshape[axis] = n
     out = None
-    for l in range(-3, 3):
-        pos = (np.arange(1, N) + l - 1) % periodic + 1 + 3   # wrapped point, storage offset 3
-        s = list(sel)
-        s[axis] = pos
-        term = rows[:, l + 3].reshape(bshape) * vel[tuple(s)]
+    for l in range(lo, lo + width):
+        sl = [slice(None)] * 3
+        sl[axis] = slice(l - lo, l - lo + n)
+        term = rows[:, l - lo].reshape(bshape) * wrapped[tuple(sl)]
         out = term if out is None else out + term
     return out
 
@@ -73,16 +104,8 @@ def lambda2(grid, vel1, vel2, vel3):
     for a in range(3):
         N = grid.N[a]
         rows = np.asarray(grid.tab["cp1"][a], dtype=np.float64).reshape(N + 1, 7)[1:N]
-        axis = 2 - a
-        bshape = [1, 1, 1]
-        bshape[axis] = N - 1
         for m in range(3):
-            acc = None
-            for l in range(-3, 4):
-                shifted = np.roll(w[m], -l, axis=axis)  # u(i + l), periodic
-                term = rows[:, l + 3].reshape(bshape) * shifted
-                acc = term if acc is None else acc + term
-            D[m][a] = acc
+            D[m][a] = _periodic_stencil(w[m], rows, 2 - a, -3)
     d = lambda m, a: D[m - 1][a - 1]  # noqa: E731  (Dvel(m, a) of the reference, 1-based)
     t1 = 2.0 * (d(1, 1) * d(1, 1) + d(1, 2) * d(2, 1) + d(1, 3) * d(3, 1))
     t2 = 2.0 * (d(2, 1) * d(1, 2) + d(2, 2) * d(2, 2) + d(2, 3) * d(3, 2))
