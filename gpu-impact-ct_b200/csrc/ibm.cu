@@ -130,9 +130,14 @@ extern "C" int impact_b200_case_set_markers(impact_b200_case* c, int n, const do
   IMPACT_CUDA_CHECK(cudaMemcpyAsync(s.ibm.geom, geom.data(), geom.size() * sizeof(double), cudaMemcpyHostToDevice,
                                     s.stream));
   if (n > s.ibm.cap) {  // grow (the old buffers stay with the case until it is destroyed)
-    if (case_alloc(s, (void**)&s.ibm.yb, (size_t)3 * n * sizeof(double))) return -1;
-    if (case_alloc(s, (void**)&s.ibm.buf, (size_t)4 * n * sizeof(double))) return -1;
-    if (case_alloc(s, (void**)&s.ibm.skip, (size_t)n)) return -1;
+    double *yb_d = nullptr, *buf_d = nullptr;
+    uint8_t* skip_d = nullptr;
+    if (case_alloc(s, (void**)&yb_d, (size_t)3 * n * sizeof(double)) ||
+        case_alloc(s, (void**)&buf_d, (size_t)4 * n * sizeof(double)) || case_alloc(s, (void**)&skip_d, (size_t)n))
+      return -1;  // the previous marker set stays in force
+    s.ibm.yb = yb_d;
+    s.ibm.buf = buf_d;
+    s.ibm.skip = skip_d;
     s.ibm.cap = n;
   }
   if (n > 0) {
