@@ -31,6 +31,7 @@ class Request:
     nsteps: int
     arrival: float = 0.0       # seconds after the start of the stream
     kinds: tuple = (0, 0, 0)   # coordinate kind per axis
+    waveform: object = None    # measured inflow (time, velocity) of a CT case, or None: sinusoid
 
 
 @dataclass
@@ -98,6 +99,8 @@ class Server:
                     c = Case(g, precision=self.precision, device=self.device)
                     lab = r.labels(g) if callable(r.labels) else r.labels
                     c.set_labels(lab)
+                    if r.waveform is not None:
+                        c.set_inflow_waveform(*r.waveform)
                     active.append({"req": r, "case": c, "bytes": need, "steps": 0, "admitted": clock() - t0})
                     self.seconds["admit"] += clock() - ta
                     used += need

@@ -37,6 +37,9 @@ class FakeCase:
     def set_labels(self, lab):
         self.labels = lab
 
+    def set_inflow_waveform(self, time=None, velocity=None):
+        self.waveform = (time, velocity)
+
     def download(self, f):
         return f
 
@@ -132,3 +135,16 @@ def test_idle_loop_sleeps_until_the_next_arrival(monkeypatch):
     _install(monkeypatch, clock, {(10, 10, 10): 10})
     done = S.Server(100).run([_req(0, 10, 5.0, 1)], clock=clock, sleep=clock.sleep)
     assert done[0].admitted == 5.0 and done[0].finished == 6.0 and done[0].latency == 1.0
+
+
+def test_ct_request_carries_its_inflow_waveform(monkeypatch):
+    clock = Clock()
+    _install(monkeypatch, clock, {(10, 10, 10): 10, (20, 20, 20): 10})
+    FakeCase.live = []
+    wf = ([0.0, 0.5, 1.0], [0.2, 0.9, 0.2])
+    reqs = [S.Request(0, (10, 10, 10), (1.0, 1.0, 1.0), "labels", None, 1, 0.0, waveform=wf),
+            _req(1, 20, 0.0, 1)]
+    S.Server(100).run(reqs, clock=clock, sleep=clock.sleep)
+    byN = {c.grid.N: c for c in FakeCase.live}
+    assert byN[(10, 10, 10)].waveform == wf
+    assert not hasattr(byN[(20, 20, 20)], "waveform")  # the default sinusoidal inflow
