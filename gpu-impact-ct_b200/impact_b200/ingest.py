@@ -321,6 +321,19 @@ def inflow_velocity(time: np.ndarray, velocity: np.ndarray, t: float):
     return u
 
 
+# RK3 coefficients of the reference (mod_vars.f90:774-775)
+A_RK = (8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0)
+B_RK = (0.0, -17.0 / 60.0, -5.0 / 12.0)
+
+
+def jor_pressures(p_inlet, p_outlet, p_outlet_2, substep, dtime):
+    """The boundary values the reference's JOR loop passes to pressure_bc_launcher_ in RK substep
+    `substep` (1..3): each pressure times (aRK + bRK) times the time step
+    (jacobi_solver_host_v4.f90:302-304); for impact_b200.jacobi_solve(..., pressures=...)."""
+    f = A_RK[substep - 1] + B_RK[substep - 1]
+    return tuple(p * f * dtime for p in (p_inlet, p_outlet, p_outlet_2))
+
+
 class AnalyticWindkessel:
     """Pressure and flow rate of the three branches -- 1 inlet, 2 first outlet, 3 second outlet --
     from the analytic two-element Windkessel of get_pressure_and_flow_rate_WKM (usr_func.f90:

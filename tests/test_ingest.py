@@ -149,6 +149,14 @@ def test_analytic_windkessel_branches():
     assert resumed(3, 15.0) == got(3, 15.0)
 
 
+def test_jor_pressures():
+    a, b = (8. / 15., 5. / 12., 3. / 4.), (0., -17. / 60., -5. / 12.)
+    for sub in (1, 2, 3):
+        got = G.jor_pressures(0.3, -0.2, 0.05, sub, 1.7e-3)
+        assert got == tuple(p * (a[sub - 1] + b[sub - 1]) * 1.7e-3 for p in (0.3, -0.2, 0.05))
+    assert math.isclose(G.jor_pressures(3.0, 0.0, 0.0, 3, 1.0)[0], 1.0)  # aRK + bRK = 1/3
+
+
 def test_ingest_rejects_volumes_that_do_not_fit():
     vol, grid = _volume(), _grid()
     y1p, y2p = G.pressure_coords(grid)
