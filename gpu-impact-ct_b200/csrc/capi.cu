@@ -1,5 +1,6 @@
 // capi.cu -- the C ABI: the reference's launcher FFI (src/*_launcher.cu, bound by the unchanged
 // src/*_host.f90 wrappers) and library control / device-resident solve entry points.
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -63,27 +64,54 @@ static bool geom_from_dev(int nx, int ny, int nz, Geom* g, const char* who) {
   return true;
 }
 
-// library-owned scratch (jor_launcher_ output, product_scalar partials), grown on demand
-static std::mutex g_scratch_mu;
-static void* g_scratch = nullptr;
-static size_t g_scratch_bytes = 0;
-static void* scratch(size_t bytes) {
+// Library-owned scratch (jor_launcher_ output, product_scalar partials, the JOR solve's
+// workspace), one buffer per (device, stream) so that launchers issued on different streams
+// never share memory.  A buffer is allocated on the first use from its stream and regrown (after
+// its stream has drained) when a larger grid arrives; it is kept until the process exits.
+namespace {
+struct ScratchSlot {
+  int dev;
+  cudaStream_t stream;
+  void* ptr;
+  size_t bytes;
+};
+std::mutex g_scratch_mu;
+std::vector<ScratchSlot> g_scratch_slots;
+}  // namespace
+
+static void* scratch(size_t bytes, cudaStream_t s) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    impact_set_error_msg(-1, "library scratch: cudaGetDevice failed");
+    return nullptr;
+  }
   std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (bytes > g_scratch_bytes) {
-    if (g_scratch) {
-      cudaStreamSynchronize(g_stream);
-      cudaFree(g_scratch);
+  ScratchSlot* slot = nullptr;
+  for (auto& x : g_scratch_slots)
+    if (x.dev == dev && x.stream == s) slot = &x;
+  if (!slot) {
+    g_scratch_slots.push_back({dev, s, nullptr, 0});
+    slot = &g_scratch_slots.back();
+  }
+  if (bytes > slot->bytes) {
+    if (slot->ptr) {
+      cudaStreamSynchronize(s);
+      cudaFree(slot->ptr);
     }
-    g_scratch = nullptr;
-    g_scratch_bytes = 0;
-    if (cudaMalloc(&g_scratch, bytes) != cudaSuccess) {
+    slot->ptr = nullptr;
+    slot->bytes = 0;
+    if (cudaMalloc(&slot->ptr, bytes) != cudaSuccess) {
+      slot->ptr = nullptr;
       impact_set_error_msg(-1, "library scratch allocation failed");
       return nullptr;
     }
-    g_scratch_bytes = bytes;
+    slot->bytes = bytes;
   }
-  return g_scratch;
+  return slot->ptr;
 }
+
+// the Part 1 launchers' stream, for the other translation units of the C ABI
+cudaStream_t impact_launcher_stream() { return g_stream; }
 
 // ---------------------------------------------------------------------------------------
 // Part 1: reference launchers
@@ -204,7 +232,7 @@ extern "C" void jor_launcher_(int* grid_id, int* nx_dev, int* ny_dev, int* nz_de
     impact_set_error_msg(-1, "jor_launcher_: expects cdg(-1:1,...) tables and grid_id >= 1");
     return;
   }
-  double* out = static_cast<double*>(scratch((size_t)g.nfield * sizeof(double)));
+  double* out = static_cast<double*>(scratch((size_t)g.nfield * sizeof(double), g_stream));
   if (!out) return;
   launch_jor_faces(g, *ny_cdg1, *ny_cdg2, *ny_cdg3, *grid_id, *omega, *cdg1_dev, *cdg2_dev, *cdg3_dev, *rel_dev,
                    *bb_dev, *rear_ghost_dev, *front_ghost_dev, *upper_ghost_dev, *lower_ghost_dev, *west_ghost_dev,
@@ -223,12 +251,27 @@ extern "C" void get_ghost_launcher_(int* nx_dev, int* ny_dev, int* nz_dev, doubl
   check_launch("get_ghost_launcher_");
 }
 
+// Plane of the inlet / first-outlet condition: 0 (default) Fortran index k == k_start_index - 1, the
+// test of apply_pressure_BC_CT (usr_func.f90:857-897); 1 the plane of the reference GPU kernel,
+// whose C-index test (k+4) == k_start_index - 1 (set_pressure_BC_kernel.cu:26) selects Fortran
+// index k_start_index - 4.
+static std::atomic<int> g_pbc_plane{0};
+extern "C" int impact_b200_set_pressure_bc_plane(int mode) {
+  if (mode != 0 && mode != 1)
+    return impact_set_error_msg(-1, "impact_b200_set_pressure_bc_plane: mode 0 (CPU routine) or 1 (reference GPU kernel)");
+  g_pbc_plane.store(mode);
+  return 0;
+}
+extern "C" int impact_b200_pressure_bc_plane(void) { return g_pbc_plane.load(); }
+// k_start_index as the kernels take it (they test Fortran index k == ks - 1)
+static int pbc_ks(int k_start_index) { return g_pbc_plane.load() == 1 ? k_start_index - 3 : k_start_index; }
+
 extern "C" void pressure_bc_launcher_(int* type_id1, int* type_id2, int* type_id3, int* k_start_index, int* nx_dev,
                                       int* ny_dev, int* nz_dev, double* pre_inlet, double* pre_outlet,
                                       double* pre_outlet_2, double** ct_geometry_dev, double** rel_dev) {
   Geom g;
   if (!geom_from_dev(*nx_dev, *ny_dev, *nz_dev, &g, "pressure_bc_launcher_")) return;
-  launch_pressure_bc_f64label(g, *type_id1, *type_id2, *type_id3, *k_start_index, *pre_inlet, *pre_outlet,
+  launch_pressure_bc_f64label(g, *type_id1, *type_id2, *type_id3, pbc_ks(*k_start_index), *pre_inlet, *pre_outlet,
                               *pre_outlet_2, *ct_geometry_dev, *rel_dev, g_stream);
   check_launch("pressure_bc_launcher_");
 }
@@ -363,21 +406,26 @@ int jacobi_solve_impl(int N1, int N2, int N3, int M1, int M2, int M3, double ome
   const size_t fb = (size_t)g.nfield * sizeof(double);
   const dim3 gr((g.n1 + BX - 1) / BX, (g.n2 + BY - 1) / BY, g.n3), bl(BX, BY);
   const long long nb = (long long)gr.x * gr.y * gr.z;
-  double *d_rel = nullptr, *d_tmp = nullptr, *d_bb = nullptr, *d_old = nullptr, *d_c = nullptr, *d_part = nullptr;
-  uint8_t* d_lab = nullptr;
   cudaStream_t s = g_stream;
   int rc = 0;
   auto fail = [&](cudaError_t e, const char* w) {
     rc = impact_set_error(e, w, __FILE__, __LINE__);
   };
-  cudaError_t e = cudaMalloc(&d_rel, fb);
-  if (e == cudaSuccess) e = cudaMalloc(&d_tmp, fb);
-  if (e == cudaSuccess) e = cudaMalloc(&d_bb, fb);
-  if (e == cudaSuccess) e = cudaMalloc(&d_old, fb);
-  if (e == cudaSuccess) e = cudaMalloc(&d_c, 3 * sizeof(double) * (N1 + N2 + N3));
-  if (e == cudaSuccess) e = cudaMalloc(&d_part, (2 * nb + 8) * sizeof(double));
-  if (e == cudaSuccess && bc.labels) e = cudaMalloc(&d_lab, (size_t)g.nfield);
-  if (e != cudaSuccess) fail(e, "impact_b200_jacobi_solve alloc");
+  // workspace: four fields, the cdg tables, the check partials and the labels, carved from the
+  // stream's library scratch (allocated once, regrown only for a larger grid)
+  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t b_c = up(3 * sizeof(double) * (N1 + N2 + N3)), b_part = up((2 * nb + 8) * sizeof(double));
+  const size_t b_lab = bc.labels ? up((size_t)g.nfield) : 0;
+  unsigned char* ws = static_cast<unsigned char*>(scratch(4 * up(fb) + b_c + b_part + b_lab, s));
+  if (!ws) return -1;
+  double* d_rel = reinterpret_cast<double*>(ws);
+  double* d_tmp = reinterpret_cast<double*>(ws + up(fb));
+  double* d_bb = reinterpret_cast<double*>(ws + 2 * up(fb));
+  double* d_old = reinterpret_cast<double*>(ws + 3 * up(fb));
+  double* d_c = reinterpret_cast<double*>(ws + 4 * up(fb));
+  double* d_part = reinterpret_cast<double*>(ws + 4 * up(fb) + b_c);
+  uint8_t* d_lab = bc.labels ? ws + 4 * up(fb) + b_c + b_part : nullptr;
+  cudaError_t e = cudaSuccess;
   const double pi_ref = 3.1415;  // the constant of the reference's stop test (jacobi_solver_host_v4.f90:383)
   const double thresh =
       20. * mode_j * 8. * 1. / 3.0 * 0.8 * pi_ref * pi_ref * (1. / ((double)M1 * M1) + 1. / ((double)M2 * M2) + 1. / ((double)M3 * M3));
@@ -401,7 +449,7 @@ int jacobi_solve_impl(int N1, int N2, int N3, int M1, int M2, int M3, double ome
     for (int iter = 1; iter <= max_sweeps; ++iter) {
       // the boundary values first, before the stop test and the sweep of this iteration
       if (d_lab)
-        launch_pressure_bc(g, bc.t1, bc.t2, bc.t3, bc.k_start_index, bc.p_in, bc.p_out, bc.p_out2, d_lab, d_rel, s);
+        launch_pressure_bc(g, bc.t1, bc.t2, bc.t3, pbc_ks(bc.k_start_index), bc.p_in, bc.p_out, bc.p_out2, d_lab, d_rel, s);
       if (iter % mode_j == 1 || mode_j == 1) {
         k_jor_check<<<gr, bl, 0, s>>>(g, c1, c2, c3, d_rel, d_bb, d_old, d_part);
         k_jor_check_fin<<<1, 1024, 0, s>>>(d_part, nb, d_part + 2 * nb);
@@ -430,13 +478,6 @@ int jacobi_solve_impl(int N1, int N2, int N3, int M1, int M2, int M3, double ome
       if (e != cudaSuccess) fail(e, "impact_b200_jacobi_solve result");
     }
   }
-  cudaFree(d_rel);
-  cudaFree(d_tmp);
-  cudaFree(d_bb);
-  cudaFree(d_old);
-  cudaFree(d_c);
-  cudaFree(d_part);
-  cudaFree(d_lab);
   if (sweeps) *sweeps = done_sweeps;
   if (res_inf) *res_inf = last_res;
   return rc;
@@ -474,7 +515,7 @@ extern "C" int impact_b200_product_scalar(int N1, int N2, int N3, const double* 
     return impact_set_error_msg(-1, "impact_b200_product_scalar: bad arguments");
   const Geom g = make_geom(N1, N2, N3);
   const long long nd = reduce_partial_doubles(g, 1);
-  double* part = static_cast<double*>(scratch((size_t)(nd + 8) * sizeof(double)));
+  double* part = static_cast<double*>(scratch((size_t)(nd + 8) * sizeof(double), g_stream));
   if (!part) return -1;
   double* out = part + nd;
   reduce_dot<double>(g, a_dev, b_dev, part, out, g_stream);

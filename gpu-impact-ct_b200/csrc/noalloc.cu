@@ -17,13 +17,19 @@
 //  * all calls share the one array: two calls whose kernels overlap on the GPU race on it and
 //    must be serialised by the caller (e.g. by issuing them on one stream, one after the other).
 //    Nothing carries over between calls: every slot a call reads is written earlier in that call.
-//  * runs on the legacy default stream and returns once the result is on the host.
+//  * runs on the library's current stream (impact_b200_set_stream; the legacy default stream
+//    unless set), like impact_b200_product_scalar and the Part 1 launchers, so it is ordered
+//    after the launchers queued on that stream; it returns once the result is on the host.
+//  * its sum runs per z-plane, then over the planes: deterministic, and equal to
+//    impact_b200_product_scalar's result up to rounding (that one sums per-tile partials).
 //  * no cudaMalloc, cudaFree or allocating library routine is called.
 #include <cstdio>
 #include <mutex>
 
 #include "../../include/impact_b200.h"
 #include "common.cuh"
+
+cudaStream_t impact_launcher_stream();  // capi.cu
 
 namespace {
 
@@ -107,8 +113,8 @@ extern "C" int impact_b200_product_scalar_noalloc(int N1, int N2, int N3, const 
   const impact::Geom g = impact::make_geom(N1, N2, N3);
   const int planes = N3 - 1;
   double* out = scratch + NOALLOC_MAX_PLANES;
-  // runs on the legacy default stream and returns after the result has reached the host
-  cudaStream_t s = nullptr;
+  // runs on the launchers' stream and returns after the result has reached the host
+  cudaStream_t s = impact_launcher_stream();
   k_plane_dot<<<planes, NOALLOC_THREADS, 0, s>>>(g, a_dev, b_dev, scratch);
   k_plane_sum<<<1, NOALLOC_THREADS, 0, s>>>(scratch, planes, out);
   e = cudaGetLastError();

@@ -127,6 +127,8 @@ def lib():
                                             _u8p, i, i, i, i, d, d, d]),
         "impact_b200_product_scalar": (i, [i, i, i, _vp, _vp, _dp]),
         "impact_b200_product_scalar_noalloc": (i, [i, i, i, _vp, _vp, _dp]),
+        "impact_b200_set_pressure_bc_plane": (i, [i]),
+        "impact_b200_pressure_bc_plane": (i, []),
         "impact_b200_profile_enable": (None, [i]),
         "impact_b200_profile_reset": (None, []),
         "impact_b200_profile_read": (i, [i, P(C.c_longlong), _dp, _dp, P(C.c_char_p)]),
@@ -522,6 +524,18 @@ def product_scalar_noalloc(N, a_dev: int, b_dev: int) -> float:
     check(lib().impact_b200_product_scalar_noalloc(N[0], N[1], N[2], a_dev, b_dev, C.byref(out)),
           "product_scalar_noalloc")
     return out.value
+
+
+def set_pressure_bc_plane(mode: int):
+    """Plane of the inlet / first-outlet pressure condition (pressure_bc_launcher_ and the JOR solve
+    with the CT condition): 0 (default) the Fortran test k == k_start_index - 1 of
+    apply_pressure_BC_CT (usr_func.f90:857-897); 1 the plane the reference GPU kernel sets,
+    k_start_index - 4 (set_pressure_BC_kernel.cu:26)."""
+    check(lib().impact_b200_set_pressure_bc_plane(int(mode)), "set_pressure_bc_plane")
+
+
+def pressure_bc_plane() -> int:
+    return int(lib().impact_b200_pressure_bc_plane())
 
 
 def jacobi_solve(grid: Grid, rel: np.ndarray, bb: np.ndarray, omega=0.8, mode_j=20, tol_abs_inf=0.0,

@@ -327,9 +327,11 @@ B_RK = (0.0, -17.0 / 60.0, -5.0 / 12.0)
 
 
 def jor_pressures(p_inlet, p_outlet, p_outlet_2, substep, dtime):
-    """The boundary values the reference's JOR loop passes to pressure_bc_launcher_ in RK substep
-    `substep` (1..3): each pressure times (aRK + bRK) times the time step
-    (jacobi_solver_host_v4.f90:302-304); for impact_b200.jacobi_solve(..., pressures=...)."""
+    """The boundary values the reference's JOR loop passes to pressure_bc_launcher_: each pressure
+    times (aRK + bRK) of RK substep `substep` (1..3) times the time step
+    (jacobi_solver_host_v4.f90:302-304); for impact_b200.jacobi_solve(..., pressures=...).  The
+    reference applies the condition in substep 3 only (jacobi_solver_host_v4.f90:304-305): pass
+    labels and these pressures to jacobi_solve in substep 3, and no labels in substeps 1 and 2."""
     f = A_RK[substep - 1] + B_RK[substep - 1]
     return tuple(p * f * dtime for p in (p_inlet, p_outlet, p_outlet_2))
 

@@ -12,7 +12,11 @@
  * Boundaries are periodic in all directions (the only case the reference kernels cover).
  * The launchers run asynchronously on the library's current stream (impact_b200_set_stream,
  * default: the legacy default stream, as the reference) and report errors through
- * impact_b200_last_error(); like the reference launchers they return nothing.
+ * impact_b200_last_error(); like the reference launchers they return nothing.  jor_launcher_,
+ * impact_b200_product_scalar and impact_b200_jacobi_solve(_bc) use a library scratch buffer of
+ * the calling (device, stream) pair, allocated on first use and regrown for a larger grid: calls
+ * on different streams never share scratch; calls on one stream from several host threads at
+ * once are not supported.
  *
  * Part 2 -- device-resident entry points that replace whole Fortran loops (the GPU
  * Poisson solve of jacobi_solver_host_v4.f90, BiCGstab_orig, one RK3 time step), so that
@@ -78,11 +82,20 @@ void get_ghost_launcher_(int* nx_dev, int* ny_dev, int* nz_dev, double** rel_dev
                          double** front_ghost_dev, double** upper_ghost_dev, double** lower_ghost_dev,
                          double** west_ghost_dev, double** east_ghost_dev);
 /* set_pressure_BC_kernel_launcher.cu:12 -- Dirichlet pressure on labelled cells (labels as FP64,
- * the ct_geometry array of the reference).  Planes are matched with the Fortran index test
- * k == k_start_index-1 of apply_pressure_BC_CT (usr_func.f90:857-897). */
+ * the ct_geometry array of the reference).  By default planes are matched with the Fortran
+ * index test k == k_start_index-1 of apply_pressure_BC_CT (usr_func.f90:857-897); see
+ * impact_b200_set_pressure_bc_plane for the reference GPU kernel's plane. */
 void pressure_bc_launcher_(int* type_id1, int* type_id2, int* type_id3, int* k_start_index, int* nx_dev,
                            int* ny_dev, int* nz_dev, double* pre_inlet, double* pre_outlet, double* pre_outlet_2,
                            double** ct_geometry_dev, double** rel_dev);
+/* Plane of the inlet (label 5) and first-outlet (label 9) conditions of pressure_bc_launcher_ and
+ * impact_b200_jacobi_solve_bc.  mode 0 (default): Fortran index k == k_start_index - 1, the test
+ * of apply_pressure_BC_CT (usr_func.f90:857-897).  mode 1: the plane the reference GPU kernel
+ * sets, whose C-index test (k+4) == k_start_index - 1 (set_pressure_BC_kernel.cu:26) selects
+ * Fortran index k_start_index - 4, three planes below the CPU routine's.  Process-wide; returns
+ * -1 for any other mode.  No counterpart in the reference (its two paths simply differ). */
+int impact_b200_set_pressure_bc_plane(int mode);
+int impact_b200_pressure_bc_plane(void);
 /* jacobi_kernel_launcher.cu:12 -- comp = one damped-Jacobi sweep of rel (multigrid level grid_id) */
 void jacobi_launcher_(int* grid_id, int* nx_dev_g, int* ny_dev_g, int* nz_dev_g, int* ny_cdg1_g, int* ny_cdg2_g,
                       int* ny_cdg3_g, int* nx_cdg1_g, double* omega_g, double** cdg1_dev3, double** cdg2_dev3,
@@ -302,7 +315,9 @@ void* impact_b200_batch_stream(impact_b200_batch* b);
  * sweeps of the compact Laplacian on the device, periodic neighbours read in place (no ghost
  * faces cross PCIe), stopping on the reference's heuristic relative-change test evaluated every
  * mode_j sweeps, or when ||bb - A rel||_inf < tol_abs_inf (if > 0), or after max_sweeps.
- * cdg1..3: host tables cdg(-1:1,1:N) of level 1.  Returns the sweeps done in *sweeps. */
+ * cdg1..3: host tables cdg(-1:1,1:N) of level 1.  Returns the sweeps done in *sweeps.  Runs on
+ * the library's current stream; its device workspace (four fields, the tables, the labels) is the
+ * stream's library scratch, so repeated solves allocate nothing after the first on a grid size. */
 int impact_b200_jacobi_solve(int N1, int N2, int N3, int M1, int M2, int M3, double omega, const double* cdg1,
                              const double* cdg2, const double* cdg3, double* rel, const double* bb, int mode_j,
                              double tol_abs_inf, int max_sweeps, int* sweeps, double* res_inf);
@@ -320,7 +335,9 @@ int impact_b200_jacobi_solve_bc(int N1, int N2, int N3, int M1, int M2, int M3, 
 
 /* Deterministic FP64 inner product over the unique periodic points (product_scalar,
  * mod_solvers.f90:2319-2354) of two device fields of a grid with N1 x N2 x N3 points.
- * Uses a per-call scratch allocation for the block partials. */
+ * The block partials live in a library scratch buffer, allocated on the first call from a
+ * (device, stream) pair and regrown for larger grids; runs on the library's current stream
+ * (impact_b200_set_stream) and returns once *result (host memory) is written. */
 int impact_b200_product_scalar(int N1, int N2, int N3, const double* a_dev, const double* b_dev, double* result);
 
 /* The same inner product for callers that cannot let the library allocate device memory: a
@@ -330,7 +347,11 @@ int impact_b200_product_scalar(int N1, int N2, int N3, const double* a_dev, cons
  * until exit; grids with more than 16384 unique z-planes (N3 > 16385) are rejected.  The first
  * call on a device resolves the array's address (make it before any stream capture there); calls
  * whose kernels overlap on the GPU share the array and race, so serialise them.  Runs on the
- * legacy default stream; returns once *result (host memory) is written. */
+ * library's current stream (impact_b200_set_stream), so it is ordered after the launchers queued
+ * there; fields written on any other stream (a case stream, a caller's non-blocking stream) must
+ * be complete before the call.  The sum runs per z-plane and then over the planes: deterministic,
+ * and equal to impact_b200_product_scalar's result up to rounding, not bit for bit.  Returns
+ * once *result (host memory) is written. */
 int impact_b200_product_scalar_noalloc(int N1, int N2, int N3, const double* a_dev, const double* b_dev,
                                        double* result);
 

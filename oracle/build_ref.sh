@@ -3,9 +3,10 @@
 # #include their *_kernel.cu) from the reference tree, unchanged, into oracle/_ref/libref_kernels.so.
 # Test infrastructure only: the GPU pin tests run them on the same inputs as the oracle to pin
 # the oracle's restatement to the reference's implementation.  Nothing is copied into this repo.
-#   usage: oracle/build_ref.sh [path/to/GPU-IMPACT-CT]
+#   usage: oracle/build_ref.sh path/to/GPU-IMPACT-CT   (or IMPACT_REFERENCE_ROOT in the environment)
 set -euo pipefail
-REF="${1:-/root/reference}"
+REF="${1:-${IMPACT_REFERENCE_ROOT:-}}"
+[ -n "$REF" ] || { echo "usage: $0 path/to/GPU-IMPACT-CT (or set IMPACT_REFERENCE_ROOT)"; exit 2; }
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
 SRC="$REF/src"

@@ -65,4 +65,7 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("IMPACT_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py path/to/GPU-IMPACT-CT (or set IMPACT_REFERENCE_ROOT)")
+    main(root)

@@ -61,3 +61,19 @@ def test_case_entry_points_reject_a_null_case_without_touching_the_gpu():
     for name, call in calls:
         assert call() != 0, name
         assert name in I.last_error(), (name, I.last_error())
+
+
+def test_pressure_bc_plane_switch_host_side():
+    """The plane switch is host state only: it round-trips without a GPU and rejects other modes."""
+    assert I.pressure_bc_plane() == 0
+    I.set_pressure_bc_plane(1)
+    try:
+        assert I.pressure_bc_plane() == 1
+    finally:
+        I.set_pressure_bc_plane(0)
+    import pytest
+
+    with pytest.raises(I.ImpactError, match="mode 0"):
+        I.set_pressure_bc_plane(2)
+    I.lib().impact_b200_clear_error()
+    assert I.pressure_bc_plane() == 0

@@ -188,3 +188,28 @@ def test_pressure_bc_pin_plane_offset(ref, grids):
     call(ref, "pressure_bc_launcher_", ("i", 1), ("i", 1), ("i", 0), ("i", ks + 3), ("i", nx), ("i", ny), ("i", nz),
          ("d", 1.5), ("d", -0.5), ("d", 0.25), ("p", ptr(d_lab)), ("p", ptr(d_rel)))
     assert np.array_equal(og.interior(host(d_rel)), og.interior(want))
+
+
+def test_pressure_bc_reference_gpu_plane_switch(ref, grids):
+    """With impact_b200_set_pressure_bc_plane(1) this library's pressure_bc_launcher_ sets the plane
+    the reference GPU kernel sets: both called with the same k_start_index give the same field."""
+    og, _ = grids
+    nx, ny, nz = _dims(og)
+    rng = np.random.default_rng(122)
+    lab = np.zeros(og.shape, dtype=np.uint8)
+    og.interior(lab)[...] = rng.choice(np.array([0, 1, 5, 9, 11], dtype=np.uint8), size=og.interior(lab).shape)
+    rel = og.random(123)
+    ks = 9
+    d_lab = dev(lab.astype(np.float64))
+    d_ref, d_own = dev(rel), dev(rel)
+    args = [("i", 1), ("i", 1), ("i", 1), ("i", ks), ("i", nx), ("i", ny), ("i", nz), ("d", 1.5), ("d", -0.5),
+            ("d", 0.25), ("p", ptr(d_lab))]
+    call(ref, "pressure_bc_launcher_", *args, ("p", ptr(d_ref)))
+    I.set_pressure_bc_plane(1)
+    try:
+        I.launchers.call("pressure_bc_launcher_", *args, ("p", ptr(d_own)))
+        I.launchers.sync()
+    finally:
+        I.set_pressure_bc_plane(0)
+    assert np.array_equal(og.interior(host(d_own)), og.interior(host(d_ref)))
+    assert not np.array_equal(og.interior(host(d_own)), og.interior(rel))  # the condition set something
