@@ -53,10 +53,14 @@ def parse():
                     help="relative tolerance of each FP32 inner solve (batch and serve cases, and --no-tune)")
     ap.add_argument("--precond", type=int, default=1, help="0: JOR sweeps, 1: multigrid V-cycle (default)")
     ap.add_argument("--check-every", type=int, default=2)
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "kernels"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "kernels", "plain",
+                                                               "operators"],
                     help="single: the 384 mixed case (default line, with short batch and serve samples); "
                          "batch / serve: the full batched or serving workload as the line; kernels: per-kernel "
-                         "micro-benchmark on resident random fields (the small case for profilers)")
+                         "micro-benchmark on resident random fields (the small case for profilers); plain: the "
+                         "64x64x128 FP64 plain step (10 steps) against the oracle on one and all host cores; "
+                         "operators: the 256x256x512 stretched operator microbench, FP64 / FP32 / the reference's "
+                         "own kernels, against the oracle")
     ap.add_argument("--kernels", default="all", help="kernels: comma-separated names to run (default all)")
     ap.add_argument("--iters", type=int, default=20, help="kernels: timed launches per kernel")
     ap.add_argument("--no-extra", action="store_true", help="skip the batch and serve samples of the default line")
@@ -282,7 +286,7 @@ def run_arm(args, precision, device, rank, world, dist, profile_on, e2e_on):
     if dist is not None:
         t_dev, t_e2e = max_over_ranks(dist, [t_dev, t_e2e], f"cuda:{device}")
     out = {"ms_dev": t_dev, "ms_e2e": t_e2e, "iterations": its, "inner_iterations": inner, "status": stats,
-           "tuning": tuning,
+           "tuning": tuning, "sp": sp, "state": (case.state.time, case.state.timestep),
            "launches": launches, "clocks": clocks, "prof": None, "bytes_in": bytes_in, "bytes_out": bytes_out,
            "dt": st.dtime, "time": st.time}
     fields = None
@@ -314,11 +318,57 @@ def run_arm(args, precision, device, rank, world, dist, profile_on, e2e_on):
     return out, fields, grid, lab
 
 
-def cpu_baseline(args, fields, lab, fp64_iters):
-    """The FP64 CPU oracle on the host cores, on a bounded sample of the same workload: one time
-    step with every Poisson solve capped at 2 BiCGstab iterations, plus 2 extra iterations on the
-    resident Poisson problem to price one iteration; scaled to a full step with the iteration count
-    the FP64 device run needed (same algorithm, same preconditioner)."""
+def _div_metric(grid, div):
+    """[max |div|, max |div weight|] over the unique points of a device-computed divergence field,
+    weight = 1 / (sum |cDu1(:,i)| + sum |cDv2(:,j)| + sum |cDw3(:,k)|) (mod_coeffs.f90:2242-2262)."""
+    import numpy as np
+    s = []
+    for a in range(3):
+        c = np.asarray(grid.tab["cD"][a]).reshape(grid.N[a] + 1, 6)
+        s.append(np.abs(c[1:grid.N[a]]).sum(axis=1))
+    w = 1.0 / (s[2][:, None, None] + s[1][None, :, None] + s[0][None, None, :])
+    d = np.abs(div[4:-4, 4:-4, 4:-4])
+    return [float(d.max()), float((d * w).max())]
+
+
+def step_from_state(args, precision, device, fields, state, sp):
+    """One untimed device step of a fresh case of the workload started from `fields` (velocity,
+    pressure) at `state` (time, step count) with the solver parameters `sp`; returns the new
+    velocity and pressure (host arrays) and the step's solver statistics."""
+    import torch
+    _, _, case = build_case(args.size, precision, device)
+    for f in ("vel1", "vel2", "vel3", "pre"):
+        case.upload(f, fields[f])
+    case.state.time, case.state.timestep = state
+    st = case.step(sp)
+    out = {f: case.download(f) for f in ("vel1", "vel2", "vel3", "pre")}
+    stats = {"iterations": list(st.poisson_iterations), "inner_iterations": list(st.inner_iterations),
+             "status": list(st.poisson_status), "dt": st.dtime}
+    case.close()
+    del case
+    torch.cuda.empty_cache()
+    return out, stats
+
+
+def _fluid_inner(og, lab):
+    """Interior points labelled fluid whose divergence stencil (3 points each way) sees only fluid."""
+    import numpy as np
+    from impact_b200 import geometry as G
+    fl = og.interior(lab) == G.FLUID
+    inner = fl.copy()
+    for ax in range(3):
+        for sh in (-3, -2, -1, 1, 2, 3):
+            inner &= np.roll(fl, sh, axis=ax)
+    return inner
+
+
+def oracle_step_leg(args, fields, lab, state, sweeps, dev_next):
+    """The FP64 CPU oracle on the host cores: ONE full time step of the workload (every Poisson
+    solve to the 1e-8 relative residual, no cap), started from the FP64 device run's state after
+    its timed steps.  Its wall time is the CPU baseline (measured, not extrapolated); its result
+    is the reference for the device's step from the same state (FP64 and mixed precision):
+    velocity and pressure errors and the divergence metric of test_divergence (mod_test.f90:300-345)
+    on all points and on the fluid points away from the mask."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
 
@@ -326,45 +376,65 @@ def cpu_baseline(args, fields, lab, fp64_iters):
 
     n = args.size
     N = (n + 1, n + 1, 2 * n + 1)
-    g = O.Grid(N, (1.0, 1.0, 2.0))
+    og = O.Grid(N, (1.0, 1.0, 2.0))
     vel = np.stack([fields["vel1"], fields["vel2"], fields["vel3"]])
     nl = np.stack([fields["nl1"], fields["nl2"], fields["nl3"]])
     pre = fields["pre"].copy()
     st = O.OrcStepState()
-    st.timestep = 10
-    mg = g.multigrid() if args.precond == 1 else None
-    p = O.step_params(Re=500.0, CFL=0.2, dtime_max=1.0, tol_rel=1e-8, max_it=1, n_sweeps=args.n_sweeps, omega=0.8,
-                      mg=mg)
+    st.time, st.timestep = state
+    mg = og.multigrid() if args.precond == 1 else None
+    p = O.step_params(Re=500.0, CFL=0.2, dtime_max=1.0, tol_rel=1e-8, max_it=2000, n_sweeps=args.n_sweeps, omega=0.8,
+                      mg=mg, mg_down=sweeps[0], mg_up=sweeps[1], mg_bottom=sweeps[2])
     t0 = time.perf_counter()
-    g.time_step(p, lab, vel, nl, pre, st)
-    t_capped = time.perf_counter() - t0
-    used = sum(st.poisson_iterations)
-    # price of two more BiCGstab iterations on the current Poisson problem
-    b = g.divergence2(vel[0].copy(), vel[1].copy(), vel[2].copy())
-    t0 = time.perf_counter()
-    if mg is not None:
-        r = mg.bicgstab(b, pre.copy(), tol_rel=0.0, max_it=2, omega=0.8, init_yes=False)
-    else:
-        r = g.bicgstab(b, pre.copy(), tol_rel=0.0, max_it=2, n_sweeps=args.n_sweeps, omega=0.8, init_yes=False)
-    t_two = time.perf_counter() - t0
-    t_it = t_two / max(1, r.iterations)
-    full = t_capped + max(0.0, sum(fp64_iters) - used) * t_it
+    og.time_step(p, lab, vel, nl, pre, st)
+    secs = time.perf_counter() - t0
     cells = n * n * 2 * n
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": cells / full / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": (f"FP64 oracle, {n}x{n}x{2*n}, same preconditioner: one step with Poisson solves capped at 1 BiCGstab "
-                       f"iterations ({t_capped:.1f} s) + 2 iterations ({t_two:.1f} s); scaled to "
-                       f"{sum(fp64_iters)} iterations per step (FP64 device run)"),
-            "seconds_per_step": full}
+    iters = list(st.poisson_iterations)
+    cpu = {"value": cells / secs / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": (f"one full FP64 oracle time step of {n}x{n}x{2*n} (same multigrid-preconditioned BiCGstab, "
+                      f"sweeps {list(sweeps)}, every Poisson solve to 1e-8, no cap; {iters} iterations) from the FP64 "
+                      f"device run's state at step {state[1]}, timed on the host: {secs:.1f} s"),
+           "seconds_per_step": secs}
+    inner = _fluid_inner(og, lab)
+    umax = max(float(np.abs(og.interior(vel[m])).max()) for m in range(3))
+    pmax = float(np.abs(og.interior(pre)).max())
+    div_all, div_in = og.test_divergence(vel), og.test_divergence(vel, inner)
+    par = {"start_step": state[1], "oracle": {"iterations": iters, "dt": st.dtime, "div_max": div_all[0],
+                                              "div_weighted_max": div_all[1], "div_fluid_inner_max": div_in[0]}}
+    for name, (d, stats) in dev_next.items():
+        if d is None:
+            continue
+        dv = np.stack([d["vel1"], d["vel2"], d["vel3"]])
+        g_all, g_in = og.test_divergence(dv), og.test_divergence(dv, inner)
+        du = max(float(np.abs(og.interior(dv[m]) - og.interior(vel[m])).max()) for m in range(3))
+        dp = float(np.abs(og.interior(d["pre"]) - og.interior(pre)).max())
+        par[name] = {"velocity_max_abs_err_rel": du / umax, "pressure_max_abs_err_rel": dp / pmax,
+                     "div_max": g_all[0], "div_weighted_max": g_all[1], "div_fluid_inner_max": g_in[0],
+                     "div_max_err_rel": abs(g_all[0] - div_all[0]) / div_all[0],
+                     "div_weighted_max_err_rel": abs(g_all[1] - div_all[1]) / div_all[1],
+                     "iterations": stats["iterations"], "inner_iterations": stats["inner_iterations"],
+                     "status": stats["status"], "dt_err_rel": abs(stats["dt"] - st.dtime) / st.dtime}
+    par["note"] = ("one step from the same state on the device and in the FP64 oracle; errors relative to max|u| and "
+                   "max|p| of the oracle's step; div_* = test_divergence's max |div2(u)| and max |div2(u) weight| over "
+                   "all points, and max |div2(u)| over fluid points whose stencil sees only fluid")
+    return cpu, par
 
 
 def reference_arm(args, rank, world):
-    """IMPACT's CPU algorithm (FP64 oracle, all host cores) on bounded samples of the workload."""
+    """IMPACT's CPU algorithm (the FP64 oracle restatement, all host cores) on the workload.
+
+    A full step of the 384 case takes about a minute on the host, so the timed steps are bounded
+    samples priced by one measured full step:
+      warm-up: step 1 from rest (its Poisson right-hand sides are zero); step 2 in full (every
+               solve to 1e-8, no cap) -- its wall time T_full and iteration count n_full are
+               measured; step 3 with every solve capped at one BiCGstab iteration (T_cap), so one
+               iteration costs t_it = (T_full - T_cap) / (n_full - 3); further warm-up steps capped.
+      timed:   K capped steps, each priced as its own wall time plus (n_full - 3) t_it.
+    ms_per_step is that full-step price; sample_ms_per_step the capped steps' own wall time."""
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
-
     import oracle as O
     from impact_b200 import geometry as G
 
@@ -374,49 +444,47 @@ def reference_arm(args, rank, world):
     lab = G.straight_vessel(g, radius_frac=0.25, stenoses=[(1.0, 0.6, 0.125)])
     vel, nl, pre = g.zeros(3), g.zeros(3), g.zeros()
     st = O.OrcStepState()
-    # warm-up: develop the flow with capped solves (bounded work), then time capped steps and
-    # price BiCGstab iterations; extrapolate to the iteration count a full 1e-8 solve needs
-    cap = 1
     mg = g.multigrid() if args.precond == 1 else None
-    p = O.step_params(Re=500.0, CFL=0.2, dtime_max=1.0, tol_rel=1e-8, max_it=cap, n_sweeps=args.n_sweeps, omega=0.8,
-                      mg=mg)
-    for _ in range(min(args.warmup, 2)):
+    sw = args.sweeps
+
+    def params(cap):
+        return O.step_params(Re=500.0, CFL=0.2, dtime_max=1.0, tol_rel=1e-8, max_it=cap, n_sweeps=args.n_sweeps,
+                             omega=0.8, mg=mg, mg_down=sw, mg_up=sw, mg_bottom=sw)
+
+    def timed(p):
+        t0 = time.perf_counter()
         g.time_step(p, lab, vel, nl, pre, st)
-    ref_iters = 3 * _iters_estimate(n, args.precond)
-    times = []
+        return time.perf_counter() - t0, list(st.poisson_iterations)
+
+    full_p, cap_p = params(2000), params(1)
+    timed(full_p)                      # from rest: zero right-hand sides
+    t_full, it_full = timed(full_p)    # one full step, measured
+    t_cap, it_cap = timed(cap_p)
+    n_full = sum(it_full)
+    t_it = max(0.0, (t_full - t_cap) / max(1, n_full - sum(it_cap)))
+    for _ in range(max(0, args.warmup - 3)):
+        timed(cap_p)
+    samples, priced = [], []
     for _ in range(args.steps):
-        t0 = time.perf_counter()
-        g.time_step(p, lab, vel, nl, pre, st)
-        t_capped = time.perf_counter() - t0
-        used = sum(st.poisson_iterations)
-        b = g.divergence2(vel[0].copy(), vel[1].copy(), vel[2].copy())
-        t0 = time.perf_counter()
-        if mg is not None:
-            r = mg.bicgstab(b, pre.copy(), tol_rel=0.0, max_it=2, omega=0.8)
-        else:
-            r = g.bicgstab(b, pre.copy(), tol_rel=0.0, max_it=2, n_sweeps=args.n_sweeps, omega=0.8)
-        t_it = (time.perf_counter() - t0) / max(1, r.iterations)
-        times.append(t_capped + max(0, ref_iters - used) * t_it)
+        t, its = timed(cap_p)
+        samples.append(t)
+        priced.append(t + max(0, n_full - sum(its)) * t_it)
     cells = n * n * 2 * n
-    val = cells * len(times) / sum(times) / 1e6
+    val = cells * len(priced) / sum(priced) / 1e6
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    sample = (f"FP64 oracle, {n}x{n}x{2*n}, multigrid-preconditioned BiCGstab (sweeps {sw}/{sw}/{sw}) to 1e-8: one "
+              f"full step measured in warm-up ({t_full:.1f} s, {it_full} iterations, {cells / t_full / 1e6:.3f} "
+              f"Mcell-steps/s); each timed step runs the full explicit part with every Poisson solve capped at one "
+              f"BiCGstab iteration ({1e3 * sum(samples) / len(samples):.0f} ms on average) and is priced with the "
+              f"remaining {n_full} - 3 iterations at the full step's {t_it:.2f} s per iteration")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "warmup": args.warmup, "ms_per_step": 1e3 * sum(priced) / len(priced),
+            "sample_ms_per_step": 1e3 * sum(samples) / len(samples), "full_step_measured_ms": 1e3 * t_full,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload(n),
-            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": (f"each step: one FP64 oracle step with Poisson solves capped at {cap} "
-                                        f"BiCGstab iterations + 2 priced iterations, extrapolated to {ref_iters} "
-                                        "iterations per step")},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-
-
-def _iters_estimate(n, precond=1):
-    """BiCGstab iterations per 1e-8 solve measured on the device for this workload family:
-    JOR-4 preconditioner ~1.6 n (64: 110, 128: 210, 256: 405); multigrid V-cycle ~8, independent
-    of n."""
-    return 8 if precond == 1 else int(round(1.6 * n))
 
 
 # ---------------------------------------------------------------------------------------------
@@ -591,6 +659,13 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
+    if args.workload in ("plain", "operators"):
+        if rank == 0:
+            (plain_main if args.workload == "plain" else operators_main)(args, device)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.workload != "single":
         extra_main(args, device, rank, world, dist)
         return
@@ -659,18 +734,22 @@ def main():
             line["mixed_vs_fp64"] = {
                 "after_steps": args.warmup + 2 * K, "velocity_max_abs_err_rel": du / umax if umax else None,
                 "pressure_max_abs_err_rel": dp / pmax if pmax else None,
-                "divergence_max_abs": {"mixed": float(np.abs(fields["div"][sl]).max()),
-                                       "fp64": float(np.abs(fields64["div"][sl]).max())},
-                "note": "same workload from rest, same steps; interior points; relative to max|.| of the FP64 run"}
+                "test_divergence": {"mixed": _div_metric(grid, fields["div"]), "fp64": _div_metric(grid, fields64["div"])},
+                "note": "same workload from rest, same steps; interior points; relative to max|.| of the FP64 run; "
+                        "test_divergence = [max |div2(u)|, max |div2(u) weight|] over all points (mod_test.f90:300-345), "
+                        "after the mask forcing, as the reference prints it at the start of a step"}
     if not args.no_extra and world == 1:
         line["batch"] = batch_bench(args, device, min(args.cases, 48), args.case_steps or 5)
         line["serve"] = serve_bench(args, device, args.requests, args.case_steps or 10)
-    if world == 1 and not args.no_cpu:
-        its = fp64["iterations"][-1] if fp64 is not None else [_iters_estimate(args.size, args.precond)] * 3
+    if world == 1 and not args.no_cpu and fp64 is not None:
         try:
-            line["cpu_baseline"] = cpu_baseline(args, fields, lab, its)
-        except Exception as ex:  # the CPU sample must never hide the device number
-            line["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
+            sw = [fp64["sp"].poisson.mg_down, fp64["sp"].poisson.mg_up, fp64["sp"].poisson.mg_bottom]
+            nxt = {"fp64": step_from_state(args, 0, device, fields64, fp64["state"], fp64["sp"]),
+                   "mixed": step_from_state(args, 1, device, fields64, fp64["state"], mixed["sp"])}
+            line["cpu_baseline"], line["parity_vs_oracle"] = oracle_step_leg(args, fields64, lab, fp64["state"], sw,
+                                                                             nxt)
+        except Exception as ex:  # the CPU leg must never hide the device number
+            line["cpu_baseline"] = {"value": None, "error": str(ex)[:300]}
     print(json.dumps(line), flush=True)
 
 
@@ -719,6 +798,287 @@ def kernels_main(args, device):
         case.close()
     print(json.dumps({"workload": f"kernels-{n}x{n}x{2 * n}", "cells": cells, "iters": args.iters,
                       "fields": "seeded U[-1, 1]", "kernels": out}), flush=True)
+
+
+def plain_main(args, device):
+    """The plain IMPACT step: 64 x 64 x 128 cells (periodic box 1 x 1 x 2), straight vessel of radius
+    0.25 L1 (label-5 inflow buffer on the first 10 planes, label-9 outlet on the last 10), pulsatile
+    plug inflow, Re = 200, dt = 0.2 x the CFL limit, 10 FP64 steps from rest, every Poisson solve
+    BiCGstab with the JOR preconditioner (omega = 0.8, 4 sweeps) to a 1e-8 relative residual.
+    Device: W warm-up and K timed runs of the 10 steps, each on a fresh case (CUDA events on the
+    case stream around the 10 steps).  CPU: the FP64 oracle's 10 steps on all host cores, and a
+    bounded single-core sample (steps 2-3: step 1 from rest has no Poisson work).  Parity of the
+    device's 10 steps against the all-core oracle run."""
+    import numpy as np
+    import torch
+
+    import impact_b200 as I
+    from impact_b200 import geometry as G
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    N, L, nsteps = (65, 65, 129), (1.0, 1.0, 2.0), 10
+    cells = 64 * 64 * 128
+    ig, og = I.Grid(N, L), O.Grid(N, L)
+    lab = G.straight_vessel(ig, radius_frac=0.25, n_in=10, n_out=10)
+    sp = I.step_params(Re=200.0, CFL=0.2, tol_rel=1e-8, n_sweeps=4, omega=0.8, max_it=2000, precond=0)
+
+    def device_run():
+        case = I.Case(ig, precision=0, device=device)
+        case.set_labels(lab)
+        stream = torch.cuda.ExternalStream(case.stream, device=device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        e0.record(stream)
+        its = []
+        for _ in range(nsteps):
+            st = case.step(sp)
+            its.append(list(st.poisson_iterations))
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        out = (ms, its, np.stack([case.download(f) for f in ("vel1", "vel2", "vel3")]), case.download("pre"))
+        case.close()
+        return out
+
+    for _ in range(args.warmup):
+        device_run()
+    sampler = ClockSampler(device)
+    runs = [device_run() for _ in range(args.steps)]
+    clocks = sampler.stop()
+    ms = sum(r[0] for r in runs) / len(runs)
+    _, dev_its, dvel, dpre = runs[-1]
+    # CPU: all cores, the full 10 steps
+    cores = O.set_threads(0)
+    vel, nl, pre = og.zeros(3), og.zeros(3), og.zeros()
+    st = O.OrcStepState()
+    op = O.step_params(Re=200.0, CFL=0.2, tol_rel=1e-8, n_sweeps=4, omega=0.8)
+    t_all, orc_its = [], []
+    for _ in range(nsteps):
+        t0 = time.perf_counter()
+        og.time_step(op, lab, vel, nl, pre, st)
+        t_all.append(time.perf_counter() - t0)
+        orc_its.append(list(st.poisson_iterations))
+    # CPU: one core, steps 1-3 of the same run (bounded sample)
+    O.set_threads(1)
+    v1, n1, p1 = og.zeros(3), og.zeros(3), og.zeros()
+    s1 = O.OrcStepState()
+    t_one = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        og.time_step(op, lab, v1, n1, p1, s1)
+        t_one.append(time.perf_counter() - t0)
+    O.set_threads(cores)
+    umax = max(float(np.abs(og.interior(vel[m])).max()) for m in range(3))
+    du = max(float(np.abs(og.interior(dvel[m]) - og.interior(vel[m])).max()) for m in range(3))
+    dp = float(np.abs(og.interior(dpre) - og.interior(pre)).max()) / float(np.abs(og.interior(pre)).max())
+    inner = _fluid_inner(og, lab)
+    w_all, g_all = og.test_divergence(vel), og.test_divergence(dvel)
+    w_in, g_in = og.test_divergence(vel, inner), og.test_divergence(dvel, inner)
+    one_ps = sum(t_one[1:]) / 2  # steps 2-3
+    all_ps_sampled = sum(t_all[1:3]) / 2
+    line = {"metric": METRIC, "value": round(cells * nsteps / (ms / 1e3) / 1e6, 3), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / nsteps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "plain-step-64x64x128", "cells": cells, "box": [1.0, 1.0, 2.0], "radius": 0.25,
+                       "Re": 200.0, "steps_per_run": nsteps, "poisson": "BiCGstab + JOR (omega 0.8, 4 sweeps) to 1e-8",
+                       "start": "rest", "timed": f"{args.steps} runs of the 10 steps, each on a fresh case",
+                       "l2_flush": "none: the whole case (about 0.3 GB) is L2-sized; each run starts from a fresh case"},
+            "clocks": clocks,
+            "iterations": {"device": dev_its, "oracle": orc_its},
+            "cpu_all_cores": {"value": cells * nsteps / sum(t_all) / 1e6, "unit": UNIT, "cores": cores,
+                              "kind": "port", "seconds_per_step": [round(t, 3) for t in t_all],
+                              "sample": "the FP64 oracle's 10 steps from rest"},
+            "cpu_single_core": {"value": cells / one_ps / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
+                                "seconds_per_step": [round(t, 3) for t in t_one],
+                                "all_cores_same_steps_s": all_ps_sampled,
+                                "sample": "steps 2-3 of the 10 on one thread (step 1 from rest has no Poisson work); "
+                                          "value = cells / their mean time"},
+            "parity_vs_oracle": {"velocity_max_abs_err_rel": du / umax, "pressure_max_abs_err_rel": dp,
+                                 "test_divergence": {"oracle": list(w_all), "device": list(g_all)},
+                                 "div_fluid_inner_max": {"oracle": w_in[0], "device": g_in[0]},
+                                 "after_steps": nsteps}}
+    print(json.dumps(line), flush=True)
+
+
+# Operator microbench: name, FP64 launcher, arguments builder key, algorithmic FP64 bytes per cell
+def operators_main(args, device):
+    """The operator microbench: 256 x 256 x 512 cells, x and y stretched by x_i = sinh(2 (i/N - 1/2)) /
+    sinh 1 (box 2 x 2 x 4), z uniform, i.i.d. U[-1, 1] fields from seeds.  Every operator of the
+    reference's launcher FFI in FP64, its _sp FP32 counterpart, and the reference's own CUDA kernel
+    (src/*_launcher.cu compiled from the reference tree for sm_100a, FP64) on the same device
+    fields: --iters launches each after 3 warm-ups, CUDA events on the launch stream; every field
+    exceeds the 126 MB L2 (FP64 270 MB, FP32 135 MB).  The FP64 oracle on all host cores gives
+    ns/cell and the values each result is compared with."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import impact_b200 as I
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    N, L, kinds = (257, 257, 513), (2.0, 2.0, 4.0), (1, 1, 0)
+    ig, og = I.Grid(N, L, kinds), O.Grid(N, L, kinds)
+    cells = 256 * 256 * 512
+    nx, ny, nz = (n + 7 for n in N)
+    refp = os.path.join(ROOT, "oracle", "_ref", "libref_kernels.so")
+    ref = C.CDLL(refp) if os.path.exists(refp) else None
+
+    def dv(a, f32=False):
+        return torch.from_numpy(np.ascontiguousarray(a.astype(np.float32) if f32 else a)).cuda(device)
+
+    def tab(name, a, f32):
+        return dv(ig.tab[name][a], f32)
+
+    def call(lib, name, spec):
+        keep, conv = [], []
+        for kind, v in spec:
+            if kind == "p":  # a device array: the launchers take double** / float** (by reference)
+                o = C.cast(C.c_void_p(int(v)), C.POINTER(C.c_double))
+            else:
+                o = {"i": C.c_int, "d": C.c_double, "f": C.c_float}[kind](v)
+            keep.append(o)
+            conv.append(C.byref(o))
+        getattr(lib, name)(*conv)
+
+    def timed(lib, name, spec, iters):
+        for _ in range(3):
+            call(lib, name, spec)
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(iters):
+            call(lib, name, spec)
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / iters
+
+    def err(d_out, want):
+        got = d_out.cpu().numpy().astype(np.float64)
+        return float(np.abs(og.interior(got) - og.interior(want)).max() / np.abs(og.interior(want)).max())
+
+    L64 = I.lib()
+    rows = {}
+    rng_seed = [2000]
+
+    def field(n=None):
+        rng_seed[0] += 1
+        a = og.random(rng_seed[0], n=n)
+        if n is None:
+            og.fill_ghosts(a)
+        else:
+            for m in range(n):
+                og.fill_ghosts(a[m])
+        return a
+
+    def run(key, name, build, cpu, bpc, out_init):
+        """build(f32, target) -> (spec, d_out); cpu() -> (oracle result, seconds)."""
+        want, secs = cpu()
+        r = {"bytes_per_cell_fp64": bpc, "cpu_ns_per_cell": round(1e9 * secs / cells, 3)}
+        for tag, lib, nm, f32 in (("fp64", L64, name + "_", False), ("fp32", L64, name + "_sp_", True),
+                                  ("reference", ref, name + "_", False)):
+            if lib is None:
+                continue
+            spec, d_out = build(f32)
+            ms = timed(lib, nm, spec, args.iters)
+            b = bpc * cells / (2 if f32 else 1)
+            spec, d_out = build(f32)  # fresh output (accumulating operators) for the values
+            call(lib, nm, spec)
+            torch.cuda.synchronize(device)
+            r[tag] = {"ms": round(ms, 4), "GB/s": round(b / (ms / 1e3) / 1e9, 1), "err_vs_oracle": err(d_out, want)}
+        if "reference" in r:
+            r["fp64_speedup_vs_reference"] = round(r["reference"]["ms"] / r["fp64"]["ms"], 2)
+        rows[key] = r
+
+    def cpu_timed(fn):
+        t0 = time.perf_counter()
+        w = fn()
+        return w, time.perf_counter() - t0
+
+    S = lambda f32: "f" if f32 else "d"  # noqa: E731
+    phi = field()
+    for m in (1, 2, 3):
+        def b_grad(f32, m=m):
+            d_in, d_out, t = dv(phi, f32), dv(og.zeros(), f32), tab("cG", m - 1, f32)
+            return ([("i", m), ("i", nx), ("i", ny), ("i", nz), ("i", 6), ("i", N[m - 1] + 1), ("p", d_in.data_ptr()),
+                     ("p", t.data_ptr()), ("p", d_out.data_ptr())], _Keep(d_out, d_in, t))
+        run(f"gradient_{m}", "gradient_launcher", b_grad, lambda m=m: cpu_timed(lambda: og.gradient(m, phi)), 16, None)
+    vel3 = field(3)
+
+    def b_div2(f32):
+        d_in, d_out = dv(vel3, f32), dv(og.zeros(), f32)
+        c = [tab("cD", a, f32) for a in range(3)]
+        return ([("i", nx), ("i", ny), ("i", nz), ("i", 6), ("i", 6), ("i", 6), ("p", d_in.data_ptr()),
+                 ("p", d_out.data_ptr())] + [("p", t.data_ptr()) for t in c], _Keep(d_out, d_in, *c))
+    run("divergence2", "divergence2_launcher", b_div2,
+        lambda: cpu_timed(lambda: og.divergence2(vel3[0], vel3[1], vel3[2])), 32, None)
+    u, nl0, pp = field(), field(), field()
+    for m in (1, 2, 3):
+        names = [("cuu" if a == m - 1 else "cpp") for a in range(3)]
+
+        def b_helm(f32, m=m, names=names):
+            d_in, d_out = dv(u, f32), dv(nl0, f32)
+            c = [tab(names[a], a, f32) for a in range(3)]
+            return ([("i", m), ("i", nx), ("i", ny), ("i", nz), ("i", 7), ("i", 7), ("i", 7), (S(f32), 1e-3),
+                     ("p", d_in.data_ptr()), ("p", d_out.data_ptr())] + [("p", t.data_ptr()) for t in c],
+                    _Keep(d_out, d_in, *c))
+        run(f"helmholtz_{m}", "helmholtz_explicit_launcher", b_helm,
+            lambda m=m: cpu_timed(lambda: og.helmholtz(m, 1e-3, u, nl0.copy())), 24, None)
+    for cid in range(1, 10):
+        m, a = (cid - 1) // 3 + 1, (cid - 1) % 3 + 1
+        up, dn = ("cNuU", "cNuD") if a == m else ("cNpU", "cNpD")
+
+        def b_up(f32, cid=cid, a=a, up=up, dn=dn):
+            d_pp, d_u, d_nl = dv(pp, f32), dv(u, f32), dv(nl0, f32)
+            t1, t2 = tab(up, a - 1, f32), tab(dn, a - 1, f32)
+            return ([("i", cid), ("i", nx), ("i", ny), ("i", nz), ("i", 7), ("i", N[a - 1] + 1),
+                     ("p", d_pp.data_ptr()), ("p", d_u.data_ptr()), ("p", d_nl.data_ptr()), ("p", t1.data_ptr()),
+                     ("p", t2.data_ptr())], _Keep(d_nl, d_pp, d_u, t1, t2))
+        run(f"upwind_{cid}", "nonlinear_upwind_launcher", b_up,
+            lambda cid=cid: cpu_timed(lambda: og.nonlinear_upwind(cid, pp, u, nl0.copy())), 24 if a == 1 else 32, None)
+    for m in (1, 2, 3):
+        for nm, tb, fn in (("interpolate2_pre_vel", "cIpu", og.interpolate_pre_vel),
+                           ("interpolate2_vel_pre", "cIup", og.interpolate_vel_pre)):
+            def b_int(f32, m=m, tb=tb):
+                d_in, d_out = dv(u, f32), dv(og.zeros(), f32)
+                t = tab(tb, m - 1, f32)
+                return ([("i", m), ("i", nx), ("i", ny), ("i", nz), ("i", 6), ("i", N[m - 1] + 1),
+                         ("p", d_in.data_ptr()), ("p", t.data_ptr()), ("p", d_out.data_ptr())], _Keep(d_out, d_in, t))
+            run(f"{nm}_{m}", nm + "_launcher", b_int, lambda m=m, fn=fn: cpu_timed(lambda: fn(m, u)), 16, None)
+    bb, rel = field(), field()
+
+    def b_jor(f32):
+        d_bb, d_rel, d_out = dv(bb, f32), dv(rel, f32), dv(og.zeros(), f32)
+        c = [tab("cdg", a, f32) for a in range(3)]
+        return ([("i", 1), ("i", nx), ("i", ny), ("i", nz), ("i", N[0]), ("i", N[1]), ("i", N[2]), ("i", 3),
+                 (S(f32), 0.8)] + [("p", t.data_ptr()) for t in c] +
+                [("p", d_rel.data_ptr()), ("p", d_bb.data_ptr()), ("p", d_out.data_ptr())], _Keep(d_out, d_bb, d_rel, *c))
+    run("jor_sweep", "jacobi_launcher", b_jor, lambda: cpu_timed(lambda: og.jacobi(bb.copy(), rel.copy(), 1, 0.8)), 24,
+        None)
+    peaks, note = measured_peaks()
+    tot = {t: sum(r[t]["ms"] for r in rows.values() if t in r) for t in ("fp64", "fp32", "reference")}
+    line = {"workload": "operators-256x256x512-stretched", "cells": cells, "iters": args.iters,
+            "grid": "x, y: x_i = sinh(2 (i/N - 1/2)) / sinh 1 (box 2 x 2 x 4), z uniform",
+            "fields": "seeded U[-1, 1], ghost layers filled periodically (the reference kernels read them)",
+            "cpu_cores": O.set_threads(0), "peak_hbm_gbs": peaks["hbm_gbs"], "peak_source": note,
+            "jor_50_sweeps_ms": {t: round(50 * rows["jor_sweep"][t]["ms"], 3) for t in ("fp64", "fp32", "reference")
+                                 if t in rows["jor_sweep"]},
+            "all_operators_ms": {t: round(v, 3) for t, v in tot.items()},
+            "reference_kernels": "oracle/_ref/libref_kernels.so" if ref is not None else "not built",
+            "operators": rows}
+    print(json.dumps(line), flush=True)
+
+
+class _Keep:
+    """Holds the device tensors of one launch alive; `first` is the output."""
+
+    def __init__(self, first, *rest):
+        self.first, self.rest = first, rest
+
+    def cpu(self):
+        return self.first.cpu()
 
 
 def extra_main(args, device, rank, world, dist):

@@ -311,6 +311,144 @@ extern "C" void product_dg_relax_launcher_(int* grid_id, int* nx_dev_g, int* ny_
 }
 
 // ---------------------------------------------------------------------------------------
+// Part 1b: FP32 launchers.  The reference's FP32 prior art (jor_kernel_v2_sp.cu,
+// jacobi_solver_host_v3_sp.f90:25-56) casts the fields and tables to real*4 and launches a
+// kernel named with the suffix _sp; these are the operator launchers above with that suffix:
+// same arguments, every array (fields and coefficient tables) and scalar in FP32, FP32
+// arithmetic and accumulation.
+// ---------------------------------------------------------------------------------------
+extern "C" void gradient_launcher_sp_(int* dimension_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nx_grad_coef,
+                                      int* ny_grad_coef, float** phi_grad_dev, float** cGp_dev, float** grad_dev) {
+  Geom g;
+  if (!geom_from_dev(*nx_dev, *ny_dev, *nz_dev, &g, "gradient_launcher_sp_")) return;
+  if (*nx_grad_coef != NG || *dimension_id < 1 || *dimension_id > 3) {
+    impact_set_error_msg(-1, "gradient_launcher_sp_: expects 6 coefficients per row and dimension_id 1..3");
+    return;
+  }
+  (void)ny_grad_coef;
+  launch_gradient<float>(*dimension_id, g, *cGp_dev, *phi_grad_dev, *grad_dev, g_stream);
+  check_launch("gradient_launcher_sp_");
+}
+
+extern "C" void divergence_launcher_sp_(int* dimension_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nx_div_coef,
+                                        int* ny_div_coef, float** phi_div_dev, float** div_dev, float** cD_dev) {
+  Geom g;
+  if (!geom_from_dev(*nx_dev, *ny_dev, *nz_dev, &g, "divergence_launcher_sp_")) return;
+  if (*nx_div_coef != ND || *dimension_id < 1 || *dimension_id > 3) {
+    impact_set_error_msg(-1, "divergence_launcher_sp_: expects 6 coefficients per row and dimension_id 1..3");
+    return;
+  }
+  (void)ny_div_coef;
+  launch_divergence<float>(*dimension_id, g, *cD_dev, *phi_div_dev, *div_dev, g_stream);
+  check_launch("divergence_launcher_sp_");
+}
+
+extern "C" void divergence2_launcher_sp_(int* nx_dev, int* ny_dev, int* nz_dev, int* nx_div_coef1, int* nx_div_coef2,
+                                         int* nx_div_coef3, float** phi_div2_dev, float** div2_dev, float** cDu1_dev,
+                                         float** cDv2_dev, float** cDw3_dev) {
+  Geom g;
+  if (!geom_from_dev(*nx_dev, *ny_dev, *nz_dev, &g, "divergence2_launcher_sp_")) return;
+  if (*nx_div_coef1 != ND || *nx_div_coef2 != ND || *nx_div_coef3 != ND) {
+    impact_set_error_msg(-1, "divergence2_launcher_sp_: expects 6 coefficients per row");
+    return;
+  }
+  const float* u = *phi_div2_dev;
+  launch_divergence2<float>(g, *cDu1_dev, *cDv2_dev, *cDw3_dev, u, u + g.nfield, u + 2 * g.nfield, *div2_dev,
+                            g_stream);
+  check_launch("divergence2_launcher_sp_");
+}
+
+extern "C" void helmholtz_explicit_launcher_sp_(int* component_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nxs1,
+                                                int* nxs2, int* nxs3, float* multL, float** vel1_dev, float** helm_dev,
+                                                float** cS1_helm_dev, float** cS2_helm_dev, float** cS3_helm_dev) {
+  Geom g;
+  if (!geom_from_dev(*nx_dev, *ny_dev, *nz_dev, &g, "helmholtz_explicit_launcher_sp_")) return;
+  if (*nxs1 != NB || *nxs2 != NB || *nxs3 != NB) {
+    impact_set_error_msg(-1, "helmholtz_explicit_launcher_sp_: expects 7 coefficients per row");
+    return;
+  }
+  launch_helmholtz<float>(*component_id, g, *cS1_helm_dev, *cS2_helm_dev, *cS3_helm_dev, *multL, *vel1_dev, *helm_dev,
+                          g_stream);
+  check_launch("helmholtz_explicit_launcher_sp_");
+}
+
+extern "C" void nonlinear_upwind_launcher_sp_(int* component_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nxn1,
+                                              int* nyn1, float** pp_dev, float** vel_dev, float** nl_dev,
+                                              float** cN1_dev, float** cN21_dev) {
+  Geom g;
+  if (!geom_from_dev(*nx_dev, *ny_dev, *nz_dev, &g, "nonlinear_upwind_launcher_sp_")) return;
+  if (*nxn1 != NB || *component_id < 1 || *component_id > 9) {
+    impact_set_error_msg(-1, "nonlinear_upwind_launcher_sp_: expects 7 coefficients per row and component_id 1..9");
+    return;
+  }
+  (void)nyn1;
+  launch_nonlinear_upwind<float>(*component_id, g, *cN1_dev, *cN21_dev, *pp_dev, *vel_dev, *nl_dev, g_stream);
+  check_launch("nonlinear_upwind_launcher_sp_");
+}
+
+extern "C" void interpolate2_pre_vel_launcher_sp_(int* dimension_id, int* nx_dev, int* ny_dev, int* nz_dev,
+                                                  int* nxIpu1, int* nyIpu1, float** phi_inter_pv_dev, float** cIpu_dev,
+                                                  float** inter_pv_dev) {
+  Geom g;
+  if (!geom_from_dev(*nx_dev, *ny_dev, *nz_dev, &g, "interpolate2_pre_vel_launcher_sp_")) return;
+  if (*nxIpu1 != NG || *dimension_id < 1 || *dimension_id > 3) {
+    impact_set_error_msg(-1, "interpolate2_pre_vel_launcher_sp_: expects 6 coefficients per row, dimension_id 1..3");
+    return;
+  }
+  (void)nyIpu1;
+  launch_interp_pre_vel<float>(*dimension_id, g, *cIpu_dev, *phi_inter_pv_dev, *inter_pv_dev, g_stream);
+  check_launch("interpolate2_pre_vel_launcher_sp_");
+}
+
+extern "C" void interpolate2_vel_pre_launcher_sp_(int* dimension_id, int* nx_dev, int* ny_dev, int* nz_dev,
+                                                  int* nxIup1, int* nyIup1, float** phi_inter_vp_dev, float** cIup_dev,
+                                                  float** inter_vp_dev) {
+  Geom g;
+  if (!geom_from_dev(*nx_dev, *ny_dev, *nz_dev, &g, "interpolate2_vel_pre_launcher_sp_")) return;
+  if (*nxIup1 != ND || *dimension_id < 1 || *dimension_id > 3) {
+    impact_set_error_msg(-1, "interpolate2_vel_pre_launcher_sp_: expects 6 coefficients per row, dimension_id 1..3");
+    return;
+  }
+  (void)nyIup1;
+  launch_interp_vel_pre<float>(*dimension_id, g, *cIup_dev, *phi_inter_vp_dev, *inter_vp_dev, g_stream);
+  check_launch("interpolate2_vel_pre_launcher_sp_");
+}
+
+extern "C" void axpby_launcher_sp_(int* nx_dev, int* ny_dev, int* nz_dev, float* a, float* b, float** d_x, float** d_y,
+                                   float** d_z) {
+  Geom g;
+  if (!geom_from_dev(*nx_dev, *ny_dev, *nz_dev, &g, "axpby_launcher_sp_")) return;
+  launch_axpby<float>(g, *a, *b, *d_x, *d_y, *d_z, g_stream);
+  check_launch("axpby_launcher_sp_");
+}
+
+extern "C" void jacobi_launcher_sp_(int* grid_id, int* nx_dev_g, int* ny_dev_g, int* nz_dev_g, int* ny_cdg1_g,
+                                    int* ny_cdg2_g, int* ny_cdg3_g, int* nx_cdg1_g, float* omega_g, float** cdg1_dev3,
+                                    float** cdg2_dev3, float** cdg3_dev3, float** rel_dev3, float** bb_dev3,
+                                    float** comp_dev3) {
+  Geom g;
+  if (!geom_from_dev(*nx_dev_g, *ny_dev_g, *nz_dev_g, &g, "jacobi_launcher_sp_")) return;
+  if (!cdg_level(*grid_id, *nx_cdg1_g, "jacobi_launcher_sp_")) return;
+  const long long lv = *grid_id - 1;
+  launch_jacobi<float>(g, *cdg1_dev3 + lv * *ny_cdg1_g * 3, *cdg2_dev3 + lv * *ny_cdg2_g * 3,
+                       *cdg3_dev3 + lv * *ny_cdg3_g * 3, *omega_g, *bb_dev3, *rel_dev3, *comp_dev3, g_stream);
+  check_launch("jacobi_launcher_sp_");
+}
+
+extern "C" void product_dg_relax_launcher_sp_(int* grid_id, int* nx_dev_g, int* ny_dev_g, int* nz_dev_g,
+                                              int* ny_cdg1_g, int* ny_cdg2_g, int* ny_cdg3_g, int* nx_cdg1_g,
+                                              float** cdg1_dev2, float** cdg2_dev2, float** cdg3_dev2,
+                                              float** rel_dev2, float** comp_dev2) {
+  Geom g;
+  if (!geom_from_dev(*nx_dev_g, *ny_dev_g, *nz_dev_g, &g, "product_dg_relax_launcher_sp_")) return;
+  if (!cdg_level(*grid_id, *nx_cdg1_g, "product_dg_relax_launcher_sp_")) return;
+  const long long lv = *grid_id - 1;
+  launch_dg_relax<float>(g, *cdg1_dev2 + lv * *ny_cdg1_g * 3, *cdg2_dev2 + lv * *ny_cdg2_g * 3,
+                         *cdg3_dev2 + lv * *ny_cdg3_g * 3, *rel_dev2, *comp_dev2, g_stream);
+  check_launch("product_dg_relax_launcher_sp_");
+}
+
+// ---------------------------------------------------------------------------------------
 // Part 2: device_jacobi_solver replacement (jacobi_solver_host_v4.f90:5-717)
 // ---------------------------------------------------------------------------------------
 namespace {

@@ -566,7 +566,8 @@ class launchers:
 
     @staticmethod
     def call(name, *args):
-        """args: ('i', int) | ('d', float) | ('p', device pointer)"""
+        """args: ('i', int) | ('d', float as FP64) | ('f', float as FP32) | ('p', device pointer);
+        the _sp_ launchers take their scalars as 'f'."""
         conv = []
         keep = []
         for kind, v in args:
@@ -574,6 +575,8 @@ class launchers:
                 o = C.c_int(int(v))
             elif kind == "d":
                 o = C.c_double(float(v))
+            elif kind == "f":
+                o = C.c_float(float(v))
             else:
                 o = C.cast(C.c_void_p(int(v)), _dp)
             keep.append(o)

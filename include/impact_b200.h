@@ -105,6 +105,41 @@ void product_dg_relax_launcher_(int* grid_id, int* nx_dev_g, int* ny_dev_g, int*
                                 int* ny_cdg2_g, int* ny_cdg3_g, int* nx_cdg1_g, double** cdg1_dev2,
                                 double** cdg2_dev2, double** cdg3_dev2, double** rel_dev2, double** comp_dev2);
 
+/* ---- Part 1b: FP32 launchers ------------------------------------------------------------
+ * The reference's FP32 prior art (jor_kernel_v2_sp.cu:5, jacobi_solver_host_v3_sp.f90:25-56)
+ * casts the fields and tables to real*4 and launches kernels suffixed _sp.  These are the
+ * operator launchers above with that suffix: the same arguments, every array (fields and
+ * coefficient tables c(lo:hi,0:N)) and scalar in FP32, FP32 arithmetic and accumulation.  No
+ * FP32 launcher of these operators exists in the reference; they replace the FP64 ones where a
+ * caller stages its fields in real*4. */
+void gradient_launcher_sp_(int* dimension_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nx_grad_coef,
+                           int* ny_grad_coef, float** phi_grad_dev, float** cGp_dev, float** grad_dev);
+void divergence_launcher_sp_(int* dimension_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nx_div_coef,
+                             int* ny_div_coef, float** phi_div_dev, float** div_dev, float** cD_dev);
+void divergence2_launcher_sp_(int* nx_dev, int* ny_dev, int* nz_dev, int* nx_div_coef1, int* nx_div_coef2,
+                              int* nx_div_coef3, float** phi_div2_dev, float** div2_dev, float** cDu1_dev,
+                              float** cDv2_dev, float** cDw3_dev);
+void helmholtz_explicit_launcher_sp_(int* component_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nxs1, int* nxs2,
+                                     int* nxs3, float* multL, float** vel1_dev, float** helm_dev,
+                                     float** cS1_helm_dev, float** cS2_helm_dev, float** cS3_helm_dev);
+void nonlinear_upwind_launcher_sp_(int* component_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nxn1, int* nyn1,
+                                   float** pp_dev, float** vel_dev, float** nl_dev, float** cN1_dev,
+                                   float** cN21_dev);
+void interpolate2_pre_vel_launcher_sp_(int* dimension_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nxIpu1,
+                                       int* nyIpu1, float** phi_inter_pv_dev, float** cIpu_dev,
+                                       float** inter_pv_dev);
+void interpolate2_vel_pre_launcher_sp_(int* dimension_id, int* nx_dev, int* ny_dev, int* nz_dev, int* nxIup1,
+                                       int* nyIup1, float** phi_inter_vp_dev, float** cIup_dev,
+                                       float** inter_vp_dev);
+void axpby_launcher_sp_(int* nx_dev, int* ny_dev, int* nz_dev, float* a, float* b, float** d_x, float** d_y,
+                        float** d_z);
+void jacobi_launcher_sp_(int* grid_id, int* nx_dev_g, int* ny_dev_g, int* nz_dev_g, int* ny_cdg1_g, int* ny_cdg2_g,
+                         int* ny_cdg3_g, int* nx_cdg1_g, float* omega_g, float** cdg1_dev3, float** cdg2_dev3,
+                         float** cdg3_dev3, float** rel_dev3, float** bb_dev3, float** comp_dev3);
+void product_dg_relax_launcher_sp_(int* grid_id, int* nx_dev_g, int* ny_dev_g, int* nz_dev_g, int* ny_cdg1_g,
+                                   int* ny_cdg2_g, int* ny_cdg3_g, int* nx_cdg1_g, float** cdg1_dev2,
+                                   float** cdg2_dev2, float** cdg3_dev2, float** rel_dev2, float** comp_dev2);
+
 /* ========================================================================================
  * Part 2: library control and device-resident entry points
  * ====================================================================================== */

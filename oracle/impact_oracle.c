@@ -1324,3 +1324,18 @@ void orc_ibm_spread(int N1, int N2, int N3, const double* const* xp, const doubl
   }
   ibm_free(dxp, dxu, dist);
 }
+
+/* Host threads of the OpenMP loops above (test infrastructure: the CPU baseline reports single-
+ * and all-core times).  n <= 0 leaves the setting unchanged; returns the threads now in use. */
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+int orc_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}

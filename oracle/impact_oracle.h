@@ -230,6 +230,9 @@ void orc_ibm_spread(int N1, int N2, int N3, const double* const* xp, const doubl
                     int delta_type, double reach, int n, const double* yb, const uint8_t* skip,
                     const double* fb, const double* node_vol, double* fd);
 
+/* OpenMP threads of the oracle's loops; n <= 0 queries.  Returns the threads in use. */
+int orc_set_threads(int n);
+
 #ifdef __cplusplus
 }
 #endif

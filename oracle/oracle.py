@@ -79,6 +79,7 @@ def lib():
             "orc_diff_coeffs": (i, [i, i, i, i, i, i, i, _dp, _dp, _dp]),
             "orc_get_stencil": (None, [i, _dp, _dp, _dp]),
             "orc_stability_limits": (None, [_dp]),
+            "orc_set_threads": (i, [i]),
             "orc_exchange": (None, [i, i, i, i, _dp]),
             "orc_gradient": (None, [i, i, i, i, P(OrcCoeffs), _dp, _dp]),
             "orc_divergence": (None, [i, i, i, i, P(OrcCoeffs), _dp, _dp]),
@@ -215,6 +216,28 @@ class Grid:
         for d in (1, 2, 3):
             lb.orc_exchange(d, *self.N, ptr(a))
         return a
+
+    # ---- divergence metric of the reference's in-code check ----
+    def divergence_weight(self):
+        """weight(i,j,k) = 1 / (sum_l |cDu1(l,i)| + sum_l |cDv2(l,j)| + sum_l |cDw3(l,k)|) at the
+        unique pressure points, shape (N3-1, N2-1, N1-1) (mod_coeffs.f90:2242-2262; the corner
+        zeroing of :2363 applies to walls only, never to a periodic box)."""
+        s = []
+        for a in range(3):
+            c = self.tab["cD"][a].reshape(self.N[a] + 1, N_DIV)
+            s.append(np.abs(c[1:self.N[a]]).sum(axis=1))
+        return 1.0 / (s[2][:, None, None] + s[1][None, :, None] + s[0][None, None, :])
+
+    def test_divergence(self, vel, where=None):
+        """(max |div2(vel)|, max |div2(vel) * weight|) over the unique pressure points, as the
+        reference's test_divergence prints them (mod_test.f90:300-345); `where` (bool, interior
+        shape) restricts both maxima to a subset of the points."""
+        d = self.interior(self.divergence2(vel[0], vel[1], vel[2]))
+        w = self.divergence_weight()
+        a, b = np.abs(d), np.abs(d * w)
+        if where is not None:
+            a, b = a[where], b[where]
+        return float(a.max()), float(b.max())
 
     # ---- operators ----
     def gradient(self, m, phi, out=None):
@@ -407,6 +430,11 @@ def step_params(Re=200.0, CFL=0.2, dtime_max=1e-2, dtime0=1e9, U0=1.0, T_pulse=1
     p = OrcStepParams(Re, CFL, dtime_max, dtime0, U0, T_pulse, level_pressure, o)
     p._keep = mg
     return p
+
+
+def set_threads(n: int) -> int:
+    """OpenMP threads of the oracle's loops (n <= 0: query); returns the threads in use."""
+    return int(lib().orc_set_threads(int(n)))
 
 
 def fd_exact(abl, n, deltaX0):

@@ -71,3 +71,31 @@ def test_time_step_vessel_runs_and_is_divergence_free():
     inflow = g.interior(lab) == G.INFLOW
     assert np.allclose(g.interior(vel[2])[inflow], u_in)
     assert np.all(g.interior(vel[0])[g.interior(lab) == G.SOLID] == 0.0)
+
+
+def test_divergence_metric_restates_the_reference_check():
+    """test_divergence (mod_test.f90:300-345): max |div2(u)| and max |div2(u) weight| with the
+    weight of mod_coeffs.f90:2242-2262, checked against loops over the tables; a field whose
+    components do not vary along their own axis has (discretely) zero divergence."""
+    og = O.Grid((13, 11, 17), (1.0, 0.8, 1.3), (1, 1, 0))
+    w = og.divergence_weight()
+    for (k, j, i) in [(0, 0, 0), (5, 3, 7), (15, 9, 11)]:
+        s = 0.0
+        for a, q in ((0, i + 1), (1, j + 1), (2, k + 1)):
+            c = og.tab["cD"][a]
+            s += sum(abs(c[q * 6 + l]) for l in range(6))
+        assert abs(w[k, j, i] - 1.0 / s) <= 1e-15 / s
+    vel = og.random(5, n=3)
+    d = og.interior(og.divergence2(vel[0], vel[1], vel[2]))
+    a, b = og.test_divergence(vel)
+    assert a == np.abs(d).max() and b == np.abs(d * w).max()
+    free = og.zeros(3)
+    rng = np.random.default_rng(6)
+    N1, N2, N3 = og.N
+    og.interior(free[0])[...] = rng.uniform(-1, 1, (N3 - 1, N2 - 1, 1))  # u(y, z)
+    og.interior(free[1])[...] = rng.uniform(-1, 1, (N3 - 1, 1, N1 - 1))  # v(x, z)
+    og.interior(free[2])[...] = rng.uniform(-1, 1, (1, N2 - 1, N1 - 1))  # w(x, y)
+    for m in range(3):
+        og.fill_ghosts(free[m])
+    a0, b0 = og.test_divergence(free)
+    assert a0 <= 1e-11 * a and b0 <= 1e-11 * b
