@@ -787,7 +787,7 @@ def kernels_main(args, device):
             case.upload(f, rng.uniform(-1.0, 1.0, grid.shape))
         if any(k[2] == "step" for k in todo):
             case.kernel_bench(13, 1)  # interpolated velocities for the rhs_vel passes
-        sp = I.solver_params(precond=1, omega=0.8, tile_kc=32, mg_down=3, mg_up=3, mg_bottom=3)
+        sp = I.solver_params(precond=1, omega=0.8, tile_kc=args.tile_kc, mg_down=3, mg_up=3, mg_bottom=3)
         for name, _, entry, kid, bpc in todo:
             if entry == "step":
                 ms = case.kernel_bench(kid, args.iters)

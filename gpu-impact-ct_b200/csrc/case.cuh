@@ -48,6 +48,7 @@ struct CaseState {
   const double* W64[3] = {};
   const float* W32[3] = {};
   int zuni = 0;      // every z row of the collapsed weights is the same (uniform z spacing)
+  int xuni = 0;      // every x row of the collapsed weights is the same (uniform x spacing)
   int cdg_zuni = 0;  // every z row of the fine compact Laplacian is the same
   // Poisson engines (a batch of one), built on first use and rebuilt when the solver
   // parameters or the right-hand side / solution fields change

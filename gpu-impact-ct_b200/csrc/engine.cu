@@ -810,7 +810,7 @@ __global__ void __launch_bounds__(AXNT, 3) k_kr_ax32(const KrylovJob<float>* __r
     const int q = find_job(ts, nj, b);
     const KrylovJob<float>& J = jobs[q];
     const SolverScalars* sc = J.sc;
-    if (MODE == 0 ? (sc->done != 0) : e_halted(sc)) continue;
+    if (J.vec || (MODE == 0 ? (sc->done != 0) : e_halted(sc))) continue;  // vector jobs: k_kr_ax32v
     const Geom g = J.g;
     const int ntx = (g.n1 + ETX - 1) / ETX, nty = (g.n2 + ETY - 1) / ETY;
     const int t0 = b - ts[q];
@@ -1032,6 +1032,255 @@ __global__ void __launch_bounds__(AXNT, 3) k_kr_ax32(const KrylovJob<float>* __r
     } else {
       __syncthreads();  // the ring and the weights are rewritten by the next tile
     }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// The FP32 operator on lists whose grids have n1 divisible by 4 and uniform x and z spacing
+// (every row of W[0] and of W[2] the same): the same collapsed 11-point product_div_grad as
+// k_kr_ax32, with the center weights of the three axes combined into one and every thread
+// owning one 16-byte vector of 4 consecutive x points of one row.
+//
+// A block of 8 x 8 threads owns one 32 x 8-column tile over kc planes.  Each plane of the tile
+// with its 5-wide halo is staged by 16-byte cp.async into a ring of AXV_R slots (48 x 18 floats:
+// columns i0-8 .. i0+39, rows j0-5 .. j0+12; chunks that would need periodic images are staged
+// element by element, on a separate branch that only threads at the box edges take), together
+// with the plane's inner-product partners (the tile's 32 x 8 points).  x neighbours come from the
+// thread's row of the slot (5 vectors), y neighbours from the 10 other rows (one vector each).
+// The z values k-5 .. k+AXV_B+4 of the 4 points stay in a register window of vectors moved on by
+// AXV_B planes per step; the window's new planes are 16-byte loads from global memory issued one
+// step ahead.  The ring holds three groups of AXV_B planes: a step computes on one while the
+// next two are in flight.
+constexpr int AXV_TX = ETX / 4, AXV_NT = AXV_TX * ETY;   // 8 x 8 threads, 4 columns each
+constexpr int AXV_HX = 8;                                // staged columns left of the tile
+constexpr int AXV_W = ETX + 16;                          // staged row: 8 + 32 + 8 (5 needed each side)
+constexpr int AXV_H = ETY + 10;                          // staged rows
+constexpr int AXV_CR = AXV_W / 4;                        // 16-byte chunks per row
+constexpr int AXV_NCH = AXV_CR * AXV_H;                  // chunks per plane
+constexpr int AXV_PER = (AXV_NCH + AXV_NT - 1) / AXV_NT; // chunks per thread and plane
+constexpr int AXV_PLANE = AXV_W * AXV_H;                 // floats per slot
+constexpr int AXV_PP = ETX * ETY;                        // partner floats per slot
+constexpr int AXV_B = 4;                                 // planes per step
+constexpr int AXV_G = 3;                                 // groups of AXV_B planes in the ring
+constexpr int AXV_R = AXV_B * AXV_G;                     // ring slots
+constexpr int AXV_ZW = AXV_B + 10;                       // z window (planes t-5 .. t+AXV_B+4)
+static_assert((AXV_PLANE * 4) % 16 == 0 && (AXV_PP * 4) % 16 == 0, "slots must keep 16-byte alignment");
+constexpr size_t axv_smem_bytes() { return sizeof(float) * (size_t)AXV_R * (AXV_PLANE + AXV_PP); }
+
+__device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+
+template <int MODE>
+__global__ void __launch_bounds__(AXV_NT, 4) k_kr_ax32v(const KrylovJob<float>* __restrict__ jobs,
+                                                        const int* __restrict__ ts, int nj, int ntiles,
+                                                        double* __restrict__ partial) {
+  static_assert(MODE >= 0 && MODE <= 2, "FP32 operator modes: 0 residual, 1 alpha, 2 omega");
+  extern __shared__ __align__(16) unsigned char axv_smem[];
+  float* ring = reinterpret_cast<float*>(axv_smem);
+  float* pring = ring + (size_t)AXV_R * AXV_PLANE;
+  __shared__ double red[2][AXV_NT / 32];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + AXV_TX * ty;
+  const int cx = AXV_HX + 4 * tx;   // the thread's first column in a staged row
+  const int pq = ty * ETX + 4 * tx;  // the thread's vector in a partner slot
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const KrylovJob<float>& J = jobs[q];
+    const SolverScalars* sc = J.sc;
+    if (!J.vec || (MODE == 0 ? (sc->done != 0) : e_halted(sc))) continue;  // the others: k_kr_ax32
+    const Geom g = J.g;
+    const int ntx = (g.n1 + ETX - 1) / ETX, nty = (g.n2 + ETY - 1) / ETY;
+    const int t0 = b - ts[q];
+    const int ta = t0 % ntx, tr = t0 / ntx, tc = tr / nty;
+    const int i0 = ta * ETX + 1, j0 = (tr - tc * nty) * ETY + 1;
+    const int k0 = tc * J.kc + 1, k1 = min(g.n3, k0 + J.kc - 1);
+    const int nk = k1 - k0 + 1;
+    const int i = i0 + 4 * tx, j = j0 + ty;
+    const bool act = i <= g.n1 && j <= g.n2;  // n1 % 4 == 0: the 4 columns are valid together
+    const float* __restrict__ x = MODE == 0 ? J.phi : (MODE == 1 ? J.z1 : J.z2);
+    float* __restrict__ out = MODE == 0 ? J.rr : (MODE == 1 ? J.Ap : J.Ar);
+    const float* __restrict__ d1 = MODE == 1 ? J.rh : J.rr;
+    const long long nxy = g.nxy;
+    // weights: x and z uniform (first rows), y of this thread's row; the three center weights
+    // combined
+    float wx[AXW], wy[AXW], wz[AXW];
+    const int jr = j <= g.n2 ? j : 1;
+#pragma unroll
+    for (int l = 0; l < AXW; ++l) {
+      wx[l] = __ldg(J.W[0] + l);
+      wy[l] = __ldg(J.W[1] + (size_t)(jr - 1) * AXW + l);
+      wz[l] = __ldg(J.W[2] + l);
+    }
+    const float wc = __fadd_rn(__fadd_rn(wx[5], wy[5]), wz[5]);
+    // this thread's chunks of a staged plane: chunk cq = tid + e*AXV_NT holds columns
+    // i0-8+4(cq%12) .. +3 of row j0-5+cq/12.  The points of the tile read columns
+    // i0-5 .. min(i0+31, n1)+5 and rows j0-5 .. min(j0+7, n2)+5.  In a tile whose needed columns
+    // are all interior (1..n1) every needed chunk is one 16-byte copy (cb[e] = its in-plane
+    // offset, -1 for a chunk nothing needs); the tiles at the x ends of the box take the element
+    // path, which copies the needed columns one by one from their periodic images.
+    const int ilast = min(i0 + ETX - 1, g.n1) + 5, jlast = min(j0 + ETY - 1, g.n2) + 5;
+    const bool tile_vec = i0 - 5 >= 1 && ilast <= g.n1;  // block-uniform
+    int cb[AXV_PER];
+#pragma unroll
+    for (int e = 0; e < AXV_PER; ++e) {
+      const int cq = tid + e * AXV_NT;
+      const int r = cq / AXV_CR, c0 = (cq % AXV_CR) * 4;
+      const int jj = j0 - 5 + r, ii = i0 - AXV_HX + c0;
+      const bool need = cq < AXV_NCH && jj <= jlast && max(ii, i0 - 5) <= min(ii + 3, ilast);
+      cb[e] = need ? (ii + 3) + g.nx * (wrapi(jj, g.n2) + 3) : -1;
+    }
+    const int own = (act ? i + 3 : 4) + g.nx * (jr + 3);  // in-plane offset of the thread's vector
+    auto zoff = [&](int k) -> long long {  // plane k (periodic) + 3 ghost planes
+      return (long long)((k < 1 ? k + g.n3 : (k > g.n3 ? k - g.n3 : k)) + 3) * nxy;
+    };
+    // group gi: planes t = gi*AXV_B .. +AXV_B-1 of the tile (t < nk) and their partners into
+    // their slots
+    auto stage_group = [&](int gi) {
+#pragma unroll
+      for (int u = 0; u < AXV_B; ++u) {
+        const int t = gi * AXV_B + u;
+        if (t < nk) {
+          const long long zo = zoff(k0 + t);
+          const float* src = x + zo;
+          float* dst = ring + (size_t)(t % AXV_R) * AXV_PLANE + tid * 4;
+          if (tile_vec) {
+#pragma unroll
+            for (int e = 0; e < AXV_PER; ++e)
+              if (cb[e] >= 0) cp_async16(dst + e * AXV_NT * 4, src + cb[e]);
+          } else {
+            for (int e = 0; e < AXV_PER; ++e) {
+              const int cq = tid + e * AXV_NT;
+              const int r = cq / AXV_CR, c0 = (cq % AXV_CR) * 4;
+              const int jj = j0 - 5 + r;
+              if (cb[e] < 0) continue;  // nothing of this chunk is needed
+              const int rowoff = g.nx * (wrapi(jj, g.n2) + 3);
+              for (int v = 0; v < 4; ++v) {
+                const int ii = i0 - AXV_HX + c0 + v;
+                if (ii >= i0 - 5 && ii <= ilast) cp_async1(dst + e * AXV_NT * 4 + v, src + (wrapi(ii, g.n1) + 3) + rowoff);
+              }
+            }
+          }
+          if (MODE != 0 && act) cp_async16(pring + (size_t)(t % AXV_R) * AXV_PP + pq, d1 + zo + own);
+        }
+      }
+      cp_commit();
+    };
+    __syncthreads();  // the ring is free (previous tile done)
+#pragma unroll
+    for (int gi = 0; gi < AXV_G - 1; ++gi) stage_group(gi);
+    // z window: planes k0-5 .. k0+AXV_B+4
+    float4 win[AXV_ZW];
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int l = 0; l < AXV_ZW; ++l) win[l] = act ? ldg4(x + zoff(k0 - 5 + l) + own) : zero4;
+    double v0 = 0.0, v1 = 0.0;
+    float* o = out + (long long)(k0 + 3) * nxy + own;
+    const int nsteps = (nk + AXV_B - 1) / AXV_B;
+    for (int s = 0; s < nsteps; ++s) {
+      const int tb = s * AXV_B;
+      cp_wait<AXV_G - 2>();  // this thread's copies of the step's group have landed
+      __syncthreads();       // everybody's have; the previous step's group is free
+      stage_group(s + AXV_G - 1);
+      // the next step's window planes
+      float4 nw[AXV_B];
+      const bool more = act && tb + AXV_B < nk;
+#pragma unroll
+      for (int u = 0; u < AXV_B; ++u) nw[u] = more ? ldg4(x + zoff(k0 + tb + AXV_B + 5 + u) + own) : zero4;
+#pragma unroll
+      for (int u = 0; u < AXV_B; ++u) {
+        const int t = tb + u;
+        if (t < nk) {
+          const float* sp = ring + (size_t)(t % AXV_R) * AXV_PLANE;
+          // x: the thread's row, columns cx-8 .. cx+11 (own vector at 8..11)
+          float xv[20];
+#pragma unroll
+          for (int m = 0; m < 5; ++m) {
+            const float4 v = lds4(sp + (ty + 5) * AXV_W + cx - 8 + 4 * m);
+            xv[4 * m] = v.x;
+            xv[4 * m + 1] = v.y;
+            xv[4 * m + 2] = v.z;
+            xv[4 * m + 3] = v.w;
+          }
+          const float4 cc = win[u + 5];
+          float r0 = mulT(wc, cc.x), r1 = mulT(wc, cc.y), r2 = mulT(wc, cc.z), r3 = mulT(wc, cc.w);
+#pragma unroll
+          for (int l = 0; l < AXW; ++l) {
+            if (l == 5) continue;
+            r0 = fmaT(wx[l], xv[3 + l], r0);
+            r1 = fmaT(wx[l], xv[4 + l], r1);
+            r2 = fmaT(wx[l], xv[5 + l], r2);
+            r3 = fmaT(wx[l], xv[6 + l], r3);
+          }
+          // y: rows ty .. ty+10 of the slot (ty+5 is the thread's own)
+          float y0 = 0.f, y1 = 0.f, y2 = 0.f, y3 = 0.f;
+#pragma unroll
+          for (int l = 0; l < AXW; ++l) {
+            if (l == 5) continue;
+            const float4 v = lds4(sp + (ty + l) * AXV_W + cx);
+            y0 = fmaT(wy[l], v.x, y0);
+            y1 = fmaT(wy[l], v.y, y1);
+            y2 = fmaT(wy[l], v.z, y2);
+            y3 = fmaT(wy[l], v.w, y3);
+          }
+          // z: the window
+          float z0 = 0.f, z1 = 0.f, z2 = 0.f, z3 = 0.f;
+#pragma unroll
+          for (int l = 0; l < AXW; ++l) {
+            if (l == 5) continue;
+            z0 = fmaT(wz[l], win[u + l].x, z0);
+            z1 = fmaT(wz[l], win[u + l].y, z1);
+            z2 = fmaT(wz[l], win[u + l].z, z2);
+            z3 = fmaT(wz[l], win[u + l].w, z3);
+          }
+          r0 = __fadd_rn(__fadd_rn(r0, y0), z0);
+          r1 = __fadd_rn(__fadd_rn(r1, y1), z1);
+          r2 = __fadd_rn(__fadd_rn(r2, y2), z2);
+          r3 = __fadd_rn(__fadd_rn(r3, y3), z3);
+          if (act) {
+            *reinterpret_cast<float4*>(o) = make_float4(r0, r1, r2, r3);
+            if (MODE != 0) {
+              const float4 pv = lds4(pring + (size_t)(t % AXV_R) * AXV_PP + pq);
+              v0 += (double)r0 * (double)pv.x;
+              v0 += (double)r1 * (double)pv.y;
+              v0 += (double)r2 * (double)pv.z;
+              v0 += (double)r3 * (double)pv.w;
+            }
+            if (MODE == 2) {
+              v1 += (double)r0 * (double)r0;
+              v1 += (double)r1 * (double)r1;
+              v1 += (double)r2 * (double)r2;
+              v1 += (double)r3 * (double)r3;
+            }
+          }
+          o += nxy;
+        }
+      }
+#pragma unroll
+      for (int l = 0; l < AXV_ZW - AXV_B; ++l) win[l] = win[l + AXV_B];
+#pragma unroll
+      for (int u = 0; u < AXV_B; ++u) win[AXV_ZW - AXV_B + u] = nw[u];
+    }
+    cp_wait<0>();
+    if (MODE != 0) {
+      v0 = e_wsum(v0);
+      v1 = e_wsum(v1);
+      if ((tid & 31) == 0) {
+        red[0][tid >> 5] = v0;
+        red[1][tid >> 5] = v1;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int w = 0; w < AXV_NT / 32; ++w) {
+          s0 += red[0][w];
+          s1 += red[1][w];
+        }
+        partial[(long long)b * 4] = s0;
+        if (MODE == 2) partial[(long long)b * 4 + 1] = s1;
+      }
+    }
+    // the ring and red are rewritten by the next tile only after its first barrier
   }
 }
 
@@ -2168,6 +2417,9 @@ void ax_attributes() {
   cudaFuncSetAttribute(k_kr_ax32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axa_smem_bytes());
   cudaFuncSetAttribute(k_kr_ax32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axa_smem_bytes());
   cudaFuncSetAttribute(k_kr_ax32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axa_smem_bytes());
+  cudaFuncSetAttribute(k_kr_ax32v<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axv_smem_bytes());
+  cudaFuncSetAttribute(k_kr_ax32v<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axv_smem_bytes());
+  cudaFuncSetAttribute(k_kr_ax32v<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axv_smem_bytes());
   cudaFuncSetAttribute(k_lv_tail<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_BYTES);
   cudaFuncSetAttribute(k_lv_tail<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_BYTES);
 #define IMPACT_MULTI_ATTR(T, N, I, R)                                                                           \
@@ -2200,13 +2452,19 @@ inline int grid_for(int ntiles) {
 }
 const dim3 kBlock(ETX, ETY);
 const dim3 kAxBlock(ETX, AXTY);  // k_kr_ax: two rows per thread
-// the operator over a Krylov list: FP32 by the 16-byte staged, stepped kernel
+// the operator over a Krylov list: FP32 by the vector kernel where every job qualifies (vec:
+// n1 divisible by 4, uniform x and z weights), else by the 16-byte staged, stepped kernel
 template <typename T, int MODE>
-void launch_ax(int grid, const KrylovJob<T>* J, const int* ts, int n, int ntiles, double* partial, cudaStream_t s) {
-  if constexpr (std::is_same<T, float>::value && MODE <= 2)
-    k_kr_ax32<MODE><<<grid, kAxBlock, axa_smem_bytes(), s>>>(J, ts, n, ntiles, partial);
-  else
+void launch_ax(int grid, const KrylovJob<T>* J, const int* ts, int n, int ntiles, double* partial, cudaStream_t s,
+               int vec) {
+  if constexpr (std::is_same<T, float>::value && MODE <= 2) {
+    if (vec != 0) k_kr_ax32v<MODE><<<grid, dim3(AXV_TX, ETY), axv_smem_bytes(), s>>>(J, ts, n, ntiles, partial);
+    if (vec != 1) k_kr_ax32<MODE><<<grid, kAxBlock, axa_smem_bytes(), s>>>(J, ts, n, ntiles, partial);
+    if (vec == 2) prof::count(1);  // two launches where the callers count one
+  } else {
+    (void)vec;
     k_kr_ax<T, MODE><<<grid, kAxBlock, ax_smem_bytes<T>(), s>>>(J, ts, n, ntiles, partial);
+  }
 }
 // the fused smoothing kernel runs one block per tile (one block per SM at a time)
 inline int grid_multi(int ntiles) { return ntiles; }
@@ -2370,6 +2628,7 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
       J.kc = kc;
       for (int m = 0; m < 3; ++m) J.W[m] = C.W[m];
       J.zuni = C.zuni;
+      J.xuni = C.xuni;
       J.bb = C.bb;
       J.phi = C.phi;
       J.rr = C.rr;
@@ -2382,6 +2641,19 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
       J.sc = scal_ + c;
       kt[c] = tiles_of(C.g, kc);
     }
+    // the FP32 operator's vector kernel takes the jobs whose grids have n1 % 4 == 0 (16-byte
+    // vectors of 4 x points), 16-byte aligned fields and uniform x and z weights (it keeps one row
+    // of each); the others stay with the staged kernel.  The choice is per job, so a case's
+    // result does not depend on the other cases of its batch.
+    int nv = 0;
+    for (auto& J : kj) {
+      const void* f[] = {J.phi, J.z1, J.z2, J.rr, J.Ap, J.Ar, J.rh};
+      bool al = true;
+      for (const void* q : f) al = al && (reinterpret_cast<uintptr_t>(q) & 15) == 0;
+      J.vec = std::is_same<T, float>::value && J.g.n1 % 4 == 0 && J.xuni && J.zuni && al;
+      nv += J.vec;
+    }
+    kr_vec_ = nv == 0 ? 0 : (nv == n ? 1 : 2);
     kr_list_ = arena_.add(kj, kt);
   }
   // ---- preconditioner schedules ----
@@ -2722,11 +2994,11 @@ void Engine<T>::enqueue_iteration() {
   prof::count(1);
   IMPACT_PROF(prof::K_P_UPDATE, 4 * fb, s, (k_kr_p<T><<<grid, kBlock, 0, s>>>(J, K.ts, n, K.ntiles)));
   enqueue_precond(0);
-  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (launch_ax<T, 1>(grid, J, K.ts, n, K.ntiles, partial_, s)));
+  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (launch_ax<T, 1>(grid, J, K.ts, n, K.ntiles, partial_, s, kr_vec_)));
   k_efin<<<n, 256, 0, s>>>(K.ts, partial_, 1, 0, EFIN_ALPHA, scal_, nullptr);
   IMPACT_PROF(prof::K_R_UPDATE, 3 * fb, s, (k_kr_r<T><<<grid, kBlock, 0, s>>>(J, K.ts, n, K.ntiles)));
   enqueue_precond(1);
-  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (launch_ax<T, 2>(grid, J, K.ts, n, K.ntiles, partial_, s)));
+  IMPACT_PROF(prof::K_DIVGRAD, 3 * fb, s, (launch_ax<T, 2>(grid, J, K.ts, n, K.ntiles, partial_, s, kr_vec_)));
   k_efin<<<n, 256, 0, s>>>(K.ts, partial_, 2, 0, EFIN_OMEGA, scal_, nullptr);
   IMPACT_PROF(prof::K_X_UPDATE, 8 * fb, s, (k_kr_x<T><<<grid, kBlock, 0, s>>>(J, K.ts, n, K.ntiles, partial_)));
   k_efin<<<n, 256, 0, s>>>(K.ts, partial_, 3, 1, EFIN_NORMS, scal_, nullptr);
@@ -2766,7 +3038,7 @@ int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::
   const KrylovJob<T>* J = static_cast<const KrylovJob<T>*>(K.jobs);
   const int grid = grid_for(K.ntiles);
   if (!zero_phi) {
-    launch_ax<T, 0>(grid, J, K.ts, n, K.ntiles, partial_, s_);
+    launch_ax<T, 0>(grid, J, K.ts, n, K.ntiles, partial_, s_, kr_vec_);
     prof::count(1);
   }
   IMPACT_PROF(prof::K_KR_INIT, 4.0 * sizeof(T) * cells_[kr_list_], s_,
@@ -2861,7 +3133,7 @@ int Engine<T>::apply_operator() {
   if (e != cudaSuccess) return impact_set_error(e, "engine scalars", __FILE__, __LINE__);
   const DevList& K = arena_.lists[kr_list_];
   const KrylovJob<T>* J = static_cast<const KrylovJob<T>*>(K.jobs);
-  launch_ax<T, 0>(grid_for(K.ntiles), J, K.ts, n, K.ntiles, partial_, s_);
+  launch_ax<T, 0>(grid_for(K.ntiles), J, K.ts, n, K.ntiles, partial_, s_, kr_vec_);
   prof::count(1);
   e = cudaStreamSynchronize(s_);
   if (e != cudaSuccess) return impact_set_error(e, "engine operator", __FILE__, __LINE__);
@@ -2909,11 +3181,11 @@ int Engine<T>::bench(int kind, int iters, double* ms, double* bytes) {
     }
     case 5:
       by = 3 * sz * fc;
-      f = [&]() { launch_ax<T, 1>(grid, J, K.ts, n, K.ntiles, partial_, s_); };
+      f = [&]() { launch_ax<T, 1>(grid, J, K.ts, n, K.ntiles, partial_, s_, kr_vec_); };
       break;
     case 6:
       by = 3 * sz * fc;
-      f = [&]() { launch_ax<T, 2>(grid, J, K.ts, n, K.ntiles, partial_, s_); };
+      f = [&]() { launch_ax<T, 2>(grid, J, K.ts, n, K.ntiles, partial_, s_, kr_vec_); };
       break;
     case 7:
       by = 8 * sz * fc;
@@ -3017,6 +3289,7 @@ int MixedEngine::build(const std::vector<Case>& cs, const EngineParams& p, cudaS
     A.kc = kc;
     for (int m = 0; m < 3; ++m) A.W[m] = C.W64[m];
     A.zuni = C.zuni;
+    A.xuni = C.xuni;
     A.phi = C.x;
     A.bb = C.bb;
     A.rr = C.r64;

@@ -73,6 +73,8 @@ struct KrylovJob {
   int kc;
   const T* W[3];  // collapsed product_div_grad weights, row (i-1) holds offsets -5..5
   int zuni;       // 1: every z row of W[2] is the same (uniform z spacing)
+  int xuni;       // 1: every x row of W[0] is the same (uniform x spacing)
+  int vec;        // FP32: the operator of this job runs in the 4-point vector kernel
   const T* bb;
   T* phi;
   T *rr, *rh, *pp, *Ap, *Ar, *z1, *z2;
@@ -105,6 +107,7 @@ struct EngineCase {
   Geom g;
   const T* W[3];         // collapsed operator weights (device)
   int zuni;              // 1: every z row of W[2] is the same
+  int xuni = 0;          // 1: every x row of W[0] is the same
   const T* cdg[3];       // fine-level compact Laplacian (device)
   int cdg_zuni;          // 1: every z row of cdg[2] is the same
   const MGData<T>* mg;   // multigrid hierarchy (level >= 1 fields owned by the case), or null
@@ -207,6 +210,7 @@ class Engine {
   // the profiler)
   std::vector<double> cells_, cells_f_, cells_c_;
   std::vector<char> fast_;  // per list: every job vectorised with uniform z (k_lv_fast)
+  int kr_vec_ = 0;          // FP32 Krylov list: jobs in the vector kernel -- 0 none, 1 all, 2 some
 };
 
 // Mixed precision: FP64 residual and correction around the FP32 engine.
@@ -216,6 +220,7 @@ class MixedEngine {
     Geom g;
     const double* W64[3];
     int zuni;
+    int xuni = 0;
     const double* bb;
     double* x;
     double* r64;

@@ -506,6 +506,7 @@ extern "C" int impact_b200_case_create(const impact_b200_case_desc* desc, const 
     // uniform z spacing: all z rows equal up to rounding of the table construction (1e-14 of the
     // largest weight), then the kernels keep one row in registers
     s.zuni = rows_uniform(w[2].data(), w[2].size() / AXW, AXW);
+    s.xuni = rows_uniform(w[0].data(), w[0].size() / AXW, AXW);
     s.cdg_zuni = rows_uniform(co->axis[2]->cdg, (size_t)(desc->N3 - 1), 3);
     std::vector<float> all32(all.begin(), all.end());
     cudaMemcpy(d64, all.data(), tot * sizeof(double), cudaMemcpyHostToDevice);
@@ -796,6 +797,7 @@ static int ensure_engine(CaseState& s, const double* b, double* x, const EngineP
       ec.cdg[m] = s.c64.cdg[m];
     }
     ec.zuni = s.zuni;
+    ec.xuni = s.xuni;
     ec.cdg_zuni = s.cdg_zuni;
     ec.mg = s.mg_levels ? &s.mg64 : nullptr;
     ec.bb = b;
@@ -818,6 +820,7 @@ static int ensure_engine(CaseState& s, const double* b, double* x, const EngineP
     mc.g = s.g;
     for (int m = 0; m < 3; ++m) mc.W64[m] = s.W64[m];
     mc.zuni = s.zuni;
+    mc.xuni = s.xuni;
     mc.bb = b;
     mc.x = x;
     mc.r64 = s.mw.r64;
@@ -830,6 +833,7 @@ static int ensure_engine(CaseState& s, const double* b, double* x, const EngineP
       ec.cdg[m] = s.c32.cdg[m];
     }
     ec.zuni = s.zuni;
+    ec.xuni = s.xuni;
     ec.cdg_zuni = s.cdg_zuni;
     ec.mg = s.mg_levels ? &s.mg32 : nullptr;
     ec.bb = s.mw.r32;
@@ -955,6 +959,7 @@ extern "C" int impact_b200_case_precond(impact_b200_case* c, int field_in, int f
       ef.cdg[m] = s.c32.cdg[m];
     }
     ef.zuni = s.zuni;
+    ef.xuni = s.xuni;
     ef.cdg_zuni = s.cdg_zuni;
     ef.mg = s.mg_levels ? &s.mg32 : nullptr;
     const KrylovWork<float>& w = s.mw.inner;
@@ -988,6 +993,7 @@ extern "C" int impact_b200_case_precond(impact_b200_case* c, int field_in, int f
     ec.cdg[m] = s.c64.cdg[m];
   }
   ec.zuni = s.zuni;
+  ec.xuni = s.xuni;
   ec.cdg_zuni = s.cdg_zuni;
   ec.mg = s.mg_levels ? &s.mg64 : nullptr;
   const KrylovWork<double>& w = s.kw64;
@@ -1043,6 +1049,7 @@ extern "C" int impact_b200_case_apply(impact_b200_case* c, int op, int field_in,
       ef.cdg[m] = s.c32.cdg[m];
     }
     ef.zuni = s.zuni;
+    ef.xuni = s.xuni;
     ef.cdg_zuni = s.cdg_zuni;
     ef.mg = nullptr;
     ef.bb = ef.phi = buf;
@@ -1070,6 +1077,7 @@ extern "C" int impact_b200_case_apply(impact_b200_case* c, int op, int field_in,
     ec.cdg[m] = s.c64.cdg[m];
   }
   ec.zuni = s.zuni;
+  ec.xuni = s.xuni;
   ec.cdg_zuni = s.cdg_zuni;
   ec.mg = nullptr;
   // field_out = A field_in (product_div_grad); the Krylov work fields of an FP64 case or the
@@ -1337,6 +1345,7 @@ static int batch_engine(impact_b200_batch* b, const impact_b200_solver_params* p
         E.cdg[m] = s.c64.cdg[m];
       }
       E.zuni = s.zuni;
+      E.xuni = s.xuni;
       E.cdg_zuni = s.cdg_zuni;
       E.mg = s.mg_levels ? &s.mg64 : nullptr;
       E.bb = s.f[IMPACT_B200_RES];
@@ -1362,6 +1371,7 @@ static int batch_engine(impact_b200_batch* b, const impact_b200_solver_params* p
     M.g = s.g;
     for (int m = 0; m < 3; ++m) M.W64[m] = s.W64[m];
     M.zuni = s.zuni;
+    M.xuni = s.xuni;
     M.bb = s.f[IMPACT_B200_RES];
     M.x = s.f[IMPACT_B200_PRE];
     M.r64 = s.mw.r64;
@@ -1374,6 +1384,7 @@ static int batch_engine(impact_b200_batch* b, const impact_b200_solver_params* p
       E.cdg[m] = s.c32.cdg[m];
     }
     E.zuni = s.zuni;
+    E.xuni = s.xuni;
     E.cdg_zuni = s.cdg_zuni;
     E.mg = s.mg_levels ? &s.mg32 : nullptr;
     E.bb = s.mw.r32;

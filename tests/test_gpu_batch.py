@@ -10,9 +10,12 @@ from impact_b200 import geometry as G
 
 pytestmark = pytest.mark.gpu
 
+# the 22 x 20 x 40 case (n1 not divisible by 4) runs the FP32 operator's staged kernel, the others
+# its vector kernel: in a batch both kernels run, each on its own cases
 SPECS = [((17, 17, 33), 200.0, 1.0, [(1.0, 0.5, 0.125)]),
          ((25, 21, 41), 500.0, 0.7, []),
-         ((33, 33, 65), 350.0, 1.3, [(0.6, 0.4, 0.1), (1.4, 0.6, 0.15)])]
+         ((33, 33, 65), 350.0, 1.3, [(0.6, 0.4, 0.1), (1.4, 0.6, 0.15)]),
+         ((23, 21, 41), 300.0, 0.9, [])]
 
 
 def _make(spec, precision):

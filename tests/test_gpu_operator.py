@@ -9,7 +9,9 @@ and wrapped chunks, unaligned rows (every chunk element-wise), ragged x / y tile
 that the step depth (four planes in FP32, two in FP64) does not divide, the smallest grid the
 library accepts and a stretched z axis (per-plane weights).  Bar: 1e-12 of max|A x| in FP64; 1e-5
 in FP32 (rounding of the input, the weights and 33 products per point; an indexing error is of
-order one).
+order one).  FP32 grids with n1 divisible by 4 and uniform x and z spacing run the vector kernel
+(16x16x32, 100x41x26, 8x9x10, 64x56x102: one to several tiles along z, ragged last steps), the
+others the staged kernel.
 """
 import numpy as np
 import pytest
@@ -25,8 +27,9 @@ GRIDS = [((17, 17, 33), (1.0, 1.0, 2.0), (0, 0, 0)),     # 16 x 16 x 32, nx 24: 
          ((22, 15, 13), (1.0, 0.7, 0.9), (1, 0, 1)),     # 21 x 14 x 12: unaligned rows, stretched x and z
          ((9, 10, 11), (1.0, 1.0, 1.0), (0, 0, 0)),      # 8 x 9 x 10: the smallest grid, one tile
          ((33, 25, 49), (1.0, 0.8, 2.0), (0, 1, 1)),     # 32 x 24 x 48: aligned, stretched y and z
-         ((70, 41, 150), (2.0, 1.0, 3.0), (0, 0, 0))]    # 69 x 40 x 149: unaligned, deep ragged tiles
-IDS = ["16x16x32", "30x18x22", "100x41x26", "21x14x12-xz", "8x9x10", "32x24x48-yz", "69x40x149"]
+         ((70, 41, 150), (2.0, 1.0, 3.0), (0, 0, 0)),    # 69 x 40 x 149: unaligned, deep ragged tiles
+         ((65, 57, 103), (1.0, 0.9, 1.6), (0, 0, 0))]    # 64 x 56 x 102: FP32 vector kernel, z tiles
+IDS = ["16x16x32", "30x18x22", "100x41x26", "21x14x12-xz", "8x9x10", "32x24x48-yz", "69x40x149", "64x56x102"]
 
 
 @pytest.mark.parametrize("op,tol", [(0, 1e-12), (2, 1e-5)], ids=["fp64", "fp32"])
