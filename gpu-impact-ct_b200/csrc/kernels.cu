@@ -68,6 +68,7 @@ __global__ void __launch_bounds__(BX* BY) k_gradient(int a, Geom g, const T* __r
 }
 template <typename T>
 void launch_gradient(int m, const Geom& g, const T* cG, const T* phi, T* grad, cudaStream_t s) {
+  if (launch_march1<T, G_LO, NG, 0>(m - 1, g, cG, nullptr, phi, nullptr, grad, 0, s)) return;
   k_gradient<T><<<grid3(g), dim3(BX, BY), 0, s>>>(m - 1, g, cG, phi, grad);
 }
 
@@ -87,6 +88,9 @@ __global__ void __launch_bounds__(BX* BY) k_divergence(int a, Geom g, const T* _
 }
 template <typename T>
 void launch_divergence(int m, const Geom& g, const T* cD, const T* phi, T* div, cudaStream_t s) {
+  if (m == 1 ? launch_march1<T, D_LO, ND, 0>(0, g, cD, nullptr, phi, nullptr, div, 0, s)
+             : launch_march1<T, D_LO, ND, 1>(m - 1, g, cD, nullptr, phi, nullptr, div, 0, s))
+    return;
   k_divergence<T><<<grid3(g), dim3(BX, BY), 0, s>>>(m - 1, g, cD, phi, div);
 }
 
@@ -140,6 +144,7 @@ template <typename T>
 void launch_helmholtz(int m, const Geom& g, const T* cx, const T* cy, const T* cz, T multL, const T* vel, T* nl,
                       cudaStream_t s) {
   (void)m;
+  if (launch_helm_march<T>(g, cx, cy, cz, multL, vel, nl, s)) return;
   k_helmholtz<T><<<grid3(g), dim3(BX, BY), 0, s>>>(g, cx, cy, cz, multL, vel, nl);
 }
 
@@ -155,10 +160,12 @@ __global__ void __launch_bounds__(BX* BY) k_interp(int a, Geom g, const T* __res
 }
 template <typename T>
 void launch_interp_pre_vel(int m, const Geom& g, const T* cI, const T* phi, T* out, cudaStream_t s) {
+  if (launch_march1<T, G_LO, NG, 0>(m - 1, g, cI, nullptr, phi, nullptr, out, 0, s)) return;
   k_interp<T, G_LO, NG><<<grid3(g), dim3(BX, BY), 0, s>>>(m - 1, g, cI, phi, out);
 }
 template <typename T>
 void launch_interp_vel_pre(int m, const Geom& g, const T* cI, const T* phi, T* out, cudaStream_t s) {
+  if (launch_march1<T, D_LO, ND, 0>(m - 1, g, cI, nullptr, phi, nullptr, out, 0, s)) return;
   k_interp<T, D_LO, ND><<<grid3(g), dim3(BX, BY), 0, s>>>(m - 1, g, cI, phi, out);
 }
 
@@ -182,6 +189,7 @@ template <typename T>
 void launch_nonlinear_upwind(int cid, const Geom& g, const T* cU, const T* cDn, const T* pp, const T* vel, T* nl,
                              cudaStream_t s) {
   const int a = (cid - 1) % 3;
+  if (launch_march1<T, B_LO, NB, 2>(a, g, cU, cDn, vel, pp, nl, a == 0, s)) return;
   k_nl_upwind<T><<<grid3(g), dim3(BX, BY), 0, s>>>(a, a == 0, g, cU, cDn, pp, vel, nl);
 }
 
@@ -260,6 +268,7 @@ __global__ void __launch_bounds__(BX* BY) k_jacobi(Geom g, const T* __restrict__
 template <typename T>
 void launch_jacobi(const Geom& g, const T* c1, const T* c2, const T* c3, T omega, const T* bb, const T* rel, T* out,
                    cudaStream_t s) {
+  if (launch_jacobi_march<T>(g, c1, c2, c3, omega, bb, rel, out, s)) return;
   k_jacobi<T><<<grid3(g), dim3(BX, BY), 0, s>>>(g, c1, c2, c3, omega, bb, rel, out);
 }
 

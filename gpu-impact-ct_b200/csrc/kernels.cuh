@@ -4,6 +4,23 @@
 
 namespace impact {
 
+// ---- one-axis stencils as streaming passes (march.cu): out (=, += for OP 1) the CNT-point
+// stencil from LO along axis a (0 x, 1 y, 2 z) of f; OP 2 the upwind term (cA where pp >= 0,
+// else cB; overwrite when first).  Returns false (nothing launched) when n1 is not divisible by
+// the 16-byte vector width or a field is not 16-byte aligned.
+template <typename T, int LO, int CNT, int OP>
+bool launch_march1(int a, const Geom& g, const T* cA, const T* cB, const T* f, const T* pp, T* out, int first,
+                   cudaStream_t s);
+
+// Helmholtz_explicit and the Jacobi / JOR sweep as z-marching passes (march.cu); false when
+// not applicable (as launch_march1)
+template <typename T>
+bool launch_helm_march(const Geom& g, const T* cx, const T* cy, const T* cz, T multL, const T* vel, T* nl,
+                       cudaStream_t s);
+template <typename T>
+bool launch_jacobi_march(const Geom& g, const T* c1, const T* c2, const T* c3, T omega, const T* bb, const T* rel,
+                         T* out, cudaStream_t s);
+
 // ---- staggered-grid operators (mod_diff.f90) ----
 template <typename T>
 void launch_gradient(int m, const Geom& g, const T* cG, const T* phi, T* grad, cudaStream_t s);

@@ -8,7 +8,9 @@ the cost of one preconditioner application against the number of BiCGstab iterat
 chosen here by timing complete Poisson solves of the case's own current right-hand side to the
 requested tolerance, one per candidate, on the device, and keeping the fastest candidate that
 converged.  In mixed precision a looser inner tolerance means cheaper inner solves and more FP64
-refinement passes; the best balance depends on the case, so it is one more tuned dimension.
+refinement passes (each one an FP64 residual and correction over the whole grid); a tighter one
+fewer passes and longer FP32 solves.  The best balance depends on the case, so it is one more
+tuned dimension.
 Results are cached per (grid, precision, device) for the life of the process.
 """
 from __future__ import annotations
@@ -20,7 +22,7 @@ from . import Case, SolverParams
 
 TILE_KC = (8, 16, 32, 64)
 SWEEPS = ((2, 2, 2), (3, 3, 3), (4, 4, 4))
-INNER_TOL = (1e-3, 3e-3, 1e-2)
+INNER_TOL = (1e-4, 3e-4, 1e-3, 3e-3, 1e-2)
 
 _cache: dict = {}
 

@@ -62,3 +62,45 @@ def test_measured_inflow_waveform_on_the_device():
     with pytest.raises(I.ImpactError):
         case.set_inflow_waveform([0.0, 1.0, 0.5], [1.0, 1.0, 1.0])  # times must not decrease
     case.close()
+
+
+def test_reference_tavi2_case_steps_like_the_oracle():
+    """The TAVI2 case built from the reference's own lumen segmentation (the CT grid labels of
+    tests/golden/tavi2_labels.npz, 160 x 80 x 160 cells): three FP64 steps on the device with the
+    multigrid-preconditioned solve equal the oracle's to 1e-6 of max|u|; then the case takes its
+    measured TAVI2 inflow waveform (converted table of the fixture) and the inflow voxels hold the
+    oracle lookup's value after every step."""
+    import json
+    import os
+
+    import oracle as O
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    fix = json.load(open(os.path.join(here, "golden", "reference_inputs.json")))
+    lab = np.load(os.path.join(here, "golden", "tavi2_labels.npz"))["labels"]
+    Np, L = tuple(fix["ct_grid"]["points"]), tuple(fix["ct_grid"]["box"])
+    og, ig = O.Grid(Np, L), I.Grid(Np, L)
+    mg = og.multigrid()
+    vel, nl, pre = og.zeros(3), og.zeros(3), og.zeros()
+    ost = O.OrcStepState()
+    op = O.step_params(Re=200.0, tol_rel=1e-8, omega=0.8, mg=mg, mg_down=3, mg_up=3, mg_bottom=3)
+    case = I.Case(ig, precision=0)
+    case.set_labels(lab)
+    sp = I.step_params(Re=200.0, tol_rel=1e-8, omega=0.8, precond=1, max_it=200, mg_down=3, mg_up=3, mg_bottom=3)
+    for _ in range(3):
+        og.time_step(op, lab, vel, nl, pre, ost)
+        st = case.step(sp)
+        assert all(s == 0 for s in st.poisson_status)
+    umax = max(np.abs(og.interior(vel[m])).max() for m in range(3))
+    for m, f in enumerate(("vel1", "vel2", "vel3")):
+        assert np.abs(og.interior(case.download(f)) - og.interior(vel[m])).max() <= 1e-6 * umax
+    w = fix["waveforms"]["TAVI2"]
+    case.set_inflow_waveform(np.array(w["time"]), np.array(w["velocity"]))
+    inflow = lab == 5
+    assert inflow.sum() == 10 * fix["ct_grid"]["counts"]["inlet_jet"]
+    for _ in range(2):
+        st = case.step(sp)
+        want = R.inflow(w["time"], w["velocity"], st.time)
+        assert want is not None
+        assert np.all(case.download("vel3")[inflow] == want)
+    case.close()
