@@ -796,8 +796,50 @@ def kernels_main(args, device):
                 ms, byts = case.engine_bench(kid, args.iters, sp)
             out[name] = {"ms": round(ms, 4), "GB/s": round(byts / (ms / 1e3) / 1e9, 1) if byts else None}
         case.close()
+    if want is None or "ibm" in want:
+        out["ibm"] = ibm_timing(args, device, n)
     print(json.dumps({"workload": f"kernels-{n}x{n}x{2 * n}", "cells": cells, "iters": args.iters,
                       "fields": "seeded U[-1, 1]", "kernels": out}), flush=True)
+
+
+def ibm_timing(args, device, n):
+    """The diffuse-interface immersed-boundary transfers (interpolate_vel_to_ib and
+    spread_force_dens_to_vel_grid, mod_ibm.f90:428-737) on the resident fields of the n x n x 2n
+    case: markers on a sphere of radius 0.2 (10^4 and 10^5 of them), hat kernel of reach 2 cells;
+    wall time per call over --iters calls after a warm-up, including the markers' host <-> device
+    transfers of each call (interpolate: the marker velocities come back; spread: the marker
+    forces go up)."""
+    import numpy as np
+    import torch
+
+    import impact_b200 as I
+    grid = I.Grid((n + 1, n + 1, 2 * n + 1), (1.0, 1.0, 2.0))
+    case = I.Case(grid, precision=0, device=device)
+    rng = np.random.default_rng(9)
+    for f in ("vel1", "vel2", "vel3"):
+        case.upload(f, rng.uniform(-1.0, 1.0, grid.shape))
+    res = {}
+    for m in (10_000, 100_000):
+        v = rng.normal(size=(m, 3))
+        yb = np.array([0.5, 0.5, 1.0]) + 0.2 * v / np.linalg.norm(v, axis=1)[:, None]
+        case.set_markers(yb, reach=2.0 / n, delta_type=2)
+        fb, vol = rng.uniform(-1.0, 1.0, (m, 3)), np.full(m, 1e-4)
+        case.ibm_interpolate()
+        case.ibm_spread(fb, vol, into="rhs")
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        for _ in range(args.iters):
+            case.ibm_interpolate()
+        torch.cuda.synchronize(device)
+        t1 = time.perf_counter()
+        for _ in range(args.iters):
+            case.ibm_spread(fb, vol, into="rhs")
+        torch.cuda.synchronize(device)
+        t2 = time.perf_counter()
+        res[f"markers_{m}"] = {"interpolate_ms": round(1e3 * (t1 - t0) / args.iters, 4),
+                               "spread_ms": round(1e3 * (t2 - t1) / args.iters, 4)}
+    case.close()
+    return res
 
 
 def plain_main(args, device):

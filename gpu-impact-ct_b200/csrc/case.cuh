@@ -31,6 +31,10 @@ struct CaseState {
   // fields
   double* f[IMPACT_B200_NFIELDS] = {};
   double* work[3] = {};   // velocities interpolated to pressure points
+  // mixed precision: the interpolated velocities and the nonlinear term of the time step in FP32
+  // (the FP32 rhs_vel pass reads and writes these; nl1..3 of such a case are not kept)
+  float* work32[3] = {};
+  float* nl32[3] = {};
   uint8_t* label = nullptr;
   // FP64 Krylov work (8 fields), or the mixed-precision set
   KrylovWork<double> kw64{};

@@ -9,8 +9,9 @@
 //   a = y or z: marches along a over a segment of the axis, keeping the CNT vectors of its
 //               stencil in registers (one new 16-byte load and one 16-byte store per step), the
 //               coefficient row of the step being the same for the whole block;
-//   a = x:      loads the few aligned vectors its points' stencils span (neighbouring vectors,
-//               periodic images at the row ends), one coefficient row per point.
+//   a = x:      marches z as well, with the coefficient rows of its points loaded once; each
+//               plane takes the few aligned vectors of the row that its points' stencils span
+//               (neighbouring vectors, periodic images at the row ends).
 // Periodic wrapping is applied to the coordinate along a only.  Each point sums its terms in
 // table order with the same fused multiply-adds as the one-point-per-thread kernels of
 // kernels.cu, so both give the same bits.
@@ -137,50 +138,61 @@ __global__ void __launch_bounds__(MBX* MBY) k_march_yz(int a, Geom g, const T* _
   }
 }
 
-// a = 0 (x): one vector of W points per thread
+// a = 0 (x): thread (vector, row j) marches z over a segment; the coefficient rows of its W
+// points are loaded once, and each plane takes the few aligned vectors of the row that the W
+// points' stencils span (neighbouring vectors, periodic images at the row ends)
 template <typename T, int LO, int CNT, int OP>
 __global__ void __launch_bounds__(MBX* MBY) k_march_x(Geom g, const T* __restrict__ cA, const T* __restrict__ cB,
                                                       const T* __restrict__ f, const T* __restrict__ pp,
-                                                      T* __restrict__ out, int first) {
+                                                      T* __restrict__ out, int first, int seg) {
   constexpr int W = V16<T>::W;
-  // the vectors that the W points' stencils span, relative to the thread's own
   constexpr int FV = (LO - (W - 1)) / W;          // floor(LO / W) for LO < 0
   constexpr int LV = (W - 1 + LO + CNT - 1) / W;  // floor of the last position / W (>= 0)
   constexpr int NV = LV - FV + 1;
   const int vx = blockIdx.x * MBX + threadIdx.x;
   const int nvx = g.n1 / W;
-  const int j = blockIdx.y * MBY + threadIdx.y + 1, k = blockIdx.z + 1;
+  const int j = blockIdx.y * MBY + threadIdx.y + 1;
   if (vx >= nvx || j > g.n2) return;
   const int i = 1 + W * vx;
-  const long long row = 4 + (long long)g.nx * (j + 3) + g.nxy * (k + 3);  // offset of (1, j, k)
-  T val[NV * W];
+  const int k0 = blockIdx.z * seg + 1, k1 = min(g.n3, k0 + seg - 1);
+  T ca[W][CNT], cb[W][CNT];
 #pragma unroll
-  for (int n = 0; n < NV; ++n) {
-    int u = vx + FV + n;
-    u = u < 0 ? u + nvx : (u >= nvx ? u - nvx : u);
-    T tmp[W];
-    vld(f + row + (long long)W * u, tmp);
-#pragma unroll
-    for (int v = 0; v < W; ++v) val[n * W + v] = tmp[v];
-  }
-  const long long p = row + (i - 1);
-  T old[W], pv[W], r[W];
-  if (OP != 0) vld_plain(out + p, old);
-  if (OP == 2) vld(pp + p, pv);
-#pragma unroll
-  for (int v = 0; v < W; ++v) {
-    const T* ca = cA + (long long)(i + v) * CNT;
-    const T* cb = OP == 2 ? cB + (long long)(i + v) * CNT : ca;
-    T ca_r[CNT], cb_r[CNT], wv[CNT];
+  for (int v = 0; v < W; ++v)
 #pragma unroll
     for (int l = 0; l < CNT; ++l) {
-      ca_r[l] = __ldg(ca + l);
-      cb_r[l] = OP == 2 ? __ldg(cb + l) : ca_r[l];
-      wv[l] = val[v + LO + l - FV * W];
+      ca[v][l] = __ldg(cA + (long long)(i + v) * CNT + l);
+      cb[v][l] = OP == 2 ? __ldg(cB + (long long)(i + v) * CNT + l) : ca[v][l];
     }
-    r[v] = point_value<T, CNT, OP>(ca_r, cb_r, wv, OP != 0 ? old[v] : T(0), OP == 2 ? pv[v] : T(0), first);
+  int us[NV];
+#pragma unroll
+  for (int n = 0; n < NV; ++n) {
+    const int u = vx + FV + n;
+    us[n] = W * (u < 0 ? u + nvx : (u >= nvx ? u - nvx : u));
   }
-  vst(out + p, r);
+  const long long rowj = 4 + (long long)g.nx * (j + 3);  // offset of (1, j, k = -3)
+  for (int k = k0; k <= k1; ++k) {
+    const long long row = rowj + g.nxy * (k + 3);
+    T val[NV * W];
+#pragma unroll
+    for (int n = 0; n < NV; ++n) {
+      T tmp[W];
+      vld(f + row + us[n], tmp);
+#pragma unroll
+      for (int v = 0; v < W; ++v) val[n * W + v] = tmp[v];
+    }
+    const long long p = row + (i - 1);
+    T old[W], pv[W], r[W];
+    if (OP != 0) vld_plain(out + p, old);
+    if (OP == 2) vld(pp + p, pv);
+#pragma unroll
+    for (int v = 0; v < W; ++v) {
+      T wv[CNT];
+#pragma unroll
+      for (int l = 0; l < CNT; ++l) wv[l] = val[v + LO + l - FV * W];
+      r[v] = point_value<T, CNT, OP>(ca[v], cb[v], wv, OP != 0 ? old[v] : T(0), OP == 2 ? pv[v] : T(0), first);
+    }
+    vst(out + p, r);
+  }
 }
 
 // Helmholtz_explicit (mod_diff.f90:549-762): nl = nl - multL (cx u_xx + cy u_yy + cz u_zz), the
@@ -333,8 +345,10 @@ bool launch_march1(int a, const Geom& g, const T* cA, const T* cB, const T* f, c
   if (g.n1 % W != 0 || !aligned16(f) || !aligned16(out) || (OP == 2 && !aligned16(pp))) return false;
   const int nvx = g.n1 / W;
   if (a == 0) {
-    const dim3 grid((nvx + MBX - 1) / MBX, (g.n2 + MBY - 1) / MBY, g.n3);
-    k_march_x<T, LO, CNT, OP><<<grid, dim3(MBX, MBY), 0, s>>>(g, cA, cB, f, pp, out, first);
+    const long long bx = (nvx + MBX - 1) / MBX, by = (g.n2 + MBY - 1) / MBY;
+    const int seg = march_seg(bx * by, g.n3);
+    const dim3 grid((unsigned)bx, (unsigned)by, (g.n3 + seg - 1) / seg);
+    k_march_x<T, LO, CNT, OP><<<grid, dim3(MBX, MBY), 0, s>>>(g, cA, cB, f, pp, out, first, seg);
   } else {
     const int na = a == 2 ? g.n3 : g.n2, no = a == 2 ? g.n2 : g.n3;
     const long long bx = (nvx + MBX - 1) / MBX, by = (no + MBY - 1) / MBY;

@@ -26,6 +26,9 @@ namespace impact {
 namespace {
 
 constexpr int RTX = 32, RTY = 8, RNT = RTX * RTY;
+// RK3 coefficients (mod_vars.f90:774-775) for the batched pass, which forms dt aRK / dt bRK itself
+__constant__ double RK_A[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+__constant__ double RK_B[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
 constexpr int RR = 7;                                 // ring slots: planes c .. c+3 resident, 3 in flight
 constexpr int VW = RTX + 6, VH = RTY + 6, VE = VW * VH;  // vel tile with the 3-wide halo
 constexpr int NXR = 27;                               // x coefficient rows: U 7, D 7, D2 7, I 6
@@ -45,9 +48,9 @@ constexpr int slot_elems() { return VE + 3 * WTile<M>::E + NCR; }  // vel tile, 
 static_assert(VE % 2 == 0 && (3 * WTile<0>::E) % 2 == 0 && (3 * WTile<1>::E) % 2 == 0 && (3 * WTile<2>::E) % 2 == 0 &&
                   (NXR * RTX) % 2 == 0,
               "z rows and y rows must stay 16-byte aligned");
-template <int M>
+template <int M, typename TW = double>
 constexpr size_t rhs_smem_bytes() {
-  return sizeof(double) * ((size_t)RR * slot_elems<M>() + (size_t)NXR * RTX + (size_t)RTY * NCR);
+  return sizeof(TW) * ((size_t)RR * slot_elems<M>() + (size_t)NXR * RTX + (size_t)RTY * NCR);
 }
 
 // periodic image of index i in 1..n, for any integer i
@@ -57,7 +60,7 @@ __device__ __forceinline__ int wrapg(int i, int n) {
   return r + 1;
 }
 
-// N consecutive doubles from 16-byte aligned shared memory, two per load
+// N consecutive values from shared memory aligned to two values, two per load
 template <int N>
 __device__ __forceinline__ void ld_row(const double* p, double (&o)[N]) {
 #pragma unroll
@@ -68,62 +71,84 @@ __device__ __forceinline__ void ld_row(const double* p, double (&o)[N]) {
   }
   if (N & 1) o[N - 1] = p[N - 1];
 }
+template <int N>
+__device__ __forceinline__ void ld_row(const float* p, float (&o)[N]) {
+#pragma unroll
+  for (int l = 0; l + 1 < N; l += 2) {
+    const float2 v = *reinterpret_cast<const float2*>(p + l);
+    o[l] = v.x;
+    o[l + 1] = v.y;
+  }
+  if (N & 1) o[N - 1] = p[N - 1];
+}
 
 __device__ __forceinline__ void cpa8(double* smem, const double* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cpa4(float* smem, const float* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cpa(double* smem, const double* gmem) { cpa8(smem, gmem); }
+__device__ __forceinline__ void cpa(float* smem, const float* gmem) { cpa4(smem, gmem); }
 __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <int M>
-__global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, double multL, double mult_b,
-                                                      double mult_a, int use_old, int kz,
-                                                      const double* __restrict__ vel, const double* __restrict__ wk0,
-                                                      const double* __restrict__ wk1, const double* __restrict__ wk2,
-                                                      double* __restrict__ nl, double* __restrict__ rhs) {
+// the pass of block (bx, by, bz) of a case's grid of blocks.  TW is the type of the work fields,
+// the nonlinear term, the staged tiles, the coefficients and the arithmetic: double (FP64 cases)
+// or float (mixed-precision cases: FP32 stencils with FP32 accumulation; the velocity and rhs_m
+// stay FP64, the FP64 velocity staged into FP32 tiles by ordinary loads one plane ahead).
+template <int M, typename TW>
+__device__ __forceinline__ void rhs_march_block(const Geom& g, const Coeffs<TW>& c, double multL, double mult_b,
+                                                double mult_a, int use_old, int kz, const double* __restrict__ vel,
+                                                const TW* __restrict__ wk0, const TW* __restrict__ wk1,
+                                                const TW* __restrict__ wk2, TW* __restrict__ nl,
+                                                double* __restrict__ rhs, int bx, int by, int bz) {
   using WT = WTile<M>;
+  constexpr bool F32 = sizeof(TW) == 4;
   constexpr int SE = slot_elems<M>();
   constexpr int VPER = (VE + RNT - 1) / RNT;
   constexpr int WPER = (3 * WT::E + RNT - 1) / RNT;
-  extern __shared__ __align__(16) double rsm[];
-  double* ring = rsm;                      // RR slots of SE doubles: vel tile, work tiles 0..2, z row
-  double* sx = rsm + (size_t)RR * SE;      // NXR x RTX transposed x rows
-  double* sy = sx + NXR * RTX;             // RTY x NCR y rows of the block's rows
+  extern __shared__ __align__(16) unsigned char rsm_raw[];
+  TW* rsm = reinterpret_cast<TW*>(rsm_raw);
+  TW* ring = rsm;                      // RR slots of SE values: vel tile, work tiles 0..2, z row
+  TW* sx = rsm + (size_t)RR * SE;      // NXR x RTX transposed x rows
+  TW* sy = sx + NXR * RTX;             // RTY x NCR y rows of the block's rows
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + RTX * ty;
-  const int i0 = blockIdx.x * RTX + 1, j0 = blockIdx.y * RTY + 1;
-  const int k0 = blockIdx.z * kz + 1;
+  const int i0 = bx * RTX + 1, j0 = by * RTY + 1;
+  const int k0 = bz * kz + 1;
   const int k1 = min(k0 + kz - 1, g.n3);
   const int i = i0 + tx, j = j0 + ty;
   const bool in = i <= g.n1 && j <= g.n2;
-  const double* yU = M == 1 ? c.cNuU[1] : c.cNpU[1];
-  const double* yD = M == 1 ? c.cNuD[1] : c.cNpD[1];
-  const double* yH = M == 1 ? c.cuu[1] : c.cpp[1];
-  const double* zU = M == 2 ? c.cNuU[2] : c.cNpU[2];
-  const double* zD = M == 2 ? c.cNuD[2] : c.cNpD[2];
-  const double* zH = M == 2 ? c.cuu[2] : c.cpp[2];
+  const TW* yU = M == 1 ? c.cNuU[1] : c.cNpU[1];
+  const TW* yD = M == 1 ? c.cNuD[1] : c.cNpD[1];
+  const TW* yH = M == 1 ? c.cuu[1] : c.cpp[1];
+  const TW* zU = M == 2 ? c.cNuU[2] : c.cNpU[2];
+  const TW* zD = M == 2 ? c.cNuD[2] : c.cNpD[2];
+  const TW* zH = M == 2 ? c.cuu[2] : c.cpp[2];
 
   // x rows of this block's columns, transposed: sx[l][tx]
   {
-    const double* xU = M == 0 ? c.cNuU[0] : c.cNpU[0];
-    const double* xD = M == 0 ? c.cNuD[0] : c.cNpD[0];
-    const double* xH = M == 0 ? c.cuu[0] : c.cpp[0];
+    const TW* xU = M == 0 ? c.cNuU[0] : c.cNpU[0];
+    const TW* xD = M == 0 ? c.cNuD[0] : c.cNpD[0];
+    const TW* xH = M == 0 ? c.cuu[0] : c.cpp[0];
     for (int t = tid; t < NXR * RTX; t += RNT) {
       const int l = t / RTX, col = t % RTX;
       const int row = wrapg(i0 + col, g.n1);
-      double v;
+      TW v;
       if (l < 7) v = xU[row * NB + l];
       else if (l < 14) v = xD[row * NB + (l - 7)];
       else if (l < 21) v = xH[row * NB + (l - 14)];
-      else v = M == 0 ? c.cIpu[0][row * NG + (l - 21)] : 0.0;
+      else v = M == 0 ? c.cIpu[0][row * NG + (l - 21)] : TW(0);
       sx[t] = v;
     }
     // y rows of the block's rows
     for (int t = tid; t < RTY * NCR; t += RNT) {
       const int r = t / NCR, e = t % NCR, grp = e / 8, l = e % 8;
       const int row = wrapg(j0 + r, g.n2);
-      double v = 0.0;
+      TW v = TW(0);
       if (grp == 0 && l < 7) v = yU[row * NB + l];
       else if (grp == 1 && l < 7) v = yD[row * NB + l];
       else if (grp == 2 && l < 7) v = yH[row * NB + l];
@@ -139,7 +164,7 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
     const int r = t / VW, col = t % VW;
     vo[e] = t < VE ? (wrapg(i0 - 3 + col, g.n1) + 3) + g.nx * (wrapg(j0 - 3 + r, g.n2) + 3) : -1;
   }
-  const double* wsrc[WPER];
+  const TW* wsrc[WPER];
   int wdst[WPER];
 #pragma unroll
   for (int e = 0; e < WPER; ++e) {
@@ -147,7 +172,7 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
     const int f = t / WT::E, u = t % WT::E;
     const int r = u / WT::W, col = u % WT::W;
     const int gi = wrapg(i0 + col - (M == 0 ? 2 : 0), g.n1), gj = wrapg(j0 + r - (M == 1 ? 2 : 0), g.n2);
-    const double* base = f == 0 ? wk0 : (f == 1 ? wk1 : wk2);
+    const TW* base = f == 0 ? wk0 : (f == 1 ? wk1 : wk2);
     wsrc[e] = t < 3 * WT::E ? base + (gi + 3) + (long long)g.nx * (gj + 3) : nullptr;
     wdst[e] = VE + t;
   }
@@ -157,43 +182,55 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
   // z row of a staged plane: thread e < NCR copies element e of the row layout
   const int zg = tid / 8, zl = tid % 8;
   const bool zcopy = tid < NCR && (zg < 3 ? zl < 7 : (zl < 6 && M == 2));
-  const double* zsrc = zg == 0 ? zU + zl : (zg == 1 ? zD + zl : (zg == 2 ? zH + zl : c.cIpu[2] + zl));
+  const TW* zsrc = zg == 0 ? zU + zl : (zg == 1 ? zD + zl : (zg == 2 ? zH + zl : c.cIpu[2] + zl));
   const int zstride = zg < 3 ? NB : NG;
+  double vpend[VPER];  // FP32: the velocity of the plane staged last, stored at the next stage()
   auto stage = [&](int q) {
-    if (q < nq) {
-      double* slot = ring + (size_t)(q % RR) * SE;
-      const long long zo = zoff(q);
+    if (F32 && q >= 1 && q - 1 < nq) {
+      TW* prev = ring + (size_t)((q - 1) % RR) * SE;
 #pragma unroll
       for (int e = 0; e < VPER; ++e)
-        if (vo[e] >= 0) cpa8(slot + tid + e * RNT, vel + zo + vo[e]);
+        if (vo[e] >= 0) prev[tid + e * RNT] = (TW)vpend[e];
+    }
+    if (q < nq) {
+      TW* slot = ring + (size_t)(q % RR) * SE;
+      const long long zo = zoff(q);
+#pragma unroll
+      for (int e = 0; e < VPER; ++e) {
+        if (vo[e] < 0) continue;
+        if constexpr (F32)
+          vpend[e] = __ldg(vel + zo + vo[e]);
+        else
+          cpa8(reinterpret_cast<double*>(slot) + tid + e * RNT, vel + zo + vo[e]);
+      }
 #pragma unroll
       for (int e = 0; e < WPER; ++e)
-        if (wsrc[e]) cpa8(slot + wdst[e], wsrc[e] + zo);
-      if (zcopy) cpa8(slot + (SE - NCR) + tid, zsrc + zwrap(q) * zstride);
+        if (wsrc[e]) cpa(slot + wdst[e], wsrc[e] + zo);
+      if (zcopy) cpa(slot + (SE - NCR) + tid, zsrc + zwrap(q) * zstride);
     }
     cpa_commit();
   };
 #pragma unroll
   for (int q = 0; q < RR - 4; ++q) stage(q);
 
-  double vq[7];                                    // vel of the column, planes c-3 .. c+3
-  double wq[3][6];                                 // m = 3: work_a of the column, planes c-2 .. c+3
+  TW vq[7];                                        // vel of the column, planes c-3 .. c+3
+  TW wq[3][6];                                    // m = 3: work_a of the column, planes c-2 .. c+3
 #pragma unroll
-  for (int l = 0; l < 7; ++l) vq[l] = 0.0;
+  for (int l = 0; l < 7; ++l) vq[l] = TW(0);
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
-    for (int l = 0; l < 6; ++l) wq[a][l] = 0.0;
+    for (int l = 0; l < 6; ++l) wq[a][l] = TW(0);
 
   const int own = (tx + 3) + VW * (ty + 3);
-  const double* cy = sy + ty * NCR;  // this thread's y row (warp-uniform)
+  const TW* cy = sy + ty * NCR;  // this thread's y row (warp-uniform)
   long long p = off(g, i, j, k0);    // output point of plane k (advanced per plane)
 
   for (int t = 0; t < nq; ++t) {
     cpa_wait<RR - 5>();   // this thread's copies of plane t have landed
     __syncthreads();      // everybody's have; the slot of plane t-4 is free again
     stage(t + RR - 4);
-    const double* slot = ring + (size_t)(t % RR) * SE;
+    const TW* slot = ring + (size_t)(t % RR) * SE;
 #pragma unroll
     for (int l = 0; l < 6; ++l) vq[l] = vq[l + 1];
     vq[6] = slot[own];
@@ -208,36 +245,36 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
     if (t < 6) continue;
     if (t > 6) p += g.nxy;
     if (!in) continue;
-    const double* cs = ring + (size_t)((t - 3) % RR) * SE;  // plane k = k0 + t - 6
-    const double* cz = cs + (SE - NCR);                     // its z row (block-uniform)
-    const double nlo = use_old ? nl[p] : 0.0;
+    const TW* cs = ring + (size_t)((t - 3) % RR) * SE;  // plane k = k0 + t - 6
+    const TW* cz = cs + (SE - NCR);                     // its z row (block-uniform)
+    const TW nlo = use_old ? nl[p] : TW(0);
     // vel_m neighbours along x and y (plane k), z (register window)
-    double xv[7], yv[7];
+    TW xv[7], yv[7];
 #pragma unroll
     for (int l = 0; l < 7; ++l) {
       xv[l] = cs[(ty + 3) * VW + tx + l];
       yv[l] = cs[(ty + l) * VW + tx + 3];
     }
     // interpolation weights along axis m, shared by the three work fields
-    double ci[6];
+    TW ci[6];
     if (M == 0) {
 #pragma unroll
       for (int l = 0; l < 6; ++l) ci[l] = sx[(21 + l) * RTX + tx];
     } else {
       ld_row((M == 1 ? cy : cz) + CI, ci);
     }
-    double acc = 0.0;
+    TW acc = TW(0);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       // pp = interpolate2_pre_vel(m, work_a) along axis m
-      double pp;
+      TW pp;
       if (M == 0) {
-        const double* w = cs + VE + a * WT::E + ty * WT::W + tx;
+        const TW* w = cs + VE + a * WT::E + ty * WT::W + tx;
         pp = ci[0] * w[0];
 #pragma unroll
         for (int l = 1; l < 6; ++l) pp = pp + ci[l] * w[l];
       } else if (M == 1) {
-        const double* w = cs + VE + a * WT::E + ty * WT::W + tx;
+        const TW* w = cs + VE + a * WT::E + ty * WT::W + tx;
         pp = ci[0] * w[0];
 #pragma unroll
         for (int l = 1; l < 6; ++l) pp = pp + ci[l] * w[l * WT::W];
@@ -246,21 +283,21 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
 #pragma unroll
         for (int l = 1; l < 6; ++l) pp = pp + ci[l] * wq[a][l];
       }
-      double dd;
+      TW dd;
       if (a == 0) {
-        const double* cr = sx + (pp >= 0.0 ? 0 : 7) * RTX + tx;
+        const TW* cr = sx + (pp >= TW(0) ? 0 : 7) * RTX + tx;
         dd = cr[0] * xv[0];
 #pragma unroll
         for (int l = 1; l < 7; ++l) dd = dd + cr[l * RTX] * xv[l];
       } else if (a == 1) {
-        double cr[7];
-        ld_row(cy + (pp >= 0.0 ? CU : CD), cr);
+        TW cr[7];
+        ld_row(cy + (pp >= TW(0) ? CU : CD), cr);
         dd = cr[0] * yv[0];
 #pragma unroll
         for (int l = 1; l < 7; ++l) dd = dd + cr[l] * yv[l];
       } else {
-        double cr[7];
-        ld_row(cz + (pp >= 0.0 ? CU : CD), cr);
+        TW cr[7];
+        ld_row(cz + (pp >= TW(0) ? CU : CD), cr);
         dd = cr[0] * vq[0];
 #pragma unroll
         for (int l = 1; l < 7; ++l) dd = dd + cr[l] * vq[l];
@@ -268,11 +305,11 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
       acc = (a == 0) ? dd * pp : acc + dd * pp;
     }
     // Helmholtz_explicit: x, y, z second derivatives of vel_m
-    double lap = sx[14 * RTX + tx] * xv[0];
+    TW lap = sx[14 * RTX + tx] * xv[0];
 #pragma unroll
     for (int l = 1; l < 7; ++l) lap = lap + sx[(14 + l) * RTX + tx] * xv[l];
     {
-      double ch[7];
+      TW ch[7];
       ld_row(cy + CH, ch);
 #pragma unroll
       for (int l = 0; l < 7; ++l) lap = lap + ch[l] * yv[l];
@@ -280,34 +317,104 @@ __global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<double> c, 
 #pragma unroll
       for (int l = 0; l < 7; ++l) lap = lap + ch[l] * vq[l];
     }
-    const double nln = acc - multL * lap;
-    double r = vq[3];
-    if (use_old) r = r - mult_b * nlo;
-    r = r - mult_a * nln;
+    const TW nln = acc - (TW)multL * lap;
+    double r = F32 ? vel[p] : (double)vq[3];  // FP32 tiles: the FP64 velocity of the point itself
+    if (use_old) r = r - mult_b * (double)nlo;
+    r = r - mult_a * (double)nln;
     nl[p] = nln;
     rhs[p] = r;
   }
   cpa_wait<0>();
 }
 
-template <int M>
-void launch_m(const Geom& g, const Coeffs<double>& c, double multL, double mult_b, double mult_a, int use_old,
-              const double* vel, const double* const work[3], double* nl, double* rhs, cudaStream_t s) {
+template <int M, typename TW>
+__global__ void __launch_bounds__(RNT, 2) k_rhs_march(Geom g, Coeffs<TW> c, double multL, double mult_b,
+                                                      double mult_a, int use_old, int kz,
+                                                      const double* __restrict__ vel, const TW* __restrict__ wk0,
+                                                      const TW* __restrict__ wk1, const TW* __restrict__ wk2,
+                                                      TW* __restrict__ nl, double* __restrict__ rhs) {
+  rhs_march_block<M, TW>(g, c, multL, mult_b, mult_a, use_old, kz, vel, wk0, wk1, wk2, nl, rhs, blockIdx.x,
+                         blockIdx.y, blockIdx.z);
+}
+
+// the pass over the cases of a batch: block b of the launch is block b - job.b0 of its case
+template <int M, typename TW>
+__global__ void __launch_bounds__(RNT, 2) k_rhs_march_batch(const RhsJob* __restrict__ jobs, int nj, int sub) {
+  int lo = 0, hi = nj - 1;
+  const int b = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].b0 <= b) lo = mid; else hi = mid - 1;
+  }
+  const RhsJob& J = jobs[lo];
+  const int lb = b - J.b0;
+  const int bx = lb % J.gx, by = (lb / J.gx) % J.gy, bz = lb / (J.gx * J.gy);
+  const double dt = *J.dt;
+  const double multL = 1.0 / *J.Re;
+  if constexpr (sizeof(TW) == 8)
+    rhs_march_block<M, double>(J.g, J.c, multL, dt * RK_B[sub], dt * RK_A[sub], sub != 0, J.kz, J.vel[M], J.work[0],
+                               J.work[1], J.work[2], J.nl[M], J.rhs[M], bx, by, bz);
+  else
+    rhs_march_block<M, float>(J.g, J.c32, multL, dt * RK_B[sub], dt * RK_A[sub], sub != 0, J.kz, J.vel[M],
+                              J.work32[0], J.work32[1], J.work32[2], J.nl32[M], J.rhs[M], bx, by, bz);
+}
+
+template <int M, typename TW>
+void launch_m(const Geom& g, const Coeffs<TW>& c, double multL, double mult_b, double mult_a, int use_old,
+              const double* vel, const TW* const work[3], TW* nl, double* rhs, cudaStream_t s) {
   static unsigned long long attr_set = 0;  // devices on which the shared-memory limit was raised
-  constexpr size_t bytes = rhs_smem_bytes<M>();
+  constexpr size_t bytes = rhs_smem_bytes<M, TW>();
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(attr_set >> dev & 1ULL)) {
-    cudaFuncSetAttribute(k_rhs_march<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(k_rhs_march<M, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     attr_set |= 1ULL << dev;
   }
   const int kz = rhs_march_kz(g);
   const dim3 grid((g.n1 + RTX - 1) / RTX, (g.n2 + RTY - 1) / RTY, (g.n3 + kz - 1) / kz);
-  k_rhs_march<M><<<grid, dim3(RTX, RTY), bytes, s>>>(g, c, multL, mult_b, mult_a, use_old, kz, vel, work[0], work[1],
-                                                     work[2], nl, rhs);
+  k_rhs_march<M, TW><<<grid, dim3(RTX, RTY), bytes, s>>>(g, c, multL, mult_b, mult_a, use_old, kz, vel, work[0],
+                                                         work[1], work[2], nl, rhs);
+}
+
+template <int M, typename TW>
+void launch_batch_m(const RhsJob* jobs, int nj, int blocks, int sub, cudaStream_t s) {
+  static unsigned long long attr_set = 0;
+  constexpr size_t bytes = rhs_smem_bytes<M, TW>();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !(attr_set >> dev & 1ULL)) {
+    cudaFuncSetAttribute(k_rhs_march_batch<M, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    attr_set |= 1ULL << dev;
+  }
+  k_rhs_march_batch<M, TW><<<blocks, dim3(RTX, RTY), bytes, s>>>(jobs, nj, sub);
 }
 
 }  // namespace
+
+void rhs_march_job_grid(const Geom& g, RhsJob& J) {
+  J.kz = rhs_march_kz(g);
+  J.gx = (g.n1 + RTX - 1) / RTX;
+  J.gy = (g.n2 + RTY - 1) / RTY;
+  J.gz = (g.n3 + J.kz - 1) / J.kz;
+}
+
+void launch_rhs_march_batch(int m, const RhsJob* jobs, int nj, int blocks, int sub, int f32, cudaStream_t s) {
+  if (f32) {
+    if (m == 0)
+      launch_batch_m<0, float>(jobs, nj, blocks, sub, s);
+    else if (m == 1)
+      launch_batch_m<1, float>(jobs, nj, blocks, sub, s);
+    else
+      launch_batch_m<2, float>(jobs, nj, blocks, sub, s);
+  } else {
+    if (m == 0)
+      launch_batch_m<0, double>(jobs, nj, blocks, sub, s);
+    else if (m == 1)
+      launch_batch_m<1, double>(jobs, nj, blocks, sub, s);
+    else
+      launch_batch_m<2, double>(jobs, nj, blocks, sub, s);
+  }
+}
 
 // planes per block: enough blocks for several waves of two blocks per SM, at most 64 planes
 int rhs_march_kz(const Geom& g) {
@@ -321,11 +428,22 @@ void launch_rhs_march(int m, const Geom& g, const Coeffs<double>& c, double mult
                       int use_old, const double* vel, const double* const work[3], double* nl, double* rhs,
                       cudaStream_t s) {
   if (m == 0)
-    launch_m<0>(g, c, multL, mult_b, mult_a, use_old, vel, work, nl, rhs, s);
+    launch_m<0, double>(g, c, multL, mult_b, mult_a, use_old, vel, work, nl, rhs, s);
   else if (m == 1)
-    launch_m<1>(g, c, multL, mult_b, mult_a, use_old, vel, work, nl, rhs, s);
+    launch_m<1, double>(g, c, multL, mult_b, mult_a, use_old, vel, work, nl, rhs, s);
   else
-    launch_m<2>(g, c, multL, mult_b, mult_a, use_old, vel, work, nl, rhs, s);
+    launch_m<2, double>(g, c, multL, mult_b, mult_a, use_old, vel, work, nl, rhs, s);
+}
+
+void launch_rhs_march32(int m, const Geom& g, const Coeffs<float>& c, double multL, double mult_b, double mult_a,
+                        int use_old, const double* vel, const float* const work[3], float* nl, double* rhs,
+                        cudaStream_t s) {
+  if (m == 0)
+    launch_m<0, float>(g, c, multL, mult_b, mult_a, use_old, vel, work, nl, rhs, s);
+  else if (m == 1)
+    launch_m<1, float>(g, c, multL, mult_b, mult_a, use_old, vel, work, nl, rhs, s);
+  else
+    launch_m<2, float>(g, c, multL, mult_b, mult_a, use_old, vel, work, nl, rhs, s);
 }
 
 }  // namespace impact

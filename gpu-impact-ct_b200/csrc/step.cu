@@ -86,12 +86,19 @@ __device__ __forceinline__ double st1w_acc(double v, const double* __restrict__ 
   for (int l = 0; l < CNT; ++l) v = v + cr[l] * __ldg(fp + l * s);
   return v;
 }
-// the block's points and their 3-point halos stay inside 1..n on every axis
-__device__ __forceinline__ bool block_interior(const Geom& g, int k) {
-  const int i0 = blockIdx.x * BX + 1, j0 = blockIdx.y * BY + 1;
+// the points of block (bx, by) on plane k and their 3-point halos stay inside 1..n on every axis
+__device__ __forceinline__ bool block_interior(const Geom& g, int bx, int by, int k) {
+  const int i0 = bx * BX + 1, j0 = by * BY + 1;
   return i0 - 3 >= 1 && i0 + BX - 1 + 3 <= g.n1 && j0 - 3 >= 1 && j0 + BY - 1 + 3 <= g.n2 && k - 3 >= 1 &&
          k + 3 <= g.n3;
 }
+// the point of this thread in block (bx, by, bz) of a grid3 launch; returns false outside the grid
+#define PTB(bx, by, bz)                                      \
+  const int i = (bx) * BX + threadIdx.x + 1;                 \
+  const int j = (by) * BY + threadIdx.y + 1;                 \
+  const int k = (bz) + 1;                                    \
+  if (i > g.n1 || j > g.n2) return;                          \
+  const long long p = off(g, i, j, k);
 
 template <int LO, int CNT>
 __device__ __forceinline__ double st1(const double* __restrict__ c, const double* __restrict__ f, const Geom& g, int a,
@@ -117,37 +124,55 @@ __device__ __forceinline__ double st1_acc(double v, const double* __restrict__ c
   return v;
 }
 
-// interpolate_vel (mod_diff.f90:1436-1472): work_m = I_{u_m -> p} vel_m, three components
+// interpolate_vel (mod_diff.f90:1436-1472): work_m = I_{u_m -> p} vel_m, three components, in
+// FP64 from the FP64 velocity; TO = float stores the FP32 work fields of a mixed-precision case
+template <typename TO>
+__device__ __forceinline__ void interp_vel3_block(const Geom& g, const Coeffs<double>& c, const double* __restrict__ u,
+                                                  const double* __restrict__ v, const double* __restrict__ w,
+                                                  TO* __restrict__ w1, TO* __restrict__ w2, TO* __restrict__ w3,
+                                                  int bx, int by, int bz) {
+  const bool wrap = !block_interior(g, bx, by, bz + 1);
+  PTB(bx, by, bz)
+  if (wrap) {
+    w1[p] = (TO)st1w<D_LO, ND, true>(c.cIup[0], u, g, 0, i, j, k, p);
+    w2[p] = (TO)st1w<D_LO, ND, true>(c.cIup[1], v, g, 1, i, j, k, p);
+    w3[p] = (TO)st1w<D_LO, ND, true>(c.cIup[2], w, g, 2, i, j, k, p);
+  } else {
+    w1[p] = (TO)st1w<D_LO, ND, false>(c.cIup[0], u, g, 0, i, j, k, p);
+    w2[p] = (TO)st1w<D_LO, ND, false>(c.cIup[1], v, g, 1, i, j, k, p);
+    w3[p] = (TO)st1w<D_LO, ND, false>(c.cIup[2], w, g, 2, i, j, k, p);
+  }
+}
+__global__ void __launch_bounds__(NT) k_interp_vel3_32(Geom g, Coeffs<double> c, const double* __restrict__ u,
+                                                       const double* __restrict__ v, const double* __restrict__ w,
+                                                       float* __restrict__ w1, float* __restrict__ w2,
+                                                       float* __restrict__ w3) {
+  interp_vel3_block<float>(g, c, u, v, w, w1, w2, w3, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 __global__ void __launch_bounds__(NT) k_interp_vel3(Geom g, Coeffs<double> c, const double* __restrict__ u,
                                                     const double* __restrict__ v, const double* __restrict__ w,
                                                     double* __restrict__ w1, double* __restrict__ w2,
                                                     double* __restrict__ w3) {
-  const bool wrap = !block_interior(g, blockIdx.z + 1);
-  PT
-  if (wrap) {
-    w1[p] = st1w<D_LO, ND, true>(c.cIup[0], u, g, 0, i, j, k, p);
-    w2[p] = st1w<D_LO, ND, true>(c.cIup[1], v, g, 1, i, j, k, p);
-    w3[p] = st1w<D_LO, ND, true>(c.cIup[2], w, g, 2, i, j, k, p);
-  } else {
-    w1[p] = st1w<D_LO, ND, false>(c.cIup[0], u, g, 0, i, j, k, p);
-    w2[p] = st1w<D_LO, ND, false>(c.cIup[1], v, g, 1, i, j, k, p);
-    w3[p] = st1w<D_LO, ND, false>(c.cIup[2], w, g, 2, i, j, k, p);
-  }
+  interp_vel3_block<double>(g, c, u, v, w, w1, w2, w3, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // pre = pre * ab * dt  (mod_timeint.f90:318)  /  pre = pre / ab / dt  (:372)
-__global__ void __launch_bounds__(NT) k_scale_pre(Geom g, double ab, double dt, int divide, double* __restrict__ pre) {
-  PT
+__device__ __forceinline__ void scale_pre_block(const Geom& g, double ab, double dt, int divide,
+                                                double* __restrict__ pre, int bx, int by, int bz) {
+  PTB(bx, by, bz)
   pre[p] = divide ? pre[p] / ab / dt : pre[p] * ab * dt;
+}
+__global__ void __launch_bounds__(NT) k_scale_pre(Geom g, double ab, double dt, int divide, double* __restrict__ pre) {
+  scale_pre_block(g, ab, dt, divide, pre, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // explicit (mod_solvers.f90:180-330): vel_m = rhs_m - G_m pre for the three components
-__global__ void __launch_bounds__(NT) k_project(Geom g, Coeffs<double> c, const double* __restrict__ pre,
-                                                const double* __restrict__ r1, const double* __restrict__ r2,
-                                                const double* __restrict__ r3, double* __restrict__ u,
-                                                double* __restrict__ v, double* __restrict__ w) {
-  const bool wrap = !block_interior(g, blockIdx.z + 1);
-  PT
+__device__ __forceinline__ void project_block(const Geom& g, const Coeffs<double>& c, const double* __restrict__ pre,
+                                              const double* __restrict__ r1, const double* __restrict__ r2,
+                                              const double* __restrict__ r3, double* __restrict__ u,
+                                              double* __restrict__ v, double* __restrict__ w, int bx, int by, int bz) {
+  const bool wrap = !block_interior(g, bx, by, bz + 1);
+  PTB(bx, by, bz)
   if (wrap) {
     u[p] = 1.0 * r1[p] + (-1.0) * st1w<G_LO, NG, true>(c.cG[0], pre, g, 0, i, j, k, p);
     v[p] = 1.0 * r2[p] + (-1.0) * st1w<G_LO, NG, true>(c.cG[1], pre, g, 1, i, j, k, p);
@@ -157,6 +182,29 @@ __global__ void __launch_bounds__(NT) k_project(Geom g, Coeffs<double> c, const 
     v[p] = 1.0 * r2[p] + (-1.0) * st1w<G_LO, NG, false>(c.cG[1], pre, g, 1, i, j, k, p);
     w[p] = 1.0 * r3[p] + (-1.0) * st1w<G_LO, NG, false>(c.cG[2], pre, g, 2, i, j, k, p);
   }
+}
+__global__ void __launch_bounds__(NT) k_project(Geom g, Coeffs<double> c, const double* __restrict__ pre,
+                                                const double* __restrict__ r1, const double* __restrict__ r2,
+                                                const double* __restrict__ r3, double* __restrict__ u,
+                                                double* __restrict__ v, double* __restrict__ w) {
+  project_block(g, c, pre, r1, r2, r3, u, v, w, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// divergence2 (mod_diff.f90:130-215) of the provisional velocity into the pressure equation's
+// right-hand side: x stencil, then y and z added in table order
+__device__ __forceinline__ void div2_block(const Geom& g, const Coeffs<double>& c, const double* __restrict__ u,
+                                           const double* __restrict__ v, const double* __restrict__ w,
+                                           double* __restrict__ div, int bx, int by, int bz) {
+  PTB(bx, by, bz)
+  double d = st1<D_LO, ND>(c.cD[0], u, g, 0, i, j, k, p);
+  d = st1_acc<D_LO, ND>(d, c.cD[1], v, g, 1, i, j, k, p);
+  d = st1_acc<D_LO, ND>(d, c.cD[2], w, g, 2, i, j, k, p);
+  div[p] = d;
+}
+__global__ void __launch_bounds__(NT) k_div2(Geom g, Coeffs<double> c, const double* __restrict__ u,
+                                             const double* __restrict__ v, const double* __restrict__ w,
+                                             double* __restrict__ div) {
+  div2_block(g, c, u, v, w, div, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // get_dtime (mod_lib.f90:46-250), timeint_mode 1: block max of radius / stabilitylimit(angle)
@@ -173,12 +221,13 @@ __device__ __forceinline__ double wsum_d(double v) {
   return v;
 }
 
-__global__ void __launch_bounds__(NT) k_dtime(Geom g, Coeffs<double> c, DtRows dr, double Re, const double* __restrict__ u,
-                                              const double* __restrict__ v, const double* __restrict__ w,
-                                              double* __restrict__ partial) {
-  const int i = blockIdx.x * BX + threadIdx.x + 1;
-  const int j = blockIdx.y * BY + threadIdx.y + 1;
-  const int k = blockIdx.z + 1;
+__device__ __forceinline__ void dtime_block(const Geom& g, const Coeffs<double>& c, const DtRows& dr, double Re,
+                                            const double* __restrict__ u, const double* __restrict__ v,
+                                            const double* __restrict__ w, double* __restrict__ partial, int bx,
+                                            int by, int bz, int gx, int gy) {
+  const int i = bx * BX + threadIdx.x + 1;
+  const int j = by * BY + threadIdx.y + 1;
+  const int k = bz + 1;
   double beta = 0.0;
   if (i <= g.n1 && j <= g.n2) {
     const long long p = off(g, i, j, k);
@@ -206,13 +255,18 @@ __global__ void __launch_bounds__(NT) k_dtime(Geom g, Coeffs<double> c, DtRows d
   if (tid < 32) {
     double x = tid < NT / 32 ? sh[tid] : 0.0;
     x = wmax_d(x);
-    if (tid == 0) partial[blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = x;
+    if (tid == 0) partial[bx + (long long)gx * (by + (long long)gy * bz)] = x;
   }
+}
+__global__ void __launch_bounds__(NT) k_dtime(Geom g, Coeffs<double> c, DtRows dr, double Re, const double* __restrict__ u,
+                                              const double* __restrict__ v, const double* __restrict__ w,
+                                              double* __restrict__ partial) {
+  dtime_block(g, c, dr, Re, u, v, w, partial, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y);
 }
 
 // fixed-order max / sum over n partials (single block)
-__global__ void __launch_bounds__(1024) k_reduce_partials(const double* __restrict__ partial, long long n, int is_max,
-                                                          double* __restrict__ out) {
+__device__ __forceinline__ void reduce_partials_block(const double* __restrict__ partial, long long n, int is_max,
+                                                      double* __restrict__ out) {
   __shared__ double sh[32];
   double v = 0.0;
   for (long long b = threadIdx.x; b < n; b += blockDim.x) v = is_max ? fmax(v, partial[b]) : v + partial[b];
@@ -225,6 +279,10 @@ __global__ void __launch_bounds__(1024) k_reduce_partials(const double* __restri
     if (threadIdx.x == 0) *out = x;
   }
 }
+__global__ void __launch_bounds__(1024) k_reduce_partials(const double* __restrict__ partial, long long n, int is_max,
+                                                          double* __restrict__ out) {
+  reduce_partials_block(partial, n, is_max, out);
+}
 
 // sum of pre over the unique points, block partials (level_pressure, mod_lib.f90:507-537)
 // FP64 -> FP32 and back, whole padded fields
@@ -236,10 +294,11 @@ __global__ void k_widen(const float* __restrict__ a, double* __restrict__ b, lon
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
     b[q] = (double)a[q];
 }
-__global__ void __launch_bounds__(NT) k_sum(Geom g, const double* __restrict__ a, double* __restrict__ partial) {
-  const int i = blockIdx.x * BX + threadIdx.x + 1;
-  const int j = blockIdx.y * BY + threadIdx.y + 1;
-  const int k = blockIdx.z + 1;
+__device__ __forceinline__ void sum_block(const Geom& g, const double* __restrict__ a, double* __restrict__ partial,
+                                          int bx, int by, int bz, int gx, int gy) {
+  const int i = bx * BX + threadIdx.x + 1;
+  const int j = by * BY + threadIdx.y + 1;
+  const int k = bz + 1;
   double s = (i <= g.n1 && j <= g.n2) ? a[off(g, i, j, k)] : 0.0;
   __shared__ double sh[NT / 32];
   const int tid = threadIdx.x + BX * threadIdx.y;
@@ -249,21 +308,29 @@ __global__ void __launch_bounds__(NT) k_sum(Geom g, const double* __restrict__ a
   if (tid < 32) {
     double x = tid < NT / 32 ? sh[tid] : 0.0;
     x = wsum_d(x);
-    if (tid == 0) partial[blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z)] = x;
+    if (tid == 0) partial[bx + (long long)gx * (by + (long long)gy * bz)] = x;
   }
 }
-__global__ void __launch_bounds__(NT) k_sub_mean(Geom g, const double* __restrict__ sum, double* __restrict__ pre) {
-  PT
+__global__ void __launch_bounds__(NT) k_sum(Geom g, const double* __restrict__ a, double* __restrict__ partial) {
+  sum_block(g, a, partial, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y);
+}
+__device__ __forceinline__ void sub_mean_block(const Geom& g, const double* __restrict__ sum, double* __restrict__ pre,
+                                               int bx, int by, int bz) {
+  PTB(bx, by, bz)
   const double m = *sum / (double)g.n1 / (double)g.n2 / (double)g.n3;
   pre[p] = pre[p] - m;
+}
+__global__ void __launch_bounds__(NT) k_sub_mean(Geom g, const double* __restrict__ sum, double* __restrict__ pre) {
+  sub_mean_block(g, sum, pre, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // apply_CT_forcing (usr_func.f90:909-1049, idealized branch): label 0/7 -> u = 0; 5 -> inflow
 // inflow_on = 0: the inflow voxels keep their velocity (a measured waveform without an interval
 // that holds the current time, as in apply_CT_forcing)
-__global__ void __launch_bounds__(NT) k_mask(Geom g, const uint8_t* __restrict__ label, double u_in, int inflow_on,
-                                             double* __restrict__ u, double* __restrict__ v, double* __restrict__ w) {
-  PT
+__device__ __forceinline__ void mask_block(const Geom& g, const uint8_t* __restrict__ label, double u_in, int inflow_on,
+                                           double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
+                                           int bx, int by, int bz) {
+  PTB(bx, by, bz)
   const uint8_t lb = label[p];
   if (lb == 0 || lb == 7) {
     u[p] = 0.0;
@@ -274,6 +341,101 @@ __global__ void __launch_bounds__(NT) k_mask(Geom g, const uint8_t* __restrict__
     v[p] = 0.0;
     u[p] = 0.0;
   }
+}
+__global__ void __launch_bounds__(NT) k_mask(Geom g, const uint8_t* __restrict__ label, double u_in, int inflow_on,
+                                             double* __restrict__ u, double* __restrict__ v, double* __restrict__ w) {
+  mask_block(g, label, u_in, inflow_on, u, v, w, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// ---------------------------------------------------------------------------------------
+// the explicit part of a batch step: one launch per kernel over all cases.  Block b of a
+// launch is block b - job.b0 of its case's grid3 grid (gx x gy x gz); every block runs the same
+// body as the single-case kernel, so a case's bits do not depend on the batch.
+// ---------------------------------------------------------------------------------------
+struct StepScal {  // per case and step: time step, Reynolds number, inflow at the step's end
+  double dt, Re, u_in;
+  int inflow_on, level_pressure;
+};
+struct ExJob {
+  Geom g;
+  Coeffs<double> c;
+  DtRows dr;
+  double* vel[3];
+  double* nl[3];
+  double* rhs[3];
+  double* work[3];
+  float* work32[3];  // mixed precision: the FP32 interpolated velocities (null in FP64)
+  double* pre;
+  double* res;
+  const uint8_t* label;
+  double* partial;
+  double* dscal;
+  const StepScal* sc;  // this case's scalars of the current step
+  int gx, gy, gz, b0;
+};
+
+__device__ __forceinline__ int ex_job(const ExJob* __restrict__ jobs, int nj, int b) {
+  int lo = 0, hi = nj - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].b0 <= b) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+#define EX_BLOCK                                                         \
+  const ExJob& J = jobs[ex_job(jobs, nj, blockIdx.x)];                   \
+  const int lb = blockIdx.x - J.b0;                                      \
+  const int bx = lb % J.gx, by = (lb / J.gx) % J.gy, bz = lb / (J.gx * J.gy); \
+  const Geom& g = J.g;                                                   \
+  (void)g;
+
+__constant__ double RKA_D[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+__constant__ double RKB_D[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+
+__global__ void __launch_bounds__(NT) k_b_dtime(const ExJob* __restrict__ jobs, int nj) {
+  EX_BLOCK
+  dtime_block(g, J.c, J.dr, J.sc->Re, J.vel[0], J.vel[1], J.vel[2], J.partial, bx, by, bz, J.gx, J.gy);
+}
+// one block per case: out = dscal[slot] of the case
+// one block per case: the case's dscal[slot], or out[case] when out is given
+__global__ void __launch_bounds__(1024) k_b_reduce(const ExJob* __restrict__ jobs, int is_max, int slot, int only_lp,
+                                                   double* __restrict__ out) {
+  const ExJob& J = jobs[blockIdx.x];
+  if (only_lp && !J.sc->level_pressure) return;
+  reduce_partials_block(J.partial, (long long)J.gx * J.gy * J.gz, is_max, out ? out + blockIdx.x : J.dscal + slot);
+}
+__global__ void __launch_bounds__(NT) k_b_interp(const ExJob* __restrict__ jobs, int nj) {
+  EX_BLOCK
+  if (J.work32[0])
+    interp_vel3_block<float>(g, J.c, J.vel[0], J.vel[1], J.vel[2], J.work32[0], J.work32[1], J.work32[2], bx, by, bz);
+  else
+    interp_vel3_block<double>(g, J.c, J.vel[0], J.vel[1], J.vel[2], J.work[0], J.work[1], J.work[2], bx, by, bz);
+}
+__global__ void __launch_bounds__(NT) k_b_scale_pre(const ExJob* __restrict__ jobs, int nj, int sub, int divide) {
+  EX_BLOCK
+  scale_pre_block(g, RKA_D[sub] + RKB_D[sub], J.sc->dt, divide, J.pre, bx, by, bz);
+}
+__global__ void __launch_bounds__(NT) k_b_div2(const ExJob* __restrict__ jobs, int nj) {
+  EX_BLOCK
+  div2_block(g, J.c, J.rhs[0], J.rhs[1], J.rhs[2], J.res, bx, by, bz);
+}
+__global__ void __launch_bounds__(NT) k_b_project(const ExJob* __restrict__ jobs, int nj) {
+  EX_BLOCK
+  project_block(g, J.c, J.pre, J.rhs[0], J.rhs[1], J.rhs[2], J.vel[0], J.vel[1], J.vel[2], bx, by, bz);
+}
+__global__ void __launch_bounds__(NT) k_b_mask(const ExJob* __restrict__ jobs, int nj) {
+  EX_BLOCK
+  mask_block(g, J.label, J.sc->u_in, J.sc->inflow_on, J.vel[0], J.vel[1], J.vel[2], bx, by, bz);
+}
+__global__ void __launch_bounds__(NT) k_b_sum(const ExJob* __restrict__ jobs, int nj) {
+  EX_BLOCK
+  if (!J.sc->level_pressure) return;
+  sum_block(g, J.pre, J.partial, bx, by, bz, J.gx, J.gy);
+}
+__global__ void __launch_bounds__(NT) k_b_sub_mean(const ExJob* __restrict__ jobs, int nj) {
+  EX_BLOCK
+  if (!J.sc->level_pressure) return;
+  sub_mean_block(g, J.dscal + 1, J.pre, bx, by, bz);
 }
 
 }  // namespace impact
@@ -516,6 +678,11 @@ extern "C" int impact_b200_case_create(const impact_b200_case_desc* desc, const 
   const size_t fb = (size_t)g.nfield * sizeof(double);
   for (int q = 0; q < IMPACT_B200_NFIELDS; ++q) rc |= case_alloc(s, (void**)&s.f[q], fb);
   for (int q = 0; q < 3; ++q) rc |= case_alloc(s, (void**)&s.work[q], fb);
+  if (s.precision == 1)
+    for (int q = 0; q < 3; ++q) {
+      rc |= case_alloc(s, (void**)&s.work32[q], (size_t)g.nfield * sizeof(float));
+      rc |= case_alloc(s, (void**)&s.nl32[q], (size_t)g.nfield * sizeof(float));
+    }
   rc |= case_alloc(s, (void**)&s.label, (size_t)g.nfield);
   const size_t pd = (size_t)reduce_partial_doubles(g, 4) * sizeof(double);
   rc |= case_alloc(s, (void**)&s.partial, pd);
@@ -624,6 +791,11 @@ extern "C" int impact_b200_case_create(const impact_b200_case_desc* desc, const 
   for (void* p : s.allocs) (void)p;
   for (int q = 0; q < IMPACT_B200_NFIELDS; ++q) cudaMemsetAsync(s.f[q], 0, fb, s.stream);
   for (int q = 0; q < 3; ++q) cudaMemsetAsync(s.work[q], 0, fb, s.stream);
+  if (s.precision == 1)
+    for (int q = 0; q < 3; ++q) {
+      cudaMemsetAsync(s.work32[q], 0, (size_t)g.nfield * sizeof(float), s.stream);
+      cudaMemsetAsync(s.nl32[q], 0, (size_t)g.nfield * sizeof(float), s.stream);
+    }
   cudaMemsetAsync(s.label, 1, (size_t)g.nfield, s.stream);
   if (s.precision == 0) {
     KrylovWork<double>& w = s.kw64;
@@ -1161,14 +1333,24 @@ static void substep_rhs(CaseState& s, const impact_b200_step_params* p, double d
   double* nl[3] = {s.f[IMPACT_B200_NL1], s.f[IMPACT_B200_NL2], s.f[IMPACT_B200_NL3]};
   double* rhs[3] = {s.f[IMPACT_B200_RHS1], s.f[IMPACT_B200_RHS2], s.f[IMPACT_B200_RHS3]};
   const double multL = 1.0 / p->Re;
-  k_interp_vel3<<<gr, bl, 0, st>>>(g, s.c64, vel[0], vel[1], vel[2], s.work[0], s.work[1], s.work[2]);
-  prof::count(1);
   const double mb = dt * bRK[sub], ma = dt * aRK[sub];
   const int use_old = sub != 0;
-  const double nlb = (use_old ? 7.0 : 6.0) * 8.0 * cells;
-  for (int m = 0; m < 3; ++m)
-    IMPACT_PROF(prof::K_NL_RHS, nlb, st,
-                launch_rhs_march(m, g, s.c64, multL, mb, ma, use_old, vel[m], s.work, nl[m], rhs[m], st));
+  if (s.precision == 1) {  // FP32 rhs_vel pass: FP32 work fields and nonlinear term
+    k_interp_vel3_32<<<gr, bl, 0, st>>>(g, s.c64, vel[0], vel[1], vel[2], s.work32[0], s.work32[1], s.work32[2]);
+    prof::count(1);
+    // bytes: vel 8 (the staged tile and the point), work 3 x 4, nl 4 (+4 old), rhs 8
+    const double nlb = (use_old ? 36.0 : 32.0) * cells;
+    for (int m = 0; m < 3; ++m)
+      IMPACT_PROF(prof::K_NL_RHS, nlb, st,
+                  launch_rhs_march32(m, g, s.c32, multL, mb, ma, use_old, vel[m], s.work32, s.nl32[m], rhs[m], st));
+  } else {
+    k_interp_vel3<<<gr, bl, 0, st>>>(g, s.c64, vel[0], vel[1], vel[2], s.work[0], s.work[1], s.work[2]);
+    prof::count(1);
+    const double nlb = (use_old ? 7.0 : 6.0) * 8.0 * cells;
+    for (int m = 0; m < 3; ++m)
+      IMPACT_PROF(prof::K_NL_RHS, nlb, st,
+                  launch_rhs_march(m, g, s.c64, multL, mb, ma, use_old, vel[m], s.work, nl[m], rhs[m], st));
+  }
   const double ab = aRK[sub] + bRK[sub];
   if (s.pre_wait) {  // a deferred pressure upload: wait for it here, at the step's first read
     cudaStreamWaitEvent(st, s.pre_wait, 0);
@@ -1177,8 +1359,7 @@ static void substep_rhs(CaseState& s, const impact_b200_step_params* p, double d
   k_scale_pre<<<gr, bl, 0, st>>>(g, ab, dt, 0, s.f[IMPACT_B200_PRE]);
   prof::count(1);
   IMPACT_PROF(prof::K_DIV2, 4.0 * 8.0 * cells, st,
-              launch_divergence2<double>(g, s.c64.cD[0], s.c64.cD[1], s.c64.cD[2], rhs[0], rhs[1], rhs[2],
-                                         s.f[IMPACT_B200_RES], st));
+              (k_div2<<<gr, bl, 0, st>>>(g, s.c64, rhs[0], rhs[1], rhs[2], s.f[IMPACT_B200_RES])));
 }
 
 // projection vel = rhs - G pre and the pressure scaling back (mod_timeint.f90:372)
@@ -1285,6 +1466,13 @@ struct impact_b200_batch {
   Engine<double> e64;
   MixedEngine emx;
   double* hbeta = nullptr;  // pinned, one per case
+  // the explicit part's job lists (built on the first step) and per-step scalars
+  ExJob* d_ex = nullptr;
+  RhsJob* d_rhs = nullptr;
+  StepScal* d_sc = nullptr;
+  StepScal* h_sc = nullptr;  // pinned
+  double* d_beta = nullptr;
+  int ex_blocks = 0, rhs_blocks = 0;
 };
 
 extern "C" int impact_b200_batch_destroy(impact_b200_batch* b) {
@@ -1294,6 +1482,11 @@ extern "C" int impact_b200_batch_destroy(impact_b200_batch* b) {
   b->e64.release();
   b->emx.release();
   if (b->hbeta) cudaFreeHost(b->hbeta);
+  if (b->h_sc) cudaFreeHost(b->h_sc);
+  cudaFree(b->d_ex);
+  cudaFree(b->d_rhs);
+  cudaFree(b->d_sc);
+  cudaFree(b->d_beta);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return 0;
@@ -1321,6 +1514,75 @@ extern "C" int impact_b200_batch_create(impact_b200_case* const* cases, int ncas
     return impact_set_error(e, "impact_b200_batch_create", __FILE__, __LINE__);
   }
   *out = b;
+  return 0;
+}
+
+// the explicit part's job lists of a batch (the cases' fields do not move while they exist)
+static int batch_jobs(impact_b200_batch* b) {
+  if (b->d_ex) return 0;
+  const int n = (int)b->cases.size();
+  std::vector<ExJob> ex(n);
+  std::vector<RhsJob> rj(n);
+  int eb = 0, rb = 0;
+  cudaError_t e = cudaMalloc((void**)&b->d_sc, n * sizeof(StepScal));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_sc, n * sizeof(StepScal));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_beta, n * sizeof(double));
+  for (int c = 0; c < n && e == cudaSuccess; ++c) {
+    CaseState& s = b->cases[c]->s;
+    ExJob& J = ex[c];
+    J = ExJob{};
+    J.g = s.g;
+    J.c = s.c64;
+    J.dr = s.dt;
+    for (int m = 0; m < 3; ++m) {
+      J.vel[m] = s.f[IMPACT_B200_VEL1 + m];
+      J.nl[m] = s.f[IMPACT_B200_NL1 + m];
+      J.rhs[m] = s.f[IMPACT_B200_RHS1 + m];
+      J.work[m] = s.work[m];
+      J.work32[m] = s.work32[m];
+    }
+    J.pre = s.f[IMPACT_B200_PRE];
+    J.res = s.f[IMPACT_B200_RES];
+    J.label = s.label;
+    J.partial = s.partial;
+    J.dscal = s.dscal;
+    J.sc = b->d_sc + c;
+    const dim3 d = grid3(s.g);
+    J.gx = d.x;
+    J.gy = d.y;
+    J.gz = d.z;
+    J.b0 = eb;
+    eb += J.gx * J.gy * J.gz;
+    RhsJob& R = rj[c];
+    R = RhsJob{};
+    R.g = s.g;
+    R.c = s.c64;
+    R.c32 = s.c32;
+    R.Re = &b->d_sc[c].Re;
+    R.dt = &b->d_sc[c].dt;
+    for (int m = 0; m < 3; ++m) {
+      R.vel[m] = J.vel[m];
+      R.work[m] = J.work[m];
+      R.nl[m] = J.nl[m];
+      R.work32[m] = s.work32[m];
+      R.nl32[m] = s.nl32[m];
+      R.rhs[m] = J.rhs[m];
+    }
+    rhs_march_job_grid(s.g, R);
+    R.b0 = rb;
+    rb += R.gx * R.gy * R.gz;
+  }
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_ex, n * sizeof(ExJob));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_rhs, n * sizeof(RhsJob));
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_ex, ex.data(), n * sizeof(ExJob), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_rhs, rj.data(), n * sizeof(RhsJob), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(b->d_ex);
+    b->d_ex = nullptr;
+    return impact_set_error(e, "batch job lists", __FILE__, __LINE__);
+  }
+  b->ex_blocks = eb;
+  b->rhs_blocks = rb;
   return 0;
 }
 
@@ -1416,18 +1678,46 @@ extern "C" int impact_b200_batch_step(impact_b200_batch* b, const impact_b200_st
   std::vector<SolverScalars> init(n);
   std::vector<SolverResult> res;
   std::vector<int> its;
+  if (batch_jobs(b)) return -1;
+  const ExJob* EJ = b->d_ex;
+  double cells = 0.0;
+  for (auto* c : b->cases) cells += (double)c->s.g.n1 * c->s.g.n2 * c->s.g.n3;
+  const dim3 bl(BX, BY);
   for (int step = 0; step < nsteps; ++step) {
+    // get_dtime of every case in one launch, the CFL bounds back in one copy
     for (int c = 0; c < n; ++c) {
-      step_beta(b->cases[c]->s, &p[c], bs);
-      IMPACT_CUDA_CHECK(cudaMemcpyAsync(b->hbeta + c, b->cases[c]->s.dscal, sizeof(double), cudaMemcpyDeviceToHost, bs));
+      b->h_sc[c] = StepScal{0.0, p[c].Re, 0.0, 1, p[c].level_pressure};
     }
+    IMPACT_CUDA_CHECK(cudaMemcpyAsync(b->d_sc, b->h_sc, n * sizeof(StepScal), cudaMemcpyHostToDevice, bs));
+    k_b_dtime<<<b->ex_blocks, bl, 0, bs>>>(EJ, n);
+    k_b_reduce<<<n, 1024, 0, bs>>>(EJ, 1, 0, 0, b->d_beta);
+    prof::count(2);
+    IMPACT_CUDA_CHECK(cudaMemcpyAsync(b->hbeta, b->d_beta, n * sizeof(double), cudaMemcpyDeviceToHost, bs));
     IMPACT_CUDA_CHECK(cudaStreamSynchronize(bs));
     for (int c = 0; c < n; ++c) {
       dt[c] = dt_from_beta(b->hbeta[c], &p[c], &st[c]);
       st[c].dtime = dt[c];
+      int on = 1;
+      const double u_in = inflow_velocity(b->cases[c]->s, &p[c], st[c].time + dt[c], &on);
+      b->h_sc[c] = StepScal{dt[c], p[c].Re, u_in, on, p[c].level_pressure};
     }
+    IMPACT_CUDA_CHECK(cudaMemcpyAsync(b->d_sc, b->h_sc, n * sizeof(StepScal), cudaMemcpyHostToDevice, bs));
     for (int sub = 0; sub < 3; ++sub) {
-      for (int c = 0; c < n; ++c) substep_rhs(b->cases[c]->s, &p[c], dt[c], sub, bs);
+      // rhs_vel and the pressure equation's right-hand side of every case, one launch per kernel
+      k_b_interp<<<b->ex_blocks, bl, 0, bs>>>(EJ, n);
+      prof::count(1);
+      const int f32 = b->precision == 1;
+      for (int m = 0; m < 3; ++m)
+        IMPACT_PROF(prof::K_NL_RHS, (f32 ? (sub != 0 ? 36.0 : 32.0) : (sub != 0 ? 56.0 : 48.0)) * cells, bs,
+                    launch_rhs_march_batch(m, b->d_rhs, n, b->rhs_blocks, sub, f32, bs));
+      for (auto* c : b->cases)
+        if (c->s.pre_wait) {  // a deferred pressure upload: wait for it at the first read
+          IMPACT_CUDA_CHECK(cudaStreamWaitEvent(bs, c->s.pre_wait, 0));
+          c->s.pre_wait = nullptr;
+        }
+      k_b_scale_pre<<<b->ex_blocks, bl, 0, bs>>>(EJ, n, sub, 0);
+      prof::count(1);
+      IMPACT_PROF(prof::K_DIV2, 4.0 * 8.0 * cells, bs, (k_b_div2<<<b->ex_blocks, bl, 0, bs>>>(EJ, n)));
       for (int c = 0; c < n; ++c) {
         init[c] = SolverScalars{};
         init[c].tol_rel = p[c].poisson.tol_rel;
@@ -1452,10 +1742,26 @@ extern "C" int impact_b200_batch_step(impact_b200_batch* b, const impact_b200_st
         r.res_two = res[c].res_two;
         r.b_two = res[c].b_two;
         record_solve(&st[c], sub, r);
-        substep_project(b->cases[c]->s, dt[c], sub, bs);
       }
+      IMPACT_PROF(prof::K_PROJECT, 7.0 * 8.0 * cells, bs, (k_b_project<<<b->ex_blocks, bl, 0, bs>>>(EJ, n)));
+      k_b_scale_pre<<<b->ex_blocks, bl, 0, bs>>>(EJ, n, sub, 1);
+      prof::count(1);
     }
-    for (int c = 0; c < n; ++c) step_finish(b->cases[c]->s, &p[c], &st[c], dt[c], bs);
+    // mask forcing at the new time and level_pressure of every case
+    bool lp = false;
+    for (int c = 0; c < n; ++c) {
+      st[c].timestep += 1;
+      st[c].time += dt[c];
+      lp = lp || p[c].level_pressure;
+    }
+    k_b_mask<<<b->ex_blocks, bl, 0, bs>>>(EJ, n);
+    prof::count(1);
+    if (lp) {
+      k_b_sum<<<b->ex_blocks, bl, 0, bs>>>(EJ, n);
+      k_b_reduce<<<n, 1024, 0, bs>>>(EJ, 0, 1, 1, nullptr);
+      k_b_sub_mean<<<b->ex_blocks, bl, 0, bs>>>(EJ, n);
+      prof::count(3);
+    }
   }
   IMPACT_CUDA_CHECK(cudaStreamSynchronize(bs));
   IMPACT_CUDA_CHECK(cudaGetLastError());
@@ -1495,7 +1801,7 @@ extern "C" int impact_b200_case_kernel_bench(impact_b200_case* c, int kid, int i
         }
         case 13: k_interp_vel3<<<gr, bl, 0, s.stream>>>(g, s.c64, vel[0], vel[1], vel[2], s.work[0], s.work[1], s.work[2]); break;
         case 14: k_project<<<gr, bl, 0, s.stream>>>(g, s.c64, s.f[IMPACT_B200_PRE], rhs[0], rhs[1], rhs[2], vel[0], vel[1], vel[2]); break;
-        case 15: launch_divergence2<double>(g, s.c64.cD[0], s.c64.cD[1], s.c64.cD[2], rhs[0], rhs[1], rhs[2], s.f[IMPACT_B200_RES], s.stream); break;
+        case 15: k_div2<<<gr, bl, 0, s.stream>>>(g, s.c64, rhs[0], rhs[1], rhs[2], s.f[IMPACT_B200_RES]); break;
         default: return -1;
       }
       return 0;
