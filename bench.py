@@ -69,6 +69,8 @@ def parse():
                     help="V-cycle sweeps down / up / bottom of the batch and serve cases, and of the single case "
                          "with --no-tune (default: the autotuner's choice on the 384 case)")
     ap.add_argument("--tile-kc", type=int, default=64, help="tile depth of the solver kernels, as --sweeps")
+    ap.add_argument("--explicit-fp32", type=int, default=0,
+                    help="mixed precision: 1 = rhs_vel as the FP32 pass (FP32 work fields and nonlinear term)")
     ap.add_argument("--copy-chunks", type=int, default=8,
                     help="element ranges per field of the end-to-end copies (download and next upload pipeline)")
     ap.add_argument("--no-profile", action="store_true", help="no per-kernel events in the timed steps (no roofline)")
@@ -105,7 +107,7 @@ def step_params(args, precision):
                          n_sweeps=args.n_sweeps, omega=0.8, init_yes=0, check_every=args.check_every,
                          inner_tol_rel=args.inner_tol, inner_max_it=4000 if args.precond == 0 else 400,
                          precond=args.precond, mg_down=args.sweeps, mg_up=args.sweeps, mg_bottom=args.sweeps,
-                         tile_kc=args.tile_kc)
+                         tile_kc=args.tile_kc, explicit_fp32=args.explicit_fp32 if precision == 1 else 0)
 
 
 class ClockSampler:

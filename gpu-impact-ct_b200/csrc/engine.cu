@@ -1284,6 +1284,231 @@ __global__ void __launch_bounds__(AXV_NT, 4) k_kr_ax32v(const KrylovJob<float>* 
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// The FP64 operator (the Krylov list of an FP64 solve, and the outer residual of the mixed
+// solve) on grids with n1 divisible by 2: the collapsed 11-point product_div_grad with every
+// thread owning one 16-byte vector of 2 consecutive x points of one row.  Same staging, ring and
+// z window as k_kr_ax32v (16 x 8 threads per 32 x 8-column tile, 48 x 18 staged doubles per
+// plane, 3 groups of 4 planes, the window k-5 .. k+8 in registers); the weights are the per-row
+// weights of every axis (the FP64 operator defines the residual): x rows of the thread's two
+// columns and the y row of its row in registers, the z rows of the tile's planes in shared memory.
+//   MODE 0: rr = A phi;  1: Ap = A z1, partial rh.Ap;  2: Ar = A z2, partials Ar.rr, Ar.Ar;
+//   3: r32 = (float)(bb - A phi), partials max|r|, sum r^2, sum bb^2
+constexpr int AXD_TX = ETX / 2, AXD_NT = AXD_TX * ETY;   // 16 x 8 threads, 2 columns each
+constexpr int AXD_W = ETX + 16, AXD_H = ETY + 10;        // staged plane, doubles
+constexpr int AXD_CR = AXD_W / 2;                        // 16-byte chunks per row
+constexpr int AXD_NCH = AXD_CR * AXD_H;
+constexpr int AXD_PER = (AXD_NCH + AXD_NT - 1) / AXD_NT;
+constexpr int AXD_PLANE = AXD_W * AXD_H;
+constexpr int AXD_PP = ETX * ETY;
+constexpr int AXD_B = 4, AXD_G = 3, AXD_R = AXD_B * AXD_G, AXD_ZW = AXD_B + 10;
+constexpr size_t axd_smem_bytes() {
+  return sizeof(double) * ((size_t)AXD_R * (AXD_PLANE + AXD_PP) + (size_t)KC_MAX * AXW);
+}
+__device__ __forceinline__ double2 ldg2d(const double* p) { return __ldg(reinterpret_cast<const double2*>(p)); }
+__device__ __forceinline__ double2 lds2d(const double* p) { return *reinterpret_cast<const double2*>(p); }
+
+template <int MODE>
+__global__ void __launch_bounds__(AXD_NT, 2) k_kr_ax64v(const KrylovJob<double>* __restrict__ jobs,
+                                                        const int* __restrict__ ts, int nj, int ntiles,
+                                                        double* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char axd_smem[];
+  double* ring = reinterpret_cast<double*>(axd_smem);
+  double* pring = ring + (size_t)AXD_R * AXD_PLANE;
+  double(*wzs)[AXW] = reinterpret_cast<double(*)[AXW]>(pring + (size_t)AXD_R * AXD_PP);
+  __shared__ double red[3][AXD_NT / 32];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + AXD_TX * ty;
+  const int cx = 8 + 2 * tx;          // the thread's first column in a staged row
+  const int pq = ty * ETX + 2 * tx;   // the thread's vector in a partner slot
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int q = find_job(ts, nj, b);
+    const KrylovJob<double>& J = jobs[q];
+    const SolverScalars* sc = J.sc;
+    if (!J.vec || (MODE == 0 ? (sc->done != 0) : e_halted(sc))) continue;  // the others: k_kr_ax
+    const Geom g = J.g;
+    const int ntx = (g.n1 + ETX - 1) / ETX, nty = (g.n2 + ETY - 1) / ETY;
+    const int t0 = b - ts[q];
+    const int ta = t0 % ntx, tr = t0 / ntx, tc = tr / nty;
+    const int i0 = ta * ETX + 1, j0 = (tr - tc * nty) * ETY + 1;
+    const int k0 = tc * J.kc + 1, k1 = min(g.n3, k0 + J.kc - 1);
+    const int nk = k1 - k0 + 1;
+    const int i = i0 + 2 * tx, j = j0 + ty;
+    const bool act = i <= g.n1 && j <= g.n2;  // n1 % 2 == 0: both columns valid together
+    const double* __restrict__ x = (MODE == 0 || MODE == 3) ? J.phi : (MODE == 1 ? J.z1 : J.z2);
+    const double* __restrict__ d1 = MODE == 1 ? J.rh : (MODE == 3 ? J.bb : J.rr);
+    const long long nxy = g.nxy;
+    const int ir = act ? i : 1, jr = j <= g.n2 ? j : 1;
+    double wx0[AXW], wx1[AXW], wy[AXW];
+#pragma unroll
+    for (int l = 0; l < AXW; ++l) {
+      wx0[l] = __ldg(J.W[0] + (size_t)(ir - 1) * AXW + l);
+      wx1[l] = __ldg(J.W[0] + (size_t)ir * AXW + l);
+      wy[l] = __ldg(J.W[1] + (size_t)(jr - 1) * AXW + l);
+    }
+    for (int t = tid; t < nk * AXW; t += AXD_NT) wzs[t / AXW][t % AXW] = __ldg(J.W[2] + (size_t)(k0 - 1) * AXW + t);
+    const int ilast = min(i0 + ETX - 1, g.n1) + 5, jlast = min(j0 + ETY - 1, g.n2) + 5;
+    const bool tile_vec = i0 - 5 >= 1 && ilast <= g.n1;  // block-uniform
+    int cb[AXD_PER];
+#pragma unroll
+    for (int e = 0; e < AXD_PER; ++e) {
+      const int cq = tid + e * AXD_NT;
+      const int r = cq / AXD_CR, c0 = (cq % AXD_CR) * 2;
+      const int jj = j0 - 5 + r, ii = i0 - 8 + c0;
+      const bool need = cq < AXD_NCH && jj <= jlast && max(ii, i0 - 5) <= min(ii + 1, ilast);
+      cb[e] = need ? (ii + 3) + g.nx * (wrapi(jj, g.n2) + 3) : -1;
+    }
+    const int own = (act ? i + 3 : 4) + g.nx * (jr + 3);
+    auto zoff = [&](int k) -> long long {
+      return (long long)((k < 1 ? k + g.n3 : (k > g.n3 ? k - g.n3 : k)) + 3) * nxy;
+    };
+    auto stage_group = [&](int gi) {
+#pragma unroll
+      for (int u = 0; u < AXD_B; ++u) {
+        const int t = gi * AXD_B + u;
+        if (t < nk) {
+          const long long zo = zoff(k0 + t);
+          const double* src = x + zo;
+          double* dst = ring + (size_t)(t % AXD_R) * AXD_PLANE + tid * 2;
+          if (tile_vec) {
+#pragma unroll
+            for (int e = 0; e < AXD_PER; ++e)
+              if (cb[e] >= 0) cp_async16(dst + e * AXD_NT * 2, src + cb[e]);
+          } else {
+            for (int e = 0; e < AXD_PER; ++e) {
+              if (cb[e] < 0) continue;
+              const int cq = tid + e * AXD_NT;
+              const int r = cq / AXD_CR, c0 = (cq % AXD_CR) * 2;
+              const int rowoff = g.nx * (wrapi(j0 - 5 + r, g.n2) + 3);
+              for (int v = 0; v < 2; ++v) {
+                const int ii = i0 - 8 + c0 + v;
+                if (ii >= i0 - 5 && ii <= ilast) cp_async1(dst + e * AXD_NT * 2 + v, src + (wrapi(ii, g.n1) + 3) + rowoff);
+              }
+            }
+          }
+          if (MODE != 0 && act) cp_async16(pring + (size_t)(t % AXD_R) * AXD_PP + pq, d1 + zo + own);
+        }
+      }
+      cp_commit();
+    };
+    __syncthreads();  // the ring and the z weights of the previous tile are no longer read
+#pragma unroll
+    for (int gi = 0; gi < AXD_G - 1; ++gi) stage_group(gi);
+    double2 win[AXD_ZW];
+    const double2 zero2 = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int l = 0; l < AXD_ZW; ++l) win[l] = act ? ldg2d(x + zoff(k0 - 5 + l) + own) : zero2;
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+    const long long obase = (long long)(k0 + 3) * nxy + own;
+    const int nsteps = (nk + AXD_B - 1) / AXD_B;
+    for (int s = 0; s < nsteps; ++s) {
+      const int tb = s * AXD_B;
+      cp_wait<AXD_G - 2>();
+      __syncthreads();  // everybody's copies of the step's group (and the z weights) are visible
+      stage_group(s + AXD_G - 1);
+      double2 nw[AXD_B];
+      const bool more = act && tb + AXD_B < nk;
+#pragma unroll
+      for (int u = 0; u < AXD_B; ++u) nw[u] = more ? ldg2d(x + zoff(k0 + tb + AXD_B + 5 + u) + own) : zero2;
+#pragma unroll
+      for (int u = 0; u < AXD_B; ++u) {
+        const int t = tb + u;
+        if (t < nk) {
+          const double* sp = ring + (size_t)(t % AXD_R) * AXD_PLANE;
+          const double* wz = wzs[t];
+          double xv[14];  // the thread's row, columns cx-6 .. cx+7 (own at 6, 7)
+#pragma unroll
+          for (int m = 0; m < 7; ++m) {
+            const double2 v = lds2d(sp + (ty + 5) * AXD_W + cx - 6 + 2 * m);
+            xv[2 * m] = v.x;
+            xv[2 * m + 1] = v.y;
+          }
+          const double wyz = __dadd_rn(wy[5], wz[5]);
+          const double2 cc = win[u + 5];
+          double r0 = mulT(__dadd_rn(wx0[5], wyz), cc.x), r1 = mulT(__dadd_rn(wx1[5], wyz), cc.y);
+#pragma unroll
+          for (int l = 0; l < AXW; ++l) {
+            if (l == 5) continue;
+            r0 = fmaT(wx0[l], xv[1 + l], r0);
+            r1 = fmaT(wx1[l], xv[2 + l], r1);
+          }
+          double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+          for (int l = 0; l < AXW; ++l) {
+            if (l == 5) continue;
+            const double2 v = lds2d(sp + (ty + l) * AXD_W + cx);
+            y0 = fmaT(wy[l], v.x, y0);
+            y1 = fmaT(wy[l], v.y, y1);
+          }
+          double z0 = 0.0, z1 = 0.0;
+#pragma unroll
+          for (int l = 0; l < AXW; ++l) {
+            if (l == 5) continue;
+            const double w = wz[l];
+            z0 = fmaT(w, win[u + l].x, z0);
+            z1 = fmaT(w, win[u + l].y, z1);
+          }
+          r0 = __dadd_rn(__dadd_rn(r0, y0), z0);
+          r1 = __dadd_rn(__dadd_rn(r1, y1), z1);
+          if (act) {
+            const long long o = obase + (long long)t * nxy;
+            if (MODE == 3) {
+              const double2 bv = lds2d(pring + (size_t)(t % AXD_R) * AXD_PP + pq);
+              const double e0 = bv.x - r0, e1 = bv.y - r1;
+              *reinterpret_cast<float2*>(J.r32 + o) = make_float2((float)e0, (float)e1);
+              v0 = fmax(v0, fmax(fabs(e0), fabs(e1)));
+              v1 += e0 * e0;
+              v1 += e1 * e1;
+              v2 += bv.x * bv.x;
+              v2 += bv.y * bv.y;
+            } else {
+              double* out = MODE == 0 ? J.rr : (MODE == 1 ? J.Ap : J.Ar);
+              *reinterpret_cast<double2*>(out + o) = make_double2(r0, r1);
+              if (MODE != 0) {
+                const double2 pv = lds2d(pring + (size_t)(t % AXD_R) * AXD_PP + pq);
+                v0 += r0 * pv.x;
+                v0 += r1 * pv.y;
+              }
+              if (MODE == 2) {
+                v1 += r0 * r0;
+                v1 += r1 * r1;
+              }
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int l = 0; l < AXD_ZW - AXD_B; ++l) win[l] = win[l + AXD_B];
+#pragma unroll
+      for (int u = 0; u < AXD_B; ++u) win[AXD_ZW - AXD_B + u] = nw[u];
+    }
+    cp_wait<0>();
+    if (MODE != 0) {
+      v0 = MODE == 3 ? e_wmax(v0) : e_wsum(v0);
+      v1 = e_wsum(v1);
+      v2 = e_wsum(v2);
+      if ((tid & 31) == 0) {
+        red[0][tid >> 5] = v0;
+        red[1][tid >> 5] = v1;
+        red[2][tid >> 5] = v2;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+        for (int w = 0; w < AXD_NT / 32; ++w) {
+          s0 = MODE == 3 ? fmax(s0, red[0][w]) : s0 + red[0][w];
+          s1 += red[1][w];
+          s2 += red[2][w];
+        }
+        partial[(long long)b * 4] = s0;
+        if (MODE >= 2) partial[(long long)b * 4 + 1] = s1;
+        if (MODE == 3) partial[(long long)b * 4 + 2] = s2;
+      }
+    }
+  }
+}
+
 // bv - a0 w - a2 e - b0 s - b2 n - cm zm - cp zp
 template <typename T>
 __device__ __forceinline__ T jres(T bv, T a0, T w, T a2, T e, T b0, T s, T b2, T n, T cm, T zm, T cp, T zp) {
@@ -2417,6 +2642,10 @@ void ax_attributes() {
   cudaFuncSetAttribute(k_kr_ax32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axa_smem_bytes());
   cudaFuncSetAttribute(k_kr_ax32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axa_smem_bytes());
   cudaFuncSetAttribute(k_kr_ax32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axa_smem_bytes());
+  cudaFuncSetAttribute(k_kr_ax64v<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axd_smem_bytes());
+  cudaFuncSetAttribute(k_kr_ax64v<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axd_smem_bytes());
+  cudaFuncSetAttribute(k_kr_ax64v<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axd_smem_bytes());
+  cudaFuncSetAttribute(k_kr_ax64v<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axd_smem_bytes());
   cudaFuncSetAttribute(k_kr_ax32v<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axv_smem_bytes());
   cudaFuncSetAttribute(k_kr_ax32v<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axv_smem_bytes());
   cudaFuncSetAttribute(k_kr_ax32v<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axv_smem_bytes());
@@ -2462,8 +2691,9 @@ void launch_ax(int grid, const KrylovJob<T>* J, const int* ts, int n, int ntiles
     if (vec != 1) k_kr_ax32<MODE><<<grid, kAxBlock, axa_smem_bytes(), s>>>(J, ts, n, ntiles, partial);
     if (vec == 2) prof::count(1);  // two launches where the callers count one
   } else {
-    (void)vec;
-    k_kr_ax<T, MODE><<<grid, kAxBlock, ax_smem_bytes<T>(), s>>>(J, ts, n, ntiles, partial);
+    if (vec != 0) k_kr_ax64v<MODE><<<grid, dim3(AXD_TX, ETY), axd_smem_bytes(), s>>>(J, ts, n, ntiles, partial);
+    if (vec != 1) k_kr_ax<T, MODE><<<grid, kAxBlock, ax_smem_bytes<T>(), s>>>(J, ts, n, ntiles, partial);
+    if (vec == 2) prof::count(1);
   }
 }
 // the fused smoothing kernel runs one block per tile (one block per SM at a time)
@@ -2641,16 +2871,17 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
       J.sc = scal_ + c;
       kt[c] = tiles_of(C.g, kc);
     }
-    // the FP32 operator's vector kernel takes the jobs whose grids have n1 % 4 == 0 (16-byte
-    // vectors of 4 x points), 16-byte aligned fields and uniform x and z weights (it keeps one row
-    // of each); the others stay with the staged kernel.  The choice is per job, so a case's
-    // result does not depend on the other cases of its batch.
+    // the vector kernels take the jobs whose rows hold whole 16-byte vectors and whose fields are
+    // 16-byte aligned: FP32 (k_kr_ax32v) n1 % 4 == 0 with uniform x and z weights (it keeps one row
+    // of each), FP64 (k_kr_ax64v, per-row weights) n1 % 2 == 0; the others stay with the staged
+    // kernels.  The choice is per job, so a case's result does not depend on the other cases of
+    // its batch.
     int nv = 0;
     for (auto& J : kj) {
       const void* f[] = {J.phi, J.z1, J.z2, J.rr, J.Ap, J.Ar, J.rh};
       bool al = true;
       for (const void* q : f) al = al && (reinterpret_cast<uintptr_t>(q) & 15) == 0;
-      J.vec = std::is_same<T, float>::value && J.g.n1 % 4 == 0 && J.xuni && J.zuni && al;
+      J.vec = std::is_same<T, float>::value ? (J.g.n1 % 4 == 0 && J.xuni && J.zuni && al) : (J.g.n1 % 2 == 0 && al);
       nv += J.vec;
     }
     kr_vec_ = nv == 0 ? 0 : (nv == n ? 1 : 2);
@@ -3295,6 +3526,8 @@ int MixedEngine::build(const std::vector<Case>& cs, const EngineParams& p, cudaS
     A.rr = C.r64;
     A.r32 = C.r32;
     A.sc = oscal_ + c;
+    A.vec = C.g.n1 % 2 == 0 && (reinterpret_cast<uintptr_t>(C.x) & 15) == 0 &&
+            (reinterpret_cast<uintptr_t>(C.bb) & 15) == 0 && (reinterpret_cast<uintptr_t>(C.r32) & 7) == 0;
     MixJob& M = mj[c];
     M = MixJob{};
     M.g = C.g;
@@ -3307,6 +3540,11 @@ int MixedEngine::build(const std::vector<Case>& cs, const EngineParams& p, cudaS
     M.q = q_ + 4 * c;
     M.isc = inner_.scal_dev() + c;
     t[c] = tiles_of(C.g, kc);
+  }
+  {
+    int nv = 0;
+    for (const auto& A : aj) nv += A.vec;
+    ax_vec_ = nv == 0 ? 0 : (nv == n ? 1 : 2);
   }
   ax_list_ = arena_.add(aj, t);
   mix_list_ = arena_.add(mj, t);
@@ -3361,8 +3599,7 @@ int MixedEngine::solve(const std::vector<SolverScalars>& outer, double inner_tol
     if (rc) return rc;
     // r = b - A x in FP64 (the reference operator), stored as the FP32 right-hand side of the
     // inner solve, with its norms
-    IMPACT_PROF(prof::K_MX_RESID, 20.0 * cells, s_,
-                (k_kr_ax<double, 3><<<grid, kAxBlock, ax_smem_bytes<double>(), s_>>>(AJ, AL.ts, n, AL.ntiles, partial_)));
+    IMPACT_PROF(prof::K_MX_RESID, 20.0 * cells, s_, (launch_ax<double, 3>(grid, AJ, AL.ts, n, AL.ntiles, partial_, s_, ax_vec_)));
     k_efin<<<n, 256, 0, s_>>>(AL.ts, partial_, 3, 1, EFIN_RAW, nullptr, q_);
     prof::count(1);
     cudaError_t e = cudaMemcpyAsync(q_host_, q_, (size_t)n * 4 * sizeof(double), cudaMemcpyDeviceToHost, s_);

@@ -248,6 +248,7 @@ class MixedEngine {
   bool built_ = false;
   ListArena arena_;
   int ax_list_ = -1, mix_list_ = -1;
+  int ax_vec_ = 0;  // outer residual jobs in the FP64 vector kernel: 0 none, 1 all, 2 some
   double* partial_ = nullptr;
   double* q_ = nullptr;       // device, 4 per case
   double* q_host_ = nullptr;  // pinned

@@ -404,9 +404,9 @@ __global__ void __launch_bounds__(1024) k_b_reduce(const ExJob* __restrict__ job
   if (only_lp && !J.sc->level_pressure) return;
   reduce_partials_block(J.partial, (long long)J.gx * J.gy * J.gz, is_max, out ? out + blockIdx.x : J.dscal + slot);
 }
-__global__ void __launch_bounds__(NT) k_b_interp(const ExJob* __restrict__ jobs, int nj) {
+__global__ void __launch_bounds__(NT) k_b_interp(const ExJob* __restrict__ jobs, int nj, int f32) {
   EX_BLOCK
-  if (J.work32[0])
+  if (f32)
     interp_vel3_block<float>(g, J.c, J.vel[0], J.vel[1], J.vel[2], J.work32[0], J.work32[1], J.work32[2], bx, by, bz);
   else
     interp_vel3_block<double>(g, J.c, J.vel[0], J.vel[1], J.vel[2], J.work[0], J.work[1], J.work[2], bx, by, bz);
@@ -1335,7 +1335,7 @@ static void substep_rhs(CaseState& s, const impact_b200_step_params* p, double d
   const double multL = 1.0 / p->Re;
   const double mb = dt * bRK[sub], ma = dt * aRK[sub];
   const int use_old = sub != 0;
-  if (s.precision == 1) {  // FP32 rhs_vel pass: FP32 work fields and nonlinear term
+  if (s.precision == 1 && p->explicit_fp32) {  // FP32 rhs_vel pass: FP32 work fields and nonlinear term
     k_interp_vel3_32<<<gr, bl, 0, st>>>(g, s.c64, vel[0], vel[1], vel[2], s.work32[0], s.work32[1], s.work32[2]);
     prof::count(1);
     // bytes: vel 8 (the staged tile and the point), work 3 x 4, nl 4 (+4 old), rhs 8
@@ -1704,9 +1704,9 @@ extern "C" int impact_b200_batch_step(impact_b200_batch* b, const impact_b200_st
     IMPACT_CUDA_CHECK(cudaMemcpyAsync(b->d_sc, b->h_sc, n * sizeof(StepScal), cudaMemcpyHostToDevice, bs));
     for (int sub = 0; sub < 3; ++sub) {
       // rhs_vel and the pressure equation's right-hand side of every case, one launch per kernel
-      k_b_interp<<<b->ex_blocks, bl, 0, bs>>>(EJ, n);
+      const int f32 = b->precision == 1 && p[0].explicit_fp32;
+      k_b_interp<<<b->ex_blocks, bl, 0, bs>>>(EJ, n, f32);
       prof::count(1);
-      const int f32 = b->precision == 1;
       for (int m = 0; m < 3; ++m)
         IMPACT_PROF(prof::K_NL_RHS, (f32 ? (sub != 0 ? 36.0 : 32.0) : (sub != 0 ? 56.0 : 48.0)) * cells, bs,
                     launch_rhs_march_batch(m, b->d_rhs, n, b->rhs_blocks, sub, f32, bs));

@@ -63,7 +63,7 @@ class SolverResult(C.Structure):
 class StepParams(C.Structure):
     _fields_ = [("Re", C.c_double), ("CFL", C.c_double), ("dtime_max", C.c_double),
                 ("dtime0", C.c_double), ("U0", C.c_double), ("T_pulse", C.c_double),
-                ("level_pressure", C.c_int), ("poisson", SolverParams)]
+                ("level_pressure", C.c_int), ("poisson", SolverParams), ("explicit_fp32", C.c_int)]
 
 
 class StepState(C.Structure):
@@ -245,8 +245,10 @@ def solver_params(tol_rel=1e-8, tol_abs_inf=0.0, max_it=2000, n_sweeps=4, omega=
 
 
 def step_params(Re=200.0, CFL=0.2, dtime_max=1e-2, dtime0=1e9, U0=1.0, T_pulse=1.0, level_pressure=1,
-                **solver) -> StepParams:
-    return StepParams(Re, CFL, dtime_max, dtime0, U0, T_pulse, level_pressure, solver_params(**solver))
+                explicit_fp32=0, **solver) -> StepParams:
+    """explicit_fp32 (mixed-precision cases): rhs_vel as the FP32 pass instead of the FP64 one."""
+    return StepParams(Re, CFL, dtime_max, dtime0, U0, T_pulse, level_pressure, solver_params(**solver),
+                      int(explicit_fp32))
 
 
 class Case:

@@ -314,6 +314,11 @@ typedef struct {
   double U0, T_pulse;                /* inflow u_z = U0 (1 + 0.5 sin(2 pi t / T)) on label 5 */
   int level_pressure;                /* subtract the mean pressure after each step */
   impact_b200_solver_params poisson;
+  /* mixed-precision cases only: 1 = rhs_vel (advection, Helmholtz, the RK update's nonlinear
+   * terms) as the FP32 pass -- FP32 interpolated velocities, nonlinear term, coefficients and
+   * accumulation, the velocity and rhs FP64; 0 (default) = the FP64 pass.  No counterpart in the
+   * reference. */
+  int explicit_fp32;
 } impact_b200_step_params;
 
 typedef struct {

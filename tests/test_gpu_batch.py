@@ -18,25 +18,25 @@ SPECS = [((17, 17, 33), 200.0, 1.0, [(1.0, 0.5, 0.125)]),
          ((23, 21, 41), 300.0, 0.9, [])]
 
 
-def _make(spec, precision):
+def _make(spec, precision, explicit_fp32=0):
     N, Re, U0, sten = spec
     g = I.Grid(N, (1.0, 1.0, 2.0))
     case = I.Case(g, precision=precision)
     case.set_labels(G.straight_vessel(g, stenoses=sten))
     p = I.step_params(Re=Re, U0=U0, tol_rel=1e-8, n_sweeps=4, omega=0.8, precond=1,
-                      max_it=200 if precision == 0 else 30, inner_tol_rel=1e-3)
+                      max_it=200 if precision == 0 else 30, inner_tol_rel=1e-3, explicit_fp32=explicit_fp32)
     return case, p
 
 
-@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
-def test_batch_equals_alone(precision):
+@pytest.mark.parametrize("precision,explicit_fp32", [(0, 0), (1, 0), (1, 1)], ids=["fp64", "mixed", "mixed-fp32-rhs"])
+def test_batch_equals_alone(precision, explicit_fp32):
     nsteps = 2
     alone = []
     for spec in SPECS:
-        case, p = _make(spec, precision)
+        case, p = _make(spec, precision, explicit_fp32)
         case.step(p, nsteps)
         alone.append((case, [case.download(f) for f in ("vel1", "vel2", "vel3", "pre")], case.state.dtime))
-    made = [_make(spec, precision) for spec in SPECS]
+    made = [_make(spec, precision, explicit_fp32) for spec in SPECS]
     batch = I.Batch([c for c, _ in made])
     for _ in range(nsteps):
         batch.step([p for _, p in made])

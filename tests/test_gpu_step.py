@@ -3,9 +3,10 @@
 Vessel geometry of the plain-step workload (straight cylinder, radius 0.25 L1, inflow buffer
 label 5 and outlet label 9), reduced to a grid the oracle finishes in seconds.  Bars: time step
 equal to 1e-12 in FP64; velocity within 1e-6 of max|u| (FP64 and mixed precision); Poisson
-iteration counts within 3 of the oracle's.  The mixed-precision step evaluates advection and
-Helmholtz in FP32 (the FP32 rhs_vel pass), so its velocity -- and the CFL time step computed from
-it -- carry FP32 rounding: its time step is held to the velocity's 1e-6 bar.
+iteration counts within 3 of the oracle's.  The mixed-precision step with explicit_fp32 = 1
+evaluates advection and Helmholtz in FP32 (the FP32 rhs_vel pass), so its velocity -- and the
+CFL time step computed from it -- carry FP32 rounding: the mixed step's time step is held to the
+velocity's 1e-6 bar.
 """
 import numpy as np
 import pytest
@@ -18,7 +19,7 @@ from _util import rel_err
 pytestmark = pytest.mark.gpu
 
 
-def _run(precision, nsteps=3, N=(33, 33, 65), L=(1.0, 1.0, 2.0), Re=200.0, precond=0):
+def _run(precision, nsteps=3, N=(33, 33, 65), L=(1.0, 1.0, 2.0), Re=200.0, precond=0, explicit_fp32=0):
     og, ig = O.Grid(N, L), I.Grid(N, L)
     lab = G.straight_vessel(ig, stenoses=[(1.0, 0.6, 0.125)])
     mg = og.multigrid() if precond == 1 else None
@@ -34,7 +35,7 @@ def _run(precision, nsteps=3, N=(33, 33, 65), L=(1.0, 1.0, 2.0), Re=200.0, preco
     case = I.Case(ig, precision=precision)
     case.set_labels(lab)
     sp = I.step_params(Re=Re, tol_rel=1e-8, n_sweeps=4, omega=0.8, max_it=2000 if precision == 0 else 30,
-                       precond=precond, inner_tol_rel=1e-3)
+                       precond=precond, inner_tol_rel=1e-3, explicit_fp32=explicit_fp32)
     dh = []
     for _ in range(nsteps):
         s = case.step(sp)
@@ -58,9 +59,10 @@ def test_step_fp64_matches_oracle(precond):
     assert np.abs(d).max() <= 1e-6 * np.abs(og.interior(pre)).max()
 
 
+@pytest.mark.parametrize("explicit_fp32", [0, 1], ids=["fp64-rhs", "fp32-rhs"])
 @pytest.mark.parametrize("precond", [0, 1], ids=["jor4", "multigrid"])
-def test_step_mixed_matches_oracle(precond):
-    og, vel, pre, hist, case, got, dh = _run(1, precond=precond)
+def test_step_mixed_matches_oracle(precond, explicit_fp32):
+    og, vel, pre, hist, case, got, dh = _run(1, precond=precond, explicit_fp32=explicit_fp32)
     for (dt_o, _), (dt_g, _, stat) in zip(hist, dh):
         assert abs(dt_g - dt_o) <= 1e-6 * dt_o
         assert all(s == 0 for s in stat)
