@@ -1043,14 +1043,15 @@ __global__ void __launch_bounds__(AXNT, 3) k_kr_ax32(const KrylovJob<float>* __r
 //
 // A block of 8 x 8 threads owns one 32 x 8-column tile over kc planes.  Each plane of the tile
 // with its 5-wide halo is staged by 16-byte cp.async into a ring of AXV_R slots (48 x 18 floats:
-// columns i0-8 .. i0+39, rows j0-5 .. j0+12; chunks that would need periodic images are staged
-// element by element, on a separate branch that only threads at the box edges take), together
-// with the plane's inner-product partners (the tile's 32 x 8 points).  x neighbours come from the
-// thread's row of the slot (5 vectors), y neighbours from the 10 other rows (one vector each).
-// The z values k-5 .. k+AXV_B+4 of the 4 points stay in a register window of vectors moved on by
-// AXV_B planes per step; the window's new planes are 16-byte loads from global memory issued one
-// step ahead.  The ring holds three groups of AXV_B planes: a step computes on one while the
-// next two are in flight.
+// columns i0-8 .. i0+39, rows j0-5 .. j0+12; at the box ends each chunk from its periodic image),
+// together with the plane's inner-product partners (the tile's 32 x 8 points).  x neighbours come
+// from the thread's row of the slot (5 vectors), y neighbours from the 10 other rows (one vector
+// each).  The z values k-5 .. k+AXV_B+4 of the 4 points stay in a register window of vectors
+// moved on by AXV_B planes per step; the window's new planes are 16-byte loads from global
+// memory issued one step ahead.  The arithmetic runs on packed FP32 pairs (fma.rn.f32x2: two
+// IEEE fmas per instruction), the per-plane inner-product terms are summed in FP32 and added
+// in FP64.  The ring holds two groups of AXV_B planes: a step computes on one while the
+// next is in flight (35.8 KB of shared memory and 166 registers: 6 blocks per SM).
 constexpr int AXV_TX = ETX / 4, AXV_NT = AXV_TX * ETY;   // 8 x 8 threads, 4 columns each
 constexpr int AXV_HX = 8;                                // staged columns left of the tile
 constexpr int AXV_W = ETX + 16;                          // staged row: 8 + 32 + 8 (5 needed each side)
@@ -1061,7 +1062,7 @@ constexpr int AXV_PER = (AXV_NCH + AXV_NT - 1) / AXV_NT; // chunks per thread an
 constexpr int AXV_PLANE = AXV_W * AXV_H;                 // floats per slot
 constexpr int AXV_PP = ETX * ETY;                        // partner floats per slot
 constexpr int AXV_B = 4;                                 // planes per step
-constexpr int AXV_G = 3;                                 // groups of AXV_B planes in the ring
+constexpr int AXV_G = 2;                                 // groups of AXV_B planes in the ring
 constexpr int AXV_R = AXV_B * AXV_G;                     // ring slots
 constexpr int AXV_ZW = AXV_B + 10;                       // z window (planes t-5 .. t+AXV_B+4)
 static_assert((AXV_PLANE * 4) % 16 == 0 && (AXV_PP * 4) % 16 == 0, "slots must keep 16-byte alignment");
@@ -1071,7 +1072,7 @@ __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpre
 __device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 
 template <int MODE>
-__global__ void __launch_bounds__(AXV_NT, 4) k_kr_ax32v(const KrylovJob<float>* __restrict__ jobs,
+__global__ void __launch_bounds__(AXV_NT, 5) k_kr_ax32v(const KrylovJob<float>* __restrict__ jobs,
                                                         const int* __restrict__ ts, int nj, int ntiles,
                                                         double* __restrict__ partial) {
   static_assert(MODE >= 0 && MODE <= 2, "FP32 operator modes: 0 residual, 1 alpha, 2 omega");
@@ -1114,20 +1115,19 @@ __global__ void __launch_bounds__(AXV_NT, 4) k_kr_ax32v(const KrylovJob<float>* 
     const float wc = __fadd_rn(__fadd_rn(wx[5], wy[5]), wz[5]);
     // this thread's chunks of a staged plane: chunk cq = tid + e*AXV_NT holds columns
     // i0-8+4(cq%12) .. +3 of row j0-5+cq/12.  The points of the tile read columns
-    // i0-5 .. min(i0+31, n1)+5 and rows j0-5 .. min(j0+7, n2)+5.  In a tile whose needed columns
-    // are all interior (1..n1) every needed chunk is one 16-byte copy (cb[e] = its in-plane
-    // offset, -1 for a chunk nothing needs); the tiles at the x ends of the box take the element
-    // path, which copies the needed columns one by one from their periodic images.
+    // i0-5 .. min(i0+31, n1)+5 and rows j0-5 .. min(j0+7, n2)+5; cb[e] is the chunk's in-plane
+    // offset, -1 for a chunk nothing needs.  A chunk starts at a column = 1 (mod 4) and n1 % 4 == 0,
+    // so a chunk outside 1..n1 lies whole in one periodic image (n1 >= 8): every chunk, at the box
+    // ends too, is one 16-byte copy from its image.
     const int ilast = min(i0 + ETX - 1, g.n1) + 5, jlast = min(j0 + ETY - 1, g.n2) + 5;
-    const bool tile_vec = i0 - 5 >= 1 && ilast <= g.n1;  // block-uniform
     int cb[AXV_PER];
 #pragma unroll
     for (int e = 0; e < AXV_PER; ++e) {
       const int cq = tid + e * AXV_NT;
       const int r = cq / AXV_CR, c0 = (cq % AXV_CR) * 4;
       const int jj = j0 - 5 + r, ii = i0 - AXV_HX + c0;
-      const bool need = cq < AXV_NCH && jj <= jlast && max(ii, i0 - 5) <= min(ii + 3, ilast);
-      cb[e] = need ? (ii + 3) + g.nx * (wrapi(jj, g.n2) + 3) : -1;
+      const bool need = cq < AXV_NCH && jj <= jlast && ii + 3 >= i0 - 5 && ii <= ilast;
+      cb[e] = need ? (wrapi(ii, g.n1) + 3) + g.nx * (wrapi(jj, g.n2) + 3) : -1;
     }
     const int own = (act ? i + 3 : 4) + g.nx * (jr + 3);  // in-plane offset of the thread's vector
     auto zoff = [&](int k) -> long long {  // plane k (periodic) + 3 ghost planes
@@ -1143,23 +1143,9 @@ __global__ void __launch_bounds__(AXV_NT, 4) k_kr_ax32v(const KrylovJob<float>* 
           const long long zo = zoff(k0 + t);
           const float* src = x + zo;
           float* dst = ring + (size_t)(t % AXV_R) * AXV_PLANE + tid * 4;
-          if (tile_vec) {
 #pragma unroll
-            for (int e = 0; e < AXV_PER; ++e)
-              if (cb[e] >= 0) cp_async16(dst + e * AXV_NT * 4, src + cb[e]);
-          } else {
-            for (int e = 0; e < AXV_PER; ++e) {
-              const int cq = tid + e * AXV_NT;
-              const int r = cq / AXV_CR, c0 = (cq % AXV_CR) * 4;
-              const int jj = j0 - 5 + r;
-              if (cb[e] < 0) continue;  // nothing of this chunk is needed
-              const int rowoff = g.nx * (wrapi(jj, g.n2) + 3);
-              for (int v = 0; v < 4; ++v) {
-                const int ii = i0 - AXV_HX + c0 + v;
-                if (ii >= i0 - 5 && ii <= ilast) cp_async1(dst + e * AXV_NT * 4 + v, src + (wrapi(ii, g.n1) + 3) + rowoff);
-              }
-            }
-          }
+          for (int e = 0; e < AXV_PER; ++e)
+            if (cb[e] >= 0) cp_async16(dst + e * AXV_NT * 4, src + cb[e]);
           if (MODE != 0 && act) cp_async16(pring + (size_t)(t % AXV_R) * AXV_PP + pq, d1 + zo + own);
         }
       }
@@ -1201,55 +1187,56 @@ __global__ void __launch_bounds__(AXV_NT, 4) k_kr_ax32v(const KrylovJob<float>* 
             xv[4 * m + 2] = v.z;
             xv[4 * m + 3] = v.w;
           }
+          // packed FP32 pairs (points 0,1 and 2,3; each lane one IEEE fma, the order of the
+          // scalar chains): center, x (odd offsets from the aligned pairs of the row, even ones
+          // per lane), y and z, then (x + y) + z
           const float4 cc = win[u + 5];
-          float r0 = mulT(wc, cc.x), r1 = mulT(wc, cc.y), r2 = mulT(wc, cc.z), r3 = mulT(wc, cc.w);
+          float2 a01 = __fmul2_rn(make_float2(wc, wc), make_float2(cc.x, cc.y));
+          float2 a23 = __fmul2_rn(make_float2(wc, wc), make_float2(cc.z, cc.w));
 #pragma unroll
           for (int l = 0; l < AXW; ++l) {
             if (l == 5) continue;
-            r0 = fmaT(wx[l], xv[3 + l], r0);
-            r1 = fmaT(wx[l], xv[4 + l], r1);
-            r2 = fmaT(wx[l], xv[5 + l], r2);
-            r3 = fmaT(wx[l], xv[6 + l], r3);
+            if (l & 1) {
+              const float2 w2 = make_float2(wx[l], wx[l]);
+              a01 = __ffma2_rn(w2, make_float2(xv[3 + l], xv[4 + l]), a01);
+              a23 = __ffma2_rn(w2, make_float2(xv[5 + l], xv[6 + l]), a23);
+            } else {
+              a01.x = fmaT(wx[l], xv[3 + l], a01.x);
+              a01.y = fmaT(wx[l], xv[4 + l], a01.y);
+              a23.x = fmaT(wx[l], xv[5 + l], a23.x);
+              a23.y = fmaT(wx[l], xv[6 + l], a23.y);
+            }
           }
-          // y: rows ty .. ty+10 of the slot (ty+5 is the thread's own)
-          float y0 = 0.f, y1 = 0.f, y2 = 0.f, y3 = 0.f;
+          float2 y01 = make_float2(0.f, 0.f), y23 = make_float2(0.f, 0.f);
 #pragma unroll
           for (int l = 0; l < AXW; ++l) {
             if (l == 5) continue;
             const float4 v = lds4(sp + (ty + l) * AXV_W + cx);
-            y0 = fmaT(wy[l], v.x, y0);
-            y1 = fmaT(wy[l], v.y, y1);
-            y2 = fmaT(wy[l], v.z, y2);
-            y3 = fmaT(wy[l], v.w, y3);
+            const float2 w2 = make_float2(wy[l], wy[l]);
+            y01 = __ffma2_rn(w2, make_float2(v.x, v.y), y01);
+            y23 = __ffma2_rn(w2, make_float2(v.z, v.w), y23);
           }
-          // z: the window
-          float z0 = 0.f, z1 = 0.f, z2 = 0.f, z3 = 0.f;
+          float2 z01 = make_float2(0.f, 0.f), z23 = make_float2(0.f, 0.f);
 #pragma unroll
           for (int l = 0; l < AXW; ++l) {
             if (l == 5) continue;
-            z0 = fmaT(wz[l], win[u + l].x, z0);
-            z1 = fmaT(wz[l], win[u + l].y, z1);
-            z2 = fmaT(wz[l], win[u + l].z, z2);
-            z3 = fmaT(wz[l], win[u + l].w, z3);
+            const float2 w2 = make_float2(wz[l], wz[l]);
+            z01 = __ffma2_rn(w2, make_float2(win[u + l].x, win[u + l].y), z01);
+            z23 = __ffma2_rn(w2, make_float2(win[u + l].z, win[u + l].w), z23);
           }
-          r0 = __fadd_rn(__fadd_rn(r0, y0), z0);
-          r1 = __fadd_rn(__fadd_rn(r1, y1), z1);
-          r2 = __fadd_rn(__fadd_rn(r2, y2), z2);
-          r3 = __fadd_rn(__fadd_rn(r3, y3), z3);
+          a01 = __fadd2_rn(__fadd2_rn(a01, y01), z01);
+          a23 = __fadd2_rn(__fadd2_rn(a23, y23), z23);
           if (act) {
-            *reinterpret_cast<float4*>(o) = make_float4(r0, r1, r2, r3);
+            *reinterpret_cast<float4*>(o) = make_float4(a01.x, a01.y, a23.x, a23.y);
+            // the plane's 4 products summed in FP32, the sum added in FP64
             if (MODE != 0) {
               const float4 pv = lds4(pring + (size_t)(t % AXV_R) * AXV_PP + pq);
-              v0 += (double)r0 * (double)pv.x;
-              v0 += (double)r1 * (double)pv.y;
-              v0 += (double)r2 * (double)pv.z;
-              v0 += (double)r3 * (double)pv.w;
+              const float2 d = __ffma2_rn(a23, make_float2(pv.z, pv.w), __fmul2_rn(a01, make_float2(pv.x, pv.y)));
+              v0 += (double)__fadd_rn(d.x, d.y);
             }
             if (MODE == 2) {
-              v1 += (double)r0 * (double)r0;
-              v1 += (double)r1 * (double)r1;
-              v1 += (double)r2 * (double)r2;
-              v1 += (double)r3 * (double)r3;
+              const float2 d = __ffma2_rn(a23, a23, __fmul2_rn(a01, a01));
+              v1 += (double)__fadd_rn(d.x, d.y);
             }
           }
           o += nxy;
@@ -1287,9 +1274,9 @@ __global__ void __launch_bounds__(AXV_NT, 4) k_kr_ax32v(const KrylovJob<float>* 
 // ------------------------------------------------------------------------------------------
 // The FP64 operator (the Krylov list of an FP64 solve, and the outer residual of the mixed
 // solve) on grids with n1 divisible by 2: the collapsed 11-point product_div_grad with every
-// thread owning one 16-byte vector of 2 consecutive x points of one row.  Same staging, ring and
-// z window as k_kr_ax32v (16 x 8 threads per 32 x 8-column tile, 48 x 18 staged doubles per
-// plane, 3 groups of 4 planes, the window k-5 .. k+8 in registers); the weights are the per-row
+// thread owning one 16-byte vector of 2 consecutive x points of one row.  The staging and z
+// window of k_kr_ax32v (16 x 8 threads per 32 x 8-column tile, 48 x 18 staged doubles per plane,
+// a ring of 2 groups of 4 planes, the window k-5 .. k+8 in registers); the weights are the per-row
 // weights of every axis (the FP64 operator defines the residual): x rows of the thread's two
 // columns and the y row of its row in registers, the z rows of the tile's planes in shared memory.
 //   MODE 0: rr = A phi;  1: Ap = A z1, partial rh.Ap;  2: Ar = A z2, partials Ar.rr, Ar.Ar;
@@ -1301,7 +1288,7 @@ constexpr int AXD_NCH = AXD_CR * AXD_H;
 constexpr int AXD_PER = (AXD_NCH + AXD_NT - 1) / AXD_NT;
 constexpr int AXD_PLANE = AXD_W * AXD_H;
 constexpr int AXD_PP = ETX * ETY;
-constexpr int AXD_B = 4, AXD_G = 3, AXD_R = AXD_B * AXD_G, AXD_ZW = AXD_B + 10;
+constexpr int AXD_B = 4, AXD_G = 2, AXD_R = AXD_B * AXD_G, AXD_ZW = AXD_B + 10;
 constexpr size_t axd_smem_bytes() {
   return sizeof(double) * ((size_t)AXD_R * (AXD_PLANE + AXD_PP) + (size_t)KC_MAX * AXW);
 }
@@ -1348,15 +1335,16 @@ __global__ void __launch_bounds__(AXD_NT, 2) k_kr_ax64v(const KrylovJob<double>*
     }
     for (int t = tid; t < nk * AXW; t += AXD_NT) wzs[t / AXW][t % AXW] = __ldg(J.W[2] + (size_t)(k0 - 1) * AXW + t);
     const int ilast = min(i0 + ETX - 1, g.n1) + 5, jlast = min(j0 + ETY - 1, g.n2) + 5;
-    const bool tile_vec = i0 - 5 >= 1 && ilast <= g.n1;  // block-uniform
+    // a chunk starts at an odd column and n1 is even, so a chunk outside 1..n1 lies whole in one
+    // periodic image (n1 >= 8): every chunk is one 16-byte copy from its image
     int cb[AXD_PER];
 #pragma unroll
     for (int e = 0; e < AXD_PER; ++e) {
       const int cq = tid + e * AXD_NT;
       const int r = cq / AXD_CR, c0 = (cq % AXD_CR) * 2;
       const int jj = j0 - 5 + r, ii = i0 - 8 + c0;
-      const bool need = cq < AXD_NCH && jj <= jlast && max(ii, i0 - 5) <= min(ii + 1, ilast);
-      cb[e] = need ? (ii + 3) + g.nx * (wrapi(jj, g.n2) + 3) : -1;
+      const bool need = cq < AXD_NCH && jj <= jlast && ii + 1 >= i0 - 5 && ii <= ilast;
+      cb[e] = need ? (wrapi(ii, g.n1) + 3) + g.nx * (wrapi(jj, g.n2) + 3) : -1;
     }
     const int own = (act ? i + 3 : 4) + g.nx * (jr + 3);
     auto zoff = [&](int k) -> long long {
@@ -1370,22 +1358,9 @@ __global__ void __launch_bounds__(AXD_NT, 2) k_kr_ax64v(const KrylovJob<double>*
           const long long zo = zoff(k0 + t);
           const double* src = x + zo;
           double* dst = ring + (size_t)(t % AXD_R) * AXD_PLANE + tid * 2;
-          if (tile_vec) {
 #pragma unroll
-            for (int e = 0; e < AXD_PER; ++e)
-              if (cb[e] >= 0) cp_async16(dst + e * AXD_NT * 2, src + cb[e]);
-          } else {
-            for (int e = 0; e < AXD_PER; ++e) {
-              if (cb[e] < 0) continue;
-              const int cq = tid + e * AXD_NT;
-              const int r = cq / AXD_CR, c0 = (cq % AXD_CR) * 2;
-              const int rowoff = g.nx * (wrapi(j0 - 5 + r, g.n2) + 3);
-              for (int v = 0; v < 2; ++v) {
-                const int ii = i0 - 8 + c0 + v;
-                if (ii >= i0 - 5 && ii <= ilast) cp_async1(dst + e * AXD_NT * 2 + v, src + (wrapi(ii, g.n1) + 3) + rowoff);
-              }
-            }
-          }
+          for (int e = 0; e < AXD_PER; ++e)
+            if (cb[e] >= 0) cp_async16(dst + e * AXD_NT * 2, src + cb[e]);
           if (MODE != 0 && act) cp_async16(pring + (size_t)(t % AXD_R) * AXD_PP + pq, d1 + zo + own);
         }
       }
@@ -2287,6 +2262,21 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
     const T zcm = cz[0], zcc = cz[1], zcp = cz[2];  // the z row of a uniform z axis
 #pragma unroll
     for (int c = 0; c < V; ++c) inv[c] = zu ? omega / (a1[c] + b1 + zcc) : T(0);
+    // FP32 fast path: the point operations on packed pairs (columns 0,1 and 2,3; fma.rn.f32x2
+    // and mul.rn.f32x2 lanes are the scalar operations, so the iterate is the same bit for bit)
+    constexpr bool PAIRS = FAST && sizeof(T) == 4;
+    float2 pna0[2], pna2[2], pa0[2], pa2[2], pinv[2], pdg[2];
+    if constexpr (PAIRS) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        pa0[h] = make_float2(a0[2 * h], a0[2 * h + 1]);
+        pa2[h] = make_float2(a2[2 * h], a2[2 * h + 1]);
+        pna0[h] = make_float2(-a0[2 * h], -a0[2 * h + 1]);
+        pna2[h] = make_float2(-a2[2 * h], -a2[2 * h + 1]);
+        pinv[h] = make_float2(inv[2 * h], inv[2 * h + 1]);
+        pdg[h] = make_float2(a1[2 * h] + b1 + zcc, a1[2 * h + 1] + b1 + zcc);
+      }
+    }
     // outputs of this thread: columns i = io + c of row jo, when its vector lies in the tile interior
     const int io = i0 + x0 - HX, jo = j0 + y - S;
     const bool rowout = y >= S && y < H0 - S && jo <= g.n2;
@@ -2367,17 +2357,56 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
             sload(pr + e0 + W0, no);
             sload(br + (qs % NBR) * R0 + e0, bv);
             T rv[V];
+            if constexpr (PAIRS) {
+              // jres / jsweep / jresid of columns 2h, 2h+1 (fast path: z uniform, cc = zcc)
 #pragma unroll
-            for (int c = 0; c < V; ++c) {
-              const T zm = Qz[s - 1][c][sm1], zc = Qz[s - 1][c][s0], zp = Qz[s - 1][c][sp1];
-              const T w = c == 0 ? wl : Qz[s - 1][c - 1][s0];
-              const T ea = c == V - 1 ? er : Qz[s - 1][c + 1][s0];
-              if (RES && s == S) {
-                rv[c] = jresid(bv[c], a0[c], w, a2[c], ea, b0, so[c], b2, no[c], cm, zm, cp, zp, a1[c] + b1 + cc, zc);
-                ov[c] = zc;
-              } else {
-                const T rr = jres(bv[c], a0[c], w, a2[c], ea, b0, so[c], b2, no[c], cm, zm, cp, zp);
-                ov[c] = jsweep(rr, zc, omega, zu, inv[c], a1[c] + b1 + cc);
+              for (int h = 0; h < 2; ++h) {
+                const int c = 2 * h;
+                const float2 zm = make_float2(Qz[s - 1][c][sm1], Qz[s - 1][c + 1][sm1]);
+                const float2 zc = make_float2(Qz[s - 1][c][s0], Qz[s - 1][c + 1][s0]);
+                const float2 zp = make_float2(Qz[s - 1][c][sp1], Qz[s - 1][c + 1][sp1]);
+                const float2 w = make_float2(c == 0 ? wl : Qz[s - 1][c - 1][s0], Qz[s - 1][c][s0]);
+                const float2 ea = make_float2(Qz[s - 1][c + 1][s0], c + 1 == V - 1 ? er : Qz[s - 1][c + 2][s0]);
+                const float2 bb2 = make_float2(bv[c], bv[c + 1]);
+                const float2 so2 = make_float2(so[c], so[c + 1]), no2 = make_float2(no[c], no[c + 1]);
+                if (RES && s == S) {
+                  float2 l = __fmul2_rn(pa0[h], w);
+                  l = __ffma2_rn(pa2[h], ea, l);
+                  l = __ffma2_rn(make_float2(b0, b0), so2, l);
+                  l = __ffma2_rn(make_float2(b2, b2), no2, l);
+                  l = __ffma2_rn(make_float2(cm, cm), zm, l);
+                  l = __ffma2_rn(make_float2(cp, cp), zp, l);
+                  l = __ffma2_rn(pdg[h], zc, l);
+                  const float2 r = __ffma2_rn(make_float2(-1.f, -1.f), l, bb2);  // bv - l
+                  rv[c] = r.x;
+                  rv[c + 1] = r.y;
+                  ov[c] = zc.x;
+                  ov[c + 1] = zc.y;
+                } else {
+                  float2 r = __ffma2_rn(pna0[h], w, bb2);
+                  r = __ffma2_rn(pna2[h], ea, r);
+                  r = __ffma2_rn(make_float2(-b0, -b0), so2, r);
+                  r = __ffma2_rn(make_float2(-b2, -b2), no2, r);
+                  r = __ffma2_rn(make_float2(-cm, -cm), zm, r);
+                  r = __ffma2_rn(make_float2(-cp, -cp), zp, r);
+                  const float2 o = __ffma2_rn(make_float2(1.f - omega, 1.f - omega), zc, __fmul2_rn(r, pinv[h]));
+                  ov[c] = o.x;
+                  ov[c + 1] = o.y;
+                }
+              }
+            } else {
+#pragma unroll
+              for (int c = 0; c < V; ++c) {
+                const T zm = Qz[s - 1][c][sm1], zc = Qz[s - 1][c][s0], zp = Qz[s - 1][c][sp1];
+                const T w = c == 0 ? wl : Qz[s - 1][c - 1][s0];
+                const T ea = c == V - 1 ? er : Qz[s - 1][c + 1][s0];
+                if (RES && s == S) {
+                  rv[c] = jresid(bv[c], a0[c], w, a2[c], ea, b0, so[c], b2, no[c], cm, zm, cp, zp, a1[c] + b1 + cc, zc);
+                  ov[c] = zc;
+                } else {
+                  const T rr = jres(bv[c], a0[c], w, a2[c], ea, b0, so[c], b2, no[c], cm, zm, cp, zp);
+                  ov[c] = jsweep(rr, zc, omega, zu, inv[c], a1[c] + b1 + cc);
+                }
               }
             }
             if (s == S && rowout) {  // the outputs: B = the last sweep (or x_NSW), C = the residual
@@ -2628,6 +2657,9 @@ __global__ void __launch_bounds__(ENT) k_mx_apply(const MixJob* __restrict__ job
   }
 }
 
+// grids of the vector operator kernels: the blocks resident at once on the device (a grid-stride
+// kernel given more would leave its last blocks to run after the others, one tile step behind)
+int g_axv_grid = 0, g_axd_grid = 0;
 // the operator kernels use more than 48 KB of dynamic shared memory: opt in once per process
 // and device
 void ax_attributes() {
@@ -2649,6 +2681,18 @@ void ax_attributes() {
   cudaFuncSetAttribute(k_kr_ax32v<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axv_smem_bytes());
   cudaFuncSetAttribute(k_kr_ax32v<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axv_smem_bytes());
   cudaFuncSetAttribute(k_kr_ax32v<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)axv_smem_bytes());
+  auto occ = [](auto kernel, int threads, size_t smem) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem) != cudaSuccess || nb < 1) nb = 1;
+    return nb;
+  };
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (nsm <= 0) nsm = 148;
+  g_axv_grid = nsm * std::min({occ(k_kr_ax32v<0>, AXV_NT, axv_smem_bytes()), occ(k_kr_ax32v<1>, AXV_NT, axv_smem_bytes()),
+                               occ(k_kr_ax32v<2>, AXV_NT, axv_smem_bytes())});
+  g_axd_grid = nsm * std::min({occ(k_kr_ax64v<0>, AXD_NT, axd_smem_bytes()), occ(k_kr_ax64v<1>, AXD_NT, axd_smem_bytes()),
+                               occ(k_kr_ax64v<2>, AXD_NT, axd_smem_bytes()), occ(k_kr_ax64v<3>, AXD_NT, axd_smem_bytes())});
   cudaFuncSetAttribute(k_lv_tail<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_BYTES);
   cudaFuncSetAttribute(k_lv_tail<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_BYTES);
 #define IMPACT_MULTI_ATTR(T, N, I, R)                                                                           \
@@ -2681,17 +2725,19 @@ inline int grid_for(int ntiles) {
 }
 const dim3 kBlock(ETX, ETY);
 const dim3 kAxBlock(ETX, AXTY);  // k_kr_ax: two rows per thread
-// the operator over a Krylov list: FP32 by the vector kernel where every job qualifies (vec:
-// n1 divisible by 4, uniform x and z weights), else by the 16-byte staged, stepped kernel
+// the operator over a Krylov list: FP32 by the vector kernel for the jobs that qualify (vec:
+// 1 all, 2 some), by the 16-byte staged, stepped kernel for the others; FP64 alike
 template <typename T, int MODE>
 void launch_ax(int grid, const KrylovJob<T>* J, const int* ts, int n, int ntiles, double* partial, cudaStream_t s,
                int vec) {
   if constexpr (std::is_same<T, float>::value && MODE <= 2) {
-    if (vec != 0) k_kr_ax32v<MODE><<<grid, dim3(AXV_TX, ETY), axv_smem_bytes(), s>>>(J, ts, n, ntiles, partial);
+    const int gv = g_axv_grid > 0 ? std::min(g_axv_grid, ntiles) : grid;
+    if (vec != 0) k_kr_ax32v<MODE><<<gv, dim3(AXV_TX, ETY), axv_smem_bytes(), s>>>(J, ts, n, ntiles, partial);
     if (vec != 1) k_kr_ax32<MODE><<<grid, kAxBlock, axa_smem_bytes(), s>>>(J, ts, n, ntiles, partial);
     if (vec == 2) prof::count(1);  // two launches where the callers count one
   } else {
-    if (vec != 0) k_kr_ax64v<MODE><<<grid, dim3(AXD_TX, ETY), axd_smem_bytes(), s>>>(J, ts, n, ntiles, partial);
+    const int gv = g_axd_grid > 0 ? std::min(g_axd_grid, ntiles) : grid;
+    if (vec != 0) k_kr_ax64v<MODE><<<gv, dim3(AXD_TX, ETY), axd_smem_bytes(), s>>>(J, ts, n, ntiles, partial);
     if (vec != 1) k_kr_ax<T, MODE><<<grid, kAxBlock, ax_smem_bytes<T>(), s>>>(J, ts, n, ntiles, partial);
     if (vec == 2) prof::count(1);
   }
@@ -2872,16 +2918,17 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
       kt[c] = tiles_of(C.g, kc);
     }
     // the vector kernels take the jobs whose rows hold whole 16-byte vectors and whose fields are
-    // 16-byte aligned: FP32 (k_kr_ax32v) n1 % 4 == 0 with uniform x and z weights (it keeps one row
-    // of each), FP64 (k_kr_ax64v, per-row weights) n1 % 2 == 0; the others stay with the staged
-    // kernels.  The choice is per job, so a case's result does not depend on the other cases of
-    // its batch.
+    // 16-byte aligned: FP32 (k_kr_ax32v) n1 % 4 == 0, n1 >= 8, with uniform x and z weights (it
+    // keeps one row of each), FP64 (k_kr_ax64v, per-row weights) n1 % 2 == 0, n1 >= 8; the others
+    // stay with the staged kernels.  The choice is per job, so a case's result does not depend on
+    // the other cases of its batch.
     int nv = 0;
     for (auto& J : kj) {
       const void* f[] = {J.phi, J.z1, J.z2, J.rr, J.Ap, J.Ar, J.rh};
       bool al = true;
       for (const void* q : f) al = al && (reinterpret_cast<uintptr_t>(q) & 15) == 0;
-      J.vec = std::is_same<T, float>::value ? (J.g.n1 % 4 == 0 && J.xuni && J.zuni && al) : (J.g.n1 % 2 == 0 && al);
+      J.vec = std::is_same<T, float>::value ? (J.g.n1 % 4 == 0 && J.g.n1 >= 8 && J.xuni && J.zuni && al)
+                                             : (J.g.n1 % 2 == 0 && J.g.n1 >= 8 && al);
       nv += J.vec;
     }
     kr_vec_ = nv == 0 ? 0 : (nv == n ? 1 : 2);
@@ -3526,7 +3573,7 @@ int MixedEngine::build(const std::vector<Case>& cs, const EngineParams& p, cudaS
     A.rr = C.r64;
     A.r32 = C.r32;
     A.sc = oscal_ + c;
-    A.vec = C.g.n1 % 2 == 0 && (reinterpret_cast<uintptr_t>(C.x) & 15) == 0 &&
+    A.vec = C.g.n1 % 2 == 0 && C.g.n1 >= 8 && (reinterpret_cast<uintptr_t>(C.x) & 15) == 0 &&
             (reinterpret_cast<uintptr_t>(C.bb) & 15) == 0 && (reinterpret_cast<uintptr_t>(C.r32) & 7) == 0;
     MixJob& M = mj[c];
     M = MixJob{};
