@@ -74,6 +74,9 @@ def parse():
     ap.add_argument("--copy-chunks", type=int, default=8,
                     help="element ranges per field of the end-to-end copies (download and next upload pipeline)")
     ap.add_argument("--no-profile", action="store_true", help="no per-kernel events in the timed steps (no roofline)")
+    ap.add_argument("--bottom-cheb", type=int, default=32,
+                    help="batch / serve: Chebyshev steps on the coarsest multigrid level (0: Jacobi "
+                         "sweeps, the reference's relax_bottom; the sequential FP64 arm always uses those)")
     ap.add_argument("--cases", type=int, default=48, help="batch: number of cases")
     ap.add_argument("--requests", type=int, default=16, help="serve: number of requests")
     ap.add_argument("--case-steps", type=int, default=0, help="batch / serve: time steps per case (0: the spec's)")
@@ -510,13 +513,14 @@ def batch_specs(n_cases, seed=7):
     return out
 
 
-def _case_params(spec, precision, args):
+def _case_params(spec, precision, args, bottom_cheb=None):
     import impact_b200 as I
     return I.step_params(Re=spec["Re"], CFL=0.2, dtime_max=1.0, dtime0=1e9, U0=spec["U0"], T_pulse=1.0,
                          level_pressure=1, tol_rel=1e-8, max_it=200 if precision == 0 else 40, omega=0.8,
                          init_yes=0, check_every=args.check_every, inner_tol_rel=args.inner_tol, inner_max_it=400,
                          precond=1, mg_down=args.sweeps, mg_up=args.sweeps, mg_bottom=args.sweeps,
-                         tile_kc=args.tile_kc)
+                         tile_kc=args.tile_kc,
+                         bottom_cheb=args.bottom_cheb if bottom_cheb is None else bottom_cheb)
 
 
 def _make_case(spec, precision, device, labels=None):
@@ -530,25 +534,19 @@ def _make_case(spec, precision, device, labels=None):
     return c
 
 
-def batch_bench(args, device, n_cases, steps):
-    """48 uneven cases x `steps` mixed-precision steps advanced as one batch, against the same
-    cases run one after another in plain FP64 (each case alone, the drop-in's way).  Device time
-    from CUDA events on the batch stream / on each case's stream; one untimed warm-up step."""
+def _batch_run(specs, cells, precision, steps, args, device, profile_steps=2):
+    """The cases of `specs` advanced `steps` steps as one batch at `precision` after one untimed
+    warm-up step: device time from CUDA events on the batch stream, no per-kernel events in the
+    timed steps; the per-kernel times come from `profile_steps` further steps."""
     import torch
 
     import impact_b200 as I
-    specs = batch_specs(n_cases)
-    cells = [s["n"] * s["n"] * 2 * s["n"] for s in specs]
-    out = {"workload": f"batched-vessels-{n_cases}", "cases": n_cases, "steps_per_case": steps,
-           "cells_total": sum(cells), "n_range": [min(s["n"] for s in specs), max(s["n"] for s in specs)]}
-    # mixed, batched
-    cases = [_make_case(s, 1, device) for s in specs]
-    params = [_case_params(s, 1, args) for s in specs]
+    cases = [_make_case(s, precision, device) for s in specs]
+    params = [_case_params(s, precision, args) for s in specs]
     batch = I.Batch(cases)
     batch.step(params, 1)
     stream = torch.cuda.ExternalStream(batch.stream, device=device)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    I.profile(True)
     launches0 = I.launch_count()
     e0.record(stream)
     for _ in range(steps):
@@ -556,23 +554,46 @@ def batch_bench(args, device, n_cases, steps):
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1)
+    launches = (I.launch_count() - launches0) / steps
+    I.profile(True)
+    for _ in range(profile_steps):
+        batch.step(params, 1)
     prof = I.profile_read()
     I.profile(False)
-    out["mixed_batched"] = {"value": round(sum(cells) * steps / (ms / 1e3) / 1e6, 3), "unit": UNIT,
-                            "ms_per_step": ms / steps, "launches_per_step": (I.launch_count() - launches0) / steps,
-                            "inner_iterations_per_substep_max": max(max(s.inner_iterations) for s in st),
-                            "status_ok": all(all(x == 0 for x in s.poisson_status) for s in st),
-                            "kernels_ms_per_step": {k: round(v[1] / steps, 2) for k, v in prof.items() if v[0] > 0}}
+    out = {"value": round(sum(cells) * steps / (ms / 1e3) / 1e6, 3), "unit": UNIT, "ms_per_step": ms / steps,
+           "launches_per_step": launches,
+           "iterations_per_substep_max": max(max(s.inner_iterations if precision else s.poisson_iterations) for s in st),
+           "status_ok": all(all(x == 0 for x in s.poisson_status) for s in st),
+           "kernels_ms_per_step": {k: round(v[1] / profile_steps, 2) for k, v in prof.items() if v[0] > 0},
+           "kernels_measured_over": f"{profile_steps} further steps with CUDA events around every launch"}
     batch.close()
     for c in cases:
         c.close()
     del cases
     torch.cuda.empty_cache()
+    return out
+
+
+def batch_bench(args, device, n_cases, steps):
+    """48 uneven cases x `steps` steps advanced as one batch in mixed precision and in plain FP64,
+    against the same cases run one after another in plain FP64 (each case alone, the drop-in's
+    way).  Device time from CUDA events on the batch stream / on each case's stream."""
+    import torch
+
+    import impact_b200 as I
+    specs = batch_specs(n_cases)
+    cells = [s["n"] * s["n"] * 2 * s["n"] for s in specs]
+    out = {"workload": f"batched-vessels-{n_cases}", "cases": n_cases, "steps_per_case": steps,
+           "cells_total": sum(cells), "n_range": [min(s["n"] for s in specs), max(s["n"] for s in specs)],
+           "bottom": (f"{args.bottom_cheb} Chebyshev steps on the coarsest level (batched arms)"
+                      if args.bottom_cheb > 0 else f"{args.sweeps} + {args.sweeps} Jacobi sweeps")}
+    out["mixed_batched"] = _batch_run(specs, cells, 1, steps, args, device)
+    out["fp64_batched"] = _batch_run(specs, cells, 0, steps, args, device)
     # plain FP64, one case after another
     total = 0.0
     for s in specs:
         c = _make_case(s, 0, device)
-        p = _case_params(s, 0, args)
+        p = _case_params(s, 0, args, bottom_cheb=0)
         c.step(p, 1)
         cs = torch.cuda.ExternalStream(c.stream, device=device)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -584,6 +605,7 @@ def batch_bench(args, device, n_cases, steps):
         c.close()
     out["fp64_sequential"] = {"value": round(sum(cells) * steps / (total / 1e3) / 1e6, 3), "unit": UNIT,
                               "ms_per_step": total / steps}
+    out["batched_mixed_over_batched_fp64"] = round(out["mixed_batched"]["value"] / out["fp64_batched"]["value"], 3)
     out["batched_mixed_over_sequential_fp64"] = round(out["mixed_batched"]["value"] / out["fp64_sequential"]["value"], 3)
     torch.cuda.empty_cache()
     return out
@@ -627,6 +649,8 @@ def serve_bench(args, device, n_req, steps, budget_gb=160.0, rate=20.0):
     stats.update({"workload": f"serving-{n_req}-requests", "arrival_rate_per_s": rate, "steps_per_case": steps,
                   "hbm_budget_gb": budget_gb, "peak_cases": srv.peak_cases, "peak_gb": round(srv.peak_bytes / 1e9, 2),
                   "batch_rebuilds": srv.batch_rebuilds, "rounds": srv.rounds,
+                  "bottom": (f"{args.bottom_cheb} Chebyshev steps on the coarsest level" if args.bottom_cheb > 0
+                             else f"{args.sweeps} + {args.sweeps} Jacobi sweeps"),
                   "host_seconds": {k: round(v, 3) for k, v in srv.seconds.items()},
                   "status_ok": all(all(x == 0 for x in d.status) for d in done),
                   "clock": "host wall clock of the request loop (latency = completion - arrival)"})

@@ -2460,11 +2460,22 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
 // smaller, whose one-launch-per-phase schedule is some 25 launches of a few microseconds each.
 // Every point sees the operations of the per-level kernels (jinit / jres / jsweep / jresid,
 // restrict7, pmix), so the V-cycle is the same bit for bit.
+// With cheb > 0 the coarsest level gets cheb steps of the Chebyshev semi-iteration of the
+// Jacobi-scaled operator D^-1 A (D = diag A) from x = 0 instead of its Jacobi sweeps, for the
+// eigenvalue interval [lmin, 2] (Gershgorin bounds D^-1 A by 2; lmin from the level's geometry):
+//   x_1 = x_0 + g z_0,  x_{k+1} = w_{k+1} (x_k + g z_k - x_{k-1}) + x_{k-1},  z_k = D^-1 (b - A x_k),
+//   g = 2 / (lmin + 2), s = (2 - lmin) / (2 + lmin), w_2 = 2 / (2 - s^2), w_{k+1} = 1 / (1 - s^2 w_k / 4)
+// (the Chebyshev semi-iterative method, Golub and Varga 1961): the error polynomial is the scaled
+// Chebyshev polynomial of degree cheb on the interval, bounded by 1 on [0, 2], so the smooth
+// modes that damped Jacobi removes in O(n^2) sweeps fall in O(n) steps, and the preconditioner
+// stays a fixed linear operator.  Such a tail may be the coarsest level alone.
 constexpr int TNT = 512;
-constexpr size_t TAIL_BYTES = 110 * 1024;
+constexpr size_t TAIL_BYTES = 200 * 1024;
 template <typename T>
 struct TailJob {
-  int nl;                          // levels in the tail (>= 2)
+  int nl;                          // levels in the tail (>= 2; >= 1 with cheb)
+  int cheb;                        // Chebyshev steps on the coarsest level (0: Jacobi sweeps)
+  T cgam, csig2;                   // their g and s^2
   LevelJob<T> lv[MG_MAX_LEVELS];   // their level jobs; lv[0].A / lv[0].B are the global fields
 };
 
@@ -2617,8 +2628,45 @@ __global__ void __launch_bounds__(TNT, 1) k_lv_tail(const TailJob<T>* __restrict
       relax(q, 2, X(q, cur[q]), X(q, cur[q] ^ 1));
       restrict_down(q);
     }
-    smooth(nl - 1, 1, n_bottom);  // relax_bottom
-    smooth(nl - 1, 0, n_bottom);
+    if (TJ.cheb > 0) {  // Chebyshev semi-iteration on the coarsest level, from x = 0
+      const int q = nl - 1;
+      const LevelJob<T>& J = TJ.lv[q];
+      const Geom& g = J.g;
+      const bool zu = J.zuni != 0;
+      const T* __restrict__ cz = J.cdg[2];
+      const T* a = Aq[q];
+      T* x0 = X0[q];
+      T* x1 = X1[q];
+      tail_cells(g, [&](int idx, int, int, int) { x0[idx] = T(0); x1[idx] = T(0); });
+      __syncthreads();
+      const T gam = TJ.cgam, s2 = TJ.csig2;
+      T w = T(1);
+      for (int it = 0; it < TJ.cheb; ++it) {
+        w = it == 0 ? T(1) : (it == 1 ? T(2) / (T(2) - s2) : T(1) / (T(1) - s2 * w / T(4)));
+        const T* src = X(q, cur[q]);
+        T* dst = X(q, cur[q] ^ 1);  // holds x_{k-1} (x_0 = 0 on the first step)
+        tail_cells(g, [&](int idx, int i, int j, int k) {
+          const T a0 = J.cdg[0][3 * (i - 1)], a1 = J.cdg[0][3 * (i - 1) + 1], a2 = J.cdg[0][3 * (i - 1) + 2];
+          const T b0 = J.cdg[1][3 * (j - 1)], b1 = J.cdg[1][3 * (j - 1) + 1], b2 = J.cdg[1][3 * (j - 1) + 2];
+          const T cm = zu ? cz[0] : cz[3 * (k - 1)], cc = zu ? cz[1] : cz[3 * (k - 1) + 1],
+                  cp = zu ? cz[2] : cz[3 * (k - 1) + 2];
+          const T diag = a1 + b1 + cc;
+          const int im = i == 1 ? idx + g.n1 - 1 : idx - 1, ip = i == g.n1 ? idx - g.n1 + 1 : idx + 1;
+          const int sy = g.n1, sz = g.n1 * g.n2;
+          const int jm = j == 1 ? idx + (g.n2 - 1) * sy : idx - sy, jp = j == g.n2 ? idx - (g.n2 - 1) * sy : idx + sy;
+          const int km = k == 1 ? idx + (g.n3 - 1) * sz : idx - sz, kp = k == g.n3 ? idx - (g.n3 - 1) * sz : idx + sz;
+          const T xk = src[idx];
+          const T r = jresid(a[idx], a0, src[im], a2, src[ip], b0, src[jm], b2, src[jp], cm, src[km], cp, src[kp], diag, xk);
+          const T xm = it == 0 ? xk : dst[idx];
+          dst[idx] = xm + w * (xk + gam * r / diag - xm);
+        });
+        cur[q] ^= 1;
+        __syncthreads();
+      }
+    } else {
+      smooth(nl - 1, 1, n_bottom);  // relax_bottom
+      smooth(nl - 1, 0, n_bottom);
+    }
     for (int q = nl - 2; q >= 0; --q) {  // interpolate_relax
       prolong_up(q);
       smooth(q, 0, n_up);
@@ -3061,7 +3109,8 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
   }
   // lt[c]: the first level of case c's coarse tail (k_lv_tail), the coarsest level from which
   // all levels' three fields fit in TAIL_BYTES; -1 without one (one-sweep schedule, no hierarchy,
-  // or fewer than two levels that fit).  Levels from lt[c] on leave the per-level lists.
+  // or fewer than two levels that fit -- one suffices with the Chebyshev bottom).  Levels from
+  // lt[c] on leave the per-level lists.
   std::vector<int> lt(n, -1);
   if (use_mg && p_.fuse && p_.mg_down >= 1 && p_.mg_bottom >= 1 && p_.mg_up >= 0) {
     for (int c = 0; c < n; ++c) {
@@ -3074,7 +3123,7 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
         if (bytes > (double)TAIL_BYTES) break;
         first = g;
       }
-      if (first >= 0 && nlev[c] - first >= 2) lt[c] = first;
+      if (first >= 0 && (nlev[c] - first >= 2 || p_.bottom_cheb > 0)) lt[c] = first;
     }
   }
   auto in_lists = [&](int c, int g) { return lt[c] < 0 || g < lt[c]; };
@@ -3110,6 +3159,13 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
           TailJob<T> job{};
           job.nl = nlev[c] - lt[c];
           for (int q = 0; q < job.nl; ++q) job.lv[q] = lvjob(c, lt[c] + q, v);
+          if (p_.bottom_cheb > 0) {
+            const double lo = std::max(1e-6, std::min(1.0, cs[c].mg->lv[nlev[c] - 1].lmin));
+            const double sg = (2.0 - lo) / (2.0 + lo);
+            job.cheb = p_.bottom_cheb;
+            job.cgam = (T)(2.0 / (2.0 + lo));
+            job.csig2 = (T)(sg * sg);
+          }
           tj.push_back(job);
           tt.push_back(1);
         }

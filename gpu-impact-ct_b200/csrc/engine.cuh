@@ -125,10 +125,11 @@ struct EngineParams {
   int kc = 16;       // z-planes per tile
   int use_graph = 1; // replay each chunk of iterations as a captured CUDA graph
   int fuse = 1;      // V-cycle smoothing phases as fused multi-sweep kernels
+  int bottom_cheb = 0;  // > 0: Chebyshev steps on a tail's coarsest level instead of Jacobi sweeps
   bool operator==(const EngineParams& o) const {
     return precond == o.precond && n_sweeps == o.n_sweeps && mg_down == o.mg_down && mg_up == o.mg_up &&
            mg_bottom == o.mg_bottom && omega == o.omega && check_every == o.check_every && kc == o.kc &&
-           use_graph == o.use_graph && fuse == o.fuse;
+           use_graph == o.use_graph && fuse == o.fuse && bottom_cheb == o.bottom_cheb;
   }
 };
 

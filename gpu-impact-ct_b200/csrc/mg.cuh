@@ -14,6 +14,7 @@ struct MGLevel {
   const T* cI[3];   // interpolation weights cI(1:2, 0:M) of the level
   int ratio[3];     // coarsening factor to the next level
   T *A, *B, *C;     // right-hand side, solution, work (levels >= 1)
+  double lmin = 0;  // estimate of the smallest nonzero eigenvalue of diag(cdg)^-1 cdg on this level
 };
 
 template <typename T>

@@ -549,6 +549,27 @@ static int rows_uniform(const double* t, size_t rows, int w) {
   return dev <= 1e-12 * mx ? 1 : 0;
 }
 
+// Estimate of the smallest nonzero eigenvalue of diag(A)^-1 A for the compact periodic Laplacian
+// A of one multigrid level (the Chebyshev bottom's lower bound): on an equidistant axis the
+// lowest mode exp(2 pi i x / L) of axis m gives w_m (1 - cos(2 pi / n_m)), w_m = the axis's share
+// of the diagonal; stretched axes use their mean centre weight.  Axes of one cell are skipped.
+static double level_lmin(const MGHostLevel& L) {
+  double c[3] = {0, 0, 0}, diag = 0;
+  for (int m = 0; m < 3; ++m) {
+    const int n = L.M[m] - 1;
+    for (int i = 0; i < n; ++i) c[m] += L.cdg[m][3 * i + 1];
+    c[m] /= n > 0 ? n : 1;
+    diag += c[m];
+  }
+  double lo = 2.0;
+  for (int m = 0; m < 3; ++m) {
+    const int n = L.M[m] - 1;
+    if (n < 2 || diag == 0.0) continue;
+    lo = std::min(lo, c[m] / diag * (1.0 - std::cos(2.0 * M_PI / n)));
+  }
+  return lo;
+}
+
 extern "C" int impact_b200_case_create(const impact_b200_case_desc* desc, const impact_b200_coeffs* co,
                                        impact_b200_case** out) {
   if (!desc || !co || !out) return impact_set_error_msg(-1, "impact_b200_case_create: null argument");
@@ -759,6 +780,7 @@ extern "C" int impact_b200_case_create(const impact_b200_case_desc* desc, const 
         a.ratio[m] = b.ratio[m] = lv[g].ratio[m];
       }
       a.zuni = b.zuni = rows_uniform(lv[g].cdg[2].data(), (size_t)(lv[g].M[2] - 1), 3);
+      a.lmin = b.lmin = level_lmin(lv[g]);
       a.A = a.B = a.C = nullptr;
       b.A = b.B = b.C = nullptr;
       if (g == 0) continue;
@@ -953,6 +975,7 @@ static EngineParams engine_params(const CaseState& s, const impact_b200_solver_p
   ep.kc = ep.kc < 1 ? 1 : (ep.kc > KC_MAX ? KC_MAX : ep.kc);
   ep.use_graph = std::getenv("IMPACT_B200_NO_GRAPH") ? 0 : 1;
   ep.fuse = p->smooth_unfused ? 0 : 1;
+  ep.bottom_cheb = p->bottom_cheb > 0 ? p->bottom_cheb : 0;
   (void)s;
   return ep;
 }

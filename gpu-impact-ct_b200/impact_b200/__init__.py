@@ -52,7 +52,7 @@ class SolverParams(C.Structure):
                 ("n_sweeps", C.c_int), ("omega", C.c_double), ("init_yes", C.c_int),
                 ("check_every", C.c_int), ("inner_tol_rel", C.c_double), ("inner_max_it", C.c_int),
                 ("precond", C.c_int), ("mg_down", C.c_int), ("mg_up", C.c_int), ("mg_bottom", C.c_int),
-                ("tile_kc", C.c_int), ("smooth_unfused", C.c_int)]
+                ("tile_kc", C.c_int), ("smooth_unfused", C.c_int), ("bottom_cheb", C.c_int)]
 
 
 class SolverResult(C.Structure):
@@ -236,12 +236,15 @@ class Grid:
 
 def solver_params(tol_rel=1e-8, tol_abs_inf=0.0, max_it=2000, n_sweeps=4, omega=0.8, init_yes=0,
                   check_every=4, inner_tol_rel=1e-3, inner_max_it=0, precond=0, mg_down=4, mg_up=4,
-                  mg_bottom=4, tile_kc=0, smooth_unfused=0) -> SolverParams:
+                  mg_bottom=4, tile_kc=0, smooth_unfused=0, bottom_cheb=0) -> SolverParams:
     """precond 0: n_sweeps damped-Jacobi sweeps; 1: multigrid V-cycle (mg_down/up/bottom sweeps).
     tile_kc: z-planes per tile of the solver kernels (0: library default).  smooth_unfused: 1 runs
-    every V-cycle sweep as its own launch instead of one fused kernel per smoothing phase."""
+    every V-cycle sweep as its own launch instead of one fused kernel per smoothing phase.
+    bottom_cheb: d > 0 replaces the coarsest level's Jacobi sweeps by d Chebyshev steps (fused
+    schedule, coarsest level within the one-block tail)."""
     return SolverParams(tol_rel, tol_abs_inf, max_it, n_sweeps, omega, init_yes, check_every,
-                        inner_tol_rel, inner_max_it, precond, mg_down, mg_up, mg_bottom, tile_kc, smooth_unfused)
+                        inner_tol_rel, inner_max_it, precond, mg_down, mg_up, mg_bottom, tile_kc, smooth_unfused,
+                        bottom_cheb)
 
 
 def step_params(Re=200.0, CFL=0.2, dtime_max=1e-2, dtime0=1e9, U0=1.0, T_pulse=1.0, level_pressure=1,

@@ -282,6 +282,13 @@ typedef struct {
                           restriction, the residual after them) run as one z-marching kernel;
                           1: one sweep per launch.  Same results bit for bit; no counterpart in
                           the reference */
+  int bottom_cheb;     /* 0 (default): the coarsest level of the V-cycle gets mg_bottom damped-Jacobi
+                          sweeps, then mg_bottom more (relax_bottom, mod_solvers.f90:420-450);
+                          d > 0: d steps of the Chebyshev semi-iteration of the Jacobi-scaled
+                          coarsest operator from x = 0 instead (a fixed polynomial in A, so the
+                          preconditioner stays linear), in the one-block coarse tail, on cases whose
+                          coarsest level fits there.  For hierarchies that stop at a large coarsest
+                          level (n = 8 x odd); no counterpart in the reference */
 } impact_b200_solver_params;
 
 typedef struct {
