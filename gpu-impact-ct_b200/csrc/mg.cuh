@@ -1,4 +1,5 @@
-// mg.cuh -- geometric multigrid V-cycle on the device (internal).
+// mg.cuh -- the multigrid hierarchy of a case on the device: per level its geometry, tables and
+// fields (the V-cycle itself runs in the engine, engine.cu).
 #pragma once
 #include "common.cuh"
 
@@ -24,10 +25,5 @@ struct MGData {
   int n_down = 4, n_up = 4, n_bottom = 4;
   double omega = 0.8;
 };
-
-// multigridV (mod_solvers.f90:456-585) with init_yes = .TRUE., gstart = 1: z = M v.
-// work0: one level-1 field; every kernel is a no-op once sc reports the solve as finished.
-template <typename T>
-void mg_vcycle(const MGData<T>& mg, const SolverScalars* sc, const T* v, T* z, T* work0, cudaStream_t s);
 
 }  // namespace impact

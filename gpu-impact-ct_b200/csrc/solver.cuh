@@ -1,22 +1,11 @@
-// solver.cuh -- device-resident pressure Poisson solvers (internal interface).
+// solver.cuh -- work-field sets of the Poisson solves and the library's stand-alone reduction
+// (internal interface).
 #pragma once
 #include "common.cuh"
 #include "kernels.cuh"
 #include "mg.cuh"
 
 namespace impact {
-
-struct SolverOpts {
-  double tol_rel;      // ||r||_2 <= tol_rel * ||b||_2   (0 = off)
-  double tol_abs_inf;  // ||r||_inf < tol_abs_inf        (0 = off; the reference's epsU)
-  int max_it;
-  int n_sweeps;        // Jacobi sweeps per preconditioner application (0 = no preconditioner)
-  double omega;        // relaxation of the preconditioner sweeps
-  int init_yes;        // start from phi = 0
-  int check_every;     // read the residual norm back to the host every this many iterations
-  int precond;         // 0: n_sweeps Jacobi sweeps (none if 0); 1: multigrid V-cycle (mg)
-  const void* mg;      // MGData<T>* of the field type when precond == 1
-};
 
 struct SolverResult {
   int iterations;
@@ -34,18 +23,8 @@ struct KrylovWork {
   SolverScalars* scal_host;  // pinned host mirror
 };
 
-template <typename T>
-long long krylov_partial_doubles(const Geom& g);
-
-// BiCGstab_orig (mod_solvers.f90:1509-1935), problem_type 2: A = product_div_grad,
-// preconditioner = n_sweeps damped-Jacobi sweeps of the compact Laplacian from zero
-// (the single-level multigridV, mod_solvers.f90:456-585 with n_grids = 1).
-template <typename T>
-int bicgstab(const Geom& g, const Coeffs<T>& c, const SolverOpts& o, const T* bb, T* phi, KrylovWork<T>& w,
-             cudaStream_t s, SolverResult* res);
-
-// Mixed precision: FP64 outer residual and correction, FP32 inner BiCGstab (fields, stencils,
-// Jacobi sweeps in FP32; inner products and norms accumulated in FP64).
+// Work fields of a mixed-precision solve: FP64 outer residual and correction around the FP32
+// inner Krylov set.
 struct MixedWork {
   double* r64;     // outer residual
   float* r32;      // inner right-hand side
@@ -55,15 +34,10 @@ struct MixedWork {
   SolverScalars* scal64;
   SolverScalars* scal64_host;
 };
-int mixed_solve(const Geom& g, const Coeffs<double>& c64, const Coeffs<float>& c32, const SolverOpts& outer,
-                const SolverOpts& inner, const double* bb, double* phi, MixedWork& w, cudaStream_t s,
-                SolverResult* res, int* inner_iterations);
-
-// helpers used by the step driver
+// deterministic inner product sum a.b over the unique points into *out_dev (solver.cu); partial
+// holds reduce_partial_doubles(g, 1) doubles
 template <typename T>
 void reduce_dot(const Geom& g, const T* a, const T* b, double* partial, double* out_dev, cudaStream_t s);
-template <typename T>
-void reduce_norms(const Geom& g, const T* a, double* partial, double* out_dev /*[inf, two_sq]*/, cudaStream_t s);
 long long reduce_partial_doubles(const Geom& g, int nq);
 
 }  // namespace impact

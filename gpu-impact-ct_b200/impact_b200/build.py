@@ -20,7 +20,7 @@ INCLUDE = os.path.join(os.path.dirname(ROOT), "include")
 OBJ = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libimpact_b200.so")
 
-SOURCES = ["kernels.cu", "stencil25d.cu", "mg.cu", "solver.cu", "engine.cu", "step.cu", "capi.cu", "prof.cu", "noalloc.cu", "rhs.cu", "ibm.cu", "march.cu", "coeffs.cpp"]
+SOURCES = ["kernels.cu", "stencil25d.cu", "solver.cu", "engine.cu", "step.cu", "capi.cu", "prof.cu", "noalloc.cu", "rhs.cu", "ibm.cu", "march.cu", "coeffs.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-I", CSRC, "-I", INCLUDE]
