@@ -2,16 +2,17 @@
 11-point stencils per axis) in FP64 and in FP32 (the mixed-precision solve's inner BiCGstab: FP32
 weights and arithmetic) against the oracle's FP64 gradient-then-divergence evaluation.
 
-The kernel stages its plane ring in 16-byte chunks where the padded rows are 16-byte aligned (nx
-a multiple of 4) and the chunk's points are interior, element by element from the periodic
-images elsewhere, and marches z four planes per step; the grids cover aligned rows with interior
-and wrapped chunks, unaligned rows (every chunk element-wise), ragged x / y tiles, tile depths
-that the step depth (four planes in FP32, two in FP64) does not divide, the smallest grid the
-library accepts and a stretched z axis (per-plane weights).  Bar: 1e-12 of max|A x| in FP64; 1e-5
-in FP32 (rounding of the input, the weights and 33 products per point; an indexing error is of
-order one).  FP32 grids with n1 divisible by 4 and uniform x and z spacing run the vector kernel
-(16x16x32, 100x41x26, 8x9x10, 64x56x102: one to several tiles along z, ragged last steps), the
-others the staged kernel.
+The staged kernels stage their plane ring in 16-byte chunks where the padded rows are 16-byte
+aligned (nx a multiple of 4) and the chunk's points are interior, element by element from the
+periodic images elsewhere; the vector kernels copy every chunk in 16 bytes, at the box ends from
+its periodic image (a tile of a narrow grid wraps at both ends).  The grids cover aligned rows
+with interior and wrapped chunks, unaligned rows (every chunk element-wise), ragged x / y tiles,
+tile depths that the step depth does not divide, the smallest grid the library accepts and a
+stretched z axis (per-plane weights).  Bar: 1e-12 of max|A x| in FP64; 1e-5 in FP32 (rounding of
+the input, the weights and 33 products per point; an indexing error is of order one).  FP32 grids
+with n1 divisible by 4 and uniform x and z spacing run the FP32 vector kernel (16x16x32,
+100x41x26, 8x9x10, 64x56x102: one to several tiles along z, ragged last steps), grids with n1 even
+the FP64 vector kernel, the others the staged kernels.
 """
 import numpy as np
 import pytest
