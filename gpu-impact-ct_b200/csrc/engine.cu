@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(AXNT, 2) k_kr_ax(const KrylovJob<T>* __restric
     const int q = find_job(ts, nj, b);
     const KrylovJob<T>& J = jobs[q];
     const SolverScalars* sc = J.sc;
-    if (MODE == 0 ? (sc->done != 0) : e_halted(sc)) continue;
+    if (J.vec || (MODE == 0 ? (sc->done != 0) : e_halted(sc))) continue;  // vector jobs: k_kr_ax64v
     const Geom g = J.g;
     const int ntx = (g.n1 + ETX - 1) / ETX, nty = (g.n2 + ETY - 1) / ETY;
     const int t0 = b - ts[q];

@@ -391,8 +391,8 @@ void launch_batch_m(const RhsJob* jobs, int nj, int blocks, int sub, cudaStream_
 
 }  // namespace
 
-void rhs_march_job_grid(const Geom& g, RhsJob& J) {
-  J.kz = rhs_march_kz(g);
+void rhs_march_job_grid(const Geom& g, RhsJob& J, int kz) {
+  J.kz = kz > 0 ? kz : rhs_march_kz(g);
   J.gx = (g.n1 + RTX - 1) / RTX;
   J.gy = (g.n2 + RTY - 1) / RTY;
   J.gz = (g.n3 + J.kz - 1) / J.kz;
@@ -416,13 +416,18 @@ void launch_rhs_march_batch(int m, const RhsJob* jobs, int nj, int blocks, int s
   }
 }
 
-// planes per block: enough blocks for several waves of two blocks per SM, at most 64 planes
-int rhs_march_kz(const Geom& g) {
-  const long long cols = (long long)((g.n1 + RTX - 1) / RTX) * ((g.n2 + RTY - 1) / RTY);
-  long long kz = (cols * g.n3) / (148LL * 2 * 8);
+// planes per block: enough blocks for several waves of two blocks per SM, at most 64 planes (a
+// block reads 6 planes beyond its own, so deeper blocks read less twice); column_planes = block
+// columns x planes of the grid, or of all grids of a batch, whose blocks run in one launch
+int rhs_march_kz_for(long long column_planes) {
+  long long kz = column_planes / (148LL * 2 * 8);
   kz = kz < 8 ? 8 : (kz > 64 ? 64 : kz);
   return (int)kz;
 }
+long long rhs_march_column_planes(const Geom& g) {
+  return (long long)((g.n1 + RTX - 1) / RTX) * ((g.n2 + RTY - 1) / RTY) * g.n3;
+}
+int rhs_march_kz(const Geom& g) { return rhs_march_kz_for(rhs_march_column_planes(g)); }
 
 void launch_rhs_march(int m, const Geom& g, const Coeffs<double>& c, double multL, double mult_b, double mult_a,
                       int use_old, const double* vel, const double* const work[3], double* nl, double* rhs,

@@ -34,7 +34,10 @@ struct RhsJob {
   int kz, gx, gy, gz, b0;
 };
 // kz, gx, gy, gz of a case of grid g (b0 and the rest are the caller's)
-void rhs_march_job_grid(const Geom& g, RhsJob& J);
+// kz: planes per block (0: the grid's own choice); a batch passes the choice for all its grids
+void rhs_march_job_grid(const Geom& g, RhsJob& J, int kz = 0);
+int rhs_march_kz_for(long long column_planes);
+long long rhs_march_column_planes(const Geom& g);
 // component m of every job in one launch of `blocks` blocks (the sum of the jobs' grids), RK
 // substep sub, FP64 or (f32) FP32 pass; job j's blocks start at jobs[j].b0 (increasing)
 void launch_rhs_march_batch(int m, const RhsJob* jobs, int nj, int blocks, int sub, int f32, cudaStream_t s);

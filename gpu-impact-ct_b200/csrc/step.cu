@@ -100,30 +100,6 @@ __device__ __forceinline__ bool block_interior(const Geom& g, int bx, int by, in
   if (i > g.n1 || j > g.n2) return;                          \
   const long long p = off(g, i, j, k);
 
-template <int LO, int CNT>
-__device__ __forceinline__ double st1(const double* __restrict__ c, const double* __restrict__ f, const Geom& g, int a,
-                                      int i, int j, int k, long long p) {
-  const int q = crd(a, i, j, k), n = ext(g, a);
-  const long long s = strd(g, a);
-  const long long base = p - (long long)q * s;  // offset with the axis coordinate at 0
-  const double* cr = c + (long long)q * CNT;
-  double v = cr[0] * __ldg(f + base + (long long)wrapi(q + LO, n) * s);
-#pragma unroll
-  for (int l = 1; l < CNT; ++l) v = v + cr[l] * __ldg(f + base + (long long)wrapi(q + LO + l, n) * s);
-  return v;
-}
-template <int LO, int CNT>
-__device__ __forceinline__ double st1_acc(double v, const double* __restrict__ c, const double* __restrict__ f,
-                                          const Geom& g, int a, int i, int j, int k, long long p) {
-  const int q = crd(a, i, j, k), n = ext(g, a);
-  const long long s = strd(g, a);
-  const long long base = p - (long long)q * s;
-  const double* cr = c + (long long)q * CNT;
-#pragma unroll
-  for (int l = 0; l < CNT; ++l) v = v + cr[l] * __ldg(f + base + (long long)wrapi(q + LO + l, n) * s);
-  return v;
-}
-
 // interpolate_vel (mod_diff.f90:1436-1472): work_m = I_{u_m -> p} vel_m, three components, in
 // FP64 from the FP64 velocity; TO = float stores the FP32 work fields of a mixed-precision case
 template <typename TO>
@@ -195,10 +171,18 @@ __global__ void __launch_bounds__(NT) k_project(Geom g, Coeffs<double> c, const 
 __device__ __forceinline__ void div2_block(const Geom& g, const Coeffs<double>& c, const double* __restrict__ u,
                                            const double* __restrict__ v, const double* __restrict__ w,
                                            double* __restrict__ div, int bx, int by, int bz) {
+  const bool wrap = !block_interior(g, bx, by, bz + 1);
   PTB(bx, by, bz)
-  double d = st1<D_LO, ND>(c.cD[0], u, g, 0, i, j, k, p);
-  d = st1_acc<D_LO, ND>(d, c.cD[1], v, g, 1, i, j, k, p);
-  d = st1_acc<D_LO, ND>(d, c.cD[2], w, g, 2, i, j, k, p);
+  double d;
+  if (wrap) {
+    d = st1w<D_LO, ND, true>(c.cD[0], u, g, 0, i, j, k, p);
+    d = st1w_acc<D_LO, ND, true>(d, c.cD[1], v, g, 1, i, j, k, p);
+    d = st1w_acc<D_LO, ND, true>(d, c.cD[2], w, g, 2, i, j, k, p);
+  } else {
+    d = st1w<D_LO, ND, false>(c.cD[0], u, g, 0, i, j, k, p);
+    d = st1w_acc<D_LO, ND, false>(d, c.cD[1], v, g, 1, i, j, k, p);
+    d = st1w_acc<D_LO, ND, false>(d, c.cD[2], w, g, 2, i, j, k, p);
+  }
   div[p] = d;
 }
 __global__ void __launch_bounds__(NT) k_div2(Geom g, Coeffs<double> c, const double* __restrict__ u,
@@ -206,6 +190,7 @@ __global__ void __launch_bounds__(NT) k_div2(Geom g, Coeffs<double> c, const dou
                                              double* __restrict__ div) {
   div2_block(g, c, u, v, w, div, blockIdx.x, blockIdx.y, blockIdx.z);
 }
+
 
 // get_dtime (mod_lib.f90:46-250), timeint_mode 1: block max of radius / stabilitylimit(angle)
 __constant__ double c_stab[41];
@@ -229,11 +214,19 @@ __device__ __forceinline__ void dtime_block(const Geom& g, const Coeffs<double>&
   const int j = by * BY + threadIdx.y + 1;
   const int k = bz + 1;
   double beta = 0.0;
+  const bool wrap = !block_interior(g, bx, by, k);
   if (i <= g.n1 && j <= g.n2) {
     const long long p = off(g, i, j, k);
-    const double w1 = st1<D_LO, ND>(c.cIup[0], u, g, 0, i, j, k, p);
-    const double w2 = st1<D_LO, ND>(c.cIup[1], v, g, 1, i, j, k, p);
-    const double w3 = st1<D_LO, ND>(c.cIup[2], w, g, 2, i, j, k, p);
+    double w1, w2, w3;
+    if (wrap) {
+      w1 = st1w<D_LO, ND, true>(c.cIup[0], u, g, 0, i, j, k, p);
+      w2 = st1w<D_LO, ND, true>(c.cIup[1], v, g, 1, i, j, k, p);
+      w3 = st1w<D_LO, ND, true>(c.cIup[2], w, g, 2, i, j, k, p);
+    } else {
+      w1 = st1w<D_LO, ND, false>(c.cIup[0], u, g, 0, i, j, k, p);
+      w2 = st1w<D_LO, ND, false>(c.cIup[1], v, g, 1, i, j, k, p);
+      w3 = st1w<D_LO, ND, false>(c.cIup[2], w, g, 2, i, j, k, p);
+    }
     double are = dr.spp[0][i] + dr.spp[1][j];
     are = are + dr.spp[2][k];
     are = are / Re;
@@ -349,8 +342,10 @@ __global__ void __launch_bounds__(NT) k_mask(Geom g, const uint8_t* __restrict__
 
 // ---------------------------------------------------------------------------------------
 // the explicit part of a batch step: one launch per kernel over all cases.  Block b of a
-// launch is block b - job.b0 of its case's grid3 grid (gx x gy x gz); every block runs the same
-// body as the single-case kernel, so a case's bits do not depend on the batch.
+// reduction launch is block b - job.b0 of its case's grid3 grid (gx x gy x gz), block b of a
+// point-kernel launch covers XPL planes of that grid from block b - job.pb0 on; every block runs
+// the body of the single-case kernel for each of its planes, so a case's bits do not depend on
+// the batch.
 // ---------------------------------------------------------------------------------------
 struct StepScal {  // per case and step: time step, Reynolds number, inflow at the step's end
   double dt, Re, u_in;
@@ -371,7 +366,8 @@ struct ExJob {
   double* partial;
   double* dscal;
   const StepScal* sc;  // this case's scalars of the current step
-  int gx, gy, gz, b0;
+  int gx, gy, gz, b0;  // grid3 blocks (one plane each) of the case, from block b0 on
+  int pb0;             // blocks of XPL planes (the point kernels), from block pb0 on
 };
 
 __device__ __forceinline__ int ex_job(const ExJob* __restrict__ jobs, int nj, int b) {
@@ -388,6 +384,24 @@ __device__ __forceinline__ int ex_job(const ExJob* __restrict__ jobs, int nj, in
   const int bx = lb % J.gx, by = (lb / J.gx) % J.gy, bz = lb / (J.gx * J.gy); \
   const Geom& g = J.g;                                                   \
   (void)g;
+// The point kernels (no reduction) give each block XPL planes of its 32 x 8 columns, so that the
+// search for the block's case and its set-up are paid once per XPL planes; the planes
+// bz = kb0 .. kb1-1 of the case's grid3 blocks.
+constexpr int XPL = 8;
+__device__ __forceinline__ int ex_pjob(const ExJob* __restrict__ jobs, int nj, int b) {
+  int lo = 0, hi = nj - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].pb0 <= b) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+#define EX_PBLOCK                                                        \
+  const ExJob& J = jobs[ex_pjob(jobs, nj, blockIdx.x)];                  \
+  const int lb = blockIdx.x - J.pb0;                                     \
+  const int bx = lb % J.gx, by = (lb / J.gx) % J.gy, bq = lb / (J.gx * J.gy); \
+  const int kb0 = bq * XPL, kb1 = min(J.gz, kb0 + XPL);                  \
+  const Geom& g = J.g;
 
 __constant__ double RKA_D[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
 __constant__ double RKB_D[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
@@ -405,27 +419,32 @@ __global__ void __launch_bounds__(1024) k_b_reduce(const ExJob* __restrict__ job
   reduce_partials_block(J.partial, (long long)J.gx * J.gy * J.gz, is_max, out ? out + blockIdx.x : J.dscal + slot);
 }
 __global__ void __launch_bounds__(NT) k_b_interp(const ExJob* __restrict__ jobs, int nj, int f32) {
-  EX_BLOCK
-  if (f32)
-    interp_vel3_block<float>(g, J.c, J.vel[0], J.vel[1], J.vel[2], J.work32[0], J.work32[1], J.work32[2], bx, by, bz);
-  else
-    interp_vel3_block<double>(g, J.c, J.vel[0], J.vel[1], J.vel[2], J.work[0], J.work[1], J.work[2], bx, by, bz);
+  EX_PBLOCK
+  for (int bz = kb0; bz < kb1; ++bz) {
+    if (f32)
+      interp_vel3_block<float>(g, J.c, J.vel[0], J.vel[1], J.vel[2], J.work32[0], J.work32[1], J.work32[2], bx, by,
+                               bz);
+    else
+      interp_vel3_block<double>(g, J.c, J.vel[0], J.vel[1], J.vel[2], J.work[0], J.work[1], J.work[2], bx, by, bz);
+  }
 }
 __global__ void __launch_bounds__(NT) k_b_scale_pre(const ExJob* __restrict__ jobs, int nj, int sub, int divide) {
-  EX_BLOCK
-  scale_pre_block(g, RKA_D[sub] + RKB_D[sub], J.sc->dt, divide, J.pre, bx, by, bz);
+  EX_PBLOCK
+  for (int bz = kb0; bz < kb1; ++bz) scale_pre_block(g, RKA_D[sub] + RKB_D[sub], J.sc->dt, divide, J.pre, bx, by, bz);
 }
 __global__ void __launch_bounds__(NT) k_b_div2(const ExJob* __restrict__ jobs, int nj) {
-  EX_BLOCK
-  div2_block(g, J.c, J.rhs[0], J.rhs[1], J.rhs[2], J.res, bx, by, bz);
+  EX_PBLOCK
+  for (int bz = kb0; bz < kb1; ++bz) div2_block(g, J.c, J.rhs[0], J.rhs[1], J.rhs[2], J.res, bx, by, bz);
 }
 __global__ void __launch_bounds__(NT) k_b_project(const ExJob* __restrict__ jobs, int nj) {
-  EX_BLOCK
-  project_block(g, J.c, J.pre, J.rhs[0], J.rhs[1], J.rhs[2], J.vel[0], J.vel[1], J.vel[2], bx, by, bz);
+  EX_PBLOCK
+  for (int bz = kb0; bz < kb1; ++bz)
+    project_block(g, J.c, J.pre, J.rhs[0], J.rhs[1], J.rhs[2], J.vel[0], J.vel[1], J.vel[2], bx, by, bz);
 }
 __global__ void __launch_bounds__(NT) k_b_mask(const ExJob* __restrict__ jobs, int nj) {
-  EX_BLOCK
-  mask_block(g, J.label, J.sc->u_in, J.sc->inflow_on, J.vel[0], J.vel[1], J.vel[2], bx, by, bz);
+  EX_PBLOCK
+  for (int bz = kb0; bz < kb1; ++bz)
+    mask_block(g, J.label, J.sc->u_in, J.sc->inflow_on, J.vel[0], J.vel[1], J.vel[2], bx, by, bz);
 }
 __global__ void __launch_bounds__(NT) k_b_sum(const ExJob* __restrict__ jobs, int nj) {
   EX_BLOCK
@@ -433,9 +452,9 @@ __global__ void __launch_bounds__(NT) k_b_sum(const ExJob* __restrict__ jobs, in
   sum_block(g, J.pre, J.partial, bx, by, bz, J.gx, J.gy);
 }
 __global__ void __launch_bounds__(NT) k_b_sub_mean(const ExJob* __restrict__ jobs, int nj) {
-  EX_BLOCK
+  EX_PBLOCK
   if (!J.sc->level_pressure) return;
-  sub_mean_block(g, J.dscal + 1, J.pre, bx, by, bz);
+  for (int bz = kb0; bz < kb1; ++bz) sub_mean_block(g, J.dscal + 1, J.pre, bx, by, bz);
 }
 
 }  // namespace impact
@@ -1495,7 +1514,7 @@ struct impact_b200_batch {
   StepScal* d_sc = nullptr;
   StepScal* h_sc = nullptr;  // pinned
   double* d_beta = nullptr;
-  int ex_blocks = 0, rhs_blocks = 0;
+  int ex_blocks = 0, ex_pblocks = 0, rhs_blocks = 0;  // grid3 blocks, XPL-plane blocks, rhs_vel blocks
 };
 
 extern "C" int impact_b200_batch_destroy(impact_b200_batch* b) {
@@ -1550,6 +1569,12 @@ static int batch_jobs(impact_b200_batch* b) {
   cudaError_t e = cudaMalloc((void**)&b->d_sc, n * sizeof(StepScal));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_sc, n * sizeof(StepScal));
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_beta, n * sizeof(double));
+  // the rhs_vel blocks of all cases run in one launch: their depth follows the batch's total
+  // (small cases alone would get shallow blocks that read their 6 halo planes again and again)
+  long long colpl = 0;
+  for (int c = 0; c < n; ++c) colpl += rhs_march_column_planes(b->cases[c]->s.g);
+  const int kz_batch = rhs_march_kz_for(colpl);
+  int pb = 0;
   for (int c = 0; c < n && e == cudaSuccess; ++c) {
     CaseState& s = b->cases[c]->s;
     ExJob& J = ex[c];
@@ -1576,6 +1601,8 @@ static int batch_jobs(impact_b200_batch* b) {
     J.gz = d.z;
     J.b0 = eb;
     eb += J.gx * J.gy * J.gz;
+    J.pb0 = pb;
+    pb += J.gx * J.gy * ((J.gz + XPL - 1) / XPL);
     RhsJob& R = rj[c];
     R = RhsJob{};
     R.g = s.g;
@@ -1591,7 +1618,7 @@ static int batch_jobs(impact_b200_batch* b) {
       R.nl32[m] = s.nl32[m];
       R.rhs[m] = J.rhs[m];
     }
-    rhs_march_job_grid(s.g, R);
+    rhs_march_job_grid(s.g, R, kz_batch);
     R.b0 = rb;
     rb += R.gx * R.gy * R.gz;
   }
@@ -1605,6 +1632,7 @@ static int batch_jobs(impact_b200_batch* b) {
     return impact_set_error(e, "batch job lists", __FILE__, __LINE__);
   }
   b->ex_blocks = eb;
+  b->ex_pblocks = pb;
   b->rhs_blocks = rb;
   return 0;
 }
@@ -1728,7 +1756,7 @@ extern "C" int impact_b200_batch_step(impact_b200_batch* b, const impact_b200_st
     for (int sub = 0; sub < 3; ++sub) {
       // rhs_vel and the pressure equation's right-hand side of every case, one launch per kernel
       const int f32 = b->precision == 1 && p[0].explicit_fp32;
-      k_b_interp<<<b->ex_blocks, bl, 0, bs>>>(EJ, n, f32);
+      k_b_interp<<<b->ex_pblocks, bl, 0, bs>>>(EJ, n, f32);
       prof::count(1);
       for (int m = 0; m < 3; ++m)
         IMPACT_PROF(prof::K_NL_RHS, (f32 ? (sub != 0 ? 36.0 : 32.0) : (sub != 0 ? 56.0 : 48.0)) * cells, bs,
@@ -1738,9 +1766,9 @@ extern "C" int impact_b200_batch_step(impact_b200_batch* b, const impact_b200_st
           IMPACT_CUDA_CHECK(cudaStreamWaitEvent(bs, c->s.pre_wait, 0));
           c->s.pre_wait = nullptr;
         }
-      k_b_scale_pre<<<b->ex_blocks, bl, 0, bs>>>(EJ, n, sub, 0);
+      k_b_scale_pre<<<b->ex_pblocks, bl, 0, bs>>>(EJ, n, sub, 0);
       prof::count(1);
-      IMPACT_PROF(prof::K_DIV2, 4.0 * 8.0 * cells, bs, (k_b_div2<<<b->ex_blocks, bl, 0, bs>>>(EJ, n)));
+      IMPACT_PROF(prof::K_DIV2, 4.0 * 8.0 * cells, bs, (k_b_div2<<<b->ex_pblocks, bl, 0, bs>>>(EJ, n)));
       for (int c = 0; c < n; ++c) {
         init[c] = SolverScalars{};
         init[c].tol_rel = p[c].poisson.tol_rel;
@@ -1766,8 +1794,8 @@ extern "C" int impact_b200_batch_step(impact_b200_batch* b, const impact_b200_st
         r.b_two = res[c].b_two;
         record_solve(&st[c], sub, r);
       }
-      IMPACT_PROF(prof::K_PROJECT, 7.0 * 8.0 * cells, bs, (k_b_project<<<b->ex_blocks, bl, 0, bs>>>(EJ, n)));
-      k_b_scale_pre<<<b->ex_blocks, bl, 0, bs>>>(EJ, n, sub, 1);
+      IMPACT_PROF(prof::K_PROJECT, 7.0 * 8.0 * cells, bs, (k_b_project<<<b->ex_pblocks, bl, 0, bs>>>(EJ, n)));
+      k_b_scale_pre<<<b->ex_pblocks, bl, 0, bs>>>(EJ, n, sub, 1);
       prof::count(1);
     }
     // mask forcing at the new time and level_pressure of every case
@@ -1777,12 +1805,12 @@ extern "C" int impact_b200_batch_step(impact_b200_batch* b, const impact_b200_st
       st[c].time += dt[c];
       lp = lp || p[c].level_pressure;
     }
-    k_b_mask<<<b->ex_blocks, bl, 0, bs>>>(EJ, n);
+    k_b_mask<<<b->ex_pblocks, bl, 0, bs>>>(EJ, n);
     prof::count(1);
     if (lp) {
       k_b_sum<<<b->ex_blocks, bl, 0, bs>>>(EJ, n);
       k_b_reduce<<<n, 1024, 0, bs>>>(EJ, 0, 1, 1, nullptr);
-      k_b_sub_mean<<<b->ex_blocks, bl, 0, bs>>>(EJ, n);
+      k_b_sub_mean<<<b->ex_pblocks, bl, 0, bs>>>(EJ, n);
       prof::count(3);
     }
   }

@@ -11,11 +11,14 @@ from impact_b200 import geometry as G
 pytestmark = pytest.mark.gpu
 
 # the 22 x 20 x 40 case (n1 not divisible by 4) runs the FP32 operator's staged kernel, the others
-# its vector kernel: in a batch both kernels run, each on its own cases
+# its vector kernel; the 19 x 20 x 40 case (n1 odd) also the FP64 operator's staged kernel (the
+# FP64 batch and the mixed solve's outer residual): in a batch both kernels run, each on its own
+# cases
 SPECS = [((17, 17, 33), 200.0, 1.0, [(1.0, 0.5, 0.125)]),
          ((25, 21, 41), 500.0, 0.7, []),
          ((33, 33, 65), 350.0, 1.3, [(0.6, 0.4, 0.1), (1.4, 0.6, 0.15)]),
-         ((23, 21, 41), 300.0, 0.9, [])]
+         ((23, 21, 41), 300.0, 0.9, []),
+         ((20, 21, 41), 250.0, 1.1, [(1.0, 0.5, 0.1)])]
 
 
 def _make(spec, precision, explicit_fp32=0):
@@ -55,3 +58,26 @@ def test_batch_rejects_mixed_precisions():
     b, _ = _make(SPECS[1], 1)
     with pytest.raises(I.ImpactError):
         I.Batch([a, b])
+
+
+@pytest.mark.parametrize("precision,explicit_fp32", [(0, 0), (1, 1)], ids=["fp64", "mixed-fp32-rhs"])
+def test_batch_rhs_depth_does_not_change_results(precision, explicit_fp32):
+    """A batch's rhs_vel blocks take their z depth from the whole batch (10 planes for these three
+    cases together, 8 for each alone): the pass's arithmetic per point does not depend on it."""
+    specs = [((129, 129, 257), 400.0, 1.0, [(1.0, 0.5, 0.1)]),
+             ((97, 97, 193), 300.0, 0.8, []),
+             ((65, 65, 129), 500.0, 1.2, [(0.8, 0.4, 0.1)])]
+    alone = []
+    for spec in specs:
+        case, p = _make(spec, precision, explicit_fp32)
+        case.step(p, 1)
+        alone.append([case.download(f) for f in ("vel1", "vel2", "vel3", "pre")])
+        case.close()
+    made = [_make(spec, precision, explicit_fp32) for spec in specs]
+    batch = I.Batch([c for c, _ in made])
+    batch.step([p for _, p in made])
+    for (case, _), ref in zip(made, alone):
+        assert all(s == 0 for s in case.state.poisson_status)
+        for a, b in zip([case.download(f) for f in ("vel1", "vel2", "vel3", "pre")], ref):
+            assert np.array_equal(a, b)
+    batch.close()
