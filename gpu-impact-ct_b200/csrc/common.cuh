@@ -76,6 +76,7 @@ struct SolverScalars {
   int max_it;
   int done;       // 1 once converged or out of iterations: every later kernel is a no-op
   int status;     // 0 ok, 1 max iterations, 2 breakdown, 3 non-finite, 4 shadow residual lost
+  int phi_zero;   // 1 until the first x update: phi holds no value yet and that update starts from 0
 };
 
 }  // namespace impact

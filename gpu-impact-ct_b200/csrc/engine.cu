@@ -162,7 +162,8 @@ __device__ void e_scalar_update(int mode, const double* q, SolverScalars* sc) {
       else
         sc->omega = q[0] / q[1];
       break;
-    case EFIN_NORMS: {
+    case EFIN_NORMS: {  // after an x update
+      sc->phi_zero = 0;
       sc->norm_inf = q[0];
       sc->norm_two_sq = q[1];
       sc->rhr_next = q[2];
@@ -265,7 +266,8 @@ __global__ void k_ebegin(SolverScalars* __restrict__ scal, int n) {
 // ------------------------------------------------------------------------------------------
 // BiCGstab vector kernels over the Krylov job list
 // ------------------------------------------------------------------------------------------
-// initial residual: rr = bb - rr (rr = A phi), or rr = bb with phi = 0; rh = rr
+// initial residual: rr = bb - rr (rr = A phi), or rr = bb from phi = 0 (zero_phi 1: phi = 0
+// written; 2: not written, the first x update starts from 0, SolverScalars::phi_zero); rh = rr
 // partials [max|rr|, sum rr^2, rr.rh, sum bb^2]
 template <typename T>
 __global__ void __launch_bounds__(ENT) k_kr_init(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts,
@@ -290,7 +292,7 @@ __global__ void __launch_bounds__(ENT) k_kr_init(const KrylovJob<T>* __restrict_
       auto point = [&](long long q, T bv, T a) {
         T r;
         if (zero_phi) {
-          phi[q] = T(0);
+          if (zero_phi == 1) phi[q] = T(0);
           r = bv;
         } else {
           r = bv - a;
@@ -424,6 +426,7 @@ __global__ void __launch_bounds__(ENT) k_kr_x(const KrylovJob<T>* __restrict__ j
       T* __restrict__ phi = J.phi;
       T* __restrict__ rr = J.rr;
       const T om = (T)sc->omega, al = (T)sc->alpha;
+      const bool pz = sc->phi_zero != 0;  // the first update of a solve started from 0 without phi = 0
       constexpr int U = Ublk<T>::U;
       const long long nxy = g.nxy;
       long long p = off(g, i, j, k0);
@@ -443,7 +446,7 @@ __global__ void __launch_bounds__(ENT) k_kr_x(const KrylovJob<T>* __restrict__ j
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const long long q = p + u * nxy;
-          ph[u] = phi[q];
+          ph[u] = pz ? T(0) : phi[q];
           a2[u] = z2[q];
           a1[u] = z1[q];
           r0[u] = rr[q];
@@ -453,7 +456,7 @@ __global__ void __launch_bounds__(ENT) k_kr_x(const KrylovJob<T>* __restrict__ j
 #pragma unroll
         for (int u = 0; u < U; ++u) point(p + u * nxy, ph[u], a2[u], a1[u], r0[u], ar[u], h[u]);
       }
-      for (; k <= k1; ++k, p += nxy) point(p, phi[p], z2[p], z1[p], rr[p], Ar[p], rh[p]);
+      for (; k <= k1; ++k, p += nxy) point(p, pz ? T(0) : phi[p], z2[p], z1[p], rr[p], Ar[p], rh[p]);
     }
     tile_partials<3, 1>(v, partial + (long long)b * 4);
   }
@@ -2692,7 +2695,7 @@ __global__ void __launch_bounds__(ENT) k_mx_apply(const MixJob* __restrict__ job
     if (osc[q].done) continue;
     const MixJob& J = jobs[q];
     const int st = J.isc->status;
-    if (st != 0 && st != 1) continue;
+    if ((st != 0 && st != 1) || J.isc->phi_zero) continue;  // no correction (or none written)
     const Geom g = J.g;
     int i, j, k0, k1;
     tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
@@ -3364,6 +3367,7 @@ int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::
     scal_host_[c] = init[c];
     scal_host_[c].it = 0;
     scal_host_[c].status = 0;
+    scal_host_[c].phi_zero = zero_phi == 2 ? 1 : 0;
     if (!init[c].done) max_it = std::max(max_it, init[c].max_it);
   }
   cudaError_t e = cudaMemcpyAsync(scal_, scal_host_, n * sizeof(SolverScalars), cudaMemcpyHostToDevice, s_);
@@ -3758,7 +3762,7 @@ int MixedEngine::solve(const std::vector<SolverScalars>& outer, double inner_tol
     if (!any) break;
     rc = push_flags();
     if (rc) return rc;
-    rc = inner_.solve(init, 1, ir);
+    rc = inner_.solve(init, 2, ir);  // e from 0, not written before the first x update
     if (rc) return rc;
     for (int c = 0; c < n; ++c) {
       if (init[c].done) continue;

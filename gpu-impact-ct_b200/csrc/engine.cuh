@@ -165,7 +165,9 @@ class Engine {
 
   int build(const std::vector<EngineCase<T>>& cs, const EngineParams& p, cudaStream_t s);
   // BiCGstab on every case.  init[c] carries tol_rel, tol_abs_inf and max_it of case c; a case
-  // with init[c].done = 1 is skipped.  zero_phi: start from phi = 0 (init_yes).
+  // with init[c].done = 1 is skipped.  zero_phi: 1 start from phi = 0 (init_yes); 2 the same
+  // without writing phi = 0 (the first x update starts from 0; a solve that ends before it
+  // leaves phi unwritten and SolverScalars::phi_zero set).
   int solve(const std::vector<SolverScalars>& init, int zero_phi, std::vector<SolverResult>& res);
   // one application of the preconditioner of every case: z1 = M pp
   int apply_precond();
