@@ -2175,21 +2175,20 @@ __global__ void __launch_bounds__(ENT, 2) k_lv_prolong(const LevelJob<T>* __rest
 constexpr int MPF = 2;  // planes staged ahead of the newest one in use
 const dim3 kMBlock(32, MNT / 32);
 
-template <typename T, int S, bool INIT, int PS = S>
+template <typename T, int S, bool INIT>
 struct MLayout {
   static constexpr int V = VecT<T>::W;
   static constexpr int W0 = 16 * V, H0 = 2 * MNT / 32, R0 = W0 * H0;
   static constexpr int NBR = S + 1 + MPF;  // A ring: planes t-S .. t+MPF
   static constexpr int NCR = MPF + 1;      // C ring (POST): planes t .. t+MPF
-  static constexpr int pub() { return 0; }                   // 2 slots x PS published stages x R0
-  static constexpr int rhs() { return 2 * PS * R0; }        // NBR x R0
+  static constexpr int pub() { return 0; }                   // 2 slots x S stages x R0
+  static constexpr int rhs() { return 2 * S * R0; }         // NBR x R0
   static constexpr int cin() { return rhs() + NBR * R0; }   // NCR x R0 (POST only)
   static constexpr int total() { return cin() + (INIT ? 0 : NCR * R0); }
 };
-template <typename T, int NSW, bool INIT, bool RES, bool RST = false>
+template <typename T, int NSW, bool INIT, bool RES>
 constexpr size_t multi_smem_bytes() {
-  constexpr int S = NSW + (RES ? 1 : 0);
-  return sizeof(T) * (size_t)MLayout<T, S, INIT, S + (RST ? 1 : 0)>::total();
+  return sizeof(T) * (size_t)MLayout<T, NSW + (RES ? 1 : 0), INIT>::total();
 }
 
 // periodic image of index i in 1..n, for any integer i
@@ -2219,32 +2218,18 @@ __device__ __forceinline__ void sload(const T* p, T (&o)[VecT<T>::W]) {
 // 16-byte vector of the field (a periodic wrap never splits it): one 16-byte cp.async per plane
 // and vector stores of the outputs; the z coefficients are constants.  Otherwise HX = S and
 // every column moves on its own.
-// RST (pre-smoothing on the fast path, every job coarsened by 2 on every axis): the residual is
-// restricted into the next coarser level's right-hand side here instead of being stored for
-// k_lv_restrict.  The tile then keeps one more row and column of halo (the residual next to the
-// tile's outputs: Y = H0 - 2S - 2, HX >= S + 1) and marches one more plane before k0, and its
-// first output row, column and plane are odd (a coarse point's 7-point stencil lies in the tile:
-// kc even).
-// The residual of each plane is published like a stage's rows; when the residual of plane k
-// (even) is done, the coarse point of plane k-1 gets restrict7 of the residual at k-2 .. k (own
-// registers) and of the rows and column next to it (published one step earlier): the operations
-// of k_lv_restrict on the same values.
-template <typename T, int NSW, bool INIT, bool RES, bool FAST, bool RST = false>
+template <typename T, int NSW, bool INIT, bool RES, bool FAST>
 __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
                                                      int nj, int ntiles, T omega) {
   constexpr int S = NSW + (RES ? 1 : 0);
-  static_assert(!RST || (INIT && RES && FAST), "the restriction is fused into the fast pre-smoothing only");
-  constexpr int PS = S + (RST ? 1 : 0);  // published stages (the residual too with RST)
-  constexpr int SY = S + (RST ? 1 : 0);  // rows before the first output row; also planes before k0
-  using LY = MLayout<T, S, INIT, PS>;
+  using LY = MLayout<T, S, INIT>;
   constexpr int V = LY::V;
   constexpr int W0 = LY::W0, H0 = LY::H0, R0 = LY::R0, NBR = LY::NBR, NCR = LY::NCR;
-  constexpr int HX = FAST ? (SY + V - 1) / V * V : S;  // x halo of the region (RST: > S, so that the
-                                                       // residual left of the outputs is there)
-  constexpr int X = W0 - 2 * HX, Y = H0 - 2 * SY;
+  constexpr int HX = FAST ? (S + V - 1) / V * V : S;  // x halo of the region
+  constexpr int X = W0 - 2 * HX, Y = H0 - 2 * S;
   extern __shared__ __align__(16) unsigned char lm_raw[];
   T* const sm = reinterpret_cast<T*>(lm_raw);
-  T* const pub = sm + LY::pub();  // pub[(slot * PS + s) * R0 + y * W0 + x]
+  T* const pub = sm + LY::pub();  // pub[(slot * S + s) * R0 + y * W0 + x]
   T* const br = sm + LY::rhs();
   T* const cr = sm + LY::cin();
   const int x0 = V * (threadIdx.x & 15);               // this thread's first column in the region
@@ -2261,7 +2246,7 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
     const int ta = t0 % ntx, tr = t0 / ntx, tc = tr / nty;
     const int i0 = ta * X + 1, j0 = (tr - tc * nty) * Y + 1;  // first output column of the tile
     const int k0 = tc * kc + 1, k1 = min(g.n3, k0 + kc - 1);
-    const int nq = (k1 - k0 + 1) + S + SY;  // planes k0-SY .. k1+S
+    const int nq = (k1 - k0 + 1) + 2 * S;  // planes k0-S .. k1+S
     const T* __restrict__ cz = J.cdg[2];
     const bool zu = FAST || J.zuni != 0;
     T a0[V], a1[V], a2[V], inv[V];
@@ -2274,7 +2259,7 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
       a2[c] = J.cdg[0][3 * (gi - 1) + 2];
       xo[c] = gi + 3;
     }
-    const int gj = wrapn(j0 - SY + y, g.n2);
+    const int gj = wrapn(j0 - S + y, g.n2);
     const T b0 = J.cdg[1][3 * (gj - 1)], b1 = J.cdg[1][3 * (gj - 1) + 1], b2 = J.cdg[1][3 * (gj - 1) + 2];
     const int yo = g.nx * (gj + 3);
     const T zcm = cz[0], zcc = cz[1], zcp = cz[2];  // the z row of a uniform z axis
@@ -2296,15 +2281,12 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
       }
     }
     // outputs of this thread: columns i = io + c of row jo, when its vector lies in the tile interior
-    const int io = i0 + x0 - HX, jo = j0 + y - SY;
-    const bool rowout = y >= SY && y < H0 - SY && jo <= g.n2;
-    // RST: the thread writes coarse points when its row is an odd output row and its vector
-    // (first column odd) lies in the tile's outputs
-    const bool cwrite = RST && rowout && (jo & 1) && x0 >= HX && x0 < W0 - HX && io <= g.n1;
+    const int io = i0 + x0 - HX, jo = j0 + y - S;
+    const bool rowout = y >= S && y < H0 - S && jo <= g.n2;
     const long long obase = (long long)(io + 3) + (long long)g.nx * (jo + 3);
     const T* __restrict__ Ab = J.A + yo + (FAST ? xo[0] : 0);
     const T* __restrict__ Cb = J.C + yo + (FAST ? xo[0] : 0);
-    int kin = wrapn(k0 - SY, g.n3);  // wrapped plane of the next stage_in
+    int kin = wrapn(k0 - S, g.n3);  // wrapped plane of the next stage_in
     auto stage_in = [&](int qq) {  // plane qq of A (and of C) at this thread's columns
       if (qq < nq) {
         const long long zo = (long long)(kin + 3) * g.nxy;
@@ -2332,9 +2314,6 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
     for (int s = 0; s < S; ++s)
 #pragma unroll
       for (int c = 0; c < V; ++c) Qz[s][c][0] = Qz[s][c][1] = Qz[s][c][2] = T(0);
-    T rp1[RST ? V : 1], rp2[RST ? V : 1];  // RST: the residual at the last two planes
-#pragma unroll
-    for (int c = 0; c < (RST ? V : 1); ++c) rp1[c] = rp2[c] = T(0);
     // one step; R = t % 3 at compile time, so that every window slot is a fixed register
     auto step = [&](int t, auto rt) {
       constexpr int R = decltype(rt)::value;
@@ -2343,7 +2322,7 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
       stage_in(t + MPF);
       const int wslot = t & 1, rslot = wslot ^ 1;
       {  // stage 0 at plane t
-        const T cc = zu ? zcc : cz[3 * (wrapn(k0 - SY + t, g.n3) - 1) + 1];
+        const T cc = zu ? zcc : cz[3 * (wrapn(k0 - S + t, g.n3) - 1) + 1];
         T v[V];
         sload(INIT ? br + (t % NBR) * R0 + e0 : cr + (t % NCR) * R0 + e0, v);
 #pragma unroll
@@ -2351,7 +2330,7 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
           if (INIT) v[c] = jinit(v[c], omega, zu, inv[c], a1[c] + b1 + cc);
           Qz[0][c][R] = v[c];
         }
-        vstore(pub + (wslot * PS + 0) * R0 + e0, v);
+        vstore(pub + (wslot * S + 0) * R0 + e0, v);
       }
 #pragma unroll
       for (int s = 1; s <= S; ++s) {
@@ -2360,8 +2339,8 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
         const int sm1 = ((R - s - 1) % 3 + 3) % 3, s0 = ((R - s) % 3 + 3) % 3, sp1 = ((R - s + 1) % 3 + 3) % 3;
         if (qs >= s) {
           const bool rowin = y >= s && y < H0 - s;  // the row lies inside stage s's region
-          const T* pr = pub + (rslot * PS + (s - 1)) * R0;  // stage s-1 at plane qs (published at t-1)
-          const int kk = k0 - SY + qs;  // unwrapped; the outputs (s == S) lie in k0..k1
+          const T* pr = pub + (rslot * S + (s - 1)) * R0;  // stage s-1 at plane qs (published at t-1)
+          const int kk = k0 - S + qs;  // unwrapped; the outputs (s == S) lie in k0..k1
           T cm = zcm, cc = zcc, cp = zcp;
           if (!zu) {
             const int k3 = 3 * (wrapn(kk, g.n3) - 1);
@@ -2433,12 +2412,12 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
                 }
               }
             }
-            if (s == S && rowout && (!RST || kk >= k0)) {  // the outputs: B = x_NSW, C = the residual
+            if (s == S && rowout) {  // the outputs: B = the last sweep (or x_NSW), C = the residual
               const long long ob = obase + (long long)g.nxy * (kk + 3);
               if constexpr (FAST) {
                 if (x0 >= HX && x0 < W0 - HX && io <= g.n1) {
                   vstore(J.B + ob, ov);
-                  if (RES && !RST) vstore(J.C + ob, rv);
+                  if (RES) vstore(J.C + ob, rv);
                 }
               } else {
 #pragma unroll
@@ -2449,33 +2428,11 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
                   }
               }
             }
-            if constexpr (RST) {
-              if (s == S) {
-                // plane kk - 1 odd, within the tile: its coarse points (odd columns io + c, c even)
-                if ((kk & 1) == 0 && kk - 1 >= k0 && kk - 1 <= k1 && cwrite) {
-                  const T* rr = pub + (rslot * PS + S) * R0;  // the residual at kk - 1
-                  const Geom& gc = J.gc;
-#pragma unroll
-                  for (int c = 0; c < V; c += 2) {
-                    const T xm = c == 0 ? rr[y * W0 + x0 - 1] : rp1[c - 1];
-                    const T v7 = restrict7(rp1[c], xm, rp1[c + 1], rr[(y - 1) * W0 + x0 + c], rr[(y + 1) * W0 + x0 + c],
-                                           rp2[c], rv[c]);
-                    J.Ac[off(gc, (io + c + 1) / 2, (jo + 1) / 2, kk / 2)] = v7;
-                  }
-                }
-                vstore(pub + (wslot * PS + S) * R0 + e0, rv);
-#pragma unroll
-                for (int c = 0; c < V; ++c) {
-                  rp2[c] = rp1[c];
-                  rp1[c] = rv[c];
-                }
-              }
-            }
           }
           if (s < S) {
 #pragma unroll
             for (int c = 0; c < V; ++c) Qz[s][c][s0] = ov[c];
-            vstore(pub + (wslot * PS + s) * R0 + e0, ov);
+            vstore(pub + (wslot * S + s) * R0 + e0, ov);
           }
         }
       }
@@ -2794,14 +2751,6 @@ void ax_attributes() {
                        (int)multi_smem_bytes<T, N, I, R>());                                                    \
   cudaFuncSetAttribute(k_lv_multi<T, N, I, R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,              \
                        (int)multi_smem_bytes<T, N, I, R>())
-  cudaFuncSetAttribute(k_lv_multi<float, 1, true, true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)multi_smem_bytes<float, 1, true, true, true>());
-  cudaFuncSetAttribute(k_lv_multi<float, 2, true, true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)multi_smem_bytes<float, 2, true, true, true>());
-  cudaFuncSetAttribute(k_lv_multi<double, 1, true, true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)multi_smem_bytes<double, 1, true, true, true>());
-  cudaFuncSetAttribute(k_lv_multi<double, 2, true, true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)multi_smem_bytes<double, 2, true, true, true>());
   IMPACT_MULTI_ATTR(float, 1, true, true);
   IMPACT_MULTI_ATTR(float, 2, true, true);
   IMPACT_MULTI_ATTR(float, 2, false, false);
@@ -2941,7 +2890,6 @@ void Engine<T>::release() {
   cells_f_.clear();
   cells_c_.clear();
   fast_.clear();
-  rst_.clear();
   cs_.clear();
   built_ = false;
 }
@@ -3076,7 +3024,6 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
         J.cI[m] = L.cI[m];
       }
       J.Bc = Cc.B;
-      J.Ac = Cc.A;
     }
     J.sc = scal_ + c;
     return J;
@@ -3101,8 +3048,7 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
   // the restriction lists keep one column per thread.  fusedS > 0: a list of the fused smoothing
   // kernel with S stencil stages (its own tile shape; tile depth per job, deep enough to stream,
   // shallow enough to give every SM a few tiles)
-  auto add_list = [&](const std::vector<std::pair<int, int>>& members, int variant, bool vec = true, int fusedS = 0,
-                      bool rst = false) {
+  auto add_list = [&](const std::vector<std::pair<int, int>>& members, int variant, bool vec = true, int fusedS = 0) {
     std::vector<LevelJob<T>> jobs;
     std::vector<int> tiles;
     double c = 0.0, f = 0.0, cc = 0.0;
@@ -3117,7 +3063,7 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
       if (!vec) jobs.back().vw = 1;
     }
     auto tiles_at_kc = [&](const LevelJob<T>& J, int kcj) {
-      return fusedS > 0 ? tiles_multi(J.g, kcj, (int)sizeof(T), fusedS, mfast, rst) : tiles_of(J.g, kcj, J.vw);
+      return fusedS > 0 ? tiles_multi(J.g, kcj, (int)sizeof(T), fusedS, mfast) : tiles_of(J.g, kcj, J.vw);
     };
     // tile depth of the list: the engine's (the deepest for the fused kernels), halved while the
     // list has fewer than two tiles per SM, so that the small coarse levels march short columns
@@ -3136,10 +3082,8 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
       if (nsm <= 0) nsm = 148;
       double best = 0.0;
-      // (with the restriction fused: even depths, one plane more per tile)
       for (int kcj = KC_MAX; kcj >= 1; --kcj) {
-        if (rst && (kcj & 1)) continue;
-        const double cost = (double)((total_at(kcj) + nsm - 1) / nsm) * (kcj + 2 * fusedS + 4 + (rst ? 1 : 0));
+        const double cost = (double)((total_at(kcj) + nsm - 1) / nsm) * (kcj + 2 * fusedS + 4);
         if (kcj == KC_MAX || cost < best) {
           best = cost;
           kcl = kcj;
@@ -3158,21 +3102,7 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
     }
     const int id = arena_.add(jobs, tiles);
     note(id, c, f, cc, fast);
-    rst_.resize(id + 1, 0);
-    rst_[id] = rst ? 1 : 0;
     return id;
-  };
-  // the pre-smoothing of a level list can restrict its residual itself when every job takes the
-  // fast path and is coarsened by 2 on every axis to a level with a right-hand side; FP32 only
-  // (measured: the FP32 V-cycle gains, the FP64 one, whose fused kernels hold fewer columns per
-  // thread, loses 5 %)
-  auto rst_ok = [&](const std::vector<std::pair<int, int>>& members, int variant) {
-    if (!std::is_same<T, float>::value || members.empty()) return false;
-    for (auto& m : members) {
-      const LevelJob<T> Jt = lvjob(m.first, m.second, variant);
-      if (Jt.vw != VecT<T>::W || !Jt.zuni || !Jt.Ac || Jt.rc[0] != 2 || Jt.rc[1] != 2 || Jt.rc[2] != 2) return false;
-    }
-    return true;
   };
   std::vector<int> nlev(n, 1);
   int gmax = 1;
@@ -3211,7 +3141,7 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
       for (int c = 0; c < n; ++c)
         if (nlev[c] >= g + 2 && in_lists(c, g)) m.push_back({c, g});
       down[g] = add_list(m, 0);
-      if (spre) dpre[g] = add_list(m, 0, true, spre, rst_ok(m, 0));
+      if (spre) dpre[g] = add_list(m, 0, true, spre);
       if (spost) dpost[g] = add_list(m, 0, true, spost);
     }
     for (int g = 1; g < gmax; ++g) {  // restriction into level g (into a tail's first level too)
@@ -3252,7 +3182,7 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
           if (lt[c] >= 0) tc += vol(cs[c].mg->lv[lt[c]].g);
         note(taill, tc, 0.0, 0.0);
       }
-      if (spre) dpre[0] = add_list(m0, v, true, spre, rst_ok(m0, v));
+      if (spre) dpre[0] = add_list(m0, v, true, spre);
       if (spost) dpost[0] = add_list(m0, v, true, spost);
       if (v == 0) {
         down0_ = down0;
@@ -3269,7 +3199,7 @@ int Engine<T>::build(const std::vector<EngineCase<T>>& cs, const EngineParams& p
           smooth(sch, D, 1, p_.mg_down);
           sch.push_back({PH_RESID, D, 0});
         }
-        if (!(spre && rst_[dpre[g]])) sch.push_back({PH_RESTRICT, rs[g + 1], 0});  // else fused
+        sch.push_back({PH_RESTRICT, rs[g + 1], 0});
       }
       smooth(sch, botl, 1, p_.mg_bottom);  // relax_bottom
       smooth(sch, botl, 0, p_.mg_bottom);
@@ -3320,16 +3250,7 @@ void launch_multi(bool fast, const LevelJob<T>* J, const DevList& L, T om, cudaS
         J, L.ts, L.njobs, L.ntiles, om);
 }
 template <typename T>
-void launch_multi_pre(int sweeps, bool fast, bool rst, const LevelJob<T>* J, const DevList& L, T om, cudaStream_t s) {
-  if (rst) {  // the fast path with the restriction fused
-    if (sweeps == 2)
-      k_lv_multi<T, 1, true, true, true, true><<<grid_multi(L.ntiles), kMBlock, multi_smem_bytes<T, 1, true, true, true>(), s>>>(
-          J, L.ts, L.njobs, L.ntiles, om);
-    else
-      k_lv_multi<T, 2, true, true, true, true><<<grid_multi(L.ntiles), kMBlock, multi_smem_bytes<T, 2, true, true, true>(), s>>>(
-          J, L.ts, L.njobs, L.ntiles, om);
-    return;
-  }
+void launch_multi_pre(int sweeps, bool fast, const LevelJob<T>* J, const DevList& L, T om, cudaStream_t s) {
   if (sweeps == 2)
     launch_multi<T, 1, true, true>(fast, J, L, om, s);
   else
@@ -3378,9 +3299,7 @@ void Engine<T>::enqueue_phase(const Phase& ph) {
       IMPACT_PROF(prof::K_MG_OTHER, sz * (2 * c + cc), s, (k_lv_prolong<T><<<grid, kBlock, 0, s>>>(J, L.ts, L.njobs, L.ntiles, ph.flip)));
       break;
     case PH_PRE:  // mg_down 2 or 3
-      IMPACT_PROF(prof::K_MG_PRE, 3 * sz * c, s,
-                  launch_multi_pre<T>(p_.mg_down, fast_[ph.list] != 0, (int)rst_.size() > ph.list && rst_[ph.list],
-                                      J, L, om, s));
+      IMPACT_PROF(prof::K_MG_PRE, 3 * sz * c, s, launch_multi_pre<T>(p_.mg_down, fast_[ph.list] != 0, J, L, om, s));
       break;
     case PH_POST:  // mg_up 2 or 3
       IMPACT_PROF(prof::K_MG_POST, 3 * sz * c, s, launch_multi_post<T>(p_.mg_up, fast_[ph.list] != 0, J, L, om, s));

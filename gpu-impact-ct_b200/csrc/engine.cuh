@@ -36,12 +36,10 @@ inline int tiles_of(const Geom& g, int kc, int vw = 1) {
 // columns, kc planes deep.
 constexpr int MNT = 512;
 // fast: the aligned path (every job with n1 divisible by V = 16 / sz and uniform z), whose x halo
-// is S rounded up to V; rst: the pre-smoothing with the restriction fused (one more halo row and
-// column on each side)
-inline int tiles_multi(const Geom& g, int kc, int sz, int S, bool fast, bool rst = false) {
-  const int SY = S + (rst ? 1 : 0);
-  const int V = 16 / sz, HX = fast ? (SY + V - 1) / V * V : S;
-  const int X = 16 * V - 2 * HX, Y = MNT / 16 - 2 * SY;
+// is S rounded up to V
+inline int tiles_multi(const Geom& g, int kc, int sz, int S, bool fast) {
+  const int V = 16 / sz, HX = fast ? (S + V - 1) / V * V : S;
+  const int X = 16 * V - 2 * HX, Y = MNT / 16 - 2 * S;
   return ((g.n1 + X - 1) / X) * ((g.n2 + Y - 1) / Y) * ((g.n3 + kc - 1) / kc);
 }
 
@@ -60,13 +58,11 @@ struct LevelJob {
   Geom gf;
   int rf[3];
   const T* Cf;
-  // prolongation into this level from the next coarser one (and, in the pre-smoothing with the
-  // restriction fused, the coarser level's right-hand side Ac)
+  // prolongation into this level from the next coarser one
   Geom gc;
   int rc[3];
   const T* cI[3];
   const T* Bc;
-  T* Ac;
   const SolverScalars* sc;
 };
 
@@ -217,7 +213,6 @@ class Engine {
   // the profiler)
   std::vector<double> cells_, cells_f_, cells_c_;
   std::vector<char> fast_;  // per list: every job vectorised with uniform z (k_lv_fast)
-  std::vector<char> rst_;   // per pre-smoothing list: the restriction is fused into it
   int kr_vec_ = 0;          // FP32 Krylov list: jobs in the vector kernel -- 0 none, 1 all, 2 some
 };
 

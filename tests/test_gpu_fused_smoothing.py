@@ -5,10 +5,9 @@ the prolongation) of a level run as one z-marching kernel instead of one launch 
 They must give the iterate of the one-sweep-per-launch schedule bit for bit (same operations per
 point in the same order), for every sweep count that has a fused kernel (2..4), on equidistant,
 stretched (z rows differ: the non-uniform path) and ragged grids whose sizes do not fill the
-64 x 16 / 32 x 16 / x 8 column tiles, in FP64 and FP32 (one V-cycle; the FP32 fast-path
-pre-smoothing coarsened by 2 on every axis also restricts its residual itself) and in the inner
-solve of the mixed-precision Poisson solve; and one V-cycle with 2 and 3 sweeps must agree with
-the oracle's multigridV to 1e-12.
+64 x 16 / 32 x 16 / x 8 column tiles, in FP64 and FP32 (one V-cycle) and in the inner solve of
+the mixed-precision Poisson solve; and one V-cycle with 2 and 3 sweeps must agree with the
+oracle's multigridV to 1e-12.
 """
 import numpy as np
 import pytest
@@ -23,7 +22,7 @@ GRIDS = [((17, 17, 33), (1.0, 1.0, 2.0), (0, 0, 0)),     # 16 x 16 x 32
          ((33, 25, 17), (1.0, 0.8, 1.0), (1, 1, 0)),     # stretched x, y
          ((25, 13, 49), (1.0, 0.5, 2.0), (0, 0, 1)),     # stretched z (per-plane diagonal)
          ((70, 41, 150), (2.0, 1.0, 3.0), (0, 0, 0)),    # 69 x 40 x 149: ragged tiles and z chunks
-         ((129, 65, 33), (1.0, 0.5, 0.25), (0, 0, 0))]   # 128 x 64 x 32: ragged x / y tiles, fused restriction
+         ((129, 65, 33), (1.0, 0.5, 0.25), (0, 0, 0))]   # 128 x 64 x 32: ragged x / y tiles of the fast path
 GIDS = ["16x16x32", "32x24x16-xy", "24x12x48-z", "69x40x149", "128x64x32"]
 SWEEPS = [(2, 2, 2), (3, 3, 3), (4, 4, 4), (2, 3, 4), (3, 2, 1)]
 
@@ -37,8 +36,7 @@ def _params(sw, unfused, omega=0.8, **kw):
 @pytest.mark.parametrize("gi", range(len(GRIDS)), ids=GIDS)
 @pytest.mark.parametrize("sw", SWEEPS, ids=lambda s: "%d%d%d" % s)
 def test_fused_vcycle_equals_one_sweep_per_launch(gi, sw, precision):
-    """precision 1: the FP32 V-cycle of the mixed solve's inner solve (the one whose fast-path
-    pre-smoothing restricts its residual itself)."""
+    """precision 1: the FP32 V-cycle of the mixed solve's inner solve."""
     N, L, kinds = GRIDS[gi]
     og, ig = O.Grid(N, L, kinds), I.Grid(N, L, kinds)
     case = I.Case(ig, precision=precision)
