@@ -24,7 +24,7 @@ namespace impact {
 
 namespace {
 
-enum EFin { EFIN_RAW = 0, EFIN_INIT, EFIN_ALPHA, EFIN_OMEGA, EFIN_NORMS, EFIN_RESET };
+enum EFin { EFIN_RAW = 0, EFIN_INIT, EFIN_ALPHA, EFIN_OMEGA, EFIN_NORMS, EFIN_RESET, EFIN_INIT_EXT };
 
 __device__ __forceinline__ bool e_halted(const SolverScalars* sc) { return sc->done | sc->status; }
 
@@ -134,10 +134,11 @@ __device__ __forceinline__ void tile_partials(double (&v)[NQ], double* __restric
 // ------------------------------------------------------------------------------------------
 __device__ void e_scalar_update(int mode, const double* q, SolverScalars* sc) {
   switch (mode) {
-    case EFIN_INIT:  // q = [max|r|, sum r^2, r.rh, sum b^2]
+    case EFIN_INIT:      // q = [max|r|, sum r^2, r.rh, sum b^2]
+    case EFIN_INIT_EXT:  // r = rh = b (from 0): q = [max|r|, -, -, sum r^2] of the caller's kernel
       sc->norm_inf = q[0];
-      sc->norm_two_sq = q[1];
-      sc->rhr_next = q[2];
+      sc->norm_two_sq = mode == EFIN_INIT ? q[1] : q[3];
+      sc->rhr_next = mode == EFIN_INIT ? q[2] : q[3];
       sc->b_two_sq = q[3];
       sc->rhr = 0.0;
       sc->alpha = sc->omega = sc->beta = 0.0;
@@ -145,7 +146,7 @@ __device__ void e_scalar_update(int mode, const double* q, SolverScalars* sc) {
       sc->status = 0;
       sc->done = (q[0] == 0.0) ? 1 : 0;  // the reference iterates at least once unless r == 0
       if (sc->max_it <= 0) sc->done = 1;
-      if (!isfinite(q[0]) || !isfinite(q[1])) sc->status = 3;
+      if (!isfinite(q[0]) || !isfinite(sc->norm_two_sq)) sc->status = 3;
       break;
     case EFIN_ALPHA:
       sc->rhAp = q[0];
@@ -200,7 +201,7 @@ __global__ void __launch_bounds__(256) k_efin(const int* __restrict__ ts, const 
   if (sc) {
     if (mode == EFIN_RESET) {
       if (sc->status != 4) return;
-    } else if (mode == EFIN_INIT) {
+    } else if (mode == EFIN_INIT || mode == EFIN_INIT_EXT) {
       if (sc->done) return;
     } else if (mode != EFIN_RAW) {
       if (e_halted(sc)) return;
@@ -632,7 +633,7 @@ __global__ void __launch_bounds__(AXNT, 2) k_kr_ax(const KrylovJob<T>* __restric
     for (int l = 5; l < AXW; ++l) za[l] = zb[l] = T(0);
 #pragma unroll
     for (int l = 0; l < AX_R - 1; ++l) stage(k0 + l);
-    double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
     const long long ob0 = (long long)(k0 + 3) * nxy + own0, ob1 = (long long)(k0 + 3) * nxy + own1;
     auto walk = [&](auto zreg) {
       constexpr bool ZR = decltype(zreg)::value;
@@ -689,15 +690,21 @@ __global__ void __launch_bounds__(AXNT, 2) k_kr_ax(const KrylovJob<T>* __restric
           if (in0) {
             const double bv = (double)dring[sl][pa];
             const double res = bv - (double)ra;
-            J.r32[ob0 + dz] = (float)res;
+            const float rf = (float)res;
+            J.r32[ob0 + dz] = rf;
+            if (J.r32b) J.r32b[ob0 + dz] = rf;
             v0 = fmax(v0, fabs(res));
             v1 += res * res;
             v2 += bv * bv;
+            v3 += (double)rf * (double)rf;
           }
           if (in1) {
             const double bv = (double)dring[sl][pb];
             const double res = bv - (double)rb;
-            J.r32[ob1 + dz] = (float)res;
+            const float rf = (float)res;
+            J.r32[ob1 + dz] = rf;
+            if (J.r32b) J.r32b[ob1 + dz] = rf;
+            v3 += (double)rf * (double)rf;
             v0 = fmax(v0, fabs(res));
             v1 += res * res;
             v2 += bv * bv;
@@ -734,8 +741,8 @@ __global__ void __launch_bounds__(AXNT, 2) k_kr_ax(const KrylovJob<T>* __restric
       double v[2] = {v0, v1};
       tile_partials<2, 0, AXNT>(v, partial + (long long)b * 4);
     } else if (MODE == 3) {
-      double v[3] = {v0, v1, v2};
-      tile_partials<3, 1, AXNT>(v, partial + (long long)b * 4);
+      double v[4] = {v0, v1, v2, v3};
+      tile_partials<4, 1, AXNT>(v, partial + (long long)b * 4);
     } else {
       __syncthreads();  // the ring and the weights are rewritten by the next tile
     }
@@ -1306,7 +1313,7 @@ __global__ void __launch_bounds__(AXD_NT, 2) k_kr_ax64v(const KrylovJob<double>*
   double* ring = reinterpret_cast<double*>(axd_smem);
   double* pring = ring + (size_t)AXD_R * AXD_PLANE;
   double(*wzs)[AXW] = reinterpret_cast<double(*)[AXW]>(pring + (size_t)AXD_R * AXD_PP);
-  __shared__ double red[3][AXD_NT / 32];
+  __shared__ double red[4][AXD_NT / 32];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + AXD_TX * ty;
   const int cx = 8 + 2 * tx;          // the thread's first column in a staged row
@@ -1376,7 +1383,7 @@ __global__ void __launch_bounds__(AXD_NT, 2) k_kr_ax64v(const KrylovJob<double>*
     const double2 zero2 = make_double2(0.0, 0.0);
 #pragma unroll
     for (int l = 0; l < AXD_ZW; ++l) win[l] = act ? ldg2d(x + zoff(k0 - 5 + l) + own) : zero2;
-    double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
     const long long obase = (long long)(k0 + 3) * nxy + own;
     const int nsteps = (nk + AXD_B - 1) / AXD_B;
     for (int s = 0; s < nsteps; ++s) {
@@ -1433,7 +1440,11 @@ __global__ void __launch_bounds__(AXD_NT, 2) k_kr_ax64v(const KrylovJob<double>*
             if (MODE == 3) {
               const double2 bv = lds2d(pring + (size_t)(t % AXD_R) * AXD_PP + pq);
               const double e0 = bv.x - r0, e1 = bv.y - r1;
-              *reinterpret_cast<float2*>(J.r32 + o) = make_float2((float)e0, (float)e1);
+              const float2 ef = make_float2((float)e0, (float)e1);
+              *reinterpret_cast<float2*>(J.r32 + o) = ef;
+              if (J.r32b) *reinterpret_cast<float2*>(J.r32b + o) = ef;
+              v3 += (double)ef.x * (double)ef.x;
+              v3 += (double)ef.y * (double)ef.y;
               v0 = fmax(v0, fmax(fabs(e0), fabs(e1)));
               v1 += e0 * e0;
               v1 += e1 * e1;
@@ -1465,23 +1476,29 @@ __global__ void __launch_bounds__(AXD_NT, 2) k_kr_ax64v(const KrylovJob<double>*
       v0 = MODE == 3 ? e_wmax(v0) : e_wsum(v0);
       v1 = e_wsum(v1);
       v2 = e_wsum(v2);
+      v3 = e_wsum(v3);
       if ((tid & 31) == 0) {
         red[0][tid >> 5] = v0;
         red[1][tid >> 5] = v1;
         red[2][tid >> 5] = v2;
+        red[3][tid >> 5] = v3;
       }
       __syncthreads();
       if (tid == 0) {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll
         for (int w = 0; w < AXD_NT / 32; ++w) {
           s0 = MODE == 3 ? fmax(s0, red[0][w]) : s0 + red[0][w];
           s1 += red[1][w];
           s2 += red[2][w];
+          s3 += red[3][w];
         }
         partial[(long long)b * 4] = s0;
         if (MODE >= 2) partial[(long long)b * 4 + 1] = s1;
-        if (MODE == 3) partial[(long long)b * 4 + 2] = s2;
+        if (MODE == 3) {
+          partial[(long long)b * 4 + 2] = s2;
+          partial[(long long)b * 4 + 3] = s3;
+        }
       }
     }
   }
@@ -3358,7 +3375,8 @@ int Engine<T>::poll(bool& all_done) {
 }
 
 template <typename T>
-int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::vector<SolverResult>& res) {
+int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::vector<SolverResult>& res,
+                     const int* ext_ts, const double* ext_partial) {
   if (!built_) return impact_set_error_msg(-1, "engine: not built");
   const int n = (int)cs_.size();
   if ((int)init.size() != n) return impact_set_error_msg(-1, "engine: wrong number of initial scalars");
@@ -3375,14 +3393,19 @@ int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::
   const DevList& K = arena_.lists[kr_list_];
   const KrylovJob<T>* J = static_cast<const KrylovJob<T>*>(K.jobs);
   const int grid = grid_for(K.ntiles);
-  if (!zero_phi) {
-    launch_ax<T, 0>(grid, J, K.ts, n, K.ntiles, partial_, s_, kr_vec_);
+  if (zero_phi && ext_partial) {  // rr = rh = bb and their norms come from the caller's kernel
+    k_efin<<<n, 256, 0, s_>>>(ext_ts, ext_partial, 4, 1, EFIN_INIT_EXT, scal_, nullptr);
+    prof::count(1);
+  } else {
+    if (!zero_phi) {
+      launch_ax<T, 0>(grid, J, K.ts, n, K.ntiles, partial_, s_, kr_vec_);
+      prof::count(1);
+    }
+    IMPACT_PROF(prof::K_KR_INIT, 4.0 * sizeof(T) * cells_[kr_list_], s_,
+                (k_kr_init<T><<<grid, kBlock, 0, s_>>>(J, K.ts, n, K.ntiles, zero_phi, partial_)));
+    k_efin<<<n, 256, 0, s_>>>(K.ts, partial_, 4, 1, EFIN_INIT, scal_, nullptr);
     prof::count(1);
   }
-  IMPACT_PROF(prof::K_KR_INIT, 4.0 * sizeof(T) * cells_[kr_list_], s_,
-              (k_kr_init<T><<<grid, kBlock, 0, s_>>>(J, K.ts, n, K.ntiles, zero_phi, partial_)));
-  k_efin<<<n, 256, 0, s_>>>(K.ts, partial_, 4, 1, EFIN_INIT, scal_, nullptr);
-  prof::count(1);
   const int chunk = p_.check_every > 0 ? p_.check_every : 1;
   const bool profiling = prof::enabled();
   if (graph_ && graph_prof_ != profiling) {  // the profiler was switched: capture again
@@ -3632,9 +3655,11 @@ int MixedEngine::build(const std::vector<Case>& cs, const EngineParams& p, cudaS
     A.bb = C.bb;
     A.rr = C.r64;
     A.r32 = C.r32;
+    A.r32b = C.inner.rr;  // the inner solve's first residual, written with r32
     A.sc = oscal_ + c;
     A.vec = C.g.n1 % 2 == 0 && C.g.n1 >= 8 && (reinterpret_cast<uintptr_t>(C.x) & 15) == 0 &&
-            (reinterpret_cast<uintptr_t>(C.bb) & 15) == 0 && (reinterpret_cast<uintptr_t>(C.r32) & 7) == 0;
+            (reinterpret_cast<uintptr_t>(C.bb) & 15) == 0 && (reinterpret_cast<uintptr_t>(C.r32) & 7) == 0 &&
+            (reinterpret_cast<uintptr_t>(C.inner.rr) & 7) == 0;
     MixJob& M = mj[c];
     M = MixJob{};
     M.g = C.g;
@@ -3742,7 +3767,7 @@ int MixedEngine::solve(const std::vector<SolverScalars>& outer, double inner_tol
         done[c] = 1;
         continue;
       }
-      // inner FP32 solve A e = r / |r|_inf from e = 0
+      // inner FP32 solve A e = r from e = 0
       double tol = inner_tol;
       int mit = inner_max_it;
       if (retries[c] > 0) {
@@ -3762,7 +3787,8 @@ int MixedEngine::solve(const std::vector<SolverScalars>& outer, double inner_tol
     if (!any) break;
     rc = push_flags();
     if (rc) return rc;
-    rc = inner_.solve(init, 2, ir);  // e from 0, not written before the first x update
+    // e from 0, not written before the first x update; rr and the norms from the residual kernel
+    rc = inner_.solve(init, 2, ir, AL.ts, partial_);
     if (rc) return rc;
     for (int c = 0; c < n; ++c) {
       if (init[c].done) continue;
