@@ -2148,9 +2148,11 @@ __device__ __forceinline__ void prolong_cols_x2(const LevelJob<T>& J, const Geom
 }
 
 // this (fine) level: B += P Bc (interpolate, mod_solvers.f90:955-1141); with flip, C = B + P Bc
-// (B unchanged) for the fused smoothing that follows
+// (B unchanged) for the fused smoothing that follows.  Latency-bound: FP32 runs at 3 blocks per
+// SM (80 registers, a few spilled: 0.22 against 0.24 ms at 384 x 384 x 768), FP64 at 2 (its
+// spills at 3 cost more than the warps gain)
 template <typename T>
-__global__ void __launch_bounds__(ENT, 2) k_lv_prolong(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
+__global__ void __launch_bounds__(ENT, sizeof(T) == 4 ? 3 : 2) k_lv_prolong(const LevelJob<T>* __restrict__ jobs, const int* __restrict__ ts,
                                                     int nj, int ntiles, int flip) {
   for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
     const int q = find_job(ts, nj, b);
