@@ -338,7 +338,8 @@ __global__ void __launch_bounds__(ENT) k_kr_p(const KrylovJob<T>* __restrict__ j
     int i, j, k0, k1;
     tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
     if (i > g.n1 || j > g.n2) continue;
-    const T* __restrict__ rr = J.rr;
+    // first iteration of a solve whose caller wrote r0 to rh alone: pp = rh
+    const T* __restrict__ rr = (sc->it == 1 && sc->rr_in_rh) ? J.rh : J.rr;
     const T* __restrict__ Ap = J.Ap;
     T* __restrict__ pp = J.pp;
     constexpr int U = 2 * Ublk<T>::U;
@@ -372,7 +373,8 @@ __global__ void __launch_bounds__(ENT) k_kr_p(const KrylovJob<T>* __restrict__ j
   }
 }
 
-// rr = rr - alpha Ap
+// rr = rr - alpha Ap (in the first iteration of a solve whose caller wrote r0 to rh alone:
+// rr = rh - alpha Ap)
 template <typename T>
 __global__ void __launch_bounds__(ENT) k_kr_r(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts, int nj,
                                               int ntiles) {
@@ -386,7 +388,8 @@ __global__ void __launch_bounds__(ENT) k_kr_r(const KrylovJob<T>* __restrict__ j
     tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
     if (i > g.n1 || j > g.n2) continue;
     const T* __restrict__ Ap = J.Ap;
-    T* __restrict__ rr = J.rr;
+    const T* rs = (sc->it == 1 && sc->rr_in_rh) ? J.rh : J.rr;  // rr itself, or rh (see above)
+    T* rr = J.rr;
     const T al = (T)sc->alpha;
     constexpr int U = 2 * Ublk<T>::U;
     const long long nxy = g.nxy;
@@ -396,13 +399,13 @@ __global__ void __launch_bounds__(ENT) k_kr_r(const KrylovJob<T>* __restrict__ j
       T r[U], a[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        r[u] = rr[p + u * nxy];
+        r[u] = rs[p + u * nxy];
         a[u] = Ap[p + u * nxy];
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) rr[p + u * nxy] = r[u] - al * a[u];
     }
-    for (; k <= k1; ++k, p += nxy) rr[p] = rr[p] - al * Ap[p];
+    for (; k <= k1; ++k, p += nxy) rr[p] = rs[p] - al * Ap[p];
   }
 }
 
@@ -476,10 +479,12 @@ __global__ void __launch_bounds__(ENT) k_kr_reset(const KrylovJob<T>* __restrict
     tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
     double v[1] = {0.0};
     if (i <= g.n1 && j <= g.n2) {
+      // in the first iteration of a solve whose caller wrote r0 to rh alone, rh already is rr
+      const bool keep = J.sc->it == 1 && J.sc->rr_in_rh;
       long long p = off(g, i, j, k0);
       for (int k = k0; k <= k1; ++k, p += g.nxy) {
-        const T r = J.rr[p];
-        J.rh[p] = r;
+        const T r = keep ? J.rh[p] : J.rr[p];
+        if (!keep) J.rh[p] = r;
         v[0] += (double)r * (double)r;
       }
     }
@@ -692,7 +697,6 @@ __global__ void __launch_bounds__(AXNT, 2) k_kr_ax(const KrylovJob<T>* __restric
             const double res = bv - (double)ra;
             const float rf = (float)res;
             J.r32[ob0 + dz] = rf;
-            if (J.r32b) J.r32b[ob0 + dz] = rf;
             v0 = fmax(v0, fabs(res));
             v1 += res * res;
             v2 += bv * bv;
@@ -703,7 +707,6 @@ __global__ void __launch_bounds__(AXNT, 2) k_kr_ax(const KrylovJob<T>* __restric
             const double res = bv - (double)rb;
             const float rf = (float)res;
             J.r32[ob1 + dz] = rf;
-            if (J.r32b) J.r32b[ob1 + dz] = rf;
             v3 += (double)rf * (double)rf;
             v0 = fmax(v0, fabs(res));
             v1 += res * res;
@@ -1442,7 +1445,6 @@ __global__ void __launch_bounds__(AXD_NT, 2) k_kr_ax64v(const KrylovJob<double>*
               const double e0 = bv.x - r0, e1 = bv.y - r1;
               const float2 ef = make_float2((float)e0, (float)e1);
               *reinterpret_cast<float2*>(J.r32 + o) = ef;
-              if (J.r32b) *reinterpret_cast<float2*>(J.r32b + o) = ef;
               v3 += (double)ef.x * (double)ef.x;
               v3 += (double)ef.y * (double)ef.y;
               v0 = fmax(v0, fmax(fabs(e0), fabs(e1)));
@@ -3388,6 +3390,7 @@ int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::
     scal_host_[c].it = 0;
     scal_host_[c].status = 0;
     scal_host_[c].phi_zero = zero_phi == 2 ? 1 : 0;
+    scal_host_[c].rr_in_rh = zero_phi && ext_partial ? 1 : 0;
     if (!init[c].done) max_it = std::max(max_it, init[c].max_it);
   }
   cudaError_t e = cudaMemcpyAsync(scal_, scal_host_, n * sizeof(SolverScalars), cudaMemcpyHostToDevice, s_);
@@ -3395,7 +3398,7 @@ int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::
   const DevList& K = arena_.lists[kr_list_];
   const KrylovJob<T>* J = static_cast<const KrylovJob<T>*>(K.jobs);
   const int grid = grid_for(K.ntiles);
-  if (zero_phi && ext_partial) {  // rr = rh = bb and their norms come from the caller's kernel
+  if (zero_phi && ext_partial) {  // rh = bb = r0 and its norms come from the caller's kernel (rr unwritten)
     k_efin<<<n, 256, 0, s_>>>(ext_ts, ext_partial, 4, 1, EFIN_INIT_EXT, scal_, nullptr);
     prof::count(1);
   } else {
@@ -3626,7 +3629,13 @@ int MixedEngine::build(const std::vector<Case>& cs, const EngineParams& p, cudaS
   s_ = s;
   const int n = (int)cs.size();
   std::vector<EngineCase<float>> ic;
-  for (const Case& c : cs) ic.push_back(c.inner);
+  for (const Case& c : cs) {
+    // the outer residual writes r0 once, into the inner solve's right-hand side, which must also
+    // be its shadow residual (the inner solve starts from e = 0)
+    if (c.inner.bb != c.r32 || c.inner.rh != c.r32)
+      return impact_set_error_msg(-1, "mixed engine: the inner bb and rh must be the FP32 residual buffer");
+    ic.push_back(c.inner);
+  }
   int rc = inner_.build(ic, p, s);
   if (rc) return rc;
   const int kc = inner_.params().kc;
@@ -3657,11 +3666,9 @@ int MixedEngine::build(const std::vector<Case>& cs, const EngineParams& p, cudaS
     A.bb = C.bb;
     A.rr = C.r64;
     A.r32 = C.r32;
-    A.r32b = C.inner.rr;  // the inner solve's first residual, written with r32
     A.sc = oscal_ + c;
     A.vec = C.g.n1 % 2 == 0 && C.g.n1 >= 8 && (reinterpret_cast<uintptr_t>(C.x) & 15) == 0 &&
-            (reinterpret_cast<uintptr_t>(C.bb) & 15) == 0 && (reinterpret_cast<uintptr_t>(C.r32) & 7) == 0 &&
-            (reinterpret_cast<uintptr_t>(C.inner.rr) & 7) == 0;
+            (reinterpret_cast<uintptr_t>(C.bb) & 15) == 0 && (reinterpret_cast<uintptr_t>(C.r32) & 7) == 0;
     MixJob& M = mj[c];
     M = MixJob{};
     M.g = C.g;

@@ -78,8 +78,7 @@ struct KrylovJob {
   const T* bb;
   T* phi;
   T *rr, *rh, *pp, *Ap, *Ar, *z1, *z2;
-  float* r32;  // mixed precision: FP32 image of the FP64 outer residual
-  float* r32b; // and its second copy, the inner solve's first residual rr (null: none)
+  float* r32;  // mixed precision: FP32 image of the FP64 outer residual (the inner solve's bb = rh)
   SolverScalars* sc;
 };
 
@@ -168,9 +167,10 @@ class Engine {
   // BiCGstab on every case.  init[c] carries tol_rel, tol_abs_inf and max_it of case c; a case
   // with init[c].done = 1 is skipped.  zero_phi: 1 start from phi = 0 (init_yes); 2 the same
   // without writing phi = 0 (the first x update starts from 0; a solve that ends before it
-  // leaves phi unwritten and SolverScalars::phi_zero set).  ext_ts / ext_partial (with zero_phi):
-  // rr already holds bb and the caller's tile partials [max|r|, -, -, sum bb^2] (tile offsets
-  // ext_ts) replace the init pass.
+  // leaves phi unwritten and SolverScalars::phi_zero set).  ext_ts / ext_partial (with zero_phi,
+  // rh sharing bb's buffer): the caller's tile partials [max|r|, -, -, sum bb^2] (tile offsets
+  // ext_ts) replace the init pass, and rr is left unwritten: the first iteration reads r0 from rh
+  // (SolverScalars::rr_in_rh).
   int solve(const std::vector<SolverScalars>& init, int zero_phi, std::vector<SolverResult>& res,
             const int* ext_ts = nullptr, const double* ext_partial = nullptr);
   // one application of the preconditioner of every case: z1 = M pp
@@ -233,7 +233,7 @@ class MixedEngine {
     double* r64;
     float* r32;
     float* e32;
-    EngineCase<float> inner;  // bb = r32, phi = e32
+    EngineCase<float> inner;  // bb = rh = r32, phi = e32
   };
   MixedEngine() = default;
   MixedEngine(const MixedEngine&) = delete;
