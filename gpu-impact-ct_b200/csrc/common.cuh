@@ -77,7 +77,7 @@ struct SolverScalars {
   int done;       // 1 once converged or out of iterations: every later kernel is a no-op
   int status;     // 0 ok, 1 max iterations, 2 breakdown, 3 non-finite, 4 shadow residual lost
   int phi_zero;   // 1 until the first x update: phi holds no value yet and that update starts from 0
-  int rr_in_rh;   // 1: rr was not written at the start; the first iteration reads r0 from rh
+  int rr_in_rh;   // 1: the caller wrote r0 to rh and pp, not to rr: the first iteration reads it there
 };
 
 }  // namespace impact

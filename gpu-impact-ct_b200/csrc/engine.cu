@@ -333,13 +333,12 @@ __global__ void __launch_bounds__(ENT) k_kr_p(const KrylovJob<T>* __restrict__ j
     const int q = find_job(ts, nj, b);
     const KrylovJob<T>& J = jobs[q];
     const SolverScalars* sc = J.sc;
-    if (e_halted(sc)) continue;
+    if (e_halted(sc) || (sc->it == 1 && sc->rr_in_rh)) continue;  // (the caller wrote pp = r0)
     const Geom g = J.g;
     int i, j, k0, k1;
     tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
     if (i > g.n1 || j > g.n2) continue;
-    // first iteration of a solve whose caller wrote r0 to rh alone: pp = rh
-    const T* __restrict__ rr = (sc->it == 1 && sc->rr_in_rh) ? J.rh : J.rr;
+    const T* __restrict__ rr = J.rr;
     const T* __restrict__ Ap = J.Ap;
     T* __restrict__ pp = J.pp;
     constexpr int U = 2 * Ublk<T>::U;
@@ -373,7 +372,7 @@ __global__ void __launch_bounds__(ENT) k_kr_p(const KrylovJob<T>* __restrict__ j
   }
 }
 
-// rr = rr - alpha Ap (in the first iteration of a solve whose caller wrote r0 to rh alone:
+// rr = rr - alpha Ap (in the first iteration of a solve whose caller left rr unwritten:
 // rr = rh - alpha Ap)
 template <typename T>
 __global__ void __launch_bounds__(ENT) k_kr_r(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts, int nj,
@@ -479,7 +478,7 @@ __global__ void __launch_bounds__(ENT) k_kr_reset(const KrylovJob<T>* __restrict
     tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
     double v[1] = {0.0};
     if (i <= g.n1 && j <= g.n2) {
-      // in the first iteration of a solve whose caller wrote r0 to rh alone, rh already is rr
+      // in the first iteration of a solve whose caller left rr unwritten, rh already is rr
       const bool keep = J.sc->it == 1 && J.sc->rr_in_rh;
       long long p = off(g, i, j, k0);
       for (int k = k0; k <= k1; ++k, p += g.nxy) {
@@ -697,6 +696,7 @@ __global__ void __launch_bounds__(AXNT, 2) k_kr_ax(const KrylovJob<T>* __restric
             const double res = bv - (double)ra;
             const float rf = (float)res;
             J.r32[ob0 + dz] = rf;
+            if (J.r32p) J.r32p[ob0 + dz] = rf;
             v0 = fmax(v0, fabs(res));
             v1 += res * res;
             v2 += bv * bv;
@@ -707,6 +707,7 @@ __global__ void __launch_bounds__(AXNT, 2) k_kr_ax(const KrylovJob<T>* __restric
             const double res = bv - (double)rb;
             const float rf = (float)res;
             J.r32[ob1 + dz] = rf;
+            if (J.r32p) J.r32p[ob1 + dz] = rf;
             v3 += (double)rf * (double)rf;
             v0 = fmax(v0, fabs(res));
             v1 += res * res;
@@ -1445,6 +1446,7 @@ __global__ void __launch_bounds__(AXD_NT, 2) k_kr_ax64v(const KrylovJob<double>*
               const double e0 = bv.x - r0, e1 = bv.y - r1;
               const float2 ef = make_float2((float)e0, (float)e1);
               *reinterpret_cast<float2*>(J.r32 + o) = ef;
+              if (J.r32p) *reinterpret_cast<float2*>(J.r32p + o) = ef;
               v3 += (double)ef.x * (double)ef.x;
               v3 += (double)ef.y * (double)ef.y;
               v0 = fmax(v0, fmax(fabs(e0), fabs(e1)));
@@ -3398,7 +3400,7 @@ int Engine<T>::solve(const std::vector<SolverScalars>& init, int zero_phi, std::
   const DevList& K = arena_.lists[kr_list_];
   const KrylovJob<T>* J = static_cast<const KrylovJob<T>*>(K.jobs);
   const int grid = grid_for(K.ntiles);
-  if (zero_phi && ext_partial) {  // rh = bb = r0 and its norms come from the caller's kernel (rr unwritten)
+  if (zero_phi && ext_partial) {  // rh = bb = pp = r0 and its norms come from the caller's kernel
     k_efin<<<n, 256, 0, s_>>>(ext_ts, ext_partial, 4, 1, EFIN_INIT_EXT, scal_, nullptr);
     prof::count(1);
   } else {
@@ -3666,9 +3668,11 @@ int MixedEngine::build(const std::vector<Case>& cs, const EngineParams& p, cudaS
     A.bb = C.bb;
     A.rr = C.r64;
     A.r32 = C.r32;
+    A.r32p = C.inner.pp;  // the inner solve's first search direction, written with r32
     A.sc = oscal_ + c;
     A.vec = C.g.n1 % 2 == 0 && C.g.n1 >= 8 && (reinterpret_cast<uintptr_t>(C.x) & 15) == 0 &&
-            (reinterpret_cast<uintptr_t>(C.bb) & 15) == 0 && (reinterpret_cast<uintptr_t>(C.r32) & 7) == 0;
+            (reinterpret_cast<uintptr_t>(C.bb) & 15) == 0 && (reinterpret_cast<uintptr_t>(C.r32) & 7) == 0 &&
+            (reinterpret_cast<uintptr_t>(C.inner.pp) & 7) == 0;
     MixJob& M = mj[c];
     M = MixJob{};
     M.g = C.g;

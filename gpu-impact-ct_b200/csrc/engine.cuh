@@ -79,6 +79,7 @@ struct KrylovJob {
   T* phi;
   T *rr, *rh, *pp, *Ap, *Ar, *z1, *z2;
   float* r32;  // mixed precision: FP32 image of the FP64 outer residual (the inner solve's bb = rh)
+  float* r32p; // and its second copy, the inner solve's first search direction pp (null: none)
   SolverScalars* sc;
 };
 
@@ -169,8 +170,8 @@ class Engine {
   // without writing phi = 0 (the first x update starts from 0; a solve that ends before it
   // leaves phi unwritten and SolverScalars::phi_zero set).  ext_ts / ext_partial (with zero_phi,
   // rh sharing bb's buffer): the caller's tile partials [max|r|, -, -, sum bb^2] (tile offsets
-  // ext_ts) replace the init pass, and rr is left unwritten: the first iteration reads r0 from rh
-  // (SolverScalars::rr_in_rh).
+  // ext_ts) replace the init pass; the caller wrote r0 to pp as well and left rr unwritten: the
+  // first iteration keeps pp and reads r0 from rh (SolverScalars::rr_in_rh).
   int solve(const std::vector<SolverScalars>& init, int zero_phi, std::vector<SolverResult>& res,
             const int* ext_ts = nullptr, const double* ext_partial = nullptr);
   // one application of the preconditioner of every case: z1 = M pp
