@@ -731,7 +731,12 @@ def main():
                                   f"{mixed['ms_dev'] / K:.1f} ms without)"),
                 "all_kernels": {k: {"launches": v[0], "ms": round(v[1], 2),
                                     "GB/s": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] > 0 else None}
-                                for k, v in prof.items() if v[0] > 0}}
+                                for k, v in prof.items() if v[0] > 0},
+                "all_kernels_note": ("launches include those whose work a device-side flag skips (BiCGstab "
+                                     "iterations queued past convergence in a graph chunk; the first p update of "
+                                     "every inner solve, whose pp the outer residual writes), and GB/s counts the "
+                                     "algorithmic bytes of every launch, so it overstates the Krylov updates "
+                                     "(p_update most)")}
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": mixed["ms_dev"] / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner solve / f64 residual+RHS", "data": "synthetic",
