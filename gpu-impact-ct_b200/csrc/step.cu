@@ -1393,6 +1393,10 @@ static void substep_rhs(CaseState& s, const impact_b200_step_params* p, double d
       IMPACT_PROF(prof::K_NL_RHS, nlb, st,
                   launch_rhs_march(m, g, s.c64, multL, mb, ma, use_old, vel[m], s.work, nl[m], rhs[m], st));
   }
+  // divergence2 reads no pressure: it runs before the pressure's first read, so that a deferred
+  // pressure upload overlaps it too
+  IMPACT_PROF(prof::K_DIV2, 4.0 * 8.0 * cells, st,
+              (k_div2<<<gr, bl, 0, st>>>(g, s.c64, rhs[0], rhs[1], rhs[2], s.f[IMPACT_B200_RES])));
   const double ab = aRK[sub] + bRK[sub];
   if (s.pre_wait) {  // a deferred pressure upload: wait for it here, at the step's first read
     cudaStreamWaitEvent(st, s.pre_wait, 0);
@@ -1400,8 +1404,6 @@ static void substep_rhs(CaseState& s, const impact_b200_step_params* p, double d
   }
   k_scale_pre<<<gr, bl, 0, st>>>(g, ab, dt, 0, s.f[IMPACT_B200_PRE]);
   prof::count(1);
-  IMPACT_PROF(prof::K_DIV2, 4.0 * 8.0 * cells, st,
-              (k_div2<<<gr, bl, 0, st>>>(g, s.c64, rhs[0], rhs[1], rhs[2], s.f[IMPACT_B200_RES])));
 }
 
 // projection vel = rhs - G pre and the pressure scaling back (mod_timeint.f90:372)
@@ -1761,6 +1763,7 @@ extern "C" int impact_b200_batch_step(impact_b200_batch* b, const impact_b200_st
       for (int m = 0; m < 3; ++m)
         IMPACT_PROF(prof::K_NL_RHS, (f32 ? (sub != 0 ? 36.0 : 32.0) : (sub != 0 ? 56.0 : 48.0)) * cells, bs,
                     launch_rhs_march_batch(m, b->d_rhs, n, b->rhs_blocks, sub, f32, bs));
+      IMPACT_PROF(prof::K_DIV2, 4.0 * 8.0 * cells, bs, (k_b_div2<<<b->ex_pblocks, bl, 0, bs>>>(EJ, n)));
       for (auto* c : b->cases)
         if (c->s.pre_wait) {  // a deferred pressure upload: wait for it at the first read
           IMPACT_CUDA_CHECK(cudaStreamWaitEvent(bs, c->s.pre_wait, 0));
@@ -1768,7 +1771,6 @@ extern "C" int impact_b200_batch_step(impact_b200_batch* b, const impact_b200_st
         }
       k_b_scale_pre<<<b->ex_pblocks, bl, 0, bs>>>(EJ, n, sub, 0);
       prof::count(1);
-      IMPACT_PROF(prof::K_DIV2, 4.0 * 8.0 * cells, bs, (k_b_div2<<<b->ex_pblocks, bl, 0, bs>>>(EJ, n)));
       for (int c = 0; c < n; ++c) {
         init[c] = SolverScalars{};
         init[c].tol_rel = p[c].poisson.tol_rel;
