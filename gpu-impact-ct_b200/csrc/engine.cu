@@ -2197,6 +2197,9 @@ __global__ void __launch_bounds__(ENT, sizeof(T) == 4 ? 3 : 2) k_lv_prolong(cons
 // Outputs: PRE (INIT, RES): B = x_NSW and C = residual; POST: B = x_NSW.
 constexpr int MPF = 2;  // planes staged ahead of the newest one in use
 const dim3 kMBlock(32, MNT / 32);
+static_assert(MNT / 32 <= 16, "one named barrier per pair of neighbouring warps (ids 1..15)");
+// named barrier `id` (1..15) of two warps, every thread of both warps arriving
+__device__ __forceinline__ void bar_pair(int id) { asm volatile("bar.sync %0, 64;\n" ::"r"(id) : "memory"); }
 
 template <typename T, int S, bool INIT>
 struct MLayout {
@@ -2337,11 +2340,28 @@ __global__ void __launch_bounds__(MNT, 1) k_lv_multi(const LevelJob<T>* __restri
     for (int s = 0; s < S; ++s)
 #pragma unroll
       for (int c = 0; c < V; ++c) Qz[s][c][0] = Qz[s][c][1] = Qz[s][c][2] = T(0);
+    // A warp (rows 2w, 2w+1) reads, of the rows other warps publish, only rows 2w-1 and 2w+2, and
+    // its own rows are read only by warps w-1 and w+1: a step need not wait for the whole block,
+    // only for those two warps.  Warps w, w+1 meet on named barrier w+1 (64 threads, ids 1..15;
+    // 0 is __syncthreads); even warps meet their upper neighbour first, odd warps their lower one,
+    // so every pair completes in one of two rounds and no cycle of waits can form.  Neighbouring
+    // warps are never more than one step apart, so the two publication slots suffice.
+    const int wid = threadIdx.y;  // warp-uniform
+    auto sync_rows = [&]() {
+      const bool lo = wid > 0, hi = wid + 1 < MNT / 32;
+      if (wid & 1) {
+        if (lo) bar_pair(wid);
+        if (hi) bar_pair(wid + 1);
+      } else {
+        if (hi) bar_pair(wid + 1);
+        if (lo) bar_pair(wid);
+      }
+    };
     // one step; R = t % 3 at compile time, so that every window slot is a fixed register
     auto step = [&](int t, auto rt) {
       constexpr int R = decltype(rt)::value;
       cp_wait<MPF - 1>();  // this thread's copies of plane t have landed (only it reads them)
-      __syncthreads();     // the rows published at step t-1 are visible; slot t%2 is free again
+      sync_rows();         // the rows published at step t-1 are visible; slot t%2 is free again
       stage_in(t + MPF);
       const int wslot = t & 1, rslot = wslot ^ 1;
       {  // stage 0 at plane t
