@@ -325,7 +325,8 @@ __global__ void __launch_bounds__(ENT) k_kr_init(const KrylovJob<T>* __restrict_
   }
 }
 
-// pp = rr (first iteration) or pp = rr + beta pp + omega Ap (omega already holds -beta omega)
+// pp = rr (first iteration; nothing when the caller wrote pp = r0, SolverScalars::rr_in_rh) or
+// pp = rr + beta pp + omega Ap (omega already holds -beta omega)
 template <typename T>
 __global__ void __launch_bounds__(ENT) k_kr_p(const KrylovJob<T>* __restrict__ jobs, const int* __restrict__ ts, int nj,
                                               int ntiles) {
@@ -333,7 +334,7 @@ __global__ void __launch_bounds__(ENT) k_kr_p(const KrylovJob<T>* __restrict__ j
     const int q = find_job(ts, nj, b);
     const KrylovJob<T>& J = jobs[q];
     const SolverScalars* sc = J.sc;
-    if (e_halted(sc) || (sc->it == 1 && sc->rr_in_rh)) continue;  // (the caller wrote pp = r0)
+    if (e_halted(sc) || (sc->it == 1 && sc->rr_in_rh)) continue;
     const Geom g = J.g;
     int i, j, k0, k1;
     tile_at(g, J.kc, b - ts[q], i, j, k0, k1);
